@@ -1,0 +1,275 @@
+/*
+ * rcmvs.h — C ABI of the B200-native dense multi-view-stereo path.
+ *
+ * This library replaces the `mvs` crate of RustCOLMAP (census patch-match
+ * stereo + geometric-consistency fusion).  Every entry point below names the
+ * reference function it stands in for (paths are relative to the reference
+ * project root).  The ABI is plain C: POD structs, raw pointers, sizes and an
+ * int status.  No CUDA or torch type appears in a signature.
+ *
+ * Conventions
+ *  - Status: RCMVS_OK (0) on success, a negative RCMVS_E_* code otherwise;
+ *    rcmvs_last_error(ctx) then holds a one-line message.
+ *  - Host buffers are caller-owned unless a function says it allocates
+ *    (rcmvs_points, freed with rcmvs_points_free).
+ *  - One rcmvs_ctx per device.  A context is not thread-safe; separate
+ *    contexts are independent.  All device work of a context runs on its
+ *    own CUDA stream (rcmvs_ctx_stream).
+ *  - Views are supplied at the stereo working resolution: the reference's
+ *    resize to `max_dim` (mvs/src/lib.rs:185-192) is not performed, and a
+ *    view whose long side exceeds opts->max_dim is rejected.
+ *  - Image rows are row-major, pixel (x, y) at index y*w + x.  A pixel's
+ *    centre sits at integer coordinates (sfm-lite/src/geom.rs:28-42).
+ */
+#ifndef RCMVS_H
+#define RCMVS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RCMVS_OK 0
+#define RCMVS_E_ARG (-1)     /* invalid argument (null pointer, bad size, bad index) */
+#define RCMVS_E_CUDA (-2)    /* a CUDA runtime call failed */
+#define RCMVS_E_NOMEM (-3)   /* device or host allocation failed */
+#define RCMVS_E_LIMIT (-4)   /* a documented size limit was exceeded */
+#define RCMVS_E_IO (-5)      /* file output failed */
+#define RCMVS_E_STATE (-6)   /* call order violated (e.g. fuse before depth) */
+
+#define RCMVS_MAX_SOURCES 32 /* support views per reference view */
+
+/* Mirrors `mvs::MvsOptions` (mvs/src/lib.rs:33-54) field for field; the
+ * extension fields at the end have no counterpart there. */
+typedef struct rcmvs_options {
+    uint32_t max_dim;        /* longest image side used for stereo */
+    uint32_t num_sources;    /* support views per reference view (K) */
+    uint32_t sweeps;         /* patch-match sweeps; passes = 2*max(sweeps,1) */
+    uint32_t num_hyp;        /* plane-sweep hypotheses; max(num_hyp,2) used */
+    uint32_t min_consistent; /* min OTHER views agreeing in fusion */
+    uint32_t save_depth_vis; /* accepted and ignored (PNG output is not built) */
+    float cost_thr;          /* max census Hamming fraction of a valid pixel */
+    uint32_t reserved0;
+    double depth_diff;       /* relative depth agreement in fusion */
+    double voxel_rel;        /* voxel cell / robust sparse bbox diagonal */
+    /* ---- extensions (no reference counterpart) ---- */
+    double reproj_px;        /* >0: fusion also requires the forward-backward
+                                reprojection error to be <= reproj_px pixels;
+                                0 = off (reference behaviour) */
+    uint32_t tile_w;         /* stereo tile width in pixels; 0 = tuned default */
+    uint32_t tile_h;         /* stereo tile height in pixels; 0 = tuned default */
+    uint32_t flags;          /* reserved, must be 0 */
+    uint32_t reserved1;
+} rcmvs_options;
+
+/* Fills `MvsOptions::default()` (mvs/src/lib.rs:56-70); extensions off. */
+void rcmvs_options_default(rcmvs_options* opts);
+
+/* One registered view at working resolution.  Replaces `mvs::ViewData`
+ * (mvs/src/lib.rs:86-101) with the grey image as u8 (ViewData.gray is
+ * u8/255 in f32, a strictly monotone map of the same values), the camera
+ * as SIMPLE_RADIAL `Cam{f,cx,cy,k}` (sfm-lite/src/geom.rs:14-20) and the
+ * world->camera pose `Pose{r,t}` (sfm-lite/src/geom.rs:50-54). */
+typedef struct rcmvs_view {
+    int32_t w, h;
+    double f, cx, cy, k;
+    double R[9];             /* row-major world->camera rotation */
+    double t[3];
+    const uint8_t* gray;     /* w*h luma */
+    const uint8_t* rgb;      /* w*h*3 colour, may be NULL when not fusing */
+} rcmvs_view;
+
+/* One depth-estimation job: reference view + ordered support views and the
+ * depth range.  The arguments of `stereo::estimate_depth`
+ * (mvs/src/stereo.rs:234-241). */
+typedef struct rcmvs_job {
+    int32_t ref_idx;
+    int32_t n_src;
+    const int32_t* srcs;     /* n_src view indices, in priority order */
+    double zmin, zmax;
+} rcmvs_job;
+
+/* Per-job host outputs (w*h floats each; normal is 3*w*h, nullable). */
+typedef struct rcmvs_depth_out {
+    float* depth;            /* DepthMap.depth: z in the reference camera, 0 = invalid */
+    float* cost;             /* DepthMap.cost: census Hamming fraction of the kept plane */
+    float* normal;           /* extension: unit plane normal per pixel (nullable) */
+} rcmvs_depth_out;
+
+/* Sparse reconstruction subset the dense stage reads (colmap-io Point3D,
+ * colmap-io/src/lib.rs:91-103).  Track entries are view indices; entries
+ * outside [0, n_views) are ignored, as the reference ignores image ids it
+ * has no view for (mvs/src/lib.rs:227-231). */
+typedef struct rcmvs_sparse {
+    uint64_t n_points;
+    const double* xyz;             /* 3*n_points */
+    const uint64_t* track_offsets; /* n_points+1 */
+    const int32_t* track_views;    /* track_offsets[n_points] entries */
+} rcmvs_sparse;
+
+/* Fused point cloud: the `Vec<(f64,f64,f64,[u8;3])>` of
+ * `fuse::fuse_depth_maps` (mvs/src/fuse.rs:64-71).  Points come out sorted
+ * by voxel key (the reference's HashMap order is unspecified).  Arrays are
+ * allocated by the library; release with rcmvs_points_free. */
+typedef struct rcmvs_points {
+    uint64_t n;
+    double* xyz;             /* 3*n */
+    uint8_t* rgb;            /* 3*n */
+} rcmvs_points;
+void rcmvs_points_free(rcmvs_points* pts);
+
+/* Run statistics: `mvs::MvsStats` (mvs/src/lib.rs:72-79) plus timings. */
+typedef struct rcmvs_stats {
+    uint64_t views;
+    uint64_t views_with_depth;
+    uint64_t dense_points;
+    uint64_t fusion_candidates;
+    float elapsed_s, stereo_s, fuse_s;
+    uint32_t reserved0;
+} rcmvs_stats;
+
+typedef struct rcmvs_ctx rcmvs_ctx;
+
+/* Context on CUDA device `device` (creates its stream). */
+int rcmvs_ctx_create(int device, rcmvs_ctx** out);
+void rcmvs_ctx_destroy(rcmvs_ctx* ctx);
+const char* rcmvs_last_error(const rcmvs_ctx* ctx);
+/* The context's cudaStream_t, as an opaque pointer (for event timing). */
+void* rcmvs_ctx_stream(rcmvs_ctx* ctx);
+/* Blocks until the context's stream has drained. */
+int rcmvs_ctx_synchronize(rcmvs_ctx* ctx);
+const char* rcmvs_version(void);
+
+/* ---------------------------------------------------------------- host API */
+
+/* 7x7 census transform, 48 bits in a u64, bit (dy+3)*7+(dx+3) set iff the
+ * clamped neighbour is darker than the centre.  Replaces `census_map`
+ * (mvs/src/lib.rs:119-142).  Host buffers. */
+int rcmvs_census(rcmvs_ctx* ctx, const uint8_t* gray, int32_t w, int32_t h,
+                 uint64_t* census_out);
+
+/* Depth (+cost, optional normal) map of one reference view.  Replaces
+ * `stereo::estimate_depth` (mvs/src/stereo.rs:234-394). Host buffers. */
+int rcmvs_estimate_depth(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views,
+                         int32_t ref_idx, const int32_t* srcs, int32_t n_src,
+                         double zmin, double zmax, const rcmvs_options* opts,
+                         float* depth_out, float* cost_out, float* normal_out);
+
+/* Many `estimate_depth` calls in one batched launch sequence (the rayon
+ * loop over views at mvs/src/lib.rs:351-374).  outs[i] receives job i. */
+int rcmvs_estimate_depth_batch(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views,
+                               const rcmvs_job* jobs, int32_t n_jobs,
+                               const rcmvs_options* opts, const rcmvs_depth_out* outs);
+
+/* Geometric-consistency fusion + voxel dedup.  Replaces
+ * `fuse::fuse_depth_maps` (mvs/src/fuse.rs:64-215).  depth_maps[v] is a
+ * w*h map of view v or NULL (the reference's `None`); fusion view lists are
+ * CSR: view v checks order[order_offsets[v] .. order_offsets[v+1]]. */
+int rcmvs_fuse_depth_maps(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views,
+                          const float* const* depth_maps,
+                          const int32_t* order_offsets, const int32_t* order,
+                          const double* sparse_xyz, uint64_t n_sparse,
+                          const rcmvs_options* opts, rcmvs_points* out);
+
+/* Binary little-endian PLY, byte-identical to `fuse::write_ply_binary`
+ * (mvs/src/fuse.rs:222-239). */
+int rcmvs_write_ply_binary(const char* path, const double* xyz, const uint8_t* rgb,
+                           uint64_t n);
+
+/* Host glue of `run_mvs` (mvs/src/lib.rs:303-342, :358, :398-418):
+ * co-visibility counts, top-K support views (count >= 10), per-view depth
+ * range, fusion order (sources first).  Outputs (caller-allocated):
+ *   src_offsets[n_views+1], srcs[n_views*num_sources]   (CSR)
+ *   zrange[2*n_views]                                   (zmin, zmax)
+ *   fuse_offsets[n_views+1], fuse_order[n_views*n_views] (CSR)
+ * Views without sources get no depth map and are left out of every fusion
+ * order, as in the reference. */
+int rcmvs_plan(const rcmvs_sparse* sparse, const rcmvs_view* views, int32_t n_views,
+               const rcmvs_options* opts, int32_t* src_offsets, int32_t* srcs,
+               double* zrange, int32_t* fuse_offsets, int32_t* fuse_order);
+
+/* The dense stage of `run_mvs` (mvs/src/lib.rs:294-517) without image
+ * decoding and without writing files: plan, batched stereo for every view
+ * with sources, fusion.  depth_outs (nullable, n_views entries) receive the
+ * depth maps; views without sources get depth 0 / cost 1.  `out` receives
+ * the fused cloud; stats (nullable) the run statistics. */
+int rcmvs_run_mvs(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views,
+                  const rcmvs_sparse* sparse, const rcmvs_options* opts,
+                  const rcmvs_depth_out* depth_outs, rcmvs_points* out,
+                  rcmvs_stats* stats);
+
+/* -------------------------------------------------- device-resident API */
+/* A scene keeps every view's grey/colour image, census, rays, planes,
+ * depth/cost/normal maps and the fused cloud in device memory, so repeated
+ * stereo and fusion calls move no image data across PCIe. */
+typedef struct rcmvs_scene rcmvs_scene;
+
+/* Uploads the views and runs census + ray kernels (device). */
+int rcmvs_scene_create(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views,
+                       rcmvs_scene** out);
+void rcmvs_scene_destroy(rcmvs_scene* scene);
+/* Recomputes census + rays of every view of the scene on the device (the
+ * census_map of mvs/src/lib.rs:198 and the rays of mvs/src/stereo.rs:118-125;
+ * rcmvs_scene_create already ran it once).  Asynchronous. */
+int rcmvs_scene_prepare(rcmvs_ctx* ctx, rcmvs_scene* scene);
+/* Device-resident batched stereo; results stay on the device. Asynchronous
+ * on the context stream. */
+int rcmvs_scene_estimate_depth(rcmvs_ctx* ctx, rcmvs_scene* scene, const rcmvs_job* jobs,
+                               int32_t n_jobs, const rcmvs_options* opts);
+/* Device-resident fusion of the scene's depth maps (views that were the
+ * reference of a job have a map).  *n_points_out gets the fused count
+ * (this call synchronises once to size the output). */
+int rcmvs_scene_fuse(rcmvs_ctx* ctx, rcmvs_scene* scene, const int32_t* order_offsets,
+                     const int32_t* order, const double* sparse_xyz, uint64_t n_sparse,
+                     const rcmvs_options* opts, uint64_t* n_points_out);
+/* Copies one view's maps to host buffers (any pointer may be NULL). */
+int rcmvs_scene_get_depth(rcmvs_ctx* ctx, rcmvs_scene* scene, int32_t view, float* depth,
+                          float* cost, float* normal);
+/* Copies one view's census (w*h u64) to the host. */
+int rcmvs_scene_get_census(rcmvs_ctx* ctx, rcmvs_scene* scene, int32_t view,
+                           uint64_t* census);
+/* Copies the fused cloud (n from rcmvs_scene_fuse) to host buffers; ply_body
+ * (nullable, 15*n bytes) receives the PLY vertex records the device packed. */
+int rcmvs_scene_get_points(rcmvs_ctx* ctx, rcmvs_scene* scene, double* xyz, uint8_t* rgb,
+                           uint8_t* ply_body);
+
+/* ---------------------------------------------------------- diagnostics */
+
+/* `plane_cost` (mvs/src/stereo.rs:158-228) evaluated at every pixel of the
+ * reference view for a caller-given plane field: planes[4*i..] = (nx, ny,
+ * nz, d) and hints[i] (early-abort hint; +inf disables).  cost_out[i] is
+ * bit-identical to the reference (1e9 when aborted); hsum_out (nullable)
+ * receives the integer Hamming sum of the evaluated in-bounds terms, plus
+ * 48 per invalid term. Host buffers. */
+int rcmvs_plane_cost_field(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views,
+                           int32_t ref_idx, const int32_t* srcs, int32_t n_src,
+                           const float* planes, const float* hints, float* cost_out,
+                           int32_t* hsum_out);
+
+/* Number of plane_cost evaluations and 5-term window rows the last
+ * rcmvs_scene_estimate_depth call performed (after gates and early aborts);
+ * counted only when the RCMVS_COUNT environment variable is set at context
+ * creation, else both are 0. */
+int rcmvs_last_work(rcmvs_ctx* ctx, uint64_t* cost_evals, uint64_t* rows);
+
+/* Per-kernel timing with CUDA events recorded on the context stream around
+ * each launch of the stereo and fusion kernels.  enable != 0 starts a new
+ * recording (dropping earlier spans); rcmvs_ctx_kernel_time synchronises and
+ * returns the summed milliseconds and launch count of one kernel name
+ * ("census_rays", "stereo_init", "stereo_pass", "stereo_gate",
+ * "fuse_candidates", "fuse_reduce"). */
+int rcmvs_ctx_timing(rcmvs_ctx* ctx, int enable);
+int rcmvs_ctx_kernel_time(rcmvs_ctx* ctx, const char* name, double* ms_total, uint64_t* launches);
+
+/* Converts n floats with the device's truncating float->int conversion, the
+ * one the cost kernel uses for the reference's `as i32` (stereo.rs:205-206):
+ * truncation toward zero, saturation, NaN -> 0.  Lets tests check those
+ * semantics on the GPU.  Host buffers. */
+int rcmvs_selftest_f2i(rcmvs_ctx* ctx, const float* in, int32_t n, int32_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RCMVS_H */

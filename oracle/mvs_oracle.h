@@ -1,0 +1,75 @@
+/*
+ * mvs_oracle.h — CPU oracle for the dense-MVS path (TEST INFRASTRUCTURE).
+ *
+ * A restatement of the reference `mvs` crate in C++ (mvs/src/stereo.rs,
+ * mvs/src/fuse.rs, the host glue of mvs/src/lib.rs, and Cam/Pose of
+ * sfm-lite/src/geom.rs).  Only the tests, the smoke check and bench.py's CPU
+ * baseline use it, as the checker; the product library never links it.
+ *
+ * PARITY UNPINNED: the reference is Rust, no Rust toolchain exists where this
+ * was built, and the reference ships no tests or golden vectors.  The oracle
+ * is pinned only by hand-derived known answers and by an independent
+ * pure-Python restatement on small inputs (tests/golden/).
+ */
+#ifndef MVS_ORACLE_H
+#define MVS_ORACLE_H
+
+#include <stdint.h>
+#include "../include/rcmvs.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+void orc_census_map(const uint8_t* gray, int32_t w, int32_t h, uint64_t* out);
+
+uint64_t orc_pixel_rng(int32_t x, int32_t y, uint64_t salt);
+uint64_t orc_next_u64(uint64_t* s);
+float orc_uniform(uint64_t* s);
+float orc_gauss(uint64_t* s);
+int32_t orc_f32_to_i32(float v);
+
+void orc_cam_normalize(double f, double cx, double cy, double k, double u, double v,
+                       double* out2);
+
+/* Rays of RefWorkspace::new (f64 normalize cast to f32). */
+void orc_rays(const rcmvs_view* v, float* rx, float* ry);
+/* rs = R_s R_r^T, ts = t_s - rs t_r (f64, cast to f32). */
+void orc_rel_pose(const rcmvs_view* ref, const rcmvs_view* src, float* rs9, float* ts3);
+
+/* plane_cost at every pixel for a given field (see rcmvs_plane_cost_field). */
+int orc_plane_cost_field(const rcmvs_view* views, int32_t n_views, int32_t ref_idx,
+                         const int32_t* srcs, int32_t n_src, const float* planes,
+                         const float* hints, float* cost_out, int32_t* hsum_out,
+                         int32_t nthreads);
+
+/* stereo::estimate_depth.  normal_out nullable.  nthreads<=0: all cores.
+ * work_out (nullable) receives {cost evaluations, 5-term rows}. */
+int orc_estimate_depth(const rcmvs_view* views, int32_t n_views, int32_t ref_idx,
+                       const int32_t* srcs, int32_t n_src, double zmin, double zmax,
+                       const rcmvs_options* opts, float* depth_out, float* cost_out,
+                       float* normal_out, int32_t nthreads, uint64_t* work_out);
+
+/* fuse::fuse_depth_maps.  Output sorted by voxel key (x, then y, then z).
+ * *xyz_out / *rgb_out are malloc'ed; release with orc_free. */
+int orc_fuse_depth_maps(const rcmvs_view* views, int32_t n_views,
+                        const float* const* depth_maps, const int32_t* order_offsets,
+                        const int32_t* order, const double* sparse_xyz, uint64_t n_sparse,
+                        const rcmvs_options* opts, double** xyz_out, uint8_t** rgb_out,
+                        uint64_t* n_out, uint64_t* n_candidates_out, int32_t nthreads);
+void orc_free(void* p);
+
+int orc_write_ply_binary(const char* path, const double* xyz, const uint8_t* rgb,
+                         uint64_t n);
+
+/* Host glue of run_mvs; same output layout as rcmvs_plan.  has_depth
+ * (nullable) marks views that have a depth map; NULL means "every view with
+ * at least one source". */
+int orc_plan(const rcmvs_sparse* sparse, const rcmvs_view* views, int32_t n_views,
+             const rcmvs_options* opts, int32_t* src_offsets, int32_t* srcs,
+             double* zrange, int32_t* fuse_offsets, int32_t* fuse_order);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,102 @@
+"""Loads the in-tree CUDA libraries and declares their C signatures.
+
+There is no CPU fallback: if librcmvs.so is missing or cannot be loaded the
+import raises, and every call reports the library's own error message.
+"""
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_MVS = os.path.join(_HERE, "librcmvs.so")
+_SCENE = os.path.join(_HERE, "librcscene.so")
+_mvs = None
+_scene = None
+
+
+class RcmvsError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"rcmvs error {code}: {msg}")
+        self.code = code
+
+
+def _load(path):
+    if not os.path.exists(path):
+        raise ImportError(
+            f"{os.path.basename(path)} is not built; run `python -m rustcolmap_b200.build` "
+            "(there is no CPU fallback for this path)")
+    return C.CDLL(path)
+
+
+def mvs():
+    global _mvs
+    if _mvs is not None:
+        return _mvs
+    L = _load(_MVS)
+    vp, i32, u64, f64, cp = C.c_void_p, C.c_int32, C.c_uint64, C.c_double, C.c_char_p
+    sig = {
+        "rcmvs_options_default": ([vp], None),
+        "rcmvs_ctx_create": ([C.c_int, vp], C.c_int),
+        "rcmvs_ctx_destroy": ([vp], None),
+        "rcmvs_last_error": ([vp], cp),
+        "rcmvs_ctx_stream": ([vp], vp),
+        "rcmvs_ctx_synchronize": ([vp], C.c_int),
+        "rcmvs_version": ([], cp),
+        "rcmvs_census": ([vp, vp, i32, i32, vp], C.c_int),
+        "rcmvs_estimate_depth": ([vp, vp, i32, i32, vp, i32, f64, f64, vp, vp, vp, vp], C.c_int),
+        "rcmvs_estimate_depth_batch": ([vp, vp, i32, vp, i32, vp, vp], C.c_int),
+        "rcmvs_fuse_depth_maps": ([vp, vp, i32, vp, vp, vp, vp, u64, vp, vp], C.c_int),
+        "rcmvs_write_ply_binary": ([cp, vp, vp, u64], C.c_int),
+        "rcmvs_plan": ([vp, vp, i32, vp, vp, vp, vp, vp, vp], C.c_int),
+        "rcmvs_run_mvs": ([vp, vp, i32, vp, vp, vp, vp, vp], C.c_int),
+        "rcmvs_points_free": ([vp], None),
+        "rcmvs_scene_create": ([vp, vp, i32, vp], C.c_int),
+        "rcmvs_scene_destroy": ([vp], None),
+        "rcmvs_scene_prepare": ([vp, vp], C.c_int),
+        "rcmvs_scene_estimate_depth": ([vp, vp, vp, i32, vp], C.c_int),
+        "rcmvs_scene_fuse": ([vp, vp, vp, vp, vp, u64, vp, vp], C.c_int),
+        "rcmvs_scene_get_depth": ([vp, vp, i32, vp, vp, vp], C.c_int),
+        "rcmvs_scene_get_census": ([vp, vp, i32, vp], C.c_int),
+        "rcmvs_scene_get_points": ([vp, vp, vp, vp, vp], C.c_int),
+        "rcmvs_plane_cost_field": ([vp, vp, i32, i32, vp, i32, vp, vp, vp, vp], C.c_int),
+        "rcmvs_last_work": ([vp, vp, vp], C.c_int),
+        "rcmvs_selftest_f2i": ([vp, vp, i32, vp], C.c_int),
+        "rcmvs_ctx_timing": ([vp, C.c_int], C.c_int),
+        "rcmvs_ctx_kernel_time": ([vp, cp, vp, vp], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    _mvs = L
+    return L
+
+
+def scene():
+    global _scene
+    if _scene is not None:
+        return _scene
+    L = _load(_SCENE)
+    vp, i32 = C.c_void_p, C.c_int32
+    L.rcscene_render.argtypes = [vp, i32, vp, i32, vp, i32, i32, i32, vp, vp, vp]
+    L.rcscene_render.restype = C.c_int
+    L.rcscene_last_error.argtypes = []
+    L.rcscene_last_error.restype = C.c_char_p
+    _scene = L
+    return L
+
+
+def exported_symbols():
+    """Names of the functions declared in include/rcmvs.h."""
+    return list(_SIG_NAMES)
+
+
+_SIG_NAMES = [
+    "rcmvs_options_default", "rcmvs_ctx_create", "rcmvs_ctx_destroy", "rcmvs_last_error",
+    "rcmvs_ctx_stream", "rcmvs_ctx_synchronize", "rcmvs_version", "rcmvs_census",
+    "rcmvs_estimate_depth", "rcmvs_estimate_depth_batch", "rcmvs_fuse_depth_maps",
+    "rcmvs_write_ply_binary", "rcmvs_plan", "rcmvs_run_mvs", "rcmvs_points_free",
+    "rcmvs_scene_create", "rcmvs_scene_destroy", "rcmvs_scene_prepare",
+    "rcmvs_scene_estimate_depth", "rcmvs_scene_fuse", "rcmvs_scene_get_depth",
+    "rcmvs_scene_get_census", "rcmvs_scene_get_points", "rcmvs_plane_cost_field",
+    "rcmvs_last_work", "rcmvs_selftest_f2i", "rcmvs_ctx_timing", "rcmvs_ctx_kernel_time",
+]

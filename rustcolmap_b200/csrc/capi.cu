@@ -1,0 +1,1088 @@
+// capi.cu — the C ABI of librcmvs (include/rcmvs.h): contexts, device-resident
+// scenes, the host-buffer entry points that stand in for the reference `mvs`
+// crate, the run_mvs host glue and the PLY writer.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "rcmvs_internal.cuh"
+
+namespace rcmvs {
+size_t stereo_smem_bytes(TileShape ts);
+cudaError_t stereo_configure(TileShape ts);
+cudaError_t launch_census_rays(const DevView* d_views, const int32_t* d_tile_start, int n_views, int total_tiles,
+                               const uint8_t* gray, uint64_t* census, float2* rays, const double* d_cams,
+                               cudaStream_t st);
+cudaError_t launch_init(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, int total_tiles, TileShape ts,
+                        int nh, const uint64_t* census, const float2* rays, PlaneBuf out, unsigned long long* d_work,
+                        cudaStream_t st);
+cudaError_t launch_pass(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, int total_tiles, TileShape ts,
+                        uint64_t pass, float sig_inv, float sig_n, const uint64_t* census, const float2* rays,
+                        PlaneBuf prev, PlaneBuf next, unsigned long long* d_work, cudaStream_t st);
+cudaError_t launch_gate(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, int total_tiles, TileShape ts,
+                        float cost_thr, const uint64_t* census, PlaneBuf planes, float* depth, float* cost,
+                        float* normal, cudaStream_t st);
+cudaError_t launch_cost_field(const DevJob* d_job, const int32_t* d_job_start, int total_tiles, TileShape ts,
+                              const uint64_t* census, const float2* rays, const float4* planes, const float* hints,
+                              float* cost_out, int32_t* hsum_out, cudaStream_t st);
+cudaError_t launch_f2i(const float* in, int n, int32_t* out, cudaStream_t st);
+
+constexpr int kCensusTileW = 32, kCensusTileH = 8;
+
+cudaError_t DeviceArena::get(int slot, size_t bytes, void** out) {
+    if ((int)slots.size() <= slot) slots.resize(slot + 1);
+    Slot& s = slots[slot];
+    if (bytes == 0) bytes = 16;
+    if (s.bytes < bytes) {
+        if (s.p) {
+            cudaError_t e = cudaFree(s.p);
+            if (e != cudaSuccess) return e;
+            s.p = nullptr;
+            s.bytes = 0;
+        }
+        size_t nb = std::max(bytes, s.bytes + s.bytes / 4);
+        cudaError_t e = cudaMalloc(&s.p, nb);
+        if (e != cudaSuccess) {
+            s.p = nullptr;
+            return e;
+        }
+        s.bytes = nb;
+    }
+    *out = s.p;
+    return cudaSuccess;
+}
+
+void DeviceArena::release() {
+    for (auto& s : slots)
+        if (s.p) cudaFree(s.p);
+    slots.clear();
+}
+
+}  // namespace rcmvs
+
+using namespace rcmvs;
+
+struct rcmvs_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    DeviceArena arena;
+    bool count_work = false;
+    unsigned long long* d_work = nullptr;
+    uint64_t last_evals = 0, last_rows = 0;
+    TileShape configured{0, 0};
+    // per-kernel CUDA-event spans (rcmvs_ctx_timing)
+    struct Span {
+        std::string name;
+        cudaEvent_t a, b;
+    };
+    bool timing = false;
+    std::vector<Span> spans;
+    SpanHook hook() {
+        SpanHook h;
+        if (timing) {
+            h.mark = &rcmvs_ctx::mark_cb;
+            h.user = this;
+        }
+        return h;
+    }
+    static void mark_cb(void* user, const char* name, int begin) {
+        rcmvs_ctx* c = (rcmvs_ctx*)user;
+        if (begin) {
+            Span s;
+            s.name = name;
+            if (cudaEventCreate(&s.a) != cudaSuccess) return;
+            if (cudaEventCreate(&s.b) != cudaSuccess) {
+                cudaEventDestroy(s.a);
+                return;
+            }
+            cudaEventRecord(s.a, c->stream);
+            c->spans.push_back(s);
+        } else if (!c->spans.empty() && c->spans.back().name == name) {
+            cudaEventRecord(c->spans.back().b, c->stream);
+        }
+    }
+    void clear_spans() {
+        for (auto& s : spans) {
+            cudaEventDestroy(s.a);
+            cudaEventDestroy(s.b);
+        }
+        spans.clear();
+    }
+};
+
+struct HostCam {
+    double f, cx, cy, k;
+    double R[9], t[3];
+};
+
+struct rcmvs_scene {
+    rcmvs_ctx* ctx = nullptr;
+    int n_views = 0;
+    int64_t n_px = 0;
+    std::vector<DevView> views;
+    std::vector<HostCam> cams;
+    std::vector<char> has_depth;
+    bool has_rgb = false;
+    int census_tiles = 0;
+    // device buffers
+    uint8_t* gray = nullptr;
+    uint8_t* rgb = nullptr;
+    uint64_t* census = nullptr;
+    float2* rays = nullptr;
+    float4* plane_a = nullptr;
+    float4* plane_b = nullptr;
+    float* pcost_a = nullptr;
+    float* pcost_b = nullptr;
+    float* depth = nullptr;
+    float* cost = nullptr;
+    float* normal = nullptr;
+    DevView* d_views = nullptr;
+    int32_t* d_tile_start = nullptr;
+    double* d_cams = nullptr;
+    DeviceArena arena;  // jobs + fusion scratch/outputs
+    uint64_t n_points = 0;
+    uint64_t n_candidates = 0;
+    double* d_pts_xyz = nullptr;
+    uint8_t* d_pts_rgb = nullptr;
+    uint8_t* d_ply = nullptr;
+};
+
+namespace {
+
+enum { S_JOBS = 0, S_JOBSTART = 1, S_CGRAY = 2, S_CCEN = 3, S_FIELD_PL = 4, S_FIELD_H = 5, S_FIELD_C = 6,
+       S_FIELD_HS = 7, S_F2I = 8 };
+
+int fail(rcmvs_ctx* ctx, int code, const std::string& msg) {
+    if (ctx) ctx->err = msg;
+    return code;
+}
+
+#define CK(x)                                                                                  \
+    do {                                                                                       \
+        cudaError_t e_ = (x);                                                                  \
+        if (e_ != cudaSuccess)                                                                 \
+            return fail(ctx, e_ == cudaErrorMemoryAllocation ? RCMVS_E_NOMEM : RCMVS_E_CUDA,    \
+                        std::string(#x) + ": " + cudaGetErrorString(e_));                      \
+    } while (0)
+
+bool finite(double x) { return std::isfinite(x); }
+
+int check_view(rcmvs_ctx* ctx, const rcmvs_view& v, int i, const rcmvs_options* opts) {
+    if (v.w <= 0 || v.h <= 0 || !v.gray)
+        return fail(ctx, RCMVS_E_ARG, "view " + std::to_string(i) + ": bad size or null gray");
+    if (!(finite(v.f) && v.f != 0.0 && finite(v.cx) && finite(v.cy) && finite(v.k)))
+        return fail(ctx, RCMVS_E_ARG, "view " + std::to_string(i) + ": non-finite or zero intrinsics");
+    for (int q = 0; q < 9; ++q)
+        if (!finite(v.R[q])) return fail(ctx, RCMVS_E_ARG, "view " + std::to_string(i) + ": non-finite pose");
+    for (int q = 0; q < 3; ++q)
+        if (!finite(v.t[q])) return fail(ctx, RCMVS_E_ARG, "view " + std::to_string(i) + ": non-finite pose");
+    if (opts && (uint32_t)std::max(v.w, v.h) > opts->max_dim)
+        return fail(ctx, RCMVS_E_ARG,
+                    "view " + std::to_string(i) + ": long side exceeds max_dim (views must be given at the "
+                    "stereo working resolution)");
+    return RCMVS_OK;
+}
+
+TileShape tile_of(const rcmvs_options* o) {
+    TileShape t{16, 16};
+    if (o && o->tile_w > 0 && o->tile_h > 0) t = TileShape{(int)o->tile_w, (int)o->tile_h};
+    return t;
+}
+
+int ensure_tile(rcmvs_ctx* ctx, TileShape ts) {
+    if (ts.tw <= 0 || ts.th <= 0 || ts.tw * ts.th > 1024 || (ts.tw * ts.th) % 32 != 0 || ts.tw > 256)
+        return fail(ctx, RCMVS_E_ARG, "tile shape must be tw*th <= 1024 and a multiple of 32");
+    if (stereo_smem_bytes(ts) > 200 * 1024) return fail(ctx, RCMVS_E_LIMIT, "tile shape needs too much shared memory");
+    if (ctx->configured.tw != ts.tw || ctx->configured.th != ts.th) {
+        CK(stereo_configure(ts));
+        ctx->configured = ts;
+    }
+    return RCMVS_OK;
+}
+
+// mvs/src/stereo.rs:131-132 in f64, cast to f32 (RefWorkspace::new)
+void rel_pose(const HostCam& r, const HostCam& s, float* rs, float* ts) {
+    double rs64[9];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            rs64[3 * i + j] = s.R[3 * i] * r.R[3 * j] + s.R[3 * i + 1] * r.R[3 * j + 1] + s.R[3 * i + 2] * r.R[3 * j + 2];
+    for (int i = 0; i < 9; ++i) rs[i] = (float)rs64[i];
+    for (int i = 0; i < 3; ++i) {
+        double rt = rs64[3 * i] * r.t[0] + rs64[3 * i + 1] * r.t[1] + rs64[3 * i + 2] * r.t[2];
+        ts[i] = (float)(s.t[i] - rt);
+    }
+}
+
+void fill_job(const rcmvs_scene* sc, int ref, const int32_t* srcs, int n_src, double zmin, double zmax, TileShape ts,
+              DevJob& J) {
+    std::memset(&J, 0, sizeof(J));
+    const DevView& V = sc->views[ref];
+    J.view = ref;
+    J.nsrc = n_src;
+    J.w = V.w;
+    J.h = V.h;
+    J.off = V.off;
+    J.zmin = (float)zmin;
+    J.zmax = (float)zmax;
+    J.inv_min = 1.0f / J.zmax;  // stereo.rs:248-249 (f32)
+    J.inv_max = 1.0f / J.zmin;
+    J.tiles_x = (V.w + ts.tw - 1) / ts.tw;
+    J.tiles_y = (V.h + ts.th - 1) / ts.th;
+    J.tiles = J.tiles_x * J.tiles_y;
+    for (int s = 0; s < n_src; ++s) {
+        const HostCam& c = sc->cams[srcs[s]];
+        DevSrc& D = J.src[s];
+        rel_pose(sc->cams[ref], c, D.rs, D.ts);
+        D.f = (float)c.f;
+        D.cx = (float)c.cx;
+        D.cy = (float)c.cy;
+        D.k = (float)c.k;
+        D.w = sc->views[srcs[s]].w;
+        D.h = sc->views[srcs[s]].h;
+        D.off = sc->views[srcs[s]].off;
+    }
+}
+
+int validate_jobs(rcmvs_ctx* ctx, int n_views, const rcmvs_job* jobs, int n_jobs) {
+    if (n_jobs < 0 || (n_jobs > 0 && !jobs)) return fail(ctx, RCMVS_E_ARG, "bad job list");
+    std::vector<char> seen(n_views, 0);
+    for (int j = 0; j < n_jobs; ++j) {
+        const rcmvs_job& b = jobs[j];
+        if (b.ref_idx < 0 || b.ref_idx >= n_views) return fail(ctx, RCMVS_E_ARG, "job ref_idx out of range");
+        if (seen[b.ref_idx]) return fail(ctx, RCMVS_E_ARG, "two jobs share a reference view");
+        seen[b.ref_idx] = 1;
+        if (b.n_src < 0 || (b.n_src > 0 && !b.srcs)) return fail(ctx, RCMVS_E_ARG, "bad source list");
+        if (b.n_src > RCMVS_MAX_SOURCES)
+            return fail(ctx, RCMVS_E_LIMIT, "more than RCMVS_MAX_SOURCES support views in one job");
+        for (int s = 0; s < b.n_src; ++s)
+            if (b.srcs[s] < 0 || b.srcs[s] >= n_views) return fail(ctx, RCMVS_E_ARG, "source index out of range");
+        if (!(finite(b.zmin) && finite(b.zmax) && b.zmin > 0.0 && b.zmax > 0.0))
+            return fail(ctx, RCMVS_E_ARG, "depth range must be finite and positive");
+    }
+    return RCMVS_OK;
+}
+
+float powf_host(float b, float e) { return powf(b, e); }
+
+}  // namespace
+
+// ================================================================ context
+extern "C" {
+
+const char* rcmvs_version(void) { return "rcmvs 0.1 (sm_100a)"; }
+
+void rcmvs_options_default(rcmvs_options* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->max_dim = 900;  // mvs/src/lib.rs:56-70
+    o->num_sources = 3;
+    o->sweeps = 4;
+    o->num_hyp = 48;
+    o->min_consistent = 2;
+    o->depth_diff = 0.03;
+    o->cost_thr = 0.38f;
+    o->voxel_rel = 0.0015;
+    o->save_depth_vis = 0;
+}
+
+int rcmvs_ctx_create(int device, rcmvs_ctx** out) {
+    if (!out) return RCMVS_E_ARG;
+    *out = nullptr;
+    rcmvs_ctx* ctx = new rcmvs_ctx();
+    ctx->device = device;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || device < 0 || device >= n) {
+        delete ctx;
+        return RCMVS_E_CUDA;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major < 10) {
+        delete ctx;
+        return RCMVS_E_CUDA;  // built for sm_100a only
+    }
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) {
+        delete ctx;
+        return RCMVS_E_CUDA;
+    }
+    const char* cw = std::getenv("RCMVS_COUNT");
+    ctx->count_work = cw && cw[0] && cw[0] != '0';
+    if (ctx->count_work) {
+        if (cudaMalloc(&ctx->d_work, 2 * sizeof(unsigned long long)) != cudaSuccess) {
+            cudaStreamDestroy(ctx->stream);
+            delete ctx;
+            return RCMVS_E_NOMEM;
+        }
+    }
+    *out = ctx;
+    return RCMVS_OK;
+}
+
+void rcmvs_ctx_destroy(rcmvs_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    ctx->arena.release();
+    ctx->clear_spans();
+    if (ctx->d_work) cudaFree(ctx->d_work);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char* rcmvs_last_error(const rcmvs_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+void* rcmvs_ctx_stream(rcmvs_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int rcmvs_ctx_synchronize(rcmvs_ctx* ctx) {
+    if (!ctx) return RCMVS_E_ARG;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return RCMVS_OK;
+}
+
+void rcmvs_points_free(rcmvs_points* p) {
+    if (!p) return;
+    std::free(p->xyz);
+    std::free(p->rgb);
+    p->xyz = nullptr;
+    p->rgb = nullptr;
+    p->n = 0;
+}
+
+// ================================================================ scene
+void rcmvs_scene_destroy(rcmvs_scene* sc) {
+    if (!sc) return;
+    if (sc->ctx) {
+        cudaSetDevice(sc->ctx->device);
+        cudaStreamSynchronize(sc->ctx->stream);
+    }
+    void* ps[] = {sc->gray, sc->rgb, sc->census, sc->rays, sc->plane_a, sc->plane_b, sc->pcost_a, sc->pcost_b,
+                  sc->depth, sc->cost, sc->normal, sc->d_views, sc->d_tile_start, sc->d_cams};
+    for (void* p : ps)
+        if (p) cudaFree(p);
+    sc->arena.release();
+    delete sc;
+}
+
+int rcmvs_scene_prepare(rcmvs_ctx* ctx, rcmvs_scene* sc);
+
+int rcmvs_scene_create(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views, rcmvs_scene** out) {
+    if (!ctx || !views || n_views <= 0 || !out) return fail(ctx, RCMVS_E_ARG, "rcmvs_scene_create: bad argument");
+    *out = nullptr;
+    for (int i = 0; i < n_views; ++i) {
+        int rc = check_view(ctx, views[i], i, nullptr);
+        if (rc) return rc;
+    }
+    CK(cudaSetDevice(ctx->device));
+    rcmvs_scene* sc = new rcmvs_scene();
+    sc->ctx = ctx;
+    sc->n_views = n_views;
+    sc->has_rgb = true;
+    int64_t off = 0;
+    std::vector<int32_t> tile_start;
+    int tiles = 0;
+    for (int i = 0; i < n_views; ++i) {
+        const rcmvs_view& v = views[i];
+        sc->views.push_back(DevView{v.w, v.h, off});
+        HostCam c;
+        c.f = v.f;
+        c.cx = v.cx;
+        c.cy = v.cy;
+        c.k = v.k;
+        std::memcpy(c.R, v.R, sizeof(c.R));
+        std::memcpy(c.t, v.t, sizeof(c.t));
+        sc->cams.push_back(c);
+        if (!v.rgb) sc->has_rgb = false;
+        tile_start.push_back(tiles);
+        tiles += ((v.w + kCensusTileW - 1) / kCensusTileW) * ((v.h + kCensusTileH - 1) / kCensusTileH);
+        off += (int64_t)v.w * v.h;
+    }
+    tile_start.push_back(tiles);
+    sc->census_tiles = tiles;
+    sc->n_px = off;
+    sc->has_depth.assign(n_views, 0);
+    const size_t np = (size_t)off;
+    auto alloc = [&](void** p, size_t bytes) { return cudaMalloc(p, bytes); };
+    cudaError_t e = cudaSuccess;
+    if (!e) e = alloc((void**)&sc->gray, np);
+    if (!e && sc->has_rgb) e = alloc((void**)&sc->rgb, 3 * np);
+    if (!e) e = alloc((void**)&sc->census, 8 * np);
+    if (!e) e = alloc((void**)&sc->rays, 8 * np);
+    if (!e) e = alloc((void**)&sc->plane_a, 16 * np);
+    if (!e) e = alloc((void**)&sc->plane_b, 16 * np);
+    if (!e) e = alloc((void**)&sc->pcost_a, 4 * np);
+    if (!e) e = alloc((void**)&sc->pcost_b, 4 * np);
+    if (!e) e = alloc((void**)&sc->depth, 4 * np);
+    if (!e) e = alloc((void**)&sc->cost, 4 * np);
+    if (!e) e = alloc((void**)&sc->normal, 12 * np);
+    if (!e) e = alloc((void**)&sc->d_views, sizeof(DevView) * n_views);
+    if (!e) e = alloc((void**)&sc->d_tile_start, sizeof(int32_t) * (n_views + 1));
+    if (!e) e = alloc((void**)&sc->d_cams, sizeof(double) * 4 * n_views);
+    if (e) {
+        rcmvs_scene_destroy(sc);
+        return fail(ctx, e == cudaErrorMemoryAllocation ? RCMVS_E_NOMEM : RCMVS_E_CUDA,
+                    std::string("rcmvs_scene_create: ") + cudaGetErrorString(e));
+    }
+    std::vector<double> cams4;
+    for (auto& c : sc->cams) cams4.insert(cams4.end(), {c.f, c.cx, c.cy, c.k});
+    cudaStream_t st = ctx->stream;
+    for (int i = 0; i < n_views && !e; ++i) {
+        const size_t n = (size_t)views[i].w * views[i].h;
+        e = cudaMemcpyAsync(sc->gray + sc->views[i].off, views[i].gray, n, cudaMemcpyHostToDevice, st);
+        if (!e && sc->has_rgb)
+            e = cudaMemcpyAsync(sc->rgb + 3 * sc->views[i].off, views[i].rgb, 3 * n, cudaMemcpyHostToDevice, st);
+    }
+    if (!e) e = cudaMemcpyAsync(sc->d_views, sc->views.data(), sizeof(DevView) * n_views, cudaMemcpyHostToDevice, st);
+    if (!e) e = cudaMemcpyAsync(sc->d_tile_start, tile_start.data(), sizeof(int32_t) * (n_views + 1),
+                                cudaMemcpyHostToDevice, st);
+    if (!e) e = cudaMemcpyAsync(sc->d_cams, cams4.data(), sizeof(double) * cams4.size(), cudaMemcpyHostToDevice, st);
+    if (!e) e = cudaStreamSynchronize(st);  // host vectors above go out of scope
+    if (e) {
+        rcmvs_scene_destroy(sc);
+        return fail(ctx, RCMVS_E_CUDA, std::string("rcmvs_scene_create: ") + cudaGetErrorString(e));
+    }
+    int rc = rcmvs_scene_prepare(ctx, sc);
+    if (rc) {
+        rcmvs_scene_destroy(sc);
+        return rc;
+    }
+    *out = sc;
+    return RCMVS_OK;
+}
+
+// census + rays of every view (kernel a).  Asynchronous.
+int rcmvs_scene_prepare(rcmvs_ctx* ctx, rcmvs_scene* sc) {
+    if (!ctx || !sc) return fail(ctx, RCMVS_E_ARG, "rcmvs_scene_prepare: bad argument");
+    CK(cudaSetDevice(ctx->device));
+    const SpanHook hk = ctx->hook();
+    hk.begin("census_rays");
+    CK(launch_census_rays(sc->d_views, sc->d_tile_start, sc->n_views, sc->census_tiles, sc->gray, sc->census,
+                          sc->rays, sc->d_cams, ctx->stream));
+    hk.end("census_rays");
+    return RCMVS_OK;
+}
+
+int rcmvs_scene_estimate_depth(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job* jobs, int32_t n_jobs,
+                               const rcmvs_options* opts) {
+    if (!ctx || !sc || !opts) return fail(ctx, RCMVS_E_ARG, "rcmvs_scene_estimate_depth: bad argument");
+    if (sc->ctx != ctx) return fail(ctx, RCMVS_E_ARG, "scene belongs to another context");
+    int rc = validate_jobs(ctx, sc->n_views, jobs, n_jobs);
+    if (rc) return rc;
+    for (int j = 0; j < n_jobs; ++j) {
+        const DevView& V = sc->views[jobs[j].ref_idx];
+        if ((uint32_t)std::max(V.w, V.h) > opts->max_dim)
+            return fail(ctx, RCMVS_E_ARG, "reference view long side exceeds max_dim");
+    }
+    if (opts->flags != 0) return fail(ctx, RCMVS_E_ARG, "opts->flags must be 0");
+    if (n_jobs == 0) return RCMVS_OK;
+    const TileShape ts = tile_of(opts);
+    CK(cudaSetDevice(ctx->device));
+    rc = ensure_tile(ctx, ts);
+    if (rc) return rc;
+    std::vector<DevJob> hj(n_jobs);
+    std::vector<int32_t> start(n_jobs + 1);
+    int64_t tiles = 0;
+    for (int j = 0; j < n_jobs; ++j) {
+        fill_job(sc, jobs[j].ref_idx, jobs[j].srcs, jobs[j].n_src, jobs[j].zmin, jobs[j].zmax, ts, hj[j]);
+        hj[j].tile_base = (int32_t)tiles;
+        start[j] = (int32_t)tiles;
+        tiles += hj[j].tiles;
+    }
+    if (tiles > INT32_MAX) return fail(ctx, RCMVS_E_LIMIT, "too many tiles in one batch");
+    start[n_jobs] = (int32_t)tiles;
+    void *pj, *ps;
+    CK(sc->arena.get(S_JOBS, sizeof(DevJob) * n_jobs, &pj));
+    CK(sc->arena.get(S_JOBSTART, sizeof(int32_t) * (n_jobs + 1), &ps));
+    cudaStream_t st = ctx->stream;
+    CK(cudaMemcpyAsync(pj, hj.data(), sizeof(DevJob) * n_jobs, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ps, start.data(), sizeof(int32_t) * (n_jobs + 1), cudaMemcpyHostToDevice, st));
+    const DevJob* dj = (const DevJob*)pj;
+    const int32_t* dst = (const int32_t*)ps;
+    unsigned long long* dw = ctx->count_work ? ctx->d_work : nullptr;
+    if (dw) CK(cudaMemsetAsync(dw, 0, 2 * sizeof(unsigned long long), st));
+    const int nh = (int)std::max<uint32_t>(opts->num_hyp, 2u);
+    PlaneBuf A{sc->plane_a, sc->pcost_a}, B{sc->plane_b, sc->pcost_b};
+    const SpanHook hk = ctx->hook();
+    hk.begin("stereo_init");
+    CK(launch_init(dj, dst, n_jobs, (int)tiles, ts, nh, sc->census, sc->rays, A, dw, st));
+    hk.end("stereo_init");
+    const uint64_t n_passes = (uint64_t)std::max<uint32_t>(opts->sweeps, 1u) * 2;
+    for (uint64_t pass = 0; pass < n_passes; ++pass) {
+        // stereo.rs:275-277 with the host's libm powf, as the reference
+        const float t = (float)pass / (float)n_passes;
+        const float sig_inv = 0.02f * powf_host(0.28f, t * 4.0f);
+        const float sig_n = 0.30f * powf_host(0.42f, t * 4.0f);
+        hk.begin("stereo_pass");
+        CK(launch_pass(dj, dst, n_jobs, (int)tiles, ts, pass, sig_inv, sig_n, sc->census, sc->rays, A, B, dw, st));
+        hk.end("stereo_pass");
+        std::swap(A, B);
+    }
+    hk.begin("stereo_gate");
+    CK(launch_gate(dj, dst, n_jobs, (int)tiles, ts, opts->cost_thr, sc->census, A, sc->depth, sc->cost, sc->normal,
+                   st));
+    hk.end("stereo_gate");
+    for (int j = 0; j < n_jobs; ++j) sc->has_depth[jobs[j].ref_idx] = 1;
+    if (dw) {
+        unsigned long long h[2];
+        CK(cudaMemcpyAsync(h, dw, sizeof(h), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        ctx->last_evals = h[0];
+        ctx->last_rows = h[1];
+    }
+    return RCMVS_OK;
+}
+
+int rcmvs_ctx_timing(rcmvs_ctx* ctx, int enable) {
+    if (!ctx) return RCMVS_E_ARG;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->clear_spans();
+    ctx->timing = enable != 0;
+    return RCMVS_OK;
+}
+
+int rcmvs_ctx_kernel_time(rcmvs_ctx* ctx, const char* name, double* ms_total, uint64_t* launches) {
+    if (!ctx || !name || !ms_total || !launches) return RCMVS_E_ARG;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->stream));
+    double t = 0.0;
+    uint64_t n = 0;
+    for (auto& s : ctx->spans) {
+        if (s.name != name) continue;
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, s.a, s.b));
+        t += ms;
+        ++n;
+    }
+    *ms_total = t;
+    *launches = n;
+    return RCMVS_OK;
+}
+
+int rcmvs_last_work(rcmvs_ctx* ctx, uint64_t* evals, uint64_t* rows) {
+    if (!ctx || !evals || !rows) return RCMVS_E_ARG;
+    *evals = ctx->count_work ? ctx->last_evals : 0;
+    *rows = ctx->count_work ? ctx->last_rows : 0;
+    return RCMVS_OK;
+}
+
+int rcmvs_scene_get_depth(rcmvs_ctx* ctx, rcmvs_scene* sc, int32_t view, float* depth, float* cost, float* normal) {
+    if (!ctx || !sc || view < 0 || view >= sc->n_views) return fail(ctx, RCMVS_E_ARG, "rcmvs_scene_get_depth: bad argument");
+    if (!sc->has_depth[view]) return fail(ctx, RCMVS_E_STATE, "view has no depth map");
+    CK(cudaSetDevice(ctx->device));
+    const DevView& V = sc->views[view];
+    const size_t n = (size_t)V.w * V.h;
+    cudaStream_t st = ctx->stream;
+    if (depth) CK(cudaMemcpyAsync(depth, sc->depth + V.off, 4 * n, cudaMemcpyDeviceToHost, st));
+    if (cost) CK(cudaMemcpyAsync(cost, sc->cost + V.off, 4 * n, cudaMemcpyDeviceToHost, st));
+    if (normal) CK(cudaMemcpyAsync(normal, sc->normal + 3 * V.off, 12 * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return RCMVS_OK;
+}
+
+int rcmvs_scene_get_census(rcmvs_ctx* ctx, rcmvs_scene* sc, int32_t view, uint64_t* census) {
+    if (!ctx || !sc || view < 0 || view >= sc->n_views || !census)
+        return fail(ctx, RCMVS_E_ARG, "rcmvs_scene_get_census: bad argument");
+    CK(cudaSetDevice(ctx->device));
+    const DevView& V = sc->views[view];
+    CK(cudaMemcpyAsync(census, sc->census + V.off, 8 * (size_t)V.w * V.h, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return RCMVS_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// mvs/src/fuse.rs:72-92: robust sparse bounding-box diagonal -> voxel cell
+double voxel_cell(const double* xyz, uint64_t n, double voxel_rel) {
+    double ext[3];
+    for (int a = 0; a < 3; ++a) {
+        std::vector<double> ax(n);
+        for (uint64_t p = 0; p < n; ++p) ax[p] = xyz[3 * p + a];
+        std::sort(ax.begin(), ax.end());
+        size_t len = ax.size();
+        size_t lo = std::min((size_t)((double)len * 0.02), len - 1);
+        size_t hi = std::min((size_t)((double)len * 0.98), len - 1);
+        ext[a] = ax[hi] - ax[lo];
+    }
+    double diag = std::sqrt(ext[0] * ext[0] + ext[1] * ext[1] + ext[2] * ext[2]);
+    return std::fmax(diag * voxel_rel, 1e-9);
+}
+
+}  // namespace
+
+extern "C" {
+
+int rcmvs_scene_fuse(rcmvs_ctx* ctx, rcmvs_scene* sc, const int32_t* order_offsets, const int32_t* order,
+                     const double* sparse_xyz, uint64_t n_sparse, const rcmvs_options* opts, uint64_t* n_points_out) {
+    if (!ctx || !sc || !order_offsets || !opts || !sparse_xyz || n_sparse == 0 || !n_points_out)
+        return fail(ctx, RCMVS_E_ARG, "rcmvs_scene_fuse: bad argument (sparse cloud must be non-empty)");
+    if (sc->ctx != ctx) return fail(ctx, RCMVS_E_ARG, "scene belongs to another context");
+    const int n = sc->n_views;
+    std::vector<FuseView> fv(n);
+    for (int v = 0; v < n; ++v) {
+        if (order_offsets[v] > order_offsets[v + 1] || order_offsets[v] < 0)
+            return fail(ctx, RCMVS_E_ARG, "fusion order offsets must be non-decreasing");
+        for (int32_t q = order_offsets[v]; q < order_offsets[v + 1]; ++q)
+            if (!order || order[q] < 0 || order[q] >= n || !sc->has_depth[order[q]])
+                return fail(ctx, RCMVS_E_ARG, "fusion order names a view without a depth map");
+    }
+    bool any = false;
+    for (int v = 0; v < n; ++v) any |= sc->has_depth[v] != 0;
+    if (any && !sc->has_rgb) return fail(ctx, RCMVS_E_ARG, "fusion needs rgb for every view");
+    for (int v = 0; v < n; ++v) {
+        FuseView& F = fv[v];
+        std::memset(&F, 0, sizeof(F));
+        F.w = sc->views[v].w;
+        F.h = sc->views[v].h;
+        F.off = sc->views[v].off;
+        F.has_depth = sc->has_depth[v];
+        F.order_begin = order_offsets[v];
+        F.order_end = order_offsets[v + 1];
+        const HostCam& c = sc->cams[v];
+        F.f = c.f;
+        F.cx = c.cx;
+        F.cy = c.cy;
+        F.k = c.k;
+        std::memcpy(F.R, c.R, sizeof(F.R));
+        std::memcpy(F.t, c.t, sizeof(F.t));
+    }
+    const double cell = voxel_cell(sparse_xyz, n_sparse, opts->voxel_rel);
+    CK(cudaSetDevice(ctx->device));
+    FuseResult res{0, 0};
+    std::string err;
+    int rc = fuse_device(sc->arena, fv.data(), n, order, order_offsets[n], sc->depth, sc->rgb, cell,
+                         opts->min_consistent, opts->depth_diff, opts->reproj_px, &sc->d_pts_xyz, &sc->d_pts_rgb,
+                         &sc->d_ply, &res, ctx->stream, &err, ctx->hook());
+    if (rc) return fail(ctx, rc, err);
+    sc->n_points = res.n_points;
+    sc->n_candidates = res.n_candidates;
+    *n_points_out = res.n_points;
+    return RCMVS_OK;
+}
+
+int rcmvs_scene_get_points(rcmvs_ctx* ctx, rcmvs_scene* sc, double* xyz, uint8_t* rgb, uint8_t* ply_body) {
+    if (!ctx || !sc) return fail(ctx, RCMVS_E_ARG, "rcmvs_scene_get_points: bad argument");
+    if (sc->n_points == 0) return RCMVS_OK;
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const size_t n = sc->n_points;
+    if (xyz) CK(cudaMemcpyAsync(xyz, sc->d_pts_xyz, 24 * n, cudaMemcpyDeviceToHost, st));
+    if (rgb) CK(cudaMemcpyAsync(rgb, sc->d_pts_rgb, 3 * n, cudaMemcpyDeviceToHost, st));
+    if (ply_body) CK(cudaMemcpyAsync(ply_body, sc->d_ply, 15 * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return RCMVS_OK;
+}
+
+// ================================================================ host API
+int rcmvs_census(rcmvs_ctx* ctx, const uint8_t* gray, int32_t w, int32_t h, uint64_t* census_out) {
+    if (!ctx || !gray || !census_out || w <= 0 || h <= 0) return fail(ctx, RCMVS_E_ARG, "rcmvs_census: bad argument");
+    rcmvs_view v;
+    std::memset(&v, 0, sizeof(v));
+    v.w = w;
+    v.h = h;
+    v.f = 1.0;
+    v.R[0] = v.R[4] = v.R[8] = 1.0;
+    v.gray = gray;
+    rcmvs_scene* sc = nullptr;
+    int rc = rcmvs_scene_create(ctx, &v, 1, &sc);
+    if (rc) return rc;
+    rc = rcmvs_scene_get_census(ctx, sc, 0, census_out);
+    rcmvs_scene_destroy(sc);
+    return rc;
+}
+
+// Builds a scene of the views jobs touch; remap[] maps caller view -> scene view.
+static int sub_scene(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views, const rcmvs_job* jobs, int32_t n_jobs,
+                     const rcmvs_options* opts, std::vector<int>& remap, rcmvs_scene** out) {
+    remap.assign(n_views, -1);
+    std::vector<rcmvs_view> sub;
+    auto use = [&](int v) {
+        if (remap[v] < 0) {
+            remap[v] = (int)sub.size();
+            sub.push_back(views[v]);
+        }
+    };
+    for (int j = 0; j < n_jobs; ++j) {
+        use(jobs[j].ref_idx);
+        for (int s = 0; s < jobs[j].n_src; ++s) use(jobs[j].srcs[s]);
+    }
+    for (size_t i = 0; i < sub.size(); ++i) {
+        int rc = check_view(ctx, sub[i], (int)i, nullptr);
+        if (rc) return rc;
+    }
+    (void)opts;
+    return rcmvs_scene_create(ctx, sub.data(), (int32_t)sub.size(), out);
+}
+
+int rcmvs_estimate_depth_batch(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views, const rcmvs_job* jobs,
+                               int32_t n_jobs, const rcmvs_options* opts, const rcmvs_depth_out* outs) {
+    if (!ctx || !views || n_views <= 0 || !opts || (n_jobs > 0 && !outs))
+        return fail(ctx, RCMVS_E_ARG, "rcmvs_estimate_depth_batch: bad argument");
+    int rc = validate_jobs(ctx, n_views, jobs, n_jobs);
+    if (rc) return rc;
+    for (int j = 0; j < n_jobs; ++j)
+        if (!outs[j].depth || !outs[j].cost) return fail(ctx, RCMVS_E_ARG, "null depth/cost output");
+    if (n_jobs == 0) return RCMVS_OK;
+    std::vector<int> remap;
+    rcmvs_scene* sc = nullptr;
+    rc = sub_scene(ctx, views, n_views, jobs, n_jobs, opts, remap, &sc);
+    if (rc) return rc;
+    std::vector<rcmvs_job> sj(jobs, jobs + n_jobs);
+    std::vector<std::vector<int32_t>> ss(n_jobs);
+    for (int j = 0; j < n_jobs; ++j) {
+        for (int s = 0; s < jobs[j].n_src; ++s) ss[j].push_back(remap[jobs[j].srcs[s]]);
+        sj[j].ref_idx = remap[jobs[j].ref_idx];
+        sj[j].srcs = ss[j].data();
+    }
+    rc = rcmvs_scene_estimate_depth(ctx, sc, sj.data(), n_jobs, opts);
+    for (int j = 0; j < n_jobs && rc == RCMVS_OK; ++j)
+        rc = rcmvs_scene_get_depth(ctx, sc, sj[j].ref_idx, outs[j].depth, outs[j].cost, outs[j].normal);
+    rcmvs_scene_destroy(sc);
+    return rc;
+}
+
+int rcmvs_estimate_depth(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views, int32_t ref_idx,
+                         const int32_t* srcs, int32_t n_src, double zmin, double zmax, const rcmvs_options* opts,
+                         float* depth_out, float* cost_out, float* normal_out) {
+    rcmvs_job j{ref_idx, n_src, srcs, zmin, zmax};
+    rcmvs_depth_out o{depth_out, cost_out, normal_out};
+    return rcmvs_estimate_depth_batch(ctx, views, n_views, &j, 1, opts, &o);
+}
+
+int rcmvs_plane_cost_field(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views, int32_t ref_idx,
+                           const int32_t* srcs, int32_t n_src, const float* planes, const float* hints,
+                           float* cost_out, int32_t* hsum_out) {
+    if (!ctx || !views || !planes || !hints || !cost_out)
+        return fail(ctx, RCMVS_E_ARG, "rcmvs_plane_cost_field: bad argument");
+    rcmvs_job job{ref_idx, n_src, srcs, 1.0, 2.0};
+    int rc = validate_jobs(ctx, n_views, &job, 1);
+    if (rc) return rc;
+    std::vector<int> remap;
+    rcmvs_scene* sc = nullptr;
+    rc = sub_scene(ctx, views, n_views, &job, 1, nullptr, remap, &sc);
+    if (rc) return rc;
+    const TileShape ts{16, 16};
+    std::vector<int32_t> ss;
+    for (int s = 0; s < n_src; ++s) ss.push_back(remap[srcs[s]]);
+    DevJob hj;
+    fill_job(sc, remap[ref_idx], ss.data(), n_src, 1.0, 2.0, ts, hj);
+    hj.tile_base = 0;
+    int32_t start[2] = {0, hj.tiles};
+    const size_t n = (size_t)views[ref_idx].w * views[ref_idx].h;
+    void *pj, *ps, *ppl, *ph, *pc, *phs;
+    cudaStream_t st = ctx->stream;
+    auto body = [&]() -> int {
+        int r = ensure_tile(ctx, ts);
+        if (r) return r;
+        CK(ctx->arena.get(S_JOBS, sizeof(DevJob), &pj));
+        CK(ctx->arena.get(S_JOBSTART, sizeof(start), &ps));
+        CK(ctx->arena.get(S_FIELD_PL, 16 * n, &ppl));
+        CK(ctx->arena.get(S_FIELD_H, 4 * n, &ph));
+        CK(ctx->arena.get(S_FIELD_C, 4 * n, &pc));
+        CK(ctx->arena.get(S_FIELD_HS, 4 * n, &phs));
+        CK(cudaMemcpyAsync(pj, &hj, sizeof(DevJob), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ps, start, sizeof(start), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ppl, planes, 16 * n, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ph, hints, 4 * n, cudaMemcpyHostToDevice, st));
+        CK(launch_cost_field((const DevJob*)pj, (const int32_t*)ps, hj.tiles, ts, sc->census, sc->rays,
+                             (const float4*)ppl, (const float*)ph, (float*)pc, (int32_t*)phs, st));
+        CK(cudaMemcpyAsync(cost_out, pc, 4 * n, cudaMemcpyDeviceToHost, st));
+        if (hsum_out) CK(cudaMemcpyAsync(hsum_out, phs, 4 * n, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        return RCMVS_OK;
+    };
+    rc = body();
+    rcmvs_scene_destroy(sc);
+    return rc;
+}
+
+int rcmvs_selftest_f2i(rcmvs_ctx* ctx, const float* in, int32_t n, int32_t* out) {
+    if (!ctx || !in || !out || n <= 0) return fail(ctx, RCMVS_E_ARG, "rcmvs_selftest_f2i: bad argument");
+    CK(cudaSetDevice(ctx->device));
+    void *pi, *po;
+    CK(ctx->arena.get(S_CGRAY, 4 * (size_t)n, &pi));
+    CK(ctx->arena.get(S_F2I, 4 * (size_t)n, &po));
+    CK(cudaMemcpyAsync(pi, in, 4 * (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
+    CK(launch_f2i((const float*)pi, n, (int32_t*)po, ctx->stream));
+    CK(cudaMemcpyAsync(out, po, 4 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return RCMVS_OK;
+}
+
+int rcmvs_fuse_depth_maps(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views, const float* const* depth_maps,
+                          const int32_t* order_offsets, const int32_t* order, const double* sparse_xyz,
+                          uint64_t n_sparse, const rcmvs_options* opts, rcmvs_points* out) {
+    if (!ctx || !views || n_views <= 0 || !depth_maps || !order_offsets || !opts || !out)
+        return fail(ctx, RCMVS_E_ARG, "rcmvs_fuse_depth_maps: bad argument");
+    out->n = 0;
+    out->xyz = nullptr;
+    out->rgb = nullptr;
+    rcmvs_scene* sc = nullptr;
+    int rc = rcmvs_scene_create(ctx, views, n_views, &sc);
+    if (rc) return rc;
+    auto body = [&]() -> int {
+        cudaStream_t st = ctx->stream;
+        for (int v = 0; v < n_views; ++v) {
+            if (!depth_maps[v]) continue;
+            const DevView& V = sc->views[v];
+            CK(cudaMemcpyAsync(sc->depth + V.off, depth_maps[v], 4 * (size_t)V.w * V.h, cudaMemcpyHostToDevice, st));
+            sc->has_depth[v] = 1;
+        }
+        uint64_t np = 0;
+        int r = rcmvs_scene_fuse(ctx, sc, order_offsets, order, sparse_xyz, n_sparse, opts, &np);
+        if (r) return r;
+        out->xyz = (double*)std::malloc(24 * std::max<uint64_t>(np, 1));
+        out->rgb = (uint8_t*)std::malloc(3 * std::max<uint64_t>(np, 1));
+        if (!out->xyz || !out->rgb) {
+            rcmvs_points_free(out);
+            return fail(ctx, RCMVS_E_NOMEM, "host allocation of the point cloud failed");
+        }
+        out->n = np;
+        return rcmvs_scene_get_points(ctx, sc, out->xyz, out->rgb, nullptr);
+    };
+    rc = body();
+    rcmvs_scene_destroy(sc);
+    return rc;
+}
+
+// mvs/src/fuse.rs:222-239
+int rcmvs_write_ply_binary(const char* path, const double* xyz, const uint8_t* rgb, uint64_t n) {
+    if (!path || (n > 0 && (!xyz || !rgb))) return RCMVS_E_ARG;
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return RCMVS_E_IO;
+    std::fprintf(f,
+                 "ply\nformat binary_little_endian 1.0\ncomment rustcolmap dense MVS fusion\n"
+                 "element vertex %llu\nproperty float x\nproperty float y\nproperty float z\n"
+                 "property uchar red\nproperty uchar green\nproperty uchar blue\nend_header\n",
+                 (unsigned long long)n);
+    std::vector<uint8_t> buf;
+    buf.reserve(15 * std::min<uint64_t>(n, 1 << 16));
+    for (uint64_t i = 0; i < n; ++i) {
+        float p[3] = {(float)xyz[3 * i], (float)xyz[3 * i + 1], (float)xyz[3 * i + 2]};
+        const uint8_t* b = reinterpret_cast<const uint8_t*>(p);  // x86-64 / aarch64: little-endian
+        buf.insert(buf.end(), b, b + 12);
+        buf.insert(buf.end(), rgb + 3 * i, rgb + 3 * i + 3);
+        if (buf.size() >= 15u * (1u << 16)) {
+            if (std::fwrite(buf.data(), 1, buf.size(), f) != buf.size()) {
+                std::fclose(f);
+                return RCMVS_E_IO;
+            }
+            buf.clear();
+        }
+    }
+    if (!buf.empty() && std::fwrite(buf.data(), 1, buf.size(), f) != buf.size()) {
+        std::fclose(f);
+        return RCMVS_E_IO;
+    }
+    return std::fclose(f) == 0 ? RCMVS_OK : RCMVS_E_IO;
+}
+
+}  // extern "C"
+
+// ================================================================ plan
+namespace {
+// mvs/src/lib.rs:245-251
+double percentile(const std::vector<double>& s, double q) {
+    if (s.empty()) return 0.0;
+    double idx = std::round(((double)s.size() - 1.0) * q);
+    idx = std::min(std::max(idx, 0.0), (double)s.size() - 1.0);
+    return s[(size_t)idx];
+}
+}  // namespace
+
+extern "C" {
+
+// Host glue of run_mvs (mvs/src/lib.rs:224-282, :303-342, :398-418).  The
+// count sorts keep ascending view index among equal counts; the reference's
+// unstable sort agrees whenever a list has <= 20 entries (insertion sort) or
+// no ties.
+int rcmvs_plan(const rcmvs_sparse* sp, const rcmvs_view* views, int32_t n_views, const rcmvs_options* opts,
+               int32_t* src_offsets, int32_t* srcs, double* zrange, int32_t* fuse_offsets, int32_t* fuse_order) {
+    if (!sp || !views || n_views <= 0 || !opts || !src_offsets || !srcs || !zrange || !fuse_offsets || !fuse_order)
+        return RCMVS_E_ARG;
+    if (sp->n_points < 8 || !sp->xyz || !sp->track_offsets || (sp->track_offsets[sp->n_points] > 0 && !sp->track_views))
+        return RCMVS_E_ARG;  // lib.rs:310-315
+    const int n = n_views;
+    std::vector<double> global(sp->n_points);
+    for (uint64_t p = 0; p < sp->n_points; ++p) {
+        const double* x = sp->xyz + 3 * p;
+        global[p] = std::sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+    }
+    std::sort(global.begin(), global.end());
+    std::vector<uint32_t> cov((size_t)n * n, 0);
+    std::vector<std::vector<uint64_t>> seen_by(n);
+    std::vector<int> ids;
+    for (uint64_t p = 0; p < sp->n_points; ++p) {
+        ids.clear();
+        for (uint64_t q = sp->track_offsets[p]; q < sp->track_offsets[p + 1]; ++q) {
+            int v = sp->track_views[q];
+            if (v >= 0 && v < n) ids.push_back(v);
+        }
+        std::sort(ids.begin(), ids.end());
+        ids.erase(std::unique(ids.begin(), ids.end()), ids.end());
+        for (int a : ids) {
+            seen_by[a].push_back(p);
+            for (int b : ids)
+                if (a != b) cov[(size_t)a * n + b]++;
+        }
+    }
+    std::vector<std::vector<int>> sources(n);
+    std::vector<char> has(n, 0);
+    int off = 0;
+    for (int i = 0; i < n; ++i) {
+        std::vector<std::pair<uint32_t, int>> o;
+        for (int j = 0; j < n; ++j)
+            if (cov[(size_t)i * n + j] >= 10) o.push_back({cov[(size_t)i * n + j], j});
+        std::stable_sort(o.begin(), o.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+        src_offsets[i] = off;
+        for (size_t q = 0; q < o.size() && q < opts->num_sources; ++q) {
+            sources[i].push_back(o[q].second);
+            srcs[off++] = o[q].second;
+        }
+        has[i] = !sources[i].empty();
+    }
+    src_offsets[n] = off;
+    for (int i = 0; i < n; ++i) {  // depth_range_for (lib.rs:253-282)
+        const rcmvs_view& v = views[i];
+        std::vector<double> ds;
+        for (uint64_t p : seen_by[i]) {
+            const double* x = sp->xyz + 3 * p;
+            double z = (v.R[6] * x[0] + v.R[7] * x[1] + v.R[8] * x[2]) + v.t[2];
+            if (z > 1e-6) ds.push_back(z);
+        }
+        const std::vector<double>* src = &global;
+        if (ds.size() >= 8) {
+            std::sort(ds.begin(), ds.end());
+            src = &ds;
+        }
+        double lo = 0.0, hi = 0.0;
+        if (src->size() >= 8) {
+            lo = percentile(*src, 0.02);
+            hi = percentile(*src, 0.98);
+        }
+        if (hi <= lo * 1.05 || lo <= 0.0) {
+            zrange[2 * i] = std::fmax(percentile(global, 0.01) * 0.7, 1e-3);
+            zrange[2 * i + 1] = percentile(global, 0.99) * 1.4;
+        } else {
+            zrange[2 * i] = lo * 0.8;
+            zrange[2 * i + 1] = hi * 1.25;
+        }
+    }
+    off = 0;
+    for (int i = 0; i < n; ++i) {  // fusion order, sources first (lib.rs:398-418)
+        std::vector<std::pair<uint32_t, int>> o;
+        for (int j = 0; j < n; ++j)
+            if (cov[(size_t)i * n + j] >= 10 && has[j]) o.push_back({cov[(size_t)i * n + j], j});
+        std::stable_sort(o.begin(), o.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+        const auto& s = sources[i];
+        auto rank = [&](int j) -> size_t {
+            auto it = std::find(s.begin(), s.end(), j);
+            return it == s.end() ? SIZE_MAX : (size_t)(it - s.begin());
+        };
+        std::stable_sort(o.begin(), o.end(), [&](const auto& a, const auto& b) { return rank(a.second) < rank(b.second); });
+        fuse_offsets[i] = off;
+        for (auto& c : o) fuse_order[off++] = c.second;
+    }
+    fuse_offsets[n] = off;
+    return RCMVS_OK;
+}
+
+int rcmvs_run_mvs(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views, const rcmvs_sparse* sparse,
+                  const rcmvs_options* opts, const rcmvs_depth_out* depth_outs, rcmvs_points* out, rcmvs_stats* stats) {
+    if (!ctx || !views || !sparse || !opts || !out) return fail(ctx, RCMVS_E_ARG, "rcmvs_run_mvs: bad argument");
+    out->n = 0;
+    out->xyz = nullptr;
+    out->rgb = nullptr;
+    if (n_views < 2) return fail(ctx, RCMVS_E_ARG, "need at least 2 registered views for MVS");  // lib.rs:175-177
+    if (sparse->n_points < 8)
+        return fail(ctx, RCMVS_E_ARG, "sparse reconstruction too small for MVS (need >= 8 points)");
+    for (int i = 0; i < n_views; ++i) {
+        int rc = check_view(ctx, views[i], i, opts);
+        if (rc) return rc;
+        if (!views[i].rgb) return fail(ctx, RCMVS_E_ARG, "run_mvs needs rgb for every view");
+    }
+    cudaEvent_t e0, e1, e2, e3;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventCreate(&e2));
+    CK(cudaEventCreate(&e3));
+    const int n = n_views;
+    std::vector<int32_t> so(n + 1), ss((size_t)n * std::max<uint32_t>(opts->num_sources, 1u)), fo(n + 1),
+        ff((size_t)n * n);
+    std::vector<double> zr(2 * n);
+    int rc = rcmvs_plan(sparse, views, n, opts, so.data(), ss.data(), zr.data(), fo.data(), ff.data());
+    if (rc) return fail(ctx, rc, "plan failed");
+    std::vector<rcmvs_job> jobs;
+    for (int i = 0; i < n; ++i)
+        if (so[i + 1] > so[i]) jobs.push_back(rcmvs_job{i, so[i + 1] - so[i], ss.data() + so[i], zr[2 * i], zr[2 * i + 1]});
+    rcmvs_scene* sc = nullptr;
+    CK(cudaEventRecord(e0, ctx->stream));
+    rc = rcmvs_scene_create(ctx, views, n, &sc);
+    if (rc) return rc;
+    auto body = [&]() -> int {
+        CK(cudaEventRecord(e1, ctx->stream));
+        int r = rcmvs_scene_estimate_depth(ctx, sc, jobs.data(), (int32_t)jobs.size(), opts);
+        if (r) return r;
+        CK(cudaEventRecord(e2, ctx->stream));
+        uint64_t np = 0;
+        r = rcmvs_scene_fuse(ctx, sc, fo.data(), ff.data(), sparse->xyz, sparse->n_points, opts, &np);
+        if (r) return r;
+        out->xyz = (double*)std::malloc(24 * std::max<uint64_t>(np, 1));
+        out->rgb = (uint8_t*)std::malloc(3 * std::max<uint64_t>(np, 1));
+        if (!out->xyz || !out->rgb) {
+            rcmvs_points_free(out);
+            return fail(ctx, RCMVS_E_NOMEM, "host allocation of the point cloud failed");
+        }
+        out->n = np;
+        r = rcmvs_scene_get_points(ctx, sc, out->xyz, out->rgb, nullptr);
+        if (r) return r;
+        CK(cudaEventRecord(e3, ctx->stream));
+        std::vector<float> zero;
+        for (int i = 0; i < n && depth_outs; ++i) {
+            const rcmvs_depth_out& d = depth_outs[i];
+            if (sc->has_depth[i]) {
+                r = rcmvs_scene_get_depth(ctx, sc, i, d.depth, d.cost, d.normal);
+                if (r) return r;
+            } else {
+                const size_t np2 = (size_t)views[i].w * views[i].h;
+                if (d.depth) std::fill(d.depth, d.depth + np2, 0.0f);
+                if (d.cost) std::fill(d.cost, d.cost + np2, 1.0f);
+                if (d.normal) std::fill(d.normal, d.normal + 3 * np2, 0.0f);
+            }
+        }
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (stats) {
+            float t_all = 0, t_st = 0, t_fu = 0;
+            cudaEventElapsedTime(&t_all, e0, e3);
+            cudaEventElapsedTime(&t_st, e1, e2);
+            cudaEventElapsedTime(&t_fu, e2, e3);
+            stats->views = n;
+            stats->views_with_depth = jobs.size();
+            stats->dense_points = np;
+            stats->fusion_candidates = sc->n_candidates;
+            stats->elapsed_s = t_all * 1e-3f;
+            stats->stereo_s = t_st * 1e-3f;
+            stats->fuse_s = t_fu * 1e-3f;
+        }
+        return RCMVS_OK;
+    };
+    rc = body();
+    rcmvs_scene_destroy(sc);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaEventDestroy(e2);
+    cudaEventDestroy(e3);
+    if (rc) rcmvs_points_free(out);
+    return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,489 @@
+// stereo.cu — census patch-match stereo on sm_100a.
+//
+// Restates mvs/src/stereo.rs:
+//   plane_cost      stereo.rs:158-228   (device function plane_cost)
+//   init sweep      stereo.rs:247-269   (init_kernel)
+//   Jacobi passes   stereo.rs:271-371   (pass_kernel, one launch per pass)
+//   texture gate    stereo.rs:373-393   (gate_kernel)
+//   pixel RNG       stereo.rs:47-78
+//
+// Bit-exactness: the library is compiled with --fmad=false and IEEE divide
+// and square root, and every f32 expression keeps the reference's operand
+// order, so each pixel's cost, abort decision, RNG draw and accepted plane is
+// identical to the CPU code.  The f32 sum of the 25*K window terms stays a
+// serial per-thread chain in (source, dy, dx) order because the early-abort
+// test reads its partial values.
+//
+// Layout: one thread per reference pixel; one block per TW x TH tile of one
+// job (all jobs of a batch in one launch).  The block stages its jobs'
+// support-view parameters, a 49-entry h/48 table, and the tile's rays and
+// census with a 2-pixel clamped halo in shared memory; support-view census
+// words are gathered through the read-only path (L1/L2).
+#include "rcmvs_internal.cuh"
+
+namespace rcmvs {
+
+namespace {
+
+constexpr int HALO = 2;  // 5x5 window (stereo.rs:41)
+
+__device__ __forceinline__ int find_item(const int32_t* start, int n, int b) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (start[mid] <= b)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+// ---------------------------------------------------------------- RNG
+// stereo.rs:47-57
+__device__ __forceinline__ uint64_t pixel_rng(int32_t x, int32_t y, uint64_t salt) {
+    uint64_t s = ((uint64_t)(int64_t)x * 0x9E3779B97F4A7C15ull) ^ ((uint64_t)(int64_t)y * 0xC2B2AE3D27D4EB4Full) ^
+                 (salt * 0x165667B19E3779F9ull);
+    s ^= s >> 30;
+    s *= 0xBF58476D1CE4E5B9ull;
+    s ^= s >> 27;
+    s *= 0x94D049BB133111EBull;
+    return s ^ (s >> 31);
+}
+// stereo.rs:59-78.  (x>>40) < 2^24 converts exactly; the divide by 2^24 is
+// an exact power-of-two scale, written as a multiply.
+__device__ __forceinline__ float uniform01(uint64_t& s) {
+    uint64_t x = s;
+    x ^= x << 13;
+    x ^= x >> 7;
+    x ^= x << 17;
+    s = x;
+    return (float)(x >> 40) * (1.0f / 16777216.0f);
+}
+__device__ __forceinline__ float gauss3(uint64_t& s) {
+    float a = uniform01(s);
+    float b = uniform01(s);
+    float c = uniform01(s);
+    return a + b + c - 1.5f;
+}
+
+// ---------------------------------------------------------------- tile setup
+struct Tile {
+    const DevJob* job;
+    int x0, y0;
+    int stw;  // shared tile row pitch (TW + 2*HALO)
+};
+
+struct Smem {
+    DevSrc* src;     // RCMVS_MAX_SOURCES
+    float* tab;      // 64 (49 used): h / 48.0f
+    float2* ray;     // (TH+4)*(TW+4)
+    uint64_t* cen;   // (TH+4)*(TW+4)
+};
+
+__host__ __device__ inline size_t smem_bytes(int tw, int th) {
+    size_t cells = (size_t)(tw + 2 * HALO) * (th + 2 * HALO);
+    return sizeof(DevSrc) * RCMVS_MAX_SOURCES + 64 * sizeof(float) + cells * sizeof(float2) +
+           cells * sizeof(uint64_t);
+}
+
+__device__ __forceinline__ Smem carve(unsigned char* base, int tw, int th) {
+    Smem s;
+    size_t cells = (size_t)(tw + 2 * HALO) * (th + 2 * HALO);
+    s.src = reinterpret_cast<DevSrc*>(base);
+    s.tab = reinterpret_cast<float*>(base + sizeof(DevSrc) * RCMVS_MAX_SOURCES);
+    s.ray = reinterpret_cast<float2*>(s.tab + 64);
+    s.cen = reinterpret_cast<uint64_t*>(s.ray + cells);
+    return s;
+}
+
+// Stages job sources, the h/48 table and the halo tile; all threads call it.
+__device__ __forceinline__ void load_tile(const DevJob* jobs, const int32_t* job_start, int n_jobs, int tw,
+                                          int th, const uint64_t* __restrict__ census,
+                                          const float2* __restrict__ rays, const Smem& sm, Tile& T) {
+    const int j = find_item(job_start, n_jobs, blockIdx.x);
+    const DevJob* J = jobs + j;
+    T.job = J;
+    const int t = blockIdx.x - job_start[j];
+    const int tiles_x = J->tiles_x;
+    T.x0 = (t % tiles_x) * tw;
+    T.y0 = (t / tiles_x) * th;
+    T.stw = tw + 2 * HALO;
+    const int nthr = tw * th;
+    {
+        const int nwords = J->nsrc * (int)(sizeof(DevSrc) / 4);
+        const uint32_t* srcw = reinterpret_cast<const uint32_t*>(J->src);
+        uint32_t* dstw = reinterpret_cast<uint32_t*>(sm.src);
+        for (int i = threadIdx.x; i < nwords; i += nthr) dstw[i] = srcw[i];
+    }
+    for (int h = threadIdx.x; h < 49; h += nthr) sm.tab[h] = (float)h / 48.0f;
+    const int w = J->w, hgt = J->h;
+    const int cells = (tw + 2 * HALO) * (th + 2 * HALO);
+    const size_t off = (size_t)J->off;
+    for (int i = threadIdx.x; i < cells; i += nthr) {
+        int sx = i % T.stw, sy = i / T.stw;
+        int gx = min(max(T.x0 - HALO + sx, 0), w - 1);
+        int gy = min(max(T.y0 - HALO + sy, 0), hgt - 1);
+        size_t g = off + (size_t)gy * w + gx;
+        sm.ray[i] = __ldg(rays + g);
+        sm.cen[i] = __ldg(census + g);
+    }
+    __syncthreads();
+}
+
+struct WorkCount {
+    unsigned long long evals, rows;
+};
+
+// ---------------------------------------------------------------- plane_cost
+// stereo.rs:158-228.  (lx, ly): the pixel's position in the tile; window
+// cell (dx, dy) of the pixel is shared cell (ly+dy)*stw + lx+dx (dx, dy in
+// 0..4), which holds the clamped pixel (stereo.rs:179-184).
+// FRONTO: n = (0,0,1).  Then denom = 0*xo + 0*yo + 1 is exactly 1.0 for the
+// finite rays the host admits, so z = d/1 = d, and both are skipped.
+template <bool FRONTO, bool COUNT, bool HSUM>
+__device__ __forceinline__ float plane_cost(const Smem& sm, int stw, int lx, int ly, int nsrc,
+                                            const uint64_t* __restrict__ census, float nx, float ny, float nz,
+                                            float d, float hint, float total, WorkCount& wc, int32_t* hsum) {
+    float sum = 0.f;
+    int32_t hs = 0;
+    const float thr = hint + 0.12f;
+    if (COUNT) wc.evals++;
+    for (int si = 0; si < nsrc; ++si) {
+        const DevSrc& s = sm.src[si];
+        const float rs0 = s.rs[0], rs1 = s.rs[1], rs2 = s.rs[2];
+        const float rs3 = s.rs[3], rs4 = s.rs[4], rs5 = s.rs[5];
+        const float rs6 = s.rs[6], rs7 = s.rs[7], rs8 = s.rs[8];
+        const float ts0 = s.ts[0], ts1 = s.ts[1], ts2 = s.ts[2];
+        const float f = s.f, cx = s.cx, cy = s.cy, k = s.k;
+        const int sw = s.w, sh = s.h;
+        const uint64_t* __restrict__ sc = census + s.off;
+        const float fsi = (float)(si + 1);
+        for (int dy = 0; dy < 5; ++dy) {
+            const int row = (ly + dy) * stw + lx;
+#pragma unroll
+            for (int dx = 0; dx < 5; ++dx) {
+                const float2 r = sm.ray[row + dx];
+                float term = 1.0f;
+                int32_t hterm = 48;
+                float denom;
+                if (FRONTO)
+                    denom = 1.0f;
+                else
+                    denom = nx * r.x + ny * r.y + nz;
+                if (!(denom < 0.05f)) {
+                    const float z = FRONTO ? d : d / denom;
+                    const float xr = z * r.x;
+                    const float yr = z * r.y;
+                    const float xs = rs0 * xr + rs1 * yr + rs2 * z + ts0;
+                    const float ys = rs3 * xr + rs4 * yr + rs5 * z + ts1;
+                    const float zs = rs6 * xr + rs7 * yr + rs8 * z + ts2;
+                    if (!(zs < 1e-3f)) {
+                        const float xn = xs / zs;
+                        const float yn = ys / zs;
+                        const float dist = 1.0f + k * (xn * xn + yn * yn);
+                        // `as i32`: truncation, saturating, NaN -> 0 (cvt.rzi)
+                        const int u = __float2int_rz(f * xn * dist + cx);
+                        const int v = __float2int_rz(f * yn * dist + cy);
+                        if (u >= 0 && v >= 0 && u < sw && v < sh) {
+                            const uint64_t cs = __ldg(sc + (size_t)v * sw + u);
+                            const int h = __popcll(sm.cen[row + dx] ^ cs);
+                            term = sm.tab[h];
+                            hterm = h;
+                        }
+                    }
+                }
+                sum += term;
+                if (HSUM) hs += hterm;
+            }
+            if (COUNT) wc.rows++;
+            const float rows_done = (float)(dy + 1);
+            if (sum / (rows_done * 5.0f * fsi) > thr) {
+                if (HSUM) *hsum = hs;
+                return 1e9f;
+            }
+        }
+    }
+    if (HSUM) *hsum = hs;
+    return sum / total;
+}
+
+__device__ __forceinline__ void flush_work(const WorkCount& wc, unsigned long long* d_work) {
+    unsigned long long e = wc.evals, r = wc.rows;
+    for (int o = 16; o > 0; o >>= 1) {
+        e += __shfl_down_sync(0xffffffffu, e, o);
+        r += __shfl_down_sync(0xffffffffu, r, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(d_work, e);
+        atomicAdd(d_work + 1, r);
+    }
+}
+
+// ---------------------------------------------------------------- init
+// stereo.rs:247-269
+template <bool COUNT>
+__global__ void init_kernel(const DevJob* __restrict__ jobs, const int32_t* __restrict__ job_start, int n_jobs,
+                            int tw, int th, int nh, const uint64_t* __restrict__ census,
+                            const float2* __restrict__ rays, PlaneBuf out, unsigned long long* d_work) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const Smem sm = carve(smem_raw, tw, th);
+    Tile T;
+    load_tile(jobs, job_start, n_jobs, tw, th, census, rays, sm, T);
+    const DevJob* J = T.job;
+    const int lx = threadIdx.x % tw, ly = threadIdx.x / tw;
+    const int x = T.x0 + lx, y = T.y0 + ly;
+    WorkCount wc{0, 0};
+    if (x < J->w && y < J->h) {
+        const int nsrc = J->nsrc;
+        const float total = 5.0f * 5.0f * (float)nsrc;
+        const float inv_min = J->inv_min, inv_max = J->inv_max;
+        float best_c = INFINITY;
+        float best_d = 0.f;
+        for (int hi = 0; hi < nh; ++hi) {
+            const float inv = inv_min + (inv_max - inv_min) * (float)hi / (float)(nh - 1);
+            const float d = 1.0f / inv;
+            const float c = plane_cost<true, COUNT, false>(sm, T.stw, lx, ly, nsrc, census, 0.f, 0.f, 1.f, d,
+                                                           best_c + 0.02f, total, wc, nullptr);
+            if (c < best_c) {
+                best_c = c;
+                best_d = d;
+            }
+        }
+        const size_t i = (size_t)J->off + (size_t)y * J->w + x;
+        out.nz[i] = make_float4(0.0f, 0.0f, 1.0f, best_d);
+        out.cost[i] = fminf(best_c, 1.0f);
+    }
+    if (COUNT) flush_work(wc, d_work);
+}
+
+// ---------------------------------------------------------------- passes
+// stereo.rs:274-371: one double-buffered pass.  Reads `prev` only, writes
+// every pixel of `next` (the carried-over plane when nothing is accepted,
+// which equals the reference's copy_from_slice at :278).
+template <bool COUNT>
+__global__ void pass_kernel(const DevJob* __restrict__ jobs, const int32_t* __restrict__ job_start, int n_jobs,
+                            int tw, int th, uint64_t pass, float sig_inv, float sig_n,
+                            const uint64_t* __restrict__ census, const float2* __restrict__ rays, PlaneBuf prev,
+                            PlaneBuf next, unsigned long long* d_work) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const Smem sm = carve(smem_raw, tw, th);
+    Tile T;
+    load_tile(jobs, job_start, n_jobs, tw, th, census, rays, sm, T);
+    const DevJob* J = T.job;
+    const int lx = threadIdx.x % tw, ly = threadIdx.x / tw;
+    const int x = T.x0 + lx, y = T.y0 + ly;
+    const int w = J->w, h = J->h;
+    WorkCount wc{0, 0};
+    if (x < w && y < h) {
+        const int nsrc = J->nsrc;
+        const float total = 5.0f * 5.0f * (float)nsrc;
+        const float inv_min = J->inv_min, inv_max = J->inv_max;
+        const float zlo = J->zmin * 0.5f, zhi = J->zmax * 2.0f;
+        const size_t base = (size_t)J->off;
+        const size_t i = base + (size_t)y * w + x;
+        const int stw = T.stw;
+        const float2 ri = sm.ray[(ly + HALO) * stw + lx + HALO];
+        uint64_t seed = pixel_rng(x, y, pass + 7);
+        const float4 cur = prev.nz[i];
+        const float cur_cost = prev.cost[i];
+        float best_c = cur_cost;
+        float bn0 = cur.x, bn1 = cur.y, bn2 = cur.z;
+        float bd = cur.w * (bn0 * ri.x + bn1 * ri.y + bn2);
+
+        // propagation from the 4 neighbours (stereo.rs:292-321)
+#pragma unroll 1
+        for (int q = 0; q < 4; ++q) {
+            const int ddx = q == 0 ? -1 : (q == 1 ? 1 : 0);
+            const int ddy = q == 2 ? -1 : (q == 3 ? 1 : 0);
+            const int xx = x + ddx, yy = y + ddy;
+            if (xx < 0 || yy < 0 || xx >= w || yy >= h) continue;
+            const float4 nb = prev.nz[base + (size_t)yy * w + xx];
+            const float2 rj = sm.ray[(ly + HALO + ddy) * stw + lx + HALO + ddx];
+            const float a_nb = nb.x * rj.x + nb.y * rj.y + nb.z;
+            if (a_nb < 0.1f) continue;
+            const float d_plane = nb.w * a_nb;
+            const float a_here = nb.x * ri.x + nb.y * ri.y + nb.z;
+            if (a_here < 0.1f) continue;
+            const float zcand = d_plane / a_here;
+            if (!(zlo <= zcand && zcand <= zhi)) continue;
+            const float c = plane_cost<false, COUNT, false>(sm, stw, lx, ly, nsrc, census, nb.x, nb.y, nb.z,
+                                                            d_plane, best_c + 0.02f, total, wc, nullptr);
+            if (c < best_c) {
+                best_c = c;
+                bn0 = nb.x;
+                bn1 = nb.y;
+                bn2 = nb.z;
+                bd = d_plane;
+            }
+        }
+
+        // random perturbations around the current plane (stereo.rs:323-353)
+#pragma unroll 1
+        for (int r = 0; r < 3; ++r) {
+            const float inv = 1.0f / fmaxf(cur.w, 1e-6f);
+            const float inv_new = inv + sig_inv * (inv_max - inv_min) * gauss3(seed);
+            if (inv_new <= 0.0f) continue;
+            const float zcand = 1.0f / inv_new;
+            if (!(zlo <= zcand && zcand <= zhi)) continue;
+            float nnx = cur.x + sig_n * gauss3(seed);
+            float nny = cur.y + sig_n * gauss3(seed);
+            float nnz = cur.z + sig_n * gauss3(seed);
+            const float len = sqrtf(nnx * nnx + nny * nny + nnz * nnz);
+            if (len < 1e-6f) continue;
+            nnx = nnx / len;
+            nny = nny / len;
+            nnz = nnz / len;
+            const float a_here = nnx * ri.x + nny * ri.y + nnz;
+            if (a_here < 0.1f) continue;
+            const float d_plane = zcand * a_here;
+            const float c = plane_cost<false, COUNT, false>(sm, stw, lx, ly, nsrc, census, nnx, nny, nnz, d_plane,
+                                                            best_c + 0.02f, total, wc, nullptr);
+            if (c < best_c) {
+                best_c = c;
+                bn0 = nnx;
+                bn1 = nny;
+                bn2 = nnz;
+                bd = d_plane;
+            }
+        }
+
+        float4 o = cur;
+        float oc = cur_cost;
+        if (best_c < cur_cost) {  // stereo.rs:355-367
+            const float a_here = bn0 * ri.x + bn1 * ri.y + bn2;
+            if (a_here > 0.05f) {
+                o = make_float4(bn0, bn1, bn2, bd / a_here);
+                oc = fminf(best_c, 1.0f);
+            }
+        }
+        next.nz[i] = o;
+        next.cost[i] = oc;
+    }
+    if (COUNT) flush_work(wc, d_work);
+}
+
+// ---------------------------------------------------------------- gate
+// stereo.rs:373-393 (+ normals, an extension)
+__global__ void gate_kernel(const DevJob* __restrict__ jobs, const int32_t* __restrict__ job_start, int n_jobs,
+                            int tw, int th, float cost_thr, const uint64_t* __restrict__ census, PlaneBuf planes,
+                            float* __restrict__ depth, float* __restrict__ cost, float* __restrict__ normal) {
+    const int j = find_item(job_start, n_jobs, blockIdx.x);
+    const DevJob* J = jobs + j;
+    const int t = blockIdx.x - job_start[j];
+    const int x = (t % J->tiles_x) * tw + (int)threadIdx.x % tw;
+    const int y = (t / J->tiles_x) * th + (int)threadIdx.x / tw;
+    if (x >= J->w || y >= J->h) return;
+    const size_t i = (size_t)J->off + (size_t)y * J->w + x;
+    const float4 p = planes.nz[i];
+    const float c = planes.cost[i];
+    const int tex = __popcll(census[i]);
+    const bool textured = tex >= 4 && tex <= 44;
+    const bool ok = textured && c < cost_thr && p.w > J->zmin * 0.5f && p.w < J->zmax * 2.0f;
+    depth[i] = ok ? p.w : 0.0f;
+    cost[i] = c;
+    if (normal) {
+        normal[3 * i] = p.x;
+        normal[3 * i + 1] = p.y;
+        normal[3 * i + 2] = p.z;
+    }
+}
+
+// ---------------------------------------------------------------- diagnostics
+__global__ void cost_field_kernel(const DevJob* __restrict__ jobs, const int32_t* __restrict__ job_start, int tw,
+                                  int th, const uint64_t* __restrict__ census, const float2* __restrict__ rays,
+                                  const float4* __restrict__ planes, const float* __restrict__ hints,
+                                  float* __restrict__ cost_out, int32_t* __restrict__ hsum_out) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const Smem sm = carve(smem_raw, tw, th);
+    Tile T;
+    load_tile(jobs, job_start, 1, tw, th, census, rays, sm, T);
+    const DevJob* J = T.job;
+    const int lx = threadIdx.x % tw, ly = threadIdx.x / tw;
+    const int x = T.x0 + lx, y = T.y0 + ly;
+    if (x >= J->w || y >= J->h) return;
+    const size_t li = (size_t)y * J->w + x;
+    const float4 p = planes[li];
+    WorkCount wc{0, 0};
+    int32_t hs = 0;
+    const float total = 5.0f * 5.0f * (float)J->nsrc;
+    cost_out[li] = plane_cost<false, false, true>(sm, T.stw, lx, ly, J->nsrc, census, p.x, p.y, p.z, p.w,
+                                                  hints[li], total, wc, &hs);
+    hsum_out[li] = hs;
+}
+
+__global__ void f2i_kernel(const float* in, int n, int32_t* out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = __float2int_rz(in[i]);
+}
+
+}  // namespace
+
+size_t stereo_smem_bytes(TileShape ts) { return smem_bytes(ts.tw, ts.th); }
+
+cudaError_t stereo_configure(TileShape ts) {
+    size_t sm = smem_bytes(ts.tw, ts.th);
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(init_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) return e;
+    if ((e = cudaFuncSetAttribute(init_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) return e;
+    if ((e = cudaFuncSetAttribute(pass_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) return e;
+    if ((e = cudaFuncSetAttribute(pass_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) return e;
+    if ((e = cudaFuncSetAttribute(cost_field_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) return e;
+    return cudaSuccess;
+}
+
+cudaError_t launch_init(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, int total_tiles, TileShape ts,
+                        int nh, const uint64_t* census, const float2* rays, PlaneBuf out, unsigned long long* d_work,
+                        cudaStream_t st) {
+    if (total_tiles <= 0) return cudaSuccess;
+    size_t sm = smem_bytes(ts.tw, ts.th);
+    if (d_work)
+        init_kernel<true><<<total_tiles, ts.tw * ts.th, sm, st>>>(d_jobs, d_job_start, n_jobs, ts.tw, ts.th, nh,
+                                                                  census, rays, out, d_work);
+    else
+        init_kernel<false><<<total_tiles, ts.tw * ts.th, sm, st>>>(d_jobs, d_job_start, n_jobs, ts.tw, ts.th, nh,
+                                                                   census, rays, out, nullptr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pass(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, int total_tiles, TileShape ts,
+                        uint64_t pass, float sig_inv, float sig_n, const uint64_t* census, const float2* rays,
+                        PlaneBuf prev, PlaneBuf next, unsigned long long* d_work, cudaStream_t st) {
+    if (total_tiles <= 0) return cudaSuccess;
+    size_t sm = smem_bytes(ts.tw, ts.th);
+    if (d_work)
+        pass_kernel<true><<<total_tiles, ts.tw * ts.th, sm, st>>>(d_jobs, d_job_start, n_jobs, ts.tw, ts.th, pass,
+                                                                  sig_inv, sig_n, census, rays, prev, next, d_work);
+    else
+        pass_kernel<false><<<total_tiles, ts.tw * ts.th, sm, st>>>(d_jobs, d_job_start, n_jobs, ts.tw, ts.th, pass,
+                                                                   sig_inv, sig_n, census, rays, prev, next,
+                                                                   nullptr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gate(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, int total_tiles, TileShape ts,
+                        float cost_thr, const uint64_t* census, PlaneBuf planes, float* depth, float* cost,
+                        float* normal, cudaStream_t st) {
+    if (total_tiles <= 0) return cudaSuccess;
+    gate_kernel<<<total_tiles, ts.tw * ts.th, 0, st>>>(d_jobs, d_job_start, n_jobs, ts.tw, ts.th, cost_thr, census,
+                                                       planes, depth, cost, normal);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cost_field(const DevJob* d_job, const int32_t* d_job_start, int total_tiles, TileShape ts,
+                              const uint64_t* census, const float2* rays, const float4* planes, const float* hints,
+                              float* cost_out, int32_t* hsum_out, cudaStream_t st) {
+    if (total_tiles <= 0) return cudaSuccess;
+    size_t sm = smem_bytes(ts.tw, ts.th);
+    cost_field_kernel<<<total_tiles, ts.tw * ts.th, sm, st>>>(d_job, d_job_start, ts.tw, ts.th, census, rays, planes,
+                                                              hints, cost_out, hsum_out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_f2i(const float* in, int n, int32_t* out, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    f2i_kernel<<<(n + 255) / 256, 256, 0, st>>>(in, n, out);
+    return cudaGetLastError();
+}
+
+}  // namespace rcmvs

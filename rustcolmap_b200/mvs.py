@@ -1,0 +1,369 @@
+"""Host-side mirror of the reference `mvs` crate's public API, running on the
+B200 kernels of librcmvs through its C ABI (include/rcmvs.h).
+
+Reference                                   here
+mvs::run_mvs            (lib.rs:294)        run_mvs
+stereo::estimate_depth  (stereo.rs:234)     estimate_depth / estimate_depth_batch
+fuse::fuse_depth_maps   (fuse.rs:64)        fuse_depth_maps
+fuse::write_ply_binary  (fuse.rs:222)       write_ply_binary
+census_map              (lib.rs:119)        census_map
+covisibility/sources/depth_range_for/fusion order (lib.rs:224-418)   plan
+
+Argument meaning and error behaviour follow the reference: estimate_depth
+and fuse_depth_maps cannot fail on valid input; run_mvs raises where the
+reference returns Err (fewer than 2 views, fewer than 8 sparse points).
+There is no CPU path: a missing library or a CUDA error raises RcmvsError.
+"""
+import ctypes as C
+import os
+import time
+
+import numpy as np
+
+from . import _abi, _lib
+from ._lib import RcmvsError
+from .types import DepthMap, MvsOptions, MvsStats, SparseModel, ViewData  # noqa: F401
+
+
+class Context:
+    """One rcmvs_ctx: a CUDA device + stream.  Not thread-safe."""
+
+    def __init__(self, device=0):
+        self._L = _lib.mvs()
+        p = C.c_void_p()
+        rc = self._L.rcmvs_ctx_create(int(device), C.byref(p))
+        if rc != 0:
+            raise RcmvsError(rc, f"cannot create a context on CUDA device {device} "
+                                 "(needs an sm_100 GPU)")
+        self.ptr = p
+        self.device = device
+
+    def check(self, rc):
+        if rc != 0:
+            raise RcmvsError(rc, self._L.rcmvs_last_error(self.ptr).decode())
+
+    @property
+    def stream(self):
+        """The context's cudaStream_t as an integer handle."""
+        return self._L.rcmvs_ctx_stream(self.ptr)
+
+    def synchronize(self):
+        self.check(self._L.rcmvs_ctx_synchronize(self.ptr))
+
+    def last_work(self):
+        e, r = C.c_uint64(), C.c_uint64()
+        self.check(self._L.rcmvs_last_work(self.ptr, C.byref(e), C.byref(r)))
+        return e.value, r.value
+
+    def timing(self, enable=True):
+        """Start (or stop) recording CUDA-event spans around each kernel launch."""
+        self.check(self._L.rcmvs_ctx_timing(self.ptr, int(bool(enable))))
+
+    def kernel_time(self, name):
+        """(total ms, launches) of kernel `name` since timing was enabled."""
+        ms, n = C.c_double(), C.c_uint64()
+        self.check(self._L.rcmvs_ctx_kernel_time(self.ptr, name.encode(), C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+    def close(self):
+        if getattr(self, "ptr", None):
+            self._L.rcmvs_ctx_destroy(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default = {}
+
+
+def default_context(device=0):
+    if device not in _default:
+        _default[device] = Context(device)
+    return _default[device]
+
+
+def _ctx(ctx):
+    return ctx if ctx is not None else default_context()
+
+
+def census_map(gray, ctx=None):
+    """7x7 census (lib.rs:119-142) of a (h, w) u8 image -> (h, w) u64."""
+    ctx = _ctx(ctx)
+    gray = np.ascontiguousarray(gray, dtype=np.uint8)
+    h, w = gray.shape
+    out = np.empty((h, w), np.uint64)
+    ctx.check(ctx._L.rcmvs_census(ctx.ptr, gray.ctypes.data, w, h, out.ctypes.data))
+    return out
+
+
+def estimate_depth(views, ref_idx, srcs, zmin, zmax, opts, ctx=None, normals=False):
+    """stereo::estimate_depth (stereo.rs:234-394) on the GPU."""
+    return estimate_depth_batch(views, [(ref_idx, srcs, zmin, zmax)], opts, ctx, normals)[0]
+
+
+def estimate_depth_batch(views, jobs, opts, ctx=None, normals=False):
+    """Many estimate_depth calls in one batched launch sequence.
+    jobs: list of (ref_idx, srcs, zmin, zmax)."""
+    ctx = _ctx(ctx)
+    va = _abi.view_array(views)
+    cj = (_abi.Job * len(jobs))()
+    outs = (_abi.DepthOut * len(jobs))()
+    keep, res = [], []
+    for i, (ref, srcs, zmin, zmax) in enumerate(jobs):
+        s = np.ascontiguousarray(srcs, dtype=np.int32)
+        r = views[ref]
+        d = np.empty((r.h, r.w), np.float32)
+        c = np.empty((r.h, r.w), np.float32)
+        n = np.empty((r.h, r.w, 3), np.float32) if normals else None
+        keep += [s]
+        cj[i] = _abi.Job(int(ref), len(s), s.ctypes.data if len(s) else None, float(zmin), float(zmax))
+        outs[i] = _abi.DepthOut(d.ctypes.data, c.ctypes.data, _abi.ptr(n))
+        res.append(DepthMap(d, c, n))
+    o = opts.to_c()
+    ctx.check(ctx._L.rcmvs_estimate_depth_batch(ctx.ptr, va, len(views), cj, len(jobs), C.byref(o), outs))
+    return res
+
+
+def _csr(lists):
+    off = np.zeros(len(lists) + 1, np.int32)
+    for i, l in enumerate(lists):
+        off[i + 1] = off[i] + len(l)
+    flat = np.array([x for l in lists for x in l] or [0], np.int32)
+    return off, flat
+
+
+def fuse_depth_maps(views, depth_maps, sources, sparse_xyz, opts, ctx=None):
+    """fuse::fuse_depth_maps (fuse.rs:64-215) on the GPU.  depth_maps: list of
+    DepthMap / (h, w) f32 / None; sources: per-view fusion order lists.
+    Returns (xyz (n, 3) f64, rgb (n, 3) u8) sorted by voxel key."""
+    ctx = _ctx(ctx)
+    va = _abi.view_array(views)
+    dms = []
+    for d in depth_maps:
+        if d is None:
+            dms.append(None)
+        else:
+            dms.append(np.ascontiguousarray(d.depth if isinstance(d, DepthMap) else d, dtype=np.float32))
+    dptr = (C.c_void_p * len(views))(*[None if d is None else d.ctypes.data for d in dms])
+    off, flat = _csr(sources)
+    sp = np.ascontiguousarray(sparse_xyz, dtype=np.float64).reshape(-1, 3)
+    pts = _abi.Points()
+    o = opts.to_c()
+    ctx.check(ctx._L.rcmvs_fuse_depth_maps(ctx.ptr, va, len(views), dptr, off.ctypes.data, flat.ctypes.data,
+                                           sp.ctypes.data, len(sp), C.byref(o), C.byref(pts)))
+    return _take_points(ctx, pts)
+
+
+def _take_points(ctx, pts):
+    n = pts.n
+    if n == 0:
+        ctx._L.rcmvs_points_free(C.byref(pts))
+        return np.zeros((0, 3), np.float64), np.zeros((0, 3), np.uint8)
+    xyz = np.ctypeslib.as_array((C.c_double * (3 * n)).from_address(pts.xyz)).reshape(n, 3).copy()
+    rgb = np.ctypeslib.as_array((C.c_uint8 * (3 * n)).from_address(pts.rgb)).reshape(n, 3).copy()
+    ctx._L.rcmvs_points_free(C.byref(pts))
+    return xyz, rgb
+
+
+def write_ply_binary(path, xyz, rgb):
+    """fuse::write_ply_binary (fuse.rs:222-239)."""
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+    rgb = np.ascontiguousarray(rgb, dtype=np.uint8)
+    rc = _lib.mvs().rcmvs_write_ply_binary(os.fsencode(path), xyz.ctypes.data, rgb.ctypes.data, len(xyz))
+    if rc != 0:
+        raise RcmvsError(rc, f"cannot write {path}")
+
+
+def plan(sparse, views, opts):
+    """Host glue of run_mvs: (sources per view, zrange (n, 2), fusion order per view)."""
+    n = len(views)
+    va = _abi.view_array(views)
+    sp = sparse.to_c()
+    so = np.zeros(n + 1, np.int32)
+    ss = np.zeros(max(1, n * opts.num_sources), np.int32)
+    zr = np.zeros((n, 2), np.float64)
+    fo = np.zeros(n + 1, np.int32)
+    ff = np.zeros(max(1, n * n), np.int32)
+    o = opts.to_c()
+    rc = _lib.mvs().rcmvs_plan(C.byref(sp), va, n, C.byref(o), so.ctypes.data, ss.ctypes.data, zr.ctypes.data,
+                               fo.ctypes.data, ff.ctypes.data)
+    if rc != 0:
+        raise RcmvsError(rc, "plan failed (need >= 8 sparse points)")
+    return ([ss[so[i]:so[i + 1]].tolist() for i in range(n)], zr,
+            [ff[fo[i]:fo[i + 1]].tolist() for i in range(n)])
+
+
+def plane_cost_field(views, ref_idx, srcs, planes, hints, ctx=None):
+    """plane_cost (stereo.rs:158-228) at every pixel for a given plane field
+    (h, w, 4) = (nx, ny, nz, d) and hints (h, w).  Returns (cost, hsum)."""
+    ctx = _ctx(ctx)
+    va = _abi.view_array(views)
+    s = np.ascontiguousarray(srcs, dtype=np.int32)
+    r = views[ref_idx]
+    planes = np.ascontiguousarray(planes, dtype=np.float32).reshape(r.h, r.w, 4)
+    hints = np.ascontiguousarray(hints, dtype=np.float32).reshape(r.h, r.w)
+    cost = np.empty((r.h, r.w), np.float32)
+    hsum = np.empty((r.h, r.w), np.int32)
+    ctx.check(ctx._L.rcmvs_plane_cost_field(ctx.ptr, va, len(views), ref_idx, s.ctypes.data if len(s) else None,
+                                            len(s), planes.ctypes.data, hints.ctypes.data, cost.ctypes.data,
+                                            hsum.ctypes.data))
+    return cost, hsum
+
+
+def selftest_f2i(values, ctx=None):
+    ctx = _ctx(ctx)
+    v = np.ascontiguousarray(values, dtype=np.float32)
+    out = np.empty(len(v), np.int32)
+    ctx.check(ctx._L.rcmvs_selftest_f2i(ctx.ptr, v.ctypes.data, len(v), out.ctypes.data))
+    return out
+
+
+class DeviceScene:
+    """Views resident in device memory (rcmvs_scene): census, rays, planes,
+    depth maps and the fused cloud never leave HBM between calls."""
+
+    def __init__(self, views, ctx=None):
+        self.ctx = _ctx(ctx)
+        self.views = views
+        self._va = _abi.view_array(views)
+        p = C.c_void_p()
+        self.ctx.check(self.ctx._L.rcmvs_scene_create(self.ctx.ptr, self._va, len(views), C.byref(p)))
+        self.ptr = p
+        self.n_points = 0
+
+    def prepare(self):
+        self.ctx.check(self.ctx._L.rcmvs_scene_prepare(self.ctx.ptr, self.ptr))
+
+    def estimate(self, jobs, opts):
+        cj = (_abi.Job * len(jobs))()
+        keep = []
+        for i, (ref, srcs, zmin, zmax) in enumerate(jobs):
+            s = np.ascontiguousarray(srcs, dtype=np.int32)
+            keep.append(s)
+            cj[i] = _abi.Job(int(ref), len(s), s.ctypes.data if len(s) else None, float(zmin), float(zmax))
+        o = opts.to_c()
+        self.ctx.check(self.ctx._L.rcmvs_scene_estimate_depth(self.ctx.ptr, self.ptr, cj, len(jobs), C.byref(o)))
+
+    def fuse(self, fusion_order, sparse_xyz, opts):
+        off, flat = _csr(fusion_order)
+        sp = np.ascontiguousarray(sparse_xyz, dtype=np.float64).reshape(-1, 3)
+        n = C.c_uint64()
+        o = opts.to_c()
+        self.ctx.check(self.ctx._L.rcmvs_scene_fuse(self.ctx.ptr, self.ptr, off.ctypes.data, flat.ctypes.data,
+                                                    sp.ctypes.data, len(sp), C.byref(o), C.byref(n)))
+        self.n_points = n.value
+        return self.n_points
+
+    def depth(self, v, normals=False):
+        w, h = self.views[v].w, self.views[v].h
+        d = np.empty((h, w), np.float32)
+        c = np.empty((h, w), np.float32)
+        n = np.empty((h, w, 3), np.float32) if normals else None
+        self.ctx.check(self.ctx._L.rcmvs_scene_get_depth(self.ctx.ptr, self.ptr, v, d.ctypes.data, c.ctypes.data,
+                                                         _abi.ptr(n)))
+        return DepthMap(d, c, n)
+
+    def census(self, v):
+        w, h = self.views[v].w, self.views[v].h
+        out = np.empty((h, w), np.uint64)
+        self.ctx.check(self.ctx._L.rcmvs_scene_get_census(self.ctx.ptr, self.ptr, v, out.ctypes.data))
+        return out
+
+    def points(self, ply_body=False):
+        n = self.n_points
+        xyz = np.empty((n, 3), np.float64)
+        rgb = np.empty((n, 3), np.uint8)
+        body = np.empty(15 * n, np.uint8) if ply_body else None
+        if n:
+            self.ctx.check(self.ctx._L.rcmvs_scene_get_points(self.ctx.ptr, self.ptr, xyz.ctypes.data,
+                                                              rgb.ctypes.data, _abi.ptr(body)))
+        return (xyz, rgb, body) if ply_body else (xyz, rgb)
+
+    def close(self):
+        if getattr(self, "ptr", None):
+            self.ctx._L.rcmvs_scene_destroy(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _web_json(xyz, rgb, path, cap=400_000):
+    """dense_web.json of run_mvs (lib.rs:437-485): robust-radius filter and
+    stride decimation to <= cap points (order follows the fused cloud)."""
+    n = len(xyz)
+    if n == 0:
+        return
+    c = xyz.sum(axis=0) / n
+    dists = np.sqrt(((xyz - c) ** 2).sum(axis=1))
+    sd = np.sort(dists)
+    med = sd[n // 2]
+    p95 = sd[min(int(n * 0.95), n - 1)]
+    r_keep = med + 6.0 * max(abs(p95 - med), max(med, 1e-9) * 0.5)
+    keep = np.nonzero(dists <= r_keep)[0]
+    stride = -(-len(keep) // cap)
+    sel = keep[::max(stride, 1)]
+    pos = ",".join("[{:.4f},{:.4f},{:.4f}]".format(*xyz[i]) for i in sel)
+    col = ",".join("[{}, {},{}]".format(*rgb[i]) for i in sel)
+    with open(path, "w") as f:
+        f.write('{"n":' + str(len(sel)) + ',"pos":[' + pos + '],"col":[' + col + ']}')
+
+
+def run_mvs(views, sparse, opts, out_dir=None, ctx=None, log=None, return_depth=False):
+    """mvs::run_mvs (lib.rs:294-517) from views already at working resolution
+    (the image decode/resize of load_views is not part of this path).  Writes
+    <out_dir>/dense/dense.ply, mvs_stats.json and dense_web.json when out_dir
+    is given.  Returns (MvsStats, xyz, rgb[, depth maps])."""
+    ctx = _ctx(ctx)
+    t0 = time.time()
+    if len(views) < 2:
+        raise RcmvsError(_abi.RCMVS_E_ARG, "need at least 2 registered views for MVS")
+    if len(sparse.xyz) < 8:
+        raise RcmvsError(_abi.RCMVS_E_ARG,
+                         f"sparse reconstruction too small for MVS ({len(sparse.xyz)} points, need >= 8)")
+    va = _abi.view_array(views)
+    sp = sparse.to_c()
+    o = opts.to_c()
+    st = _abi.Stats()
+    pts = _abi.Points()
+    douts = None
+    dms = []
+    if return_depth:
+        douts = (_abi.DepthOut * len(views))()
+        for i, v in enumerate(views):
+            d = np.empty((v.h, v.w), np.float32)
+            c = np.empty((v.h, v.w), np.float32)
+            douts[i] = _abi.DepthOut(d.ctypes.data, c.ctypes.data, None)
+            dms.append(DepthMap(d, c))
+    ctx.check(ctx._L.rcmvs_run_mvs(ctx.ptr, va, len(views), C.byref(sp), C.byref(o), douts, C.byref(pts),
+                                   C.byref(st)))
+    xyz, rgb = _take_points(ctx, pts)
+    stats = MvsStats(views=st.views, views_with_depth=st.views_with_depth, dense_points=st.dense_points,
+                     per_view_valid=[int((d.depth > 0).sum()) for d in dms] if return_depth else [],
+                     elapsed_s=time.time() - t0, stereo_s=st.stereo_s, fuse_s=st.fuse_s,
+                     fusion_candidates=st.fusion_candidates)
+    if log:
+        log(f"mvs: fused {stats.dense_points} dense points from {stats.views_with_depth} depth maps")
+    if out_dir is not None:
+        dense = os.path.join(out_dir, "dense")
+        os.makedirs(dense, exist_ok=True)
+        write_ply_binary(os.path.join(dense, "dense.ply"), xyz, rgb)
+        _web_json(xyz, rgb, os.path.join(dense, "dense_web.json"))
+        with open(os.path.join(dense, "mvs_stats.json"), "w") as f:
+            f.write('{"views": %d, "views_with_depth": %d, "dense_points": %d, "stereo_s": %.1f, '
+                    '"fuse_s": %.1f, "elapsed_s": %.1f}' % (stats.views, stats.views_with_depth,
+                                                            stats.dense_points, stats.stereo_s, stats.fuse_s,
+                                                            stats.elapsed_s))
+    return (stats, xyz, rgb, dms) if return_depth else (stats, xyz, rgb)
+
+
+__all__ = ["Context", "default_context", "census_map", "estimate_depth", "estimate_depth_batch",
+           "fuse_depth_maps", "write_ply_binary", "plan", "run_mvs", "plane_cost_field", "DeviceScene",
+           "MvsOptions", "MvsStats", "ViewData", "DepthMap", "SparseModel", "RcmvsError"]

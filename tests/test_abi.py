@@ -1,0 +1,120 @@
+"""The C-ABI libraries load and export everything include/*.h declares; host
+entry points that need no GPU behave like the reference (no compute calls on
+a GPU here)."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, has_gpu
+from oracle import oracle
+from rustcolmap_b200 import MvsOptions, _abi, _lib, mvs
+
+
+def _declared(header):
+    src = open(os.path.join(ROOT, "include", header)).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b((?:rcmvs|rcscene)_\w+)\s*\(", src)))
+
+
+def _exported(so):
+    out = subprocess.run(["nm", "-D", "--defined-only", so], capture_output=True, text=True, check=True).stdout
+    return {l.split()[-1] for l in out.splitlines() if l.strip()}
+
+
+@pytest.mark.parametrize("header,so", [("rcmvs.h", "librcmvs.so"), ("rcscene.h", "librcscene.so")])
+def test_library_exports_every_declared_symbol(header, so):
+    path = os.path.join(ROOT, "rustcolmap_b200", so)
+    C.CDLL(path)  # loads without a GPU
+    decl = _declared(header)
+    assert decl, "no declarations parsed"
+    missing = [d for d in decl if d not in _exported(path)]
+    assert not missing, missing
+
+
+def test_python_signature_table_covers_header():
+    assert set(_lib.exported_symbols()) == set(_declared("rcmvs.h"))
+
+
+def test_abi_struct_layouts_match_c(tmp_path):
+    prog = tmp_path / "layout.c"
+    prog.write_text(r"""
+#include <stdio.h>
+#include <stddef.h>
+#include "rcmvs.h"
+int main(void) {
+  printf("%zu %zu %zu %zu %zu %zu %zu\n", sizeof(rcmvs_options), sizeof(rcmvs_view), sizeof(rcmvs_job),
+         sizeof(rcmvs_depth_out), sizeof(rcmvs_sparse), sizeof(rcmvs_points), sizeof(rcmvs_stats));
+  printf("%zu %zu %zu %zu\n", offsetof(rcmvs_options, depth_diff), offsetof(rcmvs_options, reproj_px),
+         offsetof(rcmvs_view, gray), offsetof(rcmvs_job, zmin));
+  return 0; }
+""")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(prog), "-o", str(exe)], check=True)
+    lines = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    sizes = [int(x) for x in lines[0].split()]
+    offs = [int(x) for x in lines[1].split()]
+    assert sizes == [C.sizeof(t) for t in (_abi.Options, _abi.View, _abi.Job, _abi.DepthOut, _abi.Sparse,
+                                           _abi.Points, _abi.Stats)]
+    assert offs == [_abi.Options.depth_diff.offset, _abi.Options.reproj_px.offset, _abi.View.gray.offset,
+                    _abi.Job.zmin.offset]
+
+
+def test_options_default_mirrors_mvsoptions_default():
+    o = _abi.Options()
+    _lib.mvs().rcmvs_options_default(C.byref(o))
+    ref = MvsOptions().to_c()
+    for name, _ in _abi.Options._fields_:
+        assert getattr(o, name) == getattr(ref, name), name
+    # lib.rs:56-70
+    assert (o.max_dim, o.num_sources, o.sweeps, o.num_hyp, o.min_consistent) == (900, 3, 4, 48, 2)
+    assert o.depth_diff == 0.03 and abs(o.cost_thr - 0.38) < 1e-7 and o.voxel_rel == 0.0015
+
+
+def test_write_ply_matches_oracle(tmp_path):
+    rng = np.random.default_rng(0)
+    xyz = rng.normal(size=(257, 3))
+    rgb = rng.integers(0, 256, (257, 3), dtype=np.uint8)
+    a, b = str(tmp_path / "a.ply"), str(tmp_path / "b.ply")
+    mvs.write_ply_binary(a, xyz, rgb)
+    oracle.write_ply_binary(b, xyz, rgb)
+    assert open(a, "rb").read() == open(b, "rb").read()
+    mvs.write_ply_binary(a, xyz[:0], rgb[:0])
+    assert open(a, "rb").read().endswith(b"element vertex 0\nproperty float x\nproperty float y\nproperty float z\n"
+                                         b"property uchar red\nproperty uchar green\nproperty uchar blue\n"
+                                         b"end_header\n")
+
+
+def test_plan_matches_oracle(corner_scene, c1_opts):
+    a = mvs.plan(corner_scene.sparse, corner_scene.views, c1_opts)
+    b = oracle.plan(corner_scene.sparse, corner_scene.views, c1_opts)
+    assert a[0] == b[0] and a[2] == b[2]
+    assert np.array_equal(a[1], b[1])
+    assert all(len(s) == 4 for s in a[0])
+
+
+def test_plan_matches_oracle_orbit():
+    from rustcolmap_b200 import scene
+    sc = scene.orbit_room(seed=3, n_views=24, sizes=((96, 72),), n_boxes=8, per_view_sparse=120)
+    o = MvsOptions(num_sources=8)
+    a = mvs.plan(sc.sparse, sc.views, o)
+    b = oracle.plan(sc.sparse, sc.views, o)
+    assert a[0] == b[0] and a[2] == b[2] and np.array_equal(a[1], b[1])
+
+
+@pytest.mark.skipif(has_gpu(), reason="checks the no-GPU error path")
+def test_context_without_gpu_fails_loudly():
+    with pytest.raises(_lib.RcmvsError):
+        mvs.Context(0)
+
+
+def test_package_has_no_cpu_fallback():
+    """The product package never imports the oracle."""
+    pkg = os.path.join(ROOT, "rustcolmap_b200")
+    for dirpath, _, files in os.walk(pkg):
+        for f in files:
+            if f.endswith((".py", ".cu", ".cuh", ".cpp", ".h")):
+                assert "oracle" not in open(os.path.join(dirpath, f)).read().replace("the oracle", ""), f
