@@ -248,9 +248,13 @@ def main():
     ap.add_argument("--ref-rows", type=int, default=12, help="rows per step of the reference arm")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--views", type=int, default=0, help="override the number of views (profiling runs)")
     args = ap.parse_args()
     assert args.warmup >= 3 or os.environ.get("RCMVS_BENCH_ALLOW_SHORT"), "warm-up must be >= 3 steps"
     cfg = configs()[args.config]
+    if args.views and cfg["scene"] is not None:
+        cfg["scene"] = dict(cfg["scene"], n_views=args.views)
+        cfg["desc"] += f" [{args.views} views]"
     if args.impl == "reference":
         run_reference(args, cfg)
         return

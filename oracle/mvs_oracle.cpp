@@ -553,7 +553,10 @@ int orc_estimate_depth(const rcmvs_view* views, int32_t n_views, int32_t ref_idx
 static double sample_depth(const float* depth, int32_t w, int32_t h, double u, double v) {
     int32_t u0 = f64_to_i32(std::floor(u));
     int32_t v0 = f64_to_i32(std::floor(v));
-    if (u0 < 0 || v0 < 0 || u0 + 1 >= w || v0 + 1 >= h) return 0.0;
+    // fuse.rs:37 tests `u0 + 1 >= w`; written without the i32 overflow at
+    // u0 = INT_MAX (a saturated projection), where the reference would wrap
+    // and then panic on the slice index.  Such points count as off-image.
+    if (u0 < 0 || v0 < 0 || u0 >= w - 1 || v0 >= h - 1) return 0.0;
     float fx = (float)(u - (double)u0);
     float fy = (float)(v - (double)v0);
     auto idx = [&](int32_t x, int32_t y) { return depth[(size_t)y * w + x]; };

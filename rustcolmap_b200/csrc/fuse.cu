@@ -82,7 +82,11 @@ __device__ __forceinline__ int f64_to_i32(double x) { return __double2int_rz(x);
 __device__ __forceinline__ double sample_depth(const float* __restrict__ dm, int w, int h, double u, double v) {
     const int u0 = f64_to_i32(floor(u));
     const int v0 = f64_to_i32(floor(v));
-    if (u0 < 0 || v0 < 0 || u0 + 1 >= w || v0 + 1 >= h) return 0.0;
+    // The reference tests `u0 + 1 >= w`.  u0 saturates at INT_MAX for points
+    // barely in front of the camera, where `+ 1` would overflow (Rust wraps in
+    // release builds and then panics on the slice index); `u0 >= w - 1` is
+    // the same test without the overflow and treats such points as off-image.
+    if (u0 < 0 || v0 < 0 || u0 >= w - 1 || v0 >= h - 1) return 0.0;
     const float fx = (float)(u - (double)u0);
     const float fy = (float)(v - (double)v0);
     const float d00 = __ldg(dm + (size_t)v0 * w + u0), d10 = __ldg(dm + (size_t)v0 * w + u0 + 1);

@@ -270,3 +270,15 @@ def test_bad_arguments_raise(ctx, corner_scene):
         mvs.estimate_depth(v, 0, list(range(1, 8)) * 5, 3.0, 7.0, MvsOptions(max_dim=4096), ctx)
     with pytest.raises(mvs.RcmvsError):
         mvs.run_mvs(v[:1], corner_scene.sparse, MvsOptions(max_dim=4096), ctx=ctx)
+
+
+def test_fusion_saturated_projection_matches_oracle(ctx):
+    from test_oracle import saturating_projection_case
+    views, dms, sparse = saturating_projection_case()
+    for mc, order in ((0, [[], []]), (1, [[], [0]])):
+        opts = MvsOptions(min_consistent=mc)
+        g = mvs.fuse_depth_maps(views, dms if mc else [None, dms[1]], order, sparse, opts, ctx)
+        off = np.cumsum([0] + [len(f) for f in order])
+        c = oracle.fuse_depth_maps(views, dms if mc else [None, dms[1]], off, [x for f in order for x in f],
+                                   sparse, opts)
+        _assert_same_cloud(g, c[:2])

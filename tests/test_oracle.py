@@ -270,3 +270,30 @@ def test_oracle_header_says_parity_unpinned():
     here = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     for f in ("oracle/mvs_oracle.h", "oracle/mvs_oracle.cpp", "oracle/oracle.py"):
         assert "unpinned" in open(os.path.join(here, f)).read().lower()
+
+
+def saturating_projection_case():
+    """Two views: the ref's one valid pixel sees a point 1000 units to the
+    side of the source camera and ~2e-6 in front of its image plane, so the
+    source projection saturates `as i32` at INT_MAX (fuse.rs:35-37)."""
+    w, h = 8, 6
+    cam = Cam(100.0, 4.0, 3.0, 0.0)
+    src = ViewData("s", 0, w, h, cam, np.eye(3), np.zeros(3), np.zeros((h, w), np.uint8),
+                   np.zeros((h, w, 3), np.uint8))
+    ref = ViewData("r", 1, w, h, cam, np.eye(3), np.array([-1000.0, 0.0, 5.0]), np.zeros((h, w), np.uint8),
+                   np.full((h, w, 3), 9, np.uint8))
+    d_src = np.full((h, w), 3.0, np.float32)
+    d_ref = np.zeros((h, w), np.float32)
+    d_ref[3, 4] = np.float32(5.000002)
+    sparse = np.array([[0, 0, 1], [1, 1, 2], [2, 0, 3], [0, 2, 1]], np.float64)
+    return [src, ref], [d_src, d_ref], sparse
+
+
+def test_fuse_saturated_projection_is_off_image():
+    views, dms, sparse = saturating_projection_case()
+    opts = MvsOptions(min_consistent=0)
+    xyz, rgb, ncand = oracle.fuse_depth_maps(views, [None, dms[1]], [0, 0, 0], [], sparse, opts)
+    assert ncand == 1 and len(xyz) == 1  # kept with zero confirmations, no read outside the map
+    opts = MvsOptions(min_consistent=1)
+    xyz, rgb, ncand = oracle.fuse_depth_maps(views, dms, [0, 0, 1], [0], sparse, opts)
+    assert ncand == 0
