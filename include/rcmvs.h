@@ -269,6 +269,39 @@ int rcmvs_ctx_kernel_time(rcmvs_ctx* ctx, const char* name, double* ms_total, ui
  * semantics on the GPU.  Host buffers. */
 int rcmvs_selftest_f2i(rcmvs_ctx* ctx, const float* in, int32_t n, int32_t* out);
 
+/* ------------------------------------------- allocation-free variant */
+/* No counterpart in the reference: an `estimate_depth` for callers that may
+ * not allocate device memory (an application whose GPU memory belongs to
+ * another allocator, or a real-time loop that cannot afford the device-wide
+ * synchronisation of cudaMalloc/cudaFree).  It makes no cudaMalloc/cudaFree
+ * call and uses no allocating library routine: intermediates live in one
+ * fixed __device__ array of RCMVS_NOALLOC_SCRATCH_BYTES (36.6 MiB), which a
+ * device reserves when this entry point first runs there and holds until the
+ * process exits (every device that loads the library, if modules load
+ * eagerly).
+ *   - views[i].gray are DEVICE pointers (w*h u8); rgb is ignored.
+ *   - depth_dev / cost_dev are DEVICE buffers of w*h floats of the reference.
+ *   - stream is a cudaStream_t (NULL = the legacy default stream); the call
+ *     is asynchronous on it.  Results equal rcmvs_estimate_depth's bit for
+ *     bit.
+ *   - Each view at most RCMVS_NOALLOC_MAX_PIXELS pixels and at most
+ *     RCMVS_NOALLOC_MAX_SOURCES sources, else RCMVS_E_LIMIT; bad arguments
+ *     give RCMVS_E_ARG, a failed CUDA call RCMVS_E_CUDA (no message: there
+ *     is no context).
+ *   - The first call on a device looks up the array's device address
+ *     (cudaGetSymbolAddress, once per device); make that first call before
+ *     any stream capture.
+ *   - All calls on a device share the array and leave its contents behind;
+ *     calls whose GPU work overlaps (different streams or threads) race on
+ *     it and must be serialised by the caller. */
+#define RCMVS_NOALLOC_MAX_PIXELS 307200 /* 640 x 480 */
+#define RCMVS_NOALLOC_MAX_SOURCES 4
+#define RCMVS_NOALLOC_SCRATCH_BYTES 38416384
+int rcmvs_estimate_depth_noalloc(const rcmvs_view* views, int32_t n_views, int32_t ref_idx,
+                                 const int32_t* srcs, int32_t n_src, double zmin, double zmax,
+                                 const rcmvs_options* opts, float* depth_dev, float* cost_dev,
+                                 void* stream);
+
 #ifdef __cplusplus
 }
 #endif

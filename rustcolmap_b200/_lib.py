@@ -62,6 +62,7 @@ def mvs():
         "rcmvs_selftest_f2i": ([vp, vp, i32, vp], C.c_int),
         "rcmvs_ctx_timing": ([vp, C.c_int], C.c_int),
         "rcmvs_ctx_kernel_time": ([vp, cp, vp, vp], C.c_int),
+        "rcmvs_estimate_depth_noalloc": ([vp, i32, i32, vp, i32, f64, f64, vp, vp, vp, vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -99,4 +100,5 @@ _SIG_NAMES = [
     "rcmvs_scene_estimate_depth", "rcmvs_scene_fuse", "rcmvs_scene_get_depth",
     "rcmvs_scene_get_census", "rcmvs_scene_get_points", "rcmvs_plane_cost_field",
     "rcmvs_last_work", "rcmvs_selftest_f2i", "rcmvs_ctx_timing", "rcmvs_ctx_kernel_time",
+    "rcmvs_estimate_depth_noalloc",
 ]

@@ -27,7 +27,7 @@ FLAGS = ARCH + [
 ]
 
 LIBS = {
-    "librcmvs.so": ["capi.cu", "census.cu", "stereo.cu", "fuse.cu"],
+    "librcmvs.so": ["capi.cu", "census.cu", "stereo.cu", "fuse.cu", "noalloc.cu"],
     "librcscene.so": ["scene.cu"],
 }
 HEADERS = [os.path.join(CSRC, "rcmvs_internal.cuh"), os.path.join(ROOT, "include", "rcmvs.h"),
