@@ -249,6 +249,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--views", type=int, default=0, help="override the number of views (profiling runs)")
+    ap.add_argument("--no-count", action="store_true", help="skip the work-counting rerun")
+    ap.add_argument("--one-candidate", action="store_true",
+                    help="use the one-candidate-at-a-time stereo kernels (comparison)")
     args = ap.parse_args()
     assert args.warmup >= 3 or os.environ.get("RCMVS_BENCH_ALLOW_SHORT"), "warm-up must be >= 3 steps"
     cfg = configs()[args.config]
@@ -265,6 +268,8 @@ def main():
     ws, rank, local = dist_setup()
     torch.cuda.set_device(local)
     opts = cfg["opts"]
+    if args.one_candidate:
+        opts.flags |= 1
     t_setup = time.perf_counter()
     sc = make_scene(cfg, seed=5 + 1000 * rank, device=local)
     srcs, zr, fus = mvs.plan(sc.sparse, sc.views, opts)
@@ -309,14 +314,16 @@ def main():
     value = total_maps / (ms_max / 1e3)
 
     # work counters (untimed rerun with counting on): actual cost evaluations and rows
-    os.environ["RCMVS_COUNT"] = "1"
-    cctx = mvs.Context(local)
-    del os.environ["RCMVS_COUNT"]
-    cds = mvs.DeviceScene(sc.views, cctx)
-    cds.estimate(jobs, opts)
-    evals, rows5 = cctx.last_work()
-    cds.close()
-    cctx.close()
+    evals, rows5 = 0, 0
+    if not args.no_count:
+        os.environ["RCMVS_COUNT"] = "1"
+        cctx = mvs.Context(local)
+        del os.environ["RCMVS_COUNT"]
+        cds = mvs.DeviceScene(sc.views, cctx)
+        cds.estimate(jobs, opts)
+        evals, rows5 = cctx.last_work()
+        cds.close()
+        cctx.close()
 
     # end to end through the reference-facing call with pinned host buffers
     e2e = None
@@ -364,7 +371,7 @@ def main():
     step_s = ms_max / 1e3 / args.steps
     stereo_ms = sum(ktimes[k][0] for k in ("stereo_init", "stereo_pass", "stereo_gate")) / args.steps
     fp32_ops_per_term = 40
-    achieved_tops = actual_terms * fp32_ops_per_term / (stereo_ms / 1e3) / 1e12
+    achieved_tops = actual_terms * fp32_ops_per_term / (stereo_ms / 1e3) / 1e12 if actual_terms else None
 
     cpu = None
     if not args.no_cpu_baseline and rank == 0 and ws == 1:
@@ -387,7 +394,8 @@ def main():
                          "avg_launch_ms": pass_avg_s * 1e3,
                          "note": "issue-bound kernel: see compute_roofline"},
             "compute_roofline": {"bound": "fp32_issue", "achieved": achieved_tops, "peak": FP32_NOMINAL_TOPS,
-                                 "unit": "Top/s", "frac": achieved_tops / FP32_NOMINAL_TOPS,
+                                 "unit": "Top/s",
+                                 "frac": achieved_tops / FP32_NOMINAL_TOPS if achieved_tops else None,
                                  "ops_per_term": fp32_ops_per_term,
                                  "peak_source": "nominal 148 SM x 128 FP32 lanes x 1.965 GHz"},
             "gpu_launches": args.steps * (1 + 1 + 2 * opts.sweeps + 1 + 5),
@@ -404,6 +412,7 @@ def main():
             "gt": {"accuracy_median": statistics.median(accs), "completeness_median": statistics.median(comps),
                    "tol": "1% relative inverse depth", "views_sampled": len(accs)},
             "setup_s": setup_s,
+            "kernels": "one-candidate" if opts.flags & 1 else "row-step",
         }
         print(json.dumps(line), flush=True)
     ds.close()

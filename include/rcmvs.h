@@ -60,9 +60,17 @@ typedef struct rcmvs_options {
                                 0 = off (reference behaviour) */
     uint32_t tile_w;         /* stereo tile width in pixels; 0 = tuned default */
     uint32_t tile_h;         /* stereo tile height in pixels; 0 = tuned default */
-    uint32_t flags;          /* reserved, must be 0 */
+    uint32_t flags;          /* RCMVS_FLAG_* bits; 0 = defaults */
     uint32_t reserved1;
 } rcmvs_options;
+
+/* The plane-sweep init evaluates each pixel's hypotheses one at a time, a
+ * warp waiting at every hypothesis for its slowest lane, instead of the
+ * default row-step schedule (each lane advances its own hypothesis stream
+ * one 5-term window row per step).  Same results bit for bit; kept for
+ * comparison.  The pass kernel always works one candidate at a time, which
+ * keeps a warp's source-census gathers on one support view. */
+#define RCMVS_FLAG_ONE_CANDIDATE 1u
 
 /* Fills `MvsOptions::default()` (mvs/src/lib.rs:56-70); extensions off. */
 void rcmvs_options_default(rcmvs_options* opts);
@@ -268,6 +276,7 @@ int rcmvs_ctx_kernel_time(rcmvs_ctx* ctx, const char* name, double* ms_total, ui
  * truncation toward zero, saturation, NaN -> 0.  Lets tests check those
  * semantics on the GPU.  Host buffers. */
 int rcmvs_selftest_f2i(rcmvs_ctx* ctx, const float* in, int32_t n, int32_t* out);
+
 
 /* ------------------------------------------- allocation-free variant */
 /* No counterpart in the reference: an `estimate_depth` for callers that may

@@ -20,10 +20,10 @@ cudaError_t launch_census_rays(const DevView* d_views, const int32_t* d_tile_sta
                                cudaStream_t st);
 cudaError_t launch_init(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, int total_tiles, TileShape ts,
                         int nh, const uint64_t* census, const float2* rays, PlaneBuf out, unsigned long long* d_work,
-                        cudaStream_t st);
+                        cudaStream_t st, int variant);
 cudaError_t launch_pass(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, int total_tiles, TileShape ts,
                         uint64_t pass, float sig_inv, float sig_n, const uint64_t* census, const float2* rays,
-                        PlaneBuf prev, PlaneBuf next, unsigned long long* d_work, cudaStream_t st);
+                        PlaneBuf prev, PlaneBuf next, unsigned long long* d_work, cudaStream_t st, int variant);
 cudaError_t launch_gate(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, int total_tiles, TileShape ts,
                         float cost_thr, const uint64_t* census, PlaneBuf planes, float* depth, float* cost,
                         float* normal, cudaStream_t st);
@@ -156,7 +156,7 @@ struct rcmvs_scene {
 namespace {
 
 enum { S_JOBS = 0, S_JOBSTART = 1, S_CGRAY = 2, S_CCEN = 3, S_FIELD_PL = 4, S_FIELD_H = 5, S_FIELD_C = 6,
-       S_FIELD_HS = 7, S_F2I = 8 };
+       S_FIELD_HS = 7, S_F2I = 8, S_DIV_B = 9, S_DIV_OK = 10 };
 
 int fail(rcmvs_ctx* ctx, int code, const std::string& msg) {
     if (ctx) ctx->err = msg;
@@ -196,8 +196,8 @@ TileShape tile_of(const rcmvs_options* o) {
 }
 
 int ensure_tile(rcmvs_ctx* ctx, TileShape ts) {
-    if (ts.tw <= 0 || ts.th <= 0 || ts.tw * ts.th > 1024 || (ts.tw * ts.th) % 32 != 0 || ts.tw > 256)
-        return fail(ctx, RCMVS_E_ARG, "tile shape must be tw*th <= 1024 and a multiple of 32");
+    if (ts.tw <= 0 || ts.th <= 0 || ts.tw * ts.th > 256 || (ts.tw * ts.th) % 32 != 0)
+        return fail(ctx, RCMVS_E_ARG, "tile shape must have tw*th <= 256 threads, a multiple of 32");
     if (stereo_smem_bytes(ts) > 200 * 1024) return fail(ctx, RCMVS_E_LIMIT, "tile shape needs too much shared memory");
     if (ctx->configured.tw != ts.tw || ctx->configured.th != ts.th) {
         CK(stereo_configure(ts));
@@ -479,7 +479,7 @@ int rcmvs_scene_estimate_depth(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job*
         if ((uint32_t)std::max(V.w, V.h) > opts->max_dim)
             return fail(ctx, RCMVS_E_ARG, "reference view long side exceeds max_dim");
     }
-    if (opts->flags != 0) return fail(ctx, RCMVS_E_ARG, "opts->flags must be 0");
+    if (opts->flags & ~RCMVS_FLAG_ONE_CANDIDATE) return fail(ctx, RCMVS_E_ARG, "unknown bits in opts->flags");
     if (n_jobs == 0) return RCMVS_OK;
     const TileShape ts = tile_of(opts);
     CK(cudaSetDevice(ctx->device));
@@ -510,7 +510,8 @@ int rcmvs_scene_estimate_depth(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job*
     PlaneBuf A{sc->plane_a, sc->pcost_a}, B{sc->plane_b, sc->pcost_b};
     const SpanHook hk = ctx->hook();
     hk.begin("stereo_init");
-    CK(launch_init(dj, dst, n_jobs, (int)tiles, ts, nh, sc->census, sc->rays, A, dw, st));
+    const int variant = (opts->flags & RCMVS_FLAG_ONE_CANDIDATE) ? 1 : 0;
+    CK(launch_init(dj, dst, n_jobs, (int)tiles, ts, nh, sc->census, sc->rays, A, dw, st, variant));
     hk.end("stereo_init");
     const uint64_t n_passes = (uint64_t)std::max<uint32_t>(opts->sweeps, 1u) * 2;
     for (uint64_t pass = 0; pass < n_passes; ++pass) {
@@ -519,7 +520,8 @@ int rcmvs_scene_estimate_depth(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job*
         const float sig_inv = 0.02f * powf_host(0.28f, t * 4.0f);
         const float sig_n = 0.30f * powf_host(0.42f, t * 4.0f);
         hk.begin("stereo_pass");
-        CK(launch_pass(dj, dst, n_jobs, (int)tiles, ts, pass, sig_inv, sig_n, sc->census, sc->rays, A, B, dw, st));
+        CK(launch_pass(dj, dst, n_jobs, (int)tiles, ts, pass, sig_inv, sig_n, sc->census, sc->rays, A, B, dw, st,
+                       variant));
         hk.end("stereo_pass");
         std::swap(A, B);
     }

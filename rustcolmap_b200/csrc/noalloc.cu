@@ -29,10 +29,10 @@ cudaError_t launch_census_rays(const DevView* d_views, const int32_t* d_tile_sta
                                cudaStream_t st);
 cudaError_t launch_init(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, int total_tiles, TileShape ts,
                         int nh, const uint64_t* census, const float2* rays, PlaneBuf out, unsigned long long* d_work,
-                        cudaStream_t st);
+                        cudaStream_t st, int variant);
 cudaError_t launch_pass(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, int total_tiles, TileShape ts,
                         uint64_t pass, float sig_inv, float sig_n, const uint64_t* census, const float2* rays,
-                        PlaneBuf prev, PlaneBuf next, unsigned long long* d_work, cudaStream_t st);
+                        PlaneBuf prev, PlaneBuf next, unsigned long long* d_work, cudaStream_t st, int variant);
 cudaError_t launch_gate(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, int total_tiles, TileShape ts,
                         float cost_thr, const uint64_t* census, PlaneBuf planes, float* depth, float* cost,
                         float* normal, cudaStream_t st);
@@ -105,7 +105,7 @@ extern "C" int rcmvs_estimate_depth_noalloc(const rcmvs_view* views, int32_t n_v
                                             const rcmvs_options* opts, float* depth_dev, float* cost_dev,
                                             void* stream) {
     if (!views || n_views <= 0 || ref_idx < 0 || ref_idx >= n_views || n_src < 0 || (n_src > 0 && !srcs) || !opts ||
-        !depth_dev || !cost_dev || opts->flags != 0)
+        !depth_dev || !cost_dev || (opts->flags & ~RCMVS_FLAG_ONE_CANDIDATE))
         return RCMVS_E_ARG;
     if (!(finite_pos(zmin) && finite_pos(zmax))) return RCMVS_E_ARG;
     if (n_src > RCMVS_NOALLOC_MAX_SOURCES) return RCMVS_E_LIMIT;
@@ -124,7 +124,8 @@ extern "C" int rcmvs_estimate_depth_noalloc(const rcmvs_view* views, int32_t n_v
     }
     TileShape ts{16, 16};
     if (opts->tile_w > 0 && opts->tile_h > 0) ts = TileShape{(int)opts->tile_w, (int)opts->tile_h};
-    if (ts.tw * ts.th > 1024 || (ts.tw * ts.th) % 32 != 0 || stereo_smem_bytes(ts) > 48 * 1024) return RCMVS_E_ARG;
+    if (ts.tw <= 0 || ts.th <= 0 || ts.tw * ts.th > 256 || (ts.tw * ts.th) % 32 != 0 || stereo_smem_bytes(ts) > 48 * 1024)
+        return RCMVS_E_ARG;
 
     void* base = nullptr;
     int rc = scratch_for_current_device(&base);
@@ -221,13 +222,15 @@ extern "C" int rcmvs_estimate_depth_noalloc(const rcmvs_view* views, int32_t n_v
     }
     NCK(launch_census_rays(d_views, d_tile_start, nv, tiles, gray, census, rays, d_cams, st));
     const int nh = (int)(opts->num_hyp > 2u ? opts->num_hyp : 2u);
-    NCK(launch_init(d_job, d_job_start, 1, J.tiles, ts, nh, census, rays, A, nullptr, st));
+    const int variant = (opts->flags & RCMVS_FLAG_ONE_CANDIDATE) ? 1 : 0;
+    NCK(launch_init(d_job, d_job_start, 1, J.tiles, ts, nh, census, rays, A, nullptr, st, variant));
     const uint64_t n_passes = (uint64_t)(opts->sweeps > 1u ? opts->sweeps : 1u) * 2;
     for (uint64_t pass = 0; pass < n_passes; ++pass) {
         const float t = (float)pass / (float)n_passes;  // stereo.rs:275-277
         const float sig_inv = 0.02f * powf(0.28f, t * 4.0f);
         const float sig_n = 0.30f * powf(0.42f, t * 4.0f);
-        NCK(launch_pass(d_job, d_job_start, 1, J.tiles, ts, pass, sig_inv, sig_n, census, rays, A, Bp, nullptr, st));
+        NCK(launch_pass(d_job, d_job_start, 1, J.tiles, ts, pass, sig_inv, sig_n, census, rays, A, Bp, nullptr, st,
+                        variant));
         PlaneBuf tmp = A;
         A = Bp;
         Bp = tmp;

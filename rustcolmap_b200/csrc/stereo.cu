@@ -136,11 +136,88 @@ struct WorkCount {
 };
 
 // ---------------------------------------------------------------- plane_cost
-// stereo.rs:158-228.  (lx, ly): the pixel's position in the tile; window
-// cell (dx, dy) of the pixel is shared cell (ly+dy)*stw + lx+dx (dx, dy in
-// 0..4), which holds the clamped pixel (stereo.rs:179-184).
-// FRONTO: n = (0,0,1).  Then denom = 0*xo + 0*yo + 1 is exactly 1.0 for the
-// finite rays the host admits, so z = d/1 = d, and both are skipped.
+// One support view in registers.
+struct SrcRegs {
+    float rs0, rs1, rs2, rs3, rs4, rs5, rs6, rs7, rs8, ts0, ts1, ts2, f, cx, cy, k;
+    int sw, sh;
+    const uint64_t* __restrict__ sc;
+};
+
+__device__ __forceinline__ SrcRegs load_src(const DevSrc& s, const uint64_t* __restrict__ census) {
+    SrcRegs r;
+    r.rs0 = s.rs[0];
+    r.rs1 = s.rs[1];
+    r.rs2 = s.rs[2];
+    r.rs3 = s.rs[3];
+    r.rs4 = s.rs[4];
+    r.rs5 = s.rs[5];
+    r.rs6 = s.rs[6];
+    r.rs7 = s.rs[7];
+    r.rs8 = s.rs[8];
+    r.ts0 = s.ts[0];
+    r.ts1 = s.ts[1];
+    r.ts2 = s.ts[2];
+    r.f = s.f;
+    r.cx = s.cx;
+    r.cy = s.cy;
+    r.k = s.k;
+    r.sw = s.w;
+    r.sh = s.h;
+    r.sc = census + s.off;
+    return r;
+}
+
+// The five window terms of one row of one support view (stereo.rs:181-214),
+// added to `sum` in dx order.  `row`: shared-tile index of the row's first
+// window cell.  FRONTO: n = (0,0,1); then denom = 0*xo + 0*yo + 1 is exactly
+// 1.0 for the finite rays the host admits, so z = d/1 = d, and both are
+// skipped.
+// The five window terms of one row of one support view (stereo.rs:181-214),
+// added to `sum` in dx order, with IEEE divides.  `row`: shared-tile index of
+// the row's first window cell.  FRONTO: n = (0,0,1); then denom =
+// 0*xo + 0*yo + 1 is exactly 1.0 for the finite rays the host admits, so
+// z = d/1 = d, and both are skipped.
+template <bool FRONTO, bool HSUM>
+__device__ __forceinline__ float cost_row(const Smem& sm, int row, const SrcRegs& s, float nx, float ny, float nz,
+                                          float d, float sum, int32_t& hs) {
+#pragma unroll
+    for (int dx = 0; dx < 5; ++dx) {
+        const float2 r = sm.ray[row + dx];
+        float term = 1.0f;
+        int32_t hterm = 48;
+        const float denom = FRONTO ? 1.0f : nx * r.x + ny * r.y + nz;
+        if (!(denom < 0.05f)) {
+            const float z = FRONTO ? d : d / denom;
+            const float xr = z * r.x;
+            const float yr = z * r.y;
+            const float xs = s.rs0 * xr + s.rs1 * yr + s.rs2 * z + s.ts0;
+            const float ys = s.rs3 * xr + s.rs4 * yr + s.rs5 * z + s.ts1;
+            const float zs = s.rs6 * xr + s.rs7 * yr + s.rs8 * z + s.ts2;
+            if (!(zs < 1e-3f)) {
+                const float xn = xs / zs;
+                const float yn = ys / zs;
+                const float dist = 1.0f + s.k * (xn * xn + yn * yn);
+                // `as i32`: truncation, saturating, NaN -> 0 (cvt.rzi)
+                const int u = __float2int_rz(s.f * xn * dist + s.cx);
+                const int v = __float2int_rz(s.f * yn * dist + s.cy);
+                if (u >= 0 && v >= 0 && u < s.sw && v < s.sh) {
+                    const uint64_t cs = __ldg(s.sc + (size_t)v * s.sw + u);
+                    const int h = __popcll(sm.cen[row + dx] ^ cs);
+                    term = sm.tab[h];
+                    hterm = h;
+                }
+            }
+        }
+        sum += term;
+        if (HSUM) hs += hterm;
+    }
+    return sum;
+}
+
+// stereo.rs:158-228, one candidate at a time.  (lx, ly): the pixel's
+// position in the tile; window cell (dx, dy) of the pixel is shared cell
+// (ly+dy)*stw + lx+dx (dx, dy in 0..4), which holds the clamped pixel
+// (stereo.rs:179-184).
 template <bool FRONTO, bool COUNT, bool HSUM>
 __device__ __forceinline__ float plane_cost(const Smem& sm, int stw, int lx, int ly, int nsrc,
                                             const uint64_t* __restrict__ census, float nx, float ny, float nz,
@@ -150,52 +227,10 @@ __device__ __forceinline__ float plane_cost(const Smem& sm, int stw, int lx, int
     const float thr = hint + 0.12f;
     if (COUNT) wc.evals++;
     for (int si = 0; si < nsrc; ++si) {
-        const DevSrc& s = sm.src[si];
-        const float rs0 = s.rs[0], rs1 = s.rs[1], rs2 = s.rs[2];
-        const float rs3 = s.rs[3], rs4 = s.rs[4], rs5 = s.rs[5];
-        const float rs6 = s.rs[6], rs7 = s.rs[7], rs8 = s.rs[8];
-        const float ts0 = s.ts[0], ts1 = s.ts[1], ts2 = s.ts[2];
-        const float f = s.f, cx = s.cx, cy = s.cy, k = s.k;
-        const int sw = s.w, sh = s.h;
-        const uint64_t* __restrict__ sc = census + s.off;
+        const SrcRegs s = load_src(sm.src[si], census);
         const float fsi = (float)(si + 1);
         for (int dy = 0; dy < 5; ++dy) {
-            const int row = (ly + dy) * stw + lx;
-#pragma unroll
-            for (int dx = 0; dx < 5; ++dx) {
-                const float2 r = sm.ray[row + dx];
-                float term = 1.0f;
-                int32_t hterm = 48;
-                float denom;
-                if (FRONTO)
-                    denom = 1.0f;
-                else
-                    denom = nx * r.x + ny * r.y + nz;
-                if (!(denom < 0.05f)) {
-                    const float z = FRONTO ? d : d / denom;
-                    const float xr = z * r.x;
-                    const float yr = z * r.y;
-                    const float xs = rs0 * xr + rs1 * yr + rs2 * z + ts0;
-                    const float ys = rs3 * xr + rs4 * yr + rs5 * z + ts1;
-                    const float zs = rs6 * xr + rs7 * yr + rs8 * z + ts2;
-                    if (!(zs < 1e-3f)) {
-                        const float xn = xs / zs;
-                        const float yn = ys / zs;
-                        const float dist = 1.0f + k * (xn * xn + yn * yn);
-                        // `as i32`: truncation, saturating, NaN -> 0 (cvt.rzi)
-                        const int u = __float2int_rz(f * xn * dist + cx);
-                        const int v = __float2int_rz(f * yn * dist + cy);
-                        if (u >= 0 && v >= 0 && u < sw && v < sh) {
-                            const uint64_t cs = __ldg(sc + (size_t)v * sw + u);
-                            const int h = __popcll(sm.cen[row + dx] ^ cs);
-                            term = sm.tab[h];
-                            hterm = h;
-                        }
-                    }
-                }
-                sum += term;
-                if (HSUM) hs += hterm;
-            }
+            sum = cost_row<FRONTO, HSUM>(sm, (ly + dy) * stw + lx, s, nx, ny, nz, d, sum, hs);
             if (COUNT) wc.rows++;
             const float rows_done = (float)(dy + 1);
             if (sum / (rows_done * 5.0f * fsi) > thr) {
@@ -261,8 +296,10 @@ __global__ void init_kernel(const DevJob* __restrict__ jobs, const int32_t* __re
 // stereo.rs:274-371: one double-buffered pass.  Reads `prev` only, writes
 // every pixel of `next` (the carried-over plane when nothing is accepted,
 // which equals the reference's copy_from_slice at :278).
-template <bool COUNT>
-__global__ void pass_kernel(const DevJob* __restrict__ jobs, const int32_t* __restrict__ job_start, int n_jobs,
+// MINB = 3 blocks of 256 per SM (<= 80 registers) measured fastest; 4 (64
+// registers) spills and loses.
+template <bool COUNT, int MINB>
+__global__ void __launch_bounds__(256, MINB) pass_kernel(const DevJob* __restrict__ jobs, const int32_t* __restrict__ job_start, int n_jobs,
                             int tw, int th, uint64_t pass, float sig_inv, float sig_n,
                             const uint64_t* __restrict__ census, const float2* __restrict__ rays, PlaneBuf prev,
                             PlaneBuf next, unsigned long long* d_work) {
@@ -308,7 +345,7 @@ __global__ void pass_kernel(const DevJob* __restrict__ jobs, const int32_t* __re
             const float zcand = d_plane / a_here;
             if (!(zlo <= zcand && zcand <= zhi)) continue;
             const float c = plane_cost<false, COUNT, false>(sm, stw, lx, ly, nsrc, census, nb.x, nb.y, nb.z,
-                                                            d_plane, best_c + 0.02f, total, wc, nullptr);
+                                                                  d_plane, best_c + 0.02f, total, wc, nullptr);
             if (c < best_c) {
                 best_c = c;
                 bn0 = nb.x;
@@ -337,8 +374,8 @@ __global__ void pass_kernel(const DevJob* __restrict__ jobs, const int32_t* __re
             const float a_here = nnx * ri.x + nny * ri.y + nnz;
             if (a_here < 0.1f) continue;
             const float d_plane = zcand * a_here;
-            const float c = plane_cost<false, COUNT, false>(sm, stw, lx, ly, nsrc, census, nnx, nny, nnz, d_plane,
-                                                            best_c + 0.02f, total, wc, nullptr);
+            const float c = plane_cost<false, COUNT, false>(sm, stw, lx, ly, nsrc, census, nnx, nny, nnz,
+                                                                  d_plane, best_c + 0.02f, total, wc, nullptr);
             if (c < best_c) {
                 best_c = c;
                 bn0 = nnx;
@@ -359,6 +396,82 @@ __global__ void pass_kernel(const DevJob* __restrict__ jobs, const int32_t* __re
         }
         next.nz[i] = o;
         next.cost[i] = oc;
+    }
+    if (COUNT) flush_work(wc, d_work);
+}
+
+// ---------------------------------------------------------------- row-step kernels
+// The same init and pass computations with per-thread candidate streams
+// advanced one 5-term window row per loop iteration: a lane whose candidate
+// aborts early starts its next candidate at once instead of idling until
+// every lane of the warp has finished the current one.  Each candidate's
+// rows, abort tests, hint and best-cost bookkeeping happen in the
+// reference's order, so results are bit-identical to the kernels above.
+
+__device__ __forceinline__ float hyp_depth(float inv_min, float inv_max, int hi, int nh) {
+    const float inv = inv_min + (inv_max - inv_min) * (float)hi / (float)(nh - 1);  // stereo.rs:259-260
+    return 1.0f / inv;
+}
+
+template <bool COUNT, int MINB>
+__global__ void __launch_bounds__(256, MINB)
+    init_rows_kernel(const DevJob* __restrict__ jobs, const int32_t* __restrict__ job_start, int n_jobs, int tw, int th,
+                     int nh, const uint64_t* __restrict__ census, const float2* __restrict__ rays, PlaneBuf out,
+                     unsigned long long* d_work) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const Smem sm = carve(smem_raw, tw, th);
+    Tile T;
+    load_tile(jobs, job_start, n_jobs, tw, th, census, rays, sm, T);
+    const DevJob* J = T.job;
+    const int lx = threadIdx.x % tw, ly = threadIdx.x / tw;
+    const int x = T.x0 + lx, y = T.y0 + ly;
+    const bool inside = x < J->w && y < J->h;
+    WorkCount wc{0, 0};
+    const int nsrc = J->nsrc;
+    const float total = 5.0f * 5.0f * (float)nsrc;
+    const float inv_min = J->inv_min, inv_max = J->inv_max;
+    float best_c = INFINITY, best_d = 0.f;
+    int hi = 0, si = 0, dy = 0;
+    float d = hyp_depth(inv_min, inv_max, 0, nh);
+    float sum = 0.f;
+    float thr = INFINITY;  // (best_c + 0.02) + 0.12 with best_c = +inf
+    int32_t hs = 0;
+    bool live = inside;
+    if (COUNT && live) wc.evals++;
+    while (live) {
+        bool fin = true, aborted = false;
+        if (nsrc > 0) {
+            const SrcRegs s = load_src(sm.src[si], census);
+            sum = cost_row<true, false>(sm, (ly + dy) * T.stw + lx, s, 0.f, 0.f, 1.f, d, sum, hs);
+            if (COUNT) wc.rows++;
+            aborted = sum / ((float)(dy + 1) * 5.0f * (float)(si + 1)) > thr;
+            fin = aborted || (si == nsrc - 1 && dy == 4);
+        }
+        if (fin) {
+            const float c = aborted ? 1e9f : sum / total;
+            if (c < best_c) {
+                best_c = c;
+                best_d = d;
+            }
+            if (++hi >= nh) {
+                live = false;
+            } else {
+                d = hyp_depth(inv_min, inv_max, hi, nh);
+                sum = 0.f;
+                si = 0;
+                dy = 0;
+                thr = (best_c + 0.02f) + 0.12f;
+                if (COUNT) wc.evals++;
+            }
+        } else if (++dy == 5) {
+            dy = 0;
+            ++si;
+        }
+    }
+    if (inside) {
+        const size_t i = (size_t)J->off + (size_t)y * J->w + x;
+        out.nz[i] = make_float4(0.0f, 0.0f, 1.0f, best_d);
+        out.cost[i] = fminf(best_c, 1.0f);
     }
     if (COUNT) flush_work(wc, d_work);
 }
@@ -426,38 +539,53 @@ cudaError_t stereo_configure(TileShape ts) {
     cudaError_t e;
     if ((e = cudaFuncSetAttribute(init_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) return e;
     if ((e = cudaFuncSetAttribute(init_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) return e;
-    if ((e = cudaFuncSetAttribute(pass_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) return e;
-    if ((e = cudaFuncSetAttribute(pass_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) return e;
+    const void* pk[] = {(const void*)pass_kernel<false, 3>, (const void*)pass_kernel<true, 3>};
+    for (const void* k : pk)
+        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) return e;
     if ((e = cudaFuncSetAttribute(cost_field_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) return e;
+    const void* ik[] = {(const void*)init_rows_kernel<false, 4>, (const void*)init_rows_kernel<true, 4>};
+    for (const void* k : ik)
+        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) return e;
     return cudaSuccess;
 }
 
 cudaError_t launch_init(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, int total_tiles, TileShape ts,
                         int nh, const uint64_t* census, const float2* rays, PlaneBuf out, unsigned long long* d_work,
-                        cudaStream_t st) {
+                        cudaStream_t st, int variant) {
     if (total_tiles <= 0) return cudaSuccess;
-    size_t sm = smem_bytes(ts.tw, ts.th);
-    if (d_work)
-        init_kernel<true><<<total_tiles, ts.tw * ts.th, sm, st>>>(d_jobs, d_job_start, n_jobs, ts.tw, ts.th, nh,
-                                                                  census, rays, out, d_work);
-    else
-        init_kernel<false><<<total_tiles, ts.tw * ts.th, sm, st>>>(d_jobs, d_job_start, n_jobs, ts.tw, ts.th, nh,
-                                                                   census, rays, out, nullptr);
+    const size_t sm = smem_bytes(ts.tw, ts.th);
+    const int nt = ts.tw * ts.th;
+    if (variant == 1) {
+        if (d_work)
+            init_kernel<true><<<total_tiles, nt, sm, st>>>(d_jobs, d_job_start, n_jobs, ts.tw, ts.th, nh, census, rays,
+                                                           out, d_work);
+        else
+            init_kernel<false><<<total_tiles, nt, sm, st>>>(d_jobs, d_job_start, n_jobs, ts.tw, ts.th, nh, census, rays,
+                                                            out, nullptr);
+    } else {
+        if (d_work)
+            init_rows_kernel<true, 4><<<total_tiles, nt, sm, st>>>(d_jobs, d_job_start, n_jobs, ts.tw, ts.th, nh, census,
+                                                                   rays, out, d_work);
+        else
+            init_rows_kernel<false, 4><<<total_tiles, nt, sm, st>>>(d_jobs, d_job_start, n_jobs, ts.tw, ts.th, nh,
+                                                                    census, rays, out, nullptr);
+    }
     return cudaGetLastError();
 }
 
 cudaError_t launch_pass(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, int total_tiles, TileShape ts,
                         uint64_t pass, float sig_inv, float sig_n, const uint64_t* census, const float2* rays,
-                        PlaneBuf prev, PlaneBuf next, unsigned long long* d_work, cudaStream_t st) {
+                        PlaneBuf prev, PlaneBuf next, unsigned long long* d_work, cudaStream_t st, int variant) {
+    (void)variant;  // one schedule: lanes of a warp stay on the same support view (shared gathers)
     if (total_tiles <= 0) return cudaSuccess;
-    size_t sm = smem_bytes(ts.tw, ts.th);
+    const size_t sm = smem_bytes(ts.tw, ts.th);
+    const int nt = ts.tw * ts.th;
     if (d_work)
-        pass_kernel<true><<<total_tiles, ts.tw * ts.th, sm, st>>>(d_jobs, d_job_start, n_jobs, ts.tw, ts.th, pass,
-                                                                  sig_inv, sig_n, census, rays, prev, next, d_work);
+        pass_kernel<true, 3><<<total_tiles, nt, sm, st>>>(d_jobs, d_job_start, n_jobs, ts.tw, ts.th, pass, sig_inv,
+                                                          sig_n, census, rays, prev, next, d_work);
     else
-        pass_kernel<false><<<total_tiles, ts.tw * ts.th, sm, st>>>(d_jobs, d_job_start, n_jobs, ts.tw, ts.th, pass,
-                                                                   sig_inv, sig_n, census, rays, prev, next,
-                                                                   nullptr);
+        pass_kernel<false, 3><<<total_tiles, nt, sm, st>>>(d_jobs, d_job_start, n_jobs, ts.tw, ts.th, pass, sig_inv,
+                                                           sig_n, census, rays, prev, next, nullptr);
     return cudaGetLastError();
 }
 

@@ -28,6 +28,7 @@ class MvsOptions:
     reproj_px: float = 0.0
     tile_w: int = 0
     tile_h: int = 0
+    flags: int = 0  # RCMVS_FLAG_* bits
 
     def to_c(self) -> _abi.Options:
         o = _abi.Options()
@@ -43,6 +44,7 @@ class MvsOptions:
         o.reproj_px = self.reproj_px
         o.tile_w = self.tile_w
         o.tile_h = self.tile_h
+        o.flags = self.flags
         return o
 
 

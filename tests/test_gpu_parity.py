@@ -282,3 +282,29 @@ def test_fusion_saturated_projection_matches_oracle(ctx):
         c = oracle.fuse_depth_maps(views, dms if mc else [None, dms[1]], off, [x for f in order for x in f],
                                    sparse, opts)
         _assert_same_cloud(g, c[:2])
+
+
+@pytest.mark.parametrize("ref", [1, 6])
+def test_row_step_and_one_candidate_kernels_agree(ctx, corner_scene, c1_opts, ref):
+    """The default row-step schedule and the one-candidate-at-a-time kernels
+    (RCMVS_FLAG_ONE_CANDIDATE) give the same bits, and the work counters
+    agree with the oracle's plane_cost call and row counts."""
+    import dataclasses
+    import os
+    v = corner_scene.views
+    srcs, zr, _ = mvs.plan(corner_scene.sparse, v, c1_opts)
+    a = mvs.estimate_depth(v, ref, srcs[ref], zr[ref, 0], zr[ref, 1], c1_opts, ctx, normals=True)
+    one = dataclasses.replace(c1_opts, flags=1)
+    b = mvs.estimate_depth(v, ref, srcs[ref], zr[ref, 0], zr[ref, 1], one, ctx, normals=True)
+    for x, y in ((a.depth, b.depth), (a.cost, b.cost), (a.normal, b.normal)):
+        assert_bits_equal(x, y)
+    os.environ["RCMVS_COUNT"] = "1"
+    cctx = mvs.Context(0)
+    del os.environ["RCMVS_COUNT"]
+    _, _, _, work = oracle.estimate_depth(v, ref, srcs[ref], zr[ref, 0], zr[ref, 1], c1_opts)
+    for o in (c1_opts, one):
+        ds = mvs.DeviceScene(v, cctx)
+        ds.estimate([(ref, srcs[ref], zr[ref, 0], zr[ref, 1])], o)
+        assert cctx.last_work() == work
+        ds.close()
+    cctx.close()
