@@ -278,6 +278,49 @@ int rcmvs_ctx_kernel_time(rcmvs_ctx* ctx, const char* name, double* ms_total, ui
 int rcmvs_selftest_f2i(rcmvs_ctx* ctx, const float* in, int32_t n, int32_t* out);
 
 
+/* ------------------------------------------- learned plane proposals */
+/* No counterpart in the reference, which seeds every pixel with the plane
+ * sweep.  A 6-layer 3x3 convolutional network (32 channels, ReLU; BF16
+ * weights and activations, FP32 accumulation on the tensor cores) reads a
+ * quarter-resolution input of 48 channels — a 32-plane census cost volume
+ * (fronto-parallel planes at the centres of 32 equal inverse-depth bins,
+ * mean Hamming fraction over a 3x3 window and the support views), the grey
+ * image /255, 15 zeros — and predicts 16 channels per quarter pixel: t (the
+ * inverse depth as a fraction of [1/zmax, 1/zmin]), a normal (3), a
+ * confidence logit, 11 zeros.  Tensors are NHWC, BF16 unless noted. */
+typedef struct rcmvs_net rcmvs_net;
+
+/* Number of f32 parameters: for each layer W[9][cout][cin] then b[cout],
+ * with (cin, cout) = (48,32), (32,32) x4, (32,16); padded entries are 0. */
+uint64_t rcmvs_net_param_count(void);
+/* params (nullable): initial parameters; NULL = He initialisation from seed. */
+int rcmvs_net_create(rcmvs_ctx* ctx, const float* params, uint64_t seed, rcmvs_net** out);
+void rcmvs_net_destroy(rcmvs_net* net);
+int rcmvs_net_get_params(rcmvs_net* net, float* out);
+/* Forward pass on device buffers: x_dev n*h*w*48 BF16 -> out_dev n*h*w*16 f32. */
+int rcmvs_net_forward(rcmvs_ctx* ctx, rcmvs_net* net, const void* x_dev, int32_t n, int32_t h,
+                      int32_t w, float* out_dev);
+/* One training step on device buffers.  labels_dev: n*h*w*8 f32 = (t*, n*x,
+ * n*y, n*z, valid, tolerance on t, 0, 0).  Loss per valid pixel:
+ * |t - t*| + (1 - cos(n, n*)) + 0.1 BCE(sigmoid(logit), |t - t*| < tol).
+ * apply != 0 takes an Adam step (lr); loss_out / grads_host (nullable)
+ * receive the mean loss and its gradient (f32, parameter layout). */
+int rcmvs_net_train_step(rcmvs_ctx* ctx, rcmvs_net* net, const void* x_dev,
+                         const float* labels_dev, int32_t n, int32_t h, int32_t w, float lr,
+                         int32_t apply, float* loss_out, float* grads_host);
+/* Network input of each job's reference view (quarter resolution
+ * (w/4)x(h/4), jobs back to back) into out_dev (BF16). */
+int rcmvs_scene_costvol(rcmvs_ctx* ctx, rcmvs_scene* scene, const rcmvs_job* jobs, int32_t n_jobs,
+                        void* out_dev);
+/* Stereo seeded by the network: pixels whose prediction has confidence >=
+ * conf_thr and passes the stereo gates start from the predicted plane; the
+ * others run the plane sweep; then 2*max(sweeps,1) passes and the gate, as
+ * rcmvs_scene_estimate_depth.  learned_pixels (nullable): pixels seeded by
+ * the network. */
+int rcmvs_scene_estimate_depth_learned(rcmvs_ctx* ctx, rcmvs_scene* scene, const rcmvs_job* jobs,
+                                       int32_t n_jobs, const rcmvs_options* opts, rcmvs_net* net,
+                                       float conf_thr, uint64_t* learned_pixels);
+
 /* ------------------------------------------- allocation-free variant */
 /* No counterpart in the reference: an `estimate_depth` for callers that may
  * not allocate device memory (an application whose GPU memory belongs to

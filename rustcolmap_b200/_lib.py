@@ -63,6 +63,14 @@ def mvs():
         "rcmvs_ctx_timing": ([vp, C.c_int], C.c_int),
         "rcmvs_ctx_kernel_time": ([vp, cp, vp, vp], C.c_int),
         "rcmvs_estimate_depth_noalloc": ([vp, i32, i32, vp, i32, f64, f64, vp, vp, vp, vp], C.c_int),
+        "rcmvs_net_param_count": ([], u64),
+        "rcmvs_net_create": ([vp, vp, u64, vp], C.c_int),
+        "rcmvs_net_destroy": ([vp], None),
+        "rcmvs_net_get_params": ([vp, vp], C.c_int),
+        "rcmvs_net_forward": ([vp, vp, vp, i32, i32, i32, vp], C.c_int),
+        "rcmvs_net_train_step": ([vp, vp, vp, vp, i32, i32, i32, C.c_float, i32, vp, vp], C.c_int),
+        "rcmvs_scene_costvol": ([vp, vp, vp, i32, vp], C.c_int),
+        "rcmvs_scene_estimate_depth_learned": ([vp, vp, vp, i32, vp, vp, C.c_float, vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -100,5 +108,7 @@ _SIG_NAMES = [
     "rcmvs_scene_estimate_depth", "rcmvs_scene_fuse", "rcmvs_scene_get_depth",
     "rcmvs_scene_get_census", "rcmvs_scene_get_points", "rcmvs_plane_cost_field",
     "rcmvs_last_work", "rcmvs_selftest_f2i", "rcmvs_ctx_timing", "rcmvs_ctx_kernel_time",
-    "rcmvs_estimate_depth_noalloc",
+    "rcmvs_estimate_depth_noalloc", "rcmvs_net_param_count", "rcmvs_net_create", "rcmvs_net_destroy",
+    "rcmvs_net_get_params", "rcmvs_net_forward", "rcmvs_net_train_step", "rcmvs_scene_costvol",
+    "rcmvs_scene_estimate_depth_learned",
 ]

@@ -27,10 +27,11 @@ FLAGS = ARCH + [
 ]
 
 LIBS = {
-    "librcmvs.so": ["capi.cu", "census.cu", "stereo.cu", "fuse.cu", "noalloc.cu"],
+    "librcmvs.so": ["capi.cu", "census.cu", "stereo.cu", "fuse.cu", "noalloc.cu", "learned.cu", "learned_api.cu"],
     "librcscene.so": ["scene.cu"],
 }
-HEADERS = [os.path.join(CSRC, "rcmvs_internal.cuh"), os.path.join(ROOT, "include", "rcmvs.h"),
+HEADERS = [os.path.join(CSRC, "rcmvs_internal.cuh"), os.path.join(CSRC, "ctx_internal.cuh"),
+           os.path.join(CSRC, "learned.cuh"), os.path.join(ROOT, "include", "rcmvs.h"),
            os.path.join(ROOT, "include", "rcscene.h")]
 
 

@@ -1,0 +1,546 @@
+// learned.cu — learned plane proposals that seed patch-match (no reference
+// counterpart: the reference seeds every pixel with a 64-plane sweep).
+//
+//   downsample4_kernel  grey -> quarter-resolution grey (4x4 box mean)
+//   costvol_kernel      32-plane fronto-parallel census cost volume at quarter
+//                       resolution: integer Hamming sums over a 3x3 window and
+//                       K support views, normalised to [0, 1]
+//   conv3x3_kernel      3x3 convolution as an implicit GEMM on the tensor
+//                       cores (mma.sync m16n8k16, BF16 in, FP32 accumulate)
+//   conv3x3_wgrad_kernel  weight gradient of the same convolution
+//   loss/Adam kernels   training
+//   init_learned_kernel patch-match init: confident pixels take the predicted
+//                       plane, the others fall back to the plane sweep
+//
+// Tensors are NHWC, BF16, channels padded to a multiple of 16.
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "rcmvs_internal.cuh"
+#include "learned.cuh"
+
+namespace rcmvs {
+
+namespace {
+
+typedef __nv_bfloat16 bf16;
+
+__device__ __forceinline__ int find_item(const int32_t* start, int n, int b) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (start[mid] <= b)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+// ------------------------------------------------------------ downsample
+__global__ void downsample4_kernel(const DevView* __restrict__ full, const DevView* __restrict__ quarter,
+                                   const int32_t* __restrict__ blk_start, int n_views, const uint8_t* __restrict__ gray,
+                                   uint8_t* __restrict__ gray_q) {
+    const int v = find_item(blk_start, n_views, blockIdx.x);
+    const DevView F = full[v], Q = quarter[v];
+    const int64_t i = (int64_t)(blockIdx.x - blk_start[v]) * blockDim.x + threadIdx.x;
+    if (i >= (int64_t)Q.w * Q.h) return;
+    const int x = (int)(i % Q.w), y = (int)(i / Q.w);
+    const uint8_t* g = gray + F.off;
+    int s = 0;
+#pragma unroll
+    for (int dy = 0; dy < 4; ++dy)
+#pragma unroll
+        for (int dx = 0; dx < 4; ++dx) s += g[(size_t)(4 * y + dy) * F.w + 4 * x + dx];
+    gray_q[Q.off + i] = (uint8_t)((s + 8) >> 4);
+}
+
+// ------------------------------------------------------------ cost volume
+// One thread per quarter-resolution pixel of a job.  Output channel p < 32 is
+// the mean Hamming fraction of fronto-parallel plane p (inverse depths at the
+// centres of 32 equal bins of [1/zmax, 1/zmin]); channel 32 is grey/255;
+// channels 33..47 are zero.
+__global__ void costvol_kernel(const DevJob* __restrict__ jobs, const int32_t* __restrict__ blk_start, int n_jobs,
+                               const int64_t* __restrict__ out_off, const uint64_t* __restrict__ census_q,
+                               const float2* __restrict__ rays_q, const uint8_t* __restrict__ gray_q,
+                               bf16* __restrict__ out) {
+    const int j = find_item(blk_start, n_jobs, blockIdx.x);
+    const DevJob& J = jobs[j];
+    const int64_t i = (int64_t)(blockIdx.x - blk_start[j]) * blockDim.x + threadIdx.x;
+    if (i >= (int64_t)J.w * J.h) return;
+    const int x = (int)(i % J.w), y = (int)(i / J.w);
+    const size_t base = (size_t)J.off;
+    uint64_t cref[9];
+    float2 ray[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        const int xx = min(max(x + q % 3 - 1, 0), J.w - 1);
+        const int yy = min(max(y + q / 3 - 1, 0), J.h - 1);
+        cref[q] = census_q[base + (size_t)yy * J.w + xx];
+        ray[q] = rays_q[base + (size_t)yy * J.w + xx];
+    }
+    bf16* o = out + (size_t)(out_off[j] + i) * COSTVOL_C;
+    const float norm = 1.0f / (9.0f * 48.0f * (float)max(J.nsrc, 1));
+    for (int p = 0; p < COSTVOL_PLANES; ++p) {
+        const float inv = J.inv_min + (J.inv_max - J.inv_min) * ((float)p + 0.5f) / (float)COSTVOL_PLANES;
+        const float d = 1.0f / inv;
+        int hsum = 0;
+        for (int s = 0; s < J.nsrc; ++s) {
+            const DevSrc& S = J.src[s];
+            const uint64_t* sc = census_q + S.off;
+#pragma unroll
+            for (int q = 0; q < 9; ++q) {
+                const float xr = d * ray[q].x, yr = d * ray[q].y;
+                const float xs = S.rs[0] * xr + S.rs[1] * yr + S.rs[2] * d + S.ts[0];
+                const float ys = S.rs[3] * xr + S.rs[4] * yr + S.rs[5] * d + S.ts[1];
+                const float zs = S.rs[6] * xr + S.rs[7] * yr + S.rs[8] * d + S.ts[2];
+                int h = 48;
+                if (zs >= 1e-3f) {
+                    const float xn = __fdividef(xs, zs), yn = __fdividef(ys, zs);
+                    const float dist = 1.0f + S.k * (xn * xn + yn * yn);
+                    const int u = __float2int_rz(S.f * xn * dist + S.cx);
+                    const int v = __float2int_rz(S.f * yn * dist + S.cy);
+                    if (u >= 0 && v >= 0 && u < S.w && v < S.h) h = __popcll(cref[q] ^ sc[(size_t)v * S.w + u]);
+                }
+                hsum += h;
+            }
+        }
+        o[p] = __float2bfloat16((float)hsum * norm);
+    }
+    o[COSTVOL_PLANES] = __float2bfloat16((float)gray_q[base + i] * (1.0f / 255.0f));
+    for (int c = COSTVOL_PLANES + 1; c < COSTVOL_C; ++c) o[c] = __float2bfloat16(0.0f);
+}
+
+// ------------------------------------------------------------ convolution
+// mma.sync.m16n8k16 BF16 -> FP32.  Fragment layout (PTX ISA, "Matrix
+// Fragments for mma.m16n8k16 with floating point type"): lane = 4*g + t;
+// A rows g and g+8, columns 2t..2t+1 and 2t+8..2t+9; B column g, rows
+// 2t..2t+1 and 2t+8..2t+9; C rows g and g+8, columns 2t..2t+1.
+__device__ __forceinline__ void mma_bf16(float* c, const uint32_t* a, uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ uint32_t pack2(bf16 lo, bf16 hi) {
+    return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
+}
+
+constexpr int TILE_H = 8, TILE_W = 16;  // output pixels per block: 8 rows x 16 columns (4 warps x 2 rows)
+
+// y = conv3x3(x, w) + b, "same" zero padding; optional ReLU; optional f32
+// output.  w: [9][COUT][CIN] BF16.  mask (optional): x is multiplied by
+// (mask > 0) on load (ReLU derivative of the layer that produced x).
+template <int CIN, int COUT, bool RELU, bool OUT_F32, bool MASK>
+__global__ void __launch_bounds__(128) conv3x3_kernel(const bf16* __restrict__ x, const bf16* __restrict__ mask, int H,
+                                                      int W, const bf16* __restrict__ wgt,
+                                                      const float* __restrict__ bias, void* __restrict__ y) {
+    constexpr int SPX = CIN + 8;   // shared pixel stride (bank spread)
+    constexpr int SWR = CIN + 8;   // shared weight row stride
+    extern __shared__ __align__(16) unsigned char smem[];
+    bf16* sx = reinterpret_cast<bf16*>(smem);
+    bf16* sw = sx + (TILE_H + 2) * (TILE_W + 2) * SPX;
+    const int n = blockIdx.z, x0 = blockIdx.x * TILE_W, y0 = blockIdx.y * TILE_H;
+    const size_t img = (size_t)n * H * W;
+    for (int i = threadIdx.x; i < (TILE_H + 2) * (TILE_W + 2) * (CIN / 8); i += 128) {
+        const int c8 = i % (CIN / 8), p = i / (CIN / 8);
+        const int gy = y0 - 1 + p / (TILE_W + 2), gx = x0 - 1 + p % (TILE_W + 2);
+        uint4 v = make_uint4(0, 0, 0, 0);
+        if (gy >= 0 && gy < H && gx >= 0 && gx < W) {
+            const size_t gi = (img + (size_t)gy * W + gx) * CIN + c8 * 8;
+            v = *reinterpret_cast<const uint4*>(x + gi);
+            if (MASK) {
+                const uint4 m = *reinterpret_cast<const uint4*>(mask + gi);
+                const bf16* mv = reinterpret_cast<const bf16*>(&m);
+                bf16* xv = reinterpret_cast<bf16*>(&v);
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                    if (!(__bfloat162float(mv[q]) > 0.0f)) xv[q] = __float2bfloat16(0.0f);
+            }
+        }
+        *reinterpret_cast<uint4*>(sx + p * SPX + c8 * 8) = v;
+    }
+    for (int i = threadIdx.x; i < 9 * COUT * (CIN / 8); i += 128) {
+        const int c8 = i % (CIN / 8), r = i / (CIN / 8);
+        *reinterpret_cast<uint4*>(sw + r * SWR + c8 * 8) = *reinterpret_cast<const uint4*>(wgt + (size_t)r * CIN + c8 * 8);
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    float acc[2][COUT / 8][4];
+#pragma unroll
+    for (int m = 0; m < 2; ++m)
+#pragma unroll
+        for (int nt = 0; nt < COUT / 8; ++nt) acc[m][nt][0] = acc[m][nt][1] = acc[m][nt][2] = acc[m][nt][3] = 0.f;
+#pragma unroll 1
+    for (int tap = 0; tap < 9; ++tap) {
+        const int ky = tap / 3, kx = tap % 3;
+#pragma unroll
+        for (int kc = 0; kc < CIN / 16; ++kc) {
+            uint32_t a[2][4];
+#pragma unroll
+            for (int m = 0; m < 2; ++m) {
+                const int row = warp * 2 + m + ky;
+                const bf16* p0 = sx + (row * (TILE_W + 2) + g + kx) * SPX + kc * 16 + 2 * t;
+                const bf16* p1 = p0 + 8 * SPX;
+                a[m][0] = *reinterpret_cast<const uint32_t*>(p0);
+                a[m][1] = *reinterpret_cast<const uint32_t*>(p1);
+                a[m][2] = *reinterpret_cast<const uint32_t*>(p0 + 8);
+                a[m][3] = *reinterpret_cast<const uint32_t*>(p1 + 8);
+            }
+#pragma unroll
+            for (int nt = 0; nt < COUT / 8; ++nt) {
+                const bf16* q = sw + (tap * COUT + nt * 8 + g) * SWR + kc * 16 + 2 * t;
+                const uint32_t b0 = *reinterpret_cast<const uint32_t*>(q);
+                const uint32_t b1 = *reinterpret_cast<const uint32_t*>(q + 8);
+                mma_bf16(acc[0][nt], a[0], b0, b1);
+                mma_bf16(acc[1][nt], a[1], b0, b1);
+            }
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < 2; ++m) {
+        const int oy = y0 + warp * 2 + m;
+        if (oy >= H) continue;
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {
+            const int ox = x0 + g + 8 * half;
+            if (ox >= W) continue;
+            const size_t o = (img + (size_t)oy * W + ox) * COUT;
+#pragma unroll
+            for (int nt = 0; nt < COUT / 8; ++nt) {
+                const int c = nt * 8 + 2 * t;
+                float v0 = acc[m][nt][2 * half] + (bias ? bias[c] : 0.f);
+                float v1 = acc[m][nt][2 * half + 1] + (bias ? bias[c + 1] : 0.f);
+                if (RELU) {
+                    v0 = fmaxf(v0, 0.f);
+                    v1 = fmaxf(v1, 0.f);
+                }
+                if (OUT_F32) {
+                    float* yo = reinterpret_cast<float*>(y) + o + c;
+                    yo[0] = v0;
+                    yo[1] = v1;
+                } else {
+                    *reinterpret_cast<uint32_t*>(reinterpret_cast<bf16*>(y) + o + c) =
+                        pack2(__float2bfloat16(v0), __float2bfloat16(v1));
+                }
+            }
+        }
+    }
+}
+
+// dW[tap][co][ci] += sum_p dy[p][co] * x[p + tap][ci] over the block's pixel
+// tiles; dy is masked by (mask > 0) when MASK.  Grid: (tile blocks, 9 taps).
+// Per warp: M = COUT rows (co), N = CIN columns (ci), K = 32 of the tile's
+// 128 pixels; partial sums are reduced in shared memory and added to dW.
+template <int CIN, int COUT, bool MASK>
+__global__ void __launch_bounds__(128) conv3x3_wgrad_kernel(const bf16* __restrict__ x, const bf16* __restrict__ dy,
+                                                            const bf16* __restrict__ mask, int N, int H, int W,
+                                                            float* __restrict__ dW) {
+    constexpr int SPX = CIN + 8;
+    constexpr int SPY = COUT + 8;
+    extern __shared__ __align__(16) unsigned char smem[];
+    bf16* sx = reinterpret_cast<bf16*>(smem);
+    bf16* sy = sx + (TILE_H + 2) * (TILE_W + 2) * SPX;
+    float* red = reinterpret_cast<float*>(sy + TILE_H * TILE_W * SPY);
+    const int tap = blockIdx.y, ky = tap / 3, kx = tap % 3;
+    const int tiles_x = (W + TILE_W - 1) / TILE_W, tiles_y = (H + TILE_H - 1) / TILE_H;
+    const int n_tiles = N * tiles_x * tiles_y;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    constexpr int MT = COUT / 16, NT = CIN / 8;
+    float acc[MT][NT][4];
+#pragma unroll
+    for (int m = 0; m < MT; ++m)
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt) acc[m][nt][0] = acc[m][nt][1] = acc[m][nt][2] = acc[m][nt][3] = 0.f;
+    for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+        const int n = tile / (tiles_x * tiles_y), r = tile % (tiles_x * tiles_y);
+        const int x0 = (r % tiles_x) * TILE_W, y0 = (r / tiles_x) * TILE_H;
+        const size_t img = (size_t)n * H * W;
+        __syncthreads();
+        for (int i = threadIdx.x; i < (TILE_H + 2) * (TILE_W + 2) * (CIN / 8); i += 128) {
+            const int c8 = i % (CIN / 8), p = i / (CIN / 8);
+            const int gy = y0 - 1 + p / (TILE_W + 2), gx = x0 - 1 + p % (TILE_W + 2);
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if (gy >= 0 && gy < H && gx >= 0 && gx < W)
+                v = *reinterpret_cast<const uint4*>(x + (img + (size_t)gy * W + gx) * CIN + c8 * 8);
+            *reinterpret_cast<uint4*>(sx + p * SPX + c8 * 8) = v;
+        }
+        for (int i = threadIdx.x; i < TILE_H * TILE_W * (COUT / 8); i += 128) {
+            const int c8 = i % (COUT / 8), p = i / (COUT / 8);
+            const int gy = y0 + p / TILE_W, gx = x0 + p % TILE_W;
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if (gy < H && gx < W) {
+                const size_t gi = (img + (size_t)gy * W + gx) * COUT + c8 * 8;
+                v = *reinterpret_cast<const uint4*>(dy + gi);
+                if (MASK) {
+                    const uint4 mm = *reinterpret_cast<const uint4*>(mask + gi);
+                    const bf16* mv = reinterpret_cast<const bf16*>(&mm);
+                    bf16* yv = reinterpret_cast<bf16*>(&v);
+#pragma unroll
+                    for (int q = 0; q < 8; ++q)
+                        if (!(__bfloat162float(mv[q]) > 0.0f)) yv[q] = __float2bfloat16(0.0f);
+                }
+            }
+            *reinterpret_cast<uint4*>(sy + p * SPY + c8 * 8) = v;
+        }
+        __syncthreads();
+        // warp w: pixels k in [32w, 32w+32) of the tile = 2 k-steps of 16
+#pragma unroll
+        for (int ks = 0; ks < 2; ++ks) {
+            const int kbase = warp * 32 + ks * 16;
+            const int pa = kbase + 2 * t, pb = pa + 8;  // pixel indices of this lane's k pairs
+            uint32_t a[MT][4];
+#pragma unroll
+            for (int m = 0; m < MT; ++m) {
+                const int co = m * 16 + g;
+                a[m][0] = pack2(sy[pa * SPY + co], sy[(pa + 1) * SPY + co]);
+                a[m][1] = pack2(sy[pa * SPY + co + 8], sy[(pa + 1) * SPY + co + 8]);
+                a[m][2] = pack2(sy[pb * SPY + co], sy[(pb + 1) * SPY + co]);
+                a[m][3] = pack2(sy[pb * SPY + co + 8], sy[(pb + 1) * SPY + co + 8]);
+            }
+            // x at pixel p shifted by the tap: shared cell (p/16 + ky, p%16 + kx)
+            const int xa0 = ((pa / TILE_W) + ky) * (TILE_W + 2) + (pa % TILE_W) + kx;
+            const int xa1 = (((pa + 1) / TILE_W) + ky) * (TILE_W + 2) + ((pa + 1) % TILE_W) + kx;
+            const int xb0 = ((pb / TILE_W) + ky) * (TILE_W + 2) + (pb % TILE_W) + kx;
+            const int xb1 = (((pb + 1) / TILE_W) + ky) * (TILE_W + 2) + ((pb + 1) % TILE_W) + kx;
+#pragma unroll
+            for (int nt = 0; nt < NT; ++nt) {
+                const int ci = nt * 8 + g;
+                const uint32_t b0 = pack2(sx[xa0 * SPX + ci], sx[xa1 * SPX + ci]);
+                const uint32_t b1 = pack2(sx[xb0 * SPX + ci], sx[xb1 * SPX + ci]);
+#pragma unroll
+                for (int m = 0; m < MT; ++m) mma_bf16(acc[m][nt], a[m], b0, b1);
+            }
+        }
+    }
+    // reduce the 4 warps: red[co][ci]
+    __syncthreads();
+    for (int i = threadIdx.x; i < COUT * CIN; i += 128) red[i] = 0.f;
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < MT; ++m)
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt) {
+            const int co = m * 16 + g, ci = nt * 8 + 2 * t;
+            atomicAdd(&red[co * CIN + ci], acc[m][nt][0]);
+            atomicAdd(&red[co * CIN + ci + 1], acc[m][nt][1]);
+            atomicAdd(&red[(co + 8) * CIN + ci], acc[m][nt][2]);
+            atomicAdd(&red[(co + 8) * CIN + ci + 1], acc[m][nt][3]);
+        }
+    __syncthreads();
+    for (int i = threadIdx.x; i < COUT * CIN; i += 128) atomicAdd(&dW[(size_t)tap * COUT * CIN + i], red[i]);
+}
+
+// db[c] += sum over pixels of dy[p][c] * (mask[p][c] > 0)
+template <int C, bool MASK>
+__global__ void bias_grad_kernel(const bf16* __restrict__ dy, const bf16* __restrict__ mask, int64_t npx,
+                                 float* __restrict__ db) {
+    float s[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) s[c] = 0.f;
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < npx; p += (int64_t)gridDim.x * blockDim.x)
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            float v = __bfloat162float(dy[p * C + c]);
+            if (MASK && !(__bfloat162float(mask[p * C + c]) > 0.f)) v = 0.f;
+            s[c] += v;
+        }
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+        float v = s[c];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0) atomicAdd(&db[c], v);
+    }
+}
+
+// backward-data weights: wt[tap][ci][co] = w[8 - tap][co][ci]
+__global__ void flip_weights_kernel(const bf16* __restrict__ w, int cout, int cin, bf16* __restrict__ wt) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 9 * cout * cin) return;
+    const int ci = i % cin, co = (i / cin) % cout, tap = i / (cin * cout);
+    wt[((size_t)(8 - tap) * cin + ci) * cout + co] = w[i];
+}
+
+__global__ void to_bf16_kernel(const float* __restrict__ a, int64_t n, bf16* __restrict__ b) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) b[i] = __float2bfloat16(a[i]);
+}
+
+// Loss on the head output (16 channels, f32: t, nx, ny, nz, conf logit, 0...)
+// against labels (8 floats: t*, nx*, ny*, nz*, valid, tol, 0, 0):
+//   |t - t*| + LN (1 - cos(n, n*)) + LC BCE(sigmoid(c), |t - t*| < tol)
+// averaged over valid pixels; writes dL/dout (BF16, 16 channels) and adds the
+// summed loss and the valid count to acc[0..1].
+constexpr float LN = 1.0f, LC = 0.1f;
+__global__ void loss_kernel(const float* __restrict__ out, const float* __restrict__ lab, int64_t npx, float inv_n,
+                            bf16* __restrict__ dout, float* __restrict__ acc) {
+    float l = 0.f, cnt = 0.f;
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < npx; p += (int64_t)gridDim.x * blockDim.x) {
+        const float* o = out + p * NET_OUT_C;
+        const float* L = lab + p * 8;
+        float g[NET_OUT_C];
+#pragma unroll
+        for (int c = 0; c < NET_OUT_C; ++c) g[c] = 0.f;
+        if (L[4] > 0.5f) {
+            const float dt = o[0] - L[0];
+            l += fabsf(dt);
+            g[0] = (dt > 0.f ? 1.f : (dt < 0.f ? -1.f : 0.f));
+            const float nl = sqrtf(o[1] * o[1] + o[2] * o[2] + o[3] * o[3]) + 1e-6f;
+            const float c = (o[1] * L[1] + o[2] * L[2] + o[3] * L[3]) / nl;
+            l += LN * (1.f - c);
+#pragma unroll
+            for (int a = 0; a < 3; ++a) g[1 + a] = -LN * (L[1 + a] - c * o[1 + a] / nl) / nl;
+            const float pr = 1.f / (1.f + __expf(-o[4]));
+            const float tgt = fabsf(dt) < L[5] ? 1.f : 0.f;
+            l += LC * -(tgt * __logf(fmaxf(pr, 1e-7f)) + (1.f - tgt) * __logf(fmaxf(1.f - pr, 1e-7f)));
+            g[4] = LC * (pr - tgt);
+            cnt += 1.f;
+        }
+#pragma unroll
+        for (int c = 0; c < NET_OUT_C; ++c) dout[p * NET_OUT_C + c] = __float2bfloat16(g[c] * inv_n);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        l += __shfl_down_sync(0xffffffffu, l, o);
+        cnt += __shfl_down_sync(0xffffffffu, cnt, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(acc, l);
+        atomicAdd(acc + 1, cnt);
+    }
+}
+
+// Adam on the f32 master parameters (gradients scaled by gscale), then the
+// BF16 compute copy.  mask[i] = 0 pins padded weights at zero.
+__global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ gr, float* __restrict__ m,
+                            float* __restrict__ v, const uint8_t* __restrict__ mask, int64_t n, float lr, float b1,
+                            float b2, float eps, float bc1, float bc2, float gscale, bf16* __restrict__ pb) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (!mask[i]) {
+        pb[i] = __float2bfloat16(0.f);
+        return;
+    }
+    const float g = gr[i] * gscale;
+    const float mi = b1 * m[i] + (1.f - b1) * g;
+    const float vi = b2 * v[i] + (1.f - b2) * g * g;
+    m[i] = mi;
+    v[i] = vi;
+    const float pi = p[i] - lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+    p[i] = pi;
+    pb[i] = __float2bfloat16(pi);
+}
+
+}  // namespace
+
+// ------------------------------------------------------------ launchers
+cudaError_t launch_downsample4(const DevView* full, const DevView* quarter, const int32_t* blk_start, int n_views,
+                               int total_blocks, const uint8_t* gray, uint8_t* gray_q, cudaStream_t st) {
+    if (total_blocks <= 0) return cudaSuccess;
+    downsample4_kernel<<<total_blocks, 256, 0, st>>>(full, quarter, blk_start, n_views, gray, gray_q);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_costvol(const DevJob* jobs, const int32_t* blk_start, int n_jobs, int total_blocks,
+                           const int64_t* out_off, const uint64_t* census_q, const float2* rays_q,
+                           const uint8_t* gray_q, void* out, cudaStream_t st) {
+    if (total_blocks <= 0) return cudaSuccess;
+    costvol_kernel<<<total_blocks, 128, 0, st>>>(jobs, blk_start, n_jobs, out_off, census_q, rays_q, gray_q,
+                                                 reinterpret_cast<bf16*>(out));
+    return cudaGetLastError();
+}
+
+template <int CIN, int COUT, bool RELU, bool OUT_F32, bool MASK>
+static cudaError_t conv_t(const void* x, const void* mask, int N, int H, int W, const void* w, const float* b, void* y,
+                          cudaStream_t st) {
+    const size_t sm = sizeof(bf16) * ((TILE_H + 2) * (TILE_W + 2) * (CIN + 8) + 9 * COUT * (CIN + 8));
+    auto k = conv3x3_kernel<CIN, COUT, RELU, OUT_F32, MASK>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e) return e;
+    dim3 grid((W + TILE_W - 1) / TILE_W, (H + TILE_H - 1) / TILE_H, N);
+    k<<<grid, 128, sm, st>>>(reinterpret_cast<const bf16*>(x), reinterpret_cast<const bf16*>(mask), H, W,
+                             reinterpret_cast<const bf16*>(w), b, y);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_conv3x3(int cin, int cout, bool relu, bool out_f32, const void* x, const void* mask, int N, int H,
+                           int W, const void* w, const float* b, void* y, cudaStream_t st) {
+    const bool m = mask != nullptr;
+    if (cin == 48 && cout == 32 && relu && !out_f32 && !m) return conv_t<48, 32, true, false, false>(x, mask, N, H, W, w, b, y, st);
+    if (cin == 32 && cout == 32 && relu && !out_f32 && !m) return conv_t<32, 32, true, false, false>(x, mask, N, H, W, w, b, y, st);
+    if (cin == 32 && cout == 16 && !relu && out_f32 && !m) return conv_t<32, 16, false, true, false>(x, mask, N, H, W, w, b, y, st);
+    // backward data: input = masked upstream gradient, no bias, no ReLU
+    if (cin == 16 && cout == 32 && !relu && !out_f32 && !m) return conv_t<16, 32, false, false, false>(x, mask, N, H, W, w, b, y, st);
+    if (cin == 32 && cout == 32 && !relu && !out_f32 && m) return conv_t<32, 32, false, false, true>(x, mask, N, H, W, w, b, y, st);
+    return cudaErrorInvalidValue;
+}
+
+template <int CIN, int COUT, bool MASK>
+static cudaError_t wgrad_t(const void* x, const void* dy, const void* mask, int N, int H, int W, float* dW,
+                           cudaStream_t st) {
+    const size_t sm = sizeof(bf16) * ((TILE_H + 2) * (TILE_W + 2) * (CIN + 8) + TILE_H * TILE_W * (COUT + 8)) +
+                      sizeof(float) * COUT * CIN;
+    auto k = conv3x3_wgrad_kernel<CIN, COUT, MASK>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e) return e;
+    const int tiles = N * ((W + TILE_W - 1) / TILE_W) * ((H + TILE_H - 1) / TILE_H);
+    dim3 grid(std::min(tiles, 148 * 2), 9);
+    k<<<grid, 128, sm, st>>>(reinterpret_cast<const bf16*>(x), reinterpret_cast<const bf16*>(dy),
+                             reinterpret_cast<const bf16*>(mask), N, H, W, dW);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_conv3x3_wgrad(int cin, int cout, const void* x, const void* dy, const void* mask, int N, int H,
+                                 int W, float* dW, cudaStream_t st) {
+    const bool m = mask != nullptr;
+    if (cin == 48 && cout == 32 && m) return wgrad_t<48, 32, true>(x, dy, mask, N, H, W, dW, st);
+    if (cin == 32 && cout == 32 && m) return wgrad_t<32, 32, true>(x, dy, mask, N, H, W, dW, st);
+    if (cin == 32 && cout == 16 && !m) return wgrad_t<32, 16, false>(x, dy, mask, N, H, W, dW, st);
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_bias_grad(int c, const void* dy, const void* mask, int64_t npx, float* db, cudaStream_t st) {
+    const int blocks = (int)std::min<int64_t>((npx + 255) / 256, 148 * 4);
+    if (c == 32 && mask)
+        bias_grad_kernel<32, true><<<blocks, 256, 0, st>>>(reinterpret_cast<const bf16*>(dy),
+                                                           reinterpret_cast<const bf16*>(mask), npx, db);
+    else if (c == 16 && !mask)
+        bias_grad_kernel<16, false><<<blocks, 256, 0, st>>>(reinterpret_cast<const bf16*>(dy), nullptr, npx, db);
+    else
+        return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_flip_weights(const void* w, int cout, int cin, void* wt, cudaStream_t st) {
+    const int n = 9 * cout * cin;
+    flip_weights_kernel<<<(n + 255) / 256, 256, 0, st>>>(reinterpret_cast<const bf16*>(w), cout, cin,
+                                                         reinterpret_cast<bf16*>(wt));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_to_bf16(const float* a, int64_t n, void* b, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    to_bf16_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a, n, reinterpret_cast<bf16*>(b));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_loss(const float* out, const float* lab, int64_t npx, float inv_n, void* dout, float* acc,
+                        cudaStream_t st) {
+    const int blocks = (int)std::min<int64_t>((npx + 255) / 256, 148 * 4);
+    loss_kernel<<<blocks, 256, 0, st>>>(out, lab, npx, inv_n, reinterpret_cast<bf16*>(dout), acc);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adam(float* p, const float* g, float* m, float* v, const uint8_t* mask, int64_t n, float lr,
+                        float b1, float b2, float eps, float bc1, float bc2, float gscale, void* pb, cudaStream_t st) {
+    adam_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(p, g, m, v, mask, n, lr, b1, b2, eps, bc1, bc2, gscale,
+                                                             reinterpret_cast<bf16*>(pb));
+    return cudaGetLastError();
+}
+
+}  // namespace rcmvs

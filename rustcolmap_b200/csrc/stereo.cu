@@ -20,6 +20,7 @@
 // census with a 2-pixel clamped halo in shared memory; support-view census
 // words are gathered through the read-only path (L1/L2).
 #include "rcmvs_internal.cuh"
+#include "learned.cuh"
 
 namespace rcmvs {
 
@@ -476,6 +477,79 @@ __global__ void __launch_bounds__(256, MINB)
     if (COUNT) flush_work(wc, d_work);
 }
 
+// ---------------------------------------------------------------- learned init
+// Patch-match init from learned proposals (no reference counterpart).  A
+// pixel whose quarter-resolution cell predicts a plane with confidence
+// sigmoid(logit) >= conf_thr that passes the reference's own gates (positive
+// inverse depth, depth in [zmin/2, 2 zmax], n . ray >= 0.1) starts from that
+// plane with its full plane_cost; every other pixel runs the 64-plane sweep of
+// stereo.rs:247-269 unchanged.
+__global__ void __launch_bounds__(256, 3)
+    init_learned_kernel(const DevJob* __restrict__ jobs, const int32_t* __restrict__ job_start, int n_jobs, int tw,
+                        int th, int nh, const uint64_t* __restrict__ census, const float2* __restrict__ rays,
+                        PlaneBuf out, const float* __restrict__ pred, const int64_t* __restrict__ pred_off,
+                        float conf_thr, unsigned long long* d_learned) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const Smem sm = carve(smem_raw, tw, th);
+    Tile T;
+    load_tile(jobs, job_start, n_jobs, tw, th, census, rays, sm, T);
+    const DevJob* J = T.job;
+    const int j = (int)(J - jobs);
+    const int lx = threadIdx.x % tw, ly = threadIdx.x / tw;
+    const int x = T.x0 + lx, y = T.y0 + ly;
+    const bool inside = x < J->w && y < J->h;
+    bool learned = false;
+    if (inside) {
+        WorkCount wc{0, 0};
+        const int nsrc = J->nsrc;
+        const float total = 5.0f * 5.0f * (float)nsrc;
+        const float zlo = J->zmin * 0.5f, zhi = J->zmax * 2.0f;
+        const float2 ri = sm.ray[(ly + HALO) * T.stw + lx + HALO];
+        const int wq = J->w >> 2, hq = J->h >> 2;
+        float nx = 0.f, ny = 0.f, nz = 1.f, z = 0.f, a = 1.f;
+        if (wq > 0 && hq > 0) {
+            const int qx = min(x >> 2, wq - 1), qy = min(y >> 2, hq - 1);
+            const float* o = pred + (pred_off[j] + (int64_t)qy * wq + qx) * NET_OUT_C;
+            const float conf = 1.f / (1.f + __expf(-o[4]));
+            const float inv = J->inv_min + o[0] * (J->inv_max - J->inv_min);
+            const float len = sqrtf(o[1] * o[1] + o[2] * o[2] + o[3] * o[3]);
+            if (conf >= conf_thr && inv > 0.f && len > 1e-6f) {
+                nx = o[1] / len;
+                ny = o[2] / len;
+                nz = o[3] / len;
+                z = 1.f / inv;
+                a = nx * ri.x + ny * ri.y + nz;
+                learned = a >= 0.1f && z >= zlo && z <= zhi;
+            }
+        }
+        float4 plane;
+        float best_c;
+        if (learned) {
+            best_c = plane_cost<false, false, false>(sm, T.stw, lx, ly, nsrc, census, nx, ny, nz, z * a, INFINITY,
+                                                     total, wc, nullptr);
+            plane = make_float4(nx, ny, nz, z);
+        } else {
+            best_c = INFINITY;
+            float best_d = 0.f;
+            for (int hi = 0; hi < nh; ++hi) {
+                const float d = hyp_depth(J->inv_min, J->inv_max, hi, nh);
+                const float c = plane_cost<true, false, false>(sm, T.stw, lx, ly, nsrc, census, 0.f, 0.f, 1.f, d,
+                                                               best_c + 0.02f, total, wc, nullptr);
+                if (c < best_c) {
+                    best_c = c;
+                    best_d = d;
+                }
+            }
+            plane = make_float4(0.0f, 0.0f, 1.0f, best_d);
+        }
+        const size_t i = (size_t)J->off + (size_t)y * J->w + x;
+        out.nz[i] = plane;
+        out.cost[i] = fminf(best_c, 1.0f);
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, learned);
+    if ((threadIdx.x & 31) == 0 && bal) atomicAdd(d_learned, (unsigned long long)__popc(bal));
+}
+
 // ---------------------------------------------------------------- gate
 // stereo.rs:373-393 (+ normals, an extension)
 __global__ void gate_kernel(const DevJob* __restrict__ jobs, const int32_t* __restrict__ job_start, int n_jobs,
@@ -586,6 +660,19 @@ cudaError_t launch_pass(const DevJob* d_jobs, const int32_t* d_job_start, int n_
     else
         pass_kernel<false, 3><<<total_tiles, nt, sm, st>>>(d_jobs, d_job_start, n_jobs, ts.tw, ts.th, pass, sig_inv,
                                                            sig_n, census, rays, prev, next, nullptr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_init_learned(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, int total_tiles,
+                                TileShape ts, int nh, const uint64_t* census, const float2* rays, PlaneBuf out,
+                                const float* pred, const int64_t* pred_off, float conf_thr,
+                                unsigned long long* d_learned, cudaStream_t st) {
+    if (total_tiles <= 0) return cudaSuccess;
+    const size_t sm = smem_bytes(ts.tw, ts.th);
+    cudaError_t e = cudaFuncSetAttribute(init_learned_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e) return e;
+    init_learned_kernel<<<total_tiles, ts.tw * ts.th, sm, st>>>(d_jobs, d_job_start, n_jobs, ts.tw, ts.th, nh, census,
+                                                                rays, out, pred, pred_off, conf_thr, d_learned);
     return cudaGetLastError();
 }
 

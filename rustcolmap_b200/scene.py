@@ -216,10 +216,10 @@ def corner_room(seed=0, n_views=8, w=384, h=288, f=440.0, arc_deg=60.0, n_patche
 
 
 def orbit_room(seed=0, n_views=64, sizes=((960, 720),), f_rel=1.1, n_boxes=20, n_spheres=0, n_patches=200,
-               device=-1, normals=False, per_view_sparse=300, size_choice=None):
+               device=-1, normals=False, per_view_sparse=300, size_choice=None, arc_deg=360.0):
     """Room with 4 walls + floor, `n_boxes` textured boxes (0.2-1.0 units) and
     `n_spheres` spheres (radius 0.3-0.8) in the middle; `n_views` cameras on a
-    full orbit looking inward.  sizes: candidate (w, h); with size_choice
+    full orbit (or an arc of arc_deg degrees) looking inward.  sizes: candidate (w, h); with size_choice
     'random' each view draws one, else all views use sizes[0].  f = f_rel *
     long side."""
     rng = np.random.default_rng(seed)
@@ -248,7 +248,7 @@ def orbit_room(seed=0, n_views=64, sizes=((960, 720),), f_rel=1.1, n_boxes=20, n
     target = np.array([0.0, 0.0, 0.4])
     cams = []
     for i in range(n_views):
-        a = 2 * np.pi * i / n_views
+        a = np.deg2rad(arc_deg) * i / (n_views if arc_deg >= 360.0 else max(n_views - 1, 1))
         eye = np.array([4.3 * np.cos(a), 4.3 * np.sin(a), 1.8 + 0.25 * np.sin(5 * a)])
         R, t = look_at(eye, target)
         if size_choice == "random":
