@@ -312,14 +312,18 @@ int rcmvs_net_train_step(rcmvs_ctx* ctx, rcmvs_net* net, const void* x_dev,
  * (w/4)x(h/4), jobs back to back) into out_dev (BF16). */
 int rcmvs_scene_costvol(rcmvs_ctx* ctx, rcmvs_scene* scene, const rcmvs_job* jobs, int32_t n_jobs,
                         void* out_dev);
-/* Stereo seeded by the network: pixels whose prediction has confidence >=
- * conf_thr and passes the stereo gates start from the predicted plane; the
- * others run the plane sweep; then 2*max(sweeps,1) passes and the gate, as
+/* Stereo seeded by the network: a pixel whose prediction has confidence >=
+ * conf_thr starts from the best of n_local planes with the predicted normal
+ * and inverse depths spread over +-span/2 (fraction of the inverse-depth
+ * range) around the prediction (plane_cost with the sweep's early-abort
+ * hint; planes failing the stereo gates are skipped); the other pixels run
+ * the plane sweep; then 2*max(sweeps,1) passes and the gate, as
  * rcmvs_scene_estimate_depth.  learned_pixels (nullable): pixels seeded by
  * the network. */
 int rcmvs_scene_estimate_depth_learned(rcmvs_ctx* ctx, rcmvs_scene* scene, const rcmvs_job* jobs,
                                        int32_t n_jobs, const rcmvs_options* opts, rcmvs_net* net,
-                                       float conf_thr, uint64_t* learned_pixels);
+                                       float conf_thr, int32_t n_local, float span,
+                                       uint64_t* learned_pixels);
 
 /* ------------------------------------------- allocation-free variant */
 /* No counterpart in the reference: an `estimate_depth` for callers that may

@@ -70,7 +70,7 @@ def mvs():
         "rcmvs_net_forward": ([vp, vp, vp, i32, i32, i32, vp], C.c_int),
         "rcmvs_net_train_step": ([vp, vp, vp, vp, i32, i32, i32, C.c_float, i32, vp, vp], C.c_int),
         "rcmvs_scene_costvol": ([vp, vp, vp, i32, vp], C.c_int),
-        "rcmvs_scene_estimate_depth_learned": ([vp, vp, vp, i32, vp, vp, C.c_float, vp], C.c_int),
+        "rcmvs_scene_estimate_depth_learned": ([vp, vp, vp, i32, vp, vp, C.c_float, i32, C.c_float, vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)

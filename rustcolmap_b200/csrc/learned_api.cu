@@ -448,8 +448,9 @@ int rcmvs_scene_costvol(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job* jobs, 
 // fallback below conf_thr) -> 2*max(sweeps,1) Jacobi passes -> gate.
 int rcmvs_scene_estimate_depth_learned(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job* jobs, int32_t n_jobs,
                                        const rcmvs_options* opts, rcmvs_net* net, float conf_thr,
-                                       uint64_t* learned_pixels) {
-    if (!ctx || !sc || !opts || !net) return lfail(ctx, RCMVS_E_ARG, "rcmvs_scene_estimate_depth_learned: bad argument");
+                                       int32_t n_local, float span, uint64_t* learned_pixels) {
+    if (!ctx || !sc || !opts || !net || n_local < 1 || n_local > 256 || !(span >= 0.f && span <= 1.f))
+        return lfail(ctx, RCMVS_E_ARG, "rcmvs_scene_estimate_depth_learned: bad argument");
     int rc = check_jobs(ctx, sc, jobs, n_jobs);
     if (rc) return rc;
     LCK(cudaSetDevice(ctx->device));
@@ -551,7 +552,7 @@ int rcmvs_scene_estimate_depth_learned(rcmvs_ctx* ctx, rcmvs_scene* sc, const rc
     PlaneBuf A{sc->plane_a, sc->pcost_a}, B{sc->plane_b, sc->pcost_b};
     hk.begin("learned_init");
     LCK(launch_init_learned(dj, dst, n_jobs, (int)tiles, ts, nh, sc->census, sc->rays, A, (const float*)pred, dqoff,
-                            conf_thr, (unsigned long long*)pcnt, st));
+                            conf_thr, n_local, span, (unsigned long long*)pcnt, st));
     hk.end("learned_init");
     const uint64_t n_passes = (uint64_t)std::max<uint32_t>(opts->sweeps, 1u) * 2;
     for (uint64_t pass = 0; pass < n_passes; ++pass) {

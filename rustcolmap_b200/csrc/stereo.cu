@@ -480,15 +480,19 @@ __global__ void __launch_bounds__(256, MINB)
 // ---------------------------------------------------------------- learned init
 // Patch-match init from learned proposals (no reference counterpart).  A
 // pixel whose quarter-resolution cell predicts a plane with confidence
-// sigmoid(logit) >= conf_thr that passes the reference's own gates (positive
-// inverse depth, depth in [zmin/2, 2 zmax], n . ray >= 0.1) starts from that
-// plane with its full plane_cost; every other pixel runs the 64-plane sweep of
-// stereo.rs:247-269 unchanged.
+// sigmoid(logit) >= conf_thr runs a short local sweep: n_local planes with the
+// predicted normal and inverse depths evenly spread over +-span/2 (in
+// fractions of [1/zmax, 1/zmin]) around the prediction, each kept only if it
+// passes the reference's gates (positive inverse depth, depth in
+// [zmin/2, 2 zmax], n . ray >= 0.1), scored by plane_cost with the sweep's
+// early-abort hint; the best one seeds the pixel.  Every other pixel (and a
+// confident one whose local planes all fail the gates) runs the 64-plane
+// sweep of stereo.rs:247-269 unchanged.
 __global__ void __launch_bounds__(256, 3)
     init_learned_kernel(const DevJob* __restrict__ jobs, const int32_t* __restrict__ job_start, int n_jobs, int tw,
                         int th, int nh, const uint64_t* __restrict__ census, const float2* __restrict__ rays,
                         PlaneBuf out, const float* __restrict__ pred, const int64_t* __restrict__ pred_off,
-                        float conf_thr, unsigned long long* d_learned) {
+                        float conf_thr, int n_local, float span, unsigned long long* d_learned) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const Smem sm = carve(smem_raw, tw, th);
     Tile T;
@@ -506,29 +510,42 @@ __global__ void __launch_bounds__(256, 3)
         const float zlo = J->zmin * 0.5f, zhi = J->zmax * 2.0f;
         const float2 ri = sm.ray[(ly + HALO) * T.stw + lx + HALO];
         const int wq = J->w >> 2, hq = J->h >> 2;
-        float nx = 0.f, ny = 0.f, nz = 1.f, z = 0.f, a = 1.f;
+        float nx = 0.f, ny = 0.f, nz = 1.f, t0 = 0.f, a = 1.f;
         if (wq > 0 && hq > 0) {
             const int qx = min(x >> 2, wq - 1), qy = min(y >> 2, hq - 1);
             const float* o = pred + (pred_off[j] + (int64_t)qy * wq + qx) * NET_OUT_C;
             const float conf = 1.f / (1.f + __expf(-o[4]));
-            const float inv = J->inv_min + o[0] * (J->inv_max - J->inv_min);
             const float len = sqrtf(o[1] * o[1] + o[2] * o[2] + o[3] * o[3]);
-            if (conf >= conf_thr && inv > 0.f && len > 1e-6f) {
+            if (conf >= conf_thr && len > 1e-6f) {
                 nx = o[1] / len;
                 ny = o[2] / len;
                 nz = o[3] / len;
-                z = 1.f / inv;
                 a = nx * ri.x + ny * ri.y + nz;
-                learned = a >= 0.1f && z >= zlo && z <= zhi;
+                t0 = o[0];
+                learned = a >= 0.1f;
             }
         }
-        float4 plane;
-        float best_c;
+        float4 plane = make_float4(0.0f, 0.0f, 1.0f, 0.0f);
+        float best_c = INFINITY;
         if (learned) {
-            best_c = plane_cost<false, false, false>(sm, T.stw, lx, ly, nsrc, census, nx, ny, nz, z * a, INFINITY,
-                                                     total, wc, nullptr);
-            plane = make_float4(nx, ny, nz, z);
-        } else {
+            learned = false;
+            const float span_inv = J->inv_max - J->inv_min;
+            for (int k = 0; k < n_local; ++k) {
+                const float tk = t0 + span * ((float)k / (float)max(n_local - 1, 1) - 0.5f);
+                const float inv = J->inv_min + tk * span_inv;
+                if (!(inv > 0.f)) continue;
+                const float z = 1.f / inv;
+                if (!(z >= zlo && z <= zhi)) continue;
+                const float c = plane_cost<false, false, false>(sm, T.stw, lx, ly, nsrc, census, nx, ny, nz, z * a,
+                                                                best_c + 0.02f, total, wc, nullptr);
+                learned = true;
+                if (c < best_c) {
+                    best_c = c;
+                    plane = make_float4(nx, ny, nz, z);
+                }
+            }
+        }
+        if (!learned) {
             best_c = INFINITY;
             float best_d = 0.f;
             for (int hi = 0; hi < nh; ++hi) {
@@ -665,14 +682,15 @@ cudaError_t launch_pass(const DevJob* d_jobs, const int32_t* d_job_start, int n_
 
 cudaError_t launch_init_learned(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, int total_tiles,
                                 TileShape ts, int nh, const uint64_t* census, const float2* rays, PlaneBuf out,
-                                const float* pred, const int64_t* pred_off, float conf_thr,
-                                unsigned long long* d_learned, cudaStream_t st) {
+                                const float* pred, const int64_t* pred_off, float conf_thr, int n_local,
+                                float span, unsigned long long* d_learned, cudaStream_t st) {
     if (total_tiles <= 0) return cudaSuccess;
     const size_t sm = smem_bytes(ts.tw, ts.th);
     cudaError_t e = cudaFuncSetAttribute(init_learned_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e) return e;
     init_learned_kernel<<<total_tiles, ts.tw * ts.th, sm, st>>>(d_jobs, d_job_start, n_jobs, ts.tw, ts.th, nh, census,
-                                                                rays, out, pred, pred_off, conf_thr, d_learned);
+                                                                rays, out, pred, pred_off, conf_thr, n_local, span,
+                                                                d_learned);
     return cudaGetLastError();
 }
 

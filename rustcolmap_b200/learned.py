@@ -86,13 +86,17 @@ def costvol(ds, jobs, out_ptr):
     ds.ctx.check(ds.ctx._L.rcmvs_scene_costvol(ds.ctx.ptr, ds.ptr, cj, len(jobs), out_ptr))
 
 
-def estimate_learned(ds, jobs, opts, net, conf_thr=0.5):
+LOCAL_HYPS, LOCAL_SPAN, CONF_THR = 16, 0.12, 0.1
+
+
+def estimate_learned(ds, jobs, opts, net, conf_thr=CONF_THR, n_local=LOCAL_HYPS, span=LOCAL_SPAN):
     """Stereo seeded by the network; returns the number of learned-seeded pixels."""
     cj = _jobs_c(jobs)
     o = opts.to_c()
     n = C.c_uint64()
     ds.ctx.check(ds.ctx._L.rcmvs_scene_estimate_depth_learned(ds.ctx.ptr, ds.ptr, cj, len(jobs), C.byref(o),
-                                                              net.ptr, float(conf_thr), C.byref(n)))
+                                                              net.ptr, float(conf_thr), int(n_local), float(span),
+                                                              C.byref(n)))
     return n.value
 
 
@@ -188,7 +192,7 @@ def train(net, x, lab, iters=1500, batch=16, lr=1e-3, seed=0, log=print):
     return losses
 
 
-def evaluate(net, seeds, ctx, conf_thr=0.5, sweeps_learned=2, log=print):
+def evaluate(net, seeds, ctx, conf_thr=CONF_THR, sweeps_learned=2, log=print, n_local=LOCAL_HYPS, span=LOCAL_SPAN):
     """On held-out scenes: the plain method with 6 sweeps, the plain method
     with `sweeps_learned` sweeps (what the network's init replaces it with),
     and learned init + `sweeps_learned` sweeps.  Reports stereo views/s (CUDA
@@ -213,7 +217,7 @@ def evaluate(net, seeds, ctx, conf_thr=0.5, sweeps_learned=2, log=print):
                 ctx.synchronize()
                 e0.record(stream)
                 if name == "learned":
-                    nl = estimate_learned(ds, jobs, o, net, conf_thr)
+                    nl = estimate_learned(ds, jobs, o, net, conf_thr, n_local, span)
                 else:
                     ds.estimate(jobs, o)
                 e1.record(stream)
@@ -255,22 +259,27 @@ def main():
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
     ap.add_argument("--weights", default=DEFAULT_WEIGHTS)
-    ap.add_argument("--conf", type=float, default=0.5)
+    ap.add_argument("--conf", type=float, default=CONF_THR)
     ap.add_argument("--json", default=None)
+    ap.add_argument("--local-hyps", type=int, default=LOCAL_HYPS)
+    ap.add_argument("--local-span", type=float, default=LOCAL_SPAN)
     a = ap.parse_args()
     ctx = mvs.default_context()
     dev = torch.device("cuda:0")
     if a.cmd == "train":
         x, lab = make_dataset(list(range(a.seed0, a.seed0 + a.seeds)), ctx, torch, dev)
         net = ProposalNet(ctx, seed=0)
+        t0 = time.time()
         losses = train(net, x, lab, iters=a.iters, batch=a.batch, lr=a.lr)
+        print(f"train: {a.iters} iterations in {time.time() - t0:.1f} s")
         os.makedirs(os.path.dirname(os.path.abspath(a.out)), exist_ok=True)
         np.save(a.out, net.params())
         if a.json:
             json.dump({"losses": losses[::10], "seeds": a.seeds, "iters": a.iters}, open(a.json, "w"))
     else:
         net = ProposalNet(ctx, params=load_weights(a.weights))
-        agg, rows = evaluate(net, list(range(a.seed0, a.seed0 + a.seeds)), ctx, conf_thr=a.conf)
+        agg, rows = evaluate(net, list(range(a.seed0, a.seed0 + a.seeds)), ctx, conf_thr=a.conf,
+                             n_local=a.local_hyps, span=a.local_span)
         print(json.dumps(agg))
         if a.json:
             json.dump({"aggregate": agg, "per_seed": rows}, open(a.json, "w"))
