@@ -7,13 +7,17 @@ views, 64 plane-sweep hypotheses, 6 sweeps (12 Jacobi passes), fusion with
 >= 3 consistent views, 1% relative depth agreement and a 1 px reprojection
 gate.  One step = census + rays, patch-match stereo for all 100 views, and
 geometric-consistency fusion with voxel dedup (the PLY vertex records are
-packed on the device).
+packed on the device).  Two arms run on the same scene: the reference's
+schedule (plane-sweep init + 6 sweeps) and learned init (the committed
+proposal network, rustcolmap_b200/weights/proposal_c4.npy) + 2 sweeps; both
+report the fraction of ground-truth pixels within 1% inverse depth.
 
-value  depth maps/s with inputs resident in HBM (rcmvs_scene_* calls), timed
-       with CUDA events on the library's stream, max over ranks.
-e2e    the same metric through rcmvs_run_mvs with pinned host buffers:
-       host->device copy of every view's grey + colour image, device->host
-       read of the fused cloud, inside the timed region.
+value  depth maps/s of the learned arm with inputs resident in HBM
+       (rcmvs_scene_* calls), timed with CUDA events on the library's stream,
+       max over ranks; "plain" holds the reference-schedule arm.
+e2e    the same metric through rcmvs_run_mvs_learned with pinned host
+       buffers: host->device copy of every view's grey + colour image,
+       device->host read of the fused cloud, inside the timed region.
 
 --impl reference times the reference algorithm's CPU implementation (the
 oracle port; the Rust reference cannot be built here) on the host cores.
@@ -234,7 +238,20 @@ def _has_gpu():
         return False
 
 
-METRIC = "1080p depth maps/s at K=10 (plain GPU patch-match + fusion; learned init not in this number)"
+METRIC = "1080p depth maps/s at K=10: learned-init vs plain GPU patch-match at equal GT error"
+
+
+def gt_summary(ds, sc, jobs, scene):
+    """Ground truth over every job: fraction of pixels with ground truth that
+    are valid and within 1% inverse depth, and the same over valid pixels."""
+    within = gt_px = valid = 0
+    for (ref, _, _, _) in jobs:
+        m = scene.gt_metrics(ds.depth(ref).depth, sc.gt_depth[ref])
+        within += m["within"]
+        gt_px += m["gt_pixels"]
+        valid += m["valid"]
+    return {"within_1pct": within / max(gt_px, 1), "accuracy": within / max(valid, 1),
+            "tol": "1% relative inverse depth", "views": len(jobs)}
 
 
 def main():
@@ -251,7 +268,12 @@ def main():
     ap.add_argument("--views", type=int, default=0, help="override the number of views (profiling runs)")
     ap.add_argument("--no-count", action="store_true", help="skip the work-counting rerun")
     ap.add_argument("--one-candidate", action="store_true",
-                    help="use the one-candidate-at-a-time stereo kernels (comparison)")
+                    help="use the one-candidate-at-a-time init kernel (comparison)")
+    ap.add_argument("--plain-only", action="store_true", help="time only the plain (reference-schedule) arm")
+    ap.add_argument("--learned-only", action="store_true", help="time only the learned arm (tuning runs)")
+    ap.add_argument("--local-hyps", type=int, default=None)
+    ap.add_argument("--local-span", type=float, default=None)
+    ap.add_argument("--conf", type=float, default=None)
     args = ap.parse_args()
     assert args.warmup >= 3 or os.environ.get("RCMVS_BENCH_ALLOW_SHORT"), "warm-up must be >= 3 steps"
     cfg = configs()[args.config]
@@ -262,14 +284,17 @@ def main():
         run_reference(args, cfg)
         return
 
+    import dataclasses
+
     import torch
 
-    from rustcolmap_b200 import mvs, scene
+    from rustcolmap_b200 import learned, mvs, scene
     ws, rank, local = dist_setup()
     torch.cuda.set_device(local)
     opts = cfg["opts"]
     if args.one_candidate:
         opts.flags |= 1
+    lopts = dataclasses.replace(opts, sweeps=2)
     t_setup = time.perf_counter()
     sc = make_scene(cfg, seed=5 + 1000 * rank, device=local)
     srcs, zr, fus = mvs.plan(sc.sparse, sc.views, opts)
@@ -277,43 +302,73 @@ def main():
     n_maps = len(jobs)
     ctx = mvs.Context(local)
     ds = mvs.DeviceScene(sc.views, ctx)
+    net = None if args.plain_only else learned.ProposalNet(ctx, params=learned.load_weights())
     stream = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{local}")
     setup_s = time.perf_counter() - t_setup
+    seeded = [0]
 
-    def step():
+    def step_plain():
         ds.prepare()
         ds.estimate(jobs, opts)
         return ds.fuse(fus, sc.sparse.xyz, opts)
 
-    for _ in range(args.warmup):
-        step()
-    ctx.synchronize()
-    barrier(ws)
-    clk = ClockSampler(local)
-    clk.start()
-    ctx.timing(True)
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    barrier(ws)
-    e0.record(stream)
-    n_points = 0
-    for _ in range(args.steps):
-        n_points = step()
-    e1.record(stream)
-    ctx.synchronize()
-    torch.cuda.synchronize()
-    barrier(ws)
-    clocks = clk.stop()
-    ms = e0.elapsed_time(e1)
-    ktimes = {k: ctx.kernel_time(k) for k in ("census_rays", "stereo_init", "stereo_pass", "stereo_gate",
-                                              "fuse_candidates", "fuse_reduce")}
-    ctx.timing(False)
-    ms_max = max_over_ranks(ms, ws, local)
-    total_maps = sum_over_ranks(n_maps * args.steps, ws, local)
-    value = total_maps / (ms_max / 1e3)
+    lkw = {}
+    if args.local_hyps is not None:
+        lkw["n_local"] = args.local_hyps
+    if args.local_span is not None:
+        lkw["span"] = args.local_span
+    if args.conf is not None:
+        lkw["conf_thr"] = args.conf
 
-    # work counters (untimed rerun with counting on): actual cost evaluations and rows
+    def step_learned():
+        ds.prepare()
+        seeded[0] = learned.estimate_learned(ds, jobs, lopts, net, **lkw)
+        return ds.fuse(fus, sc.sparse.xyz, lopts)
+
+    def timed(step, clocks=False):
+        for _ in range(args.warmup):
+            step()
+        ctx.synchronize()
+        barrier(ws)
+        clk = ClockSampler(local)
+        if clocks:
+            clk.start()
+        ctx.timing(True)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        barrier(ws)
+        e0.record(stream)
+        npts = 0
+        for _ in range(args.steps):
+            npts = step()
+        e1.record(stream)
+        ctx.synchronize()
+        torch.cuda.synchronize()
+        barrier(ws)
+        ck = clk.stop() if clocks else None
+        ms = e0.elapsed_time(e1)
+        names = ("census_rays", "learned_costvol", "learned_net", "learned_init", "stereo_init", "stereo_pass",
+                 "stereo_gate", "fuse_candidates", "fuse_reduce")
+        kt = {k: ctx.kernel_time(k) for k in names}
+        ctx.timing(False)
+        ms_max = max_over_ranks(ms, ws, local)
+        return ms_max, kt, npts, ck, gt_summary(ds, sc, jobs, scene)
+
+    if args.learned_only:  # tuning runs: no plain arm
+        plain_ms, plain_kt, plain_pts, plain_clk, plain_gt = float("nan"), {}, 0, None, {"within_1pct": float("nan")}
+    else:
+        plain_ms, plain_kt, plain_pts, plain_clk, plain_gt = timed(step_plain, clocks=args.plain_only)
+    if args.plain_only:
+        head_ms, head_kt, head_pts, clocks, head_gt = plain_ms, plain_kt, plain_pts, plain_clk, plain_gt
+    else:
+        head_ms, head_kt, head_pts, clocks, head_gt = timed(step_learned, clocks=True)
+    total_maps = sum_over_ranks(n_maps * args.steps, ws, local)
+    value = total_maps / (head_ms / 1e3)
+    plain_value = total_maps / (plain_ms / 1e3)
+    head_opts = opts if args.plain_only else lopts
+
+    # work counters of the plain arm (untimed rerun with counting on)
     evals, rows5 = 0, 0
     if not args.no_count:
         os.environ["RCMVS_COUNT"] = "1"
@@ -329,12 +384,12 @@ def main():
     e2e = None
     if not args.no_e2e:
         pv = pinned_views(sc.views)
-        mvs.run_mvs(pv, sc.sparse, opts, ctx=ctx)  # warm
+        mvs.run_mvs(pv, sc.sparse, head_opts, ctx=ctx, net=net)  # warm
         torch.cuda.synchronize()
         barrier(ws)
         t0 = time.perf_counter()
         for _ in range(args.steps):
-            st, xyz, rgb = mvs.run_mvs(pv, sc.sparse, opts, ctx=ctx)
+            st, xyz, rgb = mvs.run_mvs(pv, sc.sparse, head_opts, ctx=ctx, net=net)
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
         barrier(ws)
@@ -342,20 +397,12 @@ def main():
         h2d = int(sum(v.gray.nbytes + v.rgb.nbytes for v in pv))
         e2e = {"value": sum_over_ranks(n_maps * args.steps, ws, local) / dt, "unit": "depth maps/s",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(xyz.nbytes + rgb.nbytes),
-               "ms_per_step": 1e3 * dt / args.steps}
+               "ms_per_step": 1e3 * dt / args.steps, "call": "rcmvs_run_mvs" + ("" if net is None else "_learned")}
 
-    # ground-truth error of this step's depth maps
-    accs, comps = [], []
-    for (ref, _, _, _) in jobs[:: max(1, len(jobs) // 20)]:
-        m = scene.gt_metrics(ds.depth(ref).depth, sc.gt_depth[ref])
-        accs.append(m["accuracy"])
-        comps.append(m["completeness"])
-
-    # roofline of the dominant kernel (the Jacobi pass)
+    # roofline of the dominant kernel (the Jacobi pass) in the headline arm
     npx = sum(sc.views[r].w * sc.views[r].h for r, _, _, _ in jobs)
     src_px = sum(sc.views[s].w * sc.views[s].h for _, ss, _, _ in jobs for s in ss)
-    K = max(len(s) for _, s, _, _ in jobs)
-    pass_ms, pass_n = ktimes["stereo_pass"]
+    pass_ms, pass_n = head_kt["stereo_pass"]
     pass_avg_s = pass_ms / max(pass_n, 1) / 1e3
     bytes_per_launch = npx * (20 + 20 + 8 + 8) + src_px * 8
     achieved_gbs = bytes_per_launch / pass_avg_s / 1e9
@@ -364,57 +411,65 @@ def main():
     if os.path.exists(pk):
         peaks = json.load(open(pk))
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
-    terms_alg_per_pass = npx * 7 * 25 * sum(len(s) for _, s, _, _ in jobs) / len(jobs)
     algo_terms_total = sum(sc.views[r].w * sc.views[r].h * 25 * len(s) * (opts.num_hyp + 7 * 2 * opts.sweeps)
                            for r, s, _, _ in jobs)
     actual_terms = rows5 * 5
-    step_s = ms_max / 1e3 / args.steps
-    stereo_ms = sum(ktimes[k][0] for k in ("stereo_init", "stereo_pass", "stereo_gate")) / args.steps
+    stereo_ms = sum(plain_kt[k][0] for k in ("stereo_init", "stereo_pass", "stereo_gate")) / args.steps if plain_kt else 0
     fp32_ops_per_term = 40
-    achieved_tops = actual_terms * fp32_ops_per_term / (stereo_ms / 1e3) / 1e12 if actual_terms else None
+    achieved_tops = actual_terms * fp32_ops_per_term / (stereo_ms / 1e3) / 1e12 if actual_terms and stereo_ms else None
 
     cpu = None
     if not args.no_cpu_baseline and rank == 0 and ws == 1:
         rate, dt, desc, nt = cpu_baseline(sc, opts, jobs, args.cpu_rows)
-        cpu = {"value": rate, "unit": "depth maps/s", "cores": nt, "kind": "port", "sample": desc,
-               "seconds": dt}
+        cpu = {"value": rate, "unit": "depth maps/s", "cores": nt, "kind": "port", "sample": desc, "seconds": dt}
 
     if rank == 0:
+        per_step = (1 + 1 + 2 * opts.sweeps + 1 + 5) if args.plain_only else (1 + 3 + 6 + 1 + 2 * lopts.sweeps + 1 + 5)
         line = {
             "metric": METRIC, "value": value, "unit": "depth maps/s", "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "warmup": args.warmup, "ms_per_step": head_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (stereo), bf16/f32-acc (proposal net)",
+            "data": "synthetic",
             "config": {"workload": args.config + ": " + cfg["desc"], "views_per_step": n_maps,
+                       "headline_arm": "plain, 6 sweeps" if args.plain_only else
+                       "learned init (proposal_c4 weights, conf >= 0.1, 16 local planes) + 2 sweeps",
                        "parallelism": f"views batched on 1 GPU; {ws} rank(s), one independent scene each",
                        "l2": "inputs larger than L2 (census 8 B/px, rays 8 B/px, planes 40 B/px over all views)"},
+            "plain": {"value": plain_value, "unit": "depth maps/s", "sweeps": opts.sweeps,
+                      "ms_per_step": plain_ms / args.steps, "gt": plain_gt, "fused_points": plain_pts,
+                      "kernel_ms_per_step": {k: v[0] / args.steps for k, v in plain_kt.items() if v[1]}},
+            "learned": None if args.plain_only else {
+                "value": value, "sweeps": lopts.sweeps, "gt": head_gt, "fused_points": head_pts,
+                "seeded_fraction": seeded[0] / max(npx, 1), "speedup_vs_plain": value / plain_value,
+                "gt_within_delta_vs_plain": head_gt["within_1pct"] - plain_gt["within_1pct"]},
             "roofline": {"bound": "hbm", "kernel": "stereo_pass", "achieved": achieved_gbs, "peak": hbm_peak,
                          "unit": "GB/s", "frac": achieved_gbs / hbm_peak, "traffic": None,
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650",
-                         "algorithmic_bytes_per_launch": bytes_per_launch,
-                         "avg_launch_ms": pass_avg_s * 1e3,
+                         "algorithmic_bytes_per_launch": bytes_per_launch, "avg_launch_ms": pass_avg_s * 1e3,
                          "note": "issue-bound kernel: see compute_roofline"},
-            "compute_roofline": {"bound": "fp32_issue", "achieved": achieved_tops, "peak": FP32_NOMINAL_TOPS,
-                                 "unit": "Top/s",
+            "compute_roofline": {"bound": "fp32_issue", "kernel": "stereo init + pass (plain arm)",
+                                 "achieved": achieved_tops, "peak": FP32_NOMINAL_TOPS, "unit": "Top/s",
                                  "frac": achieved_tops / FP32_NOMINAL_TOPS if achieved_tops else None,
                                  "ops_per_term": fp32_ops_per_term,
                                  "peak_source": "nominal 148 SM x 128 FP32 lanes x 1.965 GHz"},
-            "gpu_launches": args.steps * (1 + 1 + 2 * opts.sweeps + 1 + 5),
+            "gpu_launches": args.steps * per_step,
             "clocks": clocks,
             "e2e": e2e,
             "cpu_baseline": cpu,
-            "gcost_evals_per_s": evals * args.steps / (ms_max / 1e3) / 1e9,
-            "work": {"cost_evals_per_step": evals, "window_rows_per_step": rows5,
-                     "algorithmic_cost_evals_per_step": sum(sc.views[r].w * sc.views[r].h *
-                                                           (opts.num_hyp + 14 * opts.sweeps) for r, _, _, _ in jobs),
-                     "algorithmic_terms_per_step": algo_terms_total, "evaluated_terms_per_step": actual_terms},
-            "kernel_ms_per_step": {k: v[0] / args.steps for k, v in ktimes.items()},
-            "fused_points": n_points,
-            "gt": {"accuracy_median": statistics.median(accs), "completeness_median": statistics.median(comps),
-                   "tol": "1% relative inverse depth", "views_sampled": len(accs)},
+            "gcost_evals_per_s_plain": evals * args.steps / (plain_ms / 1e3) / 1e9 if evals else None,
+            "work_plain": {"cost_evals_per_step": evals, "window_rows_per_step": rows5,
+                           "algorithmic_cost_evals_per_step": sum(sc.views[r].w * sc.views[r].h *
+                                                                 (opts.num_hyp + 14 * opts.sweeps)
+                                                                 for r, _, _, _ in jobs),
+                           "algorithmic_terms_per_step": algo_terms_total, "evaluated_terms_per_step": actual_terms},
+            "kernel_ms_per_step": {k: v[0] / args.steps for k, v in head_kt.items() if v[1]},
+            "fused_points": head_pts,
             "setup_s": setup_s,
-            "kernels": "one-candidate" if opts.flags & 1 else "row-step",
+            "kernels": "one-candidate init" if opts.flags & 1 else "row-step init",
         }
         print(json.dumps(line), flush=True)
+    if net is not None:
+        net.close()
     ds.close()
     ctx.close()
     if ws > 1:

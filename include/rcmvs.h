@@ -325,6 +325,13 @@ int rcmvs_scene_estimate_depth_learned(rcmvs_ctx* ctx, rcmvs_scene* scene, const
                                        float conf_thr, int32_t n_local, float span,
                                        uint64_t* learned_pixels);
 
+/* rcmvs_run_mvs with stereo seeded by the network (arguments as
+ * rcmvs_scene_estimate_depth_learned; opts->sweeps sweeps after the init). */
+int rcmvs_run_mvs_learned(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views,
+                          const rcmvs_sparse* sparse, const rcmvs_options* opts, rcmvs_net* net,
+                          float conf_thr, int32_t n_local, float span,
+                          const rcmvs_depth_out* depth_outs, rcmvs_points* out, rcmvs_stats* stats);
+
 /* ------------------------------------------- allocation-free variant */
 /* No counterpart in the reference: an `estimate_depth` for callers that may
  * not allocate device memory (an application whose GPU memory belongs to

@@ -915,8 +915,13 @@ int rcmvs_plan(const rcmvs_sparse* sp, const rcmvs_view* views, int32_t n_views,
     return RCMVS_OK;
 }
 
-int rcmvs_run_mvs(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views, const rcmvs_sparse* sparse,
-                  const rcmvs_options* opts, const rcmvs_depth_out* depth_outs, rcmvs_points* out, rcmvs_stats* stats) {
+}  // extern "C"
+
+// run_mvs with either the reference's plane-sweep init (net == NULL) or the
+// learned init of rcmvs_scene_estimate_depth_learned.
+static int run_mvs_impl(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views, const rcmvs_sparse* sparse,
+                        const rcmvs_options* opts, const rcmvs_depth_out* depth_outs, rcmvs_points* out,
+                        rcmvs_stats* stats, rcmvs_net* net, float conf_thr, int32_t n_local, float span) {
     if (!ctx || !views || !sparse || !opts || !out) return fail(ctx, RCMVS_E_ARG, "rcmvs_run_mvs: bad argument");
     out->n = 0;
     out->xyz = nullptr;
@@ -950,7 +955,9 @@ int rcmvs_run_mvs(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views, cons
     if (rc) return rc;
     auto body = [&]() -> int {
         CK(cudaEventRecord(e1, ctx->stream));
-        int r = rcmvs_scene_estimate_depth(ctx, sc, jobs.data(), (int32_t)jobs.size(), opts);
+        int r = net ? rcmvs_scene_estimate_depth_learned(ctx, sc, jobs.data(), (int32_t)jobs.size(), opts, net,
+                                                         conf_thr, n_local, span, nullptr)
+                    : rcmvs_scene_estimate_depth(ctx, sc, jobs.data(), (int32_t)jobs.size(), opts);
         if (r) return r;
         CK(cudaEventRecord(e2, ctx->stream));
         uint64_t np = 0;
@@ -1003,6 +1010,20 @@ int rcmvs_run_mvs(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views, cons
     cudaEventDestroy(e3);
     if (rc) rcmvs_points_free(out);
     return rc;
+}
+
+extern "C" {
+
+int rcmvs_run_mvs(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views, const rcmvs_sparse* sparse,
+                  const rcmvs_options* opts, const rcmvs_depth_out* depth_outs, rcmvs_points* out, rcmvs_stats* stats) {
+    return run_mvs_impl(ctx, views, n_views, sparse, opts, depth_outs, out, stats, nullptr, 0.f, 1, 0.f);
+}
+
+int rcmvs_run_mvs_learned(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views, const rcmvs_sparse* sparse,
+                          const rcmvs_options* opts, rcmvs_net* net, float conf_thr, int32_t n_local, float span,
+                          const rcmvs_depth_out* depth_outs, rcmvs_points* out, rcmvs_stats* stats) {
+    if (!net) return fail(ctx, RCMVS_E_ARG, "rcmvs_run_mvs_learned: null network");
+    return run_mvs_impl(ctx, views, n_views, sparse, opts, depth_outs, out, stats, net, conf_thr, n_local, span);
 }
 
 }  // extern "C"

@@ -480,19 +480,27 @@ __global__ void __launch_bounds__(256, MINB)
 // ---------------------------------------------------------------- learned init
 // Patch-match init from learned proposals (no reference counterpart).  A
 // pixel whose quarter-resolution cell predicts a plane with confidence
-// sigmoid(logit) >= conf_thr runs a short local sweep: n_local planes with the
-// predicted normal and inverse depths evenly spread over +-span/2 (in
-// fractions of [1/zmax, 1/zmin]) around the prediction, each kept only if it
-// passes the reference's gates (positive inverse depth, depth in
-// [zmin/2, 2 zmax], n . ray >= 0.1), scored by plane_cost with the sweep's
-// early-abort hint; the best one seeds the pixel.  Every other pixel (and a
-// confident one whose local planes all fail the gates) runs the 64-plane
-// sweep of stereo.rs:247-269 unchanged.
+// sigmoid(logit) >= conf_thr tries n_local planes with the predicted normal
+// and inverse depths evenly spread over +-span/2 (in fractions of
+// [1/zmax, 1/zmin]) around the prediction, each kept only if it passes the
+// reference's gates (positive inverse depth, depth in [zmin/2, 2 zmax],
+// n . ray >= 0.1), scored by plane_cost with the sweep's early-abort hint;
+// the best one seeds the pixel.  Every other pixel (and a confident one whose
+// local planes all fail the gates) runs the 64-plane sweep of
+// stereo.rs:247-269 unchanged.
+// Row-step schedule of the learned init: each lane streams its own candidate
+// list one 5-term window row per step — the n_local planes around its
+// prediction if it is confident, else (or if none of them passes the gates)
+// the 64-plane sweep — so a warp mixing seeded and unseeded pixels does not
+// run both lists one after the other.  Fronto-parallel sweep planes go
+// through the general cost path: with n = (0,0,1), denom is exactly 1.0 and
+// d/1 = d, so each candidate's cost is the same float as in the sweep.
 __global__ void __launch_bounds__(256, 3)
-    init_learned_kernel(const DevJob* __restrict__ jobs, const int32_t* __restrict__ job_start, int n_jobs, int tw,
-                        int th, int nh, const uint64_t* __restrict__ census, const float2* __restrict__ rays,
-                        PlaneBuf out, const float* __restrict__ pred, const int64_t* __restrict__ pred_off,
-                        float conf_thr, int n_local, float span, unsigned long long* d_learned) {
+    init_learned_rows_kernel(const DevJob* __restrict__ jobs, const int32_t* __restrict__ job_start, int n_jobs,
+                             int tw, int th, int nh, const uint64_t* __restrict__ census,
+                             const float2* __restrict__ rays, PlaneBuf out, const float* __restrict__ pred,
+                             const int64_t* __restrict__ pred_off, float conf_thr, int n_local, float span,
+                             unsigned long long* d_learned) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const Smem sm = carve(smem_raw, tw, th);
     Tile T;
@@ -502,68 +510,103 @@ __global__ void __launch_bounds__(256, 3)
     const int lx = threadIdx.x % tw, ly = threadIdx.x / tw;
     const int x = T.x0 + lx, y = T.y0 + ly;
     const bool inside = x < J->w && y < J->h;
+    const int nsrc = J->nsrc;
+    const float total = 5.0f * 5.0f * (float)nsrc;
+    const float zlo = J->zmin * 0.5f, zhi = J->zmax * 2.0f;
+    const float inv_min = J->inv_min, inv_max = J->inv_max, span_inv = inv_max - inv_min;
+    const float2 ri = sm.ray[(ly + HALO) * T.stw + lx + HALO];
+    // this lane's prediction
     bool learned = false;
-    if (inside) {
-        WorkCount wc{0, 0};
-        const int nsrc = J->nsrc;
-        const float total = 5.0f * 5.0f * (float)nsrc;
-        const float zlo = J->zmin * 0.5f, zhi = J->zmax * 2.0f;
-        const float2 ri = sm.ray[(ly + HALO) * T.stw + lx + HALO];
-        const int wq = J->w >> 2, hq = J->h >> 2;
-        float nx = 0.f, ny = 0.f, nz = 1.f, t0 = 0.f, a = 1.f;
-        if (wq > 0 && hq > 0) {
-            const int qx = min(x >> 2, wq - 1), qy = min(y >> 2, hq - 1);
-            const float* o = pred + (pred_off[j] + (int64_t)qy * wq + qx) * NET_OUT_C;
-            const float conf = 1.f / (1.f + __expf(-o[4]));
-            const float len = sqrtf(o[1] * o[1] + o[2] * o[2] + o[3] * o[3]);
-            if (conf >= conf_thr && len > 1e-6f) {
-                nx = o[1] / len;
-                ny = o[2] / len;
-                nz = o[3] / len;
-                a = nx * ri.x + ny * ri.y + nz;
-                t0 = o[0];
-                learned = a >= 0.1f;
-            }
+    float pnx = 0.f, pny = 0.f, pnz = 1.f, pa = 1.f, t0 = 0.f;
+    const int wq = J->w >> 2, hq = J->h >> 2;
+    if (inside && wq > 0 && hq > 0) {
+        const int qx = min(x >> 2, wq - 1), qy = min(y >> 2, hq - 1);
+        const float* o = pred + (pred_off[j] + (int64_t)qy * wq + qx) * NET_OUT_C;
+        const float conf = 1.f / (1.f + __expf(-o[4]));
+        const float len = sqrtf(o[1] * o[1] + o[2] * o[2] + o[3] * o[3]);
+        if (conf >= conf_thr && len > 1e-6f) {
+            pnx = o[1] / len;
+            pny = o[2] / len;
+            pnz = o[3] / len;
+            pa = pnx * ri.x + pny * ri.y + pnz;
+            t0 = o[0];
+            learned = pa >= 0.1f;
         }
-        float4 plane = make_float4(0.0f, 0.0f, 1.0f, 0.0f);
-        float best_c = INFINITY;
-        if (learned) {
-            learned = false;
-            const float span_inv = J->inv_max - J->inv_min;
-            for (int k = 0; k < n_local; ++k) {
+    }
+    // candidate stream: list 1 = local planes (learned lanes), list 0 = sweep
+    int list = learned ? 1 : 0, k = 0;
+    bool any_local = false;
+    float cnx = 0.f, cny = 0.f, cnz = 1.f, cd = 0.f, cz = 0.f;
+    auto next = [&]() -> bool {
+        for (;;) {
+            if (list == 1) {
+                if (k >= n_local) {
+                    if (any_local) return false;
+                    list = 0;  // no local plane passed the gates: sweep instead
+                    k = 0;
+                    continue;
+                }
                 const float tk = t0 + span * ((float)k / (float)max(n_local - 1, 1) - 0.5f);
-                const float inv = J->inv_min + tk * span_inv;
+                ++k;
+                const float inv = inv_min + tk * span_inv;
                 if (!(inv > 0.f)) continue;
                 const float z = 1.f / inv;
                 if (!(z >= zlo && z <= zhi)) continue;
-                const float c = plane_cost<false, false, false>(sm, T.stw, lx, ly, nsrc, census, nx, ny, nz, z * a,
-                                                                best_c + 0.02f, total, wc, nullptr);
-                learned = true;
-                if (c < best_c) {
-                    best_c = c;
-                    plane = make_float4(nx, ny, nz, z);
-                }
+                cnx = pnx;
+                cny = pny;
+                cnz = pnz;
+                cz = z;
+                cd = z * pa;
+                any_local = true;
+                return true;
             }
+            if (k >= nh) return false;
+            cnx = 0.f;
+            cny = 0.f;
+            cnz = 1.f;
+            cd = hyp_depth(inv_min, inv_max, k, nh);
+            cz = cd;
+            ++k;
+            return true;
         }
-        if (!learned) {
-            best_c = INFINITY;
-            float best_d = 0.f;
-            for (int hi = 0; hi < nh; ++hi) {
-                const float d = hyp_depth(J->inv_min, J->inv_max, hi, nh);
-                const float c = plane_cost<true, false, false>(sm, T.stw, lx, ly, nsrc, census, 0.f, 0.f, 1.f, d,
-                                                               best_c + 0.02f, total, wc, nullptr);
-                if (c < best_c) {
-                    best_c = c;
-                    best_d = d;
-                }
+    };
+    float best_c = INFINITY;
+    float4 plane = make_float4(0.0f, 0.0f, 1.0f, 0.0f);
+    bool live = inside && next();
+    int si = 0, dy = 0;
+    float sum = 0.f, thr = INFINITY;
+    int32_t hs = 0;
+    while (live) {
+        bool fin = true, aborted = false;
+        if (nsrc > 0) {
+            const SrcRegs s = load_src(sm.src[si], census);
+            sum = cost_row<false, false>(sm, (ly + dy) * T.stw + lx, s, cnx, cny, cnz, cd, sum, hs);
+            aborted = sum / ((float)(dy + 1) * 5.0f * (float)(si + 1)) > thr;
+            fin = aborted || (si == nsrc - 1 && dy == 4);
+        }
+        if (fin) {
+            const float c = aborted ? 1e9f : sum / total;
+            if (c < best_c) {
+                best_c = c;
+                plane = make_float4(cnx, cny, cnz, cz);
             }
-            plane = make_float4(0.0f, 0.0f, 1.0f, best_d);
+            live = next();
+            sum = 0.f;
+            si = 0;
+            dy = 0;
+            thr = (best_c + 0.02f) + 0.12f;
+        } else if (++dy == 5) {
+            dy = 0;
+            ++si;
         }
+    }
+    const bool seeded = inside && learned && any_local;
+    if (inside) {
         const size_t i = (size_t)J->off + (size_t)y * J->w + x;
         out.nz[i] = plane;
         out.cost[i] = fminf(best_c, 1.0f);
     }
-    const unsigned bal = __ballot_sync(0xffffffffu, learned);
+    const unsigned bal = __ballot_sync(0xffffffffu, seeded);
     if ((threadIdx.x & 31) == 0 && bal) atomicAdd(d_learned, (unsigned long long)__popc(bal));
 }
 
@@ -686,11 +729,11 @@ cudaError_t launch_init_learned(const DevJob* d_jobs, const int32_t* d_job_start
                                 float span, unsigned long long* d_learned, cudaStream_t st) {
     if (total_tiles <= 0) return cudaSuccess;
     const size_t sm = smem_bytes(ts.tw, ts.th);
-    cudaError_t e = cudaFuncSetAttribute(init_learned_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaError_t e = cudaFuncSetAttribute(init_learned_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e) return e;
-    init_learned_kernel<<<total_tiles, ts.tw * ts.th, sm, st>>>(d_jobs, d_job_start, n_jobs, ts.tw, ts.th, nh, census,
-                                                                rays, out, pred, pred_off, conf_thr, n_local, span,
-                                                                d_learned);
+    init_learned_rows_kernel<<<total_tiles, ts.tw * ts.th, sm, st>>>(d_jobs, d_job_start, n_jobs, ts.tw, ts.th, nh,
+                                                                     census, rays, out, pred, pred_off, conf_thr,
+                                                                     n_local, span, d_learned);
     return cudaGetLastError();
 }
 

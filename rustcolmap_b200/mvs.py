@@ -316,11 +316,14 @@ def _web_json(xyz, rgb, path, cap=400_000):
         f.write('{"n":' + str(len(sel)) + ',"pos":[' + pos + '],"col":[' + col + ']}')
 
 
-def run_mvs(views, sparse, opts, out_dir=None, ctx=None, log=None, return_depth=False):
+def run_mvs(views, sparse, opts, out_dir=None, ctx=None, log=None, return_depth=False, net=None,
+            conf_thr=0.1, n_local=16, span=0.12):
     """mvs::run_mvs (lib.rs:294-517) from views already at working resolution
     (the image decode/resize of load_views is not part of this path).  Writes
     <out_dir>/dense/dense.ply, mvs_stats.json and dense_web.json when out_dir
-    is given.  Returns (MvsStats, xyz, rgb[, depth maps])."""
+    is given.  net (a learned.ProposalNet, extension): seed stereo with the
+    network instead of the plane sweep.  Returns (MvsStats, xyz, rgb[, depth
+    maps])."""
     ctx = _ctx(ctx)
     t0 = time.time()
     if len(views) < 2:
@@ -342,8 +345,13 @@ def run_mvs(views, sparse, opts, out_dir=None, ctx=None, log=None, return_depth=
             c = np.empty((v.h, v.w), np.float32)
             douts[i] = _abi.DepthOut(d.ctypes.data, c.ctypes.data, None)
             dms.append(DepthMap(d, c))
-    ctx.check(ctx._L.rcmvs_run_mvs(ctx.ptr, va, len(views), C.byref(sp), C.byref(o), douts, C.byref(pts),
-                                   C.byref(st)))
+    if net is None:
+        ctx.check(ctx._L.rcmvs_run_mvs(ctx.ptr, va, len(views), C.byref(sp), C.byref(o), douts, C.byref(pts),
+                                       C.byref(st)))
+    else:
+        ctx.check(ctx._L.rcmvs_run_mvs_learned(ctx.ptr, va, len(views), C.byref(sp), C.byref(o), net.ptr,
+                                               float(conf_thr), int(n_local), float(span), douts, C.byref(pts),
+                                               C.byref(st)))
     xyz, rgb = _take_points(ctx, pts)
     stats = MvsStats(views=st.views, views_with_depth=st.views_with_depth, dense_points=st.dense_points,
                      per_view_valid=[int((d.depth > 0).sum()) for d in dms] if return_depth else [],

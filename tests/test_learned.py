@@ -210,3 +210,12 @@ def test_training_reduces_loss(ctx):
     assert np.mean(losses[-20:]) < 0.7 * np.mean(losses[:5])
     ds.close()
     net.close()
+
+
+@pytest.mark.gpu
+def test_run_mvs_learned_without_confident_pixels_equals_run_mvs(ctx, corner_scene, c1_opts):
+    net = learned.ProposalNet(ctx, seed=2)
+    _, xa, ca = mvs.run_mvs(corner_scene.views, corner_scene.sparse, c1_opts, ctx=ctx)
+    _, xb, cb = mvs.run_mvs(corner_scene.views, corner_scene.sparse, c1_opts, ctx=ctx, net=net, conf_thr=2.0)
+    assert np.array_equal(xa, xb) and np.array_equal(ca, cb)
+    net.close()
