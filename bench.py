@@ -432,7 +432,8 @@ def main():
             "data": "synthetic",
             "config": {"workload": args.config + ": " + cfg["desc"], "views_per_step": n_maps,
                        "headline_arm": "plain, 6 sweeps" if args.plain_only else
-                       "learned init (proposal_c4 weights, conf >= 0.1, 16 local planes) + 2 sweeps",
+                       "learned init (proposal_c4 weights; pixels with confidence >= 0.1 start from the "
+                       "predicted plane, the others from the 64-plane sweep) + 2 sweeps",
                        "parallelism": f"views batched on 1 GPU; {ws} rank(s), one independent scene each",
                        "l2": "inputs larger than L2 (census 8 B/px, rays 8 B/px, planes 40 B/px over all views)"},
             "plain": {"value": plain_value, "unit": "depth maps/s", "sweeps": opts.sweeps,

@@ -317,7 +317,7 @@ def _web_json(xyz, rgb, path, cap=400_000):
 
 
 def run_mvs(views, sparse, opts, out_dir=None, ctx=None, log=None, return_depth=False, net=None,
-            conf_thr=0.1, n_local=16, span=0.12):
+            conf_thr=0.1, n_local=1, span=0.0):
     """mvs::run_mvs (lib.rs:294-517) from views already at working resolution
     (the image decode/resize of load_views is not part of this path).  Writes
     <out_dir>/dense/dense.ply, mvs_stats.json and dense_web.json when out_dir
