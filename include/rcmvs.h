@@ -72,6 +72,23 @@ typedef struct rcmvs_options {
  * keeps a warp's source-census gathers on one support view. */
 #define RCMVS_FLAG_ONE_CANDIDATE 1u
 
+/* Persistent (view, tile) work queue: each init/pass launch runs as many
+ * blocks as stay resident on the GPU, and every block takes tile after tile
+ * of the batch (all views, in job order) from an atomic counter instead of
+ * computing the one tile of its block index.  Same results bit for bit. */
+#define RCMVS_FLAG_PERSISTENT 2u
+
+/* Capture the batch's launch schedule (init -> 2*max(sweeps,1) passes ->
+ * gate) in a CUDA graph, cached on the scene and replayed while the job
+ * table, options and buffers are unchanged.  Ignored while per-kernel
+ * timing (rcmvs_ctx_timing) is on.  Same results bit for bit. */
+#define RCMVS_FLAG_CUDA_GRAPH 4u
+
+/* Per-resolution-class tile shapes from the autotuner (rcmvs_autotune):
+ * classes not yet tuned on this context are tuned on the batch's jobs
+ * first.  Overrides tile_w/tile_h.  Same results bit for bit. */
+#define RCMVS_FLAG_AUTOTUNE 8u
+
 /* Fills `MvsOptions::default()` (mvs/src/lib.rs:56-70); extensions off. */
 void rcmvs_options_default(rcmvs_options* opts);
 
@@ -226,6 +243,33 @@ int rcmvs_scene_prepare(rcmvs_ctx* ctx, rcmvs_scene* scene);
  * on the context stream. */
 int rcmvs_scene_estimate_depth(rcmvs_ctx* ctx, rcmvs_scene* scene, const rcmvs_job* jobs,
                                int32_t n_jobs, const rcmvs_options* opts);
+
+/* Tile-shape autotuner (no reference counterpart).  Reference views are
+ * grouped into resolution classes by (w, h).  For every class of the given
+ * jobs that this context has not tuned yet, a trial (plane-sweep init + one
+ * pass, with opts, on the class's first jobs up to about 1 Mpx) is timed
+ * with CUDA events for each candidate shape: 16x16, 32x8, 8x32, 64x4 (256
+ * threads), 16x8, 8x16, 32x4 (128) and 8x8 (64).  One thread count is kept
+ * for all classes of a context (the one with the least summed best time at
+ * the first tuning), and each class gets its fastest shape of that count.
+ * The trial overwrites the jobs' plane buffers, not their depth maps.
+ * Synchronous. */
+typedef struct rcmvs_tune_entry {
+    int32_t w, h;            /* resolution class */
+    int32_t tile_w, tile_h;  /* chosen shape */
+    float ms_best;           /* trial time of the chosen shape */
+    float ms_default;        /* trial time of the 16x16 default */
+} rcmvs_tune_entry;
+int rcmvs_autotune(rcmvs_ctx* ctx, rcmvs_scene* scene, const rcmvs_job* jobs, int32_t n_jobs,
+                   const rcmvs_options* opts);
+/* Copies up to cap tuned classes of the context; *n_out = classes stored. */
+int rcmvs_tune_table(rcmvs_ctx* ctx, rcmvs_tune_entry* out, int32_t cap, int32_t* n_out);
+/* Replaces the context's table (e.g. one saved from an earlier run); each
+ * shape must have tile_w*tile_h <= 256 pixels, a multiple of 32.  Jobs of
+ * classes whose shapes differ in pixel count may share a launch (its blocks
+ * then have the largest count of threads).  Later tuning keeps the thread
+ * count of entries[0]. */
+int rcmvs_tune_set(rcmvs_ctx* ctx, const rcmvs_tune_entry* entries, int32_t n);
 /* Device-resident fusion of the scene's depth maps (views that were the
  * reference of a job have a map).  *n_points_out gets the fused count
  * (this call synchronises once to size the output). */

@@ -63,6 +63,11 @@ class Job(C.Structure):
     ]
 
 
+class TuneEntry(C.Structure):
+    _fields_ = [("w", C.c_int32), ("h", C.c_int32), ("tile_w", C.c_int32), ("tile_h", C.c_int32),
+                ("ms_best", C.c_float), ("ms_default", C.c_float)]
+
+
 class DepthOut(C.Structure):
     _fields_ = [("depth", C.c_void_p), ("cost", C.c_void_p), ("normal", C.c_void_p)]
 

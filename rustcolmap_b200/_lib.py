@@ -72,6 +72,9 @@ def mvs():
         "rcmvs_scene_costvol": ([vp, vp, vp, i32, vp], C.c_int),
         "rcmvs_scene_estimate_depth_learned": ([vp, vp, vp, i32, vp, vp, C.c_float, i32, C.c_float, vp], C.c_int),
         "rcmvs_run_mvs_learned": ([vp, vp, i32, vp, vp, vp, C.c_float, i32, C.c_float, vp, vp, vp], C.c_int),
+        "rcmvs_autotune": ([vp, vp, vp, i32, vp], C.c_int),
+        "rcmvs_tune_table": ([vp, vp, i32, vp], C.c_int),
+        "rcmvs_tune_set": ([vp, vp, i32], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -111,5 +114,6 @@ _SIG_NAMES = [
     "rcmvs_last_work", "rcmvs_selftest_f2i", "rcmvs_ctx_timing", "rcmvs_ctx_kernel_time",
     "rcmvs_estimate_depth_noalloc", "rcmvs_net_param_count", "rcmvs_net_create", "rcmvs_net_destroy",
     "rcmvs_net_get_params", "rcmvs_net_forward", "rcmvs_net_train_step", "rcmvs_scene_costvol",
-    "rcmvs_scene_estimate_depth_learned", "rcmvs_run_mvs_learned",
+    "rcmvs_scene_estimate_depth_learned", "rcmvs_run_mvs_learned", "rcmvs_autotune", "rcmvs_tune_table",
+    "rcmvs_tune_set",
 ]

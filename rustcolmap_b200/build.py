@@ -27,7 +27,8 @@ FLAGS = ARCH + [
 ]
 
 LIBS = {
-    "librcmvs.so": ["capi.cu", "census.cu", "stereo.cu", "fuse.cu", "noalloc.cu", "learned.cu", "learned_api.cu"],
+    "librcmvs.so": ["capi.cu", "census.cu", "stereo.cu", "fuse.cu", "noalloc.cu", "learned.cu", "learned_api.cu",
+                   "schedule.cu"],
     "librcscene.so": ["scene.cu"],
 }
 HEADERS = [os.path.join(CSRC, "rcmvs_internal.cuh"), os.path.join(CSRC, "ctx_internal.cuh"),

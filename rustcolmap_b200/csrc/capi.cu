@@ -13,25 +13,6 @@
 #include "rcmvs_internal.cuh"
 
 namespace rcmvs {
-size_t stereo_smem_bytes(TileShape ts);
-cudaError_t stereo_configure(TileShape ts);
-cudaError_t launch_census_rays(const DevView* d_views, const int32_t* d_tile_start, int n_views, int total_tiles,
-                               const uint8_t* gray, uint64_t* census, float2* rays, const double* d_cams,
-                               cudaStream_t st);
-cudaError_t launch_init(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, int total_tiles, TileShape ts,
-                        int nh, const uint64_t* census, const float2* rays, PlaneBuf out, unsigned long long* d_work,
-                        cudaStream_t st, int variant);
-cudaError_t launch_pass(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, int total_tiles, TileShape ts,
-                        uint64_t pass, float sig_inv, float sig_n, const uint64_t* census, const float2* rays,
-                        PlaneBuf prev, PlaneBuf next, unsigned long long* d_work, cudaStream_t st, int variant);
-cudaError_t launch_gate(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, int total_tiles, TileShape ts,
-                        float cost_thr, const uint64_t* census, PlaneBuf planes, float* depth, float* cost,
-                        float* normal, cudaStream_t st);
-cudaError_t launch_cost_field(const DevJob* d_job, const int32_t* d_job_start, int total_tiles, TileShape ts,
-                              const uint64_t* census, const float2* rays, const float4* planes, const float* hints,
-                              float* cost_out, int32_t* hsum_out, cudaStream_t st);
-cudaError_t launch_f2i(const float* in, int n, int32_t* out, cudaStream_t st);
-
 constexpr int kCensusTileW = 32, kCensusTileH = 8;
 
 cudaError_t DeviceArena::get(int slot, size_t bytes, void** out) {
@@ -71,8 +52,8 @@ using namespace rcmvs;
 
 namespace {
 
-enum { S_JOBS = 0, S_JOBSTART = 1, S_CGRAY = 2, S_CCEN = 3, S_FIELD_PL = 4, S_FIELD_H = 5, S_FIELD_C = 6,
-       S_FIELD_HS = 7, S_F2I = 8, S_DIV_B = 9, S_DIV_OK = 10 };
+enum { S_JOBS = kSlotJobs, S_JOBSTART = kSlotJobStart, S_CGRAY = 2, S_CCEN = 3, S_FIELD_PL = 4, S_FIELD_H = 5,
+       S_FIELD_C = 6, S_FIELD_HS = 7, S_F2I = 8 };
 
 int fail(rcmvs_ctx* ctx, int code, const std::string& msg) {
     if (ctx) ctx->err = msg;
@@ -105,66 +86,6 @@ int check_view(rcmvs_ctx* ctx, const rcmvs_view& v, int i, const rcmvs_options* 
     return RCMVS_OK;
 }
 
-TileShape tile_of(const rcmvs_options* o) {
-    TileShape t{16, 16};
-    if (o && o->tile_w > 0 && o->tile_h > 0) t = TileShape{(int)o->tile_w, (int)o->tile_h};
-    return t;
-}
-
-int ensure_tile(rcmvs_ctx* ctx, TileShape ts) {
-    if (ts.tw <= 0 || ts.th <= 0 || ts.tw * ts.th > 256 || (ts.tw * ts.th) % 32 != 0)
-        return fail(ctx, RCMVS_E_ARG, "tile shape must have tw*th <= 256 threads, a multiple of 32");
-    if (stereo_smem_bytes(ts) > 200 * 1024) return fail(ctx, RCMVS_E_LIMIT, "tile shape needs too much shared memory");
-    if (ctx->configured.tw != ts.tw || ctx->configured.th != ts.th) {
-        CK(stereo_configure(ts));
-        ctx->configured = ts;
-    }
-    return RCMVS_OK;
-}
-
-// mvs/src/stereo.rs:131-132 in f64, cast to f32 (RefWorkspace::new)
-void rel_pose(const HostCam& r, const HostCam& s, float* rs, float* ts) {
-    double rs64[9];
-    for (int i = 0; i < 3; ++i)
-        for (int j = 0; j < 3; ++j)
-            rs64[3 * i + j] = s.R[3 * i] * r.R[3 * j] + s.R[3 * i + 1] * r.R[3 * j + 1] + s.R[3 * i + 2] * r.R[3 * j + 2];
-    for (int i = 0; i < 9; ++i) rs[i] = (float)rs64[i];
-    for (int i = 0; i < 3; ++i) {
-        double rt = rs64[3 * i] * r.t[0] + rs64[3 * i + 1] * r.t[1] + rs64[3 * i + 2] * r.t[2];
-        ts[i] = (float)(s.t[i] - rt);
-    }
-}
-
-void fill_job(const rcmvs_scene* sc, int ref, const int32_t* srcs, int n_src, double zmin, double zmax, TileShape ts,
-              DevJob& J) {
-    std::memset(&J, 0, sizeof(J));
-    const DevView& V = sc->views[ref];
-    J.view = ref;
-    J.nsrc = n_src;
-    J.w = V.w;
-    J.h = V.h;
-    J.off = V.off;
-    J.zmin = (float)zmin;
-    J.zmax = (float)zmax;
-    J.inv_min = 1.0f / J.zmax;  // stereo.rs:248-249 (f32)
-    J.inv_max = 1.0f / J.zmin;
-    J.tiles_x = (V.w + ts.tw - 1) / ts.tw;
-    J.tiles_y = (V.h + ts.th - 1) / ts.th;
-    J.tiles = J.tiles_x * J.tiles_y;
-    for (int s = 0; s < n_src; ++s) {
-        const HostCam& c = sc->cams[srcs[s]];
-        DevSrc& D = J.src[s];
-        rel_pose(sc->cams[ref], c, D.rs, D.ts);
-        D.f = (float)c.f;
-        D.cx = (float)c.cx;
-        D.cy = (float)c.cy;
-        D.k = (float)c.k;
-        D.w = sc->views[srcs[s]].w;
-        D.h = sc->views[srcs[s]].h;
-        D.off = sc->views[srcs[s]].off;
-    }
-}
-
 int validate_jobs(rcmvs_ctx* ctx, int n_views, const rcmvs_job* jobs, int n_jobs) {
     if (n_jobs < 0 || (n_jobs > 0 && !jobs)) return fail(ctx, RCMVS_E_ARG, "bad job list");
     std::vector<char> seen(n_views, 0);
@@ -183,8 +104,6 @@ int validate_jobs(rcmvs_ctx* ctx, int n_views, const rcmvs_job* jobs, int n_jobs
     }
     return RCMVS_OK;
 }
-
-float powf_host(float b, float e) { return powf(b, e); }
 
 }  // namespace
 
@@ -282,6 +201,7 @@ void rcmvs_scene_destroy(rcmvs_scene* sc) {
                   sc->depth, sc->cost, sc->normal, sc->d_views, sc->d_tile_start, sc->d_cams,
                   sc->gray_q, sc->census_q, sc->rays_q, sc->d_qviews, sc->d_qtile_start, sc->d_qcams,
                   sc->d_qblk_start};
+    drop_graph(sc);
     for (void* p : ps)
         if (p) cudaFree(p);
     sc->arena.release();
@@ -397,56 +317,27 @@ int rcmvs_scene_estimate_depth(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job*
         if ((uint32_t)std::max(V.w, V.h) > opts->max_dim)
             return fail(ctx, RCMVS_E_ARG, "reference view long side exceeds max_dim");
     }
-    if (opts->flags & ~RCMVS_FLAG_ONE_CANDIDATE) return fail(ctx, RCMVS_E_ARG, "unknown bits in opts->flags");
+    constexpr uint32_t kFlags = RCMVS_FLAG_ONE_CANDIDATE | RCMVS_FLAG_PERSISTENT | RCMVS_FLAG_CUDA_GRAPH |
+                                RCMVS_FLAG_AUTOTUNE;
+    if (opts->flags & ~kFlags) return fail(ctx, RCMVS_E_ARG, "unknown bits in opts->flags");
     if (n_jobs == 0) return RCMVS_OK;
-    const TileShape ts = tile_of(opts);
     CK(cudaSetDevice(ctx->device));
-    rc = ensure_tile(ctx, ts);
+    StereoBatch batch;
+    rc = build_batch(ctx, sc, jobs, n_jobs, opts, batch);
     if (rc) return rc;
-    std::vector<DevJob> hj(n_jobs);
-    std::vector<int32_t> start(n_jobs + 1);
-    int64_t tiles = 0;
-    for (int j = 0; j < n_jobs; ++j) {
-        fill_job(sc, jobs[j].ref_idx, jobs[j].srcs, jobs[j].n_src, jobs[j].zmin, jobs[j].zmax, ts, hj[j]);
-        hj[j].tile_base = (int32_t)tiles;
-        start[j] = (int32_t)tiles;
-        tiles += hj[j].tiles;
-    }
-    if (tiles > INT32_MAX) return fail(ctx, RCMVS_E_LIMIT, "too many tiles in one batch");
-    start[n_jobs] = (int32_t)tiles;
-    void *pj, *ps;
-    CK(sc->arena.get(S_JOBS, sizeof(DevJob) * n_jobs, &pj));
-    CK(sc->arena.get(S_JOBSTART, sizeof(int32_t) * (n_jobs + 1), &ps));
     cudaStream_t st = ctx->stream;
-    CK(cudaMemcpyAsync(pj, hj.data(), sizeof(DevJob) * n_jobs, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(ps, start.data(), sizeof(int32_t) * (n_jobs + 1), cudaMemcpyHostToDevice, st));
-    const DevJob* dj = (const DevJob*)pj;
-    const int32_t* dst = (const int32_t*)ps;
     unsigned long long* dw = ctx->count_work ? ctx->d_work : nullptr;
     if (dw) CK(cudaMemsetAsync(dw, 0, 2 * sizeof(unsigned long long), st));
-    const int nh = (int)std::max<uint32_t>(opts->num_hyp, 2u);
-    PlaneBuf A{sc->plane_a, sc->pcost_a}, B{sc->plane_b, sc->pcost_b};
-    const SpanHook hk = ctx->hook();
-    hk.begin("stereo_init");
-    const int variant = (opts->flags & RCMVS_FLAG_ONE_CANDIDATE) ? 1 : 0;
-    CK(launch_init(dj, dst, n_jobs, (int)tiles, ts, nh, sc->census, sc->rays, A, dw, st, variant));
-    hk.end("stereo_init");
-    const uint64_t n_passes = (uint64_t)std::max<uint32_t>(opts->sweeps, 1u) * 2;
-    for (uint64_t pass = 0; pass < n_passes; ++pass) {
-        // stereo.rs:275-277 with the host's libm powf, as the reference
-        const float t = (float)pass / (float)n_passes;
-        const float sig_inv = 0.02f * powf_host(0.28f, t * 4.0f);
-        const float sig_n = 0.30f * powf_host(0.42f, t * 4.0f);
-        hk.begin("stereo_pass");
-        CK(launch_pass(dj, dst, n_jobs, (int)tiles, ts, pass, sig_inv, sig_n, sc->census, sc->rays, A, B, dw, st,
-                       variant));
-        hk.end("stereo_pass");
-        std::swap(A, B);
-    }
-    hk.begin("stereo_gate");
-    CK(launch_gate(dj, dst, n_jobs, (int)tiles, ts, opts->cost_thr, sc->census, A, sc->depth, sc->cost, sc->normal,
-                   st));
-    hk.end("stereo_gate");
+    Schedule s;
+    s.init = (opts->flags & RCMVS_FLAG_ONE_CANDIDATE) ? Schedule::ONE_CANDIDATE : Schedule::ROWS;
+    s.nh = (int)std::max<uint32_t>(opts->num_hyp, 2u);
+    s.n_passes = (uint64_t)std::max<uint32_t>(opts->sweeps, 1u) * 2;
+    s.cost_thr = opts->cost_thr;
+    s.persistent = (opts->flags & RCMVS_FLAG_PERSISTENT) != 0;
+    s.graph = (opts->flags & RCMVS_FLAG_CUDA_GRAPH) != 0;
+    s.d_work = dw;
+    rc = run_batch(ctx, sc, batch, s);
+    if (rc) return rc;
     for (int j = 0; j < n_jobs; ++j) sc->has_depth[jobs[j].ref_idx] = 1;
     if (dw) {
         unsigned long long h[2];
@@ -700,8 +591,6 @@ int rcmvs_plane_cost_field(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_vi
     void *pj, *ps, *ppl, *ph, *pc, *phs;
     cudaStream_t st = ctx->stream;
     auto body = [&]() -> int {
-        int r = ensure_tile(ctx, ts);
-        if (r) return r;
         CK(ctx->arena.get(S_JOBS, sizeof(DevJob), &pj));
         CK(ctx->arena.get(S_JOBSTART, sizeof(start), &ps));
         CK(ctx->arena.get(S_FIELD_PL, 16 * n, &ppl));
@@ -712,7 +601,8 @@ int rcmvs_plane_cost_field(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_vi
         CK(cudaMemcpyAsync(ps, start, sizeof(start), cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(ppl, planes, 16 * n, cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(ph, hints, 4 * n, cudaMemcpyHostToDevice, st));
-        CK(launch_cost_field((const DevJob*)pj, (const int32_t*)ps, hj.tiles, ts, sc->census, sc->rays,
+        const LaunchGeom g{ts.tw * ts.th, stereo_smem_bytes(ts), hj.tiles, nullptr};
+        CK(launch_cost_field((const DevJob*)pj, (const int32_t*)ps, g, sc->census, sc->rays,
                              (const float4*)ppl, (const float*)ph, (float*)pc, (int32_t*)phs, st));
         CK(cudaMemcpyAsync(cost_out, pc, 4 * n, cudaMemcpyDeviceToHost, st));
         if (hsum_out) CK(cudaMemcpyAsync(hsum_out, phs, 4 * n, cudaMemcpyDeviceToHost, st));

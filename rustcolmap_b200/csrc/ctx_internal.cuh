@@ -20,7 +20,9 @@ struct rcmvs_ctx {
     bool count_work = false;
     unsigned long long* d_work = nullptr;
     uint64_t last_evals = 0, last_rows = 0;
-    TileShape configured{0, 0};
+    // autotuned tile shapes per resolution class, one thread count for all
+    std::vector<rcmvs_tune_entry> tuned;
+    int tune_nthr = 0;
     // per-kernel CUDA-event spans (rcmvs_ctx_timing)
     struct Span {
         std::string name;
@@ -108,5 +110,61 @@ struct rcmvs_scene {
     int32_t* d_qblk_start = nullptr;
     int qcensus_tiles = 0, qblocks = 0;
     int64_t nq_px = 0;
+    // the last captured stereo schedule (RCMVS_FLAG_CUDA_GRAPH) and its key
+    cudaGraphExec_t graph = nullptr;
+    std::vector<unsigned char> graph_key;
 };
+
+namespace rcmvs {
+
+// Arena slots of a scene shared by the translation units (the others are
+// private to capi.cu 2-10, fuse.cu 16-35 and learned_api.cu 40-47).
+constexpr int kSlotJobs = 0, kSlotJobStart = 1, kSlotQueue = 11, kSlotTuneJobs = 12, kSlotTuneStart = 13;
+
+// mvs/src/stereo.rs:131-132: source pose relative to the reference, f64
+// products cast to f32.
+void rel_pose(const HostCam& r, const HostCam& s, float* rs, float* ts);
+// mvs/src/stereo.rs:114-151: one job's device descriptor (relative poses in
+// f64 cast to f32, source intrinsics and census offsets), tile shape ts.
+void fill_job(const rcmvs_scene* sc, int ref, const int32_t* srcs, int n_src, double zmin, double zmax, TileShape ts,
+              DevJob& J);
+
+// One stereo batch as launched: jobs in launch order (longest tiles first),
+// their tile starts, the caller's index of each, and the launch geometry.
+struct StereoBatch {
+    std::vector<DevJob> jobs;
+    std::vector<int32_t> start;  // n_jobs + 1
+    std::vector<int> order;      // launch position -> caller's job index
+    LaunchGeom geom{};
+};
+
+// The launch schedule of a batch: init -> n_passes Jacobi passes -> gate.
+struct Schedule {
+    enum Init { ROWS = 0, ONE_CANDIDATE = 1, LEARNED = 2 } init = ROWS;
+    int nh = 64;
+    uint64_t n_passes = 12;
+    float cost_thr = 0.38f;
+    bool persistent = false;
+    bool graph = false;
+    unsigned long long* d_work = nullptr;  // work counters (zeroed by the caller)
+    // learned init
+    const float* pred = nullptr;
+    const int64_t* pred_off = nullptr;  // per launch position
+    float conf_thr = 0.f;
+    int n_local = 1;
+    float span = 0.f;
+    unsigned long long* d_learned = nullptr;  // zeroed inside the schedule
+};
+
+// Validates shapes, looks up (and with RCMVS_FLAG_AUTOTUNE, first tunes)
+// per-class shapes, orders jobs and fills b.  Returns an RCMVS_* code.
+int build_batch(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job* jobs, int n_jobs, const rcmvs_options* opts,
+                StereoBatch& b);
+// Uploads b's job table and runs the schedule on the context stream
+// (asynchronous).  Returns an RCMVS_* code.
+int run_batch(rcmvs_ctx* ctx, rcmvs_scene* sc, const StereoBatch& b, const Schedule& s);
+// Drops the scene's cached graph.
+void drop_graph(rcmvs_scene* sc);
+
+}  // namespace rcmvs
 

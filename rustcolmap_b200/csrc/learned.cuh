@@ -33,11 +33,4 @@ cudaError_t launch_loss(const float* out, const float* lab, int64_t npx, float i
                         cudaStream_t st);
 cudaError_t launch_adam(float* p, const float* g, float* m, float* v, const uint8_t* mask, int64_t n, float lr,
                         float b1, float b2, float eps, float bc1, float bc2, float gscale, void* pb, cudaStream_t st);
-// stereo.cu: patch-match init from per-pixel predictions (quarter resolution,
-// NET_OUT_C f32 channels per pixel; job j's predictions start at pred_off[j]).
-cudaError_t launch_init_learned(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, int total_tiles,
-                                TileShape ts, int nh, const uint64_t* census, const float2* rays, PlaneBuf out,
-                                const float* pred, const int64_t* pred_off, float conf_thr, int n_local,
-                                float span, unsigned long long* d_learned, cudaStream_t st);
-
 }  // namespace rcmvs

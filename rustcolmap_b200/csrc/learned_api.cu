@@ -11,19 +11,6 @@
 #include "ctx_internal.cuh"
 #include "learned.cuh"
 
-namespace rcmvs {
-cudaError_t launch_census_rays(const DevView* d_views, const int32_t* d_tile_start, int n_views, int total_tiles,
-                               const uint8_t* gray, uint64_t* census, float2* rays, const double* d_cams,
-                               cudaStream_t st);
-cudaError_t launch_pass(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, int total_tiles, TileShape ts,
-                        uint64_t pass, float sig_inv, float sig_n, const uint64_t* census, const float2* rays,
-                        PlaneBuf prev, PlaneBuf next, unsigned long long* d_work, cudaStream_t st, int variant);
-cudaError_t launch_gate(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, int total_tiles, TileShape ts,
-                        float cost_thr, const uint64_t* census, PlaneBuf planes, float* depth, float* cost,
-                        float* normal, cudaStream_t st);
-cudaError_t stereo_configure(TileShape ts);
-size_t stereo_smem_bytes(TileShape ts);
-}  // namespace rcmvs
 
 using namespace rcmvs;
 
@@ -335,18 +322,6 @@ int quarter_prepare(rcmvs_ctx* ctx, rcmvs_scene* sc) {
     return RCMVS_OK;
 }
 
-void rel_pose_q(const HostCam& r, const HostCam& s, float* rs, float* ts) {
-    double rs64[9];
-    for (int i = 0; i < 3; ++i)
-        for (int j = 0; j < 3; ++j)
-            rs64[3 * i + j] = s.R[3 * i] * r.R[3 * j] + s.R[3 * i + 1] * r.R[3 * j + 1] + s.R[3 * i + 2] * r.R[3 * j + 2];
-    for (int i = 0; i < 9; ++i) rs[i] = (float)rs64[i];
-    for (int i = 0; i < 3; ++i) {
-        double rt = rs64[3 * i] * r.t[0] + rs64[3 * i + 1] * r.t[1] + rs64[3 * i + 2] * r.t[2];
-        ts[i] = (float)(s.t[i] - rt);
-    }
-}
-
 // quarter-resolution jobs (for the cost volume): views, sizes and
 // intrinsics of the quarter copies; also returns each job's output offset.
 int quarter_jobs(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job* jobs, int n_jobs, DevJob** d_jobs,
@@ -375,7 +350,7 @@ int quarter_jobs(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job* jobs, int n_j
             const int sv = jobs[j].srcs[s];
             const HostCam& c = sc->cams[sv];
             DevSrc& D = J.src[s];
-            rel_pose_q(rc, c, D.rs, D.ts);
+            rel_pose(rc, c, D.rs, D.ts);
             D.f = (float)(c.f / 4.0);
             D.cx = (float)((c.cx - 1.5) / 4.0);
             D.cy = (float)((c.cy - 1.5) / 4.0);
@@ -493,82 +468,35 @@ int rcmvs_scene_estimate_depth_learned(rcmvs_ctx* ctx, rcmvs_scene* sc, const rc
         }
     }
     hk.end("learned_net");
-    // full-resolution jobs
-    const TileShape ts = (opts->tile_w > 0 && opts->tile_h > 0) ? TileShape{(int)opts->tile_w, (int)opts->tile_h}
-                                                               : TileShape{16, 16};
-    if (ts.tw * ts.th > 256 || (ts.tw * ts.th) % 32 != 0) return lfail(ctx, RCMVS_E_ARG, "bad tile shape");
-    if (ctx->configured.tw != ts.tw || ctx->configured.th != ts.th) {
-        LCK(stereo_configure(ts));
-        ctx->configured = ts;
+    // full-resolution jobs: the shared stereo batch with the learned init
+    StereoBatch batch;
+    rc = build_batch(ctx, sc, jobs, n_jobs, opts, batch);
+    if (rc) return rc;
+    std::vector<int64_t> qoff(n_jobs), poff(n_jobs);
+    for (int j = 0, o = 0; j < n_jobs; ++j) {
+        qoff[j] = o;
+        o += (int64_t)sc->qviews[jobs[j].ref_idx].w * sc->qviews[jobs[j].ref_idx].h;
     }
-    std::vector<DevJob> hj(n_jobs);
-    std::vector<int32_t> start(n_jobs + 1);
-    int64_t tiles = 0;
-    for (int j = 0; j < n_jobs; ++j) {
-        DevJob& J = hj[j];
-        std::memset(&J, 0, sizeof(J));
-        const int r = jobs[j].ref_idx;
-        const DevView& V = sc->views[r];
-        J.view = r;
-        J.nsrc = jobs[j].n_src;
-        J.w = V.w;
-        J.h = V.h;
-        J.off = V.off;
-        J.zmin = (float)jobs[j].zmin;
-        J.zmax = (float)jobs[j].zmax;
-        J.inv_min = 1.0f / J.zmax;
-        J.inv_max = 1.0f / J.zmin;
-        J.tiles_x = (V.w + ts.tw - 1) / ts.tw;
-        J.tiles_y = (V.h + ts.th - 1) / ts.th;
-        J.tiles = J.tiles_x * J.tiles_y;
-        J.tile_base = (int32_t)tiles;
-        for (int s = 0; s < J.nsrc; ++s) {
-            const int sv = jobs[j].srcs[s];
-            const HostCam& c = sc->cams[sv];
-            DevSrc& D = J.src[s];
-            rel_pose_q(sc->cams[r], c, D.rs, D.ts);
-            D.f = (float)c.f;
-            D.cx = (float)c.cx;
-            D.cy = (float)c.cy;
-            D.k = (float)c.k;
-            D.w = sc->views[sv].w;
-            D.h = sc->views[sv].h;
-            D.off = sc->views[sv].off;
-        }
-        start[j] = (int32_t)tiles;
-        tiles += J.tiles;
-    }
-    start[n_jobs] = (int32_t)tiles;
-    void *pj, *ps, *pcnt;
-    LCK(sc->arena.get(45, sizeof(DevJob) * n_jobs, &pj));
-    LCK(sc->arena.get(46, sizeof(int32_t) * (n_jobs + 1), &ps));
+    for (int p = 0; p < n_jobs; ++p) poff[p] = qoff[batch.order[p]];
+    void *ppo, *pcnt;
+    LCK(sc->arena.get(46, sizeof(int64_t) * n_jobs, &ppo));
     LCK(sc->arena.get(47, 16, &pcnt));
-    LCK(cudaMemcpyAsync(pj, hj.data(), sizeof(DevJob) * n_jobs, cudaMemcpyHostToDevice, st));
-    LCK(cudaMemcpyAsync(ps, start.data(), sizeof(int32_t) * (n_jobs + 1), cudaMemcpyHostToDevice, st));
-    LCK(cudaMemsetAsync(pcnt, 0, 16, st));
-    const DevJob* dj = (const DevJob*)pj;
-    const int32_t* dst = (const int32_t*)ps;
-    const int nh = (int)std::max<uint32_t>(opts->num_hyp, 2u);
-    PlaneBuf A{sc->plane_a, sc->pcost_a}, B{sc->plane_b, sc->pcost_b};
-    hk.begin("learned_init");
-    LCK(launch_init_learned(dj, dst, n_jobs, (int)tiles, ts, nh, sc->census, sc->rays, A, (const float*)pred, dqoff,
-                            conf_thr, n_local, span, (unsigned long long*)pcnt, st));
-    hk.end("learned_init");
-    const uint64_t n_passes = (uint64_t)std::max<uint32_t>(opts->sweeps, 1u) * 2;
-    for (uint64_t pass = 0; pass < n_passes; ++pass) {
-        const float t = (float)pass / (float)n_passes;
-        const float sig_inv = 0.02f * powf(0.28f, t * 4.0f);
-        const float sig_n = 0.30f * powf(0.42f, t * 4.0f);
-        hk.begin("stereo_pass");
-        LCK(launch_pass(dj, dst, n_jobs, (int)tiles, ts, pass, sig_inv, sig_n, sc->census, sc->rays, A, B, nullptr,
-                        st, 0));
-        hk.end("stereo_pass");
-        std::swap(A, B);
-    }
-    hk.begin("stereo_gate");
-    LCK(launch_gate(dj, dst, n_jobs, (int)tiles, ts, opts->cost_thr, sc->census, A, sc->depth, sc->cost, sc->normal,
-                    st));
-    hk.end("stereo_gate");
+    LCK(cudaMemcpyAsync(ppo, poff.data(), sizeof(int64_t) * n_jobs, cudaMemcpyHostToDevice, st));
+    Schedule sched;
+    sched.init = Schedule::LEARNED;
+    sched.nh = (int)std::max<uint32_t>(opts->num_hyp, 2u);
+    sched.n_passes = (uint64_t)std::max<uint32_t>(opts->sweeps, 1u) * 2;
+    sched.cost_thr = opts->cost_thr;
+    sched.persistent = (opts->flags & RCMVS_FLAG_PERSISTENT) != 0;
+    sched.graph = (opts->flags & RCMVS_FLAG_CUDA_GRAPH) != 0;
+    sched.pred = (const float*)pred;
+    sched.pred_off = (const int64_t*)ppo;
+    sched.conf_thr = conf_thr;
+    sched.n_local = n_local;
+    sched.span = span;
+    sched.d_learned = (unsigned long long*)pcnt;
+    rc = run_batch(ctx, sc, batch, sched);
+    if (rc) return rc;
     for (int j = 0; j < n_jobs; ++j) sc->has_depth[jobs[j].ref_idx] = 1;
     if (learned_pixels) {
         unsigned long long h = 0;

@@ -22,21 +22,6 @@
 
 #include "rcmvs_internal.cuh"
 
-namespace rcmvs {
-size_t stereo_smem_bytes(TileShape ts);
-cudaError_t launch_census_rays(const DevView* d_views, const int32_t* d_tile_start, int n_views, int total_tiles,
-                               const uint8_t* gray, uint64_t* census, float2* rays, const double* d_cams,
-                               cudaStream_t st);
-cudaError_t launch_init(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, int total_tiles, TileShape ts,
-                        int nh, const uint64_t* census, const float2* rays, PlaneBuf out, unsigned long long* d_work,
-                        cudaStream_t st, int variant);
-cudaError_t launch_pass(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, int total_tiles, TileShape ts,
-                        uint64_t pass, float sig_inv, float sig_n, const uint64_t* census, const float2* rays,
-                        PlaneBuf prev, PlaneBuf next, unsigned long long* d_work, cudaStream_t st, int variant);
-cudaError_t launch_gate(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, int total_tiles, TileShape ts,
-                        float cost_thr, const uint64_t* census, PlaneBuf planes, float* depth, float* cost,
-                        float* normal, cudaStream_t st);
-}  // namespace rcmvs
 
 using namespace rcmvs;
 
@@ -167,6 +152,8 @@ extern "C" int rcmvs_estimate_depth_noalloc(const rcmvs_view* views, int32_t n_v
     J.tiles_y = (r.h + ts.th - 1) / ts.th;
     J.tiles = J.tiles_x * J.tiles_y;
     J.tile_base = 0;
+    J.tw = ts.tw;
+    J.th = ts.th;
     for (int s = 0; s < n_src; ++s) {
         const rcmvs_view& sv = views[srcs[s]];
         DevSrc& D = J.src[s];
@@ -223,19 +210,19 @@ extern "C" int rcmvs_estimate_depth_noalloc(const rcmvs_view* views, int32_t n_v
     NCK(launch_census_rays(d_views, d_tile_start, nv, tiles, gray, census, rays, d_cams, st));
     const int nh = (int)(opts->num_hyp > 2u ? opts->num_hyp : 2u);
     const int variant = (opts->flags & RCMVS_FLAG_ONE_CANDIDATE) ? 1 : 0;
-    NCK(launch_init(d_job, d_job_start, 1, J.tiles, ts, nh, census, rays, A, nullptr, st, variant));
+    const LaunchGeom g{ts.tw * ts.th, stereo_smem_bytes(ts), J.tiles, nullptr};
+    NCK(launch_init(d_job, d_job_start, 1, g, nh, census, rays, A, nullptr, st, variant));
     const uint64_t n_passes = (uint64_t)(opts->sweeps > 1u ? opts->sweeps : 1u) * 2;
     for (uint64_t pass = 0; pass < n_passes; ++pass) {
         const float t = (float)pass / (float)n_passes;  // stereo.rs:275-277
         const float sig_inv = 0.02f * powf(0.28f, t * 4.0f);
         const float sig_n = 0.30f * powf(0.42f, t * 4.0f);
-        NCK(launch_pass(d_job, d_job_start, 1, J.tiles, ts, pass, sig_inv, sig_n, census, rays, A, Bp, nullptr, st,
-                        variant));
+        NCK(launch_pass(d_job, d_job_start, 1, g, pass, sig_inv, sig_n, census, rays, A, Bp, nullptr, st));
         PlaneBuf tmp = A;
         A = Bp;
         Bp = tmp;
     }
-    NCK(launch_gate(d_job, d_job_start, 1, J.tiles, ts, opts->cost_thr, census, A, depth_dev, cost_dev, nullptr, st));
+    NCK(launch_gate(d_job, d_job_start, 1, g, opts->cost_thr, census, A, depth_dev, cost_dev, nullptr, st));
 #undef NCK
     return RCMVS_OK;
 }

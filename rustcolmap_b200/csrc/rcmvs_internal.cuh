@@ -41,8 +41,10 @@ struct DevJob {
     float inv_min, inv_max;
     int32_t tiles_x, tiles_y;
     int32_t tile_base, tiles;
+    int32_t tw, th;     // this job's tile shape (jobs of one launch may differ)
     DevSrc src[RCMVS_MAX_SOURCES];
 };
+static_assert(sizeof(DevJob) % 8 == 0, "DevJob layout");
 
 // Plane of mvs/src/stereo.rs:24-31, split for 16-byte loads:
 // float4 (nx, ny, nz, z) + float cost.
@@ -51,14 +53,59 @@ struct PlaneBuf {
     float* cost;
 };
 
-// Kernel launch geometry of the stereo kernels.
+// Tile shape of one job's stereo launch (pixels per block = tw * th).
 struct TileShape {
     int tw, th;
 };
 
+// Launch geometry of a stereo launch over the tiles of a job list.  Every
+// job's tile has at most `nthr` pixels; blocks have `nthr` threads and
+// `smem` bytes of dynamic shared memory (the largest tile's).  With `queue`
+// set (a zeroed counter), the launch is persistent: a grid of resident blocks
+// pulls tile indices from the counter until all `tiles` are taken;
+// otherwise block b computes tile b.
+struct LaunchGeom {
+    int nthr;
+    size_t smem;
+    int tiles;
+    unsigned int* queue;
+};
+
 // ---------------------------------------------------------------- launchers
-// Declared (and documented) where they are used, in capi.cu; defined in
-// census.cu and stereo.cu.  All are asynchronous on the given stream.
+// Defined in census.cu and stereo.cu.  All are asynchronous on the given
+// stream.  The stereo launchers run one kernel over every tile of a job list
+// (job j owns tiles [job_start[j], job_start[j+1])).
+
+// census + rays of every view (mvs/src/lib.rs:119-142, sfm-lite geom.rs:28-42)
+cudaError_t launch_census_rays(const DevView* d_views, const int32_t* d_tile_start, int n_views, int total_tiles,
+                               const uint8_t* gray, uint64_t* census, float2* rays, const double* d_cams,
+                               cudaStream_t st);
+size_t stereo_smem_bytes(TileShape ts);
+// Blocks a persistent launch of the pass kernel uses for geometry g.
+int stereo_resident_grid(const LaunchGeom& g);
+// Plane-sweep init (stereo.rs:247-269).  variant 0: row-step schedule;
+// 1: one candidate at a time.  Bit-identical outputs.
+cudaError_t launch_init(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, const LaunchGeom& g, int nh,
+                        const uint64_t* census, const float2* rays, PlaneBuf out, unsigned long long* d_work,
+                        cudaStream_t st, int variant);
+// One Jacobi pass prev -> next (stereo.rs:271-371).
+cudaError_t launch_pass(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, const LaunchGeom& g,
+                        uint64_t pass, float sig_inv, float sig_n, const uint64_t* census, const float2* rays,
+                        PlaneBuf prev, PlaneBuf next, unsigned long long* d_work, cudaStream_t st);
+// Init seeded by the proposal network's predictions (no reference counterpart).
+cudaError_t launch_init_learned(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, const LaunchGeom& g,
+                                int nh, const uint64_t* census, const float2* rays, PlaneBuf out, const float* pred,
+                                const int64_t* pred_off, float conf_thr, int n_local, float span,
+                                unsigned long long* d_learned, cudaStream_t st);
+// Texture/cost/range gate (stereo.rs:373-393); never persistent.
+cudaError_t launch_gate(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, const LaunchGeom& g,
+                        float cost_thr, const uint64_t* census, PlaneBuf planes, float* depth, float* cost,
+                        float* normal, cudaStream_t st);
+// Cost of a given plane field for one job (diagnostics / parity tests).
+cudaError_t launch_cost_field(const DevJob* d_job, const int32_t* d_job_start, const LaunchGeom& g,
+                              const uint64_t* census, const float2* rays, const float4* planes, const float* hints,
+                              float* cost_out, int32_t* hsum_out, cudaStream_t st);
+cudaError_t launch_f2i(const float* in, int n, int32_t* out, cudaStream_t st);
 
 // Fusion (fuse.cu).  View arrays hold per-view f64 cameras/poses.
 struct FuseView {

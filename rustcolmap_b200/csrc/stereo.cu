@@ -19,6 +19,8 @@
 // support-view parameters, a 49-entry h/48 table, and the tile's rays and
 // census with a 2-pixel clamped halo in shared memory; support-view census
 // words are gathered through the read-only path (L1/L2).
+#include <algorithm>
+
 #include "rcmvs_internal.cuh"
 #include "learned.cuh"
 
@@ -72,14 +74,15 @@ __device__ __forceinline__ float gauss3(uint64_t& s) {
 struct Tile {
     const DevJob* job;
     int x0, y0;
-    int stw;  // shared tile row pitch (TW + 2*HALO)
+    int tw, th;  // the job's tile shape
+    int stw;     // shared tile row pitch (tw + 2*HALO)
 };
 
 struct Smem {
     DevSrc* src;     // RCMVS_MAX_SOURCES
     float* tab;      // 64 (49 used): h / 48.0f
-    float2* ray;     // (TH+4)*(TW+4)
-    uint64_t* cen;   // (TH+4)*(TW+4)
+    float2* ray;     // (th+4)*(tw+4)
+    uint64_t* cen;   // (th+4)*(tw+4)
 };
 
 __host__ __device__ inline size_t smem_bytes(int tw, int th) {
@@ -98,19 +101,39 @@ __device__ __forceinline__ Smem carve(unsigned char* base, int tw, int th) {
     return s;
 }
 
-// Stages job sources, the h/48 table and the halo tile; all threads call it.
-__device__ __forceinline__ void load_tile(const DevJob* jobs, const int32_t* job_start, int n_jobs, int tw,
-                                          int th, const uint64_t* __restrict__ census,
-                                          const float2* __restrict__ rays, const Smem& sm, Tile& T) {
-    const int j = find_item(job_start, n_jobs, blockIdx.x);
+// Tile scheduler of the persistent (PERSIST) stereo kernels; all threads of
+// the block call it and get the same answer.  The block takes tile after
+// tile from `queue` (a counter zeroed before the launch) until every tile of
+// the launch has been handed out: the (view, tile) work queue.  Returns -1
+// when the block is done.  Non-persistent kernels compute tile blockIdx.x
+// once.
+__device__ __forceinline__ int next_tile(unsigned int* queue, int tiles, int it, int* s_tile) {
+    if (it > 0) __syncthreads();  // the previous tile's shared data is no longer read
+    if (threadIdx.x == 0) *s_tile = (int)atomicAdd(queue, 1u);
+    __syncthreads();
+    const int t = *s_tile;
+    return t < tiles ? t : -1;
+}
+
+// Resolves launch tile `tile` to its job, carves shared memory for the job's
+// tile shape and stages the job's sources, the h/48 table and the halo tile.
+// All threads call it (threads past the job's tw*th pixels help load).
+__device__ __forceinline__ void load_tile(const DevJob* jobs, const int32_t* job_start, int n_jobs, int tile,
+                                          const uint64_t* __restrict__ census, const float2* __restrict__ rays,
+                                          unsigned char* smem_raw, Smem& sm, Tile& T) {
+    const int j = find_item(job_start, n_jobs, tile);
     const DevJob* J = jobs + j;
     T.job = J;
-    const int t = blockIdx.x - job_start[j];
+    const int tw = J->tw, th = J->th;
+    T.tw = tw;
+    T.th = th;
+    const int t = tile - job_start[j];
     const int tiles_x = J->tiles_x;
     T.x0 = (t % tiles_x) * tw;
     T.y0 = (t / tiles_x) * th;
     T.stw = tw + 2 * HALO;
-    const int nthr = tw * th;
+    sm = carve(smem_raw, tw, th);
+    const int nthr = blockDim.x;
     {
         const int nwords = J->nsrc * (int)(sizeof(DevSrc) / 4);
         const uint32_t* srcw = reinterpret_cast<const uint32_t*>(J->src);
@@ -168,11 +191,6 @@ __device__ __forceinline__ SrcRegs load_src(const DevSrc& s, const uint64_t* __r
     return r;
 }
 
-// The five window terms of one row of one support view (stereo.rs:181-214),
-// added to `sum` in dx order.  `row`: shared-tile index of the row's first
-// window cell.  FRONTO: n = (0,0,1); then denom = 0*xo + 0*yo + 1 is exactly
-// 1.0 for the finite rays the host admits, so z = d/1 = d, and both are
-// skipped.
 // The five window terms of one row of one support view (stereo.rs:181-214),
 // added to `sum` in dx order, with IEEE divides.  `row`: shared-tile index of
 // the row's first window cell.  FRONTO: n = (0,0,1); then denom =
@@ -258,37 +276,42 @@ __device__ __forceinline__ void flush_work(const WorkCount& wc, unsigned long lo
 
 // ---------------------------------------------------------------- init
 // stereo.rs:247-269
-template <bool COUNT>
+template <bool COUNT, bool PERSIST>
 __global__ void init_kernel(const DevJob* __restrict__ jobs, const int32_t* __restrict__ job_start, int n_jobs,
-                            int tw, int th, int nh, const uint64_t* __restrict__ census,
+                            int tiles, unsigned int* queue, int nh, const uint64_t* __restrict__ census,
                             const float2* __restrict__ rays, PlaneBuf out, unsigned long long* d_work) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const Smem sm = carve(smem_raw, tw, th);
-    Tile T;
-    load_tile(jobs, job_start, n_jobs, tw, th, census, rays, sm, T);
-    const DevJob* J = T.job;
-    const int lx = threadIdx.x % tw, ly = threadIdx.x / tw;
-    const int x = T.x0 + lx, y = T.y0 + ly;
+    __shared__ int s_tile;
     WorkCount wc{0, 0};
-    if (x < J->w && y < J->h) {
-        const int nsrc = J->nsrc;
-        const float total = 5.0f * 5.0f * (float)nsrc;
-        const float inv_min = J->inv_min, inv_max = J->inv_max;
-        float best_c = INFINITY;
-        float best_d = 0.f;
-        for (int hi = 0; hi < nh; ++hi) {
-            const float inv = inv_min + (inv_max - inv_min) * (float)hi / (float)(nh - 1);
-            const float d = 1.0f / inv;
-            const float c = plane_cost<true, COUNT, false>(sm, T.stw, lx, ly, nsrc, census, 0.f, 0.f, 1.f, d,
-                                                           best_c + 0.02f, total, wc, nullptr);
-            if (c < best_c) {
-                best_c = c;
-                best_d = d;
+    for (int it = 0; PERSIST || it == 0; ++it) {
+        const int tile = PERSIST ? next_tile(queue, tiles, it, &s_tile) : (int)blockIdx.x;
+        if (tile < 0) break;
+        Smem sm;
+        Tile T;
+        load_tile(jobs, job_start, n_jobs, tile, census, rays, smem_raw, sm, T);
+        const DevJob* J = T.job;
+        const int lx = threadIdx.x % T.tw, ly = threadIdx.x / T.tw;
+        const int x = T.x0 + lx, y = T.y0 + ly;
+        if ((int)threadIdx.x < T.tw * T.th && x < J->w && y < J->h) {
+            const int nsrc = J->nsrc;
+            const float total = 5.0f * 5.0f * (float)nsrc;
+            const float inv_min = J->inv_min, inv_max = J->inv_max;
+            float best_c = INFINITY;
+            float best_d = 0.f;
+            for (int hi = 0; hi < nh; ++hi) {
+                const float inv = inv_min + (inv_max - inv_min) * (float)hi / (float)(nh - 1);
+                const float d = 1.0f / inv;
+                const float c = plane_cost<true, COUNT, false>(sm, T.stw, lx, ly, nsrc, census, 0.f, 0.f, 1.f, d,
+                                                               best_c + 0.02f, total, wc, nullptr);
+                if (c < best_c) {
+                    best_c = c;
+                    best_d = d;
+                }
             }
+            const size_t i = (size_t)J->off + (size_t)y * J->w + x;
+            out.nz[i] = make_float4(0.0f, 0.0f, 1.0f, best_d);
+            out.cost[i] = fminf(best_c, 1.0f);
         }
-        const size_t i = (size_t)J->off + (size_t)y * J->w + x;
-        out.nz[i] = make_float4(0.0f, 0.0f, 1.0f, best_d);
-        out.cost[i] = fminf(best_c, 1.0f);
     }
     if (COUNT) flush_work(wc, d_work);
 }
@@ -299,104 +322,109 @@ __global__ void init_kernel(const DevJob* __restrict__ jobs, const int32_t* __re
 // which equals the reference's copy_from_slice at :278).
 // MINB = 3 blocks of 256 per SM (<= 80 registers) measured fastest; 4 (64
 // registers) spills and loses.
-template <bool COUNT, int MINB>
-__global__ void __launch_bounds__(256, MINB) pass_kernel(const DevJob* __restrict__ jobs, const int32_t* __restrict__ job_start, int n_jobs,
-                            int tw, int th, uint64_t pass, float sig_inv, float sig_n,
-                            const uint64_t* __restrict__ census, const float2* __restrict__ rays, PlaneBuf prev,
-                            PlaneBuf next, unsigned long long* d_work) {
+template <bool COUNT, int MINB, bool PERSIST>
+__global__ void __launch_bounds__(256, MINB)
+    pass_kernel(const DevJob* __restrict__ jobs, const int32_t* __restrict__ job_start, int n_jobs, int tiles,
+                unsigned int* queue, uint64_t pass, float sig_inv, float sig_n, const uint64_t* __restrict__ census,
+                const float2* __restrict__ rays, PlaneBuf prev, PlaneBuf next, unsigned long long* d_work) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const Smem sm = carve(smem_raw, tw, th);
-    Tile T;
-    load_tile(jobs, job_start, n_jobs, tw, th, census, rays, sm, T);
-    const DevJob* J = T.job;
-    const int lx = threadIdx.x % tw, ly = threadIdx.x / tw;
-    const int x = T.x0 + lx, y = T.y0 + ly;
-    const int w = J->w, h = J->h;
+    __shared__ int s_tile;
     WorkCount wc{0, 0};
-    if (x < w && y < h) {
-        const int nsrc = J->nsrc;
-        const float total = 5.0f * 5.0f * (float)nsrc;
-        const float inv_min = J->inv_min, inv_max = J->inv_max;
-        const float zlo = J->zmin * 0.5f, zhi = J->zmax * 2.0f;
-        const size_t base = (size_t)J->off;
-        const size_t i = base + (size_t)y * w + x;
-        const int stw = T.stw;
-        const float2 ri = sm.ray[(ly + HALO) * stw + lx + HALO];
-        uint64_t seed = pixel_rng(x, y, pass + 7);
-        const float4 cur = prev.nz[i];
-        const float cur_cost = prev.cost[i];
-        float best_c = cur_cost;
-        float bn0 = cur.x, bn1 = cur.y, bn2 = cur.z;
-        float bd = cur.w * (bn0 * ri.x + bn1 * ri.y + bn2);
+    for (int it = 0; PERSIST || it == 0; ++it) {
+        const int tile = PERSIST ? next_tile(queue, tiles, it, &s_tile) : (int)blockIdx.x;
+        if (tile < 0) break;
+        Smem sm;
+        Tile T;
+        load_tile(jobs, job_start, n_jobs, tile, census, rays, smem_raw, sm, T);
+        const DevJob* J = T.job;
+        const int lx = threadIdx.x % T.tw, ly = threadIdx.x / T.tw;
+        const int x = T.x0 + lx, y = T.y0 + ly;
+        const int w = J->w, h = J->h;
+        if ((int)threadIdx.x < T.tw * T.th && x < w && y < h) {
+            const int nsrc = J->nsrc;
+            const float total = 5.0f * 5.0f * (float)nsrc;
+            const float inv_min = J->inv_min, inv_max = J->inv_max;
+            const float zlo = J->zmin * 0.5f, zhi = J->zmax * 2.0f;
+            const size_t base = (size_t)J->off;
+            const size_t i = base + (size_t)y * w + x;
+            const int stw = T.stw;
+            const float2 ri = sm.ray[(ly + HALO) * stw + lx + HALO];
+            uint64_t seed = pixel_rng(x, y, pass + 7);
+            const float4 cur = prev.nz[i];
+            const float cur_cost = prev.cost[i];
+            float best_c = cur_cost;
+            float bn0 = cur.x, bn1 = cur.y, bn2 = cur.z;
+            float bd = cur.w * (bn0 * ri.x + bn1 * ri.y + bn2);
 
-        // propagation from the 4 neighbours (stereo.rs:292-321)
-#pragma unroll 1
-        for (int q = 0; q < 4; ++q) {
-            const int ddx = q == 0 ? -1 : (q == 1 ? 1 : 0);
-            const int ddy = q == 2 ? -1 : (q == 3 ? 1 : 0);
-            const int xx = x + ddx, yy = y + ddy;
-            if (xx < 0 || yy < 0 || xx >= w || yy >= h) continue;
-            const float4 nb = prev.nz[base + (size_t)yy * w + xx];
-            const float2 rj = sm.ray[(ly + HALO + ddy) * stw + lx + HALO + ddx];
-            const float a_nb = nb.x * rj.x + nb.y * rj.y + nb.z;
-            if (a_nb < 0.1f) continue;
-            const float d_plane = nb.w * a_nb;
-            const float a_here = nb.x * ri.x + nb.y * ri.y + nb.z;
-            if (a_here < 0.1f) continue;
-            const float zcand = d_plane / a_here;
-            if (!(zlo <= zcand && zcand <= zhi)) continue;
-            const float c = plane_cost<false, COUNT, false>(sm, stw, lx, ly, nsrc, census, nb.x, nb.y, nb.z,
-                                                                  d_plane, best_c + 0.02f, total, wc, nullptr);
-            if (c < best_c) {
-                best_c = c;
-                bn0 = nb.x;
-                bn1 = nb.y;
-                bn2 = nb.z;
-                bd = d_plane;
+            // propagation from the 4 neighbours (stereo.rs:292-321)
+    #pragma unroll 1
+            for (int q = 0; q < 4; ++q) {
+                const int ddx = q == 0 ? -1 : (q == 1 ? 1 : 0);
+                const int ddy = q == 2 ? -1 : (q == 3 ? 1 : 0);
+                const int xx = x + ddx, yy = y + ddy;
+                if (xx < 0 || yy < 0 || xx >= w || yy >= h) continue;
+                const float4 nb = prev.nz[base + (size_t)yy * w + xx];
+                const float2 rj = sm.ray[(ly + HALO + ddy) * stw + lx + HALO + ddx];
+                const float a_nb = nb.x * rj.x + nb.y * rj.y + nb.z;
+                if (a_nb < 0.1f) continue;
+                const float d_plane = nb.w * a_nb;
+                const float a_here = nb.x * ri.x + nb.y * ri.y + nb.z;
+                if (a_here < 0.1f) continue;
+                const float zcand = d_plane / a_here;
+                if (!(zlo <= zcand && zcand <= zhi)) continue;
+                const float c = plane_cost<false, COUNT, false>(sm, stw, lx, ly, nsrc, census, nb.x, nb.y, nb.z,
+                                                                      d_plane, best_c + 0.02f, total, wc, nullptr);
+                if (c < best_c) {
+                    best_c = c;
+                    bn0 = nb.x;
+                    bn1 = nb.y;
+                    bn2 = nb.z;
+                    bd = d_plane;
+                }
             }
-        }
 
-        // random perturbations around the current plane (stereo.rs:323-353)
-#pragma unroll 1
-        for (int r = 0; r < 3; ++r) {
-            const float inv = 1.0f / fmaxf(cur.w, 1e-6f);
-            const float inv_new = inv + sig_inv * (inv_max - inv_min) * gauss3(seed);
-            if (inv_new <= 0.0f) continue;
-            const float zcand = 1.0f / inv_new;
-            if (!(zlo <= zcand && zcand <= zhi)) continue;
-            float nnx = cur.x + sig_n * gauss3(seed);
-            float nny = cur.y + sig_n * gauss3(seed);
-            float nnz = cur.z + sig_n * gauss3(seed);
-            const float len = sqrtf(nnx * nnx + nny * nny + nnz * nnz);
-            if (len < 1e-6f) continue;
-            nnx = nnx / len;
-            nny = nny / len;
-            nnz = nnz / len;
-            const float a_here = nnx * ri.x + nny * ri.y + nnz;
-            if (a_here < 0.1f) continue;
-            const float d_plane = zcand * a_here;
-            const float c = plane_cost<false, COUNT, false>(sm, stw, lx, ly, nsrc, census, nnx, nny, nnz,
-                                                                  d_plane, best_c + 0.02f, total, wc, nullptr);
-            if (c < best_c) {
-                best_c = c;
-                bn0 = nnx;
-                bn1 = nny;
-                bn2 = nnz;
-                bd = d_plane;
+            // random perturbations around the current plane (stereo.rs:323-353)
+    #pragma unroll 1
+            for (int r = 0; r < 3; ++r) {
+                const float inv = 1.0f / fmaxf(cur.w, 1e-6f);
+                const float inv_new = inv + sig_inv * (inv_max - inv_min) * gauss3(seed);
+                if (inv_new <= 0.0f) continue;
+                const float zcand = 1.0f / inv_new;
+                if (!(zlo <= zcand && zcand <= zhi)) continue;
+                float nnx = cur.x + sig_n * gauss3(seed);
+                float nny = cur.y + sig_n * gauss3(seed);
+                float nnz = cur.z + sig_n * gauss3(seed);
+                const float len = sqrtf(nnx * nnx + nny * nny + nnz * nnz);
+                if (len < 1e-6f) continue;
+                nnx = nnx / len;
+                nny = nny / len;
+                nnz = nnz / len;
+                const float a_here = nnx * ri.x + nny * ri.y + nnz;
+                if (a_here < 0.1f) continue;
+                const float d_plane = zcand * a_here;
+                const float c = plane_cost<false, COUNT, false>(sm, stw, lx, ly, nsrc, census, nnx, nny, nnz,
+                                                                      d_plane, best_c + 0.02f, total, wc, nullptr);
+                if (c < best_c) {
+                    best_c = c;
+                    bn0 = nnx;
+                    bn1 = nny;
+                    bn2 = nnz;
+                    bd = d_plane;
+                }
             }
-        }
 
-        float4 o = cur;
-        float oc = cur_cost;
-        if (best_c < cur_cost) {  // stereo.rs:355-367
-            const float a_here = bn0 * ri.x + bn1 * ri.y + bn2;
-            if (a_here > 0.05f) {
-                o = make_float4(bn0, bn1, bn2, bd / a_here);
-                oc = fminf(best_c, 1.0f);
+            float4 o = cur;
+            float oc = cur_cost;
+            if (best_c < cur_cost) {  // stereo.rs:355-367
+                const float a_here = bn0 * ri.x + bn1 * ri.y + bn2;
+                if (a_here > 0.05f) {
+                    o = make_float4(bn0, bn1, bn2, bd / a_here);
+                    oc = fminf(best_c, 1.0f);
+                }
             }
+            next.nz[i] = o;
+            next.cost[i] = oc;
         }
-        next.nz[i] = o;
-        next.cost[i] = oc;
     }
     if (COUNT) flush_work(wc, d_work);
 }
@@ -414,65 +442,70 @@ __device__ __forceinline__ float hyp_depth(float inv_min, float inv_max, int hi,
     return 1.0f / inv;
 }
 
-template <bool COUNT, int MINB>
+template <bool COUNT, int MINB, bool PERSIST>
 __global__ void __launch_bounds__(256, MINB)
-    init_rows_kernel(const DevJob* __restrict__ jobs, const int32_t* __restrict__ job_start, int n_jobs, int tw, int th,
-                     int nh, const uint64_t* __restrict__ census, const float2* __restrict__ rays, PlaneBuf out,
-                     unsigned long long* d_work) {
+    init_rows_kernel(const DevJob* __restrict__ jobs, const int32_t* __restrict__ job_start, int n_jobs, int tiles,
+                     unsigned int* queue, int nh, const uint64_t* __restrict__ census, const float2* __restrict__ rays,
+                     PlaneBuf out, unsigned long long* d_work) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const Smem sm = carve(smem_raw, tw, th);
-    Tile T;
-    load_tile(jobs, job_start, n_jobs, tw, th, census, rays, sm, T);
-    const DevJob* J = T.job;
-    const int lx = threadIdx.x % tw, ly = threadIdx.x / tw;
-    const int x = T.x0 + lx, y = T.y0 + ly;
-    const bool inside = x < J->w && y < J->h;
+    __shared__ int s_tile;
     WorkCount wc{0, 0};
-    const int nsrc = J->nsrc;
-    const float total = 5.0f * 5.0f * (float)nsrc;
-    const float inv_min = J->inv_min, inv_max = J->inv_max;
-    float best_c = INFINITY, best_d = 0.f;
-    int hi = 0, si = 0, dy = 0;
-    float d = hyp_depth(inv_min, inv_max, 0, nh);
-    float sum = 0.f;
-    float thr = INFINITY;  // (best_c + 0.02) + 0.12 with best_c = +inf
-    int32_t hs = 0;
-    bool live = inside;
-    if (COUNT && live) wc.evals++;
-    while (live) {
-        bool fin = true, aborted = false;
-        if (nsrc > 0) {
-            const SrcRegs s = load_src(sm.src[si], census);
-            sum = cost_row<true, false>(sm, (ly + dy) * T.stw + lx, s, 0.f, 0.f, 1.f, d, sum, hs);
-            if (COUNT) wc.rows++;
-            aborted = sum / ((float)(dy + 1) * 5.0f * (float)(si + 1)) > thr;
-            fin = aborted || (si == nsrc - 1 && dy == 4);
-        }
-        if (fin) {
-            const float c = aborted ? 1e9f : sum / total;
-            if (c < best_c) {
-                best_c = c;
-                best_d = d;
+    for (int it = 0; PERSIST || it == 0; ++it) {
+        const int tile = PERSIST ? next_tile(queue, tiles, it, &s_tile) : (int)blockIdx.x;
+        if (tile < 0) break;
+        Smem sm;
+        Tile T;
+        load_tile(jobs, job_start, n_jobs, tile, census, rays, smem_raw, sm, T);
+        const DevJob* J = T.job;
+        const int lx = threadIdx.x % T.tw, ly = threadIdx.x / T.tw;
+        const int x = T.x0 + lx, y = T.y0 + ly;
+        const bool inside = (int)threadIdx.x < T.tw * T.th && x < J->w && y < J->h;
+        const int nsrc = J->nsrc;
+        const float total = 5.0f * 5.0f * (float)nsrc;
+        const float inv_min = J->inv_min, inv_max = J->inv_max;
+        float best_c = INFINITY, best_d = 0.f;
+        int hi = 0, si = 0, dy = 0;
+        float d = hyp_depth(inv_min, inv_max, 0, nh);
+        float sum = 0.f;
+        float thr = INFINITY;  // (best_c + 0.02) + 0.12 with best_c = +inf
+        int32_t hs = 0;
+        bool live = inside;
+        if (COUNT && live) wc.evals++;
+        while (live) {
+            bool fin = true, aborted = false;
+            if (nsrc > 0) {
+                const SrcRegs s = load_src(sm.src[si], census);
+                sum = cost_row<true, false>(sm, (ly + dy) * T.stw + lx, s, 0.f, 0.f, 1.f, d, sum, hs);
+                if (COUNT) wc.rows++;
+                aborted = sum / ((float)(dy + 1) * 5.0f * (float)(si + 1)) > thr;
+                fin = aborted || (si == nsrc - 1 && dy == 4);
             }
-            if (++hi >= nh) {
-                live = false;
-            } else {
-                d = hyp_depth(inv_min, inv_max, hi, nh);
-                sum = 0.f;
-                si = 0;
+            if (fin) {
+                const float c = aborted ? 1e9f : sum / total;
+                if (c < best_c) {
+                    best_c = c;
+                    best_d = d;
+                }
+                if (++hi >= nh) {
+                    live = false;
+                } else {
+                    d = hyp_depth(inv_min, inv_max, hi, nh);
+                    sum = 0.f;
+                    si = 0;
+                    dy = 0;
+                    thr = (best_c + 0.02f) + 0.12f;
+                    if (COUNT) wc.evals++;
+                }
+            } else if (++dy == 5) {
                 dy = 0;
-                thr = (best_c + 0.02f) + 0.12f;
-                if (COUNT) wc.evals++;
+                ++si;
             }
-        } else if (++dy == 5) {
-            dy = 0;
-            ++si;
         }
-    }
-    if (inside) {
-        const size_t i = (size_t)J->off + (size_t)y * J->w + x;
-        out.nz[i] = make_float4(0.0f, 0.0f, 1.0f, best_d);
-        out.cost[i] = fminf(best_c, 1.0f);
+        if (inside) {
+            const size_t i = (size_t)J->off + (size_t)y * J->w + x;
+            out.nz[i] = make_float4(0.0f, 0.0f, 1.0f, best_d);
+            out.cost[i] = fminf(best_c, 1.0f);
+        }
     }
     if (COUNT) flush_work(wc, d_work);
 }
@@ -495,128 +528,136 @@ __global__ void __launch_bounds__(256, MINB)
 // run both lists one after the other.  Fronto-parallel sweep planes go
 // through the general cost path: with n = (0,0,1), denom is exactly 1.0 and
 // d/1 = d, so each candidate's cost is the same float as in the sweep.
+template <bool PERSIST>
 __global__ void __launch_bounds__(256, 3)
     init_learned_rows_kernel(const DevJob* __restrict__ jobs, const int32_t* __restrict__ job_start, int n_jobs,
-                             int tw, int th, int nh, const uint64_t* __restrict__ census,
+                             int tiles, unsigned int* queue, int nh, const uint64_t* __restrict__ census,
                              const float2* __restrict__ rays, PlaneBuf out, const float* __restrict__ pred,
                              const int64_t* __restrict__ pred_off, float conf_thr, int n_local, float span,
                              unsigned long long* d_learned) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const Smem sm = carve(smem_raw, tw, th);
-    Tile T;
-    load_tile(jobs, job_start, n_jobs, tw, th, census, rays, sm, T);
-    const DevJob* J = T.job;
-    const int j = (int)(J - jobs);
-    const int lx = threadIdx.x % tw, ly = threadIdx.x / tw;
-    const int x = T.x0 + lx, y = T.y0 + ly;
-    const bool inside = x < J->w && y < J->h;
-    const int nsrc = J->nsrc;
-    const float total = 5.0f * 5.0f * (float)nsrc;
-    const float zlo = J->zmin * 0.5f, zhi = J->zmax * 2.0f;
-    const float inv_min = J->inv_min, inv_max = J->inv_max, span_inv = inv_max - inv_min;
-    const float2 ri = sm.ray[(ly + HALO) * T.stw + lx + HALO];
-    // this lane's prediction
-    bool learned = false;
-    float pnx = 0.f, pny = 0.f, pnz = 1.f, pa = 1.f, t0 = 0.f;
-    const int wq = J->w >> 2, hq = J->h >> 2;
-    if (inside && wq > 0 && hq > 0) {
-        const int qx = min(x >> 2, wq - 1), qy = min(y >> 2, hq - 1);
-        const float* o = pred + (pred_off[j] + (int64_t)qy * wq + qx) * NET_OUT_C;
-        const float conf = 1.f / (1.f + __expf(-o[4]));
-        const float len = sqrtf(o[1] * o[1] + o[2] * o[2] + o[3] * o[3]);
-        if (conf >= conf_thr && len > 1e-6f) {
-            pnx = o[1] / len;
-            pny = o[2] / len;
-            pnz = o[3] / len;
-            pa = pnx * ri.x + pny * ri.y + pnz;
-            t0 = o[0];
-            learned = pa >= 0.1f;
+    __shared__ int s_tile;
+    for (int it = 0; PERSIST || it == 0; ++it) {
+        const int tile = PERSIST ? next_tile(queue, tiles, it, &s_tile) : (int)blockIdx.x;
+        if (tile < 0) break;
+        Smem sm;
+        Tile T;
+        load_tile(jobs, job_start, n_jobs, tile, census, rays, smem_raw, sm, T);
+        const DevJob* J = T.job;
+        const int j = (int)(J - jobs);
+        const int lx = threadIdx.x % T.tw, ly = threadIdx.x / T.tw;
+        const int x = T.x0 + lx, y = T.y0 + ly;
+        const bool inside = (int)threadIdx.x < T.tw * T.th && x < J->w && y < J->h;
+        const int nsrc = J->nsrc;
+        const float total = 5.0f * 5.0f * (float)nsrc;
+        const float zlo = J->zmin * 0.5f, zhi = J->zmax * 2.0f;
+        const float inv_min = J->inv_min, inv_max = J->inv_max, span_inv = inv_max - inv_min;
+        const float2 ri = inside ? sm.ray[(ly + HALO) * T.stw + lx + HALO] : make_float2(0.f, 0.f);
+        // this lane's prediction
+        bool learned = false;
+        float pnx = 0.f, pny = 0.f, pnz = 1.f, pa = 1.f, t0 = 0.f;
+        const int wq = J->w >> 2, hq = J->h >> 2;
+        if (inside && wq > 0 && hq > 0) {
+            const int qx = min(x >> 2, wq - 1), qy = min(y >> 2, hq - 1);
+            const float* o = pred + (pred_off[j] + (int64_t)qy * wq + qx) * NET_OUT_C;
+            const float conf = 1.f / (1.f + __expf(-o[4]));
+            const float len = sqrtf(o[1] * o[1] + o[2] * o[2] + o[3] * o[3]);
+            if (conf >= conf_thr && len > 1e-6f) {
+                pnx = o[1] / len;
+                pny = o[2] / len;
+                pnz = o[3] / len;
+                pa = pnx * ri.x + pny * ri.y + pnz;
+                t0 = o[0];
+                learned = pa >= 0.1f;
+            }
         }
-    }
-    // candidate stream: list 1 = local planes (learned lanes), list 0 = sweep
-    int list = learned ? 1 : 0, k = 0;
-    bool any_local = false;
-    float cnx = 0.f, cny = 0.f, cnz = 1.f, cd = 0.f, cz = 0.f;
-    auto next = [&]() -> bool {
-        for (;;) {
-            if (list == 1) {
-                if (k >= n_local) {
-                    if (any_local) return false;
-                    list = 0;  // no local plane passed the gates: sweep instead
-                    k = 0;
-                    continue;
+        // candidate stream: list 1 = local planes (learned lanes), list 0 = sweep
+        int list = learned ? 1 : 0, k = 0;
+        bool any_local = false;
+        float cnx = 0.f, cny = 0.f, cnz = 1.f, cd = 0.f, cz = 0.f;
+        auto next = [&]() -> bool {
+            for (;;) {
+                if (list == 1) {
+                    if (k >= n_local) {
+                        if (any_local) return false;
+                        list = 0;  // no local plane passed the gates: sweep instead
+                        k = 0;
+                        continue;
+                    }
+                    const float tk = t0 + span * ((float)k / (float)max(n_local - 1, 1) - 0.5f);
+                    ++k;
+                    const float inv = inv_min + tk * span_inv;
+                    if (!(inv > 0.f)) continue;
+                    const float z = 1.f / inv;
+                    if (!(z >= zlo && z <= zhi)) continue;
+                    cnx = pnx;
+                    cny = pny;
+                    cnz = pnz;
+                    cz = z;
+                    cd = z * pa;
+                    any_local = true;
+                    return true;
                 }
-                const float tk = t0 + span * ((float)k / (float)max(n_local - 1, 1) - 0.5f);
+                if (k >= nh) return false;
+                cnx = 0.f;
+                cny = 0.f;
+                cnz = 1.f;
+                cd = hyp_depth(inv_min, inv_max, k, nh);
+                cz = cd;
                 ++k;
-                const float inv = inv_min + tk * span_inv;
-                if (!(inv > 0.f)) continue;
-                const float z = 1.f / inv;
-                if (!(z >= zlo && z <= zhi)) continue;
-                cnx = pnx;
-                cny = pny;
-                cnz = pnz;
-                cz = z;
-                cd = z * pa;
-                any_local = true;
                 return true;
             }
-            if (k >= nh) return false;
-            cnx = 0.f;
-            cny = 0.f;
-            cnz = 1.f;
-            cd = hyp_depth(inv_min, inv_max, k, nh);
-            cz = cd;
-            ++k;
-            return true;
-        }
-    };
-    float best_c = INFINITY;
-    float4 plane = make_float4(0.0f, 0.0f, 1.0f, 0.0f);
-    bool live = inside && next();
-    int si = 0, dy = 0;
-    float sum = 0.f, thr = INFINITY;
-    int32_t hs = 0;
-    while (live) {
-        bool fin = true, aborted = false;
-        if (nsrc > 0) {
-            const SrcRegs s = load_src(sm.src[si], census);
-            sum = cost_row<false, false>(sm, (ly + dy) * T.stw + lx, s, cnx, cny, cnz, cd, sum, hs);
-            aborted = sum / ((float)(dy + 1) * 5.0f * (float)(si + 1)) > thr;
-            fin = aborted || (si == nsrc - 1 && dy == 4);
-        }
-        if (fin) {
-            const float c = aborted ? 1e9f : sum / total;
-            if (c < best_c) {
-                best_c = c;
-                plane = make_float4(cnx, cny, cnz, cz);
+        };
+        float best_c = INFINITY;
+        float4 plane = make_float4(0.0f, 0.0f, 1.0f, 0.0f);
+        bool live = inside && next();
+        int si = 0, dy = 0;
+        float sum = 0.f, thr = INFINITY;
+        int32_t hs = 0;
+        while (live) {
+            bool fin = true, aborted = false;
+            if (nsrc > 0) {
+                const SrcRegs s = load_src(sm.src[si], census);
+                sum = cost_row<false, false>(sm, (ly + dy) * T.stw + lx, s, cnx, cny, cnz, cd, sum, hs);
+                aborted = sum / ((float)(dy + 1) * 5.0f * (float)(si + 1)) > thr;
+                fin = aborted || (si == nsrc - 1 && dy == 4);
             }
-            live = next();
-            sum = 0.f;
-            si = 0;
-            dy = 0;
-            thr = (best_c + 0.02f) + 0.12f;
-        } else if (++dy == 5) {
-            dy = 0;
-            ++si;
+            if (fin) {
+                const float c = aborted ? 1e9f : sum / total;
+                if (c < best_c) {
+                    best_c = c;
+                    plane = make_float4(cnx, cny, cnz, cz);
+                }
+                live = next();
+                sum = 0.f;
+                si = 0;
+                dy = 0;
+                thr = (best_c + 0.02f) + 0.12f;
+            } else if (++dy == 5) {
+                dy = 0;
+                ++si;
+            }
         }
+        const bool seeded = inside && learned && any_local;
+        if (inside) {
+            const size_t i = (size_t)J->off + (size_t)y * J->w + x;
+            out.nz[i] = plane;
+            out.cost[i] = fminf(best_c, 1.0f);
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, seeded);
+        if ((threadIdx.x & 31) == 0 && bal) atomicAdd(d_learned, (unsigned long long)__popc(bal));
     }
-    const bool seeded = inside && learned && any_local;
-    if (inside) {
-        const size_t i = (size_t)J->off + (size_t)y * J->w + x;
-        out.nz[i] = plane;
-        out.cost[i] = fminf(best_c, 1.0f);
-    }
-    const unsigned bal = __ballot_sync(0xffffffffu, seeded);
-    if ((threadIdx.x & 31) == 0 && bal) atomicAdd(d_learned, (unsigned long long)__popc(bal));
 }
 
 // ---------------------------------------------------------------- gate
 // stereo.rs:373-393 (+ normals, an extension)
 __global__ void gate_kernel(const DevJob* __restrict__ jobs, const int32_t* __restrict__ job_start, int n_jobs,
-                            int tw, int th, float cost_thr, const uint64_t* __restrict__ census, PlaneBuf planes,
+                            float cost_thr, const uint64_t* __restrict__ census, PlaneBuf planes,
                             float* __restrict__ depth, float* __restrict__ cost, float* __restrict__ normal) {
     const int j = find_item(job_start, n_jobs, blockIdx.x);
     const DevJob* J = jobs + j;
+    const int tw = J->tw, th = J->th;
+    if ((int)threadIdx.x >= tw * th) return;
     const int t = blockIdx.x - job_start[j];
     const int x = (t % J->tiles_x) * tw + (int)threadIdx.x % tw;
     const int y = (t / J->tiles_x) * th + (int)threadIdx.x / tw;
@@ -637,18 +678,18 @@ __global__ void gate_kernel(const DevJob* __restrict__ jobs, const int32_t* __re
 }
 
 // ---------------------------------------------------------------- diagnostics
-__global__ void cost_field_kernel(const DevJob* __restrict__ jobs, const int32_t* __restrict__ job_start, int tw,
-                                  int th, const uint64_t* __restrict__ census, const float2* __restrict__ rays,
+__global__ void cost_field_kernel(const DevJob* __restrict__ jobs, const int32_t* __restrict__ job_start,
+                                  const uint64_t* __restrict__ census, const float2* __restrict__ rays,
                                   const float4* __restrict__ planes, const float* __restrict__ hints,
                                   float* __restrict__ cost_out, int32_t* __restrict__ hsum_out) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const Smem sm = carve(smem_raw, tw, th);
+    Smem sm;
     Tile T;
-    load_tile(jobs, job_start, 1, tw, th, census, rays, sm, T);
+    load_tile(jobs, job_start, 1, blockIdx.x, census, rays, smem_raw, sm, T);
     const DevJob* J = T.job;
-    const int lx = threadIdx.x % tw, ly = threadIdx.x / tw;
+    const int lx = threadIdx.x % T.tw, ly = threadIdx.x / T.tw;
     const int x = T.x0 + lx, y = T.y0 + ly;
-    if (x >= J->w || y >= J->h) return;
+    if ((int)threadIdx.x >= T.tw * T.th || x >= J->w || y >= J->h) return;
     const size_t li = (size_t)y * J->w + x;
     const float4 p = planes[li];
     WorkCount wc{0, 0};
@@ -668,91 +709,119 @@ __global__ void f2i_kernel(const float* in, int n, int32_t* out) {
 
 size_t stereo_smem_bytes(TileShape ts) { return smem_bytes(ts.tw, ts.th); }
 
-cudaError_t stereo_configure(TileShape ts) {
-    size_t sm = smem_bytes(ts.tw, ts.th);
-    cudaError_t e;
-    if ((e = cudaFuncSetAttribute(init_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) return e;
-    if ((e = cudaFuncSetAttribute(init_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) return e;
-    const void* pk[] = {(const void*)pass_kernel<false, 3>, (const void*)pass_kernel<true, 3>};
-    for (const void* k : pk)
-        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) return e;
-    if ((e = cudaFuncSetAttribute(cost_field_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) return e;
-    const void* ik[] = {(const void*)init_rows_kernel<false, 4>, (const void*)init_rows_kernel<true, 4>};
-    for (const void* k : ik)
-        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) return e;
-    return cudaSuccess;
+namespace {
+// Blocks of a persistent launch: as many as stay resident on all SMs at
+// once (the queue hands out the tiles), never more than there are tiles.
+template <typename K>
+int launch_grid(K kernel, const LaunchGeom& g) {
+    if (!g.queue) return g.tiles;
+    int dev = 0, nsm = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, g.nthr, g.smem) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return g.tiles;  // any grid size is correct with a queue
+    }
+    const long long n = (long long)std::max(per_sm, 1) * std::max(nsm, 1);
+    return (int)std::min<long long>(n, g.tiles);
 }
+}  // namespace
 
-cudaError_t launch_init(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, int total_tiles, TileShape ts,
-                        int nh, const uint64_t* census, const float2* rays, PlaneBuf out, unsigned long long* d_work,
+int stereo_resident_grid(const LaunchGeom& g) { return launch_grid(pass_kernel<false, 3, true>, g); }
+
+namespace {
+template <bool COUNT, bool PERSIST>
+void init_as(int variant, const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, const LaunchGeom& g, int nh,
+             const uint64_t* census, const float2* rays, PlaneBuf out, unsigned long long* d_work, cudaStream_t st) {
+    if (variant == 1)
+        init_kernel<COUNT, PERSIST><<<launch_grid(init_kernel<COUNT, PERSIST>, g), g.nthr, g.smem, st>>>(
+            d_jobs, d_job_start, n_jobs, g.tiles, g.queue, nh, census, rays, out, d_work);
+    else
+        init_rows_kernel<COUNT, 4, PERSIST><<<launch_grid(init_rows_kernel<COUNT, 4, PERSIST>, g), g.nthr, g.smem,
+                                              st>>>(d_jobs, d_job_start, n_jobs, g.tiles, g.queue, nh, census, rays,
+                                                    out, d_work);
+}
+template <bool COUNT, bool PERSIST>
+void pass_as(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, const LaunchGeom& g, uint64_t pass,
+             float sig_inv, float sig_n, const uint64_t* census, const float2* rays, PlaneBuf prev, PlaneBuf next,
+             unsigned long long* d_work, cudaStream_t st) {
+    pass_kernel<COUNT, 3, PERSIST><<<launch_grid(pass_kernel<COUNT, 3, PERSIST>, g), g.nthr, g.smem, st>>>(
+        d_jobs, d_job_start, n_jobs, g.tiles, g.queue, pass, sig_inv, sig_n, census, rays, prev, next, d_work);
+}
+}  // namespace
+
+cudaError_t launch_init(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, const LaunchGeom& g, int nh,
+                        const uint64_t* census, const float2* rays, PlaneBuf out, unsigned long long* d_work,
                         cudaStream_t st, int variant) {
-    if (total_tiles <= 0) return cudaSuccess;
-    const size_t sm = smem_bytes(ts.tw, ts.th);
-    const int nt = ts.tw * ts.th;
-    if (variant == 1) {
-        if (d_work)
-            init_kernel<true><<<total_tiles, nt, sm, st>>>(d_jobs, d_job_start, n_jobs, ts.tw, ts.th, nh, census, rays,
-                                                           out, d_work);
+    if (g.tiles <= 0) return cudaSuccess;
+    if (d_work) {
+        if (g.queue)
+            init_as<true, true>(variant, d_jobs, d_job_start, n_jobs, g, nh, census, rays, out, d_work, st);
         else
-            init_kernel<false><<<total_tiles, nt, sm, st>>>(d_jobs, d_job_start, n_jobs, ts.tw, ts.th, nh, census, rays,
-                                                            out, nullptr);
+            init_as<true, false>(variant, d_jobs, d_job_start, n_jobs, g, nh, census, rays, out, d_work, st);
     } else {
-        if (d_work)
-            init_rows_kernel<true, 4><<<total_tiles, nt, sm, st>>>(d_jobs, d_job_start, n_jobs, ts.tw, ts.th, nh, census,
-                                                                   rays, out, d_work);
+        if (g.queue)
+            init_as<false, true>(variant, d_jobs, d_job_start, n_jobs, g, nh, census, rays, out, nullptr, st);
         else
-            init_rows_kernel<false, 4><<<total_tiles, nt, sm, st>>>(d_jobs, d_job_start, n_jobs, ts.tw, ts.th, nh,
-                                                                    census, rays, out, nullptr);
+            init_as<false, false>(variant, d_jobs, d_job_start, n_jobs, g, nh, census, rays, out, nullptr, st);
     }
     return cudaGetLastError();
 }
 
-cudaError_t launch_pass(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, int total_tiles, TileShape ts,
+cudaError_t launch_pass(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, const LaunchGeom& g,
                         uint64_t pass, float sig_inv, float sig_n, const uint64_t* census, const float2* rays,
-                        PlaneBuf prev, PlaneBuf next, unsigned long long* d_work, cudaStream_t st, int variant) {
-    (void)variant;  // one schedule: lanes of a warp stay on the same support view (shared gathers)
-    if (total_tiles <= 0) return cudaSuccess;
-    const size_t sm = smem_bytes(ts.tw, ts.th);
-    const int nt = ts.tw * ts.th;
-    if (d_work)
-        pass_kernel<true, 3><<<total_tiles, nt, sm, st>>>(d_jobs, d_job_start, n_jobs, ts.tw, ts.th, pass, sig_inv,
-                                                          sig_n, census, rays, prev, next, d_work);
+                        PlaneBuf prev, PlaneBuf next, unsigned long long* d_work, cudaStream_t st) {
+    if (g.tiles <= 0) return cudaSuccess;
+    if (d_work) {
+        if (g.queue)
+            pass_as<true, true>(d_jobs, d_job_start, n_jobs, g, pass, sig_inv, sig_n, census, rays, prev, next, d_work,
+                                st);
+        else
+            pass_as<true, false>(d_jobs, d_job_start, n_jobs, g, pass, sig_inv, sig_n, census, rays, prev, next,
+                                 d_work, st);
+    } else {
+        if (g.queue)
+            pass_as<false, true>(d_jobs, d_job_start, n_jobs, g, pass, sig_inv, sig_n, census, rays, prev, next,
+                                 nullptr, st);
+        else
+            pass_as<false, false>(d_jobs, d_job_start, n_jobs, g, pass, sig_inv, sig_n, census, rays, prev, next,
+                                  nullptr, st);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_init_learned(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, const LaunchGeom& g,
+                                int nh, const uint64_t* census, const float2* rays, PlaneBuf out, const float* pred,
+                                const int64_t* pred_off, float conf_thr, int n_local, float span,
+                                unsigned long long* d_learned, cudaStream_t st) {
+    if (g.tiles <= 0) return cudaSuccess;
+    if (g.queue)
+        init_learned_rows_kernel<true><<<launch_grid(init_learned_rows_kernel<true>, g), g.nthr, g.smem, st>>>(
+            d_jobs, d_job_start, n_jobs, g.tiles, g.queue, nh, census, rays, out, pred, pred_off, conf_thr, n_local,
+            span, d_learned);
     else
-        pass_kernel<false, 3><<<total_tiles, nt, sm, st>>>(d_jobs, d_job_start, n_jobs, ts.tw, ts.th, pass, sig_inv,
-                                                           sig_n, census, rays, prev, next, nullptr);
+        init_learned_rows_kernel<false><<<g.tiles, g.nthr, g.smem, st>>>(d_jobs, d_job_start, n_jobs, g.tiles,
+                                                                          nullptr, nh, census, rays, out, pred,
+                                                                          pred_off, conf_thr, n_local, span,
+                                                                          d_learned);
     return cudaGetLastError();
 }
 
-cudaError_t launch_init_learned(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, int total_tiles,
-                                TileShape ts, int nh, const uint64_t* census, const float2* rays, PlaneBuf out,
-                                const float* pred, const int64_t* pred_off, float conf_thr, int n_local,
-                                float span, unsigned long long* d_learned, cudaStream_t st) {
-    if (total_tiles <= 0) return cudaSuccess;
-    const size_t sm = smem_bytes(ts.tw, ts.th);
-    cudaError_t e = cudaFuncSetAttribute(init_learned_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e) return e;
-    init_learned_rows_kernel<<<total_tiles, ts.tw * ts.th, sm, st>>>(d_jobs, d_job_start, n_jobs, ts.tw, ts.th, nh,
-                                                                     census, rays, out, pred, pred_off, conf_thr,
-                                                                     n_local, span, d_learned);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_gate(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, int total_tiles, TileShape ts,
+cudaError_t launch_gate(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, const LaunchGeom& g,
                         float cost_thr, const uint64_t* census, PlaneBuf planes, float* depth, float* cost,
                         float* normal, cudaStream_t st) {
-    if (total_tiles <= 0) return cudaSuccess;
-    gate_kernel<<<total_tiles, ts.tw * ts.th, 0, st>>>(d_jobs, d_job_start, n_jobs, ts.tw, ts.th, cost_thr, census,
-                                                       planes, depth, cost, normal);
+    if (g.tiles <= 0) return cudaSuccess;
+    gate_kernel<<<g.tiles, g.nthr, 0, st>>>(d_jobs, d_job_start, n_jobs, cost_thr, census, planes, depth, cost,
+                                            normal);
     return cudaGetLastError();
 }
 
-cudaError_t launch_cost_field(const DevJob* d_job, const int32_t* d_job_start, int total_tiles, TileShape ts,
+cudaError_t launch_cost_field(const DevJob* d_job, const int32_t* d_job_start, const LaunchGeom& g,
                               const uint64_t* census, const float2* rays, const float4* planes, const float* hints,
                               float* cost_out, int32_t* hsum_out, cudaStream_t st) {
-    if (total_tiles <= 0) return cudaSuccess;
-    size_t sm = smem_bytes(ts.tw, ts.th);
-    cost_field_kernel<<<total_tiles, ts.tw * ts.th, sm, st>>>(d_job, d_job_start, ts.tw, ts.th, census, rays, planes,
-                                                              hints, cost_out, hsum_out);
+    if (g.tiles <= 0) return cudaSuccess;
+    cost_field_kernel<<<g.tiles, g.nthr, g.smem, st>>>(d_job, d_job_start, census, rays, planes, hints, cost_out,
+                                                       hsum_out);
     return cudaGetLastError();
 }
 

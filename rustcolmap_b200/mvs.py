@@ -65,6 +65,22 @@ class Context:
         self.check(self._L.rcmvs_ctx_kernel_time(self.ptr, name.encode(), C.byref(ms), C.byref(n)))
         return ms.value, n.value
 
+    def tune_table(self):
+        """Tile shapes the autotuner chose on this context, per resolution class."""
+        buf = (_abi.TuneEntry * 64)()
+        n = C.c_int32()
+        self.check(self._L.rcmvs_tune_table(self.ptr, buf, 64, C.byref(n)))
+        return [dict(w=e.w, h=e.h, tile_w=e.tile_w, tile_h=e.tile_h, ms_best=e.ms_best, ms_default=e.ms_default)
+                for e in buf[:n.value]]
+
+    def set_tune_table(self, entries):
+        """Loads a tile-shape table (dicts as returned by tune_table)."""
+        buf = (_abi.TuneEntry * max(len(entries), 1))()
+        for i, e in enumerate(entries):
+            buf[i] = _abi.TuneEntry(e["w"], e["h"], e["tile_w"], e["tile_h"], e.get("ms_best", 0.0),
+                                    e.get("ms_default", 0.0))
+        self.check(self._L.rcmvs_tune_set(self.ptr, buf, len(entries)))
+
     def close(self):
         if getattr(self, "ptr", None):
             self._L.rcmvs_ctx_destroy(self.ptr)
@@ -222,6 +238,17 @@ def selftest_f2i(values, ctx=None):
     return out
 
 
+def _jobs_c(jobs):
+    """(ref, srcs, zmin, zmax) tuples -> rcmvs_job array (+ the arrays it points into)."""
+    cj = (_abi.Job * max(len(jobs), 1))()
+    keep = []
+    for i, (ref, srcs, zmin, zmax) in enumerate(jobs):
+        s = np.ascontiguousarray(srcs, dtype=np.int32)
+        keep.append(s)
+        cj[i] = _abi.Job(int(ref), len(s), s.ctypes.data if len(s) else None, float(zmin), float(zmax))
+    return cj, keep
+
+
 class DeviceScene:
     """Views resident in device memory (rcmvs_scene): census, rays, planes,
     depth maps and the fused cloud never leave HBM between calls."""
@@ -239,14 +266,18 @@ class DeviceScene:
         self.ctx.check(self.ctx._L.rcmvs_scene_prepare(self.ctx.ptr, self.ptr))
 
     def estimate(self, jobs, opts):
-        cj = (_abi.Job * len(jobs))()
-        keep = []
-        for i, (ref, srcs, zmin, zmax) in enumerate(jobs):
-            s = np.ascontiguousarray(srcs, dtype=np.int32)
-            keep.append(s)
-            cj[i] = _abi.Job(int(ref), len(s), s.ctypes.data if len(s) else None, float(zmin), float(zmax))
+        cj, keep = _jobs_c(jobs)
         o = opts.to_c()
         self.ctx.check(self.ctx._L.rcmvs_scene_estimate_depth(self.ctx.ptr, self.ptr, cj, len(jobs), C.byref(o)))
+
+    def autotune(self, jobs, opts):
+        """Tunes the tile shape of every resolution class of `jobs` not yet
+        tuned on this context (rcmvs_autotune); returns the context's table
+        as a list of dicts."""
+        cj, keep = _jobs_c(jobs)
+        o = opts.to_c()
+        self.ctx.check(self.ctx._L.rcmvs_autotune(self.ctx.ptr, self.ptr, cj, len(jobs), C.byref(o)))
+        return self.ctx.tune_table()
 
     def fuse(self, fusion_order, sparse_xyz, opts):
         off, flat = _csr(fusion_order)

@@ -12,6 +12,14 @@ import numpy as np
 
 from . import _abi
 
+# RCMVS_FLAG_* bits of MvsOptions.flags (include/rcmvs.h); all of them leave
+# the results bit-identical.
+FLAG_ONE_CANDIDATE = 1  # one-candidate-at-a-time init schedule
+FLAG_PERSISTENT = 2     # persistent (view, tile) work-queue launches
+FLAG_CUDA_GRAPH = 4     # replay the init/pass/gate schedule from a CUDA graph
+FLAG_AUTOTUNE = 8       # per-resolution-class tile shapes from the autotuner
+FLAGS_BATCHED = FLAG_PERSISTENT | FLAG_CUDA_GRAPH | FLAG_AUTOTUNE
+
 
 @dataclass
 class MvsOptions:
