@@ -274,6 +274,9 @@ def main():
     ap.add_argument("--local-hyps", type=int, default=None)
     ap.add_argument("--local-span", type=float, default=None)
     ap.add_argument("--conf", type=float, default=None)
+    ap.add_argument("--flags", type=int, default=0,
+                    help="RCMVS_FLAG_* bits for both arms (2 persistent queue, 4 CUDA graph, 8 autotuned tiles)")
+    ap.add_argument("--tile", default="", help="WxH stereo tile (default: the library's 8x8)")
     args = ap.parse_args()
     assert args.warmup >= 3 or os.environ.get("RCMVS_BENCH_ALLOW_SHORT"), "warm-up must be >= 3 steps"
     cfg = configs()[args.config]
@@ -294,6 +297,9 @@ def main():
     opts = cfg["opts"]
     if args.one_candidate:
         opts.flags |= 1
+    opts.flags |= args.flags
+    if args.tile:
+        opts.tile_w, opts.tile_h = map(int, args.tile.lower().split("x"))
     lopts = dataclasses.replace(opts, sweeps=2)
     t_setup = time.perf_counter()
     sc = make_scene(cfg, seed=5 + 1000 * rank, device=local)
@@ -467,6 +473,10 @@ def main():
             "fused_points": head_pts,
             "setup_s": setup_s,
             "kernels": "one-candidate init" if opts.flags & 1 else "row-step init",
+            "schedule": {"tile": f"{opts.tile_w}x{opts.tile_h}" if opts.tile_w else "8x8 (library default)",
+                         "flags": opts.flags,
+                         "persistent_queue": bool(opts.flags & 2), "cuda_graph": bool(opts.flags & 4),
+                         "autotuned_tiles": bool(opts.flags & 8), "tune_table": ctx.tune_table()},
         }
         print(json.dumps(line), flush=True)
     if net is not None:

@@ -58,8 +58,8 @@ typedef struct rcmvs_options {
     double reproj_px;        /* >0: fusion also requires the forward-backward
                                 reprojection error to be <= reproj_px pixels;
                                 0 = off (reference behaviour) */
-    uint32_t tile_w;         /* stereo tile width in pixels; 0 = tuned default */
-    uint32_t tile_h;         /* stereo tile height in pixels; 0 = tuned default */
+    uint32_t tile_w;         /* stereo tile width in pixels; 0 = default (8) */
+    uint32_t tile_h;         /* stereo tile height in pixels; 0 = default (8) */
     uint32_t flags;          /* RCMVS_FLAG_* bits; 0 = defaults */
     uint32_t reserved1;
 } rcmvs_options;
@@ -246,19 +246,20 @@ int rcmvs_scene_estimate_depth(rcmvs_ctx* ctx, rcmvs_scene* scene, const rcmvs_j
 
 /* Tile-shape autotuner (no reference counterpart).  Reference views are
  * grouped into resolution classes by (w, h).  For every class of the given
- * jobs that this context has not tuned yet, a trial (plane-sweep init + one
- * pass, with opts, on the class's first jobs up to about 1 Mpx) is timed
- * with CUDA events for each candidate shape: 16x16, 32x8, 8x32, 64x4 (256
- * threads), 16x8, 8x16, 32x4 (128) and 8x8 (64).  One thread count is kept
- * for all classes of a context (the one with the least summed best time at
- * the first tuning), and each class gets its fastest shape of that count.
- * The trial overwrites the jobs' plane buffers, not their depth maps.
- * Synchronous. */
+ * jobs that this context has not tuned yet, the plane-sweep init and one
+ * pass (with opts, on the class's first jobs up to about 1 Mpx) are timed
+ * with CUDA events for each candidate shape and scored as init +
+ * 2*max(sweeps,1) passes.  Candidates: 8x8, 16x4, 4x16 (64 threads), 16x16,
+ * 32x8, 8x32, 64x4 (256), 16x8, 8x16, 32x4 (128) and 8x4, 4x8, 16x2 (32, one
+ * warp per block).  One thread count is kept for all classes of a context
+ * (the one with the least summed best score at the first tuning), and each
+ * class gets its best shape of that count.  The trial overwrites the jobs'
+ * plane buffers, not their depth maps.  Synchronous. */
 typedef struct rcmvs_tune_entry {
     int32_t w, h;            /* resolution class */
     int32_t tile_w, tile_h;  /* chosen shape */
-    float ms_best;           /* trial time of the chosen shape */
-    float ms_default;        /* trial time of the 16x16 default */
+    float ms_best;           /* trial score of the chosen shape (ms) */
+    float ms_default;        /* trial score of the 8x8 default (ms) */
 } rcmvs_tune_entry;
 int rcmvs_autotune(rcmvs_ctx* ctx, rcmvs_scene* scene, const rcmvs_job* jobs, int32_t n_jobs,
                    const rcmvs_options* opts);

@@ -2,7 +2,7 @@
 // scene (the per-view `estimate_depth` calls of mvs/src/lib.rs:345-370) in
 // one launch per step.
 //
-//   * tile shapes per job: fixed (opts tile_w x tile_h, default 16x16) or
+//   * tile shapes per job: fixed (opts tile_w x tile_h, default 8x8) or
 //     picked per resolution class by the autotuner (rcmvs_autotune);
 //   * job order: longest tiles first (pixels per tile x support views), so
 //     the blocks of the costliest jobs start first and the short ones fill
@@ -47,9 +47,13 @@ bool shape_ok(TileShape ts) {
            stereo_smem_bytes(ts) <= 48 * 1024;
 }
 
+// Default tile: 8x8 measured fastest among the fixed shapes at 960x720 (K 8),
+// 1920x1080 (K 10) and mixed batches (K 4-12) on B200, 4-7% ahead of 16x16:
+// a block holds its SM slot until its slowest warp (the one with the fewest
+// early aborts) is done, and smaller blocks release it sooner.
 TileShape fixed_shape(const rcmvs_options* o) {
     if (o && o->tile_w > 0 && o->tile_h > 0) return TileShape{(int)o->tile_w, (int)o->tile_h};
-    return TileShape{16, 16};
+    return TileShape{8, 8};
 }
 
 const rcmvs_tune_entry* find_class(const rcmvs_ctx* ctx, int w, int h) {
@@ -59,8 +63,10 @@ const rcmvs_tune_entry* find_class(const rcmvs_ctx* ctx, int w, int h) {
 }
 
 // Candidate shapes of the autotuner (pixels per tile <= 256, the block size
-// the stereo kernels are compiled for).
-const TileShape kCandidates[] = {{16, 16}, {32, 8}, {8, 32}, {64, 4}, {16, 8}, {8, 16}, {32, 4}, {8, 8}};
+// the stereo kernels are compiled for); the first one is the default.
+// Smaller blocks cost more halo loads per pixel but free their slot sooner.
+const TileShape kCandidates[] = {{8, 8},  {16, 4}, {4, 16}, {16, 16}, {32, 8}, {8, 32}, {64, 4},
+                                 {16, 8}, {8, 16}, {32, 4}, {8, 4},   {4, 8},  {16, 2}};
 constexpr int kNumCandidates = sizeof(kCandidates) / sizeof(kCandidates[0]);
 
 // Fills b for jobs with shapes shp (caller's order), then sorts launch order.
@@ -94,10 +100,10 @@ int assemble(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job* jobs, int n_jobs,
     return RCMVS_OK;
 }
 
-// Plane-sweep init + one pass over jobs with every job at shape ts; returns
-// the device time in ms.
+// Plane-sweep init and one pass over jobs with every job at shape ts, timed
+// separately; *ms = the schedule's estimate, init + 2*max(sweeps,1) passes.
 int trial(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job* jobs, int n_jobs, const rcmvs_options* opts, TileShape ts,
-          cudaEvent_t e0, cudaEvent_t e1, float* ms) {
+          cudaEvent_t e0, cudaEvent_t e1, cudaEvent_t e2, float* ms) {
     StereoBatch b;
     std::vector<TileShape> shp(n_jobs, ts);
     int rc = assemble(ctx, sc, jobs, n_jobs, shp, false, b);
@@ -115,11 +121,15 @@ int trial(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job* jobs, int n_jobs, co
     PlaneBuf A{sc->plane_a, sc->pcost_a}, B{sc->plane_b, sc->pcost_b};
     SCK(cudaEventRecord(e0, st));
     SCK(launch_init(dj, dst, n_jobs, b.geom, nh, sc->census, sc->rays, A, nullptr, st, variant));
+    SCK(cudaEventRecord(e1, st));
     const float sig_inv = 0.02f * powf_host(0.28f, 0.0f), sig_n = 0.30f * powf_host(0.42f, 0.0f);
     SCK(launch_pass(dj, dst, n_jobs, b.geom, 0, sig_inv, sig_n, sc->census, sc->rays, A, B, nullptr, st));
-    SCK(cudaEventRecord(e1, st));
-    SCK(cudaEventSynchronize(e1));
-    SCK(cudaEventElapsedTime(ms, e0, e1));
+    SCK(cudaEventRecord(e2, st));
+    SCK(cudaEventSynchronize(e2));
+    float t_init = 0.f, t_pass = 0.f;
+    SCK(cudaEventElapsedTime(&t_init, e0, e1));
+    SCK(cudaEventElapsedTime(&t_pass, e1, e2));
+    *ms = t_init + 2.0f * (float)std::max<uint32_t>(opts->sweeps, 1u) * t_pass;
     return RCMVS_OK;
 }
 
@@ -149,33 +159,34 @@ int tune_missing(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job* jobs, int n_j
         }
     }
     if (cls.empty()) return RCMVS_OK;
-    cudaEvent_t e0, e1;
-    SCK(cudaEventCreate(&e0));
-    if (cudaEventCreate(&e1) != cudaSuccess) {
-        cudaEventDestroy(e0);
-        return sfail(ctx, RCMVS_E_CUDA, "cudaEventCreate failed");
-    }
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    for (auto& e : ev)
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            for (auto& f : ev)
+                if (f) cudaEventDestroy(f);
+            return sfail(ctx, RCMVS_E_CUDA, "cudaEventCreate failed");
+        }
     int rc = RCMVS_OK;
     for (auto& c : cls) {
         float warm = 0.f;  // first launch of a class pays for cold caches
-        rc = trial(ctx, sc, c.jobs.data(), (int)c.jobs.size(), opts, kCandidates[0], e0, e1, &warm);
+        rc = trial(ctx, sc, c.jobs.data(), (int)c.jobs.size(), opts, kCandidates[0], ev[0], ev[1], ev[2], &warm);
         for (int k = 0; k < kNumCandidates && rc == RCMVS_OK; ++k) {
             float best = INFINITY;
             for (int rep = 0; rep < 2 && rc == RCMVS_OK; ++rep) {
                 float ms = 0.f;
-                rc = trial(ctx, sc, c.jobs.data(), (int)c.jobs.size(), opts, kCandidates[k], e0, e1, &ms);
+                rc = trial(ctx, sc, c.jobs.data(), (int)c.jobs.size(), opts, kCandidates[k], ev[0], ev[1], ev[2],
+                           &ms);
                 best = std::min(best, ms);
             }
             c.ms[k] = best;
         }
         if (rc) break;
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    for (auto& e : ev) cudaEventDestroy(e);
     if (rc) return rc;
     if (ctx->tune_nthr == 0) {  // the thread count with the least summed best time
         double best_sum = INFINITY;
-        for (int nthr : {256, 128, 64}) {
+        for (int nthr : {64, 256, 128, 32}) {
             double sum = 0;
             for (const auto& c : cls) {
                 float m = INFINITY;

@@ -80,6 +80,8 @@ def test_graph_replay_and_recapture(uneven):
     # different pixel counts in one launch: blocks of 256 threads, the 8x8
     # and 32x4 tiles leave threads idle
     {(96, 72): (8, 8), (128, 72): (16, 16), (64, 48): (32, 4)},
+    # one warp per tile
+    {(96, 72): (8, 4), (128, 72): (4, 8), (64, 48): (16, 2)},
 ])
 @pytest.mark.parametrize("persistent", [False, True])
 def test_per_class_tile_shapes_in_one_launch(uneven, table, persistent):
@@ -106,9 +108,9 @@ def test_autotuner_table_and_results(uneven):
     classes = {(sc.views[r].w, sc.views[r].h) for (r, _, _, _) in jobs}
     assert {(e["w"], e["h"]) for e in tab} == classes
     npx = {e["tile_w"] * e["tile_h"] for e in tab}
-    assert len(npx) == 1 and npx.pop() in (64, 128, 256)
+    assert len(npx) == 1 and npx.pop() in (32, 64, 128, 256)
     for e in tab:
-        assert 0 < e["ms_best"] <= e["ms_default"] or e["tile_w"] * e["tile_h"] != 256
+        assert 0 < e["ms_best"] <= e["ms_default"] or e["tile_w"] * e["tile_h"] != 64
     # explicit call on known classes changes nothing
     assert ds.autotune(jobs, opts) == tab
     with pytest.raises(mvs.RcmvsError):
