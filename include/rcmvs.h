@@ -89,6 +89,14 @@ typedef struct rcmvs_options {
  * first.  Overrides tile_w/tile_h.  Same results bit for bit. */
 #define RCMVS_FLAG_AUTOTUNE 8u
 
+/* Evaluate every propagation candidate, as the reference does.  By default
+ * a Jacobi pass skips a neighbour's plane that is bit for bit the plane
+ * (normal and offset d) the pixel's stored cost was computed with: its cost
+ * would be that same cost, or an early abort, and never lower, so it can
+ * not be accepted.  Skipping changes no output bit, only the work counters
+ * (rcmvs_last_work), which with this flag count the reference's calls. */
+#define RCMVS_FLAG_NO_SKIP_DUPLICATES 16u
+
 /* Fills `MvsOptions::default()` (mvs/src/lib.rs:56-70); extensions off. */
 void rcmvs_options_default(rcmvs_options* opts);
 

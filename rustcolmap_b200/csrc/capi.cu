@@ -198,6 +198,7 @@ void rcmvs_scene_destroy(rcmvs_scene* sc) {
         cudaStreamSynchronize(sc->ctx->stream);
     }
     void* ps[] = {sc->gray, sc->rgb, sc->census, sc->rays, sc->plane_a, sc->plane_b, sc->pcost_a, sc->pcost_b,
+                  sc->pd_a, sc->pd_b,
                   sc->depth, sc->cost, sc->normal, sc->d_views, sc->d_tile_start, sc->d_cams,
                   sc->gray_q, sc->census_q, sc->rays_q, sc->d_qviews, sc->d_qtile_start, sc->d_qcams,
                   sc->d_qblk_start};
@@ -256,6 +257,8 @@ int rcmvs_scene_create(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views,
     if (!e) e = alloc((void**)&sc->plane_b, 16 * np);
     if (!e) e = alloc((void**)&sc->pcost_a, 4 * np);
     if (!e) e = alloc((void**)&sc->pcost_b, 4 * np);
+    if (!e) e = alloc((void**)&sc->pd_a, 4 * np);
+    if (!e) e = alloc((void**)&sc->pd_b, 4 * np);
     if (!e) e = alloc((void**)&sc->depth, 4 * np);
     if (!e) e = alloc((void**)&sc->cost, 4 * np);
     if (!e) e = alloc((void**)&sc->normal, 12 * np);
@@ -318,7 +321,7 @@ int rcmvs_scene_estimate_depth(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job*
             return fail(ctx, RCMVS_E_ARG, "reference view long side exceeds max_dim");
     }
     constexpr uint32_t kFlags = RCMVS_FLAG_ONE_CANDIDATE | RCMVS_FLAG_PERSISTENT | RCMVS_FLAG_CUDA_GRAPH |
-                                RCMVS_FLAG_AUTOTUNE;
+                                RCMVS_FLAG_AUTOTUNE | RCMVS_FLAG_NO_SKIP_DUPLICATES;
     if (opts->flags & ~kFlags) return fail(ctx, RCMVS_E_ARG, "unknown bits in opts->flags");
     if (n_jobs == 0) return RCMVS_OK;
     CK(cudaSetDevice(ctx->device));
@@ -335,6 +338,7 @@ int rcmvs_scene_estimate_depth(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job*
     s.cost_thr = opts->cost_thr;
     s.persistent = (opts->flags & RCMVS_FLAG_PERSISTENT) != 0;
     s.graph = (opts->flags & RCMVS_FLAG_CUDA_GRAPH) != 0;
+    s.skip_duplicates = !(opts->flags & RCMVS_FLAG_NO_SKIP_DUPLICATES);
     s.d_work = dw;
     rc = run_batch(ctx, sc, batch, s);
     if (rc) return rc;

@@ -86,6 +86,8 @@ struct rcmvs_scene {
     float4* plane_b = nullptr;
     float* pcost_a = nullptr;
     float* pcost_b = nullptr;
+    float* pd_a = nullptr;  // plane offsets d (PlaneBuf::d)
+    float* pd_b = nullptr;
     float* depth = nullptr;
     float* cost = nullptr;
     float* normal = nullptr;
@@ -146,6 +148,7 @@ struct Schedule {
     float cost_thr = 0.38f;
     bool persistent = false;
     bool graph = false;
+    bool skip_duplicates = true;  // PlaneBuf::d on: skip repeated propagation candidates
     unsigned long long* d_work = nullptr;  // work counters (zeroed by the caller)
     // learned init
     const float* pred = nullptr;

@@ -489,6 +489,7 @@ int rcmvs_scene_estimate_depth_learned(rcmvs_ctx* ctx, rcmvs_scene* sc, const rc
     sched.cost_thr = opts->cost_thr;
     sched.persistent = (opts->flags & RCMVS_FLAG_PERSISTENT) != 0;
     sched.graph = (opts->flags & RCMVS_FLAG_CUDA_GRAPH) != 0;
+    sched.skip_duplicates = !(opts->flags & RCMVS_FLAG_NO_SKIP_DUPLICATES);
     sched.pred = (const float*)pred;
     sched.pred_off = (const int64_t*)ppo;
     sched.conf_thr = conf_thr;

@@ -47,10 +47,14 @@ struct DevJob {
 static_assert(sizeof(DevJob) % 8 == 0, "DevJob layout");
 
 // Plane of mvs/src/stereo.rs:24-31, split for 16-byte loads:
-// float4 (nx, ny, nz, z) + float cost.
+// float4 (nx, ny, nz, z) + float cost.  `d` (nullable) keeps, per pixel, the
+// plane offset d the stored cost was computed with (z = d / (n . ray)); with
+// it the pass kernel skips a propagation candidate that repeats the pixel's
+// own plane bit for bit (see pass_kernel).
 struct PlaneBuf {
     float4* nz;   // (nx, ny, nz, z)
     float* cost;
+    float* d = nullptr;
 };
 
 // Tile shape of one job's stereo launch (pixels per block = tw * th).

@@ -118,7 +118,9 @@ int trial(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job* jobs, int n_jobs, co
     const int32_t* dst = (const int32_t*)ps;
     const int nh = (int)std::max<uint32_t>(opts->num_hyp, 2u);
     const int variant = (opts->flags & RCMVS_FLAG_ONE_CANDIDATE) ? 1 : 0;
-    PlaneBuf A{sc->plane_a, sc->pcost_a}, B{sc->plane_b, sc->pcost_b};
+    const bool skip_dup = !(opts->flags & RCMVS_FLAG_NO_SKIP_DUPLICATES);
+    PlaneBuf A{sc->plane_a, sc->pcost_a, skip_dup ? sc->pd_a : nullptr};
+    PlaneBuf B{sc->plane_b, sc->pcost_b, skip_dup ? sc->pd_b : nullptr};
     SCK(cudaEventRecord(e0, st));
     SCK(launch_init(dj, dst, n_jobs, b.geom, nh, sc->census, sc->rays, A, nullptr, st, variant));
     SCK(cudaEventRecord(e1, st));
@@ -310,7 +312,8 @@ int run_batch(rcmvs_ctx* ctx, rcmvs_scene* sc, const StereoBatch& b, const Sched
     const DevJob* dj = (const DevJob*)pj;
     const int32_t* dst = (const int32_t*)ps;
     unsigned int* queue = (unsigned int*)pq;
-    PlaneBuf A0{sc->plane_a, sc->pcost_a}, B0{sc->plane_b, sc->pcost_b};
+    PlaneBuf A0{sc->plane_a, sc->pcost_a, s.skip_duplicates ? sc->pd_a : nullptr};
+    PlaneBuf B0{sc->plane_b, sc->pcost_b, s.skip_duplicates ? sc->pd_b : nullptr};
     std::vector<float> sig(2 * s.n_passes);
     for (uint64_t pass = 0; pass < s.n_passes; ++pass) {
         const float t = (float)pass / (float)s.n_passes;  // stereo.rs:275-277
@@ -372,7 +375,8 @@ int run_batch(rcmvs_ctx* ctx, rcmvs_scene* sc, const StereoBatch& b, const Sched
     append(key, s.n_local);
     append(key, s.span);
     const void* ptrs[] = {pj, ps, pq, s.d_work, s.pred, s.pred_off, s.d_learned, sc->census, sc->rays,
-                          sc->plane_a, sc->plane_b, sc->pcost_a, sc->pcost_b, sc->depth, sc->cost, sc->normal};
+                          sc->plane_a, sc->plane_b, sc->pcost_a, sc->pcost_b, A0.d, B0.d, sc->depth, sc->cost,
+                          sc->normal};
     append(key, ptrs, sizeof(ptrs));
     if (!sc->graph || key != sc->graph_key) {
         drop_graph(sc);

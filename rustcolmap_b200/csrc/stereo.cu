@@ -311,6 +311,7 @@ __global__ void init_kernel(const DevJob* __restrict__ jobs, const int32_t* __re
             const size_t i = (size_t)J->off + (size_t)y * J->w + x;
             out.nz[i] = make_float4(0.0f, 0.0f, 1.0f, best_d);
             out.cost[i] = fminf(best_c, 1.0f);
+            if (out.d) out.d[i] = best_d;  // n = (0,0,1): d = z
         }
     }
     if (COUNT) flush_work(wc, d_work);
@@ -320,6 +321,14 @@ __global__ void init_kernel(const DevJob* __restrict__ jobs, const int32_t* __re
 // stereo.rs:274-371: one double-buffered pass.  Reads `prev` only, writes
 // every pixel of `next` (the carried-over plane when nothing is accepted,
 // which equals the reference's copy_from_slice at :278).
+// Duplicate skip (with PlaneBuf::d): a neighbour's candidate whose normal
+// and offset d equal, bit for bit, the plane the pixel's stored cost came
+// from is not evaluated.  plane_cost is a function of the pixel, (n, d) and
+// the hint alone, so that call would return the stored cost c (or 1e9 on an
+// early abort); best_c starts at min(c, 1) <= c and only falls, so
+// `c < best_c` could not hold and the result is unchanged.  In converged
+// regions most propagated planes are such repeats, and they are the costly
+// calls: with c near best_c they rarely abort.
 // MINB = 3 blocks of 256 per SM (<= 80 registers) measured fastest; 4 (64
 // registers) spills and loses.
 template <bool COUNT, int MINB, bool PERSIST>
@@ -352,6 +361,11 @@ __global__ void __launch_bounds__(256, MINB)
             uint64_t seed = pixel_rng(x, y, pass + 7);
             const float4 cur = prev.nz[i];
             const float cur_cost = prev.cost[i];
+            // the offset d that cur_cost was computed with (PlaneBuf::d); a
+            // propagated plane equal to (cur.n, cur_d) bit for bit would cost
+            // exactly cur_cost or abort, never less, and is skipped
+            const bool skip_dup = prev.d != nullptr;
+            const float cur_d = skip_dup ? prev.d[i] : 0.f;
             float best_c = cur_cost;
             float bn0 = cur.x, bn1 = cur.y, bn2 = cur.z;
             float bd = cur.w * (bn0 * ri.x + bn1 * ri.y + bn2);
@@ -372,6 +386,10 @@ __global__ void __launch_bounds__(256, MINB)
                 if (a_here < 0.1f) continue;
                 const float zcand = d_plane / a_here;
                 if (!(zlo <= zcand && zcand <= zhi)) continue;
+                if (skip_dup && __float_as_uint(d_plane) == __float_as_uint(cur_d) &&
+                    __float_as_uint(nb.x) == __float_as_uint(cur.x) && __float_as_uint(nb.y) == __float_as_uint(cur.y) &&
+                    __float_as_uint(nb.z) == __float_as_uint(cur.z))
+                    continue;
                 const float c = plane_cost<false, COUNT, false>(sm, stw, lx, ly, nsrc, census, nb.x, nb.y, nb.z,
                                                                       d_plane, best_c + 0.02f, total, wc, nullptr);
                 if (c < best_c) {
@@ -414,16 +432,18 @@ __global__ void __launch_bounds__(256, MINB)
             }
 
             float4 o = cur;
-            float oc = cur_cost;
+            float oc = cur_cost, od = cur_d;
             if (best_c < cur_cost) {  // stereo.rs:355-367
                 const float a_here = bn0 * ri.x + bn1 * ri.y + bn2;
                 if (a_here > 0.05f) {
                     o = make_float4(bn0, bn1, bn2, bd / a_here);
                     oc = fminf(best_c, 1.0f);
+                    od = bd;
                 }
             }
             next.nz[i] = o;
             next.cost[i] = oc;
+            if (skip_dup) next.d[i] = od;
         }
     }
     if (COUNT) flush_work(wc, d_work);
@@ -505,6 +525,7 @@ __global__ void __launch_bounds__(256, MINB)
             const size_t i = (size_t)J->off + (size_t)y * J->w + x;
             out.nz[i] = make_float4(0.0f, 0.0f, 1.0f, best_d);
             out.cost[i] = fminf(best_c, 1.0f);
+            if (out.d) out.d[i] = best_d;  // n = (0,0,1): d = z
         }
     }
     if (COUNT) flush_work(wc, d_work);
@@ -610,6 +631,7 @@ __global__ void __launch_bounds__(256, 3)
         };
         float best_c = INFINITY;
         float4 plane = make_float4(0.0f, 0.0f, 1.0f, 0.0f);
+        float plane_d = 0.f;
         bool live = inside && next();
         int si = 0, dy = 0;
         float sum = 0.f, thr = INFINITY;
@@ -627,6 +649,7 @@ __global__ void __launch_bounds__(256, 3)
                 if (c < best_c) {
                     best_c = c;
                     plane = make_float4(cnx, cny, cnz, cz);
+                    plane_d = cd;
                 }
                 live = next();
                 sum = 0.f;
@@ -643,6 +666,7 @@ __global__ void __launch_bounds__(256, 3)
             const size_t i = (size_t)J->off + (size_t)y * J->w + x;
             out.nz[i] = plane;
             out.cost[i] = fminf(best_c, 1.0f);
+            if (out.d) out.d[i] = plane_d;
         }
         const unsigned bal = __ballot_sync(0xffffffffu, seeded);
         if ((threadIdx.x & 31) == 0 && bal) atomicAdd(d_learned, (unsigned long long)__popc(bal));

@@ -18,6 +18,7 @@ FLAG_ONE_CANDIDATE = 1  # one-candidate-at-a-time init schedule
 FLAG_PERSISTENT = 2     # persistent (view, tile) work-queue launches
 FLAG_CUDA_GRAPH = 4     # replay the init/pass/gate schedule from a CUDA graph
 FLAG_AUTOTUNE = 8       # per-resolution-class tile shapes from the autotuner
+FLAG_NO_SKIP_DUPLICATES = 16  # evaluate repeated propagation candidates too (reference call counts)
 FLAGS_BATCHED = FLAG_PERSISTENT | FLAG_CUDA_GRAPH | FLAG_AUTOTUNE
 
 

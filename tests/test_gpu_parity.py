@@ -287,8 +287,9 @@ def test_fusion_saturated_projection_matches_oracle(ctx):
 @pytest.mark.parametrize("ref", [1, 6])
 def test_row_step_and_one_candidate_kernels_agree(ctx, corner_scene, c1_opts, ref):
     """The default row-step schedule and the one-candidate-at-a-time kernels
-    (RCMVS_FLAG_ONE_CANDIDATE) give the same bits, and the work counters
-    agree with the oracle's plane_cost call and row counts."""
+    (RCMVS_FLAG_ONE_CANDIDATE) give the same bits, and with the duplicate
+    skip off (RCMVS_FLAG_NO_SKIP_DUPLICATES) the work counters agree with the
+    oracle's plane_cost call and row counts."""
     import dataclasses
     import os
     v = corner_scene.views
@@ -302,9 +303,38 @@ def test_row_step_and_one_candidate_kernels_agree(ctx, corner_scene, c1_opts, re
     cctx = mvs.Context(0)
     del os.environ["RCMVS_COUNT"]
     _, _, _, work = oracle.estimate_depth(v, ref, srcs[ref], zr[ref, 0], zr[ref, 1], c1_opts)
-    for o in (c1_opts, one):
+    for o in (dataclasses.replace(c1_opts, flags=16), dataclasses.replace(c1_opts, flags=1 | 16)):
         ds = mvs.DeviceScene(v, cctx)
         ds.estimate([(ref, srcs[ref], zr[ref, 0], zr[ref, 1])], o)
         assert cctx.last_work() == work
         ds.close()
     cctx.close()
+
+
+@pytest.mark.parametrize("ref", [2, 5])
+def test_duplicate_skip_keeps_bits_and_saves_rows(ctx, corner_scene, c1_opts, ref):
+    """Skipping propagated planes that repeat the pixel's own plane bit for
+    bit (the default) gives the oracle's bits with fewer window rows than
+    the reference's call sequence (RCMVS_FLAG_NO_SKIP_DUPLICATES)."""
+    import dataclasses
+    import os
+    v = corner_scene.views
+    srcs, zr, _ = mvs.plan(corner_scene.sparse, v, c1_opts)
+    job = (ref, srcs[ref], zr[ref, 0], zr[ref, 1])
+    d, c, n, (evals_ref, rows_ref) = oracle.estimate_depth(v, *job, c1_opts)
+    os.environ["RCMVS_COUNT"] = "1"
+    cctx = mvs.Context(0)
+    del os.environ["RCMVS_COUNT"]
+    counts = {}
+    for flags in (0, 16, 1, 2 | 4):
+        ds = mvs.DeviceScene(v, cctx)
+        ds.estimate([job], dataclasses.replace(c1_opts, flags=flags))
+        dm = ds.depth(ref, normals=True)
+        for got, want in ((dm.depth, d), (dm.cost, c), (dm.normal, n)):
+            assert_bits_equal(got, want, f"flags {flags}")
+        counts[flags] = cctx.last_work()
+        ds.close()
+    cctx.close()
+    assert counts[16] == (evals_ref, rows_ref)
+    assert counts[0] == counts[1] == counts[2 | 4]
+    assert counts[0][1] < 0.9 * rows_ref, (counts[0], rows_ref)
