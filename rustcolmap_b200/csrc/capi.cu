@@ -73,6 +73,8 @@ bool finite(double x) { return std::isfinite(x); }
 int check_view(rcmvs_ctx* ctx, const rcmvs_view& v, int i, const rcmvs_options* opts) {
     if (v.w <= 0 || v.h <= 0 || !v.gray)
         return fail(ctx, RCMVS_E_ARG, "view " + std::to_string(i) + ": bad size or null gray");
+    if (v.w > (1 << 23) || v.h > (1 << 23))  // the stereo kernels' exact index arithmetic
+        return fail(ctx, RCMVS_E_LIMIT, "view " + std::to_string(i) + ": a side longer than 2^23 pixels");
     if (!(finite(v.f) && v.f != 0.0 && finite(v.cx) && finite(v.cy) && finite(v.k)))
         return fail(ctx, RCMVS_E_ARG, "view " + std::to_string(i) + ": non-finite or zero intrinsics");
     for (int q = 0; q < 9; ++q)

@@ -164,6 +164,7 @@ struct WorkCount {
 struct SrcRegs {
     float rs0, rs1, rs2, rs3, rs4, rs5, rs6, rs7, rs8, ts0, ts1, ts2, f, cx, cy, k;
     int sw, sh;
+    float swf, shf;  // sw, sh as floats (exact: sizes < 2^23)
     const uint64_t* __restrict__ sc;
 };
 
@@ -187,8 +188,22 @@ __device__ __forceinline__ SrcRegs load_src(const DevSrc& s, const uint64_t* __r
     r.k = s.k;
     r.sw = s.w;
     r.sh = s.h;
+    r.swf = (float)s.w;
+    r.shf = (float)s.h;
     r.sc = census + s.off;
     return r;
+}
+
+// Rust's `x as i32` (truncation toward zero, saturating, NaN -> 0) followed
+// by the test 0 <= i < n (stereo.rs:204-210), without a conversion
+// instruction: trunc(x) lies in [0, n) exactly when x > -1 and x < n, NaN
+// included (it converts to 0).  The index is trunc(max(x, 0)), formed
+// exactly by adding 2^23 with rounding toward zero (valid for x < n <= 2^23,
+// where the sum's spacing is 1) and reading the integer off the mantissa.
+// `nf` is n as a float.
+__device__ __forceinline__ bool trunc_index(float x, float nf, int& i) {
+    i = __float_as_int(__fadd_rz(fmaxf(x, 0.0f), 8388608.0f)) - 0x4B000000;
+    return !(x <= -1.0f) && !(x >= nf);
 }
 
 // The five window terms of one row of one support view (stereo.rs:181-214),
@@ -199,36 +214,37 @@ __device__ __forceinline__ SrcRegs load_src(const DevSrc& s, const uint64_t* __r
 template <bool FRONTO, bool HSUM>
 __device__ __forceinline__ float cost_row(const Smem& sm, int row, const SrcRegs& s, float nx, float ny, float nz,
                                           float d, float sum, int32_t& hs) {
+    // Branch-free: every term's geometry is computed (a skipped term's
+    // values are discarded), the gather reads a safe address when the term
+    // is out, and the five h values are then added in dx order -- the same
+    // f32 chain as the reference's, with the five terms free to overlap.
+    int h[5];
 #pragma unroll
     for (int dx = 0; dx < 5; ++dx) {
         const float2 r = sm.ray[row + dx];
-        float term = 1.0f;
-        int32_t hterm = 48;
         const float denom = FRONTO ? 1.0f : nx * r.x + ny * r.y + nz;
-        if (!(denom < 0.05f)) {
-            const float z = FRONTO ? d : d / denom;
-            const float xr = z * r.x;
-            const float yr = z * r.y;
-            const float xs = s.rs0 * xr + s.rs1 * yr + s.rs2 * z + s.ts0;
-            const float ys = s.rs3 * xr + s.rs4 * yr + s.rs5 * z + s.ts1;
-            const float zs = s.rs6 * xr + s.rs7 * yr + s.rs8 * z + s.ts2;
-            if (!(zs < 1e-3f)) {
-                const float xn = xs / zs;
-                const float yn = ys / zs;
-                const float dist = 1.0f + s.k * (xn * xn + yn * yn);
-                // `as i32`: truncation, saturating, NaN -> 0 (cvt.rzi)
-                const int u = __float2int_rz(s.f * xn * dist + s.cx);
-                const int v = __float2int_rz(s.f * yn * dist + s.cy);
-                if (u >= 0 && v >= 0 && u < s.sw && v < s.sh) {
-                    const uint64_t cs = __ldg(s.sc + (size_t)v * s.sw + u);
-                    const int h = __popcll(sm.cen[row + dx] ^ cs);
-                    term = sm.tab[h];
-                    hterm = h;
-                }
-            }
-        }
-        sum += term;
-        if (HSUM) hs += hterm;
+        const float z = FRONTO ? d : d / denom;
+        const float xr = z * r.x;
+        const float yr = z * r.y;
+        const float xs = s.rs0 * xr + s.rs1 * yr + s.rs2 * z + s.ts0;
+        const float ys = s.rs3 * xr + s.rs4 * yr + s.rs5 * z + s.ts1;
+        const float zs = s.rs6 * xr + s.rs7 * yr + s.rs8 * z + s.ts2;
+        const float xn = xs / zs;
+        const float yn = ys / zs;
+        const float dist = 1.0f + s.k * (xn * xn + yn * yn);
+        int u, v;
+        const bool in_u = trunc_index(s.f * xn * dist + s.cx, s.swf, u);
+        const bool in_v = trunc_index(s.f * yn * dist + s.cy, s.shf, v);
+        // stereo.rs:187-191 (denom), :196-201 (zs), :202-210 (bounds)
+        const bool ok = !(denom < 0.05f) && !(zs < 1e-3f) && in_u && in_v;
+        const uint64_t cs = __ldg(s.sc + (ok ? (size_t)v * s.sw + u : (size_t)0));
+        const int hv = __popcll(sm.cen[row + dx] ^ cs);
+        h[dx] = ok ? hv : 48;  // an excluded term adds 1.0 = tab[48]
+    }
+#pragma unroll
+    for (int dx = 0; dx < 5; ++dx) {
+        sum += sm.tab[h[dx]];
+        if (HSUM) hs += h[dx];
     }
     return sum;
 }
