@@ -345,10 +345,11 @@ __global__ void init_kernel(const DevJob* __restrict__ jobs, const int32_t* __re
 // `c < best_c` could not hold and the result is unchanged.  In converged
 // regions most propagated planes are such repeats, and they are the costly
 // calls: with c near best_c they rarely abort.
-// MINB = 3 blocks of 256 per SM (<= 80 registers) measured fastest; 4 (64
-// registers) spills and loses.
+// Register cap 72 (28 warps per SM with 64-thread blocks) measured fastest
+// at 960x720 K=8: 3% ahead of 80 and 64, 10% ahead of 96.  MINB only names
+// the instantiation.
 template <bool COUNT, int MINB, bool PERSIST>
-__global__ void __launch_bounds__(256, MINB)
+__global__ void __maxnreg__(72)
     pass_kernel(const DevJob* __restrict__ jobs, const int32_t* __restrict__ job_start, int n_jobs, int tiles,
                 unsigned int* queue, uint64_t pass, float sig_inv, float sig_n, const uint64_t* __restrict__ census,
                 const float2* __restrict__ rays, PlaneBuf prev, PlaneBuf next, unsigned long long* d_work) {
@@ -386,26 +387,46 @@ __global__ void __launch_bounds__(256, MINB)
             float bn0 = cur.x, bn1 = cur.y, bn2 = cur.z;
             float bd = cur.w * (bn0 * ri.x + bn1 * ri.y + bn2);
 
-            // propagation from the 4 neighbours (stereo.rs:292-321)
-    #pragma unroll 1
-            for (int q = 0; q < 4; ++q) {
+            // propagation from the 4 neighbours (stereo.rs:292-321).  First
+            // the gates and the duplicate test of all four, then the kept ones
+            // in neighbour order: a warp runs as many plane_cost calls as its
+            // busiest lane needs, not one for every neighbour some lane needs.
+            // Each lane still sees its candidates, hints and best_c updates in
+            // the reference's order.
+            auto neighbour = [&](int q, float4& nb, float& d_plane) -> bool {
                 const int ddx = q == 0 ? -1 : (q == 1 ? 1 : 0);
                 const int ddy = q == 2 ? -1 : (q == 3 ? 1 : 0);
                 const int xx = x + ddx, yy = y + ddy;
-                if (xx < 0 || yy < 0 || xx >= w || yy >= h) continue;
-                const float4 nb = prev.nz[base + (size_t)yy * w + xx];
+                if (xx < 0 || yy < 0 || xx >= w || yy >= h) return false;
+                nb = prev.nz[base + (size_t)yy * w + xx];
                 const float2 rj = sm.ray[(ly + HALO + ddy) * stw + lx + HALO + ddx];
                 const float a_nb = nb.x * rj.x + nb.y * rj.y + nb.z;
-                if (a_nb < 0.1f) continue;
-                const float d_plane = nb.w * a_nb;
+                if (a_nb < 0.1f) return false;
+                d_plane = nb.w * a_nb;
                 const float a_here = nb.x * ri.x + nb.y * ri.y + nb.z;
-                if (a_here < 0.1f) continue;
+                if (a_here < 0.1f) return false;
                 const float zcand = d_plane / a_here;
-                if (!(zlo <= zcand && zcand <= zhi)) continue;
+                return zlo <= zcand && zcand <= zhi;
+            };
+            unsigned todo = 0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                float4 nb;
+                float d_plane;
+                if (!neighbour(q, nb, d_plane)) continue;
                 if (skip_dup && __float_as_uint(d_plane) == __float_as_uint(cur_d) &&
                     __float_as_uint(nb.x) == __float_as_uint(cur.x) && __float_as_uint(nb.y) == __float_as_uint(cur.y) &&
                     __float_as_uint(nb.z) == __float_as_uint(cur.z))
                     continue;
+                todo |= 1u << q;
+            }
+#pragma unroll 1
+            while (todo) {
+                const int q = __ffs(todo) - 1;
+                todo &= todo - 1;
+                float4 nb;
+                float d_plane;
+                neighbour(q, nb, d_plane);  // passed above; same values
                 const float c = plane_cost<false, COUNT, false>(sm, stw, lx, ly, nsrc, census, nb.x, nb.y, nb.z,
                                                                       d_plane, best_c + 0.02f, total, wc, nullptr);
                 if (c < best_c) {
