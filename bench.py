@@ -39,6 +39,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 FP32_NOMINAL_TOPS = 148 * 128 * 1.965e9 / 1e12  # SMs x FP32 lanes x max clock (ops/s, no FMA pairing)
+# DRAM bytes (read + write) per reference pixel of one pass launch, from the
+# ncu capture in profiles/pass_kernel_c2_24views.md (1.113 GB over 16.59 Mpx),
+# scaled to the measured workload's pixels for roofline.traffic.
+PASS_DRAM_BYTES_PER_PX = 1113303040 / (24 * 960 * 720)
 
 
 def configs():
@@ -49,12 +53,32 @@ def configs():
                    scene=dict(n_views=100, sizes=((1920, 1080),), f_rel=1.15, n_boxes=60, n_spheres=10),
                    opts=MvsOptions(max_dim=1920, num_sources=10, sweeps=6, num_hyp=64, min_consistent=3,
                                    depth_diff=0.01, reproj_px=1.0)),
+        "c3": dict(desc="48 views, widths {480,720,960,1440,1920} at 4:3 or 16:9 (seeded per view), room + 20 "
+                        "boxes, f=1.1*long side, K ~ U{4..12} per view (seeded), 64 hyps, 6 sweeps (12 passes)",
+                   scene=dict(n_views=48, sizes=((480, 360), (480, 270), (720, 540), (720, 405), (960, 720),
+                                                 (960, 540), (1440, 1080), (1440, 810), (1920, 1440),
+                                                 (1920, 1080)),
+                              f_rel=1.1, n_boxes=20, n_spheres=0, size_choice="random"),
+                   k_range=(4, 12),
+                   opts=MvsOptions(max_dim=1920, num_sources=12, sweeps=6, num_hyp=64)),
         "c2": dict(desc="64 views 960x720, room + 20 boxes, f=1.1*960, K=8, 64 hyps, 6 sweeps (12 passes)",
                    scene=dict(n_views=64, sizes=((960, 720),), f_rel=1.1, n_boxes=20, n_spheres=0),
                    opts=MvsOptions(max_dim=960, num_sources=8, sweeps=6, num_hyp=64)),
         "c1": dict(desc="corner room, 8 views 384x288, f=440, K=4, 64 hyps, 6 sweeps (12 passes)",
                    scene=None, opts=MvsOptions(max_dim=384, num_sources=4, sweeps=6, num_hyp=64)),
     }
+
+
+def make_jobs(cfg, sc, opts):
+    """(ref, sources, zmin, zmax) per view with sources; with k_range each
+    view keeps the first K ~ U{lo..hi} (seeded) of its planned sources."""
+    from rustcolmap_b200 import mvs
+    srcs, zr, fus = mvs.plan(sc.sparse, sc.views, opts)
+    if "k_range" in cfg:
+        rng = np.random.default_rng(3)
+        lo, hi = cfg["k_range"]
+        srcs = [s[:int(rng.integers(lo, hi + 1))] for s in srcs]
+    return [(i, srcs[i], zr[i, 0], zr[i, 1]) for i in range(len(sc.views)) if srcs[i]], fus
 
 
 def make_scene(cfg, seed, device):
@@ -209,8 +233,7 @@ def run_reference(args, cfg):
     oracle.lib()
     sc = make_scene(cfg, seed=5, device=-1 if not _has_gpu() else 0)
     opts = cfg["opts"]
-    srcs, zr, fus = mvs.plan(sc.sparse, sc.views, opts)
-    jobs = [(i, srcs[i], zr[i, 0], zr[i, 1]) for i in range(len(sc.views)) if srcs[i]]
+    jobs, fus = make_jobs(cfg, sc, opts)
     rows = args.ref_rows
     for _ in range(args.warmup):
         cpu_baseline(sc, opts, jobs, rows)
@@ -260,7 +283,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c5", choices=["c5", "c2", "c1"])
+    ap.add_argument("--config", default="c5", choices=["c5", "c3", "c2", "c1"])
     ap.add_argument("--cpu-rows", type=int, default=24, help="rows of the CPU-baseline band")
     ap.add_argument("--ref-rows", type=int, default=12, help="rows per step of the reference arm")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -303,8 +326,7 @@ def main():
     lopts = dataclasses.replace(opts, sweeps=2)
     t_setup = time.perf_counter()
     sc = make_scene(cfg, seed=5 + 1000 * rank, device=local)
-    srcs, zr, fus = mvs.plan(sc.sparse, sc.views, opts)
-    jobs = [(i, srcs[i], zr[i, 0], zr[i, 1]) for i in range(len(sc.views)) if srcs[i]]
+    jobs, fus = make_jobs(cfg, sc, opts)
     n_maps = len(jobs)
     ctx = mvs.Context(local)
     ds = mvs.DeviceScene(sc.views, ctx)
@@ -450,7 +472,10 @@ def main():
                 "seeded_fraction": seeded[0] / max(npx, 1), "speedup_vs_plain": value / plain_value,
                 "gt_within_delta_vs_plain": head_gt["within_1pct"] - plain_gt["within_1pct"]},
             "roofline": {"bound": "hbm", "kernel": "stereo_pass", "achieved": achieved_gbs, "peak": hbm_peak,
-                         "unit": "GB/s", "frac": achieved_gbs / hbm_peak, "traffic": None,
+                         "unit": "GB/s", "frac": achieved_gbs / hbm_peak,
+                         "traffic": PASS_DRAM_BYTES_PER_PX * npx,
+                         "traffic_source": "ncu dram bytes per pixel of a 24-view 960x720 capture "
+                                           "(profiles/pass_kernel_c2_24views.md) x this launch's pixels",
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650",
                          "algorithmic_bytes_per_launch": bytes_per_launch, "avg_launch_ms": pass_avg_s * 1e3,
                          "note": "issue-bound kernel: see compute_roofline"},

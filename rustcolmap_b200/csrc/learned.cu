@@ -9,8 +9,9 @@
 //                       cores (mma.sync m16n8k16, BF16 in, FP32 accumulate)
 //   conv3x3_wgrad_kernel  weight gradient of the same convolution
 //   loss/Adam kernels   training
-//   init_learned_kernel patch-match init: confident pixels take the predicted
-//                       plane, the others fall back to the plane sweep
+// The patch-match init that consumes the predictions (confident pixels take
+// the predicted plane, the others fall back to the plane sweep) is
+// init_learned_rows_kernel in stereo.cu.
 //
 // Tensors are NHWC, BF16, channels padded to a multiple of 16.
 #include <cuda_bf16.h>

@@ -1,0 +1,160 @@
+"""Single-scene multi-GPU host logic (rustcolmap_b200.shard) with world-size 2
+and 3 `gloo` process groups on the CPU: view assignment, the depth-map
+all-gather, and the sharded pipeline against the single-process one (with
+the CPU oracle standing in for the GPU stereo and fusion)."""
+import multiprocessing as mp
+import os
+import socket
+import tempfile
+
+import numpy as np
+import pytest
+
+from rustcolmap_b200 import shard
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _run_ranks(fn, world, *args):
+    """Runs fn(rank, world, outdir, *args) in `world` spawned processes joined
+    by a gloo group on 127.0.0.1; returns the outdir."""
+    port = _free_port()
+    out = tempfile.mkdtemp()
+    ctx = mp.get_context("spawn")
+    ps = [ctx.Process(target=_entry, args=(fn, r, world, port, out) + args) for r in range(world)]
+    for p in ps:
+        p.start()
+    for p in ps:
+        p.join(240)
+    for p in ps:
+        if p.is_alive():
+            p.kill()
+    assert all(p.exitcode == 0 for p in ps), [p.exitcode for p in ps]
+    return out
+
+
+def _entry(fn, rank, world, port, out, *args):
+    import datetime
+
+    import torch.distributed as dist
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        fn(rank, world, out, *args)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_assign_views_partitions_and_balances():
+    rng = np.random.default_rng(0)
+    costs = [int(c) for c in rng.integers(1, 100, 37)]
+    for world in (1, 2, 3, 8, 50):
+        parts = shard.assign_views(costs, world)
+        assert len(parts) == world
+        flat = sorted(i for p in parts for i in p)
+        assert flat == list(range(len(costs)))
+        assert parts == shard.assign_views(costs, world)  # deterministic
+        loads = [sum(costs[i] for i in p) for p in parts]
+        assert max(loads) - min(loads) <= max(costs)
+    assert shard.assign_views([], 4) == [[], [], [], []]
+    with pytest.raises(ValueError):
+        shard.assign_views([1], 0)
+
+
+SHAPES = {0: (3, 5), 1: (7, 2), 2: (1, 1), 4: (6, 6), 5: (2, 9)}
+
+
+def _map(v):
+    return (np.arange(np.prod(SHAPES[v]), dtype=np.float32) * (v + 1) + 0.5).reshape(SHAPES[v])
+
+
+def _gather_rank(rank, world, out, owners):
+    local = {v: _map(v) for v, o in owners.items() if o == rank}
+    got = shard.all_gather_maps(local, SHAPES, owners)
+    np.savez(os.path.join(out, f"r{rank}.npz"), **{str(k): v for k, v in got.items()})
+
+
+@pytest.mark.parametrize("world,owners", [
+    (2, {0: 0, 1: 1, 2: 1, 4: 0, 5: 1}),
+    (3, {0: 2, 1: 2, 2: 0, 4: 2, 5: 0}),  # rank 1 owns nothing
+])
+def test_all_gather_maps_gloo(world, owners):
+    out = _run_ranks(_gather_rank, world, owners)
+    for r in range(world):
+        got = dict(np.load(os.path.join(out, f"r{r}.npz")))
+        assert sorted(got) == sorted(str(v) for v in SHAPES)
+        for v in SHAPES:
+            assert np.array_equal(got[str(v)], _map(v))
+
+
+def _tiny():
+    from rustcolmap_b200 import MvsOptions, scene
+    sc = scene.corner_room(seed=2, n_views=5, w=96, h=64, f=110.0, arc_deg=40.0, n_patches=20, per_view_sparse=60)
+    opts = MvsOptions(max_dim=4096, num_sources=2, sweeps=1, num_hyp=8, min_consistent=1)
+    return sc, opts
+
+
+def _oracle_backends(sc, opts):
+    from oracle import oracle
+
+    def stereo(jobs):
+        return {r: oracle.estimate_depth(sc.views, r, s, a, b, opts, nthreads=1, normals=False)[0]
+                for r, s, a, b in jobs}
+
+    def fuse(depth, order):
+        off = np.cumsum([0] + [len(f) for f in order])
+        flat = [x for f in order for x in f]
+        xyz, rgb, _ = oracle.fuse_depth_maps(sc.views, depth, off, flat, sc.sparse.xyz, opts, nthreads=1)
+        return xyz, rgb
+    return stereo, fuse
+
+
+def _pipeline_rank(rank, world, out):
+    sc, opts = _tiny()
+    stereo, fuse = _oracle_backends(sc, opts)
+    xyz, rgb, depth = shard.run_mvs_sharded(sc.views, sc.sparse, opts, stereo=stereo, fuse=fuse)
+    np.savez(os.path.join(out, f"r{rank}.npz"), xyz=xyz, rgb=rgb,
+             **{f"d{i}": d for i, d in enumerate(depth) if d is not None})
+
+
+def test_sharded_pipeline_equals_single_process():
+    """Two ranks, each running the oracle on its share of the views, end with
+    the same depth maps and fused cloud as one process running all views."""
+    from rustcolmap_b200 import mvs
+    sc, opts = _tiny()
+    stereo, fuse = _oracle_backends(sc, opts)
+    srcs, zr, fus = mvs.plan(sc.sparse, sc.views, opts)
+    jobs = [(i, srcs[i], zr[i, 0], zr[i, 1]) for i in range(len(sc.views)) if srcs[i]]
+    ref_maps = stereo(jobs)
+    ref_depth = [ref_maps.get(i) for i in range(len(sc.views))]
+    ref_xyz, ref_rgb = fuse(ref_depth, fus)
+    assert len(ref_xyz) > 0
+    out = _run_ranks(_pipeline_rank, 2)
+    for r in range(2):
+        got = dict(np.load(os.path.join(out, f"r{r}.npz")))
+        assert np.array_equal(got["xyz"], ref_xyz) and np.array_equal(got["rgb"], ref_rgb)
+        for i, d in enumerate(ref_depth):
+            if d is not None:
+                assert np.array_equal(got[f"d{i}"].view(np.uint32), d.view(np.uint32))
+
+
+@pytest.mark.gpu
+def test_sharded_run_on_one_gpu_equals_run_mvs():
+    """World size 1 on the GPU: the sharded driver gives run_mvs's cloud."""
+    import torch.distributed as dist
+    from rustcolmap_b200 import mvs
+    sc, opts = _tiny()
+    ctx = mvs.Context(0)
+    _, xa, ca = mvs.run_mvs(sc.views, sc.sparse, opts, ctx=ctx)
+    port = _free_port()
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1)
+    try:
+        xb, cb, _ = shard.run_mvs_sharded(sc.views, sc.sparse, opts, ctx=ctx)
+    finally:
+        dist.destroy_process_group()
+    ctx.close()
+    assert np.array_equal(xa, xb) and np.array_equal(ca, cb)
