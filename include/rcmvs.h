@@ -49,7 +49,8 @@ typedef struct rcmvs_options {
     uint32_t sweeps;         /* patch-match sweeps; passes = 2*max(sweeps,1) */
     uint32_t num_hyp;        /* plane-sweep hypotheses; max(num_hyp,2) used */
     uint32_t min_consistent; /* min OTHER views agreeing in fusion */
-    uint32_t save_depth_vis; /* accepted and ignored (PNG output is not built) */
+    uint32_t save_depth_vis; /* PNGs are written by the callers that write files
+                                (see rcmvs_depth_vis); rcmvs_run_mvs writes none */
     float cost_thr;          /* max census Hamming fraction of a valid pixel */
     uint32_t reserved0;
     double depth_diff;       /* relative depth agreement in fusion */
@@ -211,6 +212,7 @@ int rcmvs_fuse_depth_maps(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_vie
 int rcmvs_write_ply_binary(const char* path, const double* xyz, const uint8_t* rgb,
                            uint64_t n);
 
+
 /* Host glue of `run_mvs` (mvs/src/lib.rs:303-342, :358, :398-418):
  * co-visibility counts, top-K support views (count >= 10), per-view depth
  * range, fusion order (sources first).  Outputs (caller-allocated):
@@ -295,6 +297,24 @@ int rcmvs_scene_get_census(rcmvs_ctx* ctx, rcmvs_scene* scene, int32_t view,
  * (nullable, 15*n bytes) receives the PLY vertex records the device packed. */
 int rcmvs_scene_get_points(rcmvs_ctx* ctx, rcmvs_scene* scene, double* xyz, uint8_t* rgb,
                            uint8_t* ply_body);
+
+/* Depth-map visualisation of `fuse::save_depth_vis` (mvs/src/fuse.rs:241-268)
+ * on the GPU: the 2nd/98th percentiles of the valid depths (z > 0;
+ * `ds[(n*0.02) as usize]`, `ds[(n*0.98) as usize - 1]`, or 0 and 1 below 32
+ * valid pixels) set the scale; out[i] = 0 for invalid depth, else
+ * (255 * (1 - clamp((z - lo) / range, 0, 1))) as u8, near = bright.
+ * depth and out are host buffers of w*h; lo_hi (nullable) gets lo and hi.
+ * Synchronous. */
+int rcmvs_depth_vis(rcmvs_ctx* ctx, const float* depth, int32_t w, int32_t h, uint8_t* out,
+                    float* lo_hi);
+/* The same for a scene view's device-resident depth map (RCMVS_E_STATE if
+ * the view has none). */
+int rcmvs_scene_depth_vis(rcmvs_ctx* ctx, rcmvs_scene* scene, int32_t view, uint8_t* out,
+                          float* lo_hi);
+/* 8-bit greyscale PNG of a w*h image (the file `save_depth_vis` writes;
+ * zlib-compressed, so its bytes differ from the `image` crate's while the
+ * decoded pixels are the same).  Host only. */
+int rcmvs_write_png_gray(const char* path, const uint8_t* img, int32_t w, int32_t h);
 
 /* ---------------------------------------------------------- diagnostics */
 

@@ -727,6 +727,39 @@ int orc_write_ply_binary(const char* path, const double* xyz, const uint8_t* rgb
     return std::fclose(f) == 0 ? RCMVS_OK : RCMVS_E_IO;
 }
 
+// mvs/src/fuse.rs:241-268  save_depth_vis (the image; the PNG encoding is
+// the caller's).  lo_hi (nullable) receives the two percentiles.
+void orc_depth_vis(const float* depth, int32_t w, int32_t h, uint8_t* out, float* lo_hi) {
+    const size_t n = (size_t)w * h;
+    std::vector<float> ds;
+    for (size_t i = 0; i < n; ++i)
+        if (depth[i] > 0.0f) ds.push_back(depth[i]);
+    std::sort(ds.begin(), ds.end());  // partial_cmp order; no NaN passes z > 0
+    float lo = 0.0f, hi = 1.0f;
+    if (ds.size() >= 32) {
+        lo = ds[(size_t)((double)ds.size() * 0.02)];
+        hi = ds[(size_t)((double)ds.size() * 0.98) - 1];
+    }
+    const float range = std::max(hi - lo, 1e-9f);
+    for (size_t i = 0; i < n; ++i) {
+        const float z = depth[i];
+        uint8_t val = 0;
+        if (!(z <= 0.0f)) {
+            float t = (z - lo) / range;
+            if (t < 0.0f) t = 0.0f;          // f32::clamp(0.0, 1.0)
+            else if (t > 1.0f) t = 1.0f;
+            const float v = 255.0f * (1.0f - t);
+            // `as u8`: truncation, saturating, NaN -> 0
+            val = !(v > 0.0f) ? 0 : (v >= 255.0f ? 255 : (uint8_t)(int)v);
+        }
+        out[i] = val;
+    }
+    if (lo_hi) {
+        lo_hi[0] = lo;
+        lo_hi[1] = hi;
+    }
+}
+
 // mvs/src/lib.rs:245-251  percentile
 static double percentile(const std::vector<double>& s, double q) {
     if (s.empty()) return 0.0;

@@ -62,6 +62,9 @@ void orc_free(void* p);
 int orc_write_ply_binary(const char* path, const double* xyz, const uint8_t* rgb,
                          uint64_t n);
 
+/* save_depth_vis (mvs/src/fuse.rs:241-268): the grey image and lo/hi. */
+void orc_depth_vis(const float* depth, int32_t w, int32_t h, uint8_t* out, float* lo_hi);
+
 /* Host glue of run_mvs; same output layout as rcmvs_plan.  has_depth
  * (nullable) marks views that have a depth map; NULL means "every view with
  * at least one source". */

@@ -50,6 +50,8 @@ def lib():
         L.orc_free.argtypes = [vp]
         L.orc_write_ply_binary.argtypes = [C.c_char_p, vp, vp, u64]
         L.orc_plan.argtypes = [vp, vp, i32, vp, vp, vp, vp, vp, vp]
+        L.orc_depth_vis.argtypes = [vp, i32, i32, vp, vp]
+        L.orc_depth_vis.restype = None
         _lib = L
     return _lib
 
@@ -163,6 +165,16 @@ def fuse_depth_maps(views, depth_maps, order_offsets, order, sparse_xyz, opts, n
     lib().orc_free(xyz_p)
     lib().orc_free(rgb_p)
     return xyz, rgb, ncand.value
+
+
+def depth_vis(depth):
+    """fuse::save_depth_vis's image on the CPU: ((h, w) u8, lo, hi)."""
+    d = np.ascontiguousarray(depth, dtype=np.float32)
+    h, w = d.shape
+    out = np.empty((h, w), np.uint8)
+    lh = np.zeros(2, np.float32)
+    lib().orc_depth_vis(d.ctypes.data, w, h, out.ctypes.data, lh.ctypes.data)
+    return out, float(lh[0]), float(lh[1])
 
 
 def write_ply_binary(path, xyz, rgb):

@@ -75,6 +75,9 @@ def mvs():
         "rcmvs_autotune": ([vp, vp, vp, i32, vp], C.c_int),
         "rcmvs_tune_table": ([vp, vp, i32, vp], C.c_int),
         "rcmvs_tune_set": ([vp, vp, i32], C.c_int),
+        "rcmvs_depth_vis": ([vp, vp, i32, i32, vp, vp], C.c_int),
+        "rcmvs_scene_depth_vis": ([vp, vp, i32, vp, vp], C.c_int),
+        "rcmvs_write_png_gray": ([cp, vp, i32, i32], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -115,5 +118,5 @@ _SIG_NAMES = [
     "rcmvs_estimate_depth_noalloc", "rcmvs_net_param_count", "rcmvs_net_create", "rcmvs_net_destroy",
     "rcmvs_net_get_params", "rcmvs_net_forward", "rcmvs_net_train_step", "rcmvs_scene_costvol",
     "rcmvs_scene_estimate_depth_learned", "rcmvs_run_mvs_learned", "rcmvs_autotune", "rcmvs_tune_table",
-    "rcmvs_tune_set",
+    "rcmvs_tune_set", "rcmvs_depth_vis", "rcmvs_scene_depth_vis", "rcmvs_write_png_gray",
 ]

@@ -28,9 +28,10 @@ FLAGS = ARCH + [
 
 LIBS = {
     "librcmvs.so": ["capi.cu", "census.cu", "stereo.cu", "fuse.cu", "noalloc.cu", "learned.cu", "learned_api.cu",
-                   "schedule.cu"],
+                   "schedule.cu", "depthvis.cu"],
     "librcscene.so": ["scene.cu"],
 }
+LINK = {"librcmvs.so": ["-lz"]}  # zlib: the grey PNG writer
 HEADERS = [os.path.join(CSRC, "rcmvs_internal.cuh"), os.path.join(CSRC, "ctx_internal.cuh"),
            os.path.join(CSRC, "learned.cuh"), os.path.join(ROOT, "include", "rcmvs.h"),
            os.path.join(ROOT, "include", "rcscene.h")]
@@ -59,7 +60,7 @@ def build(force=False, verbose=False):
                 subprocess.run(cmd, check=True)
             objs.append(obj)
         if force or _newer(objs, target):
-            cmd = [NVCC] + ARCH + ["-shared", "-o", target] + objs
+            cmd = [NVCC] + ARCH + ["-shared", "-o", target] + objs + LINK.get(lib, [])
             if verbose:
                 print(" ".join(cmd))
             subprocess.run(cmd, check=True)

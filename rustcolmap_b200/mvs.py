@@ -185,6 +185,33 @@ def _take_points(ctx, pts):
     return xyz, rgb
 
 
+def depth_vis(depth, ctx=None):
+    """fuse::save_depth_vis's image (fuse.rs:241-268) on the GPU: returns
+    ((h, w) u8, lo, hi)."""
+    ctx = _ctx(ctx)
+    d = np.ascontiguousarray(depth, dtype=np.float32)
+    h, w = d.shape
+    out = np.empty((h, w), np.uint8)
+    lh = np.zeros(2, np.float32)
+    ctx.check(ctx._L.rcmvs_depth_vis(ctx.ptr, d.ctypes.data, w, h, out.ctypes.data, lh.ctypes.data))
+    return out, float(lh[0]), float(lh[1])
+
+
+def write_png_gray(path, img):
+    """8-bit greyscale PNG (the file save_depth_vis writes)."""
+    img = np.ascontiguousarray(img, dtype=np.uint8)
+    h, w = img.shape
+    rc = _lib.mvs().rcmvs_write_png_gray(os.fsencode(path), img.ctypes.data, w, h)
+    if rc != 0:
+        raise RcmvsError(rc, f"cannot write {path}")
+
+
+def _vis_stem(name):
+    """Path::file_stem of the view's image name, or "view" (fuse.rs:260-263)."""
+    stem = os.path.splitext(os.path.basename(name or ""))[0] if name else ""
+    return stem or "view"
+
+
 def write_ply_binary(path, xyz, rgb):
     """fuse::write_ply_binary (fuse.rs:222-239)."""
     xyz = np.ascontiguousarray(xyz, dtype=np.float64)
@@ -279,6 +306,16 @@ class DeviceScene:
         self.ctx.check(self.ctx._L.rcmvs_autotune(self.ctx.ptr, self.ptr, cj, len(jobs), C.byref(o)))
         return self.ctx.tune_table()
 
+    def depth_vis(self, v):
+        """save_depth_vis's image of view v's device-resident depth map:
+        ((h, w) u8, lo, hi)."""
+        vw = self.views[v]
+        out = np.empty((vw.h, vw.w), np.uint8)
+        lh = np.zeros(2, np.float32)
+        self.ctx.check(self.ctx._L.rcmvs_scene_depth_vis(self.ctx.ptr, self.ptr, int(v), out.ctypes.data,
+                                                         lh.ctypes.data))
+        return out, float(lh[0]), float(lh[1])
+
     def fuse(self, fusion_order, sparse_xyz, opts):
         off, flat = _csr(fusion_order)
         sp = np.ascontiguousarray(sparse_xyz, dtype=np.float64).reshape(-1, 3)
@@ -369,7 +406,8 @@ def run_mvs(views, sparse, opts, out_dir=None, ctx=None, log=None, return_depth=
     pts = _abi.Points()
     douts = None
     dms = []
-    if return_depth:
+    want_vis = bool(opts.save_depth_vis) and out_dir is not None  # lib.rs:383-389
+    if return_depth or want_vis:
         douts = (_abi.DepthOut * len(views))()
         for i, v in enumerate(views):
             d = np.empty((v.h, v.w), np.float32)
@@ -384,6 +422,14 @@ def run_mvs(views, sparse, opts, out_dir=None, ctx=None, log=None, return_depth=
                                                float(conf_thr), int(n_local), float(span), douts, C.byref(pts),
                                                C.byref(st)))
     xyz, rgb = _take_points(ctx, pts)
+    if want_vis:
+        srcs, _, _ = plan(sparse, views, opts)
+        vis_dir = os.path.join(out_dir, "dense", "depth_vis")
+        os.makedirs(vis_dir, exist_ok=True)
+        for i, v in enumerate(views):
+            if srcs[i]:  # views with a depth map
+                img, _, _ = depth_vis(dms[i].depth, ctx)
+                write_png_gray(os.path.join(vis_dir, f"{_vis_stem(v.name)}_depth.png"), img)
     stats = MvsStats(views=st.views, views_with_depth=st.views_with_depth, dense_points=st.dense_points,
                      per_view_valid=[int((d.depth > 0).sum()) for d in dms] if return_depth else [],
                      elapsed_s=time.time() - t0, stereo_s=st.stereo_s, fuse_s=st.fuse_s,
@@ -404,5 +450,5 @@ def run_mvs(views, sparse, opts, out_dir=None, ctx=None, log=None, return_depth=
 
 
 __all__ = ["Context", "default_context", "census_map", "estimate_depth", "estimate_depth_batch",
-           "fuse_depth_maps", "write_ply_binary", "plan", "run_mvs", "plane_cost_field", "DeviceScene",
+           "fuse_depth_maps", "write_ply_binary", "depth_vis", "write_png_gray", "plan", "run_mvs", "plane_cost_field", "DeviceScene",
            "MvsOptions", "MvsStats", "ViewData", "DepthMap", "SparseModel", "RcmvsError"]
