@@ -579,13 +579,13 @@ __global__ void __launch_bounds__(256, MINB)
 // the best one seeds the pixel.  Every other pixel (and a confident one whose
 // local planes all fail the gates) runs the 64-plane sweep of
 // stereo.rs:247-269 unchanged.
-// Row-step schedule of the learned init: each lane streams its own candidate
-// list one 5-term window row per step — the n_local planes around its
-// prediction if it is confident, else (or if none of them passes the gates)
-// the 64-plane sweep — so a warp mixing seeded and unseeded pixels does not
-// run both lists one after the other.  Fronto-parallel sweep planes go
-// through the general cost path: with n = (0,0,1), denom is exactly 1.0 and
-// d/1 = d, so each candidate's cost is the same float as in the sweep.
+// Two phases per tile.  First each confident lane streams its local planes
+// one window row per step.  Then the tile's remaining pixels are listed in
+// shared memory and the block's threads take them in turn for the sweep
+// (fronto-parallel, as init_rows_kernel): a few low-confidence pixels
+// scattered over a tile occupy one warp's lanes together instead of holding
+// every warp that contains one for all 64 hypotheses.  Every pixel's
+// computation is the same; only which thread does it changes.
 template <bool PERSIST>
 __global__ void __launch_bounds__(256, 3)
     init_learned_rows_kernel(const DevJob* __restrict__ jobs, const int32_t* __restrict__ job_start, int n_jobs,
@@ -595,12 +595,15 @@ __global__ void __launch_bounds__(256, 3)
                              unsigned long long* d_learned) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int s_tile;
+    __shared__ int s_n;
+    __shared__ unsigned short s_list[256];
     for (int it = 0; PERSIST || it == 0; ++it) {
         const int tile = PERSIST ? next_tile(queue, tiles, it, &s_tile) : (int)blockIdx.x;
         if (tile < 0) break;
         Smem sm;
         Tile T;
         load_tile(jobs, job_start, n_jobs, tile, census, rays, smem_raw, sm, T);
+        if (threadIdx.x == 0) s_n = 0;
         const DevJob* J = T.job;
         const int j = (int)(J - jobs);
         const int lx = threadIdx.x % T.tw, ly = threadIdx.x / T.tw;
@@ -629,47 +632,31 @@ __global__ void __launch_bounds__(256, 3)
                 learned = pa >= 0.1f;
             }
         }
-        // candidate stream: list 1 = local planes (learned lanes), list 0 = sweep
-        int list = learned ? 1 : 0, k = 0;
+        __syncthreads();  // s_n = 0 is visible
+
+        // phase 1: the local planes of confident lanes, one row per step
+        int k = 0;
         bool any_local = false;
-        float cnx = 0.f, cny = 0.f, cnz = 1.f, cd = 0.f, cz = 0.f;
-        auto next = [&]() -> bool {
-            for (;;) {
-                if (list == 1) {
-                    if (k >= n_local) {
-                        if (any_local) return false;
-                        list = 0;  // no local plane passed the gates: sweep instead
-                        k = 0;
-                        continue;
-                    }
-                    const float tk = t0 + span * ((float)k / (float)max(n_local - 1, 1) - 0.5f);
-                    ++k;
-                    const float inv = inv_min + tk * span_inv;
-                    if (!(inv > 0.f)) continue;
-                    const float z = 1.f / inv;
-                    if (!(z >= zlo && z <= zhi)) continue;
-                    cnx = pnx;
-                    cny = pny;
-                    cnz = pnz;
-                    cz = z;
-                    cd = z * pa;
-                    any_local = true;
-                    return true;
-                }
-                if (k >= nh) return false;
-                cnx = 0.f;
-                cny = 0.f;
-                cnz = 1.f;
-                cd = hyp_depth(inv_min, inv_max, k, nh);
-                cz = cd;
+        float cz = 0.f, cd = 0.f;
+        auto next_local = [&]() -> bool {
+            while (k < n_local) {
+                const float tk = t0 + span * ((float)k / (float)max(n_local - 1, 1) - 0.5f);
                 ++k;
+                const float inv = inv_min + tk * span_inv;
+                if (!(inv > 0.f)) continue;
+                const float z = 1.f / inv;
+                if (!(z >= zlo && z <= zhi)) continue;
+                cz = z;
+                cd = z * pa;
+                any_local = true;
                 return true;
             }
+            return false;
         };
         float best_c = INFINITY;
         float4 plane = make_float4(0.0f, 0.0f, 1.0f, 0.0f);
         float plane_d = 0.f;
-        bool live = inside && next();
+        bool live = inside && learned && next_local();
         int si = 0, dy = 0;
         float sum = 0.f, thr = INFINITY;
         int32_t hs = 0;
@@ -677,7 +664,7 @@ __global__ void __launch_bounds__(256, 3)
             bool fin = true, aborted = false;
             if (nsrc > 0) {
                 const SrcRegs s = load_src(sm.src[si], census);
-                sum = cost_row<false, false>(sm, (ly + dy) * T.stw + lx, s, cnx, cny, cnz, cd, sum, hs);
+                sum = cost_row<false, false>(sm, (ly + dy) * T.stw + lx, s, pnx, pny, pnz, cd, sum, hs);
                 aborted = sum / ((float)(dy + 1) * 5.0f * (float)(si + 1)) > thr;
                 fin = aborted || (si == nsrc - 1 && dy == 4);
             }
@@ -685,10 +672,10 @@ __global__ void __launch_bounds__(256, 3)
                 const float c = aborted ? 1e9f : sum / total;
                 if (c < best_c) {
                     best_c = c;
-                    plane = make_float4(cnx, cny, cnz, cz);
+                    plane = make_float4(pnx, pny, pnz, cz);
                     plane_d = cd;
                 }
-                live = next();
+                live = next_local();
                 sum = 0.f;
                 si = 0;
                 dy = 0;
@@ -699,14 +686,62 @@ __global__ void __launch_bounds__(256, 3)
             }
         }
         const bool seeded = inside && learned && any_local;
-        if (inside) {
+        if (seeded) {
             const size_t i = (size_t)J->off + (size_t)y * J->w + x;
             out.nz[i] = plane;
             out.cost[i] = fminf(best_c, 1.0f);
             if (out.d) out.d[i] = plane_d;
+        } else if (inside) {
+            s_list[atomicAdd(&s_n, 1)] = (unsigned short)threadIdx.x;
         }
         const unsigned bal = __ballot_sync(0xffffffffu, seeded);
         if ((threadIdx.x & 31) == 0 && bal) atomicAdd(d_learned, (unsigned long long)__popc(bal));
+        __syncthreads();  // the list is complete
+
+        // phase 2: the plane sweep (stereo.rs:247-269) of the listed pixels
+        const int n_list = s_n;
+        for (int e = threadIdx.x; e < n_list; e += blockDim.x) {
+            const int pt = s_list[e];
+            const int plx = pt % T.tw, ply = pt / T.tw;
+            const int px = T.x0 + plx, py = T.y0 + ply;
+            float bc = INFINITY, bdep = 0.f;
+            int hi = 0, ssi = 0, sdy = 0;
+            float d = hyp_depth(inv_min, inv_max, 0, nh);
+            float ssum = 0.f, sthr = INFINITY;
+            bool slive = true;
+            while (slive) {
+                bool fin = true, aborted = false;
+                if (nsrc > 0) {
+                    const SrcRegs s = load_src(sm.src[ssi], census);
+                    ssum = cost_row<true, false>(sm, (ply + sdy) * T.stw + plx, s, 0.f, 0.f, 1.f, d, ssum, hs);
+                    aborted = ssum / ((float)(sdy + 1) * 5.0f * (float)(ssi + 1)) > sthr;
+                    fin = aborted || (ssi == nsrc - 1 && sdy == 4);
+                }
+                if (fin) {
+                    const float c = aborted ? 1e9f : ssum / total;
+                    if (c < bc) {
+                        bc = c;
+                        bdep = d;
+                    }
+                    if (++hi >= nh) {
+                        slive = false;
+                    } else {
+                        d = hyp_depth(inv_min, inv_max, hi, nh);
+                        ssum = 0.f;
+                        ssi = 0;
+                        sdy = 0;
+                        sthr = (bc + 0.02f) + 0.12f;
+                    }
+                } else if (++sdy == 5) {
+                    sdy = 0;
+                    ++ssi;
+                }
+            }
+            const size_t i = (size_t)J->off + (size_t)py * J->w + px;
+            out.nz[i] = make_float4(0.0f, 0.0f, 1.0f, bdep);
+            out.cost[i] = fminf(bc, 1.0f);
+            if (out.d) out.d[i] = bdep;
+        }
     }
 }
 
