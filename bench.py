@@ -397,7 +397,8 @@ def main():
     head_opts = opts if args.plain_only else lopts
 
     # work counters of the plain arm (untimed rerun with counting on)
-    evals, rows5 = 0, 0
+    # (and again with the duplicate skip off: the reference's own call count)
+    evals, rows5, ref_evals, ref_rows5 = 0, 0, 0, 0
     if not args.no_count:
         os.environ["RCMVS_COUNT"] = "1"
         cctx = mvs.Context(local)
@@ -405,6 +406,8 @@ def main():
         cds = mvs.DeviceScene(sc.views, cctx)
         cds.estimate(jobs, opts)
         evals, rows5 = cctx.last_work()
+        cds.estimate(jobs, dataclasses.replace(opts, flags=opts.flags | 16))
+        ref_evals, ref_rows5 = cctx.last_work()
         cds.close()
         cctx.close()
 
@@ -445,6 +448,7 @@ def main():
     stereo_ms = sum(plain_kt[k][0] for k in ("stereo_init", "stereo_pass", "stereo_gate")) / args.steps if plain_kt else 0
     fp32_ops_per_term = 40
     achieved_tops = actual_terms * fp32_ops_per_term / (stereo_ms / 1e3) / 1e12 if actual_terms and stereo_ms else None
+    ref_tops = ref_rows5 * 5 * fp32_ops_per_term / (stereo_ms / 1e3) / 1e12 if ref_rows5 and stereo_ms else None
 
     cpu = None
     if not args.no_cpu_baseline and rank == 0 and ws == 1:
@@ -483,17 +487,26 @@ def main():
                                  "achieved": achieved_tops, "peak": FP32_NOMINAL_TOPS, "unit": "Top/s",
                                  "frac": achieved_tops / FP32_NOMINAL_TOPS if achieved_tops else None,
                                  "ops_per_term": fp32_ops_per_term,
-                                 "peak_source": "nominal 148 SM x 128 FP32 lanes x 1.965 GHz"},
+                                 "peak_source": "nominal 148 SM x 128 FP32 lanes x 1.965 GHz",
+                                 "note": "achieved counts the terms evaluated; reference_equivalent counts the "
+                                         "terms the reference's call sequence evaluates for the same step "
+                                         "(duplicate skip off), over the same time",
+                                 "reference_equivalent": ref_tops,
+                                 "reference_equivalent_frac": ref_tops / FP32_NOMINAL_TOPS if ref_tops else None},
             "gpu_launches": args.steps * per_step,
             "clocks": clocks,
             "e2e": e2e,
             "cpu_baseline": cpu,
             "gcost_evals_per_s_plain": evals * args.steps / (plain_ms / 1e3) / 1e9 if evals else None,
+            "gcost_evals_per_s_plain_reference_equivalent":
+                ref_evals * args.steps / (plain_ms / 1e3) / 1e9 if ref_evals else None,
             "work_plain": {"cost_evals_per_step": evals, "window_rows_per_step": rows5,
                            "algorithmic_cost_evals_per_step": sum(sc.views[r].w * sc.views[r].h *
                                                                  (opts.num_hyp + 14 * opts.sweeps)
                                                                  for r, _, _, _ in jobs),
-                           "algorithmic_terms_per_step": algo_terms_total, "evaluated_terms_per_step": actual_terms},
+                           "algorithmic_terms_per_step": algo_terms_total, "evaluated_terms_per_step": actual_terms,
+                           "reference_cost_evals_per_step": ref_evals,
+                           "reference_terms_per_step": ref_rows5 * 5},
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in head_kt.items() if v[1]},
             "fused_points": head_pts,
             "setup_s": setup_s,
