@@ -415,12 +415,12 @@ def main():
     e2e = None
     if not args.no_e2e:
         pv = pinned_views(sc.views)
-        mvs.run_mvs(pv, sc.sparse, head_opts, ctx=ctx, net=net)  # warm
+        mvs.run_mvs(pv, sc.sparse, head_opts, ctx=ctx, net=net, **lkw)  # warm
         torch.cuda.synchronize()
         barrier(ws)
         t0 = time.perf_counter()
         for _ in range(args.steps):
-            st, xyz, rgb = mvs.run_mvs(pv, sc.sparse, head_opts, ctx=ctx, net=net)
+            st, xyz, rgb = mvs.run_mvs(pv, sc.sparse, head_opts, ctx=ctx, net=net, **lkw)
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
         barrier(ws)
@@ -464,7 +464,8 @@ def main():
             "data": "synthetic",
             "config": {"workload": args.config + ": " + cfg["desc"], "views_per_step": n_maps,
                        "headline_arm": "plain, 6 sweeps" if args.plain_only else
-                       "learned init (proposal_c4 weights; pixels with confidence >= 0.1 start from the "
+                       f"learned init (proposal_c4 weights; pixels with confidence >= "
+                       f"{args.conf if args.conf is not None else learned.CONF_THR} start from the "
                        "predicted plane, the others from the 64-plane sweep) + 2 sweeps",
                        "parallelism": f"views batched on 1 GPU; {ws} rank(s), one independent scene each",
                        "l2": "inputs larger than L2 (census 8 B/px, rays 8 B/px, planes 40 B/px over all views)"},

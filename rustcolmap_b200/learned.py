@@ -90,7 +90,11 @@ def costvol(ds, jobs, out_ptr):
 # confident pixels (sigmoid >= 0.1) start from the predicted plane alone; a
 # local sweep around it (3 to 16 planes over +-1% to +-6% of the range) was
 # both slower and less accurate after the 2 sweeps.
-LOCAL_HYPS, LOCAL_SPAN, CONF_THR = 1, 0.0, 0.1
+# Operating point: the predicted plane alone for pixels with confidence >=
+# 0.02, chosen on the tuning scenes (seeds 5000-5019) as the lowest threshold
+# whose accuracy stays 1 point above the plain method with 6 sweeps, with no
+# scene below it.
+LOCAL_HYPS, LOCAL_SPAN, CONF_THR = 1, 0.0, 0.02
 
 
 def estimate_learned(ds, jobs, opts, net, conf_thr=CONF_THR, n_local=LOCAL_HYPS, span=LOCAL_SPAN):

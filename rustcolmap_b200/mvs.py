@@ -385,14 +385,16 @@ def _web_json(xyz, rgb, path, cap=400_000):
 
 
 def run_mvs(views, sparse, opts, out_dir=None, ctx=None, log=None, return_depth=False, net=None,
-            conf_thr=0.1, n_local=1, span=0.0):
+            conf_thr=None, n_local=1, span=0.0):
     """mvs::run_mvs (lib.rs:294-517) from views already at working resolution
     (the image decode/resize of load_views is not part of this path).  Writes
     <out_dir>/dense/dense.ply, mvs_stats.json and dense_web.json when out_dir
     is given.  net (a learned.ProposalNet, extension): seed stereo with the
-    network instead of the plane sweep.  Returns (MvsStats, xyz, rgb[, depth
-    maps])."""
+    network instead of the plane sweep (conf_thr None: the learned module's
+    operating point).  Returns (MvsStats, xyz, rgb[, depth maps])."""
     ctx = _ctx(ctx)
+    if conf_thr is None:
+        from .learned import CONF_THR as conf_thr
     t0 = time.time()
     if len(views) < 2:
         raise RcmvsError(_abi.RCMVS_E_ARG, "need at least 2 registered views for MVS")
