@@ -15,9 +15,10 @@
  *  - One rcmvs_ctx per device.  A context is not thread-safe; separate
  *    contexts are independent.  All device work of a context runs on its
  *    own CUDA stream (rcmvs_ctx_stream).
- *  - Views are supplied at the stereo working resolution: the reference's
- *    resize to `max_dim` (mvs/src/lib.rs:185-192) is not performed, and a
- *    view whose long side exceeds opts->max_dim is rejected.
+ *  - Views are supplied at the stereo working resolution: a view whose
+ *    long side exceeds opts->max_dim is rejected.  The reference's resize to
+ *    `max_dim` (mvs/src/lib.rs:185-192) is a separate call,
+ *    rcmvs_resize_view, made while loading images.
  *  - Image rows are row-major, pixel (x, y) at index y*w + x.  A pixel's
  *    centre sits at integer coordinates (sfm-lite/src/geom.rs:28-42).
  */
@@ -183,6 +184,23 @@ const char* rcmvs_version(void);
  * (mvs/src/lib.rs:119-142).  Host buffers. */
 int rcmvs_census(rcmvs_ctx* ctx, const uint8_t* gray, int32_t w, int32_t h,
                  uint64_t* census_out);
+
+/* Working resolution of a w x h camera (mvs/src/lib.rs:155-157, :185-187):
+ * s = min(max_dim / max(w, h), 1) in f64, side = max(round(side * s), 16). */
+int rcmvs_working_size(int32_t w, int32_t h, uint32_t max_dim, int32_t* mw, int32_t* mh);
+
+/* One decoded 8-bit image brought to the working resolution the way
+ * `load_views` does (mvs/src/lib.rs:183-194): when (mw, mh) != (w, h),
+ * `resize_exact(mw, mh, FilterType::Triangle)` of the `image` crate 0.24
+ * (a vertical pass into f32, then a horizontal pass rounded to u8, each
+ * output sample a normalised triangle-weighted sum of its input samples);
+ * then `to_luma8` and `to_rgb8`.  `img` holds h rows of w pixels of
+ * `channels` bytes: 1 grey, 2 grey + alpha, 3 RGB, 4 RGBA (alpha is
+ * dropped; the colour channels resize independently).  gray_out gets mw*mh
+ * bytes, rgb_out mw*mh*3 (host buffers; either may be NULL).  Sides up to
+ * 2^23; mw, mh >= 1. */
+int rcmvs_resize_view(rcmvs_ctx* ctx, const uint8_t* img, int32_t w, int32_t h, int32_t channels,
+                      int32_t mw, int32_t mh, uint8_t* gray_out, uint8_t* rgb_out);
 
 /* Depth (+cost, optional normal) map of one reference view.  Replaces
  * `stereo::estimate_depth` (mvs/src/stereo.rs:234-394). Host buffers. */

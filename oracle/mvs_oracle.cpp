@@ -760,6 +760,80 @@ void orc_depth_vis(const float* depth, int32_t w, int32_t h, uint8_t* out, float
     }
 }
 
+// image 0.24 imageops::sample (the crate the reference resizes with at
+// mvs/src/lib.rs:188-190; not in the reference tree): the taps of output
+// sample o along an axis of n inputs resampled to m, Triangle filter
+// (support 1, kernel |x| < 1 ? 1 - |x| : 0), weights normalised by their
+// f32 sum.  Returns the first tap; ws gets the weights.
+static uint32_t triangle_taps(uint32_t n, uint32_t m, uint32_t o, std::vector<float>& ws) {
+    const float ratio = (float)n / (float)m;
+    const float sratio = ratio < 1.0f ? 1.0f : ratio;
+    const float src_support = 1.0f * sratio;
+    float input = ((float)o + 0.5f) * ratio;
+    int64_t left = (int64_t)std::floor(input - src_support);
+    left = std::min(std::max(left, (int64_t)0), (int64_t)n - 1);
+    int64_t right = (int64_t)std::ceil(input + src_support);
+    right = std::min(std::max(right, left + 1), (int64_t)n);
+    input = input - 0.5f;
+    ws.clear();
+    float sum = 0.0f;
+    for (int64_t i = left; i < right; ++i) {
+        const float x = ((float)i - input) / sratio;
+        const float w = std::fabs(x) < 1.0f ? 1.0f - std::fabs(x) : 0.0f;
+        ws.push_back(w);
+        sum += w;
+    }
+    for (float& w : ws) w /= sum;
+    return (uint32_t)left;
+}
+
+static uint8_t luma709(uint32_t r, uint32_t g, uint32_t b) {
+    return (uint8_t)((2126u * r + 7152u * g + 722u * b) / 10000u);
+}
+
+void orc_resize_view(const uint8_t* img, int32_t w, int32_t h, int32_t channels, int32_t mw, int32_t mh,
+                     uint8_t* gray, uint8_t* rgb) {
+    const int nc = channels < 3 ? 1 : 3;  // colour channels; alpha is dropped
+    const size_t n_out = (size_t)mw * mh;
+    std::vector<uint8_t> px(n_out * nc);
+    if (mw == w && mh == h) {  // lib.rs:188-192: the image as decoded
+        for (size_t i = 0; i < n_out; ++i)
+            for (int c = 0; c < nc; ++c) px[i * nc + c] = img[i * channels + c];
+    } else {
+        // vertical_sample: w columns x mh rows of f32
+        std::vector<float> tmp((size_t)w * mh * nc), ws;
+        for (int32_t oy = 0; oy < mh; ++oy) {
+            const uint32_t top = triangle_taps((uint32_t)h, (uint32_t)mh, (uint32_t)oy, ws);
+            for (int32_t x = 0; x < w; ++x)
+                for (int c = 0; c < nc; ++c) {
+                    float t = 0.0f;
+                    for (size_t i = 0; i < ws.size(); ++i)
+                        t += (float)img[(((size_t)top + i) * w + x) * channels + c] * ws[i];
+                    tmp[((size_t)oy * w + x) * nc + c] = t;
+                }
+        }
+        // horizontal_sample: clamp to [0, 255], round half away from zero
+        for (int32_t ox = 0; ox < mw; ++ox) {
+            const uint32_t first = triangle_taps((uint32_t)w, (uint32_t)mw, (uint32_t)ox, ws);
+            for (int32_t y = 0; y < mh; ++y)
+                for (int c = 0; c < nc; ++c) {
+                    float t = 0.0f;
+                    for (size_t i = 0; i < ws.size(); ++i) t += tmp[((size_t)y * w + first + i) * nc + c] * ws[i];
+                    t = t < 0.0f ? 0.0f : (t > 255.0f ? 255.0f : t);
+                    px[((size_t)y * mw + ox) * nc + c] = (uint8_t)std::round(t);
+                }
+        }
+    }
+    // to_luma8 / to_rgb8
+    for (size_t i = 0; i < n_out; ++i) {
+        const uint8_t* p = &px[i * nc];
+        const uint8_t g = nc == 1 ? p[0] : luma709(p[0], p[1], p[2]);
+        if (gray) gray[i] = g;
+        if (rgb)
+            for (int c = 0; c < 3; ++c) rgb[3 * i + c] = nc == 1 ? p[0] : p[c];
+    }
+}
+
 // mvs/src/lib.rs:245-251  percentile
 static double percentile(const std::vector<double>& s, double q) {
     if (s.empty()) return 0.0;

@@ -65,6 +65,12 @@ int orc_write_ply_binary(const char* path, const double* xyz, const uint8_t* rgb
 /* save_depth_vis (mvs/src/fuse.rs:241-268): the grey image and lo/hi. */
 void orc_depth_vis(const float* depth, int32_t w, int32_t h, uint8_t* out, float* lo_hi);
 
+/* load_views' image preparation (mvs/src/lib.rs:183-194): `image` 0.24
+ * resize_exact with the Triangle filter when (mw, mh) != (w, h), then
+ * to_luma8 / to_rgb8.  channels 1-4 (alpha dropped); gray mw*mh, rgb mw*mh*3. */
+void orc_resize_view(const uint8_t* img, int32_t w, int32_t h, int32_t channels, int32_t mw, int32_t mh,
+                     uint8_t* gray, uint8_t* rgb);
+
 /* Host glue of run_mvs; same output layout as rcmvs_plan.  has_depth
  * (nullable) marks views that have a depth map; NULL means "every view with
  * at least one source". */

@@ -52,6 +52,8 @@ def lib():
         L.orc_plan.argtypes = [vp, vp, i32, vp, vp, vp, vp, vp, vp]
         L.orc_depth_vis.argtypes = [vp, i32, i32, vp, vp]
         L.orc_depth_vis.restype = None
+        L.orc_resize_view.argtypes = [vp, i32, i32, i32, i32, i32, vp, vp]
+        L.orc_resize_view.restype = None
         _lib = L
     return _lib
 
@@ -175,6 +177,19 @@ def depth_vis(depth):
     lh = np.zeros(2, np.float32)
     lib().orc_depth_vis(d.ctypes.data, w, h, out.ctypes.data, lh.ctypes.data)
     return out, float(lh[0]), float(lh[1])
+
+
+def resize_view(img, mw, mh):
+    """load_views' image preparation on the CPU (lib.rs:183-194): (h, w) or
+    (h, w, c) u8 -> ((mh, mw) grey, (mh, mw, 3) RGB)."""
+    a = np.ascontiguousarray(img, dtype=np.uint8)
+    if a.ndim == 2:
+        a = a[:, :, None]
+    h, w, c = a.shape
+    gray = np.empty((mh, mw), np.uint8)
+    rgb = np.empty((mh, mw, 3), np.uint8)
+    lib().orc_resize_view(a.ctypes.data, w, h, c, mw, mh, gray.ctypes.data, rgb.ctypes.data)
+    return gray, rgb
 
 
 def write_ply_binary(path, xyz, rgb):

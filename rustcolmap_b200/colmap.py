@@ -14,12 +14,15 @@ Restates, for this path:
 Images: the reference decodes with the `image` crate (any format), resizes
 with its Triangle filter when the long side exceeds `max_dim`, and converts
 with `to_luma8` / `to_rgb8`.  Here PNG is decoded by a small decoder (8-bit
-grey, grey+alpha, RGB, RGBA; every filter type); other formats and any
-resize raise an error asking for images at working resolution (the Triangle
-filter is not restated).  RGB -> luma follows the `image` 0.24 conversion,
-(2126 R + 7152 G + 722 B) / 10000 in integers — not pinned here (the crate
-is not vendored); for grey input it is the identity.
+grey, grey+alpha, RGB, RGBA; every filter type; other formats raise an
+error).  A view whose working size differs from its camera's is resized on
+the GPU (rcmvs_resize_view: the `image` 0.24 Triangle resampler in f32, in
+the crate's order of operations).  RGB -> luma follows the `image`
+0.24 conversion, (2126 R + 7152 G + 722 B) / 10000 in integers; for grey
+input it is the identity.  Neither is pinned by reference outputs (the crate
+is not vendored).
 """
+import math
 import os
 import struct
 import zlib
@@ -328,10 +331,16 @@ def cam_from_rec(c, sx, sy):
     return Cam(f * s, cx * sx, cy * sy, k)
 
 
+def _round_half_away(x):
+    """f64::round for x >= 0 (Python's round() goes half to even)."""
+    f = math.floor(x)
+    return int(f) + (1 if x - f >= 0.5 else 0)
+
+
 def working_size(width, height, max_dim):
-    """mvs/src/lib.rs:165-167, :185-188."""
+    """mvs/src/lib.rs:155-157, :185-187."""
     s = min(float(max_dim) / float(max(width, height)), 1.0)
-    return max(int(round(width * s)), 16), max(int(round(height * s)), 16)
+    return max(_round_half_away(width * s), 16), max(_round_half_away(height * s), 16)
 
 
 # ------------------------------------------------------------------ images
@@ -405,10 +414,12 @@ def gray_rgb(img):
     return ((2126 * r + 7152 * gg + 722 * b) // 10000).astype(np.uint8), rgb
 
 
-def load_views(rec, image_dir, opts=None):
+def load_views(rec, image_dir, opts=None, ctx=None):
     """mvs/src/lib.rs:158-221 (views in rec.images order) plus the sparse
     points with tracks as view indices (entries of unknown images dropped,
-    as lib.rs:227-231 skips them).  Returns (views, SparseModel)."""
+    as lib.rs:227-231 skips them).  Images whose camera is larger than
+    max_dim are resized on the GPU of `ctx` (the default context when None).
+    Returns (views, SparseModel)."""
     opts = opts or MvsOptions()
     views = []
     for im in rec.images:
@@ -422,10 +433,11 @@ def load_views(rec, image_dir, opts=None):
             img = read_png(path)
         except OSError as e:
             raise RcmvsError(-5, f"cannot open {path}: {e}")
-        if (mw, mh) != (c.width, c.height):
-            raise RcmvsError(-4, f"{im.name}: the view would be resized to {mw}x{mh} (max_dim {opts.max_dim}); "
-                                 "resizing is not built, provide images at working resolution")
-        g, rgb = gray_rgb(img)
+        if (mw, mh) != (c.width, c.height):  # lib.rs:188-190
+            from . import mvs
+            g, rgb = mvs.resize_view(img, mw, mh, ctx)
+        else:
+            g, rgb = gray_rgb(img)
         views.append(ViewData(im.name, im.image_id, g.shape[1], g.shape[0], cam, quat_to_rot(im.qvec),
                               np.array(im.tvec, np.float64), g, rgb))
     if len(views) < 2:
@@ -446,7 +458,7 @@ def run_mvs_colmap(sparse_dir, image_dir, out_dir, opts=None, ctx=None, net=None
     <out_dir>/dense.  Returns (MvsStats, xyz, rgb)."""
     from . import mvs
     opts = opts or MvsOptions()
-    views, sparse = load_views(read_dir_any(sparse_dir), image_dir, opts)
+    views, sparse = load_views(read_dir_any(sparse_dir), image_dir, opts, ctx)
     if log:
         log(f"mvs: loaded {len(views)} views at working resolution (max_dim {opts.max_dim})")
     return mvs.run_mvs(views, sparse, opts, out_dir=out_dir, ctx=ctx, log=log, net=net)

@@ -197,6 +197,34 @@ def depth_vis(depth, ctx=None):
     return out, float(lh[0]), float(lh[1])
 
 
+def working_size(w, h, max_dim):
+    """Working resolution of a w x h camera (lib.rs:155-157, :185-187)."""
+    mw, mh = C.c_int32(), C.c_int32()
+    rc = _lib.mvs().rcmvs_working_size(w, h, max_dim, C.byref(mw), C.byref(mh))
+    if rc != 0:
+        raise RcmvsError(rc, f"working_size: bad size {w}x{h}")
+    return mw.value, mh.value
+
+
+def resize_view(img, mw, mh, ctx=None):
+    """load_views' image preparation (lib.rs:183-194) on the GPU: the `image`
+    crate's Triangle resize_exact to (mw, mh) when the size differs, then
+    to_luma8 / to_rgb8.  (h, w) or (h, w, c) u8 -> ((mh, mw) grey,
+    (mh, mw, 3) RGB)."""
+    ctx = _ctx(ctx)
+    a = np.ascontiguousarray(img, dtype=np.uint8)
+    if a.ndim == 2:
+        a = a[:, :, None]
+    h, w, c = a.shape
+    if mw <= 0 or mh <= 0:
+        raise RcmvsError(-1, f"resize_view: bad size {mw}x{mh}")
+    gray = np.empty((mh, mw), np.uint8)
+    rgb = np.empty((mh, mw, 3), np.uint8)
+    ctx.check(ctx._L.rcmvs_resize_view(ctx.ptr, a.ctypes.data, w, h, c, mw, mh, gray.ctypes.data,
+                                       rgb.ctypes.data))
+    return gray, rgb
+
+
 def write_png_gray(path, img):
     """8-bit greyscale PNG (the file save_depth_vis writes)."""
     img = np.ascontiguousarray(img, dtype=np.uint8)

@@ -140,6 +140,20 @@ def test_working_size():
     assert colmap.working_size(1920, 1080, 4096) == (1920, 1080)
     assert colmap.working_size(1920, 1080, 960) == (960, 540)
     assert colmap.working_size(1000, 10, 100) == (100, 16)
+    # f64::round goes half away from zero: 997 * 0.5 = 498.5 -> 499
+    assert colmap.working_size(1000, 997, 500) == (500, 499)
+    assert colmap.working_size(3, 3, 0) == (16, 16)
+
+
+def test_working_size_c_abi_agrees():
+    """rcmvs_working_size (host C, no GPU) against the Python restatement."""
+    rng = np.random.default_rng(3)
+    cases = [(1000, 997, 500), (4000, 3000, 900), (17, 9, 1), (8388608, 3, 4096)]
+    cases += [tuple(int(v) for v in rng.integers(1, 9000, 2)) + (int(rng.integers(0, 5000)),) for _ in range(300)]
+    for w, h, m in cases:
+        assert mvs.working_size(w, h, m) == colmap.working_size(w, h, m), (w, h, m)
+    with pytest.raises(mvs.RcmvsError):
+        mvs.working_size(0, 5, 100)
 
 
 def _png(img, filt):
@@ -232,9 +246,6 @@ def test_load_views_from_written_model(tmp_path):
     assert np.array_equal(sparse.xyz, sc.sparse.xyz)
     assert np.array_equal(sparse.track_offsets, sc.sparse.track_offsets)
     assert np.array_equal(sparse.track_views, sc.sparse.track_views)
-    # a model larger than max_dim would need the (not built) resize
-    with pytest.raises(RcmvsError, match="resiz"):
-        colmap.load_views(rec, str(tmp_path / "images"), MvsOptions(max_dim=64))
     rec.images[0].camera_id = 99
     with pytest.raises(RcmvsError, match="missing camera"):
         colmap.load_views(rec, str(tmp_path / "images"), MvsOptions(max_dim=4096))
@@ -255,3 +266,28 @@ def test_run_mvs_colmap_end_to_end(tmp_path):
     for f in ("dense.ply", "mvs_stats.json", "dense_web.json"):
         assert (tmp_path / "out" / "dense" / f).exists()
     assert len(os.listdir(tmp_path / "out" / "dense" / "depth_vis")) > 0
+
+
+@pytest.mark.gpu
+def test_load_views_resizes_above_max_dim(tmp_path):
+    """Cameras larger than max_dim: views come out at the working size, with
+    the oracle's resized images and scaled cameras, and the whole run works."""
+    from oracle import oracle
+    sc = _tiny()
+    write_scene_model(sc, str(tmp_path / "sparse"), str(tmp_path / "images"))
+    rec = colmap.read_dir_any(str(tmp_path / "sparse"))
+    ctx = mvs.Context(0)
+    opts = MvsOptions(max_dim=70, num_sources=2, sweeps=1, num_hyp=16, min_consistent=1)
+    views, _ = colmap.load_views(rec, str(tmp_path / "images"), opts, ctx=ctx)
+    for a, b in zip(views, sc.views):
+        mw, mh = colmap.working_size(b.w, b.h, 70)
+        assert (a.w, a.h) == (mw, mh) == (70, 47)
+        g, rgb = oracle.resize_view(b.gray, mw, mh)
+        assert np.array_equal(a.gray, g) and np.array_equal(a.rgb, rgb)
+        want = colmap.cam_from_rec(colmap.Camera(1, colmap.SIMPLE_RADIAL, b.w, b.h,
+                                                 [b.cam.f, b.cam.cx, b.cam.cy, b.cam.k]), mw / b.w, mh / b.h)
+        assert (a.cam.f, a.cam.cx, a.cam.cy, a.cam.k) == (want.f, want.cx, want.cy, want.k)
+    st, _, _ = colmap.run_mvs_colmap(str(tmp_path / "sparse"), str(tmp_path / "images"), str(tmp_path / "out"),
+                                       opts, ctx=ctx)
+    ctx.close()
+    assert st.views == len(sc.views) and st.views_with_depth > 0
