@@ -225,6 +225,27 @@ int rcmvs_fuse_depth_maps(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_vie
                           const double* sparse_xyz, uint64_t n_sparse,
                           const rcmvs_options* opts, rcmvs_points* out);
 
+/* Fusion in two halves, for a scene whose reference views are spread over
+ * several processes (no reference counterpart; in the reference both halves
+ * run inside `fuse::fuse_depth_maps`).  rcmvs_fuse_candidates runs the
+ * consistency check of fuse.rs:96-167 for the pixels of ref_views only
+ * (n_ref entries; views without a depth map contribute nothing) against
+ * every view's depth map, and returns their candidates, the averaged point
+ * and the reference pixel's colour, in view-then-pixel order (`out`,
+ * library-allocated; per_view, nullable, n_views entries, gets each view's
+ * count).  rcmvs_fuse_reduce is the voxel dedup of fuse.rs:72-92, 176-214 over
+ * candidates given in the reference's accumulation order (view, then pixel):
+ * the candidates of all reference views, concatenated in view order, give
+ * exactly the cloud of rcmvs_fuse_depth_maps. */
+int rcmvs_fuse_candidates(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views,
+                          const float* const* depth_maps,
+                          const int32_t* order_offsets, const int32_t* order,
+                          const int32_t* ref_views, int32_t n_ref,
+                          const rcmvs_options* opts, rcmvs_points* out, uint64_t* per_view);
+int rcmvs_fuse_reduce(rcmvs_ctx* ctx, const double* xyz, const uint8_t* rgb, uint64_t n,
+                      const double* sparse_xyz, uint64_t n_sparse,
+                      const rcmvs_options* opts, rcmvs_points* out);
+
 /* Binary little-endian PLY, byte-identical to `fuse::write_ply_binary`
  * (mvs/src/fuse.rs:222-239). */
 int rcmvs_write_ply_binary(const char* path, const double* xyz, const uint8_t* rgb,
@@ -305,6 +326,10 @@ int rcmvs_tune_set(rcmvs_ctx* ctx, const rcmvs_tune_entry* entries, int32_t n);
 int rcmvs_scene_fuse(rcmvs_ctx* ctx, rcmvs_scene* scene, const int32_t* order_offsets,
                      const int32_t* order, const double* sparse_xyz, uint64_t n_sparse,
                      const rcmvs_options* opts, uint64_t* n_points_out);
+/* rcmvs_fuse_candidates on the scene's device-resident depth maps. */
+int rcmvs_scene_fuse_candidates(rcmvs_ctx* ctx, rcmvs_scene* scene, const int32_t* order_offsets,
+                                const int32_t* order, const int32_t* ref_views, int32_t n_ref,
+                                const rcmvs_options* opts, rcmvs_points* out, uint64_t* per_view);
 /* Copies one view's maps to host buffers (any pointer may be NULL). */
 int rcmvs_scene_get_depth(rcmvs_ctx* ctx, rcmvs_scene* scene, int32_t view, float* depth,
                           float* cost, float* normal);

@@ -572,22 +572,8 @@ static double sample_depth(const float* depth, int32_t w, int32_t h, double u, d
     return 0.0;
 }
 
-// mvs/src/fuse.rs:64-215  fuse_depth_maps (+ the reprojection extension,
-// off unless opts->reproj_px > 0)
-int orc_fuse_depth_maps(const rcmvs_view* views, int32_t n_views, const float* const* depth_maps,
-                        const int32_t* order_offsets, const int32_t* order,
-                        const double* sparse_xyz, uint64_t n_sparse, const rcmvs_options* opts,
-                        double** xyz_out, uint8_t** rgb_out, uint64_t* n_out,
-                        uint64_t* n_candidates_out, int32_t nthreads) {
-    if (!views || n_views <= 0 || !depth_maps || !order_offsets || !opts || !xyz_out || !rgb_out ||
-        !n_out || n_sparse == 0 || !sparse_xyz)
-        return RCMVS_E_ARG;
-    for (int v = 0; v < n_views; ++v) {
-        for (int32_t q = order_offsets[v]; q < order_offsets[v + 1]; ++q)
-            if (order[q] < 0 || order[q] >= n_views || !depth_maps[order[q]]) return RCMVS_E_ARG;
-        if (depth_maps[v] && !views[v].rgb) return RCMVS_E_ARG;
-    }
-    // voxel cell from the robust sparse bbox (fuse.rs:72-92)
+// mvs/src/fuse.rs:72-92: robust sparse bounding-box diagonal -> voxel cell
+static double voxel_cell(const double* sparse_xyz, uint64_t n_sparse, double voxel_rel) {
     double ext[3];
     for (int a = 0; a < 3; ++a) {
         std::vector<double> ax(n_sparse);
@@ -599,13 +585,21 @@ int orc_fuse_depth_maps(const rcmvs_view* views, int32_t n_views, const float* c
         ext[a] = ax[ihi] - ax[ilo];
     }
     double diag = std::sqrt(ext[0] * ext[0] + ext[1] * ext[1] + ext[2] * ext[2]);
-    double cell = std::fmax(diag * opts->voxel_rel, 1e-9);
+    return std::fmax(diag * voxel_rel, 1e-9);
+}
 
-    // per-view candidates (fuse.rs:96-167)
-    std::vector<std::vector<std::array<double, 6>>> per_view(n_views);
+using Cand = std::array<double, 6>;  // averaged point, reference colour
+
+// mvs/src/fuse.rs:96-167 for the views v with a depth map and ref_mask[v]
+// (every such view when ref_mask is NULL): per view, its candidates in
+// pixel order.
+static void fuse_candidates(const rcmvs_view* views, int32_t n_views, const float* const* depth_maps,
+                            const int32_t* order_offsets, const int32_t* order, const uint8_t* ref_mask,
+                            const rcmvs_options* opts, std::vector<std::vector<Cand>>& per_view, int32_t nthreads) {
+    per_view.assign(n_views, {});
     par_for(n_views, nthreads, [&](int64_t ri, int) {
         const float* dm = depth_maps[ri];
-        if (!dm) return;
+        if (!dm || (ref_mask && !ref_mask[ri])) return;
         const rcmvs_view& v = views[ri];
         auto& out = per_view[ri];
         for (int32_t py = 0; py < v.h; ++py)
@@ -651,36 +645,35 @@ int orc_fuse_depth_maps(const rcmvs_view* views, int32_t n_views, const float* c
                 }
                 if (n_cons < opts->min_consistent) continue;
                 double m = (double)(n_cons + 1);
-                std::array<double, 6> pt = {acc[0] / m, acc[1] / m, acc[2] / m,
-                                            (double)v.rgb[3 * i], (double)v.rgb[3 * i + 1],
-                                            (double)v.rgb[3 * i + 2]};
-                out.push_back(pt);
+                out.push_back(Cand{acc[0] / m, acc[1] / m, acc[2] / m, (double)v.rgb[3 * i],
+                                   (double)v.rgb[3 * i + 1], (double)v.rgb[3 * i + 2]});
             }
     });
+}
 
-    // voxel dedup in view-then-pixel order (fuse.rs:176-214)
+// mvs/src/fuse.rs:176-214: voxel dedup, members accumulated in the order
+// given (the reference's view-then-pixel order); output in key order.
+static int fuse_reduce(const std::vector<const Cand*>& cands, double cell, double** xyz_out, uint8_t** rgb_out,
+                       uint64_t* n_out) {
     struct Fused {
         double x = 0, y = 0, z = 0;
         uint16_t r = 0, g = 0, b = 0;
         uint32_t n = 0;
     };
     std::map<std::tuple<int64_t, int64_t, int64_t>, Fused> vox;
-    uint64_t n_cand = 0;
-    for (auto& vp : per_view)
-        for (auto& p : vp) {
-            ++n_cand;
-            auto key = std::make_tuple(f64_to_i64(std::floor(p[0] / cell)),
-                                       f64_to_i64(std::floor(p[1] / cell)),
-                                       f64_to_i64(std::floor(p[2] / cell)));
-            Fused& e = vox[key];
-            e.x += p[0];
-            e.y += p[1];
-            e.z += p[2];
-            e.r = (uint16_t)(e.r + (uint16_t)p[3]);
-            e.g = (uint16_t)(e.g + (uint16_t)p[4]);
-            e.b = (uint16_t)(e.b + (uint16_t)p[5]);
-            e.n += 1;
-        }
+    for (const Cand* pp : cands) {
+        const Cand& p = *pp;
+        auto key = std::make_tuple(f64_to_i64(std::floor(p[0] / cell)), f64_to_i64(std::floor(p[1] / cell)),
+                                   f64_to_i64(std::floor(p[2] / cell)));
+        Fused& e = vox[key];
+        e.x += p[0];
+        e.y += p[1];
+        e.z += p[2];
+        e.r = (uint16_t)(e.r + (uint16_t)p[3]);
+        e.g = (uint16_t)(e.g + (uint16_t)p[4]);
+        e.b = (uint16_t)(e.b + (uint16_t)p[5]);
+        e.n += 1;
+    }
     uint64_t n = vox.size();
     double* xyz = (double*)std::malloc(sizeof(double) * 3 * (n ? n : 1));
     uint8_t* rgb = (uint8_t*)std::malloc(3 * (n ? n : 1));
@@ -704,8 +697,87 @@ int orc_fuse_depth_maps(const rcmvs_view* views, int32_t n_views, const float* c
     *xyz_out = xyz;
     *rgb_out = rgb;
     *n_out = n;
-    if (n_candidates_out) *n_candidates_out = n_cand;
     return RCMVS_OK;
+}
+
+static int check_fuse_args(const rcmvs_view* views, int32_t n_views, const float* const* depth_maps,
+                           const int32_t* order_offsets, const int32_t* order) {
+    for (int v = 0; v < n_views; ++v) {
+        for (int32_t q = order_offsets[v]; q < order_offsets[v + 1]; ++q)
+            if (order[q] < 0 || order[q] >= n_views || !depth_maps[order[q]]) return RCMVS_E_ARG;
+        if (depth_maps[v] && !views[v].rgb) return RCMVS_E_ARG;
+    }
+    return RCMVS_OK;
+}
+
+// mvs/src/fuse.rs:64-215  fuse_depth_maps (+ the reprojection extension,
+// off unless opts->reproj_px > 0)
+int orc_fuse_depth_maps(const rcmvs_view* views, int32_t n_views, const float* const* depth_maps,
+                        const int32_t* order_offsets, const int32_t* order,
+                        const double* sparse_xyz, uint64_t n_sparse, const rcmvs_options* opts,
+                        double** xyz_out, uint8_t** rgb_out, uint64_t* n_out,
+                        uint64_t* n_candidates_out, int32_t nthreads) {
+    if (!views || n_views <= 0 || !depth_maps || !order_offsets || !opts || !xyz_out || !rgb_out ||
+        !n_out || n_sparse == 0 || !sparse_xyz)
+        return RCMVS_E_ARG;
+    if (check_fuse_args(views, n_views, depth_maps, order_offsets, order)) return RCMVS_E_ARG;
+    const double cell = voxel_cell(sparse_xyz, n_sparse, opts->voxel_rel);
+    std::vector<std::vector<Cand>> per_view;
+    fuse_candidates(views, n_views, depth_maps, order_offsets, order, nullptr, opts, per_view, nthreads);
+    std::vector<const Cand*> all;
+    for (auto& vp : per_view)
+        for (auto& p : vp) all.push_back(&p);
+    if (n_candidates_out) *n_candidates_out = all.size();
+    return fuse_reduce(all, cell, xyz_out, rgb_out, n_out);
+}
+
+int orc_fuse_candidates(const rcmvs_view* views, int32_t n_views, const float* const* depth_maps,
+                        const int32_t* order_offsets, const int32_t* order, const uint8_t* ref_mask,
+                        const rcmvs_options* opts, double** xyz_out, uint8_t** rgb_out, uint64_t* n_out,
+                        uint64_t* per_view_out, int32_t nthreads) {
+    if (!views || n_views <= 0 || !depth_maps || !order_offsets || !opts || !xyz_out || !rgb_out || !n_out)
+        return RCMVS_E_ARG;
+    if (check_fuse_args(views, n_views, depth_maps, order_offsets, order)) return RCMVS_E_ARG;
+    std::vector<std::vector<Cand>> per_view;
+    fuse_candidates(views, n_views, depth_maps, order_offsets, order, ref_mask, opts, per_view, nthreads);
+    uint64_t n = 0;
+    for (auto& vp : per_view) n += vp.size();
+    double* xyz = (double*)std::malloc(sizeof(double) * 3 * (n ? n : 1));
+    uint8_t* rgb = (uint8_t*)std::malloc(3 * (n ? n : 1));
+    if (!xyz || !rgb) {
+        std::free(xyz);
+        std::free(rgb);
+        return RCMVS_E_NOMEM;
+    }
+    uint64_t o = 0;
+    for (int v = 0; v < n_views; ++v) {
+        if (per_view_out) per_view_out[v] = per_view[v].size();
+        for (const Cand& p : per_view[v]) {
+            for (int a = 0; a < 3; ++a) {
+                xyz[3 * o + a] = p[a];
+                rgb[3 * o + a] = (uint8_t)p[3 + a];
+            }
+            ++o;
+        }
+    }
+    *xyz_out = xyz;
+    *rgb_out = rgb;
+    *n_out = n;
+    return RCMVS_OK;
+}
+
+int orc_fuse_reduce(const double* xyz, const uint8_t* rgb, uint64_t n, const double* sparse_xyz, uint64_t n_sparse,
+                    const rcmvs_options* opts, double** xyz_out, uint8_t** rgb_out, uint64_t* n_out) {
+    if ((n > 0 && (!xyz || !rgb)) || !sparse_xyz || n_sparse == 0 || !opts || !xyz_out || !rgb_out || !n_out)
+        return RCMVS_E_ARG;
+    std::vector<Cand> c(n);
+    std::vector<const Cand*> all(n);
+    for (uint64_t i = 0; i < n; ++i) {
+        c[i] = Cand{xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], (double)rgb[3 * i], (double)rgb[3 * i + 1],
+                    (double)rgb[3 * i + 2]};
+        all[i] = &c[i];
+    }
+    return fuse_reduce(all, voxel_cell(sparse_xyz, n_sparse, opts->voxel_rel), xyz_out, rgb_out, n_out);
 }
 
 void orc_free(void* p) { std::free(p); }

@@ -57,6 +57,16 @@ int orc_fuse_depth_maps(const rcmvs_view* views, int32_t n_views,
                         const int32_t* order, const double* sparse_xyz, uint64_t n_sparse,
                         const rcmvs_options* opts, double** xyz_out, uint8_t** rgb_out,
                         uint64_t* n_out, uint64_t* n_candidates_out, int32_t nthreads);
+/* The two halves of orc_fuse_depth_maps.  Candidates (fuse.rs:96-167) of the
+ * views with a depth map and ref_mask[v] != 0 (all when ref_mask is NULL), in
+ * view-then-pixel order; per_view (nullable) gets each view's count. */
+int orc_fuse_candidates(const rcmvs_view* views, int32_t n_views, const float* const* depth_maps,
+                        const int32_t* order_offsets, const int32_t* order, const uint8_t* ref_mask,
+                        const rcmvs_options* opts, double** xyz_out, uint8_t** rgb_out, uint64_t* n_out,
+                        uint64_t* per_view, int32_t nthreads);
+/* Voxel dedup (fuse.rs:72-92, 176-214) of candidates in accumulation order. */
+int orc_fuse_reduce(const double* xyz, const uint8_t* rgb, uint64_t n, const double* sparse_xyz, uint64_t n_sparse,
+                    const rcmvs_options* opts, double** xyz_out, uint8_t** rgb_out, uint64_t* n_out);
 void orc_free(void* p);
 
 int orc_write_ply_binary(const char* path, const double* xyz, const uint8_t* rgb,

@@ -52,6 +52,8 @@ def lib():
         L.orc_plan.argtypes = [vp, vp, i32, vp, vp, vp, vp, vp, vp]
         L.orc_depth_vis.argtypes = [vp, i32, i32, vp, vp]
         L.orc_depth_vis.restype = None
+        L.orc_fuse_candidates.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, i32]
+        L.orc_fuse_reduce.argtypes = [vp, vp, u64, vp, u64, vp, vp, vp, vp]
         L.orc_resize_view.argtypes = [vp, i32, i32, i32, i32, i32, vp, vp]
         L.orc_resize_view.restype = None
         _lib = L
@@ -190,6 +192,54 @@ def resize_view(img, mw, mh):
     rgb = np.empty((mh, mw, 3), np.uint8)
     lib().orc_resize_view(a.ctypes.data, w, h, c, mw, mh, gray.ctypes.data, rgb.ctypes.data)
     return gray, rgb
+
+
+def _take(xyz_p, rgb_p, nn):
+    xyz = np.ctypeslib.as_array((C.c_double * (3 * max(nn, 1))).from_address(xyz_p.value))[: 3 * nn]
+    rgb = np.ctypeslib.as_array((C.c_uint8 * (3 * max(nn, 1))).from_address(rgb_p.value))[: 3 * nn]
+    xyz = xyz.reshape(nn, 3).copy()
+    rgb = rgb.reshape(nn, 3).copy()
+    lib().orc_free(xyz_p)
+    lib().orc_free(rgb_p)
+    return xyz, rgb
+
+
+def fuse_candidates(views, depth_maps, order_offsets, order, ref_views, opts, nthreads=0):
+    """The consistency half of fuse_depth_maps for the pixels of ref_views:
+    (xyz (n,3) f64, rgb (n,3) u8, per-view counts), view-then-pixel order."""
+    va = _abi.view_array(views)
+    dms = [None if d is None else np.ascontiguousarray(d, dtype=np.float32) for d in depth_maps]
+    dptr = (C.c_void_p * len(views))(*[None if d is None else d.ctypes.data for d in dms])
+    off = np.ascontiguousarray(order_offsets, dtype=np.int32)
+    ordr = np.ascontiguousarray(order, dtype=np.int32)
+    if ordr.size == 0:
+        ordr = np.zeros(1, np.int32)
+    mask = np.zeros(len(views), np.uint8)
+    mask[list(ref_views)] = 1
+    per_view = np.zeros(len(views), np.uint64)
+    xyz_p, rgb_p = C.c_void_p(), C.c_void_p()
+    n = C.c_uint64()
+    o = opts.to_c()
+    rc = lib().orc_fuse_candidates(va, len(views), dptr, off.ctypes.data, ordr.ctypes.data, mask.ctypes.data,
+                                   C.byref(o), C.byref(xyz_p), C.byref(rgb_p), C.byref(n), per_view.ctypes.data,
+                                   nthreads)
+    _chk(rc, "fuse_candidates")
+    xyz, rgb = _take(xyz_p, rgb_p, n.value)
+    return xyz, rgb, per_view
+
+
+def fuse_reduce(xyz, rgb, sparse_xyz, opts):
+    """The voxel-dedup half of fuse_depth_maps over candidates in order."""
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+    rgb = np.ascontiguousarray(rgb, dtype=np.uint8).reshape(-1, 3)
+    sp = np.ascontiguousarray(sparse_xyz, dtype=np.float64)
+    xyz_p, rgb_p = C.c_void_p(), C.c_void_p()
+    n = C.c_uint64()
+    o = opts.to_c()
+    rc = lib().orc_fuse_reduce(xyz.ctypes.data, rgb.ctypes.data, len(xyz), sp.ctypes.data, len(sp), C.byref(o),
+                               C.byref(xyz_p), C.byref(rgb_p), C.byref(n))
+    _chk(rc, "fuse_reduce")
+    return _take(xyz_p, rgb_p, n.value)
 
 
 def write_ply_binary(path, xyz, rgb):

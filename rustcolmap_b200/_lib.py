@@ -80,6 +80,9 @@ def mvs():
         "rcmvs_write_png_gray": ([cp, vp, i32, i32], C.c_int),
         "rcmvs_working_size": ([i32, i32, C.c_uint32, vp, vp], C.c_int),
         "rcmvs_resize_view": ([vp, vp, i32, i32, i32, i32, i32, vp, vp], C.c_int),
+        "rcmvs_fuse_candidates": ([vp, vp, i32, vp, vp, vp, vp, i32, vp, vp, vp], C.c_int),
+        "rcmvs_fuse_reduce": ([vp, vp, vp, u64, vp, u64, vp, vp], C.c_int),
+        "rcmvs_scene_fuse_candidates": ([vp, vp, vp, vp, vp, i32, vp, vp, vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -121,5 +124,6 @@ _SIG_NAMES = [
     "rcmvs_net_get_params", "rcmvs_net_forward", "rcmvs_net_train_step", "rcmvs_scene_costvol",
     "rcmvs_scene_estimate_depth_learned", "rcmvs_run_mvs_learned", "rcmvs_autotune", "rcmvs_tune_table",
     "rcmvs_tune_set", "rcmvs_depth_vis", "rcmvs_scene_depth_vis", "rcmvs_write_png_gray",
-    "rcmvs_working_size", "rcmvs_resize_view",
+    "rcmvs_working_size", "rcmvs_resize_view", "rcmvs_fuse_candidates", "rcmvs_fuse_reduce",
+    "rcmvs_scene_fuse_candidates",
 ]

@@ -433,17 +433,10 @@ double voxel_cell(const double* xyz, uint64_t n, double voxel_rel) {
     return std::fmax(diag * voxel_rel, 1e-9);
 }
 
-}  // namespace
-
-extern "C" {
-
-int rcmvs_scene_fuse(rcmvs_ctx* ctx, rcmvs_scene* sc, const int32_t* order_offsets, const int32_t* order,
-                     const double* sparse_xyz, uint64_t n_sparse, const rcmvs_options* opts, uint64_t* n_points_out) {
-    if (!ctx || !sc || !order_offsets || !opts || !sparse_xyz || n_sparse == 0 || !n_points_out)
-        return fail(ctx, RCMVS_E_ARG, "rcmvs_scene_fuse: bad argument (sparse cloud must be non-empty)");
-    if (sc->ctx != ctx) return fail(ctx, RCMVS_E_ARG, "scene belongs to another context");
+// Fusion views of a scene; is_ref from ref_mask (every view when null).
+int fuse_views(rcmvs_ctx* ctx, rcmvs_scene* sc, const int32_t* order_offsets, const int32_t* order,
+               const std::vector<char>* ref_mask, std::vector<FuseView>& fv) {
     const int n = sc->n_views;
-    std::vector<FuseView> fv(n);
     for (int v = 0; v < n; ++v) {
         if (order_offsets[v] > order_offsets[v + 1] || order_offsets[v] < 0)
             return fail(ctx, RCMVS_E_ARG, "fusion order offsets must be non-decreasing");
@@ -452,8 +445,9 @@ int rcmvs_scene_fuse(rcmvs_ctx* ctx, rcmvs_scene* sc, const int32_t* order_offse
                 return fail(ctx, RCMVS_E_ARG, "fusion order names a view without a depth map");
     }
     bool any = false;
-    for (int v = 0; v < n; ++v) any |= sc->has_depth[v] != 0;
+    for (int v = 0; v < n; ++v) any |= sc->has_depth[v] != 0 && (!ref_mask || (*ref_mask)[v]);
     if (any && !sc->has_rgb) return fail(ctx, RCMVS_E_ARG, "fusion needs rgb for every view");
+    fv.assign(n, FuseView{});
     for (int v = 0; v < n; ++v) {
         FuseView& F = fv[v];
         std::memset(&F, 0, sizeof(F));
@@ -461,6 +455,7 @@ int rcmvs_scene_fuse(rcmvs_ctx* ctx, rcmvs_scene* sc, const int32_t* order_offse
         F.h = sc->views[v].h;
         F.off = sc->views[v].off;
         F.has_depth = sc->has_depth[v];
+        F.is_ref = ref_mask ? (*ref_mask)[v] : 1;
         F.order_begin = order_offsets[v];
         F.order_end = order_offsets[v + 1];
         const HostCam& c = sc->cams[v];
@@ -471,18 +466,122 @@ int rcmvs_scene_fuse(rcmvs_ctx* ctx, rcmvs_scene* sc, const int32_t* order_offse
         std::memcpy(F.R, c.R, sizeof(F.R));
         std::memcpy(F.t, c.t, sizeof(F.t));
     }
+    return RCMVS_OK;
+}
+
+// Library-allocated host copy of n points (device xyz / rgb) into out.
+int take_points(rcmvs_ctx* ctx, const double* d_xyz, const uint8_t* d_rgb, uint64_t n, rcmvs_points* out) {
+    out->xyz = (double*)std::malloc(24 * std::max<uint64_t>(n, 1));
+    out->rgb = (uint8_t*)std::malloc(3 * std::max<uint64_t>(n, 1));
+    if (!out->xyz || !out->rgb) {
+        rcmvs_points_free(out);
+        return fail(ctx, RCMVS_E_NOMEM, "host allocation of the point cloud failed");
+    }
+    out->n = n;
+    if (n) {
+        CK(cudaMemcpyAsync(out->xyz, d_xyz, 24 * n, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(out->rgb, d_rgb, 3 * n, cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    return RCMVS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rcmvs_scene_fuse(rcmvs_ctx* ctx, rcmvs_scene* sc, const int32_t* order_offsets, const int32_t* order,
+                     const double* sparse_xyz, uint64_t n_sparse, const rcmvs_options* opts, uint64_t* n_points_out) {
+    if (!ctx || !sc || !order_offsets || !opts || !sparse_xyz || n_sparse == 0 || !n_points_out)
+        return fail(ctx, RCMVS_E_ARG, "rcmvs_scene_fuse: bad argument (sparse cloud must be non-empty)");
+    if (sc->ctx != ctx) return fail(ctx, RCMVS_E_ARG, "scene belongs to another context");
+    const int n = sc->n_views;
+    std::vector<FuseView> fv;
+    int rc = fuse_views(ctx, sc, order_offsets, order, nullptr, fv);
+    if (rc) return rc;
     const double cell = voxel_cell(sparse_xyz, n_sparse, opts->voxel_rel);
     CK(cudaSetDevice(ctx->device));
     FuseResult res{0, 0};
     std::string err;
-    int rc = fuse_device(sc->arena, fv.data(), n, order, order_offsets[n], sc->depth, sc->rgb, cell,
-                         opts->min_consistent, opts->depth_diff, opts->reproj_px, &sc->d_pts_xyz, &sc->d_pts_rgb,
-                         &sc->d_ply, &res, ctx->stream, &err, ctx->hook());
+    rc = fuse_device(sc->arena, fv.data(), n, order, order_offsets[n], sc->depth, sc->rgb, cell,
+                     opts->min_consistent, opts->depth_diff, opts->reproj_px, &sc->d_pts_xyz, &sc->d_pts_rgb,
+                     &sc->d_ply, &res, ctx->stream, &err, ctx->hook());
     if (rc) return fail(ctx, rc, err);
     sc->n_points = res.n_points;
     sc->n_candidates = res.n_candidates;
     *n_points_out = res.n_points;
     return RCMVS_OK;
+}
+
+int rcmvs_scene_fuse_candidates(rcmvs_ctx* ctx, rcmvs_scene* sc, const int32_t* order_offsets, const int32_t* order,
+                                const int32_t* ref_views, int32_t n_ref, const rcmvs_options* opts,
+                                rcmvs_points* out, uint64_t* per_view) {
+    if (!ctx || !sc || !order_offsets || !opts || !out || n_ref < 0 || (n_ref > 0 && !ref_views))
+        return fail(ctx, RCMVS_E_ARG, "rcmvs_scene_fuse_candidates: bad argument");
+    if (sc->ctx != ctx) return fail(ctx, RCMVS_E_ARG, "scene belongs to another context");
+    out->n = 0;
+    out->xyz = nullptr;
+    out->rgb = nullptr;
+    const int n = sc->n_views;
+    std::vector<char> mask(n, 0);
+    for (int i = 0; i < n_ref; ++i) {
+        if (ref_views[i] < 0 || ref_views[i] >= n) return fail(ctx, RCMVS_E_ARG, "reference view out of range");
+        mask[ref_views[i]] = 1;
+    }
+    std::vector<FuseView> fv;
+    int rc = fuse_views(ctx, sc, order_offsets, order, &mask, fv);
+    if (rc) return rc;
+    CK(cudaSetDevice(ctx->device));
+    std::string err;
+    const uint32_t* cand = nullptr;
+    const double* pts = nullptr;
+    uint32_t n_cand = 0;
+    rc = fuse_candidates_device(sc->arena, fv.data(), n, order, order_offsets[n], sc->depth, opts->min_consistent,
+                                opts->depth_diff, opts->reproj_px, &cand, &n_cand, &pts, ctx->stream, &err,
+                                ctx->hook());
+    if (rc) return fail(ctx, rc, err);
+    double* gx = nullptr;
+    uint8_t* gc = nullptr;
+    if (n_cand > 0) {
+        rc = fuse_gather_device(sc->arena, cand, n_cand, pts, sc->rgb, &gx, &gc, ctx->stream, &err);
+        if (rc) return fail(ctx, rc, err);
+    }
+    if (per_view) {
+        // candidates are ascending global pixel indices; views are laid out
+        // in order, so each view's candidates form one run
+        std::vector<uint32_t> idx(n_cand);
+        if (n_cand) CK(cudaMemcpyAsync(idx.data(), cand, 4 * (size_t)n_cand, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        size_t c = 0;
+        for (int v = 0; v < n; ++v) {
+            const uint64_t end = (uint64_t)sc->views[v].off + (uint64_t)sc->views[v].w * sc->views[v].h;
+            uint64_t k = 0;
+            while (c < idx.size() && idx[c] < end) {
+                ++c;
+                ++k;
+            }
+            per_view[v] = k;
+        }
+    }
+    return take_points(ctx, gx, gc, n_cand, out);
+}
+
+int rcmvs_fuse_reduce(rcmvs_ctx* ctx, const double* xyz, const uint8_t* rgb, uint64_t n, const double* sparse_xyz,
+                      uint64_t n_sparse, const rcmvs_options* opts, rcmvs_points* out) {
+    if (!ctx || (n > 0 && (!xyz || !rgb)) || !sparse_xyz || n_sparse == 0 || !opts || !out)
+        return fail(ctx, RCMVS_E_ARG, "rcmvs_fuse_reduce: bad argument (sparse cloud must be non-empty)");
+    out->n = 0;
+    out->xyz = nullptr;
+    out->rgb = nullptr;
+    CK(cudaSetDevice(ctx->device));
+    const double cell = voxel_cell(sparse_xyz, n_sparse, opts->voxel_rel);
+    double* dx = nullptr;
+    uint8_t *dc = nullptr, *dp = nullptr;
+    uint64_t np = 0;
+    std::string err;
+    int rc = fuse_reduce_host(ctx->arena, xyz, rgb, n, cell, &dx, &dc, &dp, &np, ctx->stream, &err, ctx->hook());
+    if (rc) return fail(ctx, rc, err);
+    return take_points(ctx, dx, dc, np, out);
 }
 
 int rcmvs_scene_get_points(rcmvs_ctx* ctx, rcmvs_scene* sc, double* xyz, uint8_t* rgb, uint8_t* ply_body) {
@@ -663,6 +762,32 @@ int rcmvs_fuse_depth_maps(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_vie
         }
         out->n = np;
         return rcmvs_scene_get_points(ctx, sc, out->xyz, out->rgb, nullptr);
+    };
+    rc = body();
+    rcmvs_scene_destroy(sc);
+    return rc;
+}
+
+int rcmvs_fuse_candidates(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views, const float* const* depth_maps,
+                          const int32_t* order_offsets, const int32_t* order, const int32_t* ref_views,
+                          int32_t n_ref, const rcmvs_options* opts, rcmvs_points* out, uint64_t* per_view) {
+    if (!ctx || !views || n_views <= 0 || !depth_maps || !order_offsets || !opts || !out)
+        return fail(ctx, RCMVS_E_ARG, "rcmvs_fuse_candidates: bad argument");
+    out->n = 0;
+    out->xyz = nullptr;
+    out->rgb = nullptr;
+    rcmvs_scene* sc = nullptr;
+    int rc = rcmvs_scene_create(ctx, views, n_views, &sc);
+    if (rc) return rc;
+    auto body = [&]() -> int {
+        for (int v = 0; v < n_views; ++v) {
+            if (!depth_maps[v]) continue;
+            const DevView& V = sc->views[v];
+            CK(cudaMemcpyAsync(sc->depth + V.off, depth_maps[v], 4 * (size_t)V.w * V.h, cudaMemcpyHostToDevice,
+                               ctx->stream));
+            sc->has_depth[v] = 1;
+        }
+        return rcmvs_scene_fuse_candidates(ctx, sc, order_offsets, order, ref_views, n_ref, opts, out, per_view);
     };
     rc = body();
     rcmvs_scene_destroy(sc);

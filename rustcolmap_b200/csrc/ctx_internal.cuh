@@ -120,7 +120,8 @@ struct rcmvs_scene {
 namespace rcmvs {
 
 // Arena slots of a scene shared by the translation units (the others are
-// private to capi.cu 2-10, fuse.cu 16-37, learned_api.cu 40-47 and depthvis.cu 50-55).
+// private to capi.cu 2-10, fuse.cu 16-37 and 70-74, learned_api.cu 40-47, depthvis.cu 50-55
+// and resize.cu 60-68).
 constexpr int kSlotJobs = 0, kSlotJobStart = 1, kSlotQueue = 11, kSlotTuneJobs = 12, kSlotTuneStart = 13;
 
 // mvs/src/stereo.rs:131-132: source pose relative to the reference, f64

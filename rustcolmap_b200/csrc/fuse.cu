@@ -311,6 +311,23 @@ struct CountingIt {
     using value_type = uint32_t;
 };
 
+__global__ void iota_kernel(uint32_t* __restrict__ out, uint32_t n) {
+    for (uint32_t i = blockIdx.x * FT + threadIdx.x; i < n; i += gridDim.x * FT) out[i] = i;
+}
+
+// Compacts the candidates' points and reference colours in list order.
+__global__ void gather_cand_kernel(const uint32_t* __restrict__ cand, uint32_t n, const double* __restrict__ pts,
+                                   const uint8_t* __restrict__ rgb, double* __restrict__ out_xyz,
+                                   uint8_t* __restrict__ out_rgb) {
+    for (uint32_t c = blockIdx.x * FT + threadIdx.x; c < n; c += gridDim.x * FT) {
+        const size_t g = cand[c];
+        for (int a = 0; a < 3; ++a) {
+            out_xyz[3 * (size_t)c + a] = pts[3 * g + a];
+            out_rgb[3 * (size_t)c + a] = rgb[3 * g + a];
+        }
+    }
+}
+
 }  // namespace
 
 #define FCK(x)                                                                   \
@@ -322,27 +339,33 @@ struct CountingIt {
         }                                                                        \
     } while (0)
 
-// Arena slots used by fusion (the stereo path uses slots below 16).
+// Arena slots used by fusion (the stereo path uses slots below 16): 16-37
+// and 70-74.
 enum {
     S_FLAG = 16, S_PTS, S_CAND, S_NSEL, S_KMIN, S_KEYS, S_VALS, S_KEYS2, S_VALS2, S_RUNKEY, S_RUNLEN,
     S_RUNOFF, S_NRUNS, S_TEMP, S_OUTXYZ, S_OUTRGB, S_PLY, S_FVIEWS, S_ORDER, S_BLK, S_WORK, S_VOFF
 };
+enum { S_INXYZ = 70, S_INRGB, S_IOTA, S_GXYZ, S_GRGB };
 
-int fuse_device(DeviceArena& A, const FuseView* h_views, int n_views, const int32_t* h_order, int n_order,
-                const float* depth, const uint8_t* rgb, double cell, uint32_t min_consistent, double depth_diff,
-                double reproj_px, double** d_xyz, uint8_t** d_rgb, uint8_t** d_ply, FuseResult* res,
-                cudaStream_t st, std::string* err, const SpanHook& hook) {
-    // pixel-block table over views that have a depth map
+unsigned fgrid(uint32_t n) { return (unsigned)std::max<uint32_t>(1, std::min<uint32_t>((n + FT - 1) / FT, 148u * 8u)); }
+
+int fuse_candidates_device(DeviceArena& A, const FuseView* h_views, int n_views, const int32_t* h_order,
+                           int n_order, const float* depth, uint32_t min_consistent, double depth_diff,
+                           double reproj_px, const uint32_t** d_cand, uint32_t* n_cand_out, const double** d_pts,
+                           cudaStream_t st, std::string* err, const SpanHook& hook) {
+    // pixel-block table over the reference views that have a depth map
     std::vector<int32_t> blk_start, blk_view;
     int64_t total_blocks = 0, total_px = 0;
     for (int v = 0; v < n_views; ++v) {
         total_px = std::max<int64_t>(total_px, h_views[v].off + (int64_t)h_views[v].w * h_views[v].h);
-        if (!h_views[v].has_depth) continue;
+        if (!h_views[v].has_depth || !h_views[v].is_ref) continue;
         blk_start.push_back((int32_t)total_blocks);
         blk_view.push_back(v);
         total_blocks += ((int64_t)h_views[v].w * h_views[v].h + FT - 1) / FT;
     }
-    res->n_candidates = res->n_points = 0;
+    *n_cand_out = 0;
+    *d_cand = nullptr;
+    *d_pts = nullptr;
     if (blk_view.empty() || total_px == 0) return RCMVS_OK;
     if (total_blocks > INT32_MAX || total_px > (int64_t)UINT32_MAX) {
         *err = "fusion: scene too large for 32-bit candidate indices";
@@ -400,9 +423,20 @@ int fuse_device(DeviceArena& A, const FuseView* h_views, int n_views, const int3
     uint32_t n_cand = 0;
     FCK(cudaMemcpyAsync(&n_cand, p_nsel, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     FCK(cudaStreamSynchronize(st));
-    res->n_candidates = n_cand;
-    if (n_cand == 0) return RCMVS_OK;
+    *n_cand_out = n_cand;
+    *d_cand = (const uint32_t*)p_cand;
+    *d_pts = pts;
+    return RCMVS_OK;
+}
 
+int fuse_reduce_device(DeviceArena& A, const uint32_t* d_cand, uint32_t n_cand, const double* pts,
+                       const uint8_t* rgb, double cell, double** d_xyz, uint8_t** d_rgb, uint8_t** d_ply,
+                       uint64_t* n_points, cudaStream_t st, std::string* err, const SpanHook& hook) {
+    *n_points = 0;
+    if (n_cand == 0) return RCMVS_OK;
+    const void* p_cand = d_cand;
+    void* p_temp;
+    size_t tb = 0;
     // voxel keys, packed 21 bits per axis
     void* p_kmin;
     FCK(A.get(S_KMIN, sizeof(long long) * 6, &p_kmin));
@@ -469,8 +503,58 @@ int fuse_device(DeviceArena& A, const FuseView* h_views, int n_views, const int3
     *d_xyz = (double*)p_oxyz;
     *d_rgb = (uint8_t*)p_orgb;
     *d_ply = (uint8_t*)p_ply;
-    res->n_points = n_runs;
+    *n_points = n_runs;
     return RCMVS_OK;
+}
+
+int fuse_reduce_host(DeviceArena& A, const double* h_xyz, const uint8_t* h_rgb, uint64_t n, double cell,
+                     double** d_xyz, uint8_t** d_rgb, uint8_t** d_ply, uint64_t* n_points, cudaStream_t st,
+                     std::string* err, const SpanHook& hook) {
+    *n_points = 0;
+    if (n == 0) return RCMVS_OK;
+    if (n > (uint64_t)UINT32_MAX) {
+        *err = "fusion: more than 2^32 candidates";
+        return RCMVS_E_LIMIT;
+    }
+    void *p_xyz, *p_rgb, *p_iota;
+    FCK(A.get(S_INXYZ, sizeof(double) * 3 * n, &p_xyz));
+    FCK(A.get(S_INRGB, 3 * n, &p_rgb));
+    FCK(A.get(S_IOTA, sizeof(uint32_t) * n, &p_iota));
+    FCK(cudaMemcpyAsync(p_xyz, h_xyz, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, st));
+    FCK(cudaMemcpyAsync(p_rgb, h_rgb, 3 * n, cudaMemcpyHostToDevice, st));
+    iota_kernel<<<fgrid((uint32_t)n), FT, 0, st>>>((uint32_t*)p_iota, (uint32_t)n);
+    FCK(cudaGetLastError());
+    return fuse_reduce_device(A, (const uint32_t*)p_iota, (uint32_t)n, (const double*)p_xyz, (const uint8_t*)p_rgb,
+                              cell, d_xyz, d_rgb, d_ply, n_points, st, err, hook);
+}
+
+int fuse_gather_device(DeviceArena& A, const uint32_t* d_cand, uint32_t n, const double* pts, const uint8_t* rgb,
+                       double** d_xyz, uint8_t** d_rgb, cudaStream_t st, std::string* err) {
+    void *p_xyz, *p_rgb;
+    FCK(A.get(S_GXYZ, sizeof(double) * 3 * std::max<uint32_t>(n, 1), &p_xyz));
+    FCK(A.get(S_GRGB, 3 * (size_t)std::max<uint32_t>(n, 1), &p_rgb));
+    if (n > 0) {
+        gather_cand_kernel<<<fgrid(n), FT, 0, st>>>(d_cand, n, pts, rgb, (double*)p_xyz, (uint8_t*)p_rgb);
+        FCK(cudaGetLastError());
+    }
+    *d_xyz = (double*)p_xyz;
+    *d_rgb = (uint8_t*)p_rgb;
+    return RCMVS_OK;
+}
+
+int fuse_device(DeviceArena& A, const FuseView* h_views, int n_views, const int32_t* h_order, int n_order,
+                const float* depth, const uint8_t* rgb, double cell, uint32_t min_consistent, double depth_diff,
+                double reproj_px, double** d_xyz, uint8_t** d_rgb, uint8_t** d_ply, FuseResult* res,
+                cudaStream_t st, std::string* err, const SpanHook& hook) {
+    res->n_candidates = res->n_points = 0;
+    const uint32_t* cand = nullptr;
+    const double* pts = nullptr;
+    uint32_t n_cand = 0;
+    int rc = fuse_candidates_device(A, h_views, n_views, h_order, n_order, depth, min_consistent, depth_diff,
+                                    reproj_px, &cand, &n_cand, &pts, st, err, hook);
+    if (rc) return rc;
+    res->n_candidates = n_cand;
+    return fuse_reduce_device(A, cand, n_cand, pts, rgb, cell, d_xyz, d_rgb, d_ply, &res->n_points, st, err, hook);
 }
 
 }  // namespace rcmvs

@@ -117,7 +117,7 @@ struct FuseView {
     int64_t off;
     int32_t has_depth;
     int32_t order_begin, order_end;
-    int32_t pad;
+    int32_t is_ref;  // its pixels are checked (else it only serves as a source)
     double f, cx, cy, k;
     double R[9];
     double t[3];
@@ -148,6 +148,28 @@ int fuse_device(DeviceArena& arena, const FuseView* h_views, int n_views, const 
                 int n_order, const float* depth, const uint8_t* rgb, double cell, uint32_t min_consistent,
                 double depth_diff, double reproj_px, double** d_xyz, uint8_t** d_rgb, uint8_t** d_ply,
                 FuseResult* res, cudaStream_t st, std::string* err, const SpanHook& hook);
+
+// The two stages of fuse_device.  Candidates: the consistency check of the
+// pixels of views with has_depth && is_ref; *d_cand gets the ascending
+// global pixel indices of the candidates (n_cand of them) and *d_pts the
+// per-pixel point buffer they index (3 doubles per global pixel).
+int fuse_candidates_device(DeviceArena& arena, const FuseView* h_views, int n_views, const int32_t* h_order,
+                           int n_order, const float* depth, uint32_t min_consistent, double depth_diff,
+                           double reproj_px, const uint32_t** d_cand, uint32_t* n_cand, const double** d_pts,
+                           cudaStream_t st, std::string* err, const SpanHook& hook);
+// Voxel dedup of candidates cand[0..n_cand) in that order (indices into pts,
+// 3 doubles each, and rgb, 3 bytes each).
+int fuse_reduce_device(DeviceArena& arena, const uint32_t* d_cand, uint32_t n_cand, const double* pts,
+                       const uint8_t* rgb, double cell, double** d_xyz, uint8_t** d_rgb, uint8_t** d_ply,
+                       uint64_t* n_points, cudaStream_t st, std::string* err, const SpanHook& hook);
+// fuse_reduce_device over n host candidates (3 doubles + 3 bytes each),
+// uploaded in the order given.
+int fuse_reduce_host(DeviceArena& arena, const double* h_xyz, const uint8_t* h_rgb, uint64_t n, double cell,
+                     double** d_xyz, uint8_t** d_rgb, uint8_t** d_ply, uint64_t* n_points, cudaStream_t st,
+                     std::string* err, const SpanHook& hook);
+// The candidates' points and colours compacted in list order (device).
+int fuse_gather_device(DeviceArena& arena, const uint32_t* d_cand, uint32_t n, const double* pts,
+                       const uint8_t* rgb, double** d_xyz, uint8_t** d_rgb, cudaStream_t st, std::string* err);
 
 // Grow-only device scratch memory owned by a context, carved into named
 // slots so repeated calls reuse allocations.

@@ -185,6 +185,42 @@ def _take_points(ctx, pts):
     return xyz, rgb
 
 
+def fuse_candidates(views, depth_maps, sources, ref_views, opts, ctx=None):
+    """The consistency half of fuse_depth_maps (fuse.rs:96-167) for the
+    pixels of ref_views only.  Returns (xyz (n, 3) f64, rgb (n, 3) u8,
+    per-view counts (n_views,) u64), candidates in view-then-pixel order."""
+    ctx = _ctx(ctx)
+    va = _abi.view_array(views)
+    dms = [None if d is None else np.ascontiguousarray(d.depth if isinstance(d, DepthMap) else d, dtype=np.float32)
+           for d in depth_maps]
+    dptr = (C.c_void_p * len(views))(*[None if d is None else d.ctypes.data for d in dms])
+    off, flat = _csr(sources)
+    refs = np.array(list(ref_views) or [0], np.int32)
+    per_view = np.zeros(len(views), np.uint64)
+    pts = _abi.Points()
+    o = opts.to_c()
+    ctx.check(ctx._L.rcmvs_fuse_candidates(ctx.ptr, va, len(views), dptr, off.ctypes.data, flat.ctypes.data,
+                                           refs.ctypes.data, len(ref_views), C.byref(o), C.byref(pts),
+                                           per_view.ctypes.data))
+    xyz, rgb = _take_points(ctx, pts)
+    return xyz, rgb, per_view
+
+
+def fuse_reduce(xyz, rgb, sparse_xyz, opts, ctx=None):
+    """The voxel-dedup half of fuse_depth_maps (fuse.rs:72-92, 176-214) over
+    candidates in the reference's accumulation order.  Returns (xyz, rgb)
+    sorted by voxel key."""
+    ctx = _ctx(ctx)
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+    rgb = np.ascontiguousarray(rgb, dtype=np.uint8).reshape(-1, 3)
+    sp = np.ascontiguousarray(sparse_xyz, dtype=np.float64).reshape(-1, 3)
+    pts = _abi.Points()
+    o = opts.to_c()
+    ctx.check(ctx._L.rcmvs_fuse_reduce(ctx.ptr, xyz.ctypes.data, rgb.ctypes.data, len(xyz), sp.ctypes.data, len(sp),
+                                       C.byref(o), C.byref(pts)))
+    return _take_points(ctx, pts)
+
+
 def depth_vis(depth, ctx=None):
     """fuse::save_depth_vis's image (fuse.rs:241-268) on the GPU: returns
     ((h, w) u8, lo, hi)."""
@@ -353,6 +389,19 @@ class DeviceScene:
                                                     sp.ctypes.data, len(sp), C.byref(o), C.byref(n)))
         self.n_points = n.value
         return self.n_points
+
+    def fuse_candidates(self, fusion_order, ref_views, opts):
+        """fuse_candidates on the scene's device-resident depth maps."""
+        off, flat = _csr(fusion_order)
+        refs = np.array(list(ref_views) or [0], np.int32)
+        per_view = np.zeros(len(self.views), np.uint64)
+        pts = _abi.Points()
+        o = opts.to_c()
+        self.ctx.check(self.ctx._L.rcmvs_scene_fuse_candidates(self.ctx.ptr, self.ptr, off.ctypes.data,
+                                                               flat.ctypes.data, refs.ctypes.data, len(ref_views),
+                                                               C.byref(o), C.byref(pts), per_view.ctypes.data))
+        xyz, rgb = _take_points(self.ctx, pts)
+        return xyz, rgb, per_view
 
     def depth(self, v, normals=False):
         w, h = self.views[v].w, self.views[v].h

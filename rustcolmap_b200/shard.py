@@ -1,18 +1,26 @@
 """One scene on several GPUs: one process per GPU (torch.distributed),
-reference views sharded across ranks, depth maps all-gathered for fusion.
+reference views sharded across ranks for stereo and for fusion.
 
 The reference runs `estimate_depth` for every view in a rayon `par_iter`
 (mvs/src/lib.rs:345-370) and then `fuse_depth_maps` over all of them
 (mvs/src/lib.rs:426).  Stereo for one reference view reads only its own and
 its sources' census (read-only), so views shard across ranks with no
-exchange; fusion needs every view's depth map, so one all-gather precedes
-it.  Each rank recomputes the census of all views itself (17 bytes per pixel
-of HBM traffic, a few ms for 100 1080p views) instead of receiving it: that
-is cheaper than the collective and needs no synchronisation.
+exchange.  Each rank recomputes the census of all views itself (17 bytes per
+pixel of HBM traffic, a few ms for 100 1080p views) instead of receiving it:
+that is cheaper than the collective and needs no synchronisation.
+
+Fusion checks each reference pixel against the depth maps of the views in
+its fusion order, so one all-gather of the depth maps follows stereo.  Then
+each rank runs the consistency check (fuse.rs:96-167) for the pixels of its
+own reference views, the candidates of all ranks are all-gathered and
+concatenated in view order, which is the order the reference accumulates
+them in, and every rank runs the voxel dedup (fuse.rs:176-214) on the same
+list.
 
 Every rank takes the same collective steps in the same order.  The result
-is bit-identical to the single-GPU `mvs.run_mvs` (each view's stereo and the
-fusion are the same computations; only where they run changes).
+is bit-identical to the single-GPU `mvs.run_mvs` (each view's stereo, each
+pixel's check and the dedup are the same computations; only where they run
+changes).
 """
 import numpy as np
 
@@ -80,16 +88,63 @@ def all_gather_maps(local, shapes, owners, group=None, device="cpu"):
     return out
 
 
-def run_mvs_sharded(views, sparse, opts, group=None, ctx=None, stereo=None, fuse=None, device="cpu"):
+def all_gather_candidates(xyz, rgb, per_view, group=None, device="cpu"):
+    """All-gather fusion candidates and concatenate them in view order.
+
+    xyz (n, 3) f64, rgb (n, 3) u8: this rank's candidates in view-then-pixel
+    order; per_view (n_views,): this rank's count per view (0 for views it
+    did not check; every view is checked by at most one rank).  Returns
+    (xyz, rgb) of all ranks' candidates, view by view in ascending order,
+    the same on every rank.  One all_gather of the counts, one of the
+    candidates packed as 4 f64 each (x, y, z, r | g << 8 | b << 16, exact),
+    padded to the largest rank's count."""
+    import torch
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+    rgb = np.ascontiguousarray(rgb, dtype=np.uint8).reshape(-1, 3)
+    counts = np.ascontiguousarray(per_view, dtype=np.int64)
+    if counts.sum() != len(xyz) or len(rgb) != len(xyz):
+        raise ValueError("per-view counts do not add up to the candidates")
+    nv = len(counts)
+    head = np.concatenate([[len(xyz)], counts]).astype(np.int64)
+    heads = [torch.empty(nv + 1, dtype=torch.int64, device=device) for _ in range(world)]
+    dist.all_gather(heads, torch.from_numpy(head).to(device), group=group)
+    heads = [h.cpu().numpy() for h in heads]
+    n_max = max(1, max(int(h[0]) for h in heads))
+    buf = np.zeros((n_max, 4), np.float64)
+    buf[:len(xyz), :3] = xyz
+    c = rgb.astype(np.int64)
+    buf[:len(xyz), 3] = c[:, 0] | (c[:, 1] << 8) | (c[:, 2] << 16)
+    parts = [torch.empty((n_max, 4), dtype=torch.float64, device=device) for _ in range(world)]
+    dist.all_gather(parts, torch.from_numpy(buf).to(device), group=group)
+    parts = [p.cpu().numpy() for p in parts]
+    pieces, cursor = [], [0] * world
+    for v in range(nv):
+        for r in range(world):
+            k = int(heads[r][1 + v])
+            if k:
+                pieces.append(parts[r][cursor[r]:cursor[r] + k])
+                cursor[r] += k
+    allc = np.concatenate(pieces) if pieces else np.zeros((0, 4), np.float64)
+    packed = allc[:, 3].astype(np.int64)
+    out_rgb = np.stack([packed & 255, (packed >> 8) & 255, (packed >> 16) & 255], axis=1).astype(np.uint8)
+    return np.ascontiguousarray(allc[:, :3]), out_rgb
+
+
+def run_mvs_sharded(views, sparse, opts, group=None, ctx=None, stereo=None, candidates=None, reduce=None,
+                    device="cpu"):
     """`run_mvs` with this scene's reference views spread over the ranks of
-    `group`.  Returns (fused xyz (n,3) f64, rgb (n,3) u8, depth maps per
-    view or None) on every rank.
+    `group`, for stereo and for fusion.  Returns (fused xyz (n,3) f64, rgb
+    (n,3) u8, depth maps per view or None) on every rank.
 
     stereo(jobs) -> {view: depth (h, w)} runs this rank's jobs (default: the
-    library on this rank's GPU through a DeviceScene); fuse(depth_maps,
-    fusion_order) -> (xyz, rgb) fuses (default: `mvs.fuse_depth_maps`).
-    Both are parameters so that the host logic can be exercised with other
-    back ends."""
+    library on this rank's GPU through a DeviceScene);
+    candidates(depth_maps, fusion_order, ref_views) -> (xyz, rgb, per_view)
+    checks this rank's reference pixels (default: `mvs.fuse_candidates`);
+    reduce(xyz, rgb) -> (xyz, rgb) dedups all candidates (default:
+    `mvs.fuse_reduce`).  They are parameters so that the host logic can be
+    exercised with other back ends."""
     import torch.distributed as dist
     world = dist.get_world_size(group)
     rank = dist.get_rank(group)
@@ -113,8 +168,13 @@ def run_mvs_sharded(views, sparse, opts, group=None, ctx=None, stereo=None, fuse
     shapes = {r: (views[r].h, views[r].w) for r, _, _, _ in jobs}
     maps = all_gather_maps(local, shapes, owners, group=group, device=device)
     depth = [maps.get(i) for i in range(len(views))]
-    if fuse is None:
-        def fuse(dm, order):
-            return mvs.fuse_depth_maps(views, dm, order, sparse.xyz, opts, ctx)
-    xyz, rgb = fuse(depth, fus)
+    if candidates is None:
+        def candidates(dm, order, refs):
+            return mvs.fuse_candidates(views, dm, order, refs, opts, ctx)
+    if reduce is None:
+        def reduce(cx, cc):
+            return mvs.fuse_reduce(cx, cc, sparse.xyz, opts, ctx)
+    cx, cc, per_view = candidates(depth, fus, sorted(r for r, _, _, _ in mine))
+    ax, ac = all_gather_candidates(cx, cc, per_view, group=group, device=device)
+    xyz, rgb = reduce(ax, ac)
     return xyz, rgb, depth

@@ -212,6 +212,58 @@ def test_fusion_with_missing_depth_maps(ctx, corner_scene, c1_depth):
     _assert_same_cloud(g, (xyz, rgb))
 
 
+@pytest.mark.parametrize("reproj", [0.0, 1.0])
+def test_fusion_split_matches_oracle_and_whole(ctx, corner_scene, c1_depth, reproj):
+    """Candidates of view subsets (host and device-resident entry points)
+    against the oracle's, and the dedup of all candidates in view order
+    against whole fusion."""
+    dms, fus = c1_depth
+    v = corner_scene.views
+    opts = MvsOptions(min_consistent=2, depth_diff=0.02, reproj_px=reproj)
+    off = np.cumsum([0] + [len(f) for f in fus])
+    flat = [x for f in fus for x in f]
+    depth = [d.depth for d in dms]
+    whole = mvs.fuse_depth_maps(v, depth, fus, corner_scene.sparse.xyz, opts, ctx)
+    for refs in (list(range(len(v))), [0, 3, 5], [7], []):
+        gx, gc, gp = mvs.fuse_candidates(v, depth, fus, refs, opts, ctx)
+        ox, oc, op = oracle.fuse_candidates(v, depth, off, flat, refs, opts)
+        assert np.array_equal(gx, ox) and np.array_equal(gc, oc) and np.array_equal(gp, op), refs
+        assert all(gp[i] == 0 for i in range(len(v)) if i not in refs)
+    ax, ac, ap = mvs.fuse_candidates(v, depth, fus, list(range(len(v))), opts, ctx)
+    _assert_same_cloud(mvs.fuse_reduce(ax, ac, corner_scene.sparse.xyz, opts, ctx), whole)
+    _assert_same_cloud(oracle.fuse_reduce(ax, ac, corner_scene.sparse.xyz, opts), whole)
+    # two disjoint halves, merged view by view
+    a, b = list(range(0, len(v), 2)), list(range(1, len(v), 2))
+    xa, ca, pa = mvs.fuse_candidates(v, depth, fus, a, opts, ctx)
+    xb, cb, pb = mvs.fuse_candidates(v, depth, fus, b, opts, ctx)
+    mx, mc, ia, ib = [], [], 0, 0
+    for k in range(len(v)):
+        na, nb = int(pa[k]), int(pb[k])
+        mx += [xa[ia:ia + na], xb[ib:ib + nb]]
+        mc += [ca[ia:ia + na], cb[ib:ib + nb]]
+        ia, ib = ia + na, ib + nb
+    _assert_same_cloud(mvs.fuse_reduce(np.concatenate(mx), np.concatenate(mc), corner_scene.sparse.xyz, opts, ctx),
+                       whole)
+    assert len(whole[0]) > 1000
+    empty = mvs.fuse_reduce(np.zeros((0, 3)), np.zeros((0, 3), np.uint8), corner_scene.sparse.xyz, opts, ctx)
+    assert empty[0].shape == (0, 3)
+
+
+def test_scene_fuse_candidates_matches_host_entry(ctx, corner_scene, c1_opts):
+    """Device-resident candidates after device-resident stereo."""
+    v = corner_scene.views
+    srcs, zr, fus = mvs.plan(corner_scene.sparse, v, c1_opts)
+    jobs = [(i, srcs[i], zr[i, 0], zr[i, 1]) for i in range(len(v)) if srcs[i]]
+    ds = mvs.DeviceScene(v, ctx)
+    ds.estimate(jobs, c1_opts)
+    depth = [ds.depth(i).depth if srcs[i] else None for i in range(len(v))]
+    refs = [r for r, _, _, _ in jobs][1::2]
+    sx, sc_, sp = ds.fuse_candidates(fus, refs, c1_opts)
+    hx, hc, hp = mvs.fuse_candidates(v, depth, fus, refs, c1_opts, ctx)
+    assert len(sx) > 0 and np.array_equal(sx, hx) and np.array_equal(sc_, hc) and np.array_equal(sp, hp)
+    ds.close()
+
+
 def test_run_mvs_matches_oracle_pipeline(ctx, corner_scene, c1_opts, tmp_path):
     v = corner_scene.views
     stats, xyz, rgb, dms = mvs.run_mvs(v, corner_scene.sparse, c1_opts, out_dir=str(tmp_path), ctx=ctx,

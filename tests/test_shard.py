@@ -1,7 +1,10 @@
 """Single-scene multi-GPU host logic (rustcolmap_b200.shard) with world-size 2
-and 3 `gloo` process groups on the CPU: view assignment, the depth-map
-all-gather, and the sharded pipeline against the single-process one (with
-the CPU oracle standing in for the GPU stereo and fusion)."""
+and 3 `gloo` process groups on the CPU: view assignment, the depth-map and
+candidate all-gathers, and the sharded pipeline (stereo and fusion) against
+the single-process one (with the CPU oracle standing in for the GPU stereo,
+fusion candidates and voxel dedup).  The split of fusion itself (candidates
+of view subsets, concatenated in view order, then the dedup) is checked
+against whole fusion on the oracle here and on the GPU."""
 import multiprocessing as mp
 import os
 import socket
@@ -98,6 +101,10 @@ def _tiny():
     return sc, opts
 
 
+def _csr(order):
+    return np.cumsum([0] + [len(f) for f in order]), [x for f in order for x in f]
+
+
 def _oracle_backends(sc, opts):
     from oracle import oracle
 
@@ -106,35 +113,110 @@ def _oracle_backends(sc, opts):
                 for r, s, a, b in jobs}
 
     def fuse(depth, order):
-        off = np.cumsum([0] + [len(f) for f in order])
-        flat = [x for f in order for x in f]
+        off, flat = _csr(order)
         xyz, rgb, _ = oracle.fuse_depth_maps(sc.views, depth, off, flat, sc.sparse.xyz, opts, nthreads=1)
         return xyz, rgb
-    return stereo, fuse
+
+    def candidates(depth, order, refs):
+        off, flat = _csr(order)
+        return oracle.fuse_candidates(sc.views, depth, off, flat, refs, opts, nthreads=1)
+
+    def reduce(xyz, rgb):
+        return oracle.fuse_reduce(xyz, rgb, sc.sparse.xyz, opts)
+    return stereo, fuse, candidates, reduce
+
+
+def _reference_run(sc, opts):
+    from rustcolmap_b200 import mvs
+    stereo, fuse, _, _ = _oracle_backends(sc, opts)
+    srcs, zr, fus = mvs.plan(sc.sparse, sc.views, opts)
+    jobs = [(i, srcs[i], zr[i, 0], zr[i, 1]) for i in range(len(sc.views)) if srcs[i]]
+    maps = stereo(jobs)
+    depth = [maps.get(i) for i in range(len(sc.views))]
+    xyz, rgb = fuse(depth, fus)
+    return depth, fus, xyz, rgb
+
+
+def test_oracle_fusion_split_equals_whole():
+    """Candidates of disjoint view subsets, concatenated in view order, then
+    the dedup: the cloud of whole fusion, bit for bit."""
+    sc, opts = _tiny()
+    depth, fus, ref_xyz, ref_rgb = _reference_run(sc, opts)
+    _, _, candidates, reduce = _oracle_backends(sc, opts)
+    with_map = [i for i, d in enumerate(depth) if d is not None]
+    ax, ac, pv = candidates(depth, fus, with_map)
+    assert len(ax) > 0 and int(pv.sum()) == len(ax)
+    assert all(pv[i] == 0 for i, d in enumerate(depth) if d is None)
+    xyz, rgb = reduce(ax, ac)
+    assert np.array_equal(xyz, ref_xyz) and np.array_equal(rgb, ref_rgb)
+    # subsets: every other view, and the rest
+    a, b = with_map[::2], with_map[1::2]
+    xa, ca, pa = candidates(depth, fus, a)
+    xb, cb, pb = candidates(depth, fus, b)
+    assert np.array_equal(pa + pb, pv)
+    pieces_x, pieces_c, ia, ib = [], [], 0, 0
+    for v in range(len(depth)):
+        ka, kb = int(pa[v]), int(pb[v])
+        pieces_x += [xa[ia:ia + ka], xb[ib:ib + kb]]
+        pieces_c += [ca[ia:ia + ka], cb[ib:ib + kb]]
+        ia, ib = ia + ka, ib + kb
+    mx, mc = np.concatenate(pieces_x), np.concatenate(pieces_c)
+    assert np.array_equal(mx, ax) and np.array_equal(mc, ac)
+    ex, ec = reduce(np.zeros((0, 3)), np.zeros((0, 3), np.uint8))
+    assert ex.shape == (0, 3) and ec.shape == (0, 3)
+
+
+def _cand_rank(rank, world, out, n_views, counts):
+    rng = np.random.default_rng(100 + rank)
+    pv = np.array(counts[rank], np.int64)
+    n = int(pv.sum())
+    xyz = rng.normal(size=(n, 3))
+    rgb = rng.integers(0, 256, (n, 3), dtype=np.uint8)
+    np.savez(os.path.join(out, f"in{rank}.npz"), xyz=xyz, rgb=rgb)
+    gx, gc = shard.all_gather_candidates(xyz, rgb, pv)
+    np.savez(os.path.join(out, f"r{rank}.npz"), xyz=gx, rgb=gc)
+
+
+@pytest.mark.parametrize("world,counts", [
+    (2, [[3, 0, 2, 0, 0], [0, 4, 0, 0, 1]]),
+    (3, [[0, 0, 0, 0], [5, 0, 0, 2], [0, 0, 0, 0]]),  # ranks with no candidates
+])
+def test_all_gather_candidates_gloo(world, counts):
+    n_views = len(counts[0])
+    out = _run_ranks(_cand_rank, world, n_views, counts)
+    ins = [dict(np.load(os.path.join(out, f"in{r}.npz"))) for r in range(world)]
+    want_x, want_c, cur = [], [], [0] * world
+    for v in range(n_views):
+        for r in range(world):
+            k = counts[r][v]
+            want_x.append(ins[r]["xyz"][cur[r]:cur[r] + k])
+            want_c.append(ins[r]["rgb"][cur[r]:cur[r] + k])
+            cur[r] += k
+    wx, wc = np.concatenate(want_x), np.concatenate(want_c)
+    for r in range(world):
+        got = dict(np.load(os.path.join(out, f"r{r}.npz")))
+        assert np.array_equal(got["xyz"], wx) and np.array_equal(got["rgb"], wc)
 
 
 def _pipeline_rank(rank, world, out):
     sc, opts = _tiny()
-    stereo, fuse = _oracle_backends(sc, opts)
-    xyz, rgb, depth = shard.run_mvs_sharded(sc.views, sc.sparse, opts, stereo=stereo, fuse=fuse)
+    stereo, _, candidates, reduce = _oracle_backends(sc, opts)
+    xyz, rgb, depth = shard.run_mvs_sharded(sc.views, sc.sparse, opts, stereo=stereo, candidates=candidates,
+                                            reduce=reduce)
     np.savez(os.path.join(out, f"r{rank}.npz"), xyz=xyz, rgb=rgb,
              **{f"d{i}": d for i, d in enumerate(depth) if d is not None})
 
 
-def test_sharded_pipeline_equals_single_process():
-    """Two ranks, each running the oracle on its share of the views, end with
-    the same depth maps and fused cloud as one process running all views."""
-    from rustcolmap_b200 import mvs
+@pytest.mark.parametrize("world", [2, 3])
+def test_sharded_pipeline_equals_single_process(world):
+    """Ranks, each running the oracle's stereo and consistency check on its
+    share of the views, end with the same depth maps and fused cloud as one
+    process running all views."""
     sc, opts = _tiny()
-    stereo, fuse = _oracle_backends(sc, opts)
-    srcs, zr, fus = mvs.plan(sc.sparse, sc.views, opts)
-    jobs = [(i, srcs[i], zr[i, 0], zr[i, 1]) for i in range(len(sc.views)) if srcs[i]]
-    ref_maps = stereo(jobs)
-    ref_depth = [ref_maps.get(i) for i in range(len(sc.views))]
-    ref_xyz, ref_rgb = fuse(ref_depth, fus)
+    ref_depth, _, ref_xyz, ref_rgb = _reference_run(sc, opts)
     assert len(ref_xyz) > 0
-    out = _run_ranks(_pipeline_rank, 2)
-    for r in range(2):
+    out = _run_ranks(_pipeline_rank, world)
+    for r in range(world):
         got = dict(np.load(os.path.join(out, f"r{r}.npz")))
         assert np.array_equal(got["xyz"], ref_xyz) and np.array_equal(got["rgb"], ref_rgb)
         for i, d in enumerate(ref_depth):
