@@ -359,6 +359,39 @@ int rcmvs_scene_depth_vis(rcmvs_ctx* ctx, rcmvs_scene* scene, int32_t view, uint
  * decoded pixels are the same).  Host only. */
 int rcmvs_write_png_gray(const char* path, const uint8_t* img, int32_t w, int32_t h);
 
+/* ------------------------------------------------------------------ SIFT */
+/* `sift::SiftOptions` (sfm-lite/src/sift.rs:20-32). */
+typedef struct rcmvs_sift_options {
+    uint32_t max_dim;        /* longest image side used for extraction */
+    uint32_t max_features;   /* cap after the response sort */
+    uint32_t reserved;
+    uint32_t reserved2;
+    double contrast_thr;     /* on DoG values in [0,1] intensity units */
+} rcmvs_sift_options;
+/* Fills `SiftOptions::default()` (sift.rs:27-31): 1600, 2048, 0.0067. */
+void rcmvs_sift_options_default(rcmvs_sift_options* opts);
+
+/* `sift::SiftFrame` (sfm-lite/src/sift.rs:34-41) without the name; arrays
+ * are allocated by the library (rcmvs_sift_frame_free). */
+typedef struct rcmvs_sift_frame {
+    int32_t width, height;   /* working size the keypoints refer to */
+    uint64_t n;              /* keypoints */
+    uint64_t n_raw;          /* scale-space extrema that passed the fit (diagnostic) */
+    double* pts;             /* n * 2: x, y */
+    float* desc;             /* n * 128, L2-normalised */
+    uint8_t* colors;         /* n * 3: RGB at the rounded position */
+} rcmvs_sift_frame;
+
+/* SIFT extraction of one decoded 8-bit image (h rows of w pixels of
+ * `channels` bytes, 1-4; alpha dropped).  Replaces `sift::extract_sift`
+ * (sfm-lite/src/sift.rs:435-555): Triangle resize when the long side
+ * exceeds max_dim, Gaussian pyramid and DoG, extrema with the quadratic fit
+ * and the contrast / curvature tests, orientations, 4x4x8 descriptors,
+ * response-sorted and capped. */
+int rcmvs_extract_sift(rcmvs_ctx* ctx, const uint8_t* img, int32_t w, int32_t h, int32_t channels,
+                       const rcmvs_sift_options* opts, rcmvs_sift_frame* out);
+void rcmvs_sift_frame_free(rcmvs_sift_frame* frame);
+
 /* ---------------------------------------------------------- diagnostics */
 
 /* `plane_cost` (mvs/src/stereo.rs:158-228) evaluated at every pixel of the

@@ -69,6 +69,14 @@ int orc_fuse_reduce(const double* xyz, const uint8_t* rgb, uint64_t n, const dou
                     const rcmvs_options* opts, double** xyz_out, uint8_t** rgb_out, uint64_t* n_out);
 void orc_free(void* p);
 
+/* extract_sift (sfm-lite/src/sift.rs:435-555) on an image at working
+ * resolution (gray w*h, rgb w*h*3): keypoints (x, y) n*2, descriptors
+ * n*128, colours n*3 (malloc'ed; orc_free); n_raw (nullable) gets the
+ * number of scale-space extrema kept by the fit and rejection tests. */
+int orc_extract_sift(const uint8_t* gray, const uint8_t* rgb, int32_t w, int32_t h, uint32_t max_features,
+                     double contrast_thr, double** pts_out, float** desc_out, uint8_t** colors_out,
+                     uint64_t* n_out, uint64_t* n_raw_out);
+
 int orc_write_ply_binary(const char* path, const double* xyz, const uint8_t* rgb,
                          uint64_t n);
 

@@ -55,6 +55,7 @@ def lib():
         L.orc_fuse_candidates.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, i32]
         L.orc_fuse_reduce.argtypes = [vp, vp, u64, vp, u64, vp, vp, vp, vp]
         L.orc_resize_view.argtypes = [vp, i32, i32, i32, i32, i32, vp, vp]
+        L.orc_extract_sift.argtypes = [vp, vp, i32, i32, C.c_uint32, f64, vp, vp, vp, vp, vp]
         L.orc_resize_view.restype = None
         _lib = L
     return _lib
@@ -240,6 +241,26 @@ def fuse_reduce(xyz, rgb, sparse_xyz, opts):
                                C.byref(xyz_p), C.byref(rgb_p), C.byref(n))
     _chk(rc, "fuse_reduce")
     return _take(xyz_p, rgb_p, n.value)
+
+
+def extract_sift(gray, rgb, max_features=2048, contrast_thr=0.0067):
+    """extract_sift on an image at working resolution: (pts (n,2) f64,
+    desc (n,128) f32, colors (n,3) u8, n_raw)."""
+    g = np.ascontiguousarray(gray, dtype=np.uint8)
+    c = np.ascontiguousarray(rgb, dtype=np.uint8)
+    h, w = g.shape
+    pp, dp, cp = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    n, nraw = C.c_uint64(), C.c_uint64()
+    _chk(lib().orc_extract_sift(g.ctypes.data, c.ctypes.data, w, h, max_features, contrast_thr, C.byref(pp),
+                                C.byref(dp), C.byref(cp), C.byref(n), C.byref(nraw)), "extract_sift")
+    k = n.value
+    pts = np.ctypeslib.as_array((C.c_double * (2 * max(k, 1))).from_address(pp.value))[: 2 * k].reshape(k, 2).copy()
+    desc = np.ctypeslib.as_array((C.c_float * (128 * max(k, 1))).from_address(dp.value))[: 128 * k]
+    desc = desc.reshape(k, 128).copy()
+    col = np.ctypeslib.as_array((C.c_uint8 * (3 * max(k, 1))).from_address(cp.value))[: 3 * k].reshape(k, 3).copy()
+    for p in (pp, dp, cp):
+        lib().orc_free(p)
+    return pts, desc, col, nraw.value
 
 
 def write_ply_binary(path, xyz, rgb):

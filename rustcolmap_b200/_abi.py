@@ -68,6 +68,16 @@ class TuneEntry(C.Structure):
                 ("ms_best", C.c_float), ("ms_default", C.c_float)]
 
 
+class SiftOptions(C.Structure):
+    _fields_ = [("max_dim", C.c_uint32), ("max_features", C.c_uint32), ("reserved", C.c_uint32),
+                ("reserved2", C.c_uint32), ("contrast_thr", C.c_double)]
+
+
+class SiftFrame(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("n", C.c_uint64), ("n_raw", C.c_uint64),
+                ("pts", C.c_void_p), ("desc", C.c_void_p), ("colors", C.c_void_p)]
+
+
 class DepthOut(C.Structure):
     _fields_ = [("depth", C.c_void_p), ("cost", C.c_void_p), ("normal", C.c_void_p)]
 

@@ -83,6 +83,9 @@ def mvs():
         "rcmvs_fuse_candidates": ([vp, vp, i32, vp, vp, vp, vp, i32, vp, vp, vp], C.c_int),
         "rcmvs_fuse_reduce": ([vp, vp, vp, u64, vp, u64, vp, vp], C.c_int),
         "rcmvs_scene_fuse_candidates": ([vp, vp, vp, vp, vp, i32, vp, vp, vp], C.c_int),
+        "rcmvs_sift_options_default": ([vp], None),
+        "rcmvs_extract_sift": ([vp, vp, i32, i32, i32, vp, vp], C.c_int),
+        "rcmvs_sift_frame_free": ([vp], None),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -125,5 +128,5 @@ _SIG_NAMES = [
     "rcmvs_scene_estimate_depth_learned", "rcmvs_run_mvs_learned", "rcmvs_autotune", "rcmvs_tune_table",
     "rcmvs_tune_set", "rcmvs_depth_vis", "rcmvs_scene_depth_vis", "rcmvs_write_png_gray",
     "rcmvs_working_size", "rcmvs_resize_view", "rcmvs_fuse_candidates", "rcmvs_fuse_reduce",
-    "rcmvs_scene_fuse_candidates",
+    "rcmvs_scene_fuse_candidates", "rcmvs_sift_options_default", "rcmvs_extract_sift", "rcmvs_sift_frame_free",
 ]

@@ -120,9 +120,17 @@ struct rcmvs_scene {
 namespace rcmvs {
 
 // Arena slots of a scene shared by the translation units (the others are
-// private to capi.cu 2-10, fuse.cu 16-37 and 70-74, learned_api.cu 40-47, depthvis.cu 50-55
-// and resize.cu 60-68).
+// private to capi.cu 2-10, fuse.cu 16-37 and 70-74, learned_api.cu 40-47, depthvis.cu 50-55,
+// resize.cu 60-68 and sift.cu 80-119).
 constexpr int kSlotJobs = 0, kSlotJobStart = 1, kSlotQueue = 11, kSlotTuneJobs = 12, kSlotTuneStart = 13;
+
+// resize.cu: argument and size checks of a resize, and the resize itself
+// on device buffers (d_gray mw*mh, d_rgb mw*mh*3), queued on the context's
+// stream; *d_err (null when no resize ran) is a device flag, non-zero if a
+// tap table overflowed.  Uses context arena slots 61 and 64-68.
+int resize_check(rcmvs_ctx* ctx, int w, int h, int channels, int mw, int mh);
+int resize_device(rcmvs_ctx* ctx, const uint8_t* d_in, int w, int h, int channels, int mw, int mh, uint8_t* d_gray,
+                  uint8_t* d_rgb, const int** d_err);
 
 // mvs/src/stereo.rs:131-132: source pose relative to the reference, f64
 // products cast to f32.

@@ -188,6 +188,57 @@ unsigned grid_for(int64_t n) {
 }
 
 }  // namespace
+
+int resize_check(rcmvs_ctx* ctx, int w, int h, int channels, int mw, int mh) {
+    if (w <= 0 || h <= 0 || mw <= 0 || mh <= 0 || channels < 1 || channels > 4)
+        return rfail(ctx, RCMVS_E_ARG, "resize: bad size or channel count");
+    if (w > kMaxSide || h > kMaxSide || mw > kMaxSide || mh > kMaxSide || (int64_t)w * h > INT32_MAX ||
+        (int64_t)mw * mh > INT32_MAX || (int64_t)w * mh > INT32_MAX)
+        return rfail(ctx, RCMVS_E_LIMIT, "resize: image side above 2^23 or more than 2^31 pixels");
+    return RCMVS_OK;
+}
+
+int resize_device(rcmvs_ctx* ctx, const uint8_t* d_in, int w, int h, int channels, int mw, int mh, uint8_t* d_gray,
+                  uint8_t* d_rgb, const int** d_err) {
+    cudaStream_t st = ctx->stream;
+    DeviceArena& A = ctx->arena;
+    const int64_t n_in = (int64_t)w * h, n_out = (int64_t)mw * mh;
+    *d_err = nullptr;
+    if (mw == w && mh == h) {  // mvs/src/lib.rs:188-192: no resize
+        convert_kernel<<<grid_for(n_in), 256, 0, st>>>(d_in, n_in, channels, d_gray, d_rgb);
+        RCK(cudaGetLastError());
+        return RCMVS_OK;
+    }
+    const int nc = channels < 3 ? 1 : 3;
+    const int tv = taps_bound(h, mh), th = taps_bound(w, mw);
+    void *p_tmp, *p_vidx, *p_vw, *p_hidx, *p_hw, *p_err;
+    RCK(A.get(R_TMP, sizeof(float) * (size_t)w * mh * nc, &p_tmp));
+    RCK(A.get(R_VIDX, sizeof(int32_t) * 2 * (size_t)mh, &p_vidx));
+    RCK(A.get(R_VW, sizeof(float) * (size_t)mh * tv, &p_vw));
+    RCK(A.get(R_HIDX, sizeof(int32_t) * 2 * (size_t)mw, &p_hidx));
+    RCK(A.get(R_HW, sizeof(float) * (size_t)mw * th, &p_hw));
+    RCK(A.get(R_ERR, sizeof(int), &p_err));
+    RCK(cudaMemsetAsync(p_err, 0, sizeof(int), st));
+    int32_t* vfirst = (int32_t*)p_vidx;
+    int32_t* hfirst = (int32_t*)p_hidx;
+    taps_kernel<<<(mh + 127) / 128, 128, 0, st>>>(h, mh, tv, vfirst, vfirst + mh, (float*)p_vw, (int*)p_err);
+    RCK(cudaGetLastError());
+    taps_kernel<<<(mw + 127) / 128, 128, 0, st>>>(w, mw, th, hfirst, hfirst + mw, (float*)p_hw, (int*)p_err);
+    RCK(cudaGetLastError());
+    vert_kernel<<<grid_for((int64_t)w * nc * mh), 256, 0, st>>>(d_in, w, channels, nc, mh, vfirst, vfirst + mh,
+                                                                 (const float*)p_vw, tv, (float*)p_tmp);
+    RCK(cudaGetLastError());
+    if (nc == 1)
+        horiz_kernel<1><<<grid_for(n_out), 256, 0, st>>>((const float*)p_tmp, w, mw, mh, hfirst, hfirst + mw,
+                                                          (const float*)p_hw, th, d_gray, d_rgb);
+    else
+        horiz_kernel<3><<<grid_for(n_out), 256, 0, st>>>((const float*)p_tmp, w, mw, mh, hfirst, hfirst + mw,
+                                                          (const float*)p_hw, th, d_gray, d_rgb);
+    RCK(cudaGetLastError());
+    *d_err = (const int*)p_err;
+    return RCMVS_OK;
+}
+
 }  // namespace rcmvs
 
 using namespace rcmvs;
@@ -206,11 +257,9 @@ int rcmvs_working_size(int32_t w, int32_t h, uint32_t max_dim, int32_t* mw, int3
 
 int rcmvs_resize_view(rcmvs_ctx* ctx, const uint8_t* img, int32_t w, int32_t h, int32_t channels, int32_t mw,
                       int32_t mh, uint8_t* gray_out, uint8_t* rgb_out) {
-    if (!ctx || !img || w <= 0 || h <= 0 || mw <= 0 || mh <= 0 || channels < 1 || channels > 4)
-        return rfail(ctx, RCMVS_E_ARG, "rcmvs_resize_view: bad argument");
-    if (w > kMaxSide || h > kMaxSide || mw > kMaxSide || mh > kMaxSide || (int64_t)w * h > INT32_MAX ||
-        (int64_t)mw * mh > INT32_MAX || (int64_t)w * mh > INT32_MAX)
-        return rfail(ctx, RCMVS_E_LIMIT, "rcmvs_resize_view: image side above 2^23 or more than 2^31 pixels");
+    if (!ctx || !img) return rfail(ctx, RCMVS_E_ARG, "rcmvs_resize_view: bad argument");
+    int rc = resize_check(ctx, w, h, channels, mw, mh);
+    if (rc) return rc;
     RCK(cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;
     DeviceArena& A = ctx->arena;
@@ -220,43 +269,11 @@ int rcmvs_resize_view(rcmvs_ctx* ctx, const uint8_t* img, int32_t w, int32_t h, 
     RCK(A.get(R_GRAY, (size_t)n_out, &p_gray));
     RCK(A.get(R_RGB, (size_t)n_out * 3, &p_rgb));
     RCK(cudaMemcpyAsync(p_in, img, (size_t)n_in * channels, cudaMemcpyHostToDevice, st));
+    const int* d_err = nullptr;
+    rc = resize_device(ctx, (const uint8_t*)p_in, w, h, channels, mw, mh, (uint8_t*)p_gray, (uint8_t*)p_rgb, &d_err);
+    if (rc) return rc;
     int bad = 0;
-    if (mw == w && mh == h) {  // mvs/src/lib.rs:188-192: no resize
-        convert_kernel<<<grid_for(n_in), 256, 0, st>>>((const uint8_t*)p_in, n_in, channels, (uint8_t*)p_gray,
-                                                       (uint8_t*)p_rgb);
-        RCK(cudaGetLastError());
-    } else {
-        const int nc = channels < 3 ? 1 : 3;
-        const int tv = taps_bound(h, mh), th = taps_bound(w, mw);
-        void *p_tmp, *p_vidx, *p_vw, *p_hidx, *p_hw, *p_err;
-        RCK(A.get(R_TMP, sizeof(float) * (size_t)w * mh * nc, &p_tmp));
-        RCK(A.get(R_VIDX, sizeof(int32_t) * 2 * (size_t)mh, &p_vidx));
-        RCK(A.get(R_VW, sizeof(float) * (size_t)mh * tv, &p_vw));
-        RCK(A.get(R_HIDX, sizeof(int32_t) * 2 * (size_t)mw, &p_hidx));
-        RCK(A.get(R_HW, sizeof(float) * (size_t)mw * th, &p_hw));
-        RCK(A.get(R_ERR, sizeof(int), &p_err));
-        RCK(cudaMemsetAsync(p_err, 0, sizeof(int), st));
-        int32_t* vfirst = (int32_t*)p_vidx;
-        int32_t* hfirst = (int32_t*)p_hidx;
-        taps_kernel<<<(mh + 127) / 128, 128, 0, st>>>(h, mh, tv, vfirst, vfirst + mh, (float*)p_vw, (int*)p_err);
-        RCK(cudaGetLastError());
-        taps_kernel<<<(mw + 127) / 128, 128, 0, st>>>(w, mw, th, hfirst, hfirst + mw, (float*)p_hw, (int*)p_err);
-        RCK(cudaGetLastError());
-        vert_kernel<<<grid_for((int64_t)w * nc * mh), 256, 0, st>>>((const uint8_t*)p_in, w, channels, nc, mh, vfirst,
-                                                                     vfirst + mh, (const float*)p_vw, tv,
-                                                                     (float*)p_tmp);
-        RCK(cudaGetLastError());
-        if (nc == 1)
-            horiz_kernel<1><<<grid_for(n_out), 256, 0, st>>>((const float*)p_tmp, w, mw, mh, hfirst, hfirst + mw,
-                                                              (const float*)p_hw, th, (uint8_t*)p_gray,
-                                                              (uint8_t*)p_rgb);
-        else
-            horiz_kernel<3><<<grid_for(n_out), 256, 0, st>>>((const float*)p_tmp, w, mw, mh, hfirst, hfirst + mw,
-                                                              (const float*)p_hw, th, (uint8_t*)p_gray,
-                                                              (uint8_t*)p_rgb);
-        RCK(cudaGetLastError());
-        RCK(cudaMemcpyAsync(&bad, p_err, sizeof(int), cudaMemcpyDeviceToHost, st));
-    }
+    if (d_err) RCK(cudaMemcpyAsync(&bad, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
     if (gray_out) RCK(cudaMemcpyAsync(gray_out, p_gray, (size_t)n_out, cudaMemcpyDeviceToHost, st));
     if (rgb_out) RCK(cudaMemcpyAsync(rgb_out, p_rgb, (size_t)n_out * 3, cudaMemcpyDeviceToHost, st));
     RCK(cudaStreamSynchronize(st));

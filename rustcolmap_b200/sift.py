@@ -1,0 +1,63 @@
+"""SIFT feature extraction on the GPU: the mirror of `sift::extract_sift`
+(sfm-lite/src/sift.rs:435-555) over librcmvs (rcmvs_extract_sift).
+
+There is no CPU path: a missing library or a CUDA error raises RcmvsError.
+"""
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _abi
+from ._lib import RcmvsError  # noqa: F401
+
+DESC_LEN = 128
+
+
+@dataclass
+class SiftOptions:
+    """`sift::SiftOptions` (sift.rs:20-32) with its defaults."""
+    max_dim: int = 1600
+    max_features: int = 2048
+    contrast_thr: float = 0.0067
+
+    def to_c(self):
+        return _abi.SiftOptions(self.max_dim, self.max_features, 0, 0, self.contrast_thr)
+
+
+@dataclass
+class SiftFrame:
+    """`sift::SiftFrame` (sift.rs:34-41)."""
+    name: str
+    width: int
+    height: int
+    pts: np.ndarray                      # (n, 2) f64
+    desc: np.ndarray                     # (n, 128) f32
+    colors: np.ndarray                   # (n, 3) u8
+    n_raw: int = 0                       # extrema kept by the fit (diagnostic)
+    extra: dict = field(default_factory=dict)
+
+
+def extract_sift(img, name="", opts=None, ctx=None):
+    """SIFT keypoints and descriptors of one decoded 8-bit image ((h, w) or
+    (h, w, c), c = 1-4) on the GPU."""
+    from .mvs import _ctx
+    ctx = _ctx(ctx)
+    opts = opts or SiftOptions()
+    a = np.ascontiguousarray(img, dtype=np.uint8)
+    if a.ndim == 2:
+        a = a[:, :, None]
+    h, w, c = a.shape
+    o = opts.to_c()
+    f = _abi.SiftFrame()
+    ctx.check(ctx._L.rcmvs_extract_sift(ctx.ptr, a.ctypes.data, w, h, c, C.byref(o), C.byref(f)))
+    try:
+        n = f.n
+        k = max(n, 1)
+        pts = np.ctypeslib.as_array((C.c_double * (2 * k)).from_address(f.pts))[: 2 * n].reshape(n, 2).copy()
+        desc = np.ctypeslib.as_array((C.c_float * (DESC_LEN * k)).from_address(f.desc))[: DESC_LEN * n]
+        desc = desc.reshape(n, DESC_LEN).copy()
+        col = np.ctypeslib.as_array((C.c_uint8 * (3 * k)).from_address(f.colors))[: 3 * n].reshape(n, 3).copy()
+        return SiftFrame(name, f.width, f.height, pts, desc, col, int(f.n_raw))
+    finally:
+        ctx._L.rcmvs_sift_frame_free(C.byref(f))

@@ -1,0 +1,152 @@
+"""SIFT extraction (sfm-lite/src/sift.rs): the CPU oracle against properties
+the reference's algorithm guarantees, and the GPU (rcmvs_extract_sift)
+against the oracle.
+
+Parity bar.  The pyramid, the DoGs and the extrema with their fitted
+positions and responses use only f32/f64 arithmetic, so the count of
+extrema must be equal and every keypoint position exact.  Orientations and
+descriptors go through exp / atan2 / sin / cos, whose device and host-libm
+results may differ in the last bit; descriptors must agree to 1e-4 per
+component, and at most 1% of keypoints may differ (a histogram bin or a
+peak decision that sits on an exact boundary)."""
+import numpy as np
+import pytest
+
+from oracle import oracle
+from rustcolmap_b200 import scene, sift
+
+DESC_TOL = 1e-4
+
+
+def sift_size(w, h, max_dim):
+    """sift.rs:436-444: long side to max_dim when larger, sides >= 1."""
+    m = max(w, h)
+    if m <= max_dim:
+        return w, h
+    s = max_dim / m
+    r = lambda v: int(np.floor(v * s + 0.5))
+    return max(r(w), 1), max(r(h), 1)
+
+
+def oracle_sift(img, max_dim=1600, max_features=2048, thr=0.0067):
+    a = img if img.ndim == 3 else img[:, :, None]
+    h, w = a.shape[:2]
+    mw, mh = sift_size(w, h, max_dim)
+    g, rgb = oracle.resize_view(a, mw, mh)
+    return oracle.extract_sift(g, rgb, max_features, thr), (mw, mh)
+
+
+def blob(h=96, w=128, cx=60.5, cy=40.0, s=5.0):
+    yy, xx = np.mgrid[0:h, 0:w]
+    v = 30 + 200 * np.exp(-((xx - cx) ** 2 + (yy - cy) ** 2) / (2 * s * s))
+    return v.astype(np.uint8)
+
+
+def views():
+    sc = scene.corner_room(seed=0)
+    big = scene.orbit_room(seed=3, n_views=2, sizes=((960, 720),), n_boxes=20, per_view_sparse=10)
+    return [sc.views[0], sc.views[5], big.views[0]]
+
+
+# ------------------------------------------------------------------ CPU
+def test_oracle_flat_image_has_no_features():
+    img = np.full((80, 120), 128, np.uint8)
+    (pts, desc, col, nraw), _ = oracle_sift(img)
+    assert nraw == 0 and len(pts) == 0
+
+
+def test_oracle_blob():
+    """A bright Gaussian blob: keypoints near its centre, unit descriptors
+    clipped at 0.2 before the second normalisation."""
+    img = blob()
+    (pts, desc, col, nraw), _ = oracle_sift(img)
+    assert len(pts) > 0 and nraw > 0
+    d = np.hypot(pts[:, 0] - 60.5, pts[:, 1] - 40.0)
+    assert d.min() < 2.0
+    assert np.allclose(np.linalg.norm(desc, axis=1), 1.0, atol=1e-5)
+    assert (desc >= 0).all()
+
+
+def test_oracle_properties_on_rendered_views():
+    for v in views()[:2]:
+        img = np.ascontiguousarray(v.rgb)
+        (pts, desc, col, nraw), (w, h) = oracle_sift(img)
+        assert 0 < len(pts) <= 2048 and nraw >= len(set(map(tuple, pts)))
+        assert (pts[:, 0] >= 0).all() and (pts[:, 0] <= w - 1).all() and (pts[:, 1] <= h - 1).all()
+        # colours: the image at the rounded position (half away from zero)
+        px = np.minimum(np.floor(pts + 0.5).astype(int), [w - 1, h - 1])
+        assert np.array_equal(col, img[px[:, 1], px[:, 0]])
+        assert np.allclose(np.linalg.norm(desc, axis=1), 1.0, atol=1e-5)
+        # the cap keeps a prefix of the response-sorted list
+        (p10, d10, c10, _), _ = oracle_sift(img, max_features=10)
+        assert np.array_equal(p10, pts[:10]) and np.array_equal(d10, desc[:10])
+
+
+def test_oracle_contrast_threshold_monotone():
+    img = np.ascontiguousarray(views()[0].gray)
+    n = [oracle_sift(img, thr=t)[0][3] for t in (0.02, 0.0067, 0.003)]
+    assert n[0] <= n[1] <= n[2]
+
+
+# ------------------------------------------------------------------ GPU
+def match(g, o):
+    """Fraction of GPU keypoints with an oracle keypoint at the exact same
+    position whose descriptor agrees within DESC_TOL."""
+    gp, gd = g
+    op, od = o
+    index = {}
+    for i, p in enumerate(map(tuple, op)):
+        index.setdefault(p, []).append(i)
+    ok = 0
+    for i, p in enumerate(map(tuple, gp)):
+        cands = index.get(p, [])
+        if cands and min(np.abs(od[j] - gd[i]).max() for j in cands) <= DESC_TOL:
+            ok += 1
+    return ok / max(len(gp), 1)
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    from rustcolmap_b200 import mvs
+    c = mvs.Context(0)
+    yield c
+    c.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("k,channels,max_dim", [(0, 3, 1600), (1, 1, 1600), (2, 3, 1600), (2, 1, 700),
+                                                (0, 4, 200)])
+def test_gpu_sift_matches_oracle(ctx, k, channels, max_dim):
+    v = views()[k]
+    img = np.ascontiguousarray(v.gray if channels == 1 else v.rgb)
+    if channels == 4:
+        img = np.concatenate([img, np.full(img.shape[:2] + (1,), 77, np.uint8)], axis=2)
+    opts = sift.SiftOptions(max_dim=max_dim)
+    f = sift.extract_sift(img, "v", opts, ctx)
+    (pts, desc, col, nraw), (w, h) = oracle_sift(img, max_dim)
+    assert (f.width, f.height) == (w, h)
+    assert f.n_raw == nraw, "scale-space extrema differ"
+    assert abs(len(f.pts) - len(pts)) <= max(1, len(pts) // 100)
+    assert match((f.pts, f.desc), (pts, desc)) >= 0.99
+    same = min(len(pts), len(f.pts))
+    exact = np.mean([np.array_equal(f.pts[i], pts[i]) for i in range(same)])
+    print(f"\n{w}x{h} c={channels}: {len(f.pts)} keypoints, {nraw} extrema, "
+          f"{exact:.4f} in identical order, max desc diff "
+          f"{np.abs(f.desc[:same] - desc[:same]).max() if same else 0:.2e}")
+    assert np.allclose(np.linalg.norm(f.desc, axis=1), 1.0, atol=1e-5)
+
+
+@pytest.mark.gpu
+def test_gpu_sift_edge_cases(ctx):
+    f = sift.extract_sift(np.full((50, 70), 9, np.uint8), ctx=ctx)
+    assert len(f.pts) == 0 and f.n_raw == 0
+    f = sift.extract_sift(np.zeros((1, 1), np.uint8), ctx=ctx)
+    assert len(f.pts) == 0 and (f.width, f.height) == (1, 1)
+    img = blob()
+    f = sift.extract_sift(img, ctx=ctx)
+    (pts, desc, _, nraw), _ = oracle_sift(img)
+    assert f.n_raw == nraw and match((f.pts, f.desc), (pts, desc)) >= 0.99
+    f10 = sift.extract_sift(np.ascontiguousarray(views()[0].rgb), opts=sift.SiftOptions(max_features=10), ctx=ctx)
+    assert len(f10.pts) == 10
+    with pytest.raises(sift.RcmvsError):
+        sift.extract_sift(np.zeros((4, 4, 5), np.uint8), ctx=ctx)
