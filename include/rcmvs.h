@@ -392,6 +392,26 @@ int rcmvs_extract_sift(rcmvs_ctx* ctx, const uint8_t* img, int32_t w, int32_t h,
                        const rcmvs_sift_options* opts, rcmvs_sift_frame* out);
 void rcmvs_sift_frame_free(rcmvs_sift_frame* frame);
 
+/* Matches of a batch of image pairs; pair p's matches are
+ * a[offsets[p] .. offsets[p+1]) (indices into the first frame's keypoints,
+ * ascending) and b[...] (into the second's).  Library-allocated
+ * (rcmvs_matches_free). */
+typedef struct rcmvs_matches {
+    uint64_t n_pairs;
+    uint64_t* offsets;       /* n_pairs + 1 */
+    uint32_t* a;
+    uint32_t* b;
+} rcmvs_matches;
+
+/* `matching::match_pair` (sfm-lite/src/matching.rs:22-95) for n_pairs pairs
+ * (pairs[2p], pairs[2p+1]) of frames whose descriptors are desc[f]
+ * (n_desc[f] x 128 floats each): mutual nearest neighbours by squared L2
+ * distance, summed in f32 in the reference's order, with Lowe's ratio test
+ * (`ratio`, cast to f32) both ways and the 0.9 absolute cap. */
+int rcmvs_match_pairs(rcmvs_ctx* ctx, const float* const* desc, const int32_t* n_desc, int32_t n_frames,
+                      const int32_t* pairs, int32_t n_pairs, double ratio, rcmvs_matches* out);
+void rcmvs_matches_free(rcmvs_matches* matches);
+
 /* ---------------------------------------------------------- diagnostics */
 
 /* `plane_cost` (mvs/src/stereo.rs:158-228) evaluated at every pixel of the

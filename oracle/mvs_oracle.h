@@ -73,6 +73,10 @@ void orc_free(void* p);
  * resolution (gray w*h, rgb w*h*3): keypoints (x, y) n*2, descriptors
  * n*128, colours n*3 (malloc'ed; orc_free); n_raw (nullable) gets the
  * number of scale-space extrema kept by the fit and rejection tests. */
+/* match_pair (sfm-lite/src/matching.rs:22-95) of two descriptor sets
+ * (na x 128, nb x 128); out_a / out_b need min(na, nb) entries. */
+void orc_match_pair(const float* a, uint32_t na, const float* b, uint32_t nb, double ratio, uint32_t* out_a,
+                    uint32_t* out_b, uint64_t* n_out);
 int orc_extract_sift(const uint8_t* gray, const uint8_t* rgb, int32_t w, int32_t h, uint32_t max_features,
                      double contrast_thr, double** pts_out, float** desc_out, uint8_t** colors_out,
                      uint64_t* n_out, uint64_t* n_raw_out);

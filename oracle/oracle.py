@@ -56,6 +56,8 @@ def lib():
         L.orc_fuse_reduce.argtypes = [vp, vp, u64, vp, u64, vp, vp, vp, vp]
         L.orc_resize_view.argtypes = [vp, i32, i32, i32, i32, i32, vp, vp]
         L.orc_extract_sift.argtypes = [vp, vp, i32, i32, C.c_uint32, f64, vp, vp, vp, vp, vp]
+        L.orc_match_pair.argtypes = [vp, C.c_uint32, vp, C.c_uint32, f64, vp, vp, vp]
+        L.orc_match_pair.restype = None
         L.orc_resize_view.restype = None
         _lib = L
     return _lib
@@ -261,6 +263,18 @@ def extract_sift(gray, rgb, max_features=2048, contrast_thr=0.0067):
     for p in (pp, dp, cp):
         lib().orc_free(p)
     return pts, desc, col, nraw.value
+
+
+def match_pair(da, db, ratio=0.8):
+    """match_pair of two descriptor sets: (a indices, b indices) u32."""
+    a = np.ascontiguousarray(da, dtype=np.float32).reshape(-1, 128)
+    b = np.ascontiguousarray(db, dtype=np.float32).reshape(-1, 128)
+    k = max(min(len(a), len(b)), 1)
+    oa, ob = np.zeros(k, np.uint32), np.zeros(k, np.uint32)
+    n = C.c_uint64()
+    lib().orc_match_pair(a.ctypes.data, len(a), b.ctypes.data, len(b), ratio, oa.ctypes.data, ob.ctypes.data,
+                         C.byref(n))
+    return oa[: n.value].copy(), ob[: n.value].copy()
 
 
 def write_ply_binary(path, xyz, rgb):

@@ -415,3 +415,76 @@ int orc_extract_sift(const uint8_t* gray, const uint8_t* rgb, int32_t w32, int32
 }
 
 }  // extern "C"
+
+extern "C" {
+
+// sfm-lite/src/matching.rs:22-95  match_pair: nearest and second-nearest
+// neighbour by serial f32 squared distance in both directions, Lowe ratio
+// test both ways and the mutual check.  out_a / out_b need min(na, nb)
+// entries.
+void orc_match_pair(const float* a, uint32_t na, const float* b, uint32_t nb, double ratio64, uint32_t* out_a,
+                    uint32_t* out_b, uint64_t* n_out) {
+    *n_out = 0;
+    if (na == 0 || nb == 0) return;
+    struct Best {
+        uint32_t idx;
+        float d1, d2;
+    };
+    auto scan = [](const float* q, const float* set, uint32_t n) {
+        float best = INFINITY, second = INFINITY;
+        uint32_t bi = UINT32_MAX;
+        for (uint32_t j = 0; j < n; ++j) {
+            float s = 0.0f;
+            for (int k = 0; k < DESC_LEN; ++k) {
+                const float d = q[k] - set[(size_t)j * DESC_LEN + k];
+                s += d * d;
+            }
+            if (s < best) {
+                second = best;
+                best = s;
+                bi = j;
+            } else if (s < second) {
+                second = s;
+            }
+        }
+        return Best{bi, best, second};
+    };
+    std::vector<Best> fwd(na), bwd(nb);
+    for (uint32_t i = 0; i < na; ++i) fwd[i] = scan(a + (size_t)i * DESC_LEN, b, nb);
+    // backward distances subtract in the same order (a - b), as the reference
+    for (uint32_t j = 0; j < nb; ++j) {
+        float best = INFINITY, second = INFINITY;
+        uint32_t bi = UINT32_MAX;
+        for (uint32_t i = 0; i < na; ++i) {
+            float s = 0.0f;
+            for (int k = 0; k < DESC_LEN; ++k) {
+                const float d = a[(size_t)i * DESC_LEN + k] - b[(size_t)j * DESC_LEN + k];
+                s += d * d;
+            }
+            if (s < best) {
+                second = best;
+                best = s;
+                bi = i;
+            } else if (s < second) {
+                second = s;
+            }
+        }
+        bwd[j] = Best{bi, best, second};
+    }
+    const float ratio = (float)ratio64;
+    uint64_t n = 0;
+    for (uint32_t i = 0; i < na; ++i) {
+        const Best& f = fwd[i];
+        if (f.idx == UINT32_MAX || !std::isfinite(f.d2)) continue;
+        if (f.d1 > 0.9f || f.d1 > ratio * f.d2) continue;
+        const Best& g = bwd[f.idx];
+        if (g.idx != i) continue;
+        if (!std::isfinite(g.d2) || g.d1 > ratio * g.d2) continue;
+        out_a[n] = i;
+        out_b[n] = f.idx;
+        ++n;
+    }
+    *n_out = n;
+}
+
+}  // extern "C"

@@ -78,6 +78,10 @@ class SiftFrame(C.Structure):
                 ("pts", C.c_void_p), ("desc", C.c_void_p), ("colors", C.c_void_p)]
 
 
+class Matches(C.Structure):
+    _fields_ = [("n_pairs", C.c_uint64), ("offsets", C.c_void_p), ("a", C.c_void_p), ("b", C.c_void_p)]
+
+
 class DepthOut(C.Structure):
     _fields_ = [("depth", C.c_void_p), ("cost", C.c_void_p), ("normal", C.c_void_p)]
 

@@ -86,6 +86,8 @@ def mvs():
         "rcmvs_sift_options_default": ([vp], None),
         "rcmvs_extract_sift": ([vp, vp, i32, i32, i32, vp, vp], C.c_int),
         "rcmvs_sift_frame_free": ([vp], None),
+        "rcmvs_match_pairs": ([vp, vp, vp, i32, vp, i32, C.c_double, vp], C.c_int),
+        "rcmvs_matches_free": ([vp], None),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -129,4 +131,5 @@ _SIG_NAMES = [
     "rcmvs_tune_set", "rcmvs_depth_vis", "rcmvs_scene_depth_vis", "rcmvs_write_png_gray",
     "rcmvs_working_size", "rcmvs_resize_view", "rcmvs_fuse_candidates", "rcmvs_fuse_reduce",
     "rcmvs_scene_fuse_candidates", "rcmvs_sift_options_default", "rcmvs_extract_sift", "rcmvs_sift_frame_free",
+    "rcmvs_match_pairs", "rcmvs_matches_free",
 ]

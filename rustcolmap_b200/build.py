@@ -28,7 +28,7 @@ FLAGS = ARCH + [
 
 LIBS = {
     "librcmvs.so": ["capi.cu", "census.cu", "stereo.cu", "fuse.cu", "noalloc.cu", "learned.cu", "learned_api.cu",
-                   "schedule.cu", "depthvis.cu", "resize.cu", "sift.cu"],
+                   "schedule.cu", "depthvis.cu", "resize.cu", "sift.cu", "match.cu"],
     "librcscene.so": ["scene.cu"],
 }
 LINK = {"librcmvs.so": ["-lz"]}  # zlib: the grey PNG writer

@@ -1,5 +1,7 @@
-"""SIFT feature extraction on the GPU: the mirror of `sift::extract_sift`
-(sfm-lite/src/sift.rs:435-555) over librcmvs (rcmvs_extract_sift).
+"""SIFT features and descriptor matching on the GPU: the mirrors of
+`sift::extract_sift` (sfm-lite/src/sift.rs:435-555) and
+`matching::match_pair` (sfm-lite/src/matching.rs:22-95) over librcmvs
+(rcmvs_extract_sift, rcmvs_match_pairs).
 
 There is no CPU path: a missing library or a CUDA error raises RcmvsError.
 """
@@ -61,3 +63,36 @@ def extract_sift(img, name="", opts=None, ctx=None):
         return SiftFrame(name, f.width, f.height, pts, desc, col, int(f.n_raw))
     finally:
         ctx._L.rcmvs_sift_frame_free(C.byref(f))
+
+
+def match_pairs(descs, pairs, ratio=0.8, ctx=None):
+    """match_pair for many pairs of frames in one batched call.  descs: list
+    of (n_f, 128) f32 descriptor arrays; pairs: list of (i, j).  Returns one
+    (a indices, b indices) pair of u32 arrays per pair, in the reference's
+    order."""
+    from .mvs import _ctx
+    ctx = _ctx(ctx)
+    ds = [np.ascontiguousarray(d, dtype=np.float32).reshape(-1, DESC_LEN) for d in descs]
+    ptrs = (C.c_void_p * max(len(ds), 1))(*[d.ctypes.data if len(d) else None for d in ds])
+    nd = np.array([len(d) for d in ds] or [0], np.int32)
+    pr = np.array(list(pairs) or [(0, 0)], np.int32).reshape(-1, 2)
+    m = _abi.Matches()
+    ctx.check(ctx._L.rcmvs_match_pairs(ctx.ptr, ptrs, nd.ctypes.data, len(ds), pr.ctypes.data, len(pairs),
+                                       float(ratio), C.byref(m)))
+    try:
+        npairs = len(pairs)
+        off = np.ctypeslib.as_array((C.c_uint64 * (npairs + 1)).from_address(m.offsets)).copy()
+        tot = int(off[-1])
+        k = max(tot, 1)
+        a = np.ctypeslib.as_array((C.c_uint32 * k).from_address(m.a))[:tot].copy()
+        b = np.ctypeslib.as_array((C.c_uint32 * k).from_address(m.b))[:tot].copy()
+        return [(a[off[p]:off[p + 1]], b[off[p]:off[p + 1]]) for p in range(npairs)]
+    finally:
+        ctx._L.rcmvs_matches_free(C.byref(m))
+
+
+def match_pair(fa, fb, ratio=0.8, ctx=None):
+    """matching::match_pair of two SiftFrames (or descriptor arrays)."""
+    da = fa.desc if isinstance(fa, SiftFrame) else fa
+    db = fb.desc if isinstance(fb, SiftFrame) else fb
+    return match_pairs([da, db], [(0, 1)], ratio, ctx)[0]

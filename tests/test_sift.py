@@ -150,3 +150,96 @@ def test_gpu_sift_edge_cases(ctx):
     assert len(f10.pts) == 10
     with pytest.raises(sift.RcmvsError):
         sift.extract_sift(np.zeros((4, 4, 5), np.uint8), ctx=ctx)
+
+
+# ------------------------------------------------------------------ matching
+def match_numpy(a, b, ratio=0.8):
+    """Second restatement of match_pair: the same serial f32 sums,
+    vectorised over the pairs of descriptors."""
+    a = np.asarray(a, np.float32)
+    b = np.asarray(b, np.float32)
+    if len(a) == 0 or len(b) == 0:
+        return np.zeros(0, np.uint32), np.zeros(0, np.uint32)
+    s = np.zeros((len(a), len(b)), np.float32)
+    for k in range(128):
+        d = a[:, None, k] - b[None, :, k]
+        s = s + d * d
+
+    def two(m):  # first minimum and second smallest, row-wise
+        idx = np.argmin(m, axis=1)
+        best = m[np.arange(len(m)), idx]
+        rest = m.copy()
+        rest[np.arange(len(m)), idx] = np.inf
+        return idx, best, rest.min(axis=1)
+    fi, f1, f2 = two(s)
+    bi, b1, b2 = two(s.T)
+    r = np.float32(ratio)
+    oa, ob = [], []
+    for i in range(len(a)):
+        if not np.isfinite(f2[i]) or f1[i] > np.float32(0.9) or f1[i] > r * f2[i]:
+            continue
+        j = fi[i]
+        if bi[j] != i or not np.isfinite(b2[j]) or b1[j] > r * b2[j]:
+            continue
+        oa.append(i)
+        ob.append(j)
+    return np.array(oa, np.uint32), np.array(ob, np.uint32)
+
+
+def desc_sets(seed, na, nb, noise=0.02, dup=0):
+    rng = np.random.default_rng(seed)
+    a = rng.random((na, 128)).astype(np.float32)
+    a /= np.linalg.norm(a, axis=1, keepdims=True)
+    perm = rng.permutation(max(na, nb))[:nb] % max(na, 1)
+    b = (a[perm] if na else rng.random((nb, 128)).astype(np.float32)) + rng.normal(0, noise, (nb, 128)).astype(np.float32)
+    b = np.abs(b)
+    b /= np.maximum(np.linalg.norm(b, axis=1, keepdims=True), 1e-12)
+    if dup and nb > dup:
+        b[-dup:] = b[:dup]  # exact duplicates: equal distances, index ties
+    return a, b.astype(np.float32)
+
+
+def test_oracle_match_pair_known_answers():
+    a, _ = desc_sets(0, 50, 50)
+    ma, mb = oracle.match_pair(a, a)
+    assert np.array_equal(ma, np.arange(50)) and np.array_equal(mb, np.arange(50))
+    ma, mb = oracle.match_pair(a, a[::-1])
+    assert np.array_equal(mb, 49 - ma) and len(ma) == 50
+    # a noisy copy with its first five rows twice: those five are ambiguous
+    # (equal nonzero best and second distances fail the ratio test) ...
+    noisy = a + np.float32(0.01) * desc_sets(9, 50, 50)[0]
+    dup = np.concatenate([noisy, noisy[:5]])
+    ma, mb = oracle.match_pair(a, dup)
+    assert ma.tolist() == list(range(5, 50)) and mb.tolist() == list(range(5, 50))
+    # ... while an exact duplicate at distance 0 passes (0 > 0.8 * 0 is false)
+    ma, mb = oracle.match_pair(a, np.concatenate([a, a[:5]]))
+    assert ma.tolist() == list(range(50))
+    assert len(oracle.match_pair(a[:0], a)[0]) == 0 and len(oracle.match_pair(a, a[:1])[0]) == 0
+
+
+@pytest.mark.parametrize("na,nb,noise,dup", [(120, 90, 0.02, 0), (64, 64, 0.05, 7), (1, 40, 0.0, 0), (33, 2, 0.01, 0)])
+def test_oracle_match_pair_matches_numpy(na, nb, noise, dup):
+    a, b = desc_sets(na * nb, na, nb, noise, dup)
+    for ratio in (0.8, 0.6):
+        x = oracle.match_pair(a, b, ratio)
+        y = match_numpy(a, b, ratio)
+        assert np.array_equal(x[0], y[0]) and np.array_equal(x[1], y[1])
+
+
+@pytest.mark.gpu
+def test_gpu_match_pairs_matches_oracle(ctx):
+    sets = [desc_sets(1, 300, 250, 0.03, 6)[0], desc_sets(1, 300, 250, 0.03, 6)[1], desc_sets(2, 65, 129)[1],
+            desc_sets(3, 1, 1)[0], np.zeros((0, 128), np.float32)]
+    v = views()
+    f0 = sift.extract_sift(np.ascontiguousarray(v[0].rgb), ctx=ctx)
+    f1 = sift.extract_sift(np.ascontiguousarray(v[1].rgb), ctx=ctx)
+    sets += [f0.desc, f1.desc]
+    pairs = [(0, 1), (1, 0), (0, 2), (2, 1), (3, 0), (0, 3), (4, 0), (1, 4), (5, 6), (6, 5), (5, 5), (2, 2)]
+    for ratio in (0.8, 0.7):
+        got = sift.match_pairs(sets, pairs, ratio, ctx)
+        for (i, j), (ga, gb) in zip(pairs, got):
+            oa, ob = oracle.match_pair(sets[i], sets[j], ratio)
+            assert np.array_equal(ga, oa) and np.array_equal(gb, ob), (i, j, ratio)
+    ga, gb = sift.match_pair(f0, f1, ctx=ctx)
+    assert len(ga) > 50
+    print(f"\nSIFT 384x288 views 0 and 5: {len(ga)} mutual matches of {len(f0.pts)} x {len(f1.pts)}")
