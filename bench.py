@@ -22,7 +22,11 @@ e2e    the same metric through rcmvs_run_mvs_learned with pinned host
 --impl reference times the reference algorithm's CPU implementation (the
 oracle port; the Rust reference cannot be built here) on the host cores.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--config c5|c2|c1]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config c5|c3|c2|c1|sfm]
+
+--config sfm times the SfM front end instead: SIFT extraction of 48 RGB
+1600x1200 images and exhaustive mutual matching of their 1128 pairs per
+step, through the host-buffer API (its own metric, images/s).
 """
 import argparse
 import json
@@ -277,13 +281,147 @@ def gt_summary(ds, sc, jobs, scene):
             "tol": "1% relative inverse depth", "views": len(jobs)}
 
 
+SFM_METRIC = "1600x1200 images/s through SIFT (2048 features) + exhaustive mutual matching of all pairs"
+SFM_IMAGES = 48
+SFM_DESC = (f"{SFM_IMAGES} synthetic RGB views 1600x1200 (room + 20 boxes, orbit); step = extract_sift on every "
+            f"view (max_dim 1600, 2048 features, contrast 0.0067) + match_pair on all "
+            f"{SFM_IMAGES * (SFM_IMAGES - 1) // 2} pairs (ratio 0.8)")
+
+
+def sfm_images(device):
+    from rustcolmap_b200 import scene
+    sc = scene.orbit_room(seed=11, n_views=SFM_IMAGES, sizes=((1600, 1200),), n_boxes=20, per_view_sparse=10,
+                          device=device)
+    return [np.ascontiguousarray(v.rgb) for v in sc.views]
+
+
+def sfm_cpu(imgs, n_img, n_pairs):
+    """The oracle on all host cores: SIFT on n_img images and match_pair on
+    n_pairs pairs of their descriptors, images and pairs spread over a
+    thread pool (the oracle's C calls release the GIL).  Returns (images/s
+    of the full step composition, sample description, threads)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from oracle import oracle
+    from rustcolmap_b200 import colmap
+    nt = os.cpu_count() or 1
+    preps = [colmap.gray_rgb(im) for im in imgs[:n_img]]
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(nt) as ex:
+        outs = list(ex.map(lambda p: oracle.extract_sift(p[0], p[1]), preps))
+    t_img = (time.perf_counter() - t0) / n_img
+    descs = [o[1] for o in outs]
+    prs = [(i % n_img, (i + 1 + i // n_img) % n_img) for i in range(n_pairs)]
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(nt) as ex:
+        list(ex.map(lambda q: oracle.match_pair(descs[q[0]], descs[q[1]]), prs))
+    t_pair = (time.perf_counter() - t0) / n_pairs
+    step = SFM_IMAGES * t_img + SFM_IMAGES * (SFM_IMAGES - 1) // 2 * t_pair
+    desc = (f"{n_img} images and {n_pairs} pairs on {nt} threads ({1e3 * t_img:.0f} ms per image, "
+            f"{1e3 * t_pair:.1f} ms per pair, amortised), scaled to the step's {SFM_IMAGES} images and "
+            f"{SFM_IMAGES * (SFM_IMAGES - 1) // 2} pairs")
+    return SFM_IMAGES / step, desc, nt
+
+
+def run_sfm(args):
+    """--config sfm: the SfM front end (SIFT + matching) on one GPU."""
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        imgs = sfm_images(0 if _has_gpu() else -1)
+        for _ in range(args.warmup):
+            sfm_cpu(imgs, 2, 4)
+        vals = [sfm_cpu(imgs, 16, 48) for _ in range(args.steps)]
+        v = statistics.median(x[0] for x in vals)
+        line = {"impl": "reference", "metric": SFM_METRIC, "value": v, "unit": "images/s", "n_gpus": ws,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * SFM_IMAGES / v,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64",
+                "data": "synthetic", "config": {"workload": "sfm: " + SFM_DESC},
+                "cpu_baseline": {"value": v, "unit": "images/s", "cores": vals[0][2], "kind": "port",
+                                 "sample": vals[0][1]},
+                "e2e": {"value": v, "unit": "images/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+    import torch
+
+    from rustcolmap_b200 import mvs, sift
+    ws, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    imgs = sfm_images(local)
+    ctx = mvs.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{local}")
+    pairs = [(i, j) for i in range(SFM_IMAGES) for j in range(i + 1, SFM_IMAGES)]
+    state = {}
+
+    def step():
+        frames = [sift.extract_sift(im, ctx=ctx) for im in imgs]
+        m = sift.match_pairs([f.desc for f in frames], pairs, 0.8, ctx)
+        state.update(frames=frames, matches=m)
+
+    for _ in range(args.warmup):
+        step()
+    clk = ClockSampler(local)
+    ctx.timing(True)
+    max_over_ranks(0.0, ws, local)
+    torch.cuda.synchronize()
+    clk.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    ms = max_over_ranks(ms, ws, local)
+    kt = {k: ctx.kernel_time(k) for k in ("sift_pyramid", "sift_extrema", "sift_orient", "sift_desc",
+                                          "match_dist", "match_select")}
+    ctx.timing(False)
+    frames, m = state["frames"], state["matches"]
+    nfeat = [len(f.pts) for f in frames]
+    ops = sum(nfeat[i] * nfeat[j] for i, j in pairs) * 128 * 3  # sub, mul, add per component
+    dist_ms, dist_n = kt["match_dist"]
+    dist_launch_ms = dist_ms / max(dist_n, 1)
+    ops_per_launch = ops * args.steps / max(dist_n, 1)
+    achieved = ops_per_launch / (dist_launch_ms * 1e-3) / 1e12
+    value = ws * SFM_IMAGES / (ms * 1e-3)
+    h2d = sum(im.nbytes for im in imgs) + sum(f.desc.nbytes for f in frames)
+    d2h = sum(f.pts.nbytes + f.desc.nbytes + f.colors.nbytes for f in frames) + sum(a.nbytes + b.nbytes for a, b in m)
+    line = {"metric": SFM_METRIC, "value": value, "unit": "images/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32/f64 (SIFT), f32 (matching)", "data": "synthetic",
+            "config": {"workload": "sfm: " + SFM_DESC, "l2": "inputs larger than L2 (276 MB of images)",
+                       "features_mean": float(np.mean(nfeat)),
+                       "matches_mean": float(np.mean([len(a) for a, _ in m]))},
+            "roofline": {"bound": "fp32_issue", "kernel": "match_dist", "achieved": achieved,
+                         "peak": FP32_NOMINAL_TOPS, "unit": "Top/s", "frac": achieved / FP32_NOMINAL_TOPS,
+                         "traffic": None, "peak_source": "nominal 148 SM x 128 FP32 lanes x 1.965 GHz",
+                         "ops_per_launch": ops_per_launch, "avg_launch_ms": dist_launch_ms},
+            "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kt.items()},
+            "e2e": {"value": value, "unit": "images/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "note": "value itself is measured through the host-buffer API (rcmvs_extract_sift, "
+                            "rcmvs_match_pairs), copies included"},
+            "clocks": clocks}
+    if rank == 0 and not args.no_cpu_baseline:
+        v, desc, nt = sfm_cpu(imgs, 16, 48)
+        line["cpu_baseline"] = {"value": v, "unit": "images/s", "cores": nt, "kind": "port", "sample": desc}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c5", choices=["c5", "c3", "c2", "c1"])
+    ap.add_argument("--config", default="c5", choices=["c5", "c3", "c2", "c1", "sfm"])
     ap.add_argument("--cpu-rows", type=int, default=24, help="rows of the CPU-baseline band")
     ap.add_argument("--ref-rows", type=int, default=12, help="rows per step of the reference arm")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -302,6 +440,9 @@ def main():
     ap.add_argument("--tile", default="", help="WxH stereo tile (default: the library's 8x8)")
     args = ap.parse_args()
     assert args.warmup >= 3 or os.environ.get("RCMVS_BENCH_ALLOW_SHORT"), "warm-up must be >= 3 steps"
+    if args.config == "sfm":
+        run_sfm(args)
+        return
     cfg = configs()[args.config]
     if args.views and cfg["scene"] is not None:
         cfg["scene"] = dict(cfg["scene"], n_views=args.views)

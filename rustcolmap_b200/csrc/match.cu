@@ -270,9 +270,13 @@ int rcmvs_match_pairs(rcmvs_ctx* ctx, const float* const* desc, const int32_t* n
             MCK(A.get(M_MB, sizeof(uint32_t) * (size_t)rows, &p_mb));
             MCK(cudaMemcpyAsync(p_jobs, jobs.data(), sizeof(PairJob) * jobs.size(), cudaMemcpyHostToDevice, st));
             const unsigned nj = (unsigned)jobs.size();
+            const SpanHook& hook = ctx->hook();
+            hook.begin("match_dist");
             dist_kernel<<<dim3((max_nb + TILE - 1) / TILE, (max_na + TILE - 1) / TILE, nj), 256, 0, st>>>(
                 (const float*)p_desc, (const PairJob*)p_jobs, (float*)p_dmat);
             MCK(cudaGetLastError());
+            hook.end("match_dist");
+            hook.begin("match_select");
             rows_kernel<<<dim3((max_na + 7) / 8, nj), 256, 0, st>>>((const PairJob*)p_jobs, (const float*)p_dmat,
                                                                    (Nearest*)p_fwd);
             MCK(cudaGetLastError());
@@ -282,6 +286,7 @@ int rcmvs_match_pairs(rcmvs_ctx* ctx, const float* const* desc, const int32_t* n
             decide_kernel<<<dim3((max_na + 255) / 256, nj), 256, 0, st>>>(
                 (const PairJob*)p_jobs, (const Nearest*)p_fwd, (const Nearest*)p_bwd, r32, (uint32_t*)p_mb);
             MCK(cudaGetLastError());
+            hook.end("match_select");
             std::vector<uint32_t> mb((size_t)rows);
             MCK(cudaMemcpyAsync(mb.data(), p_mb, sizeof(uint32_t) * rows, cudaMemcpyDeviceToHost, st));
             MCK(cudaStreamSynchronize(st));

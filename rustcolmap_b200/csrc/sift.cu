@@ -19,8 +19,10 @@
 //               picks up to four peaks (sift.rs:274-334)
 //   descriptor  one warp per (keypoint, peak): the same split over the window
 //               (bilinear gradients, rotation, trilinear weights; up to 8
-//               histogram entries per sample), lanes owning 4 of the 128 bins;
-//               L2 -> clip 0.2 -> L2 in f32 (sift.rs:340-431)
+//               histogram entries per sample).  Lane L owns the 4 bins of cell
+//               column L / 8 and orientation L % 8, so it finds its share of a
+//               sample from the sample's (row, column, orientation) base by
+//               arithmetic; L2 -> clip 0.2 -> L2 in f32 (sift.rs:340-431)
 //   output      stable descending radix sort on the response (the reference's
 //               stable sort_by), the first max_features, clamped positions and
 //               colours (sift.rs:519-554)
@@ -365,7 +367,7 @@ __global__ void __launch_bounds__(32 * WARPS) desc_kernel(KpArrays kp, const int
                                                          const float* __restrict__ gy_all, int w, int h,
                                                          float* __restrict__ desc, uint8_t* __restrict__ valid) {
     constexpr int D = 4, N = 8;
-    __shared__ int16_t cb[WARPS][32 * 8];
+    __shared__ int hdr[WARPS][32];  // per sample: packed (by0, bx0, ob0 mod 8), or -1
     __shared__ double cv[WARPS][32 * 8];
     __shared__ float sd[WARPS][DESC_LEN];
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -384,13 +386,13 @@ __global__ void __launch_bounds__(32 * WARPS) desc_kernel(KpArrays kp, const int
     const double exp_scale = -1.0 / ((double)(D * D) * 0.5);
     const double half = (double)D * 0.5;
     const int side = 2 * radius + 1, total = side * side;
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};  // bins lane, lane + 32, lane + 64, lane + 96
+    // Lane L owns the bins 32q + L (q = 0..3): cell row q, cell column L / 8,
+    // orientation L % 8.  A sample adds to such a bin at most once.
+    const int cx = lane >> 3, co = lane & 7;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
     for (int base = 0; base < total; base += 32) {
         const int s = base + lane;
-        int16_t bins[8];
-        double vals[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) bins[j] = -1, vals[j] = 0.0;
+        int hd = -1;
         if (s < total) {
             const int dy = s / side - radius, dx = s % side - radius;
             const double sx = x + (double)dx, sy = y + (double)dy;
@@ -409,40 +411,41 @@ __global__ void __launch_bounds__(32 * WARPS) desc_kernel(KpArrays kp, const int
                         double wgt =
                             ((bx - half + 0.5) * (bx - half + 0.5) + (by - half + 0.5) * (by - half + 0.5)) * exp_scale;
                         wgt = exp(wgt) * mag;
-                        const long long bx0 = (long long)floor(bx), by0 = (long long)floor(by),
-                                        ob0 = (long long)floor(ob);
+                        // bx, by in [-1, 4], ob in [0, 8]
+                        const int bx0 = (int)floor(bx), by0 = (int)floor(by), ob0 = (int)floor(ob);
                         const double fx = bx - (double)bx0, fy = by - (double)by0, fo = ob - (double)ob0;
 #pragma unroll
                         for (int iy = 0; iy < 2; ++iy)
 #pragma unroll
                             for (int ix = 0; ix < 2; ++ix) {
-                                const long long bxi = bx0 + ix, byi = by0 + iy;
-                                if (bxi < 0 || byi < 0 || bxi >= D || byi >= D) continue;
                                 const double wy = iy == 0 ? 1.0 - fy : fy;
                                 const double wx = ix == 0 ? 1.0 - fx : fx;
 #pragma unroll
                                 for (int io = 0; io < 2; ++io) {
-                                    const int obi = (int)(((ob0 + io) % N + N) % N);
                                     const double wo = io == 0 ? 1.0 - fo : fo;
-                                    const int j = iy * 4 + ix * 2 + io;
-                                    bins[j] = (int16_t)((byi * D + bxi) * N + obi);
-                                    vals[j] = wgt * wx * wy * wo;
+                                    cv[wid][lane * 8 + iy * 4 + ix * 2 + io] = wgt * wx * wy * wo;
                                 }
                             }
+                        hd = ((by0 + 2) << 8) | ((bx0 + 2) << 4) | (ob0 & 7);
                     }
                 }
             }
         }
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            cb[wid][lane * 8 + j] = bins[j];
-            cv[wid][lane * 8 + j] = vals[j];
-        }
+        hdr[wid][lane] = hd;
         __syncwarp();
         const int m = min(32, total - base);
-        for (int t = 0; t < m * 8; ++t) {
-            const int b = cb[wid][t];
-            if (b >= 0 && (b & 31) == lane) acc[b >> 5] += cv[wid][t];
+        for (int t = 0; t < m; ++t) {
+            const int hv = hdr[wid][t];
+            if (hv < 0) continue;
+            const int ix = cx - (((hv >> 4) & 15) - 2);
+            const int io = (co - (hv & 7)) & 7;
+            if ((unsigned)ix > 1u || io > 1) continue;
+            const int by0 = (hv >> 8) - 2;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int iy = q - by0;
+                if (iy == 0 || iy == 1) acc[q] += cv[wid][t * 8 + iy * 4 + ix * 2 + io];
+            }
         }
         __syncwarp();
     }
@@ -514,6 +517,11 @@ __global__ void final_kernel(const uint32_t* __restrict__ order, int n, const do
         odesc[(int64_t)wid * DESC_LEN + lane + 32 * q] = desc[(int64_t)s * DESC_LEN + lane + 32 * q];
 }
 
+__global__ void iota_kernel(uint32_t* __restrict__ out, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = (uint32_t)i;
+}
+
 unsigned grid_of(int64_t n, int threads = 256) {
     const int64_t b = (n + threads - 1) / threads;
     return (unsigned)std::max<int64_t>(1, std::min<int64_t>(b, 148 * 16));
@@ -556,21 +564,26 @@ enum {
     F_ORESP, F_OXY, F_ODESC, F_SRESP, F_IDX, F_SIDX, F_PTS, F_FDESC, F_COL, F_NEXT
 };
 
+// Grows an arena slot to `need` bytes keeping its first `keep` bytes: a
+// device-to-device copy into a buffer of twice the need when the slot is too
+// small, else the slot as it is.
 int grow_copy(rcmvs_ctx* ctx, int slot, size_t need, size_t keep, void** p) {
-    // grows a slot while keeping its first `keep` bytes
-    void* old = nullptr;
-    SCK(ctx->arena.get(slot, std::max<size_t>(keep, 1), &old));
-    if (need <= keep) {
-        *p = old;
+    DeviceArena& A = ctx->arena;
+    if ((int)A.slots.size() <= slot) A.slots.resize(slot + 1);
+    DeviceArena::Slot& s = A.slots[slot];
+    if (s.p && s.bytes >= need) {
+        *p = s.p;
         return RCMVS_OK;
     }
-    std::vector<unsigned char> host(keep);
-    if (keep) {
-        SCK(cudaMemcpyAsync(host.data(), old, keep, cudaMemcpyDeviceToHost, ctx->stream));
-        SCK(cudaStreamSynchronize(ctx->stream));
-    }
-    SCK(ctx->arena.get(slot, need, p));
-    if (keep) SCK(cudaMemcpyAsync(*p, host.data(), keep, cudaMemcpyHostToDevice, ctx->stream));
+    void* np_ = nullptr;
+    const size_t cap = std::max<size_t>(2 * need, 1 << 20);
+    SCK(cudaMalloc(&np_, cap));
+    if (keep && s.p) SCK(cudaMemcpyAsync(np_, s.p, keep, cudaMemcpyDeviceToDevice, ctx->stream));
+    SCK(cudaStreamSynchronize(ctx->stream));
+    if (s.p) SCK(cudaFree(s.p));
+    s.p = np_;
+    s.bytes = cap;
+    *p = np_;
     return RCMVS_OK;
 }
 
@@ -642,6 +655,7 @@ int rcmvs_extract_sift(rcmvs_ctx* ctx, const uint8_t* img, int32_t w0, int32_t h
             return sfail(ctx, RCMVS_E_LIMIT, "sift: blur kernel too wide");
     }
 
+    const SpanHook& hook = ctx->hook();
     int64_t n_cand = 0;  // descriptors appended so far
     uint64_t n_raw = 0;
     int ow = w, oh = h;
@@ -656,6 +670,7 @@ int rcmvs_extract_sift(rcmvs_ctx* ctx, const uint8_t* img, int32_t w0, int32_t h
         float* tmp = (float*)p_tmp;
         // level 0: the base (blurred by the first sigma in octave 0)
         const float* base = (const float*)p_base;
+        hook.begin("sift_pyramid");
         if (o == 0) {
             blur_kernel<false><<<grid_of(npx), 256, 0, st>>>(base, tmp, ow, oh, first);
             blur_kernel<true><<<grid_of(npx), 256, 0, st>>>(tmp, lev, ow, oh, first);
@@ -669,6 +684,7 @@ int rcmvs_extract_sift(rcmvs_ctx* ctx, const uint8_t* img, int32_t w0, int32_t h
         SCK(cudaGetLastError());
         dog_kernel<<<grid_of(npx), 256, 0, st>>>(lev, (float*)p_dog, npx);
         SCK(cudaGetLastError());
+        hook.end("sift_pyramid");
         const int64_t nt = NSPO * npx;
         if (nt > (int64_t)UINT32_MAX) return sfail(ctx, RCMVS_E_LIMIT, "sift: octave too large");
         SCK(A.get(F_FLAG, (size_t)nt, &p_flag));
@@ -677,9 +693,11 @@ int rcmvs_extract_sift(rcmvs_ctx* ctx, const uint8_t* img, int32_t w0, int32_t h
         SCK(A.get(F_KRESP, sizeof(double) * (size_t)nt, &p_kr));
         SCK(A.get(F_SEL, sizeof(uint32_t) * (size_t)nt, &p_sel));
         SCK(A.get(F_NSEL, sizeof(int) * 4, &p_nsel));
+        hook.begin("sift_extrema");
         extrema_kernel<<<grid_of(nt), 256, 0, st>>>((const float*)p_dog, ow, oh, opts->contrast_thr,
                                                      (uint8_t*)p_flag, (double*)p_kx, (double*)p_ky, (double*)p_kr);
         SCK(cudaGetLastError());
+        hook.end("sift_extrema");
         size_t tb = 0;
         SCK(cub::DeviceSelect::Flagged(nullptr, tb, it, (const uint8_t*)p_flag, (uint32_t*)p_sel, (int*)p_nsel,
                                        (int)nt, st));
@@ -709,9 +727,11 @@ int rcmvs_extract_sift(rcmvs_ctx* ctx, const uint8_t* img, int32_t w0, int32_t h
             SCK(A.get(F_THETA, sizeof(double) * 4 * (size_t)nk, &p_th));
             SCK(A.get(F_CNT, sizeof(int32_t) * (size_t)nk, &p_cnt));
             SCK(A.get(F_OFF, sizeof(int32_t) * ((size_t)nk + 1), &p_off));
+            hook.begin("sift_orient");
             orient_kernel<<<(nk + WARPS - 1) / WARPS, 32 * WARPS, 0, st>>>(
                 kp, nk, (const float*)p_gx, (const float*)p_gy, ow, oh, scale, w, h, (double*)p_th, (int32_t*)p_cnt);
             SCK(cudaGetLastError());
+            hook.end("sift_orient");
             tb = 0;
             SCK(cub::DeviceScan::ExclusiveSum(nullptr, tb, (const int32_t*)p_cnt, (int32_t*)p_off, nk, st));
             SCK(A.get(F_TEMP, tb, &p_temp));
@@ -731,10 +751,12 @@ int rcmvs_extract_sift(rcmvs_ctx* ctx, const uint8_t* img, int32_t w0, int32_t h
                 pairs_kernel<<<grid_of(nk), 256, 0, st>>>((const int32_t*)p_cnt, (const int32_t*)p_off, nk,
                                                           (const double*)p_th, (int32_t*)p_pkp, (double*)p_pth);
                 SCK(cudaGetLastError());
+                hook.begin("sift_desc");
                 desc_kernel<<<(np + WARPS - 1) / WARPS, 32 * WARPS, 0, st>>>(
                     kp, (const int32_t*)p_pkp, (const double*)p_pth, np, (const float*)p_gx, (const float*)p_gy, ow,
                     oh, (float*)p_desc, (uint8_t*)p_valid);
                 SCK(cudaGetLastError());
+                hook.end("sift_desc");
                 tb = 0;
                 SCK(cub::DeviceSelect::Flagged(nullptr, tb, it, (const uint8_t*)p_valid, (uint32_t*)p_psel,
                                                (int*)p_nsel + 1, np, st));
@@ -807,19 +829,17 @@ int rcmvs_extract_sift(rcmvs_ctx* ctx, const uint8_t* img, int32_t w0, int32_t h
     SCK(A.get(F_FDESC, sizeof(float) * DESC_LEN * n_out, &p_fdesc));
     SCK(A.get(F_COL, 3 * (size_t)n_out, &p_col));
     {
-        // indices 0..n_cand-1 as the sort's values
+        // indices 0..n_cand-1 as the sort's values; a stable descending sort
         size_t tb = 0;
         SCK(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, (const double*)p_oresp, (double*)p_sresp,
                                                       (const uint32_t*)p_idx, (uint32_t*)p_sidx, (int)n_cand, 0, 64,
                                                       st));
         SCK(A.get(F_TEMP, tb, &p_temp));
-        std::vector<uint32_t> iota(n_cand);
-        for (int64_t i = 0; i < n_cand; ++i) iota[i] = (uint32_t)i;
-        SCK(cudaMemcpyAsync(p_idx, iota.data(), sizeof(uint32_t) * n_cand, cudaMemcpyHostToDevice, st));
+        iota_kernel<<<grid_of(n_cand), 256, 0, st>>>((uint32_t*)p_idx, n_cand);
+        SCK(cudaGetLastError());
         SCK(cub::DeviceRadixSort::SortPairsDescending(p_temp, tb, (const double*)p_oresp, (double*)p_sresp,
                                                       (const uint32_t*)p_idx, (uint32_t*)p_sidx, (int)n_cand, 0, 64,
                                                       st));
-        SCK(cudaStreamSynchronize(st));  // iota must outlive its copy
     }
     final_kernel<<<(int)((n_out + WARPS - 1) / WARPS), 32 * WARPS, 0, st>>>(
         (const uint32_t*)p_sidx, (int)n_out, (const double*)p_oxy, (const float*)p_odesc, (const uint8_t*)p_rgb, w, h,
