@@ -121,7 +121,7 @@ namespace rcmvs {
 
 // Arena slots of a scene shared by the translation units (the others are
 // private to capi.cu 2-10, fuse.cu 16-37 and 70-74, learned_api.cu 40-47, depthvis.cu 50-55,
-// resize.cu 60-68, sift.cu 80-119 and match.cu 120-127).
+// resize.cu 60-68, sift.cu 80-159 and match.cu 160-167).
 constexpr int kSlotJobs = 0, kSlotJobStart = 1, kSlotQueue = 11, kSlotTuneJobs = 12, kSlotTuneStart = 13;
 
 // resize.cu: argument and size checks of a resize, and the resize itself

@@ -192,8 +192,8 @@ int mfail(rcmvs_ctx* ctx, int code, const std::string& msg) {
                          std::string(#x) + ": " + cudaGetErrorString(e_));                     \
     } while (0)
 
-// Context arena slots 120-127.
-enum { M_DESC = 120, M_JOBS, M_DMAT, M_FWD, M_BWD, M_MB };
+// Context arena slots 160-167.
+enum { M_DESC = 160, M_JOBS, M_DMAT, M_FWD, M_BWD, M_MB };
 
 }  // namespace
 }  // namespace rcmvs
@@ -212,12 +212,22 @@ void rcmvs_matches_free(rcmvs_matches* m) {
     m->n_pairs = 0;
 }
 
+static int match_pairs_impl(rcmvs_ctx* ctx, const float* const* desc, const int32_t* n_desc, int32_t n_frames,
+                            const int32_t* pairs, int32_t n_pairs, double ratio, rcmvs_matches* out);
+
 int rcmvs_match_pairs(rcmvs_ctx* ctx, const float* const* desc, const int32_t* n_desc, int32_t n_frames,
                       const int32_t* pairs, int32_t n_pairs, double ratio, rcmvs_matches* out) {
     if (!ctx || !out || n_frames < 0 || n_pairs < 0 || (n_frames > 0 && (!desc || !n_desc)) ||
         (n_pairs > 0 && !pairs))
         return mfail(ctx, RCMVS_E_ARG, "rcmvs_match_pairs: bad argument");
     std::memset(out, 0, sizeof(*out));
+    const int rc = match_pairs_impl(ctx, desc, n_desc, n_frames, pairs, n_pairs, ratio, out);
+    if (rc) rcmvs_matches_free(out);  // nothing half-built reaches the caller
+    return rc;
+}
+
+static int match_pairs_impl(rcmvs_ctx* ctx, const float* const* desc, const int32_t* n_desc, int32_t n_frames,
+                            const int32_t* pairs, int32_t n_pairs, double ratio, rcmvs_matches* out) {
     std::vector<int64_t> foff(n_frames + 1, 0);
     for (int f = 0; f < n_frames; ++f) {
         if (n_desc[f] < 0 || (n_desc[f] > 0 && !desc[f])) return mfail(ctx, RCMVS_E_ARG, "bad descriptor set");

@@ -23,9 +23,13 @@
 //               column L / 8 and orientation L % 8, so it finds its share of a
 //               sample from the sample's (row, column, orientation) base by
 //               arithmetic; L2 -> clip 0.2 -> L2 in f32 (sift.rs:340-431)
-//   output      stable descending radix sort on the response (the reference's
-//               stable sort_by), the first max_features, clamped positions and
-//               colours (sift.rs:519-554)
+//   output      the reference sorts its descriptors by response (stable) and
+//               keeps the first max_features (sift.rs:543-544).  Responses are
+//               known before descriptors, so the (keypoint, peak) pairs of all
+//               octaves are radix-sorted first (stable, descending) and
+//               descriptors are computed in that order until max_features
+//               valid ones exist: the same output without the descriptors the
+//               cap would discard (about 2k of 30k at 1600x1200)
 //
 // The library builds with --fmad=false: every f32/f64 product and sum rounds
 // as written, so the pyramid, the DoGs and the extrema with their fitted
@@ -65,11 +69,20 @@ struct BlurTaps {
     float k[MAX_TAPS];
 };
 
-struct KpArrays {  // raw keypoints of one octave, in (level, y, x) order
-    double* x;
+struct KpArrays {  // raw keypoints in the reference's (octave, level, y, x) order
+    double* x;       // octave coordinates
     double* y;
     double* resp;
     int32_t* level;
+    int32_t* oct;
+};
+
+constexpr int MAX_OCT = 8;
+struct OctTable {  // per octave: gradients of DoG levels 1..NSPO, size, scale
+    const float* gx[MAX_OCT];
+    const float* gy[MAX_OCT];
+    int w[MAX_OCT], h[MAX_OCT];
+    double scale[MAX_OCT];
 };
 
 __device__ __host__ __forceinline__ double level_sigma(int l) {
@@ -228,13 +241,15 @@ __global__ void extrema_kernel(const float* __restrict__ dogs, int w, int h, dou
 
 // Gathers the compacted keypoints (sel: indices into the flag space).
 __global__ void gather_kp_kernel(const uint32_t* __restrict__ sel, int n, int64_t npx, const double* __restrict__ kx,
-                                 const double* __restrict__ ky, const double* __restrict__ kresp, KpArrays kp) {
+                                 const double* __restrict__ ky, const double* __restrict__ kresp, int octave,
+                                 KpArrays kp) {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const uint32_t t = sel[k];
         kp.x[k] = kx[t];
         kp.y[k] = ky[t];
         kp.resp[k] = kresp[t];
         kp.level[k] = 1 + (int)((int64_t)t / npx);
+        kp.oct[k] = octave;
     }
 }
 
@@ -339,12 +354,15 @@ __global__ void __launch_bounds__(32 * WARPS) orient_kernel(KpArrays kp, int n, 
 
 // (keypoint, peak) pairs in keypoint order, peaks in order
 __global__ void pairs_kernel(const int32_t* __restrict__ cnt, const int32_t* __restrict__ off, int n,
-                             const double* __restrict__ theta, int32_t* __restrict__ pair_kp,
-                             double* __restrict__ pair_theta) {
+                             const double* __restrict__ theta, const double* __restrict__ resp,
+                             int32_t* __restrict__ pair_kp, double* __restrict__ pair_theta,
+                             double* __restrict__ pair_resp, uint32_t* __restrict__ pair_idx) {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
         for (int p = 0; p < cnt[k]; ++p) {
             pair_kp[off[k] + p] = k;
             pair_theta[off[k] + p] = theta[4 * (int64_t)k + p];
+            pair_resp[off[k] + p] = resp[k];
+            pair_idx[off[k] + p] = (uint32_t)(off[k] + p);
         }
 }
 
@@ -360,25 +378,31 @@ __device__ __forceinline__ float bilinear(const float* __restrict__ img, int w, 
     return a * (1.0f - fy) + b * fy;
 }
 
-// sift.rs:340-431.  One warp per (keypoint, peak) pair.
-__global__ void __launch_bounds__(32 * WARPS) desc_kernel(KpArrays kp, const int32_t* __restrict__ pair_kp,
-                                                         const double* __restrict__ pair_theta, int n_pairs,
-                                                         const float* __restrict__ gx_all,
-                                                         const float* __restrict__ gy_all, int w, int h,
+// sift.rs:340-431.  One warp per (keypoint, peak) pair: the pairs at sorted
+// positions base .. base + n_pairs - 1 (order[pos] = pair); descriptor and
+// validity stored at the sorted position.
+__global__ void __launch_bounds__(32 * WARPS) desc_kernel(KpArrays kp, const uint32_t* __restrict__ order,
+                                                         int64_t base, int n_pairs,
+                                                         const int32_t* __restrict__ pair_kp,
+                                                         const double* __restrict__ pair_theta,
+                                                         const __grid_constant__ OctTable oct,
                                                          float* __restrict__ desc, uint8_t* __restrict__ valid) {
     constexpr int D = 4, N = 8;
     __shared__ int hdr[WARPS][32];  // per sample: packed (by0, bx0, ob0 mod 8), or -1
     __shared__ double cv[WARPS][32 * 8];
     __shared__ float sd[WARPS][DESC_LEN];
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int p = blockIdx.x * WARPS + wid;
-    if (p >= n_pairs) return;
-    const int k = pair_kp[p];
-    const double x = kp.x[k], y = kp.y[k], th = pair_theta[p];
-    const int level = kp.level[k];
+    const int i = blockIdx.x * WARPS + wid;
+    if (i >= n_pairs) return;
+    const int64_t pos = base + i;
+    const uint32_t pr = order[pos];
+    const int k = pair_kp[pr];
+    const double x = kp.x[k], y = kp.y[k], th = pair_theta[pr];
+    const int level = kp.level[k], o = kp.oct[k];
+    const int w = oct.w[o], h = oct.h[o];
     const int64_t npx = (int64_t)w * h;
-    const float* gxi = gx_all + (level - 1) * npx;
-    const float* gyi = gy_all + (level - 1) * npx;
+    const float* gxi = oct.gx[o] + (level - 1) * npx;
+    const float* gyi = oct.gy[o] + (level - 1) * npx;
     const double sigma = level_sigma(level);
     const double cell = 3.0 * sigma;
     const int radius = (int)ceil(sqrt(1.5) * cell * ((double)D + 1.0) * 0.5);
@@ -469,43 +493,27 @@ __global__ void __launch_bounds__(32 * WARPS) desc_kernel(KpArrays kp, const int
             if (ok)
                 for (int i = 0; i < DESC_LEN; ++i) d[i] = d[i] / norm2;
         }
-        valid[p] = ok ? 1 : 0;
+        valid[pos] = ok ? 1 : 0;
     }
     __syncwarp();
 #pragma unroll
-    for (int q = 0; q < 4; ++q) desc[(int64_t)p * DESC_LEN + lane + 32 * q] = sd[wid][lane + 32 * q];
+    for (int q = 0; q < 4; ++q) desc[pos * DESC_LEN + lane + 32 * q] = sd[wid][lane + 32 * q];
 }
 
-// Appends the valid (keypoint, peak) descriptors of one octave to the
-// frame's candidate list at offset `at`.
-__global__ void append_kernel(const uint32_t* __restrict__ sel, int n, const int32_t* __restrict__ pair_kp,
-                              KpArrays kp, double scale, const float* __restrict__ desc, int64_t at,
-                              double* __restrict__ out_resp, double* __restrict__ out_xy,
-                              float* __restrict__ out_desc) {
-    const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (wid >= n) return;
-    const uint32_t p = sel[wid];
-    const int k = pair_kp[p];
-    if (lane == 0) {
-        out_resp[at + wid] = kp.resp[k];
-        out_xy[2 * (at + wid)] = kp.x[k] * scale;
-        out_xy[2 * (at + wid) + 1] = kp.y[k] * scale;
-    }
-#pragma unroll
-    for (int q = 0; q < 4; ++q)
-        out_desc[(at + wid) * DESC_LEN + lane + 32 * q] = desc[(int64_t)p * DESC_LEN + lane + 32 * q];
-}
-
-// sift.rs:543-554: the first n after the sort, clamped positions, colours
-__global__ void final_kernel(const uint32_t* __restrict__ order, int n, const double* __restrict__ xy,
+// sift.rs:543-554: output i is the sorted position sel[i] (the i-th valid
+// descriptor in response order); clamped position, descriptor, colour.
+__global__ void final_kernel(const uint32_t* __restrict__ sel, int n, const uint32_t* __restrict__ order,
+                             const int32_t* __restrict__ pair_kp, KpArrays kp, const __grid_constant__ OctTable oct,
                              const float* __restrict__ desc, const uint8_t* __restrict__ rgb, int w, int h,
                              double* __restrict__ pts, float* __restrict__ odesc, uint8_t* __restrict__ col) {
     const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (wid >= n) return;
-    const uint32_t s = order[wid];
+    const uint32_t pos = sel[wid];
     if (lane == 0) {
-        const double x = fmin(fmax(xy[2 * (int64_t)s], 0.0), (double)(w - 1));
-        const double y = fmin(fmax(xy[2 * (int64_t)s + 1], 0.0), (double)(h - 1));
+        const int k = pair_kp[order[pos]];
+        const double scale = oct.scale[kp.oct[k]];
+        const double x = fmin(fmax(kp.x[k] * scale, 0.0), (double)(w - 1));
+        const double y = fmin(fmax(kp.y[k] * scale, 0.0), (double)(h - 1));
         const long long px = min((long long)round(x), (long long)(w - 1));
         const long long py = min((long long)round(y), (long long)(h - 1));
         pts[2 * wid] = x;
@@ -514,12 +522,7 @@ __global__ void final_kernel(const uint32_t* __restrict__ order, int n, const do
     }
 #pragma unroll
     for (int q = 0; q < 4; ++q)
-        odesc[(int64_t)wid * DESC_LEN + lane + 32 * q] = desc[(int64_t)s * DESC_LEN + lane + 32 * q];
-}
-
-__global__ void iota_kernel(uint32_t* __restrict__ out, int64_t n) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        out[i] = (uint32_t)i;
+        odesc[(int64_t)wid * DESC_LEN + lane + 32 * q] = desc[(int64_t)pos * DESC_LEN + lane + 32 * q];
 }
 
 unsigned grid_of(int64_t n, int threads = 256) {
@@ -557,11 +560,12 @@ int sfail(rcmvs_ctx* ctx, int code, const std::string& msg) {
                          std::string(#x) + ": " + cudaGetErrorString(e_));                     \
     } while (0)
 
-// Context arena slots 80-119.
+// Context arena slots 80-159.
 enum {
     F_IN = 80, F_GRAY, F_RGB, F_BASE, F_LEV, F_TMP, F_DOG, F_FLAG, F_KX, F_KY, F_KRESP, F_SEL, F_NSEL, F_TEMP,
-    F_KPX, F_KPY, F_KPRESP, F_KPLEV, F_GX, F_GY, F_THETA, F_CNT, F_OFF, F_PKP, F_PTH, F_DESC, F_VALID, F_PSEL,
-    F_ORESP, F_OXY, F_ODESC, F_SRESP, F_IDX, F_SIDX, F_PTS, F_FDESC, F_COL, F_NEXT
+    F_KPX, F_KPY, F_KPRESP, F_KPLEV, F_KPOCT, F_THETA, F_CNT, F_OFF, F_PKP, F_PTH, F_PRESP, F_PIDX, F_SRESP, F_SIDX,
+    F_DESC, F_VALID, F_OSEL, F_PTS, F_FDESC, F_COL, F_NEXT,
+    F_GRAD = 130  // 130 + 2 * octave: gx, + 1: gy (octaves 0..7)
 };
 
 // Grows an arena slot to `need` bytes keeping its first `keep` bytes: a
@@ -656,13 +660,19 @@ int rcmvs_extract_sift(rcmvs_ctx* ctx, const uint8_t* img, int32_t w0, int32_t h
     }
 
     const SpanHook& hook = ctx->hook();
-    int64_t n_cand = 0;  // descriptors appended so far
+    if (n_oct > MAX_OCT) return sfail(ctx, RCMVS_E_LIMIT, "sift: too many octaves");
+    OctTable table{};
+    int64_t nkp = 0;  // keypoints of all octaves so far
     uint64_t n_raw = 0;
     int ow = w, oh = h;
     thrust::counting_iterator<uint32_t> it(0);
+    void *p_temp, *p_nsel;
+    SCK(A.get(F_NSEL, sizeof(int) * 4, &p_nsel));
+    KpArrays kp{};
+    void *p_th = nullptr, *p_cnt = nullptr;
     for (int o = 0; o < n_oct; ++o) {
         const int64_t npx = (int64_t)ow * oh;
-        void *p_lev, *p_tmp, *p_dog, *p_flag, *p_kx, *p_ky, *p_kr, *p_sel, *p_nsel;
+        void *p_lev, *p_tmp, *p_dog, *p_flag, *p_kx, *p_ky, *p_kr, *p_sel;
         SCK(A.get(F_LEV, sizeof(float) * NLEV * (size_t)npx, &p_lev));
         SCK(A.get(F_TMP, sizeof(float) * (size_t)npx, &p_tmp));
         SCK(A.get(F_DOG, sizeof(float) * NDOG * (size_t)npx, &p_dog));
@@ -692,7 +702,6 @@ int rcmvs_extract_sift(rcmvs_ctx* ctx, const uint8_t* img, int32_t w0, int32_t h
         SCK(A.get(F_KY, sizeof(double) * (size_t)nt, &p_ky));
         SCK(A.get(F_KRESP, sizeof(double) * (size_t)nt, &p_kr));
         SCK(A.get(F_SEL, sizeof(uint32_t) * (size_t)nt, &p_sel));
-        SCK(A.get(F_NSEL, sizeof(int) * 4, &p_nsel));
         hook.begin("sift_extrema");
         extrema_kernel<<<grid_of(nt), 256, 0, st>>>((const float*)p_dog, ow, oh, opts->contrast_thr,
                                                      (uint8_t*)p_flag, (double*)p_kx, (double*)p_ky, (double*)p_kr);
@@ -701,7 +710,6 @@ int rcmvs_extract_sift(rcmvs_ctx* ctx, const uint8_t* img, int32_t w0, int32_t h
         size_t tb = 0;
         SCK(cub::DeviceSelect::Flagged(nullptr, tb, it, (const uint8_t*)p_flag, (uint32_t*)p_sel, (int*)p_nsel,
                                        (int)nt, st));
-        void* p_temp;
         SCK(A.get(F_TEMP, tb, &p_temp));
         SCK(cub::DeviceSelect::Flagged(p_temp, tb, it, (const uint8_t*)p_flag, (uint32_t*)p_sel, (int*)p_nsel,
                                        (int)nt, st));
@@ -710,79 +718,41 @@ int rcmvs_extract_sift(rcmvs_ctx* ctx, const uint8_t* img, int32_t w0, int32_t h
         SCK(cudaStreamSynchronize(st));
         n_raw += (uint64_t)nk;
         const double scale = std::pow(2.0, o);
+        table.w[o] = ow;
+        table.h[o] = oh;
+        table.scale[o] = scale;
         if (nk > 0) {
-            void *p_x, *p_y, *p_r, *p_l, *p_gx, *p_gy, *p_th, *p_cnt, *p_off;
-            SCK(A.get(F_KPX, sizeof(double) * nk, &p_x));
-            SCK(A.get(F_KPY, sizeof(double) * nk, &p_y));
-            SCK(A.get(F_KPRESP, sizeof(double) * nk, &p_r));
-            SCK(A.get(F_KPLEV, sizeof(int32_t) * nk, &p_l));
-            KpArrays kp{(double*)p_x, (double*)p_y, (double*)p_r, (int32_t*)p_l};
+            // this octave's keypoints appended to the list of all octaves
+            const size_t keep = (size_t)nkp, need = (size_t)(nkp + nk);
+            void *p_x, *p_y, *p_r, *p_l, *p_o;
+            int rc2;
+            if ((rc2 = grow_copy(ctx, F_KPX, 8 * need, 8 * keep, &p_x)) ||
+                (rc2 = grow_copy(ctx, F_KPY, 8 * need, 8 * keep, &p_y)) ||
+                (rc2 = grow_copy(ctx, F_KPRESP, 8 * need, 8 * keep, &p_r)) ||
+                (rc2 = grow_copy(ctx, F_KPLEV, 4 * need, 4 * keep, &p_l)) ||
+                (rc2 = grow_copy(ctx, F_KPOCT, 4 * need, 4 * keep, &p_o)) ||
+                (rc2 = grow_copy(ctx, F_THETA, 8 * 4 * need, 8 * 4 * keep, &p_th)) ||
+                (rc2 = grow_copy(ctx, F_CNT, 4 * need, 4 * keep, &p_cnt)))
+                return rc2;
+            kp = KpArrays{(double*)p_x, (double*)p_y, (double*)p_r, (int32_t*)p_l, (int32_t*)p_o};
+            const KpArrays here{kp.x + nkp, kp.y + nkp, kp.resp + nkp, kp.level + nkp, kp.oct + nkp};
             gather_kp_kernel<<<grid_of(nk), 256, 0, st>>>((const uint32_t*)p_sel, nk, npx, (const double*)p_kx,
-                                                           (const double*)p_ky, (const double*)p_kr, kp);
+                                                           (const double*)p_ky, (const double*)p_kr, o, here);
             SCK(cudaGetLastError());
-            SCK(A.get(F_GX, sizeof(float) * NSPO * (size_t)npx, &p_gx));
-            SCK(A.get(F_GY, sizeof(float) * NSPO * (size_t)npx, &p_gy));
+            void *p_gx, *p_gy;
+            SCK(A.get(F_GRAD + 2 * o, sizeof(float) * NSPO * (size_t)npx, &p_gx));
+            SCK(A.get(F_GRAD + 2 * o + 1, sizeof(float) * NSPO * (size_t)npx, &p_gy));
+            table.gx[o] = (const float*)p_gx;
+            table.gy[o] = (const float*)p_gy;
             grad_kernel<<<grid_of(NSPO * npx), 256, 0, st>>>(lev, ow, oh, (float*)p_gx, (float*)p_gy);
             SCK(cudaGetLastError());
-            SCK(A.get(F_THETA, sizeof(double) * 4 * (size_t)nk, &p_th));
-            SCK(A.get(F_CNT, sizeof(int32_t) * (size_t)nk, &p_cnt));
-            SCK(A.get(F_OFF, sizeof(int32_t) * ((size_t)nk + 1), &p_off));
             hook.begin("sift_orient");
             orient_kernel<<<(nk + WARPS - 1) / WARPS, 32 * WARPS, 0, st>>>(
-                kp, nk, (const float*)p_gx, (const float*)p_gy, ow, oh, scale, w, h, (double*)p_th, (int32_t*)p_cnt);
+                here, nk, (const float*)p_gx, (const float*)p_gy, ow, oh, scale, w, h, (double*)p_th + 4 * nkp,
+                (int32_t*)p_cnt + nkp);
             SCK(cudaGetLastError());
             hook.end("sift_orient");
-            tb = 0;
-            SCK(cub::DeviceScan::ExclusiveSum(nullptr, tb, (const int32_t*)p_cnt, (int32_t*)p_off, nk, st));
-            SCK(A.get(F_TEMP, tb, &p_temp));
-            SCK(cub::DeviceScan::ExclusiveSum(p_temp, tb, (const int32_t*)p_cnt, (int32_t*)p_off, nk, st));
-            int last_off = 0, last_cnt = 0;
-            SCK(cudaMemcpyAsync(&last_off, (int32_t*)p_off + nk - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
-            SCK(cudaMemcpyAsync(&last_cnt, (int32_t*)p_cnt + nk - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
-            SCK(cudaStreamSynchronize(st));
-            const int np = last_off + last_cnt;
-            if (np > 0) {
-                void *p_pkp, *p_pth, *p_desc, *p_valid, *p_psel;
-                SCK(A.get(F_PKP, sizeof(int32_t) * np, &p_pkp));
-                SCK(A.get(F_PTH, sizeof(double) * np, &p_pth));
-                SCK(A.get(F_DESC, sizeof(float) * DESC_LEN * (size_t)np, &p_desc));
-                SCK(A.get(F_VALID, (size_t)np, &p_valid));
-                SCK(A.get(F_PSEL, sizeof(uint32_t) * np, &p_psel));
-                pairs_kernel<<<grid_of(nk), 256, 0, st>>>((const int32_t*)p_cnt, (const int32_t*)p_off, nk,
-                                                          (const double*)p_th, (int32_t*)p_pkp, (double*)p_pth);
-                SCK(cudaGetLastError());
-                hook.begin("sift_desc");
-                desc_kernel<<<(np + WARPS - 1) / WARPS, 32 * WARPS, 0, st>>>(
-                    kp, (const int32_t*)p_pkp, (const double*)p_pth, np, (const float*)p_gx, (const float*)p_gy, ow,
-                    oh, (float*)p_desc, (uint8_t*)p_valid);
-                SCK(cudaGetLastError());
-                hook.end("sift_desc");
-                tb = 0;
-                SCK(cub::DeviceSelect::Flagged(nullptr, tb, it, (const uint8_t*)p_valid, (uint32_t*)p_psel,
-                                               (int*)p_nsel + 1, np, st));
-                SCK(A.get(F_TEMP, tb, &p_temp));
-                SCK(cub::DeviceSelect::Flagged(p_temp, tb, it, (const uint8_t*)p_valid, (uint32_t*)p_psel,
-                                               (int*)p_nsel + 1, np, st));
-                int nv = 0;
-                SCK(cudaMemcpyAsync(&nv, (int*)p_nsel + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
-                SCK(cudaStreamSynchronize(st));
-                if (nv > 0) {
-                    void *p_oresp, *p_oxy, *p_odesc;
-                    const size_t keep = (size_t)n_cand, need = (size_t)(n_cand + nv);
-                    if ((rc = grow_copy(ctx, F_ORESP, sizeof(double) * need, sizeof(double) * keep, &p_oresp)))
-                        return rc;
-                    if ((rc = grow_copy(ctx, F_OXY, sizeof(double) * 2 * need, sizeof(double) * 2 * keep, &p_oxy)))
-                        return rc;
-                    if ((rc = grow_copy(ctx, F_ODESC, sizeof(float) * DESC_LEN * need,
-                                        sizeof(float) * DESC_LEN * keep, &p_odesc)))
-                        return rc;
-                    append_kernel<<<(nv + WARPS - 1) / WARPS, 32 * WARPS, 0, st>>>(
-                        (const uint32_t*)p_psel, nv, (const int32_t*)p_pkp, kp, scale, (const float*)p_desc, n_cand,
-                        (double*)p_oresp, (double*)p_oxy, (float*)p_odesc);
-                    SCK(cudaGetLastError());
-                    n_cand += nv;
-                }
-            }
+            nkp += nk;
         }
         // next octave's base: level NSPO downsampled 2x2 (sift.rs:488-492)
         const int nw = std::max(ow / 2, 1), nh = std::max(oh / 2, 1);
@@ -802,9 +772,80 @@ int rcmvs_extract_sift(rcmvs_ctx* ctx, const uint8_t* img, int32_t w0, int32_t h
     if (d_err) SCK(cudaMemcpyAsync(&bad, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
     SCK(cudaStreamSynchronize(st));
     if (bad) return sfail(ctx, RCMVS_E_CUDA, "sift: resize tap table overflow");
+    if (nkp > INT32_MAX / 4) return sfail(ctx, RCMVS_E_LIMIT, "sift: too many keypoints");
 
-    // sift.rs:543-544: stable sort by response, descending; the first max_features
-    const int64_t n_out = std::min<int64_t>(n_cand, (int64_t)opts->max_features);
+    // (keypoint, peak) pairs in the reference's output order (octave, keypoint,
+    // peak), each with its keypoint's response
+    int64_t np = 0;
+    void *p_pkp = nullptr, *p_pth = nullptr, *p_presp = nullptr, *p_pidx = nullptr, *p_sresp = nullptr,
+         *p_sidx = nullptr, *p_desc = nullptr, *p_valid = nullptr, *p_osel = nullptr;
+    if (nkp > 0) {
+        void* p_off;
+        SCK(A.get(F_OFF, sizeof(int32_t) * (size_t)nkp, &p_off));
+        size_t tb = 0;
+        SCK(cub::DeviceScan::ExclusiveSum(nullptr, tb, (const int32_t*)p_cnt, (int32_t*)p_off, (int)nkp, st));
+        SCK(A.get(F_TEMP, tb, &p_temp));
+        SCK(cub::DeviceScan::ExclusiveSum(p_temp, tb, (const int32_t*)p_cnt, (int32_t*)p_off, (int)nkp, st));
+        int last_off = 0, last_cnt = 0;
+        SCK(cudaMemcpyAsync(&last_off, (int32_t*)p_off + nkp - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+        SCK(cudaMemcpyAsync(&last_cnt, (int32_t*)p_cnt + nkp - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+        SCK(cudaStreamSynchronize(st));
+        np = (int64_t)last_off + last_cnt;
+        if (np > 0) {
+            SCK(A.get(F_PKP, sizeof(int32_t) * np, &p_pkp));
+            SCK(A.get(F_PTH, sizeof(double) * np, &p_pth));
+            SCK(A.get(F_PRESP, sizeof(double) * np, &p_presp));
+            SCK(A.get(F_PIDX, sizeof(uint32_t) * np, &p_pidx));
+            SCK(A.get(F_SRESP, sizeof(double) * np, &p_sresp));
+            SCK(A.get(F_SIDX, sizeof(uint32_t) * np, &p_sidx));
+            SCK(A.get(F_DESC, sizeof(float) * DESC_LEN * (size_t)np, &p_desc));
+            SCK(A.get(F_VALID, (size_t)np, &p_valid));
+            SCK(A.get(F_OSEL, sizeof(uint32_t) * np, &p_osel));
+            pairs_kernel<<<grid_of(nkp), 256, 0, st>>>((const int32_t*)p_cnt, (const int32_t*)p_off, (int)nkp,
+                                                       (const double*)p_th, kp.resp, (int32_t*)p_pkp,
+                                                       (double*)p_pth, (double*)p_presp, (uint32_t*)p_pidx);
+            SCK(cudaGetLastError());
+            // sift.rs:543: the reference sorts its descriptors by response with a
+            // stable sort; the same order over the pairs, before any descriptor
+            tb = 0;
+            SCK(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, (const double*)p_presp, (double*)p_sresp,
+                                                          (const uint32_t*)p_pidx, (uint32_t*)p_sidx, (int)np, 0, 64,
+                                                          st));
+            SCK(A.get(F_TEMP, tb, &p_temp));
+            SCK(cub::DeviceRadixSort::SortPairsDescending(p_temp, tb, (const double*)p_presp, (double*)p_sresp,
+                                                          (const uint32_t*)p_pidx, (uint32_t*)p_sidx, (int)np, 0, 64,
+                                                          st));
+            SCK(cudaGetLastError());
+        }
+    }
+    // Descriptors in sorted order until max_features valid ones (a pair whose
+    // descriptor normalises to nothing is dropped, as the reference drops it
+    // before its sort); descriptors of pairs beyond that cannot be output.
+    int64_t done = 0, n_valid = 0;
+    const int64_t cap = (int64_t)opts->max_features;
+    while (n_valid < cap && done < np) {
+        const int64_t chunk = std::min<int64_t>(np - done, std::max<int64_t>(cap - n_valid, 32));
+        hook.begin("sift_desc");
+        desc_kernel<<<(unsigned)((chunk + WARPS - 1) / WARPS), 32 * WARPS, 0, st>>>(
+            kp, (const uint32_t*)p_sidx, done, (int)chunk, (const int32_t*)p_pkp, (const double*)p_pth, table,
+            (float*)p_desc, (uint8_t*)p_valid);
+        SCK(cudaGetLastError());
+        hook.end("sift_desc");
+        done += chunk;
+        size_t tb = 0;
+        SCK(cub::DeviceSelect::Flagged(nullptr, tb, it, (const uint8_t*)p_valid, (uint32_t*)p_osel,
+                                       (int*)p_nsel + 1, (int)done, st));
+        SCK(A.get(F_TEMP, tb, &p_temp));
+        SCK(cub::DeviceSelect::Flagged(p_temp, tb, it, (const uint8_t*)p_valid, (uint32_t*)p_osel,
+                                       (int*)p_nsel + 1, (int)done, st));
+        int nv = 0;
+        SCK(cudaMemcpyAsync(&nv, (int*)p_nsel + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+        SCK(cudaStreamSynchronize(st));
+        n_valid = nv;
+    }
+
+    // sift.rs:543-544: the first max_features
+    const int64_t n_out = std::min<int64_t>(n_valid, cap);
     out->width = w;
     out->height = h;
     out->n_raw = n_raw;
@@ -817,33 +858,13 @@ int rcmvs_extract_sift(rcmvs_ctx* ctx, const uint8_t* img, int32_t w0, int32_t h
         return sfail(ctx, RCMVS_E_NOMEM, "sift: host allocation failed");
     }
     if (n_out == 0) return RCMVS_OK;
-    if (n_cand > INT32_MAX) return sfail(ctx, RCMVS_E_LIMIT, "sift: too many features");
-    void *p_oresp, *p_oxy, *p_odesc, *p_sresp, *p_idx, *p_sidx, *p_pts, *p_fdesc, *p_col, *p_temp;
-    SCK(A.get(F_ORESP, sizeof(double) * n_cand, &p_oresp));
-    SCK(A.get(F_OXY, sizeof(double) * 2 * n_cand, &p_oxy));
-    SCK(A.get(F_ODESC, sizeof(float) * DESC_LEN * n_cand, &p_odesc));
-    SCK(A.get(F_SRESP, sizeof(double) * n_cand, &p_sresp));
-    SCK(A.get(F_IDX, sizeof(uint32_t) * n_cand, &p_idx));
-    SCK(A.get(F_SIDX, sizeof(uint32_t) * n_cand, &p_sidx));
+    void *p_pts, *p_fdesc, *p_col;
     SCK(A.get(F_PTS, sizeof(double) * 2 * n_out, &p_pts));
     SCK(A.get(F_FDESC, sizeof(float) * DESC_LEN * n_out, &p_fdesc));
     SCK(A.get(F_COL, 3 * (size_t)n_out, &p_col));
-    {
-        // indices 0..n_cand-1 as the sort's values; a stable descending sort
-        size_t tb = 0;
-        SCK(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, (const double*)p_oresp, (double*)p_sresp,
-                                                      (const uint32_t*)p_idx, (uint32_t*)p_sidx, (int)n_cand, 0, 64,
-                                                      st));
-        SCK(A.get(F_TEMP, tb, &p_temp));
-        iota_kernel<<<grid_of(n_cand), 256, 0, st>>>((uint32_t*)p_idx, n_cand);
-        SCK(cudaGetLastError());
-        SCK(cub::DeviceRadixSort::SortPairsDescending(p_temp, tb, (const double*)p_oresp, (double*)p_sresp,
-                                                      (const uint32_t*)p_idx, (uint32_t*)p_sidx, (int)n_cand, 0, 64,
-                                                      st));
-    }
     final_kernel<<<(int)((n_out + WARPS - 1) / WARPS), 32 * WARPS, 0, st>>>(
-        (const uint32_t*)p_sidx, (int)n_out, (const double*)p_oxy, (const float*)p_odesc, (const uint8_t*)p_rgb, w, h,
-        (double*)p_pts, (float*)p_fdesc, (uint8_t*)p_col);
+        (const uint32_t*)p_osel, (int)n_out, (const uint32_t*)p_sidx, (const int32_t*)p_pkp, kp, table,
+        (const float*)p_desc, (const uint8_t*)p_rgb, w, h, (double*)p_pts, (float*)p_fdesc, (uint8_t*)p_col);
     SCK(cudaGetLastError());
     SCK(cudaMemcpyAsync(out->pts, p_pts, sizeof(double) * 2 * n_out, cudaMemcpyDeviceToHost, st));
     SCK(cudaMemcpyAsync(out->desc, p_fdesc, sizeof(float) * DESC_LEN * n_out, cudaMemcpyDeviceToHost, st));

@@ -114,16 +114,18 @@ def ctx():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("k,channels,max_dim", [(0, 3, 1600), (1, 1, 1600), (2, 3, 1600), (2, 1, 700),
-                                                (0, 4, 200)])
-def test_gpu_sift_matches_oracle(ctx, k, channels, max_dim):
+@pytest.mark.parametrize("k,channels,max_dim,cap", [(0, 3, 1600, 2048), (1, 1, 1600, 2048), (2, 3, 1600, 2048),
+                                                    (2, 1, 700, 2048), (0, 4, 200, 2048), (2, 3, 1600, 100000),
+                                                    (1, 3, 1600, 7)])
+def test_gpu_sift_matches_oracle(ctx, k, channels, max_dim, cap):
     v = views()[k]
     img = np.ascontiguousarray(v.gray if channels == 1 else v.rgb)
     if channels == 4:
         img = np.concatenate([img, np.full(img.shape[:2] + (1,), 77, np.uint8)], axis=2)
-    opts = sift.SiftOptions(max_dim=max_dim)
+    opts = sift.SiftOptions(max_dim=max_dim, max_features=cap)
     f = sift.extract_sift(img, "v", opts, ctx)
-    (pts, desc, col, nraw), (w, h) = oracle_sift(img, max_dim)
+    (pts, desc, col, nraw), (w, h) = oracle_sift(img, max_dim, max_features=cap)
+    assert np.array_equal(f.colors, col) or len(f.pts) != len(pts)
     assert (f.width, f.height) == (w, h)
     assert f.n_raw == nraw, "scale-space extrema differ"
     assert abs(len(f.pts) - len(pts)) <= max(1, len(pts) // 100)
