@@ -12,8 +12,9 @@
 //               contrast and curvature tests (sift.rs:176-262); flags are
 //               compacted stably, so keypoints keep the reference's
 //               (level, y, x) order
-//   orientation one warp per keypoint: lanes evaluate 32 window samples at a
-//               time (atan2, exp in f64), each lane owns histogram bins and
+//   orientation one warp per keypoint (in response order, see output):
+//               lanes evaluate 32 window samples at a time (atan2, exp in
+//               f64), each lane owns histogram bins and
 //               adds the samples that fall in them in window order, so every
 //               bin is the reference's sequential f64 sum; lane 0 smooths and
 //               picks up to four peaks (sift.rs:274-334)
@@ -24,12 +25,14 @@
 //               sample from the sample's (row, column, orientation) base by
 //               arithmetic; L2 -> clip 0.2 -> L2 in f32 (sift.rs:340-431)
 //   output      the reference sorts its descriptors by response (stable) and
-//               keeps the first max_features (sift.rs:543-544).  Responses are
-//               known before descriptors, so the (keypoint, peak) pairs of all
-//               octaves are radix-sorted first (stable, descending) and
-//               descriptors are computed in that order until max_features
-//               valid ones exist: the same output without the descriptors the
-//               cap would discard (about 2k of 30k at 1600x1200)
+//               keeps the first max_features (sift.rs:543-544).  A descriptor's
+//               response is its keypoint's, so that order is the keypoints of
+//               all octaves sorted stably by response (CUB radix sort) with
+//               each keypoint's peaks in turn; orientations, pairs and
+//               descriptors are produced in that order until max_features
+//               valid ones exist -- the same output without the orientations
+//               and descriptors the cap would discard (about 2k of 27k
+//               keypoints at 1600x1200)
 //
 // The library builds with --fmad=false: every f32/f64 product and sum rounds
 // as written, so the pyramid, the DoGs and the extrema with their fitted
@@ -258,28 +261,34 @@ __device__ __forceinline__ double rem_euclid(double a, double b) {
     return r < 0.0 ? r + fabs(b) : r;
 }
 
-// sift.rs:274-334.  One warp per keypoint; theta[4k..], cnt[k] (0 when the
-// keypoint is outside the 8-pixel margin of the image, sift.rs:519-521).
-__global__ void __launch_bounds__(32 * WARPS) orient_kernel(KpArrays kp, int n, const float* __restrict__ gx_all,
-                                                           const float* __restrict__ gy_all, int w, int h,
-                                                           double scale, int img_w, int img_h,
-                                                           double* __restrict__ theta, int32_t* __restrict__ cnt) {
+// sift.rs:274-334.  One warp per keypoint, for the keypoints at sorted
+// positions base .. base + n - 1 (skp[pos] = keypoint); theta[4 pos ..] and
+// cnt[pos] (0 when the keypoint is outside the 8-pixel margin of the image,
+// sift.rs:519-521).
+__global__ void __launch_bounds__(32 * WARPS) orient_kernel(KpArrays kp, const uint32_t* __restrict__ skp,
+                                                           int64_t base, int n, const __grid_constant__ OctTable oct,
+                                                           int img_w, int img_h, double* __restrict__ theta,
+                                                           int32_t* __restrict__ cnt) {
     __shared__ int sbin[WARPS][32];
     __shared__ double sval[WARPS][32];
     __shared__ double shist[WARPS][36];
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int k = blockIdx.x * WARPS + wid;
-    if (k >= n) return;
-    const double kx = kp.x[k], ky = kp.y[k];
-    const int level = kp.level[k];
+    const int i = blockIdx.x * WARPS + wid;
+    if (i >= n) return;
+    const int64_t k = base + i;  // output position
+    const uint32_t kk = skp[k];
+    const double kx = kp.x[kk], ky = kp.y[kk];
+    const int level = kp.level[kk], o = kp.oct[kk];
+    const double scale = oct.scale[o];
     const double x0 = kx * scale, y0 = ky * scale;
     if (x0 < 8.0 || y0 < 8.0 || x0 >= (double)img_w - 8.0 || y0 >= (double)img_h - 8.0) {
         if (lane == 0) cnt[k] = 0;
         return;
     }
+    const int w = oct.w[o], h = oct.h[o];
     const int64_t npx = (int64_t)w * h;
-    const float* gx = gx_all + (level - 1) * npx;
-    const float* gy = gy_all + (level - 1) * npx;
+    const float* gx = oct.gx[o] + (level - 1) * npx;
+    const float* gy = oct.gy[o] + (level - 1) * npx;
     const double sigma = 1.5 * level_sigma(level);
     const int radius = (int)fmax(ceil(3.0 * sigma), 1.0);
     const double s2 = 2.0 * sigma * sigma;
@@ -352,18 +361,23 @@ __global__ void __launch_bounds__(32 * WARPS) orient_kernel(KpArrays kp, int n, 
     }
 }
 
-// (keypoint, peak) pairs in keypoint order, peaks in order
-__global__ void pairs_kernel(const int32_t* __restrict__ cnt, const int32_t* __restrict__ off, int n,
-                             const double* __restrict__ theta, const double* __restrict__ resp,
-                             int32_t* __restrict__ pair_kp, double* __restrict__ pair_theta,
-                             double* __restrict__ pair_resp, uint32_t* __restrict__ pair_idx) {
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
-        for (int p = 0; p < cnt[k]; ++p) {
-            pair_kp[off[k] + p] = k;
-            pair_theta[off[k] + p] = theta[4 * (int64_t)k + p];
-            pair_resp[off[k] + p] = resp[k];
-            pair_idx[off[k] + p] = (uint32_t)(off[k] + p);
+// (keypoint, peak) pairs of the keypoints at sorted positions base ..
+// base + n - 1, peaks in order, appended at pair index at + off[i] + p.
+__global__ void pairs_kernel(const uint32_t* __restrict__ skp, int64_t base, int n, const int32_t* __restrict__ cnt,
+                             const int32_t* __restrict__ off, const double* __restrict__ theta, int64_t at,
+                             int32_t* __restrict__ pair_kp, double* __restrict__ pair_theta) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int64_t pos = base + i;
+        for (int p = 0; p < cnt[pos]; ++p) {
+            pair_kp[at + off[i] + p] = (int32_t)skp[pos];
+            pair_theta[at + off[i] + p] = theta[4 * pos + p];
         }
+    }
+}
+
+__global__ void iota_kernel(uint32_t* __restrict__ out, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = (uint32_t)i;
 }
 
 // sift.rs:151-166
@@ -378,11 +392,10 @@ __device__ __forceinline__ float bilinear(const float* __restrict__ img, int w, 
     return a * (1.0f - fy) + b * fy;
 }
 
-// sift.rs:340-431.  One warp per (keypoint, peak) pair: the pairs at sorted
-// positions base .. base + n_pairs - 1 (order[pos] = pair); descriptor and
-// validity stored at the sorted position.
-__global__ void __launch_bounds__(32 * WARPS) desc_kernel(KpArrays kp, const uint32_t* __restrict__ order,
-                                                         int64_t base, int n_pairs,
+// sift.rs:340-431.  One warp per (keypoint, peak) pair, for the pairs
+// base .. base + n_pairs - 1 (in output order); descriptor and validity
+// stored at the pair's index.
+__global__ void __launch_bounds__(32 * WARPS) desc_kernel(KpArrays kp, int64_t base, int n_pairs,
                                                          const int32_t* __restrict__ pair_kp,
                                                          const double* __restrict__ pair_theta,
                                                          const __grid_constant__ OctTable oct,
@@ -395,9 +408,8 @@ __global__ void __launch_bounds__(32 * WARPS) desc_kernel(KpArrays kp, const uin
     const int i = blockIdx.x * WARPS + wid;
     if (i >= n_pairs) return;
     const int64_t pos = base + i;
-    const uint32_t pr = order[pos];
-    const int k = pair_kp[pr];
-    const double x = kp.x[k], y = kp.y[k], th = pair_theta[pr];
+    const int k = pair_kp[pos];
+    const double x = kp.x[k], y = kp.y[k], th = pair_theta[pos];
     const int level = kp.level[k], o = kp.oct[k];
     const int w = oct.w[o], h = oct.h[o];
     const int64_t npx = (int64_t)w * h;
@@ -502,15 +514,15 @@ __global__ void __launch_bounds__(32 * WARPS) desc_kernel(KpArrays kp, const uin
 
 // sift.rs:543-554: output i is the sorted position sel[i] (the i-th valid
 // descriptor in response order); clamped position, descriptor, colour.
-__global__ void final_kernel(const uint32_t* __restrict__ sel, int n, const uint32_t* __restrict__ order,
-                             const int32_t* __restrict__ pair_kp, KpArrays kp, const __grid_constant__ OctTable oct,
+__global__ void final_kernel(const uint32_t* __restrict__ sel, int n, const int32_t* __restrict__ pair_kp, KpArrays kp,
+                             const __grid_constant__ OctTable oct,
                              const float* __restrict__ desc, const uint8_t* __restrict__ rgb, int w, int h,
                              double* __restrict__ pts, float* __restrict__ odesc, uint8_t* __restrict__ col) {
     const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (wid >= n) return;
     const uint32_t pos = sel[wid];
     if (lane == 0) {
-        const int k = pair_kp[order[pos]];
+        const int k = pair_kp[pos];
         const double scale = oct.scale[kp.oct[k]];
         const double x = fmin(fmax(kp.x[k] * scale, 0.0), (double)(w - 1));
         const double y = fmin(fmax(kp.y[k] * scale, 0.0), (double)(h - 1));
@@ -563,7 +575,7 @@ int sfail(rcmvs_ctx* ctx, int code, const std::string& msg) {
 // Context arena slots 80-159.
 enum {
     F_IN = 80, F_GRAY, F_RGB, F_BASE, F_LEV, F_TMP, F_DOG, F_FLAG, F_KX, F_KY, F_KRESP, F_SEL, F_NSEL, F_TEMP,
-    F_KPX, F_KPY, F_KPRESP, F_KPLEV, F_KPOCT, F_THETA, F_CNT, F_OFF, F_PKP, F_PTH, F_PRESP, F_PIDX, F_SRESP, F_SIDX,
+    F_KPX, F_KPY, F_KPRESP, F_KPLEV, F_KPOCT, F_THETA, F_CNT, F_OFF, F_PKP, F_PTH, F_PIDX, F_SRESP, F_SIDX,
     F_DESC, F_VALID, F_OSEL, F_PTS, F_FDESC, F_COL, F_NEXT,
     F_GRAD = 130  // 130 + 2 * octave: gx, + 1: gy (octaves 0..7)
 };
@@ -669,7 +681,6 @@ int rcmvs_extract_sift(rcmvs_ctx* ctx, const uint8_t* img, int32_t w0, int32_t h
     void *p_temp, *p_nsel;
     SCK(A.get(F_NSEL, sizeof(int) * 4, &p_nsel));
     KpArrays kp{};
-    void *p_th = nullptr, *p_cnt = nullptr;
     for (int o = 0; o < n_oct; ++o) {
         const int64_t npx = (int64_t)ow * oh;
         void *p_lev, *p_tmp, *p_dog, *p_flag, *p_kx, *p_ky, *p_kr, *p_sel;
@@ -730,9 +741,7 @@ int rcmvs_extract_sift(rcmvs_ctx* ctx, const uint8_t* img, int32_t w0, int32_t h
                 (rc2 = grow_copy(ctx, F_KPY, 8 * need, 8 * keep, &p_y)) ||
                 (rc2 = grow_copy(ctx, F_KPRESP, 8 * need, 8 * keep, &p_r)) ||
                 (rc2 = grow_copy(ctx, F_KPLEV, 4 * need, 4 * keep, &p_l)) ||
-                (rc2 = grow_copy(ctx, F_KPOCT, 4 * need, 4 * keep, &p_o)) ||
-                (rc2 = grow_copy(ctx, F_THETA, 8 * 4 * need, 8 * 4 * keep, &p_th)) ||
-                (rc2 = grow_copy(ctx, F_CNT, 4 * need, 4 * keep, &p_cnt)))
+                (rc2 = grow_copy(ctx, F_KPOCT, 4 * need, 4 * keep, &p_o)))
                 return rc2;
             kp = KpArrays{(double*)p_x, (double*)p_y, (double*)p_r, (int32_t*)p_l, (int32_t*)p_o};
             const KpArrays here{kp.x + nkp, kp.y + nkp, kp.resp + nkp, kp.level + nkp, kp.oct + nkp};
@@ -746,12 +755,6 @@ int rcmvs_extract_sift(rcmvs_ctx* ctx, const uint8_t* img, int32_t w0, int32_t h
             table.gy[o] = (const float*)p_gy;
             grad_kernel<<<grid_of(NSPO * npx), 256, 0, st>>>(lev, ow, oh, (float*)p_gx, (float*)p_gy);
             SCK(cudaGetLastError());
-            hook.begin("sift_orient");
-            orient_kernel<<<(nk + WARPS - 1) / WARPS, 32 * WARPS, 0, st>>>(
-                here, nk, (const float*)p_gx, (const float*)p_gy, ow, oh, scale, w, h, (double*)p_th + 4 * nkp,
-                (int32_t*)p_cnt + nkp);
-            SCK(cudaGetLastError());
-            hook.end("sift_orient");
             nkp += nk;
         }
         // next octave's base: level NSPO downsampled 2x2 (sift.rs:488-492)
@@ -774,61 +777,79 @@ int rcmvs_extract_sift(rcmvs_ctx* ctx, const uint8_t* img, int32_t w0, int32_t h
     if (bad) return sfail(ctx, RCMVS_E_CUDA, "sift: resize tap table overflow");
     if (nkp > INT32_MAX / 4) return sfail(ctx, RCMVS_E_LIMIT, "sift: too many keypoints");
 
-    // (keypoint, peak) pairs in the reference's output order (octave, keypoint,
-    // peak), each with its keypoint's response
-    int64_t np = 0;
-    void *p_pkp = nullptr, *p_pth = nullptr, *p_presp = nullptr, *p_pidx = nullptr, *p_sresp = nullptr,
-         *p_sidx = nullptr, *p_desc = nullptr, *p_valid = nullptr, *p_osel = nullptr;
-    if (nkp > 0) {
-        void* p_off;
-        SCK(A.get(F_OFF, sizeof(int32_t) * (size_t)nkp, &p_off));
-        size_t tb = 0;
-        SCK(cub::DeviceScan::ExclusiveSum(nullptr, tb, (const int32_t*)p_cnt, (int32_t*)p_off, (int)nkp, st));
-        SCK(A.get(F_TEMP, tb, &p_temp));
-        SCK(cub::DeviceScan::ExclusiveSum(p_temp, tb, (const int32_t*)p_cnt, (int32_t*)p_off, (int)nkp, st));
-        int last_off = 0, last_cnt = 0;
-        SCK(cudaMemcpyAsync(&last_off, (int32_t*)p_off + nkp - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
-        SCK(cudaMemcpyAsync(&last_cnt, (int32_t*)p_cnt + nkp - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
-        SCK(cudaStreamSynchronize(st));
-        np = (int64_t)last_off + last_cnt;
-        if (np > 0) {
-            SCK(A.get(F_PKP, sizeof(int32_t) * np, &p_pkp));
-            SCK(A.get(F_PTH, sizeof(double) * np, &p_pth));
-            SCK(A.get(F_PRESP, sizeof(double) * np, &p_presp));
-            SCK(A.get(F_PIDX, sizeof(uint32_t) * np, &p_pidx));
-            SCK(A.get(F_SRESP, sizeof(double) * np, &p_sresp));
-            SCK(A.get(F_SIDX, sizeof(uint32_t) * np, &p_sidx));
-            SCK(A.get(F_DESC, sizeof(float) * DESC_LEN * (size_t)np, &p_desc));
-            SCK(A.get(F_VALID, (size_t)np, &p_valid));
-            SCK(A.get(F_OSEL, sizeof(uint32_t) * np, &p_osel));
-            pairs_kernel<<<grid_of(nkp), 256, 0, st>>>((const int32_t*)p_cnt, (const int32_t*)p_off, (int)nkp,
-                                                       (const double*)p_th, kp.resp, (int32_t*)p_pkp,
-                                                       (double*)p_pth, (double*)p_presp, (uint32_t*)p_pidx);
-            SCK(cudaGetLastError());
-            // sift.rs:543: the reference sorts its descriptors by response with a
-            // stable sort; the same order over the pairs, before any descriptor
-            tb = 0;
-            SCK(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, (const double*)p_presp, (double*)p_sresp,
-                                                          (const uint32_t*)p_pidx, (uint32_t*)p_sidx, (int)np, 0, 64,
-                                                          st));
-            SCK(A.get(F_TEMP, tb, &p_temp));
-            SCK(cub::DeviceRadixSort::SortPairsDescending(p_temp, tb, (const double*)p_presp, (double*)p_sresp,
-                                                          (const uint32_t*)p_pidx, (uint32_t*)p_sidx, (int)np, 0, 64,
-                                                          st));
-            SCK(cudaGetLastError());
-        }
-    }
-    // Descriptors in sorted order until max_features valid ones (a pair whose
-    // descriptor normalises to nothing is dropped, as the reference drops it
-    // before its sort); descriptors of pairs beyond that cannot be output.
-    int64_t done = 0, n_valid = 0;
+    // The reference computes every (keypoint, peak) descriptor in (octave,
+    // keypoint, peak) order, sorts them by their keypoint's response with a
+    // stable sort and keeps the first max_features (sift.rs:497-544).  The
+    // same order is the keypoints sorted stably by response with each one's
+    // peaks in turn, so keypoints are sorted first and orientations, pairs
+    // and descriptors are produced in that order until max_features valid
+    // descriptors exist (a descriptor that normalises to nothing is dropped,
+    // as in the reference).
     const int64_t cap = (int64_t)opts->max_features;
-    while (n_valid < cap && done < np) {
+    int64_t kdone = 0, np = 0, done = 0, n_valid = 0;
+    void *p_kidx = nullptr, *p_sresp = nullptr, *p_skp = nullptr, *p_th = nullptr, *p_cnt = nullptr,
+         *p_off = nullptr, *p_pkp = nullptr, *p_pth = nullptr, *p_desc = nullptr, *p_valid = nullptr,
+         *p_osel = nullptr;
+    if (nkp > 0 && cap > 0) {
+        SCK(A.get(F_PIDX, sizeof(uint32_t) * (size_t)nkp, &p_kidx));
+        SCK(A.get(F_SRESP, sizeof(double) * (size_t)nkp, &p_sresp));
+        SCK(A.get(F_SIDX, sizeof(uint32_t) * (size_t)nkp, &p_skp));
+        SCK(A.get(F_THETA, sizeof(double) * 4 * (size_t)nkp, &p_th));
+        SCK(A.get(F_CNT, sizeof(int32_t) * (size_t)nkp, &p_cnt));
+        SCK(A.get(F_OFF, sizeof(int32_t) * (size_t)nkp, &p_off));
+        SCK(A.get(F_PKP, sizeof(int32_t) * 4 * (size_t)nkp, &p_pkp));
+        SCK(A.get(F_PTH, sizeof(double) * 4 * (size_t)nkp, &p_pth));
+        SCK(A.get(F_VALID, 4 * (size_t)nkp, &p_valid));
+        SCK(A.get(F_OSEL, sizeof(uint32_t) * 4 * (size_t)nkp, &p_osel));
+        iota_kernel<<<grid_of(nkp), 256, 0, st>>>((uint32_t*)p_kidx, nkp);
+        SCK(cudaGetLastError());
+        size_t tb = 0;
+        SCK(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, (const double*)kp.resp, (double*)p_sresp,
+                                                      (const uint32_t*)p_kidx, (uint32_t*)p_skp, (int)nkp, 0, 64,
+                                                      st));
+        SCK(A.get(F_TEMP, tb, &p_temp));
+        SCK(cub::DeviceRadixSort::SortPairsDescending(p_temp, tb, (const double*)kp.resp, (double*)p_sresp,
+                                                      (const uint32_t*)p_kidx, (uint32_t*)p_skp, (int)nkp, 0, 64,
+                                                      st));
+    }
+    while (n_valid < cap && (done < np || kdone < nkp)) {
+        if (done == np) {
+            // orientations of the next keypoints in response order, and their pairs
+            const int64_t ck = std::min<int64_t>(nkp - kdone, std::max<int64_t>(cap - n_valid, 64));
+            hook.begin("sift_orient");
+            orient_kernel<<<(unsigned)((ck + WARPS - 1) / WARPS), 32 * WARPS, 0, st>>>(
+                kp, (const uint32_t*)p_skp, kdone, (int)ck, table, w, h, (double*)p_th, (int32_t*)p_cnt);
+            SCK(cudaGetLastError());
+            hook.end("sift_orient");
+            size_t tb = 0;
+            SCK(cub::DeviceScan::ExclusiveSum(nullptr, tb, (const int32_t*)p_cnt + kdone, (int32_t*)p_off, (int)ck,
+                                              st));
+            SCK(A.get(F_TEMP, tb, &p_temp));
+            SCK(cub::DeviceScan::ExclusiveSum(p_temp, tb, (const int32_t*)p_cnt + kdone, (int32_t*)p_off, (int)ck,
+                                              st));
+            pairs_kernel<<<grid_of(ck), 256, 0, st>>>((const uint32_t*)p_skp, kdone, (int)ck, (const int32_t*)p_cnt,
+                                                      (const int32_t*)p_off, (const double*)p_th, np,
+                                                      (int32_t*)p_pkp, (double*)p_pth);
+            SCK(cudaGetLastError());
+            int last_off = 0, last_cnt = 0;
+            SCK(cudaMemcpyAsync(&last_off, (int32_t*)p_off + ck - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+            SCK(cudaMemcpyAsync(&last_cnt, (int32_t*)p_cnt + kdone + ck - 1, sizeof(int), cudaMemcpyDeviceToHost,
+                                st));
+            SCK(cudaStreamSynchronize(st));
+            kdone += ck;
+            np += (int64_t)last_off + last_cnt;
+            continue;
+        }
         const int64_t chunk = std::min<int64_t>(np - done, std::max<int64_t>(cap - n_valid, 32));
+        void* p_d;
+        if ((rc = grow_copy(ctx, F_DESC, sizeof(float) * DESC_LEN * (size_t)(done + chunk),
+                            sizeof(float) * DESC_LEN * (size_t)done, &p_d)))
+            return rc;
+        p_desc = p_d;
         hook.begin("sift_desc");
         desc_kernel<<<(unsigned)((chunk + WARPS - 1) / WARPS), 32 * WARPS, 0, st>>>(
-            kp, (const uint32_t*)p_sidx, done, (int)chunk, (const int32_t*)p_pkp, (const double*)p_pth, table,
-            (float*)p_desc, (uint8_t*)p_valid);
+            kp, done, (int)chunk, (const int32_t*)p_pkp, (const double*)p_pth, table, (float*)p_desc,
+            (uint8_t*)p_valid);
         SCK(cudaGetLastError());
         hook.end("sift_desc");
         done += chunk;
@@ -863,7 +884,7 @@ int rcmvs_extract_sift(rcmvs_ctx* ctx, const uint8_t* img, int32_t w0, int32_t h
     SCK(A.get(F_FDESC, sizeof(float) * DESC_LEN * n_out, &p_fdesc));
     SCK(A.get(F_COL, 3 * (size_t)n_out, &p_col));
     final_kernel<<<(int)((n_out + WARPS - 1) / WARPS), 32 * WARPS, 0, st>>>(
-        (const uint32_t*)p_osel, (int)n_out, (const uint32_t*)p_sidx, (const int32_t*)p_pkp, kp, table,
+        (const uint32_t*)p_osel, (int)n_out, (const int32_t*)p_pkp, kp, table,
         (const float*)p_desc, (const uint8_t*)p_rgb, w, h, (double*)p_pts, (float*)p_fdesc, (uint8_t*)p_col);
     SCK(cudaGetLastError());
     SCK(cudaMemcpyAsync(out->pts, p_pts, sizeof(double) * 2 * n_out, cudaMemcpyDeviceToHost, st));
