@@ -52,6 +52,8 @@ using namespace rcmvs;
 
 namespace {
 
+void free_spare(rcmvs_ctx* ctx);
+
 enum { S_JOBS = kSlotJobs, S_JOBSTART = kSlotJobStart, S_CGRAY = 2, S_CCEN = 3, S_FIELD_PL = 4, S_FIELD_H = 5,
        S_FIELD_C = 6, S_FIELD_HS = 7, S_F2I = 8 };
 
@@ -166,6 +168,8 @@ void rcmvs_ctx_destroy(rcmvs_ctx* ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     ctx->arena.release();
+    free_spare(ctx);
+    for (rcmvs_scene* sc : ctx->live) sc->ctx = nullptr;
     ctx->clear_spans();
     if (ctx->d_work) cudaFree(ctx->d_work);
     cudaStreamDestroy(ctx->stream);
@@ -193,21 +197,74 @@ void rcmvs_points_free(rcmvs_points* p) {
 }
 
 // ================================================================ scene
+}  // extern "C"
+
+namespace {
+
+void** scene_big(rcmvs_scene* sc, int i) {
+    void** m[13] = {(void**)&sc->gray,    (void**)&sc->rgb,     (void**)&sc->census, (void**)&sc->rays,
+                    (void**)&sc->plane_a, (void**)&sc->plane_b, (void**)&sc->pcost_a, (void**)&sc->pcost_b,
+                    (void**)&sc->pd_a,    (void**)&sc->pd_b,    (void**)&sc->depth,   (void**)&sc->cost,
+                    (void**)&sc->normal};
+    return m[i];
+}
+
+void** scene_small(rcmvs_scene* sc, int i) {
+    void** m[3] = {(void**)&sc->d_views, (void**)&sc->d_tile_start, (void**)&sc->d_cams};
+    return m[i];
+}
+
+void free_spare(rcmvs_ctx* ctx) {
+    rcmvs_ctx::SpareScene& s = ctx->spare;
+    for (void*& p : s.big) {
+        if (p) cudaFree(p);
+        p = nullptr;
+    }
+    for (void*& p : s.small) {
+        if (p) cudaFree(p);
+        p = nullptr;
+    }
+    s.arena.release();
+    s.valid = false;
+    s.cap_px = 0;
+    s.cap_views = 0;
+}
+
+}  // namespace
+
+extern "C" {
+
 void rcmvs_scene_destroy(rcmvs_scene* sc) {
     if (!sc) return;
     if (sc->ctx) {
         cudaSetDevice(sc->ctx->device);
         cudaStreamSynchronize(sc->ctx->stream);
+        auto& live = sc->ctx->live;
+        live.erase(std::remove(live.begin(), live.end(), sc), live.end());
     }
-    void* ps[] = {sc->gray, sc->rgb, sc->census, sc->rays, sc->plane_a, sc->plane_b, sc->pcost_a, sc->pcost_b,
-                  sc->pd_a, sc->pd_b,
-                  sc->depth, sc->cost, sc->normal, sc->d_views, sc->d_tile_start, sc->d_cams,
-                  sc->gray_q, sc->census_q, sc->rays_q, sc->d_qviews, sc->d_qtile_start, sc->d_qcams,
-                  sc->d_qblk_start};
+    void* quarter[] = {sc->gray_q, sc->census_q, sc->rays_q, sc->d_qviews, sc->d_qtile_start, sc->d_qcams,
+                       sc->d_qblk_start};
     drop_graph(sc);
-    for (void* p : ps)
+    for (void* p : quarter)
         if (p) cudaFree(p);
-    sc->arena.release();
+    if (sc->ctx && sc->cap_px > 0) {
+        // keep the buffers for the context's next scene
+        free_spare(sc->ctx);
+        rcmvs_ctx::SpareScene& s = sc->ctx->spare;
+        for (int i = 0; i < 13; ++i) s.big[i] = *scene_big(sc, i);
+        for (int i = 0; i < 3; ++i) s.small[i] = *scene_small(sc, i);
+        s.arena.slots = std::move(sc->arena.slots);
+        sc->arena.slots.clear();
+        s.cap_px = sc->cap_px;
+        s.cap_views = sc->cap_views;
+        s.valid = true;
+    } else {
+        for (int i = 0; i < 13; ++i)
+            if (*scene_big(sc, i)) cudaFree(*scene_big(sc, i));
+        for (int i = 0; i < 3; ++i)
+            if (*scene_small(sc, i)) cudaFree(*scene_small(sc, i));
+        sc->arena.release();
+    }
     delete sc;
 }
 
@@ -223,6 +280,7 @@ int rcmvs_scene_create(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views,
     CK(cudaSetDevice(ctx->device));
     rcmvs_scene* sc = new rcmvs_scene();
     sc->ctx = ctx;
+    ctx->live.push_back(sc);
     sc->n_views = n_views;
     sc->has_rgb = true;
     int64_t off = 0;
@@ -251,6 +309,19 @@ int rcmvs_scene_create(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views,
     const size_t np = (size_t)off;
     auto alloc = [&](void** p, size_t bytes) { return cudaMalloc(p, bytes); };
     cudaError_t e = cudaSuccess;
+    rcmvs_ctx::SpareScene& spare = ctx->spare;
+    if (spare.valid && spare.cap_px >= np && spare.cap_views >= n_views && (spare.big[1] || !sc->has_rgb)) {
+        // the previous scene's buffers and scratch: every one is written before it is read
+        for (int i = 0; i < 13; ++i) *scene_big(sc, i) = spare.big[i];
+        for (int i = 0; i < 3; ++i) *scene_small(sc, i) = spare.small[i];
+        sc->arena.slots = std::move(spare.arena.slots);
+        spare.arena.slots.clear();
+        sc->cap_px = spare.cap_px;
+        sc->cap_views = spare.cap_views;
+        for (void*& p : spare.big) p = nullptr;
+        for (void*& p : spare.small) p = nullptr;
+        spare.valid = false;
+    } else {
     if (!e) e = alloc((void**)&sc->gray, np);
     if (!e && sc->has_rgb) e = alloc((void**)&sc->rgb, 3 * np);
     if (!e) e = alloc((void**)&sc->census, 8 * np);
@@ -267,6 +338,11 @@ int rcmvs_scene_create(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views,
     if (!e) e = alloc((void**)&sc->d_views, sizeof(DevView) * n_views);
     if (!e) e = alloc((void**)&sc->d_tile_start, sizeof(int32_t) * (n_views + 1));
     if (!e) e = alloc((void**)&sc->d_cams, sizeof(double) * 4 * n_views);
+    if (!e) {
+        sc->cap_px = np;
+        sc->cap_views = n_views;
+    }
+    }
     if (e) {
         rcmvs_scene_destroy(sc);
         return fail(ctx, e == cudaErrorMemoryAllocation ? RCMVS_E_NOMEM : RCMVS_E_CUDA,

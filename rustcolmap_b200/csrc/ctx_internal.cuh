@@ -30,6 +30,23 @@ struct rcmvs_ctx {
     };
     bool timing = false;
     std::vector<Span> spans;
+    // Device buffers and scratch arena of the last destroyed scene, adopted
+    // by the next scene they are large enough for (rcmvs_scene_create), so
+    // repeated rcmvs_run_mvs* calls on a workload allocate nothing.  Freed
+    // with the context.  Order of `big`: gray, rgb, census, rays, plane_a,
+    // plane_b, pcost_a, pcost_b, pd_a, pd_b, depth, cost, normal; `small`:
+    // d_views, d_tile_start, d_cams.
+    struct SpareScene {
+        bool valid = false;
+        size_t cap_px = 0;
+        int cap_views = 0;
+        void* big[13] = {};
+        void* small[3] = {};
+        DeviceArena arena;
+    } spare;
+    // scenes created on this context and not yet destroyed; a context that
+    // is destroyed first detaches them (they then free their own buffers)
+    std::vector<rcmvs_scene*> live;
     SpanHook hook() {
         SpanHook h;
         if (timing) {
@@ -72,6 +89,8 @@ struct rcmvs_scene {
     rcmvs_ctx* ctx = nullptr;
     int n_views = 0;
     int64_t n_px = 0;
+    size_t cap_px = 0;  // pixels / views the device buffers hold (0 until allocated)
+    int cap_views = 0;
     std::vector<DevView> views;
     std::vector<HostCam> cams;
     std::vector<char> has_depth;

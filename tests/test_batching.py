@@ -139,3 +139,30 @@ def test_learned_init_with_batched_schedules(uneven):
     b.close()
     net.close()
     ctx.close()
+
+
+def test_scene_buffers_reused_across_scenes(uneven):
+    """A context hands the buffers of a destroyed scene to the next scene
+    that fits in them: results stay the oracle's whatever the sequence of
+    scene sizes, and a context closed before its scene detaches it."""
+    sc, opts, jobs, ref = uneven
+    ctx = mvs.Context(0)
+    big = mvs.DeviceScene(sc.views, ctx)
+    big.estimate(jobs, opts)
+    _check(big, jobs, ref, "first scene")
+    big.close()
+    # smaller scenes (the views one job touches) adopt the buffers, larger ones allocate
+    for (r, srcs, a, b) in jobs[:3] + [jobs[0]]:
+        sub = [r] + list(srcs)
+        remap = {v: i for i, v in enumerate(sub)}
+        views = [sc.views[v] for v in sub]
+        dm = mvs.estimate_depth(views, 0, [remap[s] for s in srcs], a, b, opts, ctx, normals=True)
+        d, c, n = ref[r]
+        assert np.array_equal(bits(dm.depth), bits(d)) and np.array_equal(bits(dm.cost), bits(c))
+        again = mvs.DeviceScene(sc.views, ctx)
+        again.estimate(jobs, opts)
+        _check(again, jobs, ref, "after a smaller scene")
+        again.close()
+    orphan = mvs.DeviceScene(sc.views, ctx)
+    ctx.close()
+    orphan.close()  # its context is gone: the scene frees its own buffers
