@@ -2,6 +2,7 @@
 // scenes, the host-buffer entry points that stand in for the reference `mvs`
 // crate, the run_mvs host glue and the PLY writer.
 #include <algorithm>
+#include <thread>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -913,6 +914,36 @@ double percentile(const std::vector<double>& s, double q) {
     idx = std::min(std::max(idx, 0.0), (double)s.size() - 1.0);
     return s[(size_t)idx];
 }
+
+// The same on an unsorted sample: the element a sort would put at that
+// index, found by selection (same value, linear time; reorders s).
+double percentile_select(std::vector<double>& s, double q) {
+    if (s.empty()) return 0.0;
+    double idx = std::round(((double)s.size() - 1.0) * q);
+    idx = std::min(std::max(idx, 0.0), (double)s.size() - 1.0);
+    auto it = s.begin() + (std::ptrdiff_t)idx;
+    std::nth_element(s.begin(), it, s.end());
+    return *it;
+}
+
+// Runs f(t, begin, end) on nt threads over [0, n) in contiguous chunks.
+template <class F>
+void par_chunks(int64_t n, int nt, F&& f) {
+    nt = (int)std::max<int64_t>(1, std::min<int64_t>(nt, n));
+    if (nt == 1) {
+        f(0, (int64_t)0, n);
+        return;
+    }
+    std::vector<std::thread> ts;
+    for (int t = 0; t < nt; ++t)
+        ts.emplace_back([&, t] { f(t, n * t / nt, n * (t + 1) / nt); });
+    for (auto& th : ts) th.join();
+}
+
+int plan_threads() {
+    const unsigned hc = std::thread::hardware_concurrency();
+    return (int)std::min(16u, std::max(1u, hc));
+}
 }  // namespace
 
 extern "C" {
@@ -934,23 +965,34 @@ int rcmvs_plan(const rcmvs_sparse* sp, const rcmvs_view* views, int32_t n_views,
         global[p] = std::sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
     }
     std::sort(global.begin(), global.end());
-    std::vector<uint32_t> cov((size_t)n * n, 0);
-    std::vector<std::vector<uint64_t>> seen_by(n);
-    std::vector<int> ids;
-    for (uint64_t p = 0; p < sp->n_points; ++p) {
-        ids.clear();
-        for (uint64_t q = sp->track_offsets[p]; q < sp->track_offsets[p + 1]; ++q) {
-            int v = sp->track_views[q];
-            if (v >= 0 && v < n) ids.push_back(v);
+    // co-visibility counts and the points each view sees (lib.rs:224-243):
+    // integer counts, summed over threads that each take a range of points
+    // with their own count matrix (at most 256 MB of them)
+    const int nt = (int)std::max<int64_t>(
+        1, std::min<int64_t>(plan_threads(), (int64_t(64) << 20) / std::max<int64_t>(1, (int64_t)n * n)));
+    std::vector<std::vector<uint32_t>> covt(nt, std::vector<uint32_t>((size_t)n * n, 0));
+    std::vector<std::vector<std::vector<uint64_t>>> seen_t(nt, std::vector<std::vector<uint64_t>>(n));
+    par_chunks((int64_t)sp->n_points, nt, [&](int t, int64_t p0, int64_t p1) {
+        std::vector<int> ids;
+        std::vector<uint32_t>& cv = covt[t];
+        for (int64_t p = p0; p < p1; ++p) {
+            ids.clear();
+            for (uint64_t q = sp->track_offsets[p]; q < sp->track_offsets[p + 1]; ++q) {
+                int v = sp->track_views[q];
+                if (v >= 0 && v < n) ids.push_back(v);
+            }
+            std::sort(ids.begin(), ids.end());
+            ids.erase(std::unique(ids.begin(), ids.end()), ids.end());
+            for (int a : ids) {
+                seen_t[t][a].push_back((uint64_t)p);
+                for (int b : ids)
+                    if (a != b) cv[(size_t)a * n + b]++;
+            }
         }
-        std::sort(ids.begin(), ids.end());
-        ids.erase(std::unique(ids.begin(), ids.end()), ids.end());
-        for (int a : ids) {
-            seen_by[a].push_back(p);
-            for (int b : ids)
-                if (a != b) cov[(size_t)a * n + b]++;
-        }
-    }
+    });
+    std::vector<uint32_t>& cov = covt[0];
+    for (int t = 1; t < nt; ++t)
+        for (size_t e = 0; e < cov.size(); ++e) cov[e] += covt[t][e];
     std::vector<std::vector<int>> sources(n);
     std::vector<char> has(n, 0);
     int off = 0;
@@ -967,32 +1009,36 @@ int rcmvs_plan(const rcmvs_sparse* sp, const rcmvs_view* views, int32_t n_views,
         has[i] = !sources[i].empty();
     }
     src_offsets[n] = off;
-    for (int i = 0; i < n; ++i) {  // depth_range_for (lib.rs:253-282)
-        const rcmvs_view& v = views[i];
+    // depth_range_for (lib.rs:253-282), views in parallel; the percentiles
+    // are order statistics, so selection gives the sorted list's values
+    par_chunks(n, plan_threads(), [&](int, int64_t i0, int64_t i1) {
         std::vector<double> ds;
-        for (uint64_t p : seen_by[i]) {
-            const double* x = sp->xyz + 3 * p;
-            double z = (v.R[6] * x[0] + v.R[7] * x[1] + v.R[8] * x[2]) + v.t[2];
-            if (z > 1e-6) ds.push_back(z);
+        for (int64_t i = i0; i < i1; ++i) {
+            const rcmvs_view& v = views[i];
+            ds.clear();
+            for (int t = 0; t < nt; ++t)
+                for (uint64_t p : seen_t[t][i]) {
+                    const double* x = sp->xyz + 3 * p;
+                    double z = (v.R[6] * x[0] + v.R[7] * x[1] + v.R[8] * x[2]) + v.t[2];
+                    if (z > 1e-6) ds.push_back(z);
+                }
+            double lo = 0.0, hi = 0.0;
+            if (ds.size() >= 8) {
+                lo = percentile_select(ds, 0.02);
+                hi = percentile_select(ds, 0.98);
+            } else if (global.size() >= 8) {
+                lo = percentile(global, 0.02);
+                hi = percentile(global, 0.98);
+            }
+            if (hi <= lo * 1.05 || lo <= 0.0) {
+                zrange[2 * i] = std::fmax(percentile(global, 0.01) * 0.7, 1e-3);
+                zrange[2 * i + 1] = percentile(global, 0.99) * 1.4;
+            } else {
+                zrange[2 * i] = lo * 0.8;
+                zrange[2 * i + 1] = hi * 1.25;
+            }
         }
-        const std::vector<double>* src = &global;
-        if (ds.size() >= 8) {
-            std::sort(ds.begin(), ds.end());
-            src = &ds;
-        }
-        double lo = 0.0, hi = 0.0;
-        if (src->size() >= 8) {
-            lo = percentile(*src, 0.02);
-            hi = percentile(*src, 0.98);
-        }
-        if (hi <= lo * 1.05 || lo <= 0.0) {
-            zrange[2 * i] = std::fmax(percentile(global, 0.01) * 0.7, 1e-3);
-            zrange[2 * i + 1] = percentile(global, 0.99) * 1.4;
-        } else {
-            zrange[2 * i] = lo * 0.8;
-            zrange[2 * i + 1] = hi * 1.25;
-        }
-    }
+    });
     off = 0;
     for (int i = 0; i < n; ++i) {  // fusion order, sources first (lib.rs:398-418)
         std::vector<std::pair<uint32_t, int>> o;

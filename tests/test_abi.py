@@ -96,10 +96,14 @@ def test_plan_matches_oracle(corner_scene, c1_opts):
     assert all(len(s) == 4 for s in a[0])
 
 
-def test_plan_matches_oracle_orbit():
+@pytest.mark.parametrize("n_views,per_view,k", [(24, 120, 8), (100, 300, 10)])
+def test_plan_matches_oracle_orbit(n_views, per_view, k):
+    """The library's plan (threaded co-visibility, depth percentiles by
+    selection) against the oracle's sequential one; the second case has the
+    C5 workload's view count and sparse density."""
     from rustcolmap_b200 import scene
-    sc = scene.orbit_room(seed=3, n_views=24, sizes=((96, 72),), n_boxes=8, per_view_sparse=120)
-    o = MvsOptions(num_sources=8)
+    sc = scene.orbit_room(seed=3, n_views=n_views, sizes=((96, 72),), n_boxes=8, per_view_sparse=per_view)
+    o = MvsOptions(num_sources=k)
     a = mvs.plan(sc.sparse, sc.views, o)
     b = oracle.plan(sc.sparse, sc.views, o)
     assert a[0] == b[0] and a[2] == b[2] and np.array_equal(a[1], b[1])
