@@ -43,9 +43,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 FP32_NOMINAL_TOPS = 148 * 128 * 1.965e9 / 1e12  # SMs x FP32 lanes x max clock (ops/s, no FMA pairing)
-# DRAM bytes (read + write) per reference pixel of one pass launch, from the
-# ncu capture in profiles/pass_kernel_c2_24views.md (1.113 GB over 16.59 Mpx),
-# scaled to the measured workload's pixels for roofline.traffic.
+# DRAM bytes (read + write) per reference pixel of one pass launch, from an
+# ncu capture of the pass kernel on 24 views at 960x720 (1.113 GB over 16.59
+# Mpx), scaled to the measured workload's pixels for roofline.traffic.
 PASS_DRAM_BYTES_PER_PX = 1113303040 / (24 * 960 * 720)
 
 
@@ -620,8 +620,8 @@ def main():
             "roofline": {"bound": "hbm", "kernel": "stereo_pass", "achieved": achieved_gbs, "peak": hbm_peak,
                          "unit": "GB/s", "frac": achieved_gbs / hbm_peak,
                          "traffic": PASS_DRAM_BYTES_PER_PX * npx,
-                         "traffic_source": "ncu dram bytes per pixel of a 24-view 960x720 capture "
-                                           "(profiles/pass_kernel_c2_24views.md) x this launch's pixels",
+                         "traffic_source": "ncu dram bytes per pixel of a 24-view 960x720 capture of the "
+                                           "pass kernel x this launch's pixels",
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650",
                          "algorithmic_bytes_per_launch": bytes_per_launch, "avg_launch_ms": pass_avg_s * 1e3,
                          "note": "issue-bound kernel: see compute_roofline"},
