@@ -11,7 +11,8 @@
 //               the quadratic fit (nalgebra's cofactor 3x3 inverse, f64), the
 //               contrast and curvature tests (sift.rs:176-262); flags are
 //               compacted stably, so keypoints keep the reference's
-//               (level, y, x) order
+//               (octave, level, y, x) order; each octave's count stays on the
+//               device and the next octave starts without waiting for it
 //   orientation one warp per keypoint (in response order, see output):
 //               lanes evaluate 32 window samples at a time (atan2, exp in
 //               f64), each lane owns histogram bins and
@@ -242,17 +243,22 @@ __global__ void extrema_kernel(const float* __restrict__ dogs, int w, int h, dou
     }
 }
 
-// Gathers the compacted keypoints (sel: indices into the flag space).
-__global__ void gather_kp_kernel(const uint32_t* __restrict__ sel, int n, int64_t npx, const double* __restrict__ kx,
-                                 const double* __restrict__ ky, const double* __restrict__ kresp, int octave,
-                                 KpArrays kp) {
+// Appends the compacted keypoints of one octave (sel: indices into its flag
+// space; counts[o]: each octave's count, on the device) after those of the
+// octaves before it.
+__global__ void gather_kp_kernel(const uint32_t* __restrict__ sel, const int* __restrict__ counts, int octave,
+                                 int64_t npx, const double* __restrict__ kx, const double* __restrict__ ky,
+                                 const double* __restrict__ kresp, KpArrays kp) {
+    int64_t base = 0;
+    for (int q = 0; q < octave; ++q) base += counts[q];
+    const int n = counts[octave];
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const uint32_t t = sel[k];
-        kp.x[k] = kx[t];
-        kp.y[k] = ky[t];
-        kp.resp[k] = kresp[t];
-        kp.level[k] = 1 + (int)((int64_t)t / npx);
-        kp.oct[k] = octave;
+        kp.x[base + k] = kx[t];
+        kp.y[base + k] = ky[t];
+        kp.resp[base + k] = kresp[t];
+        kp.level[base + k] = 1 + (int)((int64_t)t / npx);
+        kp.oct[base + k] = octave;
     }
 }
 
@@ -576,7 +582,7 @@ int sfail(rcmvs_ctx* ctx, int code, const std::string& msg) {
 enum {
     F_IN = 80, F_GRAY, F_RGB, F_BASE, F_LEV, F_TMP, F_DOG, F_FLAG, F_KX, F_KY, F_KRESP, F_SEL, F_NSEL, F_TEMP,
     F_KPX, F_KPY, F_KPRESP, F_KPLEV, F_KPOCT, F_THETA, F_CNT, F_OFF, F_PKP, F_PTH, F_PIDX, F_SRESP, F_SIDX,
-    F_DESC, F_VALID, F_OSEL, F_PTS, F_FDESC, F_COL, F_NEXT,
+    F_DESC, F_VALID, F_OSEL, F_PTS, F_FDESC, F_COL, F_NEXT, F_OCTCNT,
     F_GRAD = 130  // 130 + 2 * octave: gx, + 1: gy (octaves 0..7)
 };
 
@@ -674,13 +680,27 @@ int rcmvs_extract_sift(rcmvs_ctx* ctx, const uint8_t* img, int32_t w0, int32_t h
     const SpanHook& hook = ctx->hook();
     if (n_oct > MAX_OCT) return sfail(ctx, RCMVS_E_LIMIT, "sift: too many octaves");
     OctTable table{};
-    int64_t nkp = 0;  // keypoints of all octaves so far
-    uint64_t n_raw = 0;
     int ow = w, oh = h;
     thrust::counting_iterator<uint32_t> it(0);
-    void *p_temp, *p_nsel;
+    void *p_temp, *p_nsel, *p_octcnt;
     SCK(A.get(F_NSEL, sizeof(int) * 4, &p_nsel));
+    SCK(A.get(F_OCTCNT, sizeof(int) * MAX_OCT, &p_octcnt));
+    int* d_oct = (int*)p_octcnt;
+    // keypoint arrays sized for every pixel of DoG levels 1-3 of every
+    // octave, so the octaves run back to back with their counts on the device
+    int64_t kcap = 0;
+    for (int o = 0, tw = w, th = h; o < n_oct; ++o, tw = std::max(tw / 2, 1), th = std::max(th / 2, 1))
+        kcap += NSPO * (int64_t)tw * th;
     KpArrays kp{};
+    {
+        void *p_x, *p_y, *p_r, *p_l, *p_o;
+        SCK(A.get(F_KPX, 8 * (size_t)kcap, &p_x));
+        SCK(A.get(F_KPY, 8 * (size_t)kcap, &p_y));
+        SCK(A.get(F_KPRESP, 8 * (size_t)kcap, &p_r));
+        SCK(A.get(F_KPLEV, 4 * (size_t)kcap, &p_l));
+        SCK(A.get(F_KPOCT, 4 * (size_t)kcap, &p_o));
+        kp = KpArrays{(double*)p_x, (double*)p_y, (double*)p_r, (int32_t*)p_l, (int32_t*)p_o};
+    }
     for (int o = 0; o < n_oct; ++o) {
         const int64_t npx = (int64_t)ow * oh;
         void *p_lev, *p_tmp, *p_dog, *p_flag, *p_kx, *p_ky, *p_kr, *p_sel;
@@ -719,44 +739,24 @@ int rcmvs_extract_sift(rcmvs_ctx* ctx, const uint8_t* img, int32_t w0, int32_t h
         SCK(cudaGetLastError());
         hook.end("sift_extrema");
         size_t tb = 0;
-        SCK(cub::DeviceSelect::Flagged(nullptr, tb, it, (const uint8_t*)p_flag, (uint32_t*)p_sel, (int*)p_nsel,
+        SCK(cub::DeviceSelect::Flagged(nullptr, tb, it, (const uint8_t*)p_flag, (uint32_t*)p_sel, d_oct + o,
                                        (int)nt, st));
         SCK(A.get(F_TEMP, tb, &p_temp));
-        SCK(cub::DeviceSelect::Flagged(p_temp, tb, it, (const uint8_t*)p_flag, (uint32_t*)p_sel, (int*)p_nsel,
+        SCK(cub::DeviceSelect::Flagged(p_temp, tb, it, (const uint8_t*)p_flag, (uint32_t*)p_sel, d_oct + o,
                                        (int)nt, st));
-        int nk = 0;
-        SCK(cudaMemcpyAsync(&nk, p_nsel, sizeof(int), cudaMemcpyDeviceToHost, st));
-        SCK(cudaStreamSynchronize(st));
-        n_raw += (uint64_t)nk;
-        const double scale = std::pow(2.0, o);
         table.w[o] = ow;
         table.h[o] = oh;
-        table.scale[o] = scale;
-        if (nk > 0) {
-            // this octave's keypoints appended to the list of all octaves
-            const size_t keep = (size_t)nkp, need = (size_t)(nkp + nk);
-            void *p_x, *p_y, *p_r, *p_l, *p_o;
-            int rc2;
-            if ((rc2 = grow_copy(ctx, F_KPX, 8 * need, 8 * keep, &p_x)) ||
-                (rc2 = grow_copy(ctx, F_KPY, 8 * need, 8 * keep, &p_y)) ||
-                (rc2 = grow_copy(ctx, F_KPRESP, 8 * need, 8 * keep, &p_r)) ||
-                (rc2 = grow_copy(ctx, F_KPLEV, 4 * need, 4 * keep, &p_l)) ||
-                (rc2 = grow_copy(ctx, F_KPOCT, 4 * need, 4 * keep, &p_o)))
-                return rc2;
-            kp = KpArrays{(double*)p_x, (double*)p_y, (double*)p_r, (int32_t*)p_l, (int32_t*)p_o};
-            const KpArrays here{kp.x + nkp, kp.y + nkp, kp.resp + nkp, kp.level + nkp, kp.oct + nkp};
-            gather_kp_kernel<<<grid_of(nk), 256, 0, st>>>((const uint32_t*)p_sel, nk, npx, (const double*)p_kx,
-                                                           (const double*)p_ky, (const double*)p_kr, o, here);
-            SCK(cudaGetLastError());
-            void *p_gx, *p_gy;
-            SCK(A.get(F_GRAD + 2 * o, sizeof(float) * NSPO * (size_t)npx, &p_gx));
-            SCK(A.get(F_GRAD + 2 * o + 1, sizeof(float) * NSPO * (size_t)npx, &p_gy));
-            table.gx[o] = (const float*)p_gx;
-            table.gy[o] = (const float*)p_gy;
-            grad_kernel<<<grid_of(NSPO * npx), 256, 0, st>>>(lev, ow, oh, (float*)p_gx, (float*)p_gy);
-            SCK(cudaGetLastError());
-            nkp += nk;
-        }
+        table.scale[o] = std::pow(2.0, o);
+        gather_kp_kernel<<<grid_of(nt), 256, 0, st>>>((const uint32_t*)p_sel, d_oct, o, npx, (const double*)p_kx,
+                                                       (const double*)p_ky, (const double*)p_kr, kp);
+        SCK(cudaGetLastError());
+        void *p_gx, *p_gy;
+        SCK(A.get(F_GRAD + 2 * o, sizeof(float) * NSPO * (size_t)npx, &p_gx));
+        SCK(A.get(F_GRAD + 2 * o + 1, sizeof(float) * NSPO * (size_t)npx, &p_gy));
+        table.gx[o] = (const float*)p_gx;
+        table.gy[o] = (const float*)p_gy;
+        grad_kernel<<<grid_of(NSPO * npx), 256, 0, st>>>(lev, ow, oh, (float*)p_gx, (float*)p_gy);
+        SCK(cudaGetLastError());
         // next octave's base: level NSPO downsampled 2x2 (sift.rs:488-492)
         const int nw = std::max(ow / 2, 1), nh = std::max(oh / 2, 1);
         if (o + 1 < n_oct) {
@@ -772,9 +772,14 @@ int rcmvs_extract_sift(rcmvs_ctx* ctx, const uint8_t* img, int32_t w0, int32_t h
         oh = nh;
     }
     int bad = 0;
+    int oc[MAX_OCT] = {0};
     if (d_err) SCK(cudaMemcpyAsync(&bad, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SCK(cudaMemcpyAsync(oc, d_oct, sizeof(int) * n_oct, cudaMemcpyDeviceToHost, st));
     SCK(cudaStreamSynchronize(st));
     if (bad) return sfail(ctx, RCMVS_E_CUDA, "sift: resize tap table overflow");
+    int64_t nkp = 0;  // keypoints of all octaves
+    for (int o = 0; o < n_oct; ++o) nkp += oc[o];
+    const uint64_t n_raw = (uint64_t)nkp;
     if (nkp > INT32_MAX / 4) return sfail(ctx, RCMVS_E_LIMIT, "sift: too many keypoints");
 
     // The reference computes every (keypoint, peak) descriptor in (octave,
