@@ -96,3 +96,26 @@ def match_pair(fa, fb, ratio=0.8, ctx=None):
     da = fa.desc if isinstance(fa, SiftFrame) else fa
     db = fb.desc if isinstance(fb, SiftFrame) else fb
     return match_pairs([da, db], [(0, 1)], ratio, ctx)[0]
+
+
+def job_pairs(n, sequential=False):
+    """The image pairs sfm-lite matches (sfm-lite/src/lib.rs:197-212): each
+    image with the next three when `sequential`, else every pair i < j, in
+    the reference's order."""
+    if sequential:
+        return [(i, i + k) for i in range(n) for k in (1, 2, 3) if i + k < n]
+    return [(i, j) for i in range(n) for j in range(i + 1, n)]
+
+
+def extract_and_match(images, names=None, opts=None, ratio=0.75, sequential=False, ctx=None):
+    """The feature stage of sfm-lite's run_sfm (sfm-lite/src/lib.rs:137-225,
+    two-view verification excluded): SIFT of every decoded image, then
+    match_pair on every job pair in one batched call.  `ratio` defaults to
+    sfm-lite's Options::default() (lib.rs:61).  Returns (frames, pairs,
+    matches) with matches[p] = (a indices, b indices) of pairs[p]."""
+    if len(images) < 2:
+        raise RcmvsError(-1, "need at least 2 images")
+    names = names or [""] * len(images)
+    frames = [extract_sift(im, nm, opts, ctx) for im, nm in zip(images, names)]
+    pairs = job_pairs(len(frames), sequential)
+    return frames, pairs, match_pairs([f.desc for f in frames], pairs, ratio, ctx)

@@ -245,3 +245,24 @@ def test_gpu_match_pairs_matches_oracle(ctx):
     ga, gb = sift.match_pair(f0, f1, ctx=ctx)
     assert len(ga) > 50
     print(f"\nSIFT 384x288 views 0 and 5: {len(ga)} mutual matches of {len(f0.pts)} x {len(f1.pts)}")
+
+
+def test_job_pairs():
+    assert sift.job_pairs(4) == [(0, 1), (0, 2), (0, 3), (1, 2), (1, 3), (2, 3)]
+    assert sift.job_pairs(5, sequential=True) == [(0, 1), (0, 2), (0, 3), (1, 2), (1, 3), (1, 4), (2, 3), (2, 4),
+                                                  (3, 4)]
+    assert sift.job_pairs(1) == [] and sift.job_pairs(2, True) == [(0, 1)]
+    with pytest.raises(sift.RcmvsError):
+        sift.extract_and_match([np.zeros((8, 8), np.uint8)])
+
+
+@pytest.mark.gpu
+def test_extract_and_match_pipeline(ctx):
+    sc = scene.corner_room(seed=4, n_views=4, w=160, h=120, f=180.0, arc_deg=30.0, n_patches=40, per_view_sparse=10)
+    imgs = [np.ascontiguousarray(v.rgb) for v in sc.views]
+    frames, pairs, matches = sift.extract_and_match(imgs, sequential=True, ctx=ctx)
+    assert pairs == sift.job_pairs(4, True) and len(matches) == len(pairs)
+    for (i, j), (a, b) in zip(pairs, matches):
+        oa, ob = oracle.match_pair(frames[i].desc, frames[j].desc, 0.75)
+        assert np.array_equal(a, oa) and np.array_equal(b, ob)
+    assert sum(len(a) for a, _ in matches) > 0
