@@ -157,3 +157,16 @@ def test_gpu_resize_arguments(ctx):
             mvs.resize_view(img, mw, mh, ctx)
     with pytest.raises(mvs.RcmvsError):
         mvs.resize_view(np.zeros((4, 4, 5), np.uint8), 2, 2, ctx)
+
+
+def test_oracle_matches_numpy_random_sizes():
+    """Seeded random shapes, ratios (down and up, per axis) and channel counts."""
+    rng = np.random.default_rng(2024)
+    for k in range(24):
+        h, w = (int(v) for v in rng.integers(1, 90, 2))
+        c = int(rng.integers(1, 5))
+        mh, mw = (int(v) for v in rng.integers(1, 120, 2))
+        img = image(100 + k, h, w, c)
+        a = oracle.resize_view(img, mw, mh)
+        b = resize_np(img, mw, mh)
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]), (h, w, c, mw, mh)

@@ -266,3 +266,17 @@ def test_extract_and_match_pipeline(ctx):
         oa, ob = oracle.match_pair(frames[i].desc, frames[j].desc, 0.75)
         assert np.array_equal(a, oa) and np.array_equal(b, ob)
     assert sum(len(a) for a, _ in matches) > 0
+
+
+def test_oracle_match_pair_matches_numpy_random():
+    """Seeded random set sizes, noise, duplicate counts and ratios."""
+    rng = np.random.default_rng(77)
+    for k in range(12):
+        na, nb = (int(v) for v in rng.integers(1, 90, 2))
+        noise = float(rng.choice([0.0, 0.005, 0.03, 0.1]))
+        dup = int(rng.integers(0, 4))
+        a, b = desc_sets(1000 + k, na, nb, noise, dup)
+        ratio = float(rng.choice([0.6, 0.75, 0.8, 0.95]))
+        x = oracle.match_pair(a, b, ratio)
+        y = match_numpy(a, b, ratio)
+        assert np.array_equal(x[0], y[0]) and np.array_equal(x[1], y[1]), (na, nb, noise, dup, ratio)
