@@ -178,3 +178,102 @@ def run_mvs_sharded(views, sparse, opts, group=None, ctx=None, stereo=None, cand
     ax, ac = all_gather_candidates(cx, cc, per_view, group=group, device=device)
     xyz, rgb = reduce(ax, ac)
     return xyz, rgb, depth
+
+
+# ------------------------------------------------------------ SfM front end
+def _gather_items(local, n_items, group=None, device="cpu"):
+    """All-gather variable-size float64 vectors keyed 0..n_items-1, each
+    produced on exactly one rank: local = {item: 1-D array}.  Returns
+    {item: array} for every item, the same on every rank.  One all_gather of
+    the per-rank sizes and item lengths, one of the data padded to the
+    largest rank's size."""
+    import torch
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    lens = np.full(n_items, -1, np.int64)
+    for k, v in local.items():
+        lens[k] = len(v)
+    flat = np.concatenate([np.asarray(local[k], np.float64).ravel() for k in sorted(local)]) if local \
+        else np.zeros(0, np.float64)
+    head = np.concatenate([[len(flat)], lens]).astype(np.int64)
+    heads = [torch.empty(n_items + 1, dtype=torch.int64, device=device) for _ in range(world)]
+    dist.all_gather(heads, torch.from_numpy(head).to(device), group=group)
+    heads = [h.cpu().numpy() for h in heads]
+    n_max = max(1, max(int(h[0]) for h in heads))
+    buf = np.zeros(n_max, np.float64)
+    buf[:len(flat)] = flat
+    parts = [torch.empty(n_max, dtype=torch.float64, device=device) for _ in range(world)]
+    dist.all_gather(parts, torch.from_numpy(buf).to(device), group=group)
+    out = {}
+    for r in range(world):
+        data = parts[r].cpu().numpy()
+        o = 0
+        for k in range(n_items):
+            ln = int(heads[r][1 + k])
+            if ln >= 0:
+                out[k] = data[o:o + ln].copy()
+                o += ln
+    return out
+
+
+def _pack_frame(f):
+    n = len(f.pts)
+    return np.concatenate([[f.width, f.height, n, f.n_raw], f.pts.ravel(), f.desc.ravel().astype(np.float64),
+                           f.colors.ravel().astype(np.float64)])
+
+
+def _unpack_frame(v, name):
+    from .sift import DESC_LEN, SiftFrame
+    w, h, n, n_raw = (int(x) for x in v[:4])
+    o = 4
+    pts = v[o:o + 2 * n].reshape(n, 2).copy()
+    o += 2 * n
+    desc = v[o:o + DESC_LEN * n].astype(np.float32).reshape(n, DESC_LEN)
+    o += DESC_LEN * n
+    col = v[o:o + 3 * n].astype(np.uint8).reshape(n, 3)
+    return SiftFrame(name, w, h, pts, desc, col, n_raw)
+
+
+def extract_and_match_sharded(images, names=None, opts=None, ratio=0.75, sequential=False, group=None, ctx=None,
+                              extract=None, match=None, device="cpu"):
+    """sift.extract_and_match with images and pairs spread over the ranks of
+    `group`: each rank extracts the SIFT features of its share of the images
+    (longest-processing-time order on pixel counts), the frames are
+    all-gathered, each rank matches its share of the job pairs (by na * nb),
+    and the matches are all-gathered.  Returns (frames, pairs, matches) on
+    every rank, equal to the single-process result (the same computations,
+    spread differently; descriptors travel as exact f64).
+
+    extract(image, name) -> SiftFrame and match(descs, pairs) -> [(a, b)]
+    default to the library on this rank's GPU; they are parameters so that
+    the host logic can run with other back ends."""
+    import torch.distributed as dist
+    from . import sift
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    n = len(images)
+    if n < 2:
+        raise sift.RcmvsError(-1, "need at least 2 images")
+    names = names or [""] * n
+    if extract is None:
+        def extract(im, nm):
+            return sift.extract_sift(im, nm, opts, ctx)
+    if match is None:
+        def match(descs, prs):
+            return sift.match_pairs(descs, prs, ratio, ctx)
+    img_parts = assign_views([int(np.asarray(im).shape[0]) * int(np.asarray(im).shape[1]) for im in images], world)
+    local = {i: _pack_frame(extract(images[i], names[i])) for i in img_parts[rank]}
+    packed = _gather_items(local, n, group, device)
+    frames = [_unpack_frame(packed[i], names[i]) for i in range(n)]
+    pairs = sift.job_pairs(n, sequential)
+    pair_parts = assign_views([max(len(frames[i].pts) * len(frames[j].pts), 1) for i, j in pairs], world)
+    mine = pair_parts[rank]
+    got = match([f.desc for f in frames], [pairs[p] for p in mine]) if mine else []
+    local_m = {p: np.concatenate([a, b]).astype(np.float64) for p, (a, b) in zip(mine, got)}
+    allm = _gather_items(local_m, len(pairs), group, device)
+    matches = []
+    for p in range(len(pairs)):
+        v = allm[p].astype(np.uint32)
+        k = len(v) // 2
+        matches.append((v[:k], v[k:]))
+    return frames, pairs, matches

@@ -13,7 +13,7 @@ import tempfile
 import numpy as np
 import pytest
 
-from rustcolmap_b200 import shard
+from rustcolmap_b200 import scene, shard
 
 
 def _free_port():
@@ -95,7 +95,7 @@ def test_all_gather_maps_gloo(world, owners):
 
 
 def _tiny():
-    from rustcolmap_b200 import MvsOptions, scene
+    from rustcolmap_b200 import MvsOptions
     sc = scene.corner_room(seed=2, n_views=5, w=96, h=64, f=110.0, arc_deg=40.0, n_patches=20, per_view_sparse=60)
     opts = MvsOptions(max_dim=4096, num_sources=2, sweeps=1, num_hyp=8, min_consistent=1)
     return sc, opts
@@ -240,3 +240,53 @@ def test_sharded_run_on_one_gpu_equals_run_mvs():
         dist.destroy_process_group()
     ctx.close()
     assert np.array_equal(xa, xb) and np.array_equal(ca, cb)
+
+
+# ------------------------------------------------------------ SfM front end
+def _sfm_images():
+    sc = scene.corner_room(seed=6, n_views=5, w=120, h=90, f=140.0, arc_deg=30.0, n_patches=30, per_view_sparse=10)
+    return [np.ascontiguousarray(v.rgb) for v in sc.views]
+
+
+def _sfm_backends():
+    from oracle import oracle
+    from rustcolmap_b200 import colmap, sift
+
+    def extract(im, name):
+        g, rgb = colmap.gray_rgb(im)
+        pts, desc, col, nraw = oracle.extract_sift(g, rgb)
+        return sift.SiftFrame(name, im.shape[1], im.shape[0], pts, desc, col, nraw)
+
+    def match(descs, prs):
+        return [oracle.match_pair(descs[i], descs[j], 0.75) for i, j in prs]
+    return extract, match
+
+
+def _sfm_rank(rank, world, out, sequential):
+    extract, match = _sfm_backends()
+    frames, pairs, matches = shard.extract_and_match_sharded(_sfm_images(), sequential=sequential,
+                                                             extract=extract, match=match)
+    np.savez(os.path.join(out, f"r{rank}.npz"), pairs=np.array(pairs),
+             **{f"p{i}": f.pts for i, f in enumerate(frames)}, **{f"d{i}": f.desc for i, f in enumerate(frames)},
+             **{f"c{i}": f.colors for i, f in enumerate(frames)},
+             **{f"a{p}": a for p, (a, _) in enumerate(matches)}, **{f"b{p}": b for p, (_, b) in enumerate(matches)})
+
+
+@pytest.mark.parametrize("world,sequential", [(2, False), (3, True)])
+def test_sfm_front_end_sharded_equals_single_process(world, sequential):
+    from rustcolmap_b200 import sift
+    extract, match = _sfm_backends()
+    imgs = _sfm_images()
+    frames = [extract(im, "") for im in imgs]
+    pairs = sift.job_pairs(len(imgs), sequential)
+    ref = match([f.desc for f in frames], pairs)
+    assert sum(len(a) for a, _ in ref) > 0
+    out = _run_ranks(_sfm_rank, world, sequential)
+    for r in range(world):
+        got = dict(np.load(os.path.join(out, f"r{r}.npz")))
+        assert [tuple(p) for p in got["pairs"]] == pairs
+        for i, f in enumerate(frames):
+            assert np.array_equal(got[f"p{i}"], f.pts) and np.array_equal(got[f"c{i}"], f.colors)
+            assert np.array_equal(got[f"d{i}"].view(np.uint32), f.desc.view(np.uint32))
+        for p, (a, b) in enumerate(ref):
+            assert np.array_equal(got[f"a{p}"], a) and np.array_equal(got[f"b{p}"], b)
