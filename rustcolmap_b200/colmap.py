@@ -14,13 +14,13 @@ Restates, for this path:
 Images: the reference decodes with the `image` crate (any format), resizes
 with its Triangle filter when the long side exceeds `max_dim`, and converts
 with `to_luma8` / `to_rgb8`.  Here PNG is decoded by a small decoder (8-bit
-grey, grey+alpha, RGB, RGBA; every filter type; other formats raise an
-error).  A view whose working size differs from its camera's is resized on
-the GPU (rcmvs_resize_view: the `image` 0.24 Triangle resampler in f32, in
-the crate's order of operations).  RGB -> luma follows the `image`
-0.24 conversion, (2126 R + 7152 G + 722 B) / 10000 in integers; for grey
-input it is the identity.  Neither is pinned by reference outputs (the crate
-is not vendored).
+grey, grey+alpha, RGB, RGBA; every filter type) and other formats (JPEG,
+...) by Pillow (read_image).  A view whose working size differs from its
+camera's is resized on the GPU (rcmvs_resize_view: the `image` 0.24
+Triangle resampler in f32, in the crate's order of operations).  RGB ->
+luma follows the `image` 0.24 conversion, (2126 R + 7152 G + 722 B) / 10000
+in integers; for grey input it is the identity.  Neither is pinned by
+reference outputs (the crate is not vendored).
 """
 import math
 import os
@@ -402,6 +402,32 @@ def read_png(path):
     return out.reshape(h, w, chans)
 
 
+def read_image(path):
+    """Decoded 8-bit image (h, w, channels).  PNG goes through read_png (the
+    pixels the reference's decoder gives); other formats (JPEG, BMP, TIFF,
+    ...) through Pillow, whose JPEG inverse DCT is not the `image` crate's,
+    so lossy images may differ from the reference's by a grey level in
+    places.  Palette, 16-bit and other modes are converted to RGB."""
+    with open(path, "rb") as f:
+        sig = f.read(8)
+    if sig == b"\x89PNG\r\n\x1a\n":
+        return read_png(path)
+    try:
+        from PIL import Image
+    except ImportError:
+        raise RcmvsError(-5, f"{path}: not a PNG and Pillow is not installed to decode it")
+    try:
+        with Image.open(path) as im:
+            mode = im.mode
+            if mode not in ("L", "LA", "RGB", "RGBA"):
+                im = im.convert("RGB")
+                mode = "RGB"
+            a = np.asarray(im, dtype=np.uint8)
+    except OSError as e:
+        raise RcmvsError(-5, f"cannot decode {path}: {e}")
+    return np.ascontiguousarray(a.reshape(a.shape[0], a.shape[1], -1))
+
+
 def gray_rgb(img):
     """`to_luma8` / `to_rgb8` of a decoded image: grey as is, RGB -> luma
     (2126 R + 7152 G + 722 B) / 10000 (integer), alpha dropped."""
@@ -430,7 +456,7 @@ def load_views(rec, image_dir, opts=None, ctx=None):
         cam = cam_from_rec(c, mw / c.width, mh / c.height)
         path = os.path.join(image_dir, im.name)
         try:
-            img = read_png(path)
+            img = read_image(path)
         except OSError as e:
             raise RcmvsError(-5, f"cannot open {path}: {e}")
         if (mw, mh) != (c.width, c.height):  # lib.rs:188-190

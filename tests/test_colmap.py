@@ -291,3 +291,44 @@ def test_load_views_resizes_above_max_dim(tmp_path):
                                        opts, ctx=ctx)
     ctx.close()
     assert st.views == len(sc.views) and st.views_with_depth > 0
+
+
+def test_read_image_formats(tmp_path):
+    """PNG through the in-repo decoder, JPEG and BMP through Pillow; modes
+    without a direct counterpart come back as RGB."""
+    from PIL import Image
+    rng = np.random.default_rng(8)
+    rgb = rng.integers(0, 256, (21, 34, 3), dtype=np.uint8)
+    grey = rgb[:, :, 0].copy()
+    Image.fromarray(rgb).save(tmp_path / "a.png")
+    Image.fromarray(rgb).save(tmp_path / "a.bmp")
+    Image.fromarray(rgb).save(tmp_path / "a.jpg", quality=95)
+    Image.fromarray(grey).save(tmp_path / "g.jpg", quality=95)
+    Image.fromarray(rgb).convert("P").save(tmp_path / "p.bmp")
+    assert np.array_equal(colmap.read_image(str(tmp_path / "a.png")), rgb)
+    assert np.array_equal(colmap.read_image(str(tmp_path / "a.bmp")), rgb)
+    j = colmap.read_image(str(tmp_path / "a.jpg"))
+    assert j.shape == rgb.shape and np.array_equal(j, np.asarray(Image.open(tmp_path / "a.jpg")))
+    g = colmap.read_image(str(tmp_path / "g.jpg"))
+    assert g.shape == (21, 34, 1)
+    p = colmap.read_image(str(tmp_path / "p.bmp"))
+    assert p.shape == (21, 34, 3)
+    (tmp_path / "bad.jpg").write_bytes(b"not an image")
+    with pytest.raises(RcmvsError):
+        colmap.read_image(str(tmp_path / "bad.jpg"))
+
+
+def test_load_views_from_jpeg_model(tmp_path):
+    from PIL import Image
+    sc = _tiny()
+    write_scene_model(sc, str(tmp_path / "sparse"), str(tmp_path / "images"))
+    rec = colmap.read_dir_any(str(tmp_path / "sparse"))
+    for im in rec.images:  # the same model with JPEG files
+        v = sc.views[im.image_id - 100]
+        name = os.path.splitext(im.name)[0] + ".jpg"
+        Image.fromarray(np.ascontiguousarray(v.rgb)).save(tmp_path / "images" / name, quality=98)
+        im.name = name
+    views, _ = colmap.load_views(rec, str(tmp_path / "images"), MvsOptions(max_dim=4096))
+    for a, b in zip(views, sc.views):
+        assert (a.w, a.h) == (b.w, b.h)
+        assert np.abs(a.rgb.astype(int) - np.asarray(b.rgb, int)).mean() < 4.0  # lossy, but close
