@@ -479,12 +479,14 @@ def load_views(rec, image_dir, opts=None, ctx=None):
 
 
 def run_mvs_colmap(sparse_dir, image_dir, out_dir, opts=None, ctx=None, net=None, log=None):
-    """mvs::run_mvs (mvs/src/lib.rs:294-300) from a COLMAP model directory
-    and its images: load_views, stereo, fusion, and the files under
-    <out_dir>/dense.  Returns (MvsStats, xyz, rgb)."""
+    """mvs::run_mvs (mvs/src/lib.rs:294-300) from a COLMAP model (a model
+    directory or a Reconstruction, as the reference takes) and its images:
+    load_views, stereo, fusion, and the files under <out_dir>/dense.
+    Returns (MvsStats, xyz, rgb)."""
     from . import mvs
     opts = opts or MvsOptions()
-    views, sparse = load_views(read_dir_any(sparse_dir), image_dir, opts, ctx)
+    rec = sparse_dir if isinstance(sparse_dir, Reconstruction) else read_dir_any(sparse_dir)
+    views, sparse = load_views(rec, image_dir, opts, ctx)
     if log:
         log(f"mvs: loaded {len(views)} views at working resolution (max_dim {opts.max_dim})")
     return mvs.run_mvs(views, sparse, opts, out_dir=out_dir, ctx=ctx, log=log, net=net)

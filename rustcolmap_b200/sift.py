@@ -119,3 +119,30 @@ def extract_and_match(images, names=None, opts=None, ratio=0.75, sequential=Fals
     frames = [extract_sift(im, nm, opts, ctx) for im, nm in zip(images, names)]
     pairs = job_pairs(len(frames), sequential)
     return frames, pairs, match_pairs([f.desc for f in frames], pairs, ratio, ctx)
+
+
+IMAGE_EXTENSIONS = ("jpg", "jpeg", "png", "bmp", "tif", "tiff", "webp")  # sfm-lite/src/lib.rs:83-91
+
+
+def image_files(images_dir):
+    """The images sfm-lite's run_sfm_dir takes (sfm-lite/src/lib.rs:119-126):
+    regular files with an image extension (case-insensitive), sorted by
+    path."""
+    import os
+    out = []
+    for e in os.listdir(images_dir):
+        p = os.path.join(images_dir, e)
+        ext = os.path.splitext(e)[1][1:].lower()
+        if os.path.isfile(p) and ext in IMAGE_EXTENSIONS:
+            out.append(p)
+    return sorted(out)
+
+
+def extract_and_match_dir(images_dir, opts=None, ratio=0.75, sequential=False, ctx=None):
+    """extract_and_match over the images of a directory, in run_sfm_dir's
+    order; frame names are the file names (sfm-lite/src/lib.rs:141-146)."""
+    import os
+    from .colmap import read_image
+    paths = image_files(images_dir)
+    return extract_and_match([read_image(p) for p in paths], [os.path.basename(p) for p in paths], opts, ratio,
+                             sequential, ctx)

@@ -280,3 +280,11 @@ def test_oracle_match_pair_matches_numpy_random():
         x = oracle.match_pair(a, b, ratio)
         y = match_numpy(a, b, ratio)
         assert np.array_equal(x[0], y[0]) and np.array_equal(x[1], y[1]), (na, nb, noise, dup, ratio)
+
+
+def test_image_files(tmp_path):
+    for n in ("b.JPG", "a.png", "c.txt", "d.webp", "e.tiff", "noext"):
+        (tmp_path / n).write_bytes(b"x")
+    (tmp_path / "dir.png").mkdir()
+    got = [p.rsplit("/", 1)[1] for p in sift.image_files(str(tmp_path))]
+    assert got == ["a.png", "b.JPG", "d.webp", "e.tiff"]
