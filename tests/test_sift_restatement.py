@@ -285,9 +285,13 @@ def extract(gray, rgb, max_features=2048, thr=0.0067):
     return pts, desc, col, len(raw)
 
 
-@pytest.mark.parametrize("which", ["blob", "view"])
+@pytest.mark.parametrize("which", ["blob", "view", "view3"])
 def test_numpy_restatement_equals_oracle(which):
-    if which == "blob":
+    if which == "view3":  # 160x120: three octaves, keypoints scaled by 2 and 4
+        v = scene.corner_room(seed=8, n_views=2, w=160, h=120, f=180.0, arc_deg=20.0, n_patches=40,
+                              per_view_sparse=10).views[0]
+        g, rgb = np.ascontiguousarray(v.gray), np.ascontiguousarray(v.rgb)
+    elif which == "blob":
         yy, xx = np.mgrid[0:72, 0:96]
         g = (30 + 200 * np.exp(-((xx - 47.5) ** 2 + (yy - 35.0) ** 2) / 50.0)
              + 40 * np.exp(-((xx - 20.0) ** 2 + (yy - 50.0) ** 2) / 8.0)).astype(np.uint8)
