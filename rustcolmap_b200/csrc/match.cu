@@ -13,15 +13,16 @@
 //                 of both tiles staged k-major in shared memory (float4 reads,
 //                 conflict-free), each distance accumulated in k order; with
 //                 --fmad=false every difference, square and sum rounds as in
-//                 the reference.  The matrix of a pair is written once and
-//                 serves both directions: (a - b)^2 and the reference's
-//                 backward (a - b)^2 are the same numbers.
-//   rows_kernel   one warp per row: each lane scans its columns in order, the
-//                 lanes' (best, index, second) merge by value with the lower
-//                 index winning ties -- the first minimum and the second
-//                 smallest value of the row, exactly what the reference's
-//                 sequential scan keeps
-//   cols_kernel   one thread per column, rows scanned in order (coalesced)
+//                 the reference.  The distances never leave the block: it
+//                 writes, for each of its rows and columns, the (best, index,
+//                 second) over the tile, merged through shuffles and shared
+//                 memory.  One distance serves both directions: (a - b)^2 and
+//                 the reference's backward (a - b)^2 are the same number.
+//   rows_kernel   one thread per row: the tiles' partials merged by value
+//   cols_kernel   with the lower index winning ties -- the first minimum and
+//                 the second smallest value, exactly what the reference's
+//                 sequential scan keeps (the merge is associative, so the
+//                 order of the tiles does not matter)
 //   decide_kernel the reference's tests per row of A
 //
 // Pairs run in chunks sized to a fixed distance-matrix budget; results come
@@ -41,11 +42,11 @@ namespace {
 constexpr int DESC_LEN = 128;
 constexpr int TILE = 64;
 constexpr int KC = 32;
-constexpr size_t D_BUDGET = size_t(1) << 30;  // bytes of distance matrices per chunk
+constexpr size_t P_BUDGET = size_t(1) << 28;  // bytes of tile partials per chunk
 
 struct PairJob {
-    int64_t a_off, b_off;  // first descriptor of each frame (in descriptors)
-    int64_t d_off;         // distance matrix (na * nb floats)
+    int64_t a_off, b_off;      // first descriptor of each frame (in descriptors)
+    int64_t prow_off, pcol_off;  // tile partials: [column tile][na] rows, [row tile][nb] columns
     int32_t na, nb;
     int32_t row_off, col_off;  // into the chunk's forward / backward results
 };
@@ -55,10 +56,33 @@ struct Nearest {
     float d1, d2;
 };
 
+// Sequential-scan state: the first minimum and the second smallest value.
+__device__ __forceinline__ void push(float s, uint32_t j, float& best, uint32_t& bi, float& second) {
+    if (s < best) {
+        second = best;
+        best = s;
+        bi = j;
+    } else if (s < second) {
+        second = s;
+    }
+}
+
+// The same state of a union of two disjoint parts: the smaller best (the
+// lower index among equal values) and the second smallest value of the union.
+__device__ __forceinline__ void merge(float& best, uint32_t& bi, float& second, float ob, uint32_t oi, float os) {
+    const float nsec = fminf(fmaxf(best, ob), fminf(second, os));
+    if (ob < best || (ob == best && oi < bi)) {
+        best = ob;
+        bi = oi;
+    }
+    second = nsec;
+}
+
 __global__ void __launch_bounds__(256) dist_kernel(const float* __restrict__ desc, const PairJob* __restrict__ jobs,
-                                                   float* __restrict__ dmat) {
+                                                   Nearest* __restrict__ rowpart, Nearest* __restrict__ colpart) {
     __shared__ __align__(16) float As[KC][TILE];
     __shared__ __align__(16) float Bs[KC][TILE];
+    __shared__ Nearest cpart[8][TILE];
     const PairJob J = jobs[blockIdx.z];
     const int r0 = blockIdx.y * TILE, c0 = blockIdx.x * TILE;
     if (r0 >= J.na || c0 >= J.nb) return;
@@ -103,65 +127,82 @@ __global__ void __launch_bounds__(256) dist_kernel(const float* __restrict__ des
         }
         __syncthreads();
     }
-    float* D = dmat + J.d_off;
+    // Rows: each of this thread's 4 rows over its 4 columns, then over the
+    // 16 threads of the row group (lanes 0-15 or 16-31 of the warp).
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
         const int ia = r0 + ty * 4 + r;
-        if (ia >= J.na) continue;
+        float best = INFINITY, second = INFINITY;
+        uint32_t bi = UINT32_MAX;
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             const int ib = c0 + tx * 4 + c;
-            if (ib < J.nb) D[(int64_t)ia * J.nb + ib] = acc[r][c];
+            if (ia < J.na && ib < J.nb) push(acc[r][c], (uint32_t)ib, best, bi, second);
         }
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1)
+            merge(best, bi, second, __shfl_xor_sync(0xffffffffu, best, o), __shfl_xor_sync(0xffffffffu, bi, o),
+                  __shfl_xor_sync(0xffffffffu, second, o));
+        if (tx == 0 && ia < J.na) rowpart[J.prow_off + (int64_t)blockIdx.x * J.na + ia] = Nearest{bi, best, second};
+    }
+    // Columns: each of this thread's 4 columns over its 4 rows, then the two
+    // row groups of the warp, then the 8 warps through shared memory.
+    const int wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const int ib = c0 + tx * 4 + c;
+        float best = INFINITY, second = INFINITY;
+        uint32_t bi = UINT32_MAX;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const int ia = r0 + ty * 4 + r;
+            if (ia < J.na && ib < J.nb) push(acc[r][c], (uint32_t)ia, best, bi, second);
+        }
+        merge(best, bi, second, __shfl_xor_sync(0xffffffffu, best, 16), __shfl_xor_sync(0xffffffffu, bi, 16),
+              __shfl_xor_sync(0xffffffffu, second, 16));
+        if ((threadIdx.x & 16) == 0) cpart[wid][tx * 4 + c] = Nearest{bi, best, second};
+    }
+    __syncthreads();
+    if (threadIdx.x < TILE) {
+        const int ib = c0 + threadIdx.x;
+        Nearest m = cpart[0][threadIdx.x];
+        for (int q = 1; q < 8; ++q) {
+            const Nearest o = cpart[q][threadIdx.x];
+            merge(m.d1, m.idx, m.d2, o.d1, o.idx, o.d2);
+        }
+        if (ib < J.nb) colpart[J.pcol_off + (int64_t)blockIdx.y * J.nb + ib] = m;
     }
 }
 
-// Sequential-scan state: the first minimum and the second smallest value.
-__device__ __forceinline__ void push(float s, uint32_t j, float& best, uint32_t& bi, float& second) {
-    if (s < best) {
-        second = best;
-        best = s;
-        bi = j;
-    } else if (s < second) {
-        second = s;
-    }
-}
-
-__global__ void __launch_bounds__(256) rows_kernel(const PairJob* __restrict__ jobs, const float* __restrict__ dmat,
+// The tiles' partials of each row (over column tiles) and of each column
+// (over row tiles), merged into the nearest and second-nearest of the row or
+// column; one thread each.
+__global__ void __launch_bounds__(256) rows_kernel(const PairJob* __restrict__ jobs, const Nearest* __restrict__ rowpart,
                                                    Nearest* __restrict__ fwd) {
     const PairJob J = jobs[blockIdx.y];
-    const int ia = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    const int ia = blockIdx.x * 256 + threadIdx.x;
     if (ia >= J.na) return;
-    const float* row = dmat + J.d_off + (int64_t)ia * J.nb;
-    float best = INFINITY, second = INFINITY;
-    uint32_t bi = UINT32_MAX;
-    for (int ib = lane; ib < J.nb; ib += 32) push(row[ib], (uint32_t)ib, best, bi, second);
-    for (int o = 16; o > 0; o >>= 1) {
-        const float ob = __shfl_down_sync(0xffffffffu, best, o);
-        const float os = __shfl_down_sync(0xffffffffu, second, o);
-        const uint32_t oi = __shfl_down_sync(0xffffffffu, bi, o);
-        // two smallest of the union; ties of the minimum go to the lower index
-        const float nsec = fminf(fmaxf(best, ob), fminf(second, os));
-        if (ob < best || (ob == best && oi < bi)) {
-            best = ob;
-            bi = oi;
-        }
-        second = nsec;
+    const int nct = (J.nb + TILE - 1) / TILE;
+    Nearest m{UINT32_MAX, INFINITY, INFINITY};
+    for (int t = 0; t < nct; ++t) {
+        const Nearest o = rowpart[J.prow_off + (int64_t)t * J.na + ia];
+        merge(m.d1, m.idx, m.d2, o.d1, o.idx, o.d2);
     }
-    if (lane == 0) fwd[J.row_off + ia] = Nearest{bi, best, second};
+    fwd[J.row_off + ia] = m;
 }
 
-__global__ void __launch_bounds__(256) cols_kernel(const PairJob* __restrict__ jobs, const float* __restrict__ dmat,
+__global__ void __launch_bounds__(256) cols_kernel(const PairJob* __restrict__ jobs, const Nearest* __restrict__ colpart,
                                                    Nearest* __restrict__ bwd) {
     const PairJob J = jobs[blockIdx.y];
     const int ib = blockIdx.x * 256 + threadIdx.x;
     if (ib >= J.nb) return;
-    const float* col = dmat + J.d_off + ib;
-    float best = INFINITY, second = INFINITY;
-    uint32_t bi = UINT32_MAX;
-#pragma unroll 8
-    for (int ia = 0; ia < J.na; ++ia) push(col[(int64_t)ia * J.nb], (uint32_t)ia, best, bi, second);
-    bwd[J.col_off + ib] = Nearest{bi, best, second};
+    const int nrt = (J.na + TILE - 1) / TILE;
+    Nearest m{UINT32_MAX, INFINITY, INFINITY};
+    for (int t = 0; t < nrt; ++t) {
+        const Nearest o = colpart[J.pcol_off + (int64_t)t * J.nb + ib];
+        merge(m.d1, m.idx, m.d2, o.d1, o.idx, o.d2);
+    }
+    bwd[J.col_off + ib] = m;
 }
 
 // matching.rs:74-94
@@ -193,7 +234,7 @@ int mfail(rcmvs_ctx* ctx, int code, const std::string& msg) {
     } while (0)
 
 // Context arena slots 160-167.
-enum { M_DESC = 160, M_JOBS, M_DMAT, M_FWD, M_BWD, M_MB };
+enum { M_DESC = 160, M_JOBS, M_ROWP, M_FWD, M_BWD, M_MB, M_COLP };
 
 }  // namespace
 }  // namespace rcmvs
@@ -254,15 +295,16 @@ static int match_pairs_impl(rcmvs_ctx* ctx, const float* const* desc, const int3
     while (p < n_pairs) {
         // a chunk of pairs whose distance matrices fit the budget (at least one)
         std::vector<PairJob> jobs;
-        int64_t d = 0, rows = 0, cols = 0;
+        int64_t prow = 0, pcol = 0, rows = 0, cols = 0;
         int max_na = 0, max_nb = 0;
         while (p < n_pairs && jobs.size() < 65535) {
             const int fa = pairs[2 * p], fb = pairs[2 * p + 1];
             const int na = n_desc[fa], nb = n_desc[fb];
-            const int64_t cells = (int64_t)na * nb;
-            if (!jobs.empty() && (size_t)(d + cells) * sizeof(float) > D_BUDGET) break;
-            jobs.push_back(PairJob{foff[fa], foff[fb], d, na, nb, (int32_t)rows, (int32_t)cols});
-            d += cells;
+            const int64_t pr = (int64_t)((nb + TILE - 1) / TILE) * na, pc = (int64_t)((na + TILE - 1) / TILE) * nb;
+            if (!jobs.empty() && (size_t)(prow + pr + pcol + pc) * sizeof(Nearest) > P_BUDGET) break;
+            jobs.push_back(PairJob{foff[fa], foff[fb], prow, pcol, na, nb, (int32_t)rows, (int32_t)cols});
+            prow += pr;
+            pcol += pc;
             rows += na;
             cols += nb;
             max_na = std::max(max_na, na);
@@ -272,9 +314,10 @@ static int match_pairs_impl(rcmvs_ctx* ctx, const float* const* desc, const int3
         }
         const int first = p - (int)jobs.size();
         if (max_na > 0 && max_nb > 0) {
-            void *p_jobs, *p_dmat, *p_fwd, *p_bwd, *p_mb;
+            void *p_jobs, *p_rowp, *p_colp, *p_fwd, *p_bwd, *p_mb;
             MCK(A.get(M_JOBS, sizeof(PairJob) * jobs.size(), &p_jobs));
-            MCK(A.get(M_DMAT, sizeof(float) * (size_t)std::max<int64_t>(d, 1), &p_dmat));
+            MCK(A.get(M_ROWP, sizeof(Nearest) * (size_t)std::max<int64_t>(prow, 1), &p_rowp));
+            MCK(A.get(M_COLP, sizeof(Nearest) * (size_t)std::max<int64_t>(pcol, 1), &p_colp));
             MCK(A.get(M_FWD, sizeof(Nearest) * (size_t)rows, &p_fwd));
             MCK(A.get(M_BWD, sizeof(Nearest) * (size_t)cols, &p_bwd));
             MCK(A.get(M_MB, sizeof(uint32_t) * (size_t)rows, &p_mb));
@@ -283,15 +326,15 @@ static int match_pairs_impl(rcmvs_ctx* ctx, const float* const* desc, const int3
             const SpanHook& hook = ctx->hook();
             hook.begin("match_dist");
             dist_kernel<<<dim3((max_nb + TILE - 1) / TILE, (max_na + TILE - 1) / TILE, nj), 256, 0, st>>>(
-                (const float*)p_desc, (const PairJob*)p_jobs, (float*)p_dmat);
+                (const float*)p_desc, (const PairJob*)p_jobs, (Nearest*)p_rowp, (Nearest*)p_colp);
             MCK(cudaGetLastError());
             hook.end("match_dist");
             hook.begin("match_select");
-            rows_kernel<<<dim3((max_na + 7) / 8, nj), 256, 0, st>>>((const PairJob*)p_jobs, (const float*)p_dmat,
-                                                                   (Nearest*)p_fwd);
+            rows_kernel<<<dim3((max_na + 255) / 256, nj), 256, 0, st>>>((const PairJob*)p_jobs,
+                                                                       (const Nearest*)p_rowp, (Nearest*)p_fwd);
             MCK(cudaGetLastError());
-            cols_kernel<<<dim3((max_nb + 255) / 256, nj), 256, 0, st>>>((const PairJob*)p_jobs, (const float*)p_dmat,
-                                                                       (Nearest*)p_bwd);
+            cols_kernel<<<dim3((max_nb + 255) / 256, nj), 256, 0, st>>>((const PairJob*)p_jobs,
+                                                                       (const Nearest*)p_colp, (Nearest*)p_bwd);
             MCK(cudaGetLastError());
             decide_kernel<<<dim3((max_na + 255) / 256, nj), 256, 0, st>>>(
                 (const PairJob*)p_jobs, (const Nearest*)p_fwd, (const Nearest*)p_bwd, r32, (uint32_t*)p_mb);
