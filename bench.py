@@ -73,11 +73,14 @@ def configs():
     }
 
 
-def make_jobs(cfg, sc, opts):
+def make_jobs(cfg, sc, opts, planner=None):
     """(ref, sources, zmin, zmax) per view with sources; with k_range each
-    view keeps the first K ~ U{lo..hi} (seeded) of its planned sources."""
-    from rustcolmap_b200 import mvs
-    srcs, zr, fus = mvs.plan(sc.sparse, sc.views, opts)
+    view keeps the first K ~ U{lo..hi} (seeded) of its planned sources.
+    planner: the plan glue to use (default the library's rcmvs_plan)."""
+    if planner is None:
+        from rustcolmap_b200 import mvs
+        planner = mvs.plan
+    srcs, zr, fus = planner(sc.sparse, sc.views, opts)
     if "k_range" in cfg:
         rng = np.random.default_rng(3)
         lo, hi = cfg["k_range"]
@@ -200,10 +203,17 @@ def pinned_views(views):
     return out
 
 
+def cpu_rows(args):
+    """Rows of the CPU band: --cpu-rows, else two per host thread (the
+    oracle threads over rows, so every thread gets work)."""
+    return args.cpu_rows or 2 * (os.cpu_count() or 1)
+
+
 def cpu_baseline(sc, opts, jobs, rows, threads=0):
     """Times the oracle's estimate_depth on a band of `rows` rows of the first
-    job's reference view (a bounded sample of one view).  Returns (depth
-    maps/s, seconds, sample description, threads)."""
+    job's reference view (a bounded sample of one view; stereo only, the
+    fusion is not part of the sample).  Returns (depth maps/s, seconds,
+    sample description, threads)."""
     import copy
 
     from oracle import oracle
@@ -222,35 +232,44 @@ def cpu_baseline(sc, opts, jobs, rows, threads=0):
     dt = time.perf_counter() - t0
     frac = band.h / v.h
     desc = (f"oracle estimate_depth on a {v.w}x{band.h} band (rows {y0}-{y0 + band.h}) of one "
-            f"{v.w}x{v.h} view, K={len(srcs)}, {opts.num_hyp} hyps, {2 * opts.sweeps} passes; "
-            f"{frac:.4f} of a depth map per sample, stereo only")
+            f"{v.w}x{v.h} view, K={len(srcs)}, {opts.num_hyp} hyps, {2 * opts.sweeps} passes, {nt} threads; "
+            f"{frac:.4f} of a depth map per sample; stereo only (fusion not sampled)")
     return frac / dt, dt, desc, nt
 
 
 def run_reference(args, cfg):
+    """The reference algorithm's CPU implementation (the oracle port) on the
+    host cores, rank 0 only.  Loads no library of the product: the scene is
+    rendered by the host-only build of the renderer (oracle/libscene_host.so)
+    and planned by the oracle's plan glue."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     from oracle import oracle
-    from rustcolmap_b200 import mvs
+    from rustcolmap_b200 import scene
     oracle.lib()
-    sc = make_scene(cfg, seed=5, device=-1 if not _has_gpu() else 0)
+    scene.use_host_renderer(os.path.join(ROOT, "oracle", "libscene_host.so"))
+    t_setup = time.perf_counter()
+    sc = make_scene(cfg, seed=5, device=-1)
     opts = cfg["opts"]
-    jobs, fus = make_jobs(cfg, sc, opts)
-    rows = args.ref_rows
+    jobs, fus = make_jobs(cfg, sc, opts, planner=oracle.plan)
+    setup_s = time.perf_counter() - t_setup
+    rows = cpu_rows(args)
     for _ in range(args.warmup):
         cpu_baseline(sc, opts, jobs, rows)
     times, rate, desc, nt = [], 0.0, "", 0
     for _ in range(args.steps):
         r, dt, desc, nt = cpu_baseline(sc, opts, jobs, rows)
         times.append(dt)
-    frac = rows / sc.views[jobs[0][0]].h
+    frac = min(rows, sc.views[jobs[0][0]].h) / sc.views[jobs[0][0]].h
     rate = frac * len(times) / sum(times)
     line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": "depth maps/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", "config": {"workload": args.config + ": " + cfg["desc"]},
+            "data": "synthetic", "config": {"workload": args.config + ": " + cfg["desc"], "setup_s": setup_s,
+                                            "inputs": "scene rendered on the host (oracle/libscene_host.so), "
+                                                      "plan by the oracle (orc_plan)"},
             "cpu_baseline": {"value": rate, "unit": "depth maps/s", "cores": nt, "kind": "port",
                              "sample": desc},
             "e2e": {"value": rate, "unit": "depth maps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -330,7 +349,9 @@ def run_sfm(args):
     if args.impl == "reference":
         if rank != 0:
             return
-        imgs = sfm_images(0 if _has_gpu() else -1)
+        from rustcolmap_b200 import scene
+        scene.use_host_renderer(os.path.join(ROOT, "oracle", "libscene_host.so"))
+        imgs = sfm_images(-1)
         for _ in range(args.warmup):
             sfm_cpu(imgs, 2, 4)
         vals = [sfm_cpu(imgs, 16, 48) for _ in range(args.steps)]
@@ -422,8 +443,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c5", choices=["c5", "c3", "c2", "c1", "sfm"])
-    ap.add_argument("--cpu-rows", type=int, default=24, help="rows of the CPU-baseline band")
-    ap.add_argument("--ref-rows", type=int, default=12, help="rows per step of the reference arm")
+    ap.add_argument("--cpu-rows", type=int, default=0,
+                    help="rows of the CPU band (cpu_baseline and --impl reference; default 2 per host thread)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--views", type=int, default=0, help="override the number of views (profiling runs)")
@@ -593,7 +614,7 @@ def main():
 
     cpu = None
     if not args.no_cpu_baseline and rank == 0 and ws == 1:
-        rate, dt, desc, nt = cpu_baseline(sc, opts, jobs, args.cpu_rows)
+        rate, dt, desc, nt = cpu_baseline(sc, opts, jobs, cpu_rows(args))
         cpu = {"value": rate, "unit": "depth maps/s", "cores": nt, "kind": "port", "sample": desc, "seconds": dt}
 
     if rank == 0:

@@ -99,6 +99,19 @@ typedef struct rcmvs_options {
  * (rcmvs_last_work), which with this flag count the reference's calls. */
 #define RCMVS_FLAG_NO_SKIP_DUPLICATES 16u
 
+/* Diagnostic: run the init (plane sweep, or the learned init) and the gate
+ * only, without the Jacobi passes, so the init's planes and costs can be
+ * compared on their own.  Not a reference schedule. */
+#define RCMVS_FLAG_INIT_ONLY 32u
+
+/* Learned init only (rcmvs_scene_estimate_depth_learned / _seeded,
+ * rcmvs_run_mvs_learned): a pixel seeded by a proposal also runs the
+ * plane sweep, starting from the proposal's cost as its best so far (the
+ * sweep's early-abort hint is then tight from the first hypothesis), and
+ * keeps a sweep plane only when it is strictly cheaper.  Without it a seeded
+ * pixel skips the sweep. */
+#define RCMVS_FLAG_SEED_AND_SWEEP 64u
+
 /* Fills `MvsOptions::default()` (mvs/src/lib.rs:56-70); extensions off. */
 void rcmvs_options_default(rcmvs_options* opts);
 
@@ -494,6 +507,17 @@ int rcmvs_scene_estimate_depth_learned(rcmvs_ctx* ctx, rcmvs_scene* scene, const
                                        float conf_thr, int32_t n_local, float span,
                                        uint64_t* learned_pixels);
 
+/* rcmvs_scene_estimate_depth_learned with caller-given proposals in place of
+ * the network's: pred holds, for each job in order, its reference view's
+ * (w/4)*(h/4) quarter cells of 16 f32 (t, normal xyz, confidence logit, 11
+ * unused; the layout rcmvs_net_forward writes), jobs back to back;
+ * pred_on_device != 0 when pred is device memory.  A cell's confidence is
+ * sigmoid(logit), tested as logit >= ln(conf_thr / (1 - conf_thr)). */
+int rcmvs_scene_estimate_depth_seeded(rcmvs_ctx* ctx, rcmvs_scene* scene, const rcmvs_job* jobs,
+                                      int32_t n_jobs, const rcmvs_options* opts, const float* pred,
+                                      int32_t pred_on_device, float conf_thr, int32_t n_local,
+                                      float span, uint64_t* learned_pixels);
+
 /* rcmvs_run_mvs with stereo seeded by the network (arguments as
  * rcmvs_scene_estimate_depth_learned; opts->sweeps sweeps after the init). */
 int rcmvs_run_mvs_learned(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views,
@@ -520,9 +544,15 @@ int rcmvs_run_mvs_learned(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_vie
  *     RCMVS_NOALLOC_MAX_SOURCES sources, else RCMVS_E_LIMIT; bad arguments
  *     give RCMVS_E_ARG, a failed CUDA call RCMVS_E_CUDA (no message: there
  *     is no context).
- *   - The first call on a device looks up the array's device address
- *     (cudaGetSymbolAddress, once per device); make that first call before
- *     any stream capture.
+ *   - Every call looks up the array's device address on the current device
+ *     (cudaGetSymbolAddress, which allocates nothing); the first lookup on
+ *     a device loads the library's module there, so make the first call on
+ *     a device before any stream capture.
+ *   - opts->flags may hold RCMVS_FLAG_ONE_CANDIDATE, RCMVS_FLAG_INIT_ONLY,
+ *     RCMVS_FLAG_NO_SKIP_DUPLICATES (this entry point never skips) and
+ *     RCMVS_FLAG_SEED_AND_SWEEP (no effect here); the scheduling flags
+ *     (PERSISTENT, CUDA_GRAPH, AUTOTUNE) give RCMVS_E_ARG.  The tile is
+ *     tile_w x tile_h, default 8x8, as for rcmvs_estimate_depth.
  *   - All calls on a device share the array and leave its contents behind;
  *     calls whose GPU work overlaps (different streams or threads) race on
  *     it and must be serialised by the caller. */

@@ -402,11 +402,109 @@ int orc_plane_cost_field(const rcmvs_view* views, int32_t n_views, int32_t ref_i
     return RCMVS_OK;
 }
 
-// mvs/src/stereo.rs:234-394  estimate_depth
-int orc_estimate_depth(const rcmvs_view* views, int32_t n_views, int32_t ref_idx,
-                       const int32_t* srcs, int32_t n_src, double zmin, double zmax,
-                       const rcmvs_options* opts, float* depth_out, float* cost_out,
-                       float* normal_out, int32_t nthreads, uint64_t* work_out) {
+}  // extern "C"
+
+namespace {
+
+// Learned-proposal seeding of the init (no reference counterpart): the
+// quarter-resolution predictions of the reference view (wq*hq cells of 16
+// f32: t, normal xyz, confidence logit, ...) and the selection parameters.
+struct Seed {
+    const float* pred;
+    float logit_thr;  // confident iff logit >= logit_thr
+    int32_t n_local;
+    float span;
+    bool sweep_seeded;  // a seeded pixel also runs the sweep (RCMVS_FLAG_SEED_AND_SWEEP)
+    uint64_t seeded = 0;
+};
+
+// Plane-sweep init of one pixel (stereo.rs:247-269).  `start` (nullable) is
+// a plane already scored for the pixel: the sweep then begins with its cost
+// as the best so far and keeps it unless a hypothesis is strictly cheaper.
+Plane sweep_init(const RefWorkspace& ws, int32_t x, int32_t y, int32_t nh, float inv_min, float inv_max, Work* wk,
+                 const Plane* start = nullptr) {
+    float best_c = start ? start->cost : INFINITY;
+    float best_d = 0.f;
+    bool improved = false;
+    for (int32_t hi = 0; hi < nh; ++hi) {
+        float inv = inv_min + (inv_max - inv_min) * (float)hi / (float)(nh - 1);
+        float d = 1.0f / inv;
+        float c = plane_cost(ws, x, y, 0.0f, 0.0f, 1.0f, d, best_c + 0.02f, wk, nullptr);
+        if (c < best_c) {
+            best_c = c;
+            best_d = d;
+            improved = true;
+        }
+    }
+    if (start && !improved) return *start;
+    return Plane{0.0f, 0.0f, 1.0f, best_d, std::fmin(best_c, 1.0f)};
+}
+
+// Learned init of one pixel, as the library's init_learned_rows_kernel
+// computes it: the pixel's quarter cell (min(x/4, wq-1), min(y/4, hq-1))
+// proposes a plane when its logit >= logit_thr and its normal is not
+// degenerate; the predicted inverse depth t (a fraction of [1/zmax, 1/zmin])
+// is placed on the ray of the cell's anchor pixel (4qx+1, 4qy+1), so every
+// pixel of the cell gets the same plane (n, d).  n_local planes spread over
+// +-span/2 around t are scored with plane_cost and the sweep's hint rule;
+// one that fails the stereo gates (n.ray >= 0.1 at the pixel and the anchor,
+// positive inverse depth, depth in [zmin/2, 2 zmax]) is skipped.  A pixel
+// without a usable proposal runs the plane sweep.  Returns whether the
+// pixel was seeded.  With sweep_seeded a seeded pixel then runs the sweep
+// from its proposal's cost (the GPU's phase 2 does the same).
+bool learned_init(const RefWorkspace& ws, const Seed& sd, int32_t x, int32_t y, int32_t nh, float inv_min,
+                  float inv_max, Work* wk, Plane* out) {
+    const int32_t w = ws.w, h = ws.h;
+    const int32_t wq = w >> 2, hq = h >> 2;
+    const size_t i = (size_t)y * w + x;
+    const float zlo = ws.zmin * 0.5f, zhi = ws.zmax * 2.0f;
+    const float span_inv = inv_max - inv_min;
+    if (wq > 0 && hq > 0) {
+        const int32_t qx = std::min(x >> 2, wq - 1), qy = std::min(y >> 2, hq - 1);
+        const float* o = sd.pred + ((size_t)qy * wq + qx) * 16;
+        const float len = std::sqrt(o[1] * o[1] + o[2] * o[2] + o[3] * o[3]);
+        if (o[4] >= sd.logit_thr && len > 1e-6f) {
+            const float pnx = o[1] / len, pny = o[2] / len, pnz = o[3] / len;
+            const float pa = pnx * ws.rx[i] + pny * ws.ry[i] + pnz;
+            const size_t ia = (size_t)(4 * qy + 1) * w + (4 * qx + 1);
+            const float pac = pnx * ws.rx[ia] + pny * ws.ry[ia] + pnz;
+            if (pa >= 0.1f && pac >= 0.1f) {
+                const float t0 = o[0];
+                float best_c = INFINITY;
+                Plane best{0.0f, 0.0f, 1.0f, 0.0f, 0.0f};
+                bool any = false;
+                for (int32_t k = 0; k < sd.n_local; ++k) {
+                    const float tk = t0 + sd.span * ((float)k / (float)std::max(sd.n_local - 1, 1) - 0.5f);
+                    const float inv = inv_min + tk * span_inv;
+                    if (!(inv > 0.f)) continue;
+                    const float z = 1.0f / inv;   // depth on the anchor ray
+                    const float dcell = z * pac;  // the cell's plane offset
+                    const float zi = dcell / pa;  // depth on this pixel's ray
+                    if (!(zi >= zlo && zi <= zhi)) continue;
+                    any = true;
+                    const float c = plane_cost(ws, x, y, pnx, pny, pnz, dcell, best_c + 0.02f, wk, nullptr);
+                    if (c < best_c) {
+                        best_c = c;
+                        best = Plane{pnx, pny, pnz, zi, 0.0f};
+                    }
+                }
+                if (any) {
+                    best.cost = std::fmin(best_c, 1.0f);
+                    *out = sd.sweep_seeded ? sweep_init(ws, x, y, nh, inv_min, inv_max, wk, &best) : best;
+                    return true;
+                }
+            }
+        }
+    }
+    *out = sweep_init(ws, x, y, nh, inv_min, inv_max, wk);
+    return false;
+}
+
+// stereo::estimate_depth, with the init optionally seeded (sd != nullptr)
+// and the passes optionally left out (RCMVS_FLAG_INIT_ONLY).
+int estimate_impl(const rcmvs_view* views, int32_t n_views, int32_t ref_idx, const int32_t* srcs, int32_t n_src,
+                  double zmin, double zmax, const rcmvs_options* opts, float* depth_out, float* cost_out,
+                  float* normal_out, int32_t nthreads, uint64_t* work_out, Seed* sd) {
     if (!check_views(views, n_views, ref_idx, srcs, n_src) || !opts || !depth_out || !cost_out)
         return RCMVS_E_ARG;
     std::vector<int> needed{ref_idx};
@@ -426,26 +524,22 @@ int orc_estimate_depth(const rcmvs_view* views, int32_t n_views, int32_t ref_idx
     const float inv_max = 1.0f / ws.zmin;
     const int32_t nh = (int32_t)std::max<uint32_t>(opts->num_hyp, 2u);
     std::vector<Plane> prev(npx);
+    std::vector<uint64_t> seeded(nt, 0);
     par_for(h, nt, [&](int64_t y, int t) {
         for (int32_t x = 0; x < w; ++x) {
-            float best_c = INFINITY;
-            float best_d = 0.f;
-            for (int32_t hi = 0; hi < nh; ++hi) {
-                float inv = inv_min + (inv_max - inv_min) * (float)hi / (float)(nh - 1);
-                float d = 1.0f / inv;
-                float c = plane_cost(ws, x, (int32_t)y, 0.0f, 0.0f, 1.0f, d, best_c + 0.02f, &work[t],
-                                     nullptr);
-                if (c < best_c) {
-                    best_c = c;
-                    best_d = d;
-                }
-            }
-            prev[(size_t)y * w + x] = Plane{0.0f, 0.0f, 1.0f, best_d, std::fmin(best_c, 1.0f)};
+            Plane& p = prev[(size_t)y * w + x];
+            if (sd)
+                seeded[t] += learned_init(ws, *sd, x, (int32_t)y, nh, inv_min, inv_max, &work[t], &p);
+            else
+                p = sweep_init(ws, x, (int32_t)y, nh, inv_min, inv_max, &work[t]);
         }
     });
+    if (sd)
+        for (uint64_t c : seeded) sd->seeded += c;
 
-    // ---- double-buffered passes (stereo.rs:271-371)
-    const uint64_t n_passes = (uint64_t)std::max<uint32_t>(opts->sweeps, 1u) * 2;
+    // ---- double-buffered passes (stereo.rs:271-371); none with RCMVS_FLAG_INIT_ONLY
+    const uint64_t n_passes =
+        (opts->flags & RCMVS_FLAG_INIT_ONLY) ? 0 : (uint64_t)std::max<uint32_t>(opts->sweeps, 1u) * 2;
     std::vector<Plane> next = prev;
     const float zlo = ws.zmin * 0.5f, zhi = ws.zmax * 2.0f;
     for (uint64_t pass = 0; pass < n_passes; ++pass) {
@@ -547,6 +641,42 @@ int orc_estimate_depth(const rcmvs_view* views, int32_t n_views, int32_t ref_idx
         }
     }
     return RCMVS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+// mvs/src/stereo.rs:234-394  estimate_depth
+int orc_estimate_depth(const rcmvs_view* views, int32_t n_views, int32_t ref_idx,
+                       const int32_t* srcs, int32_t n_src, double zmin, double zmax,
+                       const rcmvs_options* opts, float* depth_out, float* cost_out,
+                       float* normal_out, int32_t nthreads, uint64_t* work_out) {
+    return estimate_impl(views, n_views, ref_idx, srcs, n_src, zmin, zmax, opts, depth_out, cost_out, normal_out,
+                         nthreads, work_out, nullptr);
+}
+
+int orc_estimate_depth_seeded(const rcmvs_view* views, int32_t n_views, int32_t ref_idx,
+                              const int32_t* srcs, int32_t n_src, double zmin, double zmax,
+                              const rcmvs_options* opts, const float* pred, float conf_thr,
+                              int32_t n_local, float span, float* depth_out, float* cost_out,
+                              float* normal_out, int32_t nthreads, uint64_t* seeded_out) {
+    if (!pred || n_local < 1 || n_local > 256 || !(span >= 0.f && span <= 1.f) || std::isnan(conf_thr))
+        return RCMVS_E_ARG;
+    Seed sd{pred, orc_logit_threshold(conf_thr), n_local, span, (opts->flags & RCMVS_FLAG_SEED_AND_SWEEP) != 0};
+    const int rc = estimate_impl(views, n_views, ref_idx, srcs, n_src, zmin, zmax, opts, depth_out, cost_out,
+                                 normal_out, nthreads, nullptr, &sd);
+    if (seeded_out) *seeded_out = sd.seeded;
+    return rc;
+}
+
+// The confidence test sigmoid(logit) >= conf_thr as a logit threshold,
+// ln(c / (1 - c)) in f64 rounded to f32 (-inf for c <= 0, +inf for c >= 1).
+float orc_logit_threshold(float conf_thr) {
+    if (!(conf_thr > 0.0f)) return -INFINITY;
+    if (!(conf_thr < 1.0f)) return INFINITY;
+    const double c = (double)conf_thr;
+    return (float)std::log(c / (1.0 - c));
 }
 
 // mvs/src/fuse.rs:32-62  sample_depth

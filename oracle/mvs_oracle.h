@@ -50,6 +50,22 @@ int orc_estimate_depth(const rcmvs_view* views, int32_t n_views, int32_t ref_idx
                        const rcmvs_options* opts, float* depth_out, float* cost_out,
                        float* normal_out, int32_t nthreads, uint64_t* work_out);
 
+/* estimate_depth with the learned init (no reference counterpart): the plane
+ * sweep of stereo.rs:247-269 is replaced, for pixels whose quarter cell
+ * proposes a usable plane, by the best of n_local planes around it, as the
+ * library's rcmvs_scene_estimate_depth_seeded computes it.  pred holds the
+ * reference view's (w/4)*(h/4) cells of 16 f32 (t, normal xyz, confidence
+ * logit, 11 unused).  seeded_out (nullable) gets the number of seeded pixels.
+ * RCMVS_FLAG_INIT_ONLY in opts->flags leaves the passes out (both here and
+ * in orc_estimate_depth). */
+int orc_estimate_depth_seeded(const rcmvs_view* views, int32_t n_views, int32_t ref_idx,
+                              const int32_t* srcs, int32_t n_src, double zmin, double zmax,
+                              const rcmvs_options* opts, const float* pred, float conf_thr,
+                              int32_t n_local, float span, float* depth_out, float* cost_out,
+                              float* normal_out, int32_t nthreads, uint64_t* seeded_out);
+/* ln(c / (1 - c)) in f64 rounded to f32; -inf for c <= 0, +inf for c >= 1. */
+float orc_logit_threshold(float conf_thr);
+
 /* fuse::fuse_depth_maps.  Output sorted by voxel key (x, then y, then z).
  * *xyz_out / *rgb_out are malloc'ed; release with orc_free. */
 int orc_fuse_depth_maps(const rcmvs_view* views, int32_t n_views,

@@ -46,6 +46,10 @@ def lib():
         L.orc_rel_pose.argtypes = [vp, vp, vp, vp]
         L.orc_plane_cost_field.argtypes = [vp, i32, i32, vp, i32, vp, vp, vp, vp, i32]
         L.orc_estimate_depth.argtypes = [vp, i32, i32, vp, i32, f64, f64, vp, vp, vp, vp, i32, vp]
+        L.orc_estimate_depth_seeded.argtypes = [vp, i32, i32, vp, i32, f64, f64, vp, vp, f32, i32, f32, vp, vp,
+                                                vp, i32, vp]
+        L.orc_logit_threshold.argtypes = [f32]
+        L.orc_logit_threshold.restype = f32
         L.orc_fuse_depth_maps.argtypes = [vp, i32, vp, vp, vp, vp, u64, vp, vp, vp, vp, vp, i32]
         L.orc_free.argtypes = [vp]
         L.orc_write_ply_binary.argtypes = [C.c_char_p, vp, vp, u64]
@@ -142,6 +146,35 @@ def estimate_depth(views, ref_idx, srcs, zmin, zmax, opts, nthreads=0, normals=T
                                   _abi.ptr(normal), nthreads, work.ctypes.data)
     _chk(rc, "estimate_depth")
     return depth, cost, normal, (int(work[0]), int(work[1]))
+
+
+def estimate_depth_seeded(views, ref_idx, srcs, zmin, zmax, opts, pred, conf_thr, n_local=1, span=0.0,
+                          nthreads=0, normals=True):
+    """estimate_depth with the learned init (no reference counterpart): pred
+    is the reference view's (h/4, w/4, 16) f32 prediction map.  Returns
+    (depth, cost, normal|None, seeded pixel count)."""
+    va = _abi.view_array(views)
+    srcs = np.ascontiguousarray(srcs, dtype=np.int32)
+    r = views[ref_idx]
+    pred = np.ascontiguousarray(pred, dtype=np.float32)
+    assert pred.size == (r.h // 4) * (r.w // 4) * 16
+    if pred.size == 0:
+        pred = np.zeros(16, np.float32)
+    depth = np.empty((r.h, r.w), np.float32)
+    cost = np.empty((r.h, r.w), np.float32)
+    normal = np.empty((r.h, r.w, 3), np.float32) if normals else None
+    seeded = C.c_uint64()
+    o = opts.to_c()
+    rc = lib().orc_estimate_depth_seeded(va, len(views), ref_idx, srcs.ctypes.data, len(srcs), float(zmin),
+                                         float(zmax), C.byref(o), pred.ctypes.data, float(conf_thr), int(n_local),
+                                         float(span), depth.ctypes.data, cost.ctypes.data, _abi.ptr(normal),
+                                         nthreads, C.byref(seeded))
+    _chk(rc, "estimate_depth_seeded")
+    return depth, cost, normal, seeded.value
+
+
+def logit_threshold(conf_thr):
+    return float(lib().orc_logit_threshold(float(conf_thr)))
 
 
 def fuse_depth_maps(views, depth_maps, order_offsets, order, sparse_xyz, opts, nthreads=0):

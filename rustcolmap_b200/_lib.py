@@ -71,6 +71,8 @@ def mvs():
         "rcmvs_net_train_step": ([vp, vp, vp, vp, i32, i32, i32, C.c_float, i32, vp, vp], C.c_int),
         "rcmvs_scene_costvol": ([vp, vp, vp, i32, vp], C.c_int),
         "rcmvs_scene_estimate_depth_learned": ([vp, vp, vp, i32, vp, vp, C.c_float, i32, C.c_float, vp], C.c_int),
+        "rcmvs_scene_estimate_depth_seeded": ([vp, vp, vp, i32, vp, vp, i32, C.c_float, i32, C.c_float, vp],
+                                              C.c_int),
         "rcmvs_run_mvs_learned": ([vp, vp, i32, vp, vp, vp, C.c_float, i32, C.c_float, vp, vp, vp], C.c_int),
         "rcmvs_autotune": ([vp, vp, vp, i32, vp], C.c_int),
         "rcmvs_tune_table": ([vp, vp, i32, vp], C.c_int),
@@ -127,7 +129,7 @@ _SIG_NAMES = [
     "rcmvs_last_work", "rcmvs_selftest_f2i", "rcmvs_ctx_timing", "rcmvs_ctx_kernel_time",
     "rcmvs_estimate_depth_noalloc", "rcmvs_net_param_count", "rcmvs_net_create", "rcmvs_net_destroy",
     "rcmvs_net_get_params", "rcmvs_net_forward", "rcmvs_net_train_step", "rcmvs_scene_costvol",
-    "rcmvs_scene_estimate_depth_learned", "rcmvs_run_mvs_learned", "rcmvs_autotune", "rcmvs_tune_table",
+    "rcmvs_scene_estimate_depth_learned", "rcmvs_scene_estimate_depth_seeded", "rcmvs_run_mvs_learned", "rcmvs_autotune", "rcmvs_tune_table",
     "rcmvs_tune_set", "rcmvs_depth_vis", "rcmvs_scene_depth_vis", "rcmvs_write_png_gray",
     "rcmvs_working_size", "rcmvs_resize_view", "rcmvs_fuse_candidates", "rcmvs_fuse_reduce",
     "rcmvs_scene_fuse_candidates", "rcmvs_sift_options_default", "rcmvs_extract_sift", "rcmvs_sift_frame_free",

@@ -402,16 +402,36 @@ def read_png(path):
     return out.reshape(h, w, chans)
 
 
+def _png_with_pillow(path):
+    """An 8-bit grey/RGB(A) PNG decoded by Pillow (PNG is lossless, so the
+    pixels are read_png's), or None when Pillow is missing or the file holds
+    another kind of PNG."""
+    try:
+        from PIL import Image
+    except ImportError:
+        return None
+    try:
+        with Image.open(path) as im:
+            if im.format != "PNG" or im.mode not in ("L", "LA", "RGB", "RGBA") or im.info.get("interlace"):
+                return None
+            a = np.asarray(im, dtype=np.uint8)
+    except OSError:
+        return None
+    return np.ascontiguousarray(a.reshape(a.shape[0], a.shape[1], -1))
+
+
 def read_image(path):
-    """Decoded 8-bit image (h, w, channels).  PNG goes through read_png (the
-    pixels the reference's decoder gives); other formats (JPEG, BMP, TIFF,
-    ...) through Pillow, whose JPEG inverse DCT is not the `image` crate's,
-    so lossy images may differ from the reference's by a grey level in
-    places.  Palette, 16-bit and other modes are converted to RGB."""
+    """Decoded 8-bit image (h, w, channels).  PNG gives the pixels the
+    reference's decoder gives: through Pillow when it is installed (its
+    per-row filters run in C), else through read_png; other formats (JPEG,
+    BMP, TIFF, ...) through Pillow, whose JPEG inverse DCT is not the `image`
+    crate's, so lossy images may differ from the reference's by a grey level
+    in places.  Palette, 16-bit and other modes are converted to RGB."""
     with open(path, "rb") as f:
         sig = f.read(8)
     if sig == b"\x89PNG\r\n\x1a\n":
-        return read_png(path)
+        a = _png_with_pillow(path)
+        return read_png(path) if a is None else a
     try:
         from PIL import Image
     except ImportError:

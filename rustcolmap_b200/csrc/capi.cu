@@ -14,7 +14,6 @@
 #include "rcmvs_internal.cuh"
 
 namespace rcmvs {
-constexpr int kCensusTileW = 32, kCensusTileH = 8;
 
 cudaError_t DeviceArena::get(int slot, size_t bytes, void** out) {
     if ((int)slots.size() <= slot) slots.resize(slot + 1);
@@ -300,7 +299,7 @@ int rcmvs_scene_create(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views,
         sc->cams.push_back(c);
         if (!v.rgb) sc->has_rgb = false;
         tile_start.push_back(tiles);
-        tiles += ((v.w + kCensusTileW - 1) / kCensusTileW) * ((v.h + kCensusTileH - 1) / kCensusTileH);
+        tiles += census_tiles(v.w, v.h);
         off += (int64_t)v.w * v.h;
     }
     tile_start.push_back(tiles);
@@ -400,7 +399,8 @@ int rcmvs_scene_estimate_depth(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job*
             return fail(ctx, RCMVS_E_ARG, "reference view long side exceeds max_dim");
     }
     constexpr uint32_t kFlags = RCMVS_FLAG_ONE_CANDIDATE | RCMVS_FLAG_PERSISTENT | RCMVS_FLAG_CUDA_GRAPH |
-                                RCMVS_FLAG_AUTOTUNE | RCMVS_FLAG_NO_SKIP_DUPLICATES;
+                                RCMVS_FLAG_AUTOTUNE | RCMVS_FLAG_NO_SKIP_DUPLICATES | RCMVS_FLAG_INIT_ONLY |
+                                RCMVS_FLAG_SEED_AND_SWEEP;  // the last one only affects the learned init
     if (opts->flags & ~kFlags) return fail(ctx, RCMVS_E_ARG, "unknown bits in opts->flags");
     if (n_jobs == 0) return RCMVS_OK;
     CK(cudaSetDevice(ctx->device));
@@ -413,7 +413,7 @@ int rcmvs_scene_estimate_depth(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job*
     Schedule s;
     s.init = (opts->flags & RCMVS_FLAG_ONE_CANDIDATE) ? Schedule::ONE_CANDIDATE : Schedule::ROWS;
     s.nh = (int)std::max<uint32_t>(opts->num_hyp, 2u);
-    s.n_passes = (uint64_t)std::max<uint32_t>(opts->sweeps, 1u) * 2;
+    s.n_passes = (opts->flags & RCMVS_FLAG_INIT_ONLY) ? 0 : (uint64_t)std::max<uint32_t>(opts->sweeps, 1u) * 2;
     s.cost_thr = opts->cost_thr;
     s.persistent = (opts->flags & RCMVS_FLAG_PERSISTENT) != 0;
     s.graph = (opts->flags & RCMVS_FLAG_CUDA_GRAPH) != 0;

@@ -181,9 +181,10 @@ struct Schedule {
     // learned init
     const float* pred = nullptr;
     const int64_t* pred_off = nullptr;  // per launch position
-    float conf_thr = 0.f;
+    float logit_thr = 0.f;  // confident iff logit >= logit_thr
     int n_local = 1;
     float span = 0.f;
+    bool sweep_seeded = false;  // seeded pixels also run the plane sweep (RCMVS_FLAG_SEED_AND_SWEEP)
     unsigned long long* d_learned = nullptr;  // zeroed inside the schedule
 };
 

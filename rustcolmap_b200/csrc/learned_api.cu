@@ -282,7 +282,7 @@ int ensure_quarter(rcmvs_ctx* ctx, rcmvs_scene* sc) {
         blk.push_back(nb);
         tiles.push_back(nt);
         nb += (int)(((int64_t)w * h + 255) / 256);
-        nt += ((w + 31) / 32) * ((h + 7) / 8);
+        nt += census_tiles(w, h);
         off += (int64_t)w * h;
         // pixel centre of quarter cell X is full-res 4X + 1.5
         const HostCam& c = sc->cams[v];
@@ -397,6 +397,82 @@ int check_jobs(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job* jobs, int n_job
     return RCMVS_OK;
 }
 
+constexpr uint32_t kSeedFlags = RCMVS_FLAG_PERSISTENT | RCMVS_FLAG_CUDA_GRAPH | RCMVS_FLAG_AUTOTUNE |
+                               RCMVS_FLAG_NO_SKIP_DUPLICATES | RCMVS_FLAG_INIT_ONLY | RCMVS_FLAG_SEED_AND_SWEEP;
+
+int check_seed_args(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job* jobs, int n_jobs, const rcmvs_options* opts,
+                    float conf_thr, int n_local, float span) {
+    if (n_local < 1 || n_local > 256 || !(span >= 0.f && span <= 1.f) || std::isnan(conf_thr))
+        return lfail(ctx, RCMVS_E_ARG, "learned init: n_local must be 1..256, span in [0, 1], conf_thr a number");
+    if (opts->flags & ~kSeedFlags) return lfail(ctx, RCMVS_E_ARG, "learned init: unsupported bits in opts->flags");
+    if (sc->ctx != ctx) return lfail(ctx, RCMVS_E_ARG, "scene belongs to another context");
+    return check_jobs(ctx, sc, jobs, n_jobs);
+}
+
+// The confidence test sigmoid(logit) >= conf_thr as a threshold on the
+// logit: ln(c / (1 - c)) in f64, rounded to f32; -inf for c <= 0 (every
+// finite logit passes), +inf for c >= 1 (none does).
+float logit_threshold(float conf_thr) {
+    if (!(conf_thr > 0.0f)) return -INFINITY;
+    if (!(conf_thr < 1.0f)) return INFINITY;
+    const double c = (double)conf_thr;
+    return (float)std::log(c / (1.0 - c));
+}
+
+struct QuarterDims {
+    int w, h;
+};
+QuarterDims quarter_dims(const rcmvs_scene* sc, int view) {
+    return QuarterDims{sc->views[view].w >> 2, sc->views[view].h >> 2};
+}
+
+// The full-resolution stereo batch with the learned init from `pred` (the
+// jobs' quarter-resolution predictions back to back, device memory).
+int seeded_stereo(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job* jobs, int n_jobs, const rcmvs_options* opts,
+                  const float* pred, float conf_thr, int n_local, float span, uint64_t* learned_pixels) {
+    cudaStream_t st = ctx->stream;
+    StereoBatch batch;
+    int rc = build_batch(ctx, sc, jobs, n_jobs, opts, batch);
+    if (rc) return rc;
+    std::vector<int64_t> qoff(n_jobs), poff(n_jobs);
+    for (int j = 0, o = 0; j < n_jobs; ++j) {
+        qoff[j] = o;
+        const QuarterDims q = quarter_dims(sc, jobs[j].ref_idx);
+        o += (int64_t)q.w * q.h;
+    }
+    for (int p = 0; p < n_jobs; ++p) poff[p] = qoff[batch.order[p]];
+    void *ppo, *pcnt;
+    LCK(sc->arena.get(46, sizeof(int64_t) * n_jobs, &ppo));
+    LCK(sc->arena.get(47, 16, &pcnt));
+    LCK(cudaMemcpyAsync(ppo, poff.data(), sizeof(int64_t) * n_jobs, cudaMemcpyHostToDevice, st));
+    Schedule sched;
+    sched.init = Schedule::LEARNED;
+    sched.nh = (int)std::max<uint32_t>(opts->num_hyp, 2u);
+    sched.n_passes =
+        (opts->flags & RCMVS_FLAG_INIT_ONLY) ? 0 : (uint64_t)std::max<uint32_t>(opts->sweeps, 1u) * 2;
+    sched.cost_thr = opts->cost_thr;
+    sched.persistent = (opts->flags & RCMVS_FLAG_PERSISTENT) != 0;
+    sched.graph = (opts->flags & RCMVS_FLAG_CUDA_GRAPH) != 0;
+    sched.skip_duplicates = !(opts->flags & RCMVS_FLAG_NO_SKIP_DUPLICATES);
+    sched.pred = pred;
+    sched.pred_off = (const int64_t*)ppo;
+    sched.logit_thr = logit_threshold(conf_thr);
+    sched.n_local = n_local;
+    sched.span = span;
+    sched.sweep_seeded = (opts->flags & RCMVS_FLAG_SEED_AND_SWEEP) != 0;
+    sched.d_learned = (unsigned long long*)pcnt;
+    rc = run_batch(ctx, sc, batch, sched);
+    if (rc) return rc;
+    for (int j = 0; j < n_jobs; ++j) sc->has_depth[jobs[j].ref_idx] = 1;
+    if (learned_pixels) {
+        unsigned long long h = 0;
+        LCK(cudaMemcpyAsync(&h, pcnt, 8, cudaMemcpyDeviceToHost, st));
+        LCK(cudaStreamSynchronize(st));
+        *learned_pixels = h;
+    }
+    return RCMVS_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -424,9 +500,9 @@ int rcmvs_scene_costvol(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job* jobs, 
 int rcmvs_scene_estimate_depth_learned(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job* jobs, int32_t n_jobs,
                                        const rcmvs_options* opts, rcmvs_net* net, float conf_thr,
                                        int32_t n_local, float span, uint64_t* learned_pixels) {
-    if (!ctx || !sc || !opts || !net || n_local < 1 || n_local > 256 || !(span >= 0.f && span <= 1.f))
+    if (!ctx || !sc || !opts || !net)
         return lfail(ctx, RCMVS_E_ARG, "rcmvs_scene_estimate_depth_learned: bad argument");
-    int rc = check_jobs(ctx, sc, jobs, n_jobs);
+    int rc = check_seed_args(ctx, sc, jobs, n_jobs, opts, conf_thr, n_local, span);
     if (rc) return rc;
     LCK(cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;
@@ -468,44 +544,30 @@ int rcmvs_scene_estimate_depth_learned(rcmvs_ctx* ctx, rcmvs_scene* sc, const rc
         }
     }
     hk.end("learned_net");
-    // full-resolution jobs: the shared stereo batch with the learned init
-    StereoBatch batch;
-    rc = build_batch(ctx, sc, jobs, n_jobs, opts, batch);
+    return seeded_stereo(ctx, sc, jobs, n_jobs, opts, (const float*)pred, conf_thr, n_local, span, learned_pixels);
+}
+
+// Stereo seeded by caller-given proposals (the network's output format).
+int rcmvs_scene_estimate_depth_seeded(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job* jobs, int32_t n_jobs,
+                                      const rcmvs_options* opts, const float* pred, int32_t pred_on_device,
+                                      float conf_thr, int32_t n_local, float span, uint64_t* learned_pixels) {
+    if (!ctx || !sc || !opts || !pred)
+        return lfail(ctx, RCMVS_E_ARG, "rcmvs_scene_estimate_depth_seeded: bad argument");
+    int rc = check_seed_args(ctx, sc, jobs, n_jobs, opts, conf_thr, n_local, span);
     if (rc) return rc;
-    std::vector<int64_t> qoff(n_jobs), poff(n_jobs);
-    for (int j = 0, o = 0; j < n_jobs; ++j) {
-        qoff[j] = o;
-        o += (int64_t)sc->qviews[jobs[j].ref_idx].w * sc->qviews[jobs[j].ref_idx].h;
+    LCK(cudaSetDevice(ctx->device));
+    if (!pred_on_device) {
+        int64_t qpx = 0;
+        for (int j = 0; j < n_jobs; ++j) {
+            const QuarterDims q = quarter_dims(sc, jobs[j].ref_idx);
+            qpx += (int64_t)q.w * q.h;
+        }
+        void* dp;
+        LCK(sc->arena.get(44, 4 * (size_t)std::max<int64_t>(qpx, 1) * NET_OUT_C, &dp));
+        LCK(cudaMemcpyAsync(dp, pred, 4 * (size_t)qpx * NET_OUT_C, cudaMemcpyHostToDevice, ctx->stream));
+        pred = (const float*)dp;
     }
-    for (int p = 0; p < n_jobs; ++p) poff[p] = qoff[batch.order[p]];
-    void *ppo, *pcnt;
-    LCK(sc->arena.get(46, sizeof(int64_t) * n_jobs, &ppo));
-    LCK(sc->arena.get(47, 16, &pcnt));
-    LCK(cudaMemcpyAsync(ppo, poff.data(), sizeof(int64_t) * n_jobs, cudaMemcpyHostToDevice, st));
-    Schedule sched;
-    sched.init = Schedule::LEARNED;
-    sched.nh = (int)std::max<uint32_t>(opts->num_hyp, 2u);
-    sched.n_passes = (uint64_t)std::max<uint32_t>(opts->sweeps, 1u) * 2;
-    sched.cost_thr = opts->cost_thr;
-    sched.persistent = (opts->flags & RCMVS_FLAG_PERSISTENT) != 0;
-    sched.graph = (opts->flags & RCMVS_FLAG_CUDA_GRAPH) != 0;
-    sched.skip_duplicates = !(opts->flags & RCMVS_FLAG_NO_SKIP_DUPLICATES);
-    sched.pred = (const float*)pred;
-    sched.pred_off = (const int64_t*)ppo;
-    sched.conf_thr = conf_thr;
-    sched.n_local = n_local;
-    sched.span = span;
-    sched.d_learned = (unsigned long long*)pcnt;
-    rc = run_batch(ctx, sc, batch, sched);
-    if (rc) return rc;
-    for (int j = 0; j < n_jobs; ++j) sc->has_depth[jobs[j].ref_idx] = 1;
-    if (learned_pixels) {
-        unsigned long long h = 0;
-        LCK(cudaMemcpyAsync(&h, pcnt, 8, cudaMemcpyDeviceToHost, st));
-        LCK(cudaStreamSynchronize(st));
-        *learned_pixels = h;
-    }
-    return RCMVS_OK;
+    return seeded_stereo(ctx, sc, jobs, n_jobs, opts, pred, conf_thr, n_local, span, learned_pixels);
 }
 
 }  // extern "C"

@@ -25,8 +25,10 @@
 //                 order of the tiles does not matter)
 //   decide_kernel the reference's tests per row of A
 //
-// Pairs run in chunks sized to a fixed distance-matrix budget; results come
-// back as per-pair lists in the reference's order (ascending index in A).
+// Pairs run in chunks whose tile partials (the per-tile best/second entries
+// of every row and column, 12 bytes each; no distance matrix is written)
+// fit P_BUDGET; results come back as per-pair lists in the reference's order
+// (ascending index in A).
 #include <climits>
 #include <cmath>
 #include <cstring>

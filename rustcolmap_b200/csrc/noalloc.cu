@@ -18,7 +18,6 @@
 // Calls whose GPU work overlaps (two streams, or two host threads) race on
 // the array: serialise them.
 #include <cstring>
-#include <mutex>
 
 #include "rcmvs_internal.cuh"
 
@@ -44,12 +43,6 @@ static_assert(al(sizeof(DevView) * kViews) + al(sizeof(int32_t) * (kViews + 1)) 
                       al(sizeof(DevJob)) + al(2 * sizeof(int32_t)) <= kDesc,
               "descriptor region too small");
 
-constexpr int kMaxDevices = 64;
-std::mutex g_setup_mu;
-void* g_scratch[kMaxDevices];  // device address of the array, per device
-
-constexpr int kCensusTileW = 32, kCensusTileH = 8;  // census.cu's tile
-
 }  // namespace
 
 // The scratch array.  Host code must not use this name as a device address:
@@ -58,18 +51,24 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[RCMVS_NOALLOC_S
 
 namespace {
 
+// The array's device address on the current device.  Looked up on every
+// call rather than cached: the lookup allocates nothing, and after a
+// cudaDeviceReset the module is loaded again in a new context where the
+// array may sit at another address.  The first lookup on a device loads the
+// module there (reserving the array), which is why the first call on a
+// device must not be made during a stream capture.
 int scratch_for_current_device(void** out) {
-    int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return RCMVS_E_CUDA;
-    std::lock_guard<std::mutex> lk(g_setup_mu);
-    if (!g_scratch[dev]) {
-        void* p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return RCMVS_E_CUDA;
-        g_scratch[dev] = p;
-    }
-    *out = g_scratch[dev];
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return RCMVS_E_CUDA;
+    *out = p;
     return RCMVS_OK;
 }
+
+// Flags this entry point accepts: it always runs the one-launch-per-step
+// schedule and never skips duplicate candidates (so NO_SKIP_DUPLICATES holds
+// trivially); SEED_AND_SWEEP concerns the learned init only.
+constexpr uint32_t kNoallocFlags = RCMVS_FLAG_ONE_CANDIDATE | RCMVS_FLAG_NO_SKIP_DUPLICATES | RCMVS_FLAG_INIT_ONLY |
+                                   RCMVS_FLAG_SEED_AND_SWEEP;
 
 bool finite_pos(double x) { return x > 0.0 && x < 1e300; }
 
@@ -90,7 +89,7 @@ extern "C" int rcmvs_estimate_depth_noalloc(const rcmvs_view* views, int32_t n_v
                                             const rcmvs_options* opts, float* depth_dev, float* cost_dev,
                                             void* stream) {
     if (!views || n_views <= 0 || ref_idx < 0 || ref_idx >= n_views || n_src < 0 || (n_src > 0 && !srcs) || !opts ||
-        !depth_dev || !cost_dev || (opts->flags & ~RCMVS_FLAG_ONE_CANDIDATE))
+        !depth_dev || !cost_dev || (opts->flags & ~kNoallocFlags))
         return RCMVS_E_ARG;
     if (!(finite_pos(zmin) && finite_pos(zmax))) return RCMVS_E_ARG;
     if (n_src > RCMVS_NOALLOC_MAX_SOURCES) return RCMVS_E_LIMIT;
@@ -107,10 +106,8 @@ extern "C" int rcmvs_estimate_depth_noalloc(const rcmvs_view* views, int32_t n_v
         if ((uint32_t)(v.w > v.h ? v.w : v.h) > opts->max_dim) return RCMVS_E_ARG;
         if ((size_t)v.w * (size_t)v.h > kPx) return RCMVS_E_LIMIT;
     }
-    TileShape ts{16, 16};
-    if (opts->tile_w > 0 && opts->tile_h > 0) ts = TileShape{(int)opts->tile_w, (int)opts->tile_h};
-    if (ts.tw <= 0 || ts.th <= 0 || ts.tw * ts.th > 256 || (ts.tw * ts.th) % 32 != 0 || stereo_smem_bytes(ts) > 48 * 1024)
-        return RCMVS_E_ARG;
+    const TileShape ts = default_tile_shape(opts);
+    if (!tile_shape_ok(ts)) return RCMVS_E_ARG;
 
     void* base = nullptr;
     int rc = scratch_for_current_device(&base);
@@ -127,7 +124,7 @@ extern "C" int rcmvs_estimate_depth_noalloc(const rcmvs_view* views, int32_t n_v
         const rcmvs_view& v = views[local[i]];
         dv[i] = DevView{v.w, v.h, (int64_t)(i * kPx)};
         tile_start[i] = tiles;
-        tiles += ((v.w + kCensusTileW - 1) / kCensusTileW) * ((v.h + kCensusTileH - 1) / kCensusTileH);
+        tiles += census_tiles(v.w, v.h);
         cams[4 * i] = v.f;
         cams[4 * i + 1] = v.cx;
         cams[4 * i + 2] = v.cy;
@@ -212,7 +209,8 @@ extern "C" int rcmvs_estimate_depth_noalloc(const rcmvs_view* views, int32_t n_v
     const int variant = (opts->flags & RCMVS_FLAG_ONE_CANDIDATE) ? 1 : 0;
     const LaunchGeom g{ts.tw * ts.th, stereo_smem_bytes(ts), J.tiles, nullptr};
     NCK(launch_init(d_job, d_job_start, 1, g, nh, census, rays, A, nullptr, st, variant));
-    const uint64_t n_passes = (uint64_t)(opts->sweeps > 1u ? opts->sweeps : 1u) * 2;
+    const uint64_t n_passes =
+        (opts->flags & RCMVS_FLAG_INIT_ONLY) ? 0 : (uint64_t)(opts->sweeps > 1u ? opts->sweeps : 1u) * 2;
     for (uint64_t pass = 0; pass < n_passes; ++pass) {
         const float t = (float)pass / (float)n_passes;  // stereo.rs:275-277
         const float sig_inv = 0.02f * powf(0.28f, t * 4.0f);

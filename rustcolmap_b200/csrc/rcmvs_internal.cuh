@@ -81,6 +81,13 @@ struct LaunchGeom {
 // (job j owns tiles [job_start[j], job_start[j+1])).
 
 // census + rays of every view (mvs/src/lib.rs:119-142, sfm-lite geom.rs:28-42)
+// Stereo tile shapes: at most 256 pixels, a multiple of 32, shared memory
+// within 48 KB; the default is opts' tile_w x tile_h, else 8x8.
+bool tile_shape_ok(TileShape ts);
+TileShape default_tile_shape(const rcmvs_options* opts);
+// Tiles (blocks) the census kernel uses for a w x h view; a scene's views
+// take consecutive tile ranges.
+int census_tiles(int w, int h);
 cudaError_t launch_census_rays(const DevView* d_views, const int32_t* d_tile_start, int n_views, int total_tiles,
                                const uint8_t* gray, uint64_t* census, float2* rays, const double* d_cams,
                                cudaStream_t st);
@@ -99,7 +106,7 @@ cudaError_t launch_pass(const DevJob* d_jobs, const int32_t* d_job_start, int n_
 // Init seeded by the proposal network's predictions (no reference counterpart).
 cudaError_t launch_init_learned(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, const LaunchGeom& g,
                                 int nh, const uint64_t* census, const float2* rays, PlaneBuf out, const float* pred,
-                                const int64_t* pred_off, float conf_thr, int n_local, float span,
+                                const int64_t* pred_off, float logit_thr, int n_local, float span, bool sweep_seeded,
                                 unsigned long long* d_learned, cudaStream_t st);
 // Texture/cost/range gate (stereo.rs:373-393); never persistent.
 cudaError_t launch_gate(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, const LaunchGeom& g,

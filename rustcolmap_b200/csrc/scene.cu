@@ -2,9 +2,14 @@
 // benchmarks; not part of the stereo/fusion path).  Ray casting of rectangles,
 // boxes and spheres with 4-octave value-noise texture.  Host and device run
 // the same __host__ __device__ code; the build uses --fmad=false (device) and
-// -ffp-contract=off (host), so both produce identical images.
+// -ffp-contract=off (host), so both produce identical images.  Compiled as
+// plain C++ (no __CUDACC__) it is the host renderer alone, for programs that
+// must not load the CUDA library (device >= 0 is then refused).
+#ifdef __CUDACC__
 #include <cuda_runtime.h>
+#endif
 
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdio>
@@ -15,7 +20,11 @@
 
 #include "../../include/rcscene.h"
 
+#ifdef __CUDACC__
 #define HD __host__ __device__ __forceinline__
+#else
+#define HD inline
+#endif
 
 namespace {
 
@@ -230,6 +239,7 @@ HD void render_px(const rcscene_prim* prims, int np, const rcscene_patch* patche
     }
 }
 
+#ifdef __CUDACC__
 __global__ void render_kernel(const rcscene_prim* prims, int np, const rcscene_patch* patches, int npatch,
                               RCam c, int ss, uint8_t* gray, float* depth, float* normal) {
     int x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -237,6 +247,8 @@ __global__ void render_kernel(const rcscene_prim* prims, int np, const rcscene_p
     if (x >= c.w || y >= c.h) return;
     render_px(prims, np, patches, npatch, c, x, y, ss, gray, depth, normal);
 }
+
+#endif
 
 RCam make_cam(const rcscene_cam& k) {
     RCam c;
@@ -251,6 +263,7 @@ RCam make_cam(const rcscene_cam& k) {
     return c;
 }
 
+#ifdef __CUDACC__
 #define CK(x)                                                                  \
     do {                                                                       \
         cudaError_t e_ = (x);                                                  \
@@ -260,6 +273,7 @@ RCam make_cam(const rcscene_cam& k) {
             goto done;                                                         \
         }                                                                      \
     } while (0)
+#endif
 
 }  // namespace
 
@@ -301,6 +315,10 @@ extern "C" int rcscene_render(const rcscene_prim* prims, int32_t n_prims, const 
         }
         return 0;
     }
+#ifndef __CUDACC__
+    g_err = "rcscene_render: this build renders on the host only (device = -1)";
+    return -1;
+#else
     int rc = 0;
     rcscene_prim* dprims = nullptr;
     rcscene_patch* dpatch = nullptr;
@@ -336,4 +354,5 @@ done:
     cudaFree(dd);
     cudaFree(dn);
     return rc;
+#endif
 }

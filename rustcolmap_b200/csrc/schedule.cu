@@ -42,19 +42,8 @@ int sfail(rcmvs_ctx* ctx, int code, const std::string& msg) {
 // powf as in the reference.
 float powf_host(float b, float e) { return powf(b, e); }
 
-bool shape_ok(TileShape ts) {
-    return ts.tw > 0 && ts.th > 0 && ts.tw * ts.th <= 256 && (ts.tw * ts.th) % 32 == 0 &&
-           stereo_smem_bytes(ts) <= 48 * 1024;
-}
-
-// Default tile: 8x8 measured fastest among the fixed shapes at 960x720 (K 8),
-// 1920x1080 (K 10) and mixed batches (K 4-12) on B200, 4-7% ahead of 16x16:
-// a block holds its SM slot until its slowest warp (the one with the fewest
-// early aborts) is done, and smaller blocks release it sooner.
-TileShape fixed_shape(const rcmvs_options* o) {
-    if (o && o->tile_w > 0 && o->tile_h > 0) return TileShape{(int)o->tile_w, (int)o->tile_h};
-    return TileShape{8, 8};
-}
+bool shape_ok(TileShape ts) { return tile_shape_ok(ts); }
+TileShape fixed_shape(const rcmvs_options* o) { return default_tile_shape(o); }
 
 const rcmvs_tune_entry* find_class(const rcmvs_ctx* ctx, int w, int h) {
     for (const auto& e : ctx->tuned)
@@ -335,7 +324,7 @@ int run_batch(rcmvs_ctx* ctx, rcmvs_scene* sc, const StereoBatch& b, const Sched
         hk.begin(s.init == Schedule::LEARNED ? "learned_init" : "stereo_init");
         if (s.init == Schedule::LEARNED)
             e = launch_init_learned(dj, dst, n_jobs, g, s.nh, sc->census, sc->rays, A, s.pred, s.pred_off,
-                                    s.conf_thr, s.n_local, s.span, s.d_learned, st);
+                                    s.logit_thr, s.n_local, s.span, s.sweep_seeded, s.d_learned, st);
         else
             e = launch_init(dj, dst, n_jobs, g, s.nh, sc->census, sc->rays, A, s.d_work, st,
                             s.init == Schedule::ONE_CANDIDATE ? 1 : 0);
@@ -371,9 +360,10 @@ int run_batch(rcmvs_ctx* ctx, rcmvs_scene* sc, const StereoBatch& b, const Sched
     append(key, s.nh);
     append(key, s.n_passes);
     append(key, s.cost_thr);
-    append(key, s.conf_thr);
+    append(key, s.logit_thr);
     append(key, s.n_local);
     append(key, s.span);
+    append(key, s.sweep_seeded);
     const void* ptrs[] = {pj, ps, pq, s.d_work, s.pred, s.pred_off, s.d_learned, sc->census, sc->rays,
                           sc->plane_a, sc->plane_b, sc->pcost_a, sc->pcost_b, A0.d, B0.d, sc->depth, sc->cost,
                           sc->normal};
@@ -397,6 +387,20 @@ int run_batch(rcmvs_ctx* ctx, rcmvs_scene* sc, const StereoBatch& b, const Sched
     }
     SCK(cudaGraphLaunch(sc->graph, st));
     return RCMVS_OK;
+}
+
+bool tile_shape_ok(TileShape ts) {
+    return ts.tw > 0 && ts.th > 0 && ts.tw * ts.th <= 256 && (ts.tw * ts.th) % 32 == 0 &&
+           stereo_smem_bytes(ts) <= 48 * 1024;
+}
+
+// Default tile: 8x8 measured fastest among the fixed shapes at 960x720 (K 8),
+// 1920x1080 (K 10) and mixed batches (K 4-12) on B200, 4-7% ahead of 16x16:
+// a block holds its SM slot until its slowest warp (the one with the fewest
+// early aborts) is done, and smaller blocks release it sooner.
+TileShape default_tile_shape(const rcmvs_options* o) {
+    if (o && o->tile_w > 0 && o->tile_h > 0) return TileShape{(int)o->tile_w, (int)o->tile_h};
+    return TileShape{8, 8};
 }
 
 }  // namespace rcmvs

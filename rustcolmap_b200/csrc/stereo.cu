@@ -571,7 +571,8 @@ __global__ void __launch_bounds__(256, MINB)
 // ---------------------------------------------------------------- learned init
 // Patch-match init from learned proposals (no reference counterpart).  A
 // pixel whose quarter-resolution cell predicts a plane with confidence
-// sigmoid(logit) >= conf_thr tries n_local planes with the predicted normal
+// sigmoid(logit) >= conf_thr (tested as logit >= logit_thr, the threshold's
+// logit, computed once on the host) tries n_local planes with the predicted normal
 // and inverse depths evenly spread over +-span/2 (in fractions of
 // [1/zmax, 1/zmin]) around the prediction, each kept only if it passes the
 // reference's gates (positive inverse depth, depth in [zmin/2, 2 zmax],
@@ -595,12 +596,13 @@ __global__ void __launch_bounds__(256, 3)
     init_learned_rows_kernel(const DevJob* __restrict__ jobs, const int32_t* __restrict__ job_start, int n_jobs,
                              int tiles, unsigned int* queue, int nh, const uint64_t* __restrict__ census,
                              const float2* __restrict__ rays, PlaneBuf out, const float* __restrict__ pred,
-                             const int64_t* __restrict__ pred_off, float conf_thr, int n_local, float span,
-                             unsigned long long* d_learned) {
+                             const int64_t* __restrict__ pred_off, float logit_thr, int n_local, float span,
+                             int sweep_seeded, unsigned long long* d_learned) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int s_tile;
     __shared__ int s_n;
     __shared__ unsigned short s_list[256];
+    __shared__ float s_seed_cost[256];  // phase 1's best cost per tile pixel (+inf: not seeded)
     for (int it = 0; PERSIST || it == 0; ++it) {
         const int tile = PERSIST ? next_tile(queue, tiles, it, &s_tile) : (int)blockIdx.x;
         if (tile < 0) break;
@@ -625,9 +627,8 @@ __global__ void __launch_bounds__(256, 3)
         if (inside && wq > 0 && hq > 0) {
             const int qx = min(x >> 2, wq - 1), qy = min(y >> 2, hq - 1);
             const float* o = pred + (pred_off[j] + (int64_t)qy * wq + qx) * NET_OUT_C;
-            const float conf = 1.f / (1.f + __expf(-o[4]));
             const float len = sqrtf(o[1] * o[1] + o[2] * o[2] + o[3] * o[3]);
-            if (conf >= conf_thr && len > 1e-6f) {
+            if (o[4] >= logit_thr && len > 1e-6f) {
                 pnx = o[1] / len;
                 pny = o[2] / len;
                 pnz = o[3] / len;
@@ -703,9 +704,9 @@ __global__ void __launch_bounds__(256, 3)
             out.nz[i] = plane;
             out.cost[i] = fminf(best_c, 1.0f);
             if (out.d) out.d[i] = plane_d;
-        } else if (inside) {
-            s_list[atomicAdd(&s_n, 1)] = (unsigned short)threadIdx.x;
         }
+        if ((int)threadIdx.x < 256) s_seed_cost[threadIdx.x] = seeded ? best_c : INFINITY;
+        if (inside && (!seeded || sweep_seeded)) s_list[atomicAdd(&s_n, 1)] = (unsigned short)threadIdx.x;
         const unsigned bal = __ballot_sync(0xffffffffu, seeded);
         if ((threadIdx.x & 31) == 0 && bal) atomicAdd(d_learned, (unsigned long long)__popc(bal));
         __syncthreads();  // the list is complete
@@ -716,10 +717,15 @@ __global__ void __launch_bounds__(256, 3)
             const int pt = s_list[e];
             const int plx = pt % T.tw, ply = pt / T.tw;
             const int px = T.x0 + plx, py = T.y0 + ply;
-            float bc = INFINITY, bdep = 0.f;
+            // a seeded pixel (sweep_seeded) starts the sweep from its
+            // proposal's cost: the sweep's hint rule then holds from the first
+            // hypothesis, and a sweep plane replaces the proposal only when
+            // strictly cheaper
+            float bc = s_seed_cost[pt], bdep = 0.f;
+            bool improved = false;
             int hi = 0, ssi = 0, sdy = 0;
             float d = hyp_depth(inv_min, inv_max, 0, nh);
-            float ssum = 0.f, sthr = INFINITY;
+            float ssum = 0.f, sthr = (bc + 0.02f) + 0.12f;
             bool slive = true;
             while (slive) {
                 bool fin = true, aborted = false;
@@ -734,6 +740,7 @@ __global__ void __launch_bounds__(256, 3)
                     if (c < bc) {
                         bc = c;
                         bdep = d;
+                        improved = true;
                     }
                     if (++hi >= nh) {
                         slive = false;
@@ -749,10 +756,12 @@ __global__ void __launch_bounds__(256, 3)
                     ++ssi;
                 }
             }
-            const size_t i = (size_t)J->off + (size_t)py * J->w + px;
-            out.nz[i] = make_float4(0.0f, 0.0f, 1.0f, bdep);
-            out.cost[i] = fminf(bc, 1.0f);
-            if (out.d) out.d[i] = bdep;
+            if (improved || !(s_seed_cost[pt] < INFINITY)) {
+                const size_t i = (size_t)J->off + (size_t)py * J->w + px;
+                out.nz[i] = make_float4(0.0f, 0.0f, 1.0f, bdep);
+                out.cost[i] = fminf(bc, 1.0f);
+                if (out.d) out.d[i] = bdep;
+            }
         }
     }
 }
@@ -900,18 +909,18 @@ cudaError_t launch_pass(const DevJob* d_jobs, const int32_t* d_job_start, int n_
 
 cudaError_t launch_init_learned(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, const LaunchGeom& g,
                                 int nh, const uint64_t* census, const float2* rays, PlaneBuf out, const float* pred,
-                                const int64_t* pred_off, float conf_thr, int n_local, float span,
+                                const int64_t* pred_off, float logit_thr, int n_local, float span, bool sweep_seeded,
                                 unsigned long long* d_learned, cudaStream_t st) {
     if (g.tiles <= 0) return cudaSuccess;
     if (g.queue)
         init_learned_rows_kernel<true><<<launch_grid(init_learned_rows_kernel<true>, g), g.nthr, g.smem, st>>>(
-            d_jobs, d_job_start, n_jobs, g.tiles, g.queue, nh, census, rays, out, pred, pred_off, conf_thr, n_local,
-            span, d_learned);
+            d_jobs, d_job_start, n_jobs, g.tiles, g.queue, nh, census, rays, out, pred, pred_off, logit_thr, n_local,
+            span, (int)sweep_seeded, d_learned);
     else
         init_learned_rows_kernel<false><<<g.tiles, g.nthr, g.smem, st>>>(d_jobs, d_job_start, n_jobs, g.tiles,
                                                                           nullptr, nh, census, rays, out, pred,
-                                                                          pred_off, conf_thr, n_local, span,
-                                                                          d_learned);
+                                                                          pred_off, logit_thr, n_local, span,
+                                                                          (int)sweep_seeded, d_learned);
     return cudaGetLastError();
 }
 

@@ -86,15 +86,13 @@ def costvol(ds, jobs, out_ptr):
     ds.ctx.check(ds.ctx._L.rcmvs_scene_costvol(ds.ctx.ptr, ds.ptr, cj, len(jobs), out_ptr))
 
 
-# Operating point, chosen on held-out seeds (6000-6007, and the C5 bench scene):
-# confident pixels (sigmoid >= 0.1) start from the predicted plane alone; a
-# local sweep around it (3 to 16 planes over +-1% to +-6% of the range) was
-# both slower and less accurate after the 2 sweeps.
 # Operating point: the predicted plane alone for pixels with confidence >=
 # 0.02, chosen on the tuning scenes (seeds 5000-5019) as the lowest threshold
 # whose accuracy stays 1 point above the plain method with 6 sweeps, with no
-# scene below it.
+# scene below it.  (A local sweep of 3 to 16 planes over +-1% to +-6% of the
+# range around the prediction was both slower and less accurate.)
 LOCAL_HYPS, LOCAL_SPAN, CONF_THR = 1, 0.0, 0.02
+LEARNED_FLAGS = 0  # RCMVS_FLAG_* bits of the learned arm
 
 
 def estimate_learned(ds, jobs, opts, net, conf_thr=CONF_THR, n_local=LOCAL_HYPS, span=LOCAL_SPAN):
@@ -106,6 +104,42 @@ def estimate_learned(ds, jobs, opts, net, conf_thr=CONF_THR, n_local=LOCAL_HYPS,
                                                               net.ptr, float(conf_thr), int(n_local), float(span),
                                                               C.byref(n)))
     return n.value
+
+
+def estimate_seeded(ds, jobs, opts, pred, conf_thr=CONF_THR, n_local=LOCAL_HYPS, span=LOCAL_SPAN):
+    """Stereo seeded by caller-given proposals: pred holds each job's
+    quarter-resolution (h/4, w/4, 16) f32 map, jobs back to back, as a numpy
+    array (host) or a CUDA tensor (device).  Returns the number of seeded
+    pixels."""
+    cj = _jobs_c(jobs)
+    o = opts.to_c()
+    n = C.c_uint64()
+    if isinstance(pred, np.ndarray):
+        arr = np.ascontiguousarray(pred, dtype=np.float32)
+        ptr, on_dev = arr.ctypes.data, 0
+    else:
+        assert pred.is_cuda and pred.is_contiguous() and str(pred.dtype) == "torch.float32"
+        ptr, on_dev = pred.data_ptr(), 1
+    ds.ctx.check(ds.ctx._L.rcmvs_scene_estimate_depth_seeded(ds.ctx.ptr, ds.ptr, cj, len(jobs), C.byref(o), ptr,
+                                                             on_dev, float(conf_thr), int(n_local), float(span),
+                                                             C.byref(n)))
+    return n.value
+
+
+def predict(ds, jobs, net):
+    """The network's quarter-resolution predictions of every job (jobs whose
+    reference views share one size), as a CUDA tensor (n, h/4, w/4, 16)."""
+    import torch
+    sizes = {(ds.views[j[0]].w, ds.views[j[0]].h) for j in jobs}
+    assert len(sizes) == 1, "predict() takes jobs of one view size"
+    w, h = sizes.pop()
+    hq, wq = h // 4, w // 4
+    x = torch.empty((len(jobs), hq, wq, COSTVOL_C), dtype=torch.bfloat16, device=f"cuda:{ds.ctx.device}")
+    costvol(ds, jobs, x.data_ptr())
+    out = torch.empty((len(jobs), hq, wq, NET_OUT_C), dtype=torch.float32, device=x.device)
+    net.forward(x.data_ptr(), len(jobs), hq, wq, out.data_ptr())
+    ds.ctx.synchronize()
+    return out
 
 
 def inv_range(zmin, zmax):
@@ -200,7 +234,8 @@ def train(net, x, lab, iters=1500, batch=16, lr=1e-3, seed=0, log=print):
     return losses
 
 
-def evaluate(net, seeds, ctx, conf_thr=CONF_THR, sweeps_learned=2, log=print, n_local=LOCAL_HYPS, span=LOCAL_SPAN):
+def evaluate(net, seeds, ctx, conf_thr=CONF_THR, sweeps_learned=2, log=print, n_local=LOCAL_HYPS, span=LOCAL_SPAN,
+             flags=None):
     """On held-out scenes: the plain method with 6 sweeps, the plain method
     with `sweeps_learned` sweeps (what the network's init replaces it with),
     and learned init + `sweeps_learned` sweeps.  Reports stereo views/s (CUDA
@@ -211,6 +246,8 @@ def evaluate(net, seeds, ctx, conf_thr=CONF_THR, sweeps_learned=2, log=print, n_
     rows = []
     short = MvsOptions(max_dim=C4_OPTS.max_dim, num_sources=C4_OPTS.num_sources, sweeps=sweeps_learned,
                        num_hyp=C4_OPTS.num_hyp)
+    lopts = MvsOptions(max_dim=C4_OPTS.max_dim, num_sources=C4_OPTS.num_sources, sweeps=sweeps_learned,
+                       num_hyp=C4_OPTS.num_hyp, flags=LEARNED_FLAGS if flags is None else flags)
     for seed in seeds:
         sc = orbit_c4(seed)
         srcs, zr, _ = mvs.plan(sc.sparse, sc.views, C4_OPTS)
@@ -218,7 +255,7 @@ def evaluate(net, seeds, ctx, conf_thr=CONF_THR, sweeps_learned=2, log=print, n_
         ds = mvs.DeviceScene(sc.views, ctx)
         stream = torch.cuda.ExternalStream(ctx.stream)
         res = {}
-        for name, o in (("plain6", C4_OPTS), ("plain_short", short), ("learned", short)):
+        for name, o in (("plain6", C4_OPTS), ("plain_short", short), ("learned", lopts)):
             nl = 0
             for rep in range(2):  # the first run warms up
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

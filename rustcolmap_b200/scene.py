@@ -114,9 +114,26 @@ def _patches(rects_idx, prims, n, rng):
     return out
 
 
+_HOST_RENDERER = None
+
+
+def use_host_renderer(path):
+    """Renders through `path`, a host-only build of the same renderer
+    (scene.cu compiled as plain C++), instead of librcscene.so: for CPU-only
+    programs that must not load the CUDA libraries.  device must then be -1."""
+    global _HOST_RENDERER
+    L = C.CDLL(path)
+    vp, i32 = C.c_void_p, C.c_int32
+    L.rcscene_render.argtypes = [vp, i32, vp, i32, vp, i32, i32, i32, vp, vp, vp]
+    L.rcscene_render.restype = C.c_int
+    L.rcscene_last_error.argtypes = []
+    L.rcscene_last_error.restype = C.c_char_p
+    _HOST_RENDERER = L
+
+
 def render(prims, patches, cams, supersample=2, device=-1, normals=False):
     """Ray-cast every camera: returns (gray list, depth list, normal list|None)."""
-    L = _lib.scene()
+    L = _HOST_RENDERER if _HOST_RENDERER is not None else _lib.scene()
     pa = (Prim * len(prims))(*prims)
     qa = (Patch * max(1, len(patches)))(*patches) if patches else None
     ca = (RCam * len(cams))(*cams)

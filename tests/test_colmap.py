@@ -202,6 +202,21 @@ def test_png_decoder_all_filters(tmp_path):
         colmap.read_png(str(tmp_path / "j.jpg"))
 
 
+def test_png_decoders_agree_on_every_filter(tmp_path):
+    """read_image decodes PNG with Pillow when it is installed; the pixels
+    must be read_png's for every filter type and channel count."""
+    pytest.importorskip("PIL")
+    rng = np.random.default_rng(5)
+    for c in (1, 2, 3, 4):
+        img = rng.integers(0, 256, (23, 31, c), dtype=np.uint8)
+        for filt in range(5):
+            p = tmp_path / f"y{c}{filt}.png"
+            p.write_bytes(_png(img, filt))
+            a = colmap._png_with_pillow(str(p))
+            assert a is not None and np.array_equal(a, colmap.read_png(str(p))), (c, filt)
+            assert np.array_equal(colmap.read_image(str(p)), img)
+
+
 def test_gray_rgb_conversion():
     rgb = np.array([[[255, 255, 255], [10, 20, 30], [0, 0, 255]]], np.uint8)
     g, out = colmap.gray_rgb(rgb)

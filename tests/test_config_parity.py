@@ -1,0 +1,129 @@
+"""GPU parity at the benchmark's own configurations.
+
+The stereo kernels are checked against the oracle on bands of rows of real
+reference views of the full-size scenes the benchmark runs (config 5: 1920
+wide, f = 2208, K = 10; config 2: 960x720, K = 8; config 3: a view with
+K = 12), so the geometry, source count and image size of the measured
+workload are the ones under test, at a cost the CPU oracle finishes in
+seconds.  A band is the view's rows [y0, y0 + rows) with the principal point
+moved up by y0 (its rays equal the full view's rows exactly); the source
+views stay whole.  Depth, cost and normal maps must be bit-identical, which
+meets the depth bar of at least 99% of valid pixels within 1e-3 relative
+inverse depth (reported too).  Fusion is checked at config-5 scale on the
+consistency stage of two reference views against all 100 depth maps."""
+import copy
+
+import numpy as np
+import pytest
+
+from oracle import oracle
+from rustcolmap_b200 import MvsOptions, mvs, scene
+
+pytestmark = pytest.mark.gpu
+
+# the benchmark's scenes (bench.py configs(), seed 5)
+C5 = dict(n_views=100, sizes=((1920, 1080),), f_rel=1.15, n_boxes=60, n_spheres=10)
+C2 = dict(n_views=64, sizes=((960, 720),), f_rel=1.1, n_boxes=20, n_spheres=0)
+C3 = dict(n_views=48, sizes=((480, 360), (480, 270), (720, 540), (720, 405), (960, 720), (960, 540),
+                             (1440, 1080), (1440, 810), (1920, 1440), (1920, 1080)),
+          f_rel=1.1, n_boxes=20, n_spheres=0, size_choice="random")
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = mvs.Context(0)
+    yield c
+    c.close()
+
+
+@pytest.fixture(scope="module")
+def c5_scene():
+    return scene.orbit_room(seed=5, device=0, per_view_sparse=300, **C5)
+
+
+def _band(views, ref, srcs, y0, rows):
+    """The views a band job needs: the band of the reference view, then its
+    sources whole; returns (views, 0, [1..K])."""
+    v = views[ref]
+    b = copy.copy(v)
+    b.gray = np.ascontiguousarray(v.gray[y0:y0 + rows])
+    b.rgb = np.ascontiguousarray(v.rgb[y0:y0 + rows])
+    b.h = b.gray.shape[0]
+    b.cam = type(v.cam)(v.cam.f, v.cam.cx, v.cam.cy - y0, v.cam.k)
+    return [b] + [views[s] for s in srcs], 0, list(range(1, len(srcs) + 1))
+
+
+def _within_1e3(a, b):
+    """Fraction of pixels valid in the oracle's map whose inverse depth in
+    `a` is within 1e-3 (relative) of the oracle's."""
+    v = b > 0
+    if not v.any():
+        return 1.0
+    with np.errstate(divide="ignore", invalid="ignore"):
+        rel = np.abs(1.0 / a[v] - 1.0 / b[v]) * b[v]
+    return float((rel <= 1e-3).mean())
+
+
+def _check_band(ctx, views, ref, srcs, zmin, zmax, opts, y0, rows):
+    bv, r, s = _band(views, ref, srcs, y0, rows)
+    g = mvs.estimate_depth(bv, r, s, zmin, zmax, opts, ctx=ctx, normals=True)
+    d, c, n, _ = oracle.estimate_depth(bv, r, s, zmin, zmax, opts)
+    assert _within_1e3(g.depth, d) >= 0.99
+    assert np.array_equal(g.depth.view(np.uint32), d.view(np.uint32)), "depth"
+    assert np.array_equal(g.cost.view(np.uint32), c.view(np.uint32)), "cost"
+    assert np.array_equal(g.normal.view(np.uint32), n.view(np.uint32)), "normal"
+    assert (d > 0).mean() > 0.05, "the band should hold valid depths"
+
+
+C5_OPTS = MvsOptions(max_dim=1920, num_sources=10, sweeps=6, num_hyp=64, min_consistent=3, depth_diff=0.01,
+                     reproj_px=1.0)
+
+
+@pytest.mark.parametrize("y0", [0, 528, 1056])  # top border, centre, bottom border
+def test_c5_bands_match_oracle(ctx, c5_scene, y0):
+    srcs, zr, _ = mvs.plan(c5_scene.sparse, c5_scene.views, C5_OPTS)
+    ref = 37
+    assert len(srcs[ref]) == 10
+    _check_band(ctx, c5_scene.views, ref, srcs[ref], zr[ref, 0], zr[ref, 1], C5_OPTS, y0, 24)
+
+
+def test_c2_band_matches_oracle(ctx):
+    sc = scene.orbit_room(seed=5, device=0, per_view_sparse=300, **C2)
+    opts = MvsOptions(max_dim=960, num_sources=8, sweeps=6, num_hyp=64)
+    srcs, zr, _ = mvs.plan(sc.sparse, sc.views, opts)
+    ref = 11
+    assert len(srcs[ref]) == 8
+    _check_band(ctx, sc.views, ref, srcs[ref], zr[ref, 0], zr[ref, 1], opts, 344, 32)
+
+
+def test_c3_view_with_twelve_sources_matches_oracle(ctx):
+    sc = scene.orbit_room(seed=5, device=0, per_view_sparse=300, **C3)
+    opts = MvsOptions(max_dim=1920, num_sources=12, sweeps=6, num_hyp=64)
+    srcs, zr, _ = mvs.plan(sc.sparse, sc.views, opts)
+    ref = next(i for i in range(len(sc.views)) if len(srcs[i]) == 12 and sc.views[i].w >= 960)
+    v = sc.views[ref]
+    _check_band(ctx, sc.views, ref, srcs[ref], zr[ref, 0], zr[ref, 1], opts, v.h // 2 - 16, 32)
+
+
+def test_c5_fusion_candidates_match_oracle(ctx, c5_scene):
+    """Consistency stage at config-5 scale: candidates of two reference views
+    checked against all 100 depth maps (>= 3 consistent views, 1% depth,
+    1 px reprojection), bit for bit and in the same order."""
+    views = c5_scene.views
+    opts = MvsOptions(max_dim=1920, num_sources=10, sweeps=1, num_hyp=32, min_consistent=3, depth_diff=0.01,
+                      reproj_px=1.0)
+    srcs, zr, fus = mvs.plan(c5_scene.sparse, views, opts)
+    jobs = [(i, srcs[i], zr[i, 0], zr[i, 1]) for i in range(len(views)) if srcs[i]]
+    ds = mvs.DeviceScene(views, ctx)
+    ds.estimate(jobs, opts)
+    maps = [None] * len(views)
+    for j in jobs:
+        maps[j[0]] = ds.depth(j[0]).depth
+    refs = [0, 63]
+    gx, grgb, gper = ds.fuse_candidates(fus, refs, opts)
+    off = np.cumsum([0] + [len(f) for f in fus])
+    ox, orgb, oper = oracle.fuse_candidates(views, maps, off, [x for f in fus for x in f], refs, opts)
+    assert np.array_equal(gper, oper)
+    assert np.array_equal(gx.view(np.uint64), ox.view(np.uint64)) and np.array_equal(grgb, orgb)
+    assert len(gx) > 100_000, "the two views should fuse many candidates"
+    ds.close()

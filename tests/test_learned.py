@@ -2,6 +2,8 @@
 construction, GPU checks of the tensor-core network kernels against the
 oracle, of the cost volume against a numpy restatement, and of the seeded
 stereo."""
+import os
+
 import numpy as np
 import pytest
 
@@ -219,3 +221,174 @@ def test_run_mvs_learned_without_confident_pixels_equals_run_mvs(ctx, corner_sce
     _, xb, cb = mvs.run_mvs(corner_scene.views, corner_scene.sparse, c1_opts, ctx=ctx, net=net, conf_thr=2.0)
     assert np.array_equal(xa, xb) and np.array_equal(ca, cb)
     net.close()
+
+
+# ---------------------------------------------------- learned init vs oracle
+def _seeded_scene():
+    """A config-4 style scene (room + 20 boxes, views about 8.6 degrees
+    apart) at 480x360, small enough for the oracle."""
+    return scene.orbit_room(seed=6003, n_views=8, sizes=((480, 360),), f_rel=1.1, n_boxes=20, n_spheres=0,
+                            device=0, per_view_sparse=300, arc_deg=60.0)
+
+
+def _assert_same_maps(ds, views, jobs, opts, pred_host, conf_thr, n_local, span):
+    """GPU maps of every job equal the oracle's seeded estimate_depth bit for
+    bit; returns the oracle's seeded pixel count."""
+    n_orc = 0
+    for k, (ref, s, z0, z1) in enumerate(jobs):
+        d, c, nrm, ns = oracle.estimate_depth_seeded(views, ref, s, z0, z1, opts, pred_host[k], conf_thr,
+                                                     n_local, span)
+        g = ds.depth(ref, normals=True)
+        assert np.array_equal(g.depth.view(np.uint32), d.view(np.uint32)), f"depth of view {ref}"
+        assert np.array_equal(g.cost.view(np.uint32), c.view(np.uint32)), f"cost of view {ref}"
+        assert np.array_equal(g.normal.view(np.uint32), nrm.view(np.uint32)), f"normal of view {ref}"
+        n_orc += ns
+    return n_orc
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("flags", [32, 32 | 64, 0, 64])  # init only / init with seed-and-sweep / + 2 sweeps
+def test_learned_init_with_committed_weights_matches_oracle(ctx, flags):
+    """The learned init (confident cells start from the network's plane on
+    the cell's anchor ray, the rest run the sweep) and the passes after it,
+    seeded by the committed network on a real scene, equal the oracle."""
+    import dataclasses
+    sc = _seeded_scene()
+    opts = MvsOptions(max_dim=4096, num_sources=4, sweeps=2, num_hyp=64, flags=flags)
+    srcs, zr, _ = mvs.plan(sc.sparse, sc.views, opts)
+    jobs = [(i, srcs[i], zr[i, 0], zr[i, 1]) for i in (1, 4, 6) if srcs[i]]
+    assert len(jobs) == 3
+    ds = mvs.DeviceScene(sc.views, ctx)
+    net = learned.ProposalNet(ctx, params=learned.load_weights())
+    pred = learned.predict(ds, jobs, net)
+    n_gpu = learned.estimate_seeded(ds, jobs, opts, pred, conf_thr=learned.CONF_THR)
+    n_orc = _assert_same_maps(ds, sc.views, jobs, opts, pred.cpu().numpy(), learned.CONF_THR, 1, 0.0)
+    assert n_gpu == n_orc
+    npx = sum(sc.views[j[0]].w * sc.views[j[0]].h for j in jobs)
+    assert n_gpu > 0.5 * npx, "the committed network should seed most pixels of this scene"
+    # the network path (cost volume -> network -> init) gives the same bits
+    ds2 = mvs.DeviceScene(sc.views, ctx)
+    assert learned.estimate_learned(ds2, jobs, dataclasses.replace(opts), net) == n_gpu
+    for j in jobs:
+        a, b = ds.depth(j[0], normals=True), ds2.depth(j[0], normals=True)
+        assert np.array_equal(a.depth.view(np.uint32), b.depth.view(np.uint32))
+        assert np.array_equal(a.cost.view(np.uint32), b.cost.view(np.uint32))
+    ds.close()
+    ds2.close()
+    net.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("w,h,n_local,span,flags", [(98, 71, 3, 0.2, 32), (98, 71, 3, 0.2, 0),
+                                                    (101, 64, 1, 0.0, 64), (64, 43, 5, 1.0, 32 | 64)])
+def test_learned_init_random_proposals_match_oracle(ctx, w, h, n_local, span, flags):
+    """Random proposals exercise every branch of the learned init: logits
+    around the threshold and NaN, degenerate normals, normals facing away
+    (n . ray < 0.1 at the pixel or the anchor), t outside [0, 1] (negative
+    inverse depth, depths outside [zmin/2, 2 zmax]), several local planes,
+    and view sizes that are not multiples of 4 (clamped quarter cells)."""
+    sc = scene.corner_room(seed=9, n_views=4, w=w, h=h, f=1.2 * w, arc_deg=36.0, n_patches=30,
+                           per_view_sparse=80, device=0)
+    opts = MvsOptions(max_dim=4096, num_sources=2, sweeps=1, num_hyp=24, flags=flags)
+    srcs, zr, _ = mvs.plan(sc.sparse, sc.views, opts)
+    jobs = [(i, srcs[i], zr[i, 0], zr[i, 1]) for i in range(4) if srcs[i]]
+    assert jobs
+    rng = np.random.default_rng(w * 1000 + h + n_local)
+    hq, wq = h // 4, w // 4
+    pred = np.zeros((len(jobs), hq, wq, 16), np.float32)
+    pred[..., 0] = rng.uniform(-1.5, 2.0, size=(len(jobs), hq, wq))
+    nrm = rng.normal(size=(len(jobs), hq, wq, 3))
+    nrm[..., 2] = np.abs(nrm[..., 2]) + 0.3
+    nrm[rng.uniform(size=(len(jobs), hq, wq)) < 0.15] *= -1  # facing away
+    nrm[rng.uniform(size=(len(jobs), hq, wq)) < 0.05] = 0  # degenerate
+    pred[..., 1:4] = nrm * rng.uniform(0.2, 3.0, size=(len(jobs), hq, wq, 1))
+    pred[..., 4] = rng.normal(0.0, 2.0, size=(len(jobs), hq, wq))
+    pred[..., 4][rng.uniform(size=(len(jobs), hq, wq)) < 0.03] = np.nan
+    conf = 0.3
+    # a logit exactly at the threshold counts as confident
+    pred[:, 0, 0, 4] = oracle.logit_threshold(conf)
+    pred[..., 5:] = rng.normal(size=(len(jobs), hq, wq, 11))  # unused channels
+    ds = mvs.DeviceScene(sc.views, ctx)
+    n_gpu = learned.estimate_seeded(ds, jobs, opts, pred, conf_thr=conf, n_local=n_local, span=span)
+    n_orc = _assert_same_maps(ds, sc.views, jobs, opts, pred, conf, n_local, span)
+    assert n_gpu == n_orc and 0 < n_gpu < sum(sc.views[j[0]].w * sc.views[j[0]].h for j in jobs)
+    ds.close()
+
+
+def test_logit_threshold_oracle():
+    assert oracle.logit_threshold(0.5) == 0.0
+    assert oracle.logit_threshold(0.0) == -np.inf and oracle.logit_threshold(-1.0) == -np.inf
+    assert oracle.logit_threshold(1.0) == np.inf and oracle.logit_threshold(2.0) == np.inf
+    c = float(np.float32(0.02))  # the threshold arrives as an f32
+    assert oracle.logit_threshold(0.02) == np.float32(np.log(c / (1.0 - c)))
+
+
+def _tiny_views():
+    from conftest import golden_views
+    return golden_views(dict(np.load(os.path.join(os.path.dirname(__file__), "golden", "tiny_corner.npz"))))
+
+
+def test_seeded_oracle_without_proposals_is_the_plain_oracle():
+    """With no usable proposal (threshold above every logit, or degenerate
+    normals) the seeded oracle is estimate_depth itself, bit for bit."""
+    views = _tiny_views()
+    v = views[0]
+    opts = MvsOptions(max_dim=4096, num_sources=2, sweeps=1, num_hyp=16)
+    d0, c0, n0, _ = oracle.estimate_depth(views, 0, [1, 2], 2.5, 9.0, opts)
+    rng = np.random.default_rng(3)
+    pred = rng.normal(size=(v.h // 4, v.w // 4, 16)).astype(np.float32)
+    d1, c1, n1, s1 = oracle.estimate_depth_seeded(views, 0, [1, 2], 2.5, 9.0, opts, pred, conf_thr=1.0)
+    pred0 = pred.copy()
+    pred0[..., 1:4] = 0
+    d2, c2, n2, s2 = oracle.estimate_depth_seeded(views, 0, [1, 2], 2.5, 9.0, opts, pred0, conf_thr=0.0)
+    assert s1 == 0 and s2 == 0
+    for d, c, n in ((d1, c1, n1), (d2, c2, n2)):
+        assert np.array_equal(d.view(np.uint32), d0.view(np.uint32))
+        assert np.array_equal(c.view(np.uint32), c0.view(np.uint32))
+        assert np.array_equal(n.view(np.uint32), n0.view(np.uint32))
+
+
+def test_seeded_oracle_selects_the_gated_proposals():
+    """The seeded pixel count equals a numpy restatement of the selection:
+    logit >= threshold, a non-degenerate normal, n . ray >= 0.1 at the pixel
+    and at its cell's anchor pixel (4qx+1, 4qy+1), and a depth inside
+    [zmin/2, 2 zmax] for the one local plane."""
+    views = _tiny_views()
+    v = views[0]
+    zmin, zmax = 2.5, 9.0
+    opts = MvsOptions(max_dim=4096, num_sources=2, sweeps=1, num_hyp=8, flags=32)
+    rng = np.random.default_rng(11)
+    hq, wq = v.h // 4, v.w // 4
+    pred = np.zeros((hq, wq, 16), np.float32)
+    pred[..., 0] = rng.uniform(-0.5, 1.5, size=(hq, wq))
+    nrm = rng.normal(size=(hq, wq, 3))
+    nrm[..., 2] = np.abs(nrm[..., 2])
+    pred[..., 1:4] = nrm
+    pred[..., 4] = rng.normal(0, 1.5, size=(hq, wq))
+    conf = 0.4
+    _, _, _, seeded = oracle.estimate_depth_seeded(views, 0, [1, 2], zmin, zmax, opts, pred, conf)
+    rx, ry = oracle.rays(v)
+    f32 = np.float32
+    thr = f32(oracle.logit_threshold(conf))
+    inv_min, inv_max = f32(1) / f32(zmax), f32(1) / f32(zmin)
+    zlo, zhi = f32(zmin) * f32(0.5), f32(zmax) * f32(2.0)
+    count = 0
+    for y in range(v.h):
+        for x in range(v.w):
+            qx, qy = min(x >> 2, wq - 1), min(y >> 2, hq - 1)
+            o = pred[qy, qx]
+            ln = f32(np.sqrt(f32(f32(o[1] * o[1]) + f32(o[2] * o[2])) + f32(o[3] * o[3])))
+            if not (o[4] >= thr and ln > f32(1e-6)):
+                continue
+            n = [f32(o[1] / ln), f32(o[2] / ln), f32(o[3] / ln)]
+            pa = f32(f32(f32(n[0] * rx[y, x]) + f32(n[1] * ry[y, x])) + n[2])
+            ay, ax = 4 * qy + 1, 4 * qx + 1
+            pac = f32(f32(f32(n[0] * rx[ay, ax]) + f32(n[1] * ry[ay, ax])) + n[2])
+            if not (pa >= f32(0.1) and pac >= f32(0.1)):
+                continue
+            inv = f32(inv_min + f32(o[0] * f32(inv_max - inv_min)))
+            if not inv > 0:
+                continue
+            zi = f32(f32(f32(f32(1) / inv) * pac) / pa)
+            count += bool(zlo <= zi <= zhi)
+    assert seeded == count and count > 0
