@@ -265,6 +265,16 @@ int rcmvs_write_ply_binary(const char* path, const double* xyz, const uint8_t* r
                            uint64_t n);
 
 
+/* The files `run_mvs` writes into <out>/dense after fusion
+ * (mvs/src/lib.rs:429-501): dense.ply (as rcmvs_write_ply_binary),
+ * dense_web.json (the decimated copy for web viewers: points farther from
+ * the centroid than the robust radius dropped, then every ceil(kept / cap)-th
+ * point, 4 decimals; none for an empty cloud) and, when stats is non-NULL,
+ * mvs_stats.json.  dense_dir must exist.  web_cap 0 = the reference's
+ * 400000.  Host only. */
+int rcmvs_write_dense_outputs(const char* dense_dir, const double* xyz, const uint8_t* rgb, uint64_t n,
+                              const rcmvs_stats* stats, uint64_t web_cap);
+
 /* Host glue of `run_mvs` (mvs/src/lib.rs:303-342, :358, :398-418):
  * co-visibility counts, top-K support views (count >= 10), per-view depth
  * range, fusion order (sources first).  Outputs (caller-allocated):

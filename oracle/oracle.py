@@ -7,6 +7,7 @@ does.  The oracle restates the reference `mvs` crate in C++
 Rust toolchain, no reference golden vectors) — see oracle/mvs_oracle.h.
 """
 import ctypes as C
+import math
 import os
 import subprocess
 
@@ -334,3 +335,34 @@ def plan(sparse, views, opts):
     srcs = [ss[so[i]:so[i + 1]].tolist() for i in range(n)]
     fus = [ff[fo[i]:fo[i + 1]].tolist() for i in range(n)]
     return srcs, zr, fus
+
+
+def web_json(xyz, rgb, cap=400_000):
+    """dense_web.json of run_mvs (mvs/src/lib.rs:434-485) in plain Python
+    floats (IEEE f64): the centroid as sequential sums, the robust radius
+    from the sorted distances, stride decimation of the kept points in the
+    cloud's order, 4-decimal positions.  None for an empty cloud."""
+    pts = [tuple(float(c) for c in p) for p in xyz]
+    n = len(pts)
+    if n == 0:
+        return None
+    cx = cy = cz = 0.0
+    for p in pts:
+        cx += p[0]
+    for p in pts:
+        cy += p[1]
+    for p in pts:
+        cz += p[2]
+    cx, cy, cz = cx / n, cy / n, cz / n
+    dist = [math.sqrt((p[0] - cx) * (p[0] - cx) + (p[1] - cy) * (p[1] - cy) + (p[2] - cz) * (p[2] - cz))
+            for p in pts]
+    sd = sorted(dist)
+    med = sd[n // 2]
+    p95 = sd[min(int(n * 0.95), n - 1)]
+    r_keep = med + 6.0 * max(abs(p95 - med), max(med, 1e-9) * 0.5)
+    kept = [i for i in range(n) if dist[i] <= r_keep]
+    stride = -(-len(kept) // cap)
+    web = kept[::stride]
+    pos = ",".join("[%.4f,%.4f,%.4f]" % pts[i] for i in web)
+    col = ",".join("[%d, %d,%d]" % tuple(int(c) for c in rgb[i]) for i in web)
+    return '{"n":' + str(len(web)) + ',"pos":[' + pos + '],"col":[' + col + ']}'

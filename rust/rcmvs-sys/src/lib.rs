@@ -231,6 +231,9 @@ pub fn rcmvs_options_default(opts: *mut rcmvs_options);
                              n_sparse: u64, opts: *const rcmvs_options, out: *mut rcmvs_points) -> c_int;
     /// fuse::write_ply_binary (mvs/src/fuse.rs:222-239), byte-identical.
     pub fn rcmvs_write_ply_binary(path: *const c_char, xyz: *const f64, rgb: *const u8, n: u64) -> c_int;
+    /// The files run_mvs writes into <out>/dense (mvs/src/lib.rs:429-501).
+    pub fn rcmvs_write_dense_outputs(dense_dir: *const c_char, xyz: *const f64, rgb: *const u8, n: u64,
+                                     stats: *const rcmvs_stats, web_cap: u64) -> c_int;
     /// run_mvs host glue: covisibility, sources, depth ranges, fusion order (mvs/src/lib.rs:224-282, 303-342, 398-418).
     pub fn rcmvs_plan(sparse: *const rcmvs_sparse, views: *const rcmvs_view, n_views: i32,
                       opts: *const rcmvs_options, src_offsets: *mut i32, srcs: *mut i32, zrange: *mut f64,

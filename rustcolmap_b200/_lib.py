@@ -46,6 +46,7 @@ def mvs():
         "rcmvs_estimate_depth_batch": ([vp, vp, i32, vp, i32, vp, vp], C.c_int),
         "rcmvs_fuse_depth_maps": ([vp, vp, i32, vp, vp, vp, vp, u64, vp, vp], C.c_int),
         "rcmvs_write_ply_binary": ([cp, vp, vp, u64], C.c_int),
+        "rcmvs_write_dense_outputs": ([cp, vp, vp, u64, vp, u64], C.c_int),
         "rcmvs_plan": ([vp, vp, i32, vp, vp, vp, vp, vp, vp], C.c_int),
         "rcmvs_run_mvs": ([vp, vp, i32, vp, vp, vp, vp, vp], C.c_int),
         "rcmvs_points_free": ([vp], None),
@@ -122,7 +123,7 @@ _SIG_NAMES = [
     "rcmvs_options_default", "rcmvs_ctx_create", "rcmvs_ctx_destroy", "rcmvs_last_error",
     "rcmvs_ctx_stream", "rcmvs_ctx_synchronize", "rcmvs_version", "rcmvs_census",
     "rcmvs_estimate_depth", "rcmvs_estimate_depth_batch", "rcmvs_fuse_depth_maps",
-    "rcmvs_write_ply_binary", "rcmvs_plan", "rcmvs_run_mvs", "rcmvs_points_free",
+    "rcmvs_write_ply_binary", "rcmvs_write_dense_outputs", "rcmvs_plan", "rcmvs_run_mvs", "rcmvs_points_free",
     "rcmvs_scene_create", "rcmvs_scene_destroy", "rcmvs_scene_prepare",
     "rcmvs_scene_estimate_depth", "rcmvs_scene_fuse", "rcmvs_scene_get_depth",
     "rcmvs_scene_get_census", "rcmvs_scene_get_points", "rcmvs_plane_cost_field",

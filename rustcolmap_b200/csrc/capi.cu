@@ -872,6 +872,77 @@ int rcmvs_fuse_candidates(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_vie
 }
 
 // mvs/src/fuse.rs:222-239
+// mvs/src/lib.rs:434-485: the decimated copy for web viewers.  Centroid as
+// sequential f64 sums, distances to it, the robust radius med + 6 *
+// max(|p95 - med|, max(med, 1e-9) / 2) from the sorted distances, then every
+// stride-th kept point (stride = ceil(kept / cap)), in the cloud's order.
+static int write_web_json(const std::string& path, const double* xyz, const uint8_t* rgb, uint64_t n,
+                          uint64_t cap) {
+    if (n == 0) return RCMVS_OK;  // the reference writes no file for an empty cloud
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    for (uint64_t i = 0; i < n; ++i) sx += xyz[3 * i];
+    for (uint64_t i = 0; i < n; ++i) sy += xyz[3 * i + 1];
+    for (uint64_t i = 0; i < n; ++i) sz += xyz[3 * i + 2];
+    const double cx = sx / (double)n, cy = sy / (double)n, cz = sz / (double)n;
+    std::vector<double> d(n);
+    for (uint64_t i = 0; i < n; ++i) {
+        const double dx = xyz[3 * i] - cx, dy = xyz[3 * i + 1] - cy, dz = xyz[3 * i + 2] - cz;
+        d[i] = std::sqrt(dx * dx + dy * dy + dz * dz);
+    }
+    std::vector<double> sd(d);
+    std::sort(sd.begin(), sd.end());
+    const double med = sd[n / 2];
+    const double p95 = sd[std::min<uint64_t>((uint64_t)((double)n * 0.95), n - 1)];
+    const double r_keep = med + 6.0 * std::max(std::fabs(p95 - med), std::max(med, 1e-9) * 0.5);
+    std::vector<uint64_t> kept;
+    for (uint64_t i = 0; i < n; ++i)
+        if (d[i] <= r_keep) kept.push_back(i);
+    const uint64_t stride = std::max<uint64_t>((kept.size() + cap - 1) / cap, 1);
+    std::vector<uint64_t> web;
+    for (uint64_t k = 0; k < kept.size(); k += stride) web.push_back(kept[k]);
+    std::string out = "{\"n\":" + std::to_string(web.size()) + ",\"pos\":[";
+    char tmp[128];
+    for (size_t k = 0; k < web.size(); ++k) {
+        const uint64_t i = web[k];
+        std::snprintf(tmp, sizeof(tmp), "%s[%.4f,%.4f,%.4f]", k ? "," : "", xyz[3 * i], xyz[3 * i + 1],
+                      xyz[3 * i + 2]);
+        out += tmp;
+    }
+    out += "],\"col\":[";
+    for (size_t k = 0; k < web.size(); ++k) {
+        const uint64_t i = web[k];
+        std::snprintf(tmp, sizeof(tmp), "%s[%u, %u,%u]", k ? "," : "", rgb[3 * i], rgb[3 * i + 1], rgb[3 * i + 2]);
+        out += tmp;
+    }
+    out += "]}";
+    FILE* f = std::fopen(path.c_str(), "wb");
+    if (!f) return RCMVS_E_IO;
+    const bool ok = std::fwrite(out.data(), 1, out.size(), f) == out.size();
+    return (std::fclose(f) == 0 && ok) ? RCMVS_OK : RCMVS_E_IO;
+}
+
+int rcmvs_write_dense_outputs(const char* dense_dir, const double* xyz, const uint8_t* rgb, uint64_t n,
+                              const rcmvs_stats* stats, uint64_t web_cap) {
+    if (!dense_dir || (n > 0 && (!xyz || !rgb))) return RCMVS_E_ARG;
+    const std::string dir(dense_dir);
+    int rc = rcmvs_write_ply_binary((dir + "/dense.ply").c_str(), xyz, rgb, n);
+    if (rc) return rc;
+    rc = write_web_json(dir + "/dense_web.json", xyz, rgb, n, web_cap ? web_cap : 400000);
+    if (rc) return rc;
+    if (stats) {  // mvs/src/lib.rs:497-501
+        FILE* f = std::fopen((dir + "/mvs_stats.json").c_str(), "wb");
+        if (!f) return RCMVS_E_IO;
+        std::fprintf(f,
+                     "{\"views\": %llu, \"views_with_depth\": %llu, \"dense_points\": %llu, \"stereo_s\": %.1f, "
+                     "\"fuse_s\": %.1f, \"elapsed_s\": %.1f}",
+                     (unsigned long long)stats->views, (unsigned long long)stats->views_with_depth,
+                     (unsigned long long)stats->dense_points, (double)stats->stereo_s, (double)stats->fuse_s,
+                     (double)stats->elapsed_s);
+        if (std::fclose(f) != 0) return RCMVS_E_IO;
+    }
+    return RCMVS_OK;
+}
+
 int rcmvs_write_ply_binary(const char* path, const double* xyz, const uint8_t* rgb, uint64_t n) {
     if (!path || (n > 0 && (!xyz || !rgb))) return RCMVS_E_ARG;
     FILE* f = std::fopen(path, "wb");

@@ -440,25 +440,21 @@ class DeviceScene:
             pass
 
 
-def _web_json(xyz, rgb, path, cap=400_000):
-    """dense_web.json of run_mvs (lib.rs:437-485): robust-radius filter and
-    stride decimation to <= cap points (order follows the fused cloud)."""
-    n = len(xyz)
-    if n == 0:
-        return
-    c = xyz.sum(axis=0) / n
-    dists = np.sqrt(((xyz - c) ** 2).sum(axis=1))
-    sd = np.sort(dists)
-    med = sd[n // 2]
-    p95 = sd[min(int(n * 0.95), n - 1)]
-    r_keep = med + 6.0 * max(abs(p95 - med), max(med, 1e-9) * 0.5)
-    keep = np.nonzero(dists <= r_keep)[0]
-    stride = -(-len(keep) // cap)
-    sel = keep[::max(stride, 1)]
-    pos = ",".join("[{:.4f},{:.4f},{:.4f}]".format(*xyz[i]) for i in sel)
-    col = ",".join("[{}, {},{}]".format(*rgb[i]) for i in sel)
-    with open(path, "w") as f:
-        f.write('{"n":' + str(len(sel)) + ',"pos":[' + pos + '],"col":[' + col + ']}')
+def write_dense_outputs(dense_dir, xyz, rgb, stats=None, web_cap=0):
+    """The files run_mvs writes (lib.rs:429-501): dense.ply, dense_web.json
+    and, with stats (an MvsStats), mvs_stats.json, by the library's writer."""
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+    rgb = np.ascontiguousarray(rgb, dtype=np.uint8).reshape(-1, 3)
+    st = None
+    if stats is not None:
+        st = _abi.Stats()
+        st.views, st.views_with_depth, st.dense_points = stats.views, stats.views_with_depth, stats.dense_points
+        st.fusion_candidates = stats.fusion_candidates
+        st.elapsed_s, st.stereo_s, st.fuse_s = stats.elapsed_s, stats.stereo_s, stats.fuse_s
+    rc = _lib.mvs().rcmvs_write_dense_outputs(os.fsencode(dense_dir), xyz.ctypes.data, rgb.ctypes.data, len(xyz),
+                                              C.byref(st) if st is not None else None, int(web_cap))
+    if rc != 0:
+        raise RcmvsError(rc, f"cannot write the dense outputs into {dense_dir}")
 
 
 def run_mvs(views, sparse, opts, out_dir=None, ctx=None, log=None, return_depth=False, net=None,
@@ -518,16 +514,10 @@ def run_mvs(views, sparse, opts, out_dir=None, ctx=None, log=None, return_depth=
     if out_dir is not None:
         dense = os.path.join(out_dir, "dense")
         os.makedirs(dense, exist_ok=True)
-        write_ply_binary(os.path.join(dense, "dense.ply"), xyz, rgb)
-        _web_json(xyz, rgb, os.path.join(dense, "dense_web.json"))
-        with open(os.path.join(dense, "mvs_stats.json"), "w") as f:
-            f.write('{"views": %d, "views_with_depth": %d, "dense_points": %d, "stereo_s": %.1f, '
-                    '"fuse_s": %.1f, "elapsed_s": %.1f}' % (stats.views, stats.views_with_depth,
-                                                            stats.dense_points, stats.stereo_s, stats.fuse_s,
-                                                            stats.elapsed_s))
+        write_dense_outputs(dense, xyz, rgb, stats)
     return (stats, xyz, rgb, dms) if return_depth else (stats, xyz, rgb)
 
 
 __all__ = ["Context", "default_context", "census_map", "estimate_depth", "estimate_depth_batch",
-           "fuse_depth_maps", "write_ply_binary", "depth_vis", "write_png_gray", "plan", "run_mvs", "plane_cost_field", "DeviceScene",
+           "fuse_depth_maps", "write_ply_binary", "write_dense_outputs", "depth_vis", "write_png_gray", "plan", "run_mvs", "plane_cost_field", "DeviceScene",
            "MvsOptions", "MvsStats", "ViewData", "DepthMap", "SparseModel", "RcmvsError"]

@@ -122,3 +122,29 @@ def test_package_has_no_cpu_fallback():
         for f in files:
             if f.endswith((".py", ".cu", ".cuh", ".cpp", ".h")):
                 assert "oracle" not in open(os.path.join(dirpath, f)).read().replace("the oracle", ""), f
+
+
+@pytest.mark.parametrize("n,cap", [(5000, 700), (5000, 0), (1, 0), (2, 1), (37, 5)])
+def test_dense_outputs_match_oracle(tmp_path, n, cap):
+    """dense_web.json (mvs/src/lib.rs:434-485) against the oracle's plain
+    Python restatement on a fixed-order cloud with outliers; dense.ply
+    against the PLY writer; mvs_stats.json's format."""
+    rng = np.random.default_rng(n + cap)
+    xyz = rng.normal(size=(n, 3)) * [2.0, 1.0, 0.5] + [10.0, -3.0, 4.0]
+    if n > 10:
+        xyz[:: max(n // 20, 1)] *= 40.0  # far outliers, dropped from the web copy
+    rgb = rng.integers(0, 256, (n, 3), dtype=np.uint8)
+    stats = mvs.MvsStats(views=12, views_with_depth=11, dense_points=n, per_view_valid=[], elapsed_s=3.25,
+                         stereo_s=1.04, fuse_s=0.96, fusion_candidates=0)
+    mvs.write_dense_outputs(str(tmp_path), xyz, rgb, stats, web_cap=cap)
+    assert open(tmp_path / "dense_web.json").read() == oracle.web_json(xyz, rgb, cap or 400_000)
+    oracle.write_ply_binary(str(tmp_path / "o.ply"), xyz, rgb)
+    assert open(tmp_path / "dense.ply", "rb").read() == open(tmp_path / "o.ply", "rb").read()
+    assert open(tmp_path / "mvs_stats.json").read() == (
+        '{"views": 12, "views_with_depth": 11, "dense_points": %d, "stereo_s": 1.0, "fuse_s": 1.0, '
+        '"elapsed_s": %.1f}' % (n, np.float32(3.25)))
+
+
+def test_dense_outputs_of_an_empty_cloud(tmp_path):
+    mvs.write_dense_outputs(str(tmp_path), np.zeros((0, 3)), np.zeros((0, 3), np.uint8))
+    assert (tmp_path / "dense.ply").exists() and not (tmp_path / "dense_web.json").exists()
