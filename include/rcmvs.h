@@ -356,6 +356,35 @@ int rcmvs_scene_fuse_candidates(rcmvs_ctx* ctx, rcmvs_scene* scene, const int32_
 /* Copies one view's maps to host buffers (any pointer may be NULL). */
 int rcmvs_scene_get_depth(rcmvs_ctx* ctx, rcmvs_scene* scene, int32_t view, float* depth,
                           float* cost, float* normal);
+/* Device-to-device moves of depth maps and fusion candidates, for callers
+ * that exchange them between GPUs themselves (one scene sharded over
+ * several processes, each with its own context; no reference counterpart).
+ * All are asynchronous on the context stream: synchronise it
+ * (rcmvs_ctx_synchronize) before another stream reads what they wrote, and
+ * make the writes of another stream visible before calling them.
+ *   rcmvs_scene_depth_to_device: one view's depth map (w*h f32) into a
+ *     caller device buffer (RCMVS_E_STATE if the view has none).
+ *   rcmvs_scene_set_depth: a view's depth map from a caller buffer (device
+ *     memory when on_device != 0, else host memory, copied before return);
+ *     the view then counts as having a map for fusion.
+ *   rcmvs_scene_fuse_candidates_device: rcmvs_scene_fuse_candidates with the
+ *     candidates kept in the scene; *n_out gets their count (this call
+ *     synchronises once to learn it), per_view (nullable) the count per view.
+ *   rcmvs_scene_candidates_to_device: the kept candidates (3 f64 + 3 u8
+ *     each, view-then-pixel order) into caller device buffers.
+ *   rcmvs_scene_fuse_reduce_device: the voxel dedup of rcmvs_fuse_reduce over
+ *     n device-resident candidates into the scene's fused cloud (read it with
+ *     rcmvs_scene_get_points); *n_points_out gets the count. */
+int rcmvs_scene_depth_to_device(rcmvs_ctx* ctx, rcmvs_scene* scene, int32_t view, float* depth_dev);
+int rcmvs_scene_set_depth(rcmvs_ctx* ctx, rcmvs_scene* scene, int32_t view, const float* depth,
+                          int32_t on_device);
+int rcmvs_scene_fuse_candidates_device(rcmvs_ctx* ctx, rcmvs_scene* scene, const int32_t* order_offsets,
+                                       const int32_t* order, const int32_t* ref_views, int32_t n_ref,
+                                       const rcmvs_options* opts, uint64_t* n_out, uint64_t* per_view);
+int rcmvs_scene_candidates_to_device(rcmvs_ctx* ctx, rcmvs_scene* scene, double* xyz_dev, uint8_t* rgb_dev);
+int rcmvs_scene_fuse_reduce_device(rcmvs_ctx* ctx, rcmvs_scene* scene, const double* xyz_dev,
+                                   const uint8_t* rgb_dev, uint64_t n, const double* sparse_xyz,
+                                   uint64_t n_sparse, const rcmvs_options* opts, uint64_t* n_points_out);
 /* Copies one view's census (w*h u64) to the host. */
 int rcmvs_scene_get_census(rcmvs_ctx* ctx, rcmvs_scene* scene, int32_t view,
                            uint64_t* census);

@@ -260,6 +260,19 @@ pub fn rcmvs_options_default(opts: *mut rcmvs_options);
                                        opts: *const rcmvs_options, out: *mut rcmvs_points, per_view: *mut u64) -> c_int;
     pub fn rcmvs_scene_get_depth(ctx: *mut rcmvs_ctx, scene: *mut rcmvs_scene, view: i32, depth: *mut f32,
                                  cost: *mut f32, normal: *mut f32) -> c_int;
+    /// Device-to-device moves of depth maps and fusion candidates (one scene over several processes).
+    pub fn rcmvs_scene_depth_to_device(ctx: *mut rcmvs_ctx, scene: *mut rcmvs_scene, view: i32, depth_dev: *mut f32) -> c_int;
+    pub fn rcmvs_scene_set_depth(ctx: *mut rcmvs_ctx, scene: *mut rcmvs_scene, view: i32, depth: *const f32,
+                                 on_device: i32) -> c_int;
+    pub fn rcmvs_scene_fuse_candidates_device(ctx: *mut rcmvs_ctx, scene: *mut rcmvs_scene,
+                                              order_offsets: *const i32, order: *const i32, ref_views: *const i32,
+                                              n_ref: i32, opts: *const rcmvs_options, n_out: *mut u64,
+                                              per_view: *mut u64) -> c_int;
+    pub fn rcmvs_scene_candidates_to_device(ctx: *mut rcmvs_ctx, scene: *mut rcmvs_scene, xyz_dev: *mut f64,
+                                            rgb_dev: *mut u8) -> c_int;
+    pub fn rcmvs_scene_fuse_reduce_device(ctx: *mut rcmvs_ctx, scene: *mut rcmvs_scene, xyz_dev: *const f64,
+                                          rgb_dev: *const u8, n: u64, sparse_xyz: *const f64, n_sparse: u64,
+                                          opts: *const rcmvs_options, n_points_out: *mut u64) -> c_int;
     pub fn rcmvs_scene_get_census(ctx: *mut rcmvs_ctx, scene: *mut rcmvs_scene, view: i32, census: *mut u64) -> c_int;
     pub fn rcmvs_scene_get_points(ctx: *mut rcmvs_ctx, scene: *mut rcmvs_scene, xyz: *mut f64, rgb: *mut u8,
                                   ply_body: *mut u8) -> c_int;

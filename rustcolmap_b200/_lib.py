@@ -57,6 +57,11 @@ def mvs():
         "rcmvs_scene_fuse": ([vp, vp, vp, vp, vp, u64, vp, vp], C.c_int),
         "rcmvs_scene_get_depth": ([vp, vp, i32, vp, vp, vp], C.c_int),
         "rcmvs_scene_get_census": ([vp, vp, i32, vp], C.c_int),
+        "rcmvs_scene_depth_to_device": ([vp, vp, i32, vp], C.c_int),
+        "rcmvs_scene_set_depth": ([vp, vp, i32, vp, i32], C.c_int),
+        "rcmvs_scene_fuse_candidates_device": ([vp, vp, vp, vp, vp, i32, vp, vp, vp], C.c_int),
+        "rcmvs_scene_candidates_to_device": ([vp, vp, vp, vp], C.c_int),
+        "rcmvs_scene_fuse_reduce_device": ([vp, vp, vp, vp, u64, vp, u64, vp, vp], C.c_int),
         "rcmvs_scene_get_points": ([vp, vp, vp, vp, vp], C.c_int),
         "rcmvs_plane_cost_field": ([vp, vp, i32, i32, vp, i32, vp, vp, vp, vp], C.c_int),
         "rcmvs_last_work": ([vp, vp, vp], C.c_int),
@@ -126,7 +131,8 @@ _SIG_NAMES = [
     "rcmvs_write_ply_binary", "rcmvs_write_dense_outputs", "rcmvs_plan", "rcmvs_run_mvs", "rcmvs_points_free",
     "rcmvs_scene_create", "rcmvs_scene_destroy", "rcmvs_scene_prepare",
     "rcmvs_scene_estimate_depth", "rcmvs_scene_fuse", "rcmvs_scene_get_depth",
-    "rcmvs_scene_get_census", "rcmvs_scene_get_points", "rcmvs_plane_cost_field",
+    "rcmvs_scene_get_census", "rcmvs_scene_get_points", "rcmvs_scene_depth_to_device", "rcmvs_scene_set_depth",
+    "rcmvs_scene_fuse_candidates_device", "rcmvs_scene_candidates_to_device", "rcmvs_scene_fuse_reduce_device", "rcmvs_plane_cost_field",
     "rcmvs_last_work", "rcmvs_selftest_f2i", "rcmvs_ctx_timing", "rcmvs_ctx_kernel_time",
     "rcmvs_estimate_depth_noalloc", "rcmvs_net_param_count", "rcmvs_net_create", "rcmvs_net_destroy",
     "rcmvs_net_get_params", "rcmvs_net_forward", "rcmvs_net_train_step", "rcmvs_scene_costvol",

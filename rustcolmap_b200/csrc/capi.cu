@@ -480,6 +480,28 @@ int rcmvs_scene_get_depth(rcmvs_ctx* ctx, rcmvs_scene* sc, int32_t view, float* 
     return RCMVS_OK;
 }
 
+int rcmvs_scene_depth_to_device(rcmvs_ctx* ctx, rcmvs_scene* sc, int32_t view, float* depth_dev) {
+    if (!ctx || !sc || view < 0 || view >= sc->n_views || !depth_dev)
+        return fail(ctx, RCMVS_E_ARG, "rcmvs_scene_depth_to_device: bad argument");
+    if (!sc->has_depth[view]) return fail(ctx, RCMVS_E_STATE, "view has no depth map");
+    CK(cudaSetDevice(ctx->device));
+    const DevView& V = sc->views[view];
+    CK(cudaMemcpyAsync(depth_dev, sc->depth + V.off, 4 * (size_t)V.w * V.h, cudaMemcpyDeviceToDevice, ctx->stream));
+    return RCMVS_OK;
+}
+
+int rcmvs_scene_set_depth(rcmvs_ctx* ctx, rcmvs_scene* sc, int32_t view, const float* depth, int32_t on_device) {
+    if (!ctx || !sc || view < 0 || view >= sc->n_views || !depth)
+        return fail(ctx, RCMVS_E_ARG, "rcmvs_scene_set_depth: bad argument");
+    CK(cudaSetDevice(ctx->device));
+    const DevView& V = sc->views[view];
+    CK(cudaMemcpyAsync(sc->depth + V.off, depth, 4 * (size_t)V.w * V.h,
+                       on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
+    if (!on_device) CK(cudaStreamSynchronize(ctx->stream));  // the host buffer may go away on return
+    sc->has_depth[view] = 1;
+    return RCMVS_OK;
+}
+
 int rcmvs_scene_get_census(rcmvs_ctx* ctx, rcmvs_scene* sc, int32_t view, uint64_t* census) {
     if (!ctx || !sc || view < 0 || view >= sc->n_views || !census)
         return fail(ctx, RCMVS_E_ARG, "rcmvs_scene_get_census: bad argument");
@@ -641,6 +663,89 @@ int rcmvs_scene_fuse_candidates(rcmvs_ctx* ctx, rcmvs_scene* sc, const int32_t* 
         }
     }
     return take_points(ctx, gx, gc, n_cand, out);
+}
+
+int rcmvs_scene_fuse_candidates_device(rcmvs_ctx* ctx, rcmvs_scene* sc, const int32_t* order_offsets,
+                                       const int32_t* order, const int32_t* ref_views, int32_t n_ref,
+                                       const rcmvs_options* opts, uint64_t* n_out, uint64_t* per_view) {
+    if (!ctx || !sc || !order_offsets || !opts || !n_out || n_ref < 0 || (n_ref > 0 && !ref_views))
+        return fail(ctx, RCMVS_E_ARG, "rcmvs_scene_fuse_candidates_device: bad argument");
+    if (sc->ctx != ctx) return fail(ctx, RCMVS_E_ARG, "scene belongs to another context");
+    *n_out = 0;
+    sc->n_kept = 0;
+    sc->d_kept_xyz = nullptr;
+    sc->d_kept_rgb = nullptr;
+    const int n = sc->n_views;
+    std::vector<char> mask(n, 0);
+    for (int i = 0; i < n_ref; ++i) {
+        if (ref_views[i] < 0 || ref_views[i] >= n) return fail(ctx, RCMVS_E_ARG, "reference view out of range");
+        mask[ref_views[i]] = 1;
+    }
+    std::vector<FuseView> fv;
+    int rc = fuse_views(ctx, sc, order_offsets, order, &mask, fv);
+    if (rc) return rc;
+    CK(cudaSetDevice(ctx->device));
+    std::string err;
+    const uint32_t* cand = nullptr;
+    const double* pts = nullptr;
+    uint32_t n_cand = 0;
+    rc = fuse_candidates_device(sc->arena, fv.data(), n, order, order_offsets[n], sc->depth, opts->min_consistent,
+                                opts->depth_diff, opts->reproj_px, &cand, &n_cand, &pts, ctx->stream, &err,
+                                ctx->hook());
+    if (rc) return fail(ctx, rc, err);
+    double* gx = nullptr;
+    uint8_t* gc = nullptr;
+    rc = fuse_gather_device(sc->arena, cand, n_cand, pts, sc->rgb, &gx, &gc, ctx->stream, &err);
+    if (rc) return fail(ctx, rc, err);
+    if (per_view) {
+        std::vector<uint32_t> idx(n_cand);
+        if (n_cand) CK(cudaMemcpyAsync(idx.data(), cand, 4 * (size_t)n_cand, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        size_t c = 0;
+        for (int v = 0; v < n; ++v) {
+            const uint64_t end = (uint64_t)sc->views[v].off + (uint64_t)sc->views[v].w * sc->views[v].h;
+            uint64_t k = 0;
+            while (c < idx.size() && idx[c] < end) {
+                ++c;
+                ++k;
+            }
+            per_view[v] = k;
+        }
+    }
+    sc->n_kept = n_cand;
+    sc->d_kept_xyz = gx;
+    sc->d_kept_rgb = gc;
+    *n_out = n_cand;
+    return RCMVS_OK;
+}
+
+int rcmvs_scene_candidates_to_device(rcmvs_ctx* ctx, rcmvs_scene* sc, double* xyz_dev, uint8_t* rgb_dev) {
+    if (!ctx || !sc || (sc->n_kept > 0 && (!xyz_dev || !rgb_dev)))
+        return fail(ctx, RCMVS_E_ARG, "rcmvs_scene_candidates_to_device: bad argument");
+    if (sc->n_kept == 0) return RCMVS_OK;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemcpyAsync(xyz_dev, sc->d_kept_xyz, 24 * sc->n_kept, cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(rgb_dev, sc->d_kept_rgb, 3 * sc->n_kept, cudaMemcpyDeviceToDevice, ctx->stream));
+    return RCMVS_OK;
+}
+
+int rcmvs_scene_fuse_reduce_device(rcmvs_ctx* ctx, rcmvs_scene* sc, const double* xyz_dev, const uint8_t* rgb_dev,
+                                   uint64_t n, const double* sparse_xyz, uint64_t n_sparse,
+                                   const rcmvs_options* opts, uint64_t* n_points_out) {
+    if (!ctx || !sc || (n > 0 && (!xyz_dev || !rgb_dev)) || !sparse_xyz || n_sparse == 0 || !opts || !n_points_out)
+        return fail(ctx, RCMVS_E_ARG, "rcmvs_scene_fuse_reduce_device: bad argument (sparse cloud must be non-empty)");
+    if (sc->ctx != ctx) return fail(ctx, RCMVS_E_ARG, "scene belongs to another context");
+    CK(cudaSetDevice(ctx->device));
+    const double cell = voxel_cell(sparse_xyz, n_sparse, opts->voxel_rel);
+    std::string err;
+    uint64_t np = 0;
+    int rc = fuse_reduce_devptr(sc->arena, xyz_dev, rgb_dev, n, cell, &sc->d_pts_xyz, &sc->d_pts_rgb, &sc->d_ply, &np,
+                                ctx->stream, &err, ctx->hook());
+    if (rc) return fail(ctx, rc, err);
+    sc->n_points = np;
+    sc->n_candidates = n;
+    *n_points_out = np;
+    return RCMVS_OK;
 }
 
 int rcmvs_fuse_reduce(rcmvs_ctx* ctx, const double* xyz, const uint8_t* rgb, uint64_t n, const double* sparse_xyz,

@@ -119,6 +119,10 @@ struct rcmvs_scene {
     double* d_pts_xyz = nullptr;
     uint8_t* d_pts_rgb = nullptr;
     uint8_t* d_ply = nullptr;
+    // candidates kept by rcmvs_scene_fuse_candidates_device (arena memory)
+    uint64_t n_kept = 0;
+    const double* d_kept_xyz = nullptr;
+    const uint8_t* d_kept_rgb = nullptr;
     // quarter-resolution copies for learned proposals (allocated on first use)
     bool have_quarter = false;
     std::vector<DevView> qviews;

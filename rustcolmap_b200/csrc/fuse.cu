@@ -528,6 +528,23 @@ int fuse_reduce_host(DeviceArena& A, const double* h_xyz, const uint8_t* h_rgb, 
                               cell, d_xyz, d_rgb, d_ply, n_points, st, err, hook);
 }
 
+int fuse_reduce_devptr(DeviceArena& A, const double* d_in_xyz, const uint8_t* d_in_rgb, uint64_t n, double cell,
+                       double** d_xyz, uint8_t** d_rgb, uint8_t** d_ply, uint64_t* n_points, cudaStream_t st,
+                       std::string* err, const SpanHook& hook) {
+    *n_points = 0;
+    if (n == 0) return RCMVS_OK;
+    if (n > (uint64_t)UINT32_MAX) {
+        *err = "fusion: more than 2^32 candidates";
+        return RCMVS_E_LIMIT;
+    }
+    void* p_iota;
+    FCK(A.get(S_IOTA, sizeof(uint32_t) * n, &p_iota));
+    iota_kernel<<<fgrid((uint32_t)n), FT, 0, st>>>((uint32_t*)p_iota, (uint32_t)n);
+    FCK(cudaGetLastError());
+    return fuse_reduce_device(A, (const uint32_t*)p_iota, (uint32_t)n, d_in_xyz, d_in_rgb, cell, d_xyz, d_rgb, d_ply,
+                              n_points, st, err, hook);
+}
+
 int fuse_gather_device(DeviceArena& A, const uint32_t* d_cand, uint32_t n, const double* pts, const uint8_t* rgb,
                        double** d_xyz, uint8_t** d_rgb, cudaStream_t st, std::string* err) {
     void *p_xyz, *p_rgb;

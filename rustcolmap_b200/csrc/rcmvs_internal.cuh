@@ -175,6 +175,11 @@ int fuse_reduce_host(DeviceArena& arena, const double* h_xyz, const uint8_t* h_r
                      double** d_xyz, uint8_t** d_rgb, uint8_t** d_ply, uint64_t* n_points, cudaStream_t st,
                      std::string* err, const SpanHook& hook);
 // The candidates' points and colours compacted in list order (device).
+// fuse_reduce_device over n device-resident candidates (3 doubles + 3
+// bytes each, caller memory), in the order given.
+int fuse_reduce_devptr(DeviceArena& arena, const double* d_in_xyz, const uint8_t* d_in_rgb, uint64_t n, double cell,
+                       double** d_xyz, uint8_t** d_rgb, uint8_t** d_ply, uint64_t* n_points, cudaStream_t st,
+                       std::string* err, const SpanHook& hook);
 int fuse_gather_device(DeviceArena& arena, const uint32_t* d_cand, uint32_t n, const double* pts,
                        const uint8_t* rgb, double** d_xyz, uint8_t** d_rgb, cudaStream_t st, std::string* err);
 

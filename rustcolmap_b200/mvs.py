@@ -403,6 +403,52 @@ class DeviceScene:
         xyz, rgb = _take_points(self.ctx, pts)
         return xyz, rgb, per_view
 
+    # device-to-device moves (one scene over several processes); ptr
+    # arguments are device addresses (e.g. torch CUDA tensors' data_ptr())
+    def depth_to_device(self, v, ptr):
+        """Enqueues a copy of view v's depth map into device memory at ptr."""
+        self.ctx.check(self.ctx._L.rcmvs_scene_depth_to_device(self.ctx.ptr, self.ptr, v, ptr))
+
+    def set_depth(self, v, depth):
+        """View v's depth map from a numpy array (copied before return) or a
+        device address (copied on the library's stream)."""
+        if isinstance(depth, np.ndarray):
+            d = np.ascontiguousarray(depth, dtype=np.float32)
+            assert d.size == self.views[v].w * self.views[v].h
+            self.ctx.check(self.ctx._L.rcmvs_scene_set_depth(self.ctx.ptr, self.ptr, v, d.ctypes.data, 0))
+        else:
+            self.ctx.check(self.ctx._L.rcmvs_scene_set_depth(self.ctx.ptr, self.ptr, v, int(depth), 1))
+
+    def fuse_candidates_device(self, fusion_order, ref_views, opts):
+        """fuse_candidates with the candidates kept on the device; returns
+        (count, per-view counts)."""
+        off, flat = _csr(fusion_order)
+        refs = np.array(list(ref_views) or [0], np.int32)
+        per_view = np.zeros(len(self.views), np.uint64)
+        n = C.c_uint64()
+        o = opts.to_c()
+        self.ctx.check(self.ctx._L.rcmvs_scene_fuse_candidates_device(self.ctx.ptr, self.ptr, off.ctypes.data,
+                                                                      flat.ctypes.data, refs.ctypes.data,
+                                                                      len(ref_views), C.byref(o), C.byref(n),
+                                                                      per_view.ctypes.data))
+        return n.value, per_view
+
+    def candidates_to_device(self, xyz_ptr, rgb_ptr):
+        """Enqueues copies of the kept candidates (n x 3 f64, n x 3 u8)."""
+        self.ctx.check(self.ctx._L.rcmvs_scene_candidates_to_device(self.ctx.ptr, self.ptr, xyz_ptr, rgb_ptr))
+
+    def fuse_reduce_device(self, xyz_ptr, rgb_ptr, n, sparse_xyz, opts):
+        """Voxel dedup of n device-resident candidates into the scene's cloud
+        (read with points()); returns the point count."""
+        sp = np.ascontiguousarray(sparse_xyz, dtype=np.float64)
+        npts = C.c_uint64()
+        o = opts.to_c()
+        self.ctx.check(self.ctx._L.rcmvs_scene_fuse_reduce_device(self.ctx.ptr, self.ptr, xyz_ptr, rgb_ptr, int(n),
+                                                                  sp.ctypes.data, len(sp), C.byref(o),
+                                                                  C.byref(npts)))
+        self.n_points = npts.value
+        return npts.value
+
     def depth(self, v, normals=False):
         w, h = self.views[v].w, self.views[v].h
         d = np.empty((h, w), np.float32)

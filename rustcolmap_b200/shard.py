@@ -21,6 +21,11 @@ Every rank takes the same collective steps in the same order.  The result
 is bit-identical to the single-GPU `mvs.run_mvs` (each view's stereo, each
 pixel's check and the dedup are the same computations; only where they run
 changes).
+
+Two data planes: `run_mvs_sharded_device` keeps the scene resident on each
+rank's GPU and moves depth maps and candidates device to device through the
+collectives (the NCCL path); `run_mvs_sharded` moves them through host
+arrays, with pluggable stereo/fusion back ends.
 """
 import numpy as np
 
@@ -177,6 +182,171 @@ def run_mvs_sharded(views, sparse, opts, group=None, ctx=None, stereo=None, cand
     cx, cc, per_view = candidates(depth, fus, sorted(r for r, _, _, _ in mine))
     ax, ac = all_gather_candidates(cx, cc, per_view, group=group, device=device)
     xyz, rgb = reduce(ax, ac)
+    return xyz, rgb, depth
+
+
+# ------------------------------------------------- device data plane
+class SceneOps:
+    """The scene operations the device data plane needs, on this rank's GPU
+    through the library (one DeviceScene kept for the whole run).  Tensors
+    passed in are CUDA tensors of this rank's device; the library works on
+    its own stream, so `sync()` separates its writes from the collectives'
+    reads, and the caller synchronises the collectives' stream before the
+    library reads what they wrote."""
+
+    def __init__(self, views, opts, ctx):
+        self.views, self.opts = views, opts
+        self.ds = mvs.DeviceScene(views, ctx)
+        self.ds.prepare()
+
+    def stereo(self, jobs):
+        if jobs:
+            self.ds.estimate(jobs, self.opts)
+
+    def depth_into(self, v, t):
+        self.ds.depth_to_device(v, t.data_ptr())
+
+    def set_depth(self, v, t):
+        self.ds.set_depth(v, t.data_ptr())
+
+    def candidates(self, fusion_order, refs):
+        return self.ds.fuse_candidates_device(fusion_order, refs, self.opts)
+
+    def candidates_into(self, xyz, rgb):
+        self.ds.candidates_to_device(xyz.data_ptr(), rgb.data_ptr())
+
+    def reduce(self, xyz, rgb, n, sparse_xyz):
+        self.ds.fuse_reduce_device(xyz.data_ptr(), rgb.data_ptr(), n, sparse_xyz, self.opts)
+        return self.ds.points()
+
+    def depth_host(self, v):
+        return self.ds.depth(v).depth
+
+    def sync(self):
+        self.ds.ctx.synchronize()
+
+    def close(self):
+        self.ds.close()
+
+
+def _stream_sync(device):
+    import torch
+    if torch.device(device).type == "cuda":
+        torch.cuda.current_stream(device).synchronize()
+
+
+def gather_maps_device(ops, shapes, owners, group=None, device="cuda"):
+    """All-gather of the per-view depth maps between devices: each rank's
+    maps go from its scene into one send tensor (device to device), one
+    all_gather moves every rank's tensor, and each received map goes into
+    this rank's scene (device to device).  No host copy of a map."""
+    import torch
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    per_rank = [sorted(v for v, o in owners.items() if o == r) for r in range(world)]
+    sizes = [sum(int(np.prod(shapes[v])) for v in views) for views in per_rank]
+    n = max(max(sizes), 1)
+    send = torch.zeros(n, dtype=torch.float32, device=device)
+    o = 0
+    for v in per_rank[rank]:
+        k = int(np.prod(shapes[v]))
+        ops.depth_into(v, send[o:o + k])
+        o += k
+    ops.sync()
+    parts = [torch.empty(n, dtype=torch.float32, device=device) for _ in range(world)]
+    dist.all_gather(parts, send, group=group)
+    _stream_sync(device)
+    for r in range(world):
+        if r == rank:
+            continue
+        o = 0
+        for v in per_rank[r]:
+            k = int(np.prod(shapes[v]))
+            ops.set_depth(v, parts[r][o:o + k])
+            o += k
+    ops.sync()
+    return parts  # kept alive until the library's copies have run
+
+
+def gather_candidates_device(ops, n_mine, per_view, group=None, device="cuda"):
+    """All-gather of the fusion candidates between devices, concatenated in
+    view order (the reference's accumulation order): one all_gather of the
+    per-view counts (small, read on the host to cut the pieces), one of the
+    positions (f64) and one of the colours (u8), each padded to the largest
+    rank's count.  Returns (xyz (N, 3) f64, rgb (N, 3) u8) tensors on
+    `device`, the same on every rank."""
+    import torch
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    nv = len(per_view)
+    head = torch.tensor([int(n_mine)] + [int(c) for c in per_view], dtype=torch.int64, device=device)
+    heads = [torch.empty(nv + 1, dtype=torch.int64, device=device) for _ in range(world)]
+    dist.all_gather(heads, head, group=group)
+    heads = [h.cpu().numpy() for h in heads]
+    n_max = max(1, max(int(h[0]) for h in heads))
+    sx = torch.zeros((n_max, 3), dtype=torch.float64, device=device)
+    sc = torch.zeros((n_max, 3), dtype=torch.uint8, device=device)
+    if n_mine:
+        ops.candidates_into(sx, sc)
+    ops.sync()
+    px = [torch.empty((n_max, 3), dtype=torch.float64, device=device) for _ in range(world)]
+    pc = [torch.empty((n_max, 3), dtype=torch.uint8, device=device) for _ in range(world)]
+    dist.all_gather(px, sx, group=group)
+    dist.all_gather(pc, sc, group=group)
+    pieces_x, pieces_c, cursor = [], [], [0] * world
+    for v in range(nv):
+        for r in range(world):
+            k = int(heads[r][1 + v])
+            if k:
+                pieces_x.append(px[r][cursor[r]:cursor[r] + k])
+                pieces_c.append(pc[r][cursor[r]:cursor[r] + k])
+                cursor[r] += k
+    if not pieces_x:
+        return (torch.zeros((0, 3), dtype=torch.float64, device=device),
+                torch.zeros((0, 3), dtype=torch.uint8, device=device))
+    ax, ac = torch.cat(pieces_x).contiguous(), torch.cat(pieces_c).contiguous()
+    _stream_sync(device)
+    return ax, ac
+
+
+def run_mvs_sharded_device(views, sparse, opts, group=None, ctx=None, device=None, ops=None, planner=None,
+                           return_depth=False):
+    """run_mvs_sharded with the data plane on the devices: the scene stays
+    resident on each rank's GPU from census to fusion, depth maps and
+    candidates move device to device through the collectives (NCCL over
+    NVLink with a `nccl` group), and the only host copy is the fused cloud
+    at the end.  Returns (xyz (n, 3) f64, rgb (n, 3) u8, depth maps or
+    None).  ops: the scene operations (default SceneOps, the library on this
+    rank's GPU; the CPU tests pass the oracle behind the same methods);
+    planner: the host glue (default the library's rcmvs_plan)."""
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    planner = planner or mvs.plan
+    srcs, zr, fus = planner(sparse, views, opts)
+    jobs = [(i, srcs[i], zr[i, 0], zr[i, 1]) for i in range(len(views)) if srcs[i]]
+    parts = assign_views(job_costs(jobs, views), world)
+    owners = {jobs[j][0]: r for r in range(world) for j in parts[r]}
+    mine = [jobs[j] for j in parts[rank]]
+    own = ops is None
+    if own:
+        ctx = ctx or mvs.default_context()
+        ops = SceneOps(views, opts, ctx)
+        device = device or f"cuda:{ctx.device}"
+    device = device or "cpu"
+    try:
+        ops.stereo(mine)
+        shapes = {r: (views[r].h, views[r].w) for r, _, _, _ in jobs}
+        keep = gather_maps_device(ops, shapes, owners, group=group, device=device)
+        n_mine, per_view = ops.candidates(fus, sorted(r for r, _, _, _ in mine))
+        ax, ac = gather_candidates_device(ops, n_mine, per_view, group=group, device=device)
+        xyz, rgb = ops.reduce(ax, ac, len(ax), sparse.xyz)
+        depth = [ops.depth_host(i) if i in shapes else None for i in range(len(views))] if return_depth else None
+        del keep
+    finally:
+        if own:
+            ops.close()
     return xyz, rgb, depth
 
 

@@ -290,3 +290,101 @@ def test_sfm_front_end_sharded_equals_single_process(world, sequential):
             assert np.array_equal(got[f"d{i}"].view(np.uint32), f.desc.view(np.uint32))
         for p, (a, b) in enumerate(ref):
             assert np.array_equal(got[f"a{p}"], a) and np.array_equal(got[f"b{p}"], b)
+
+
+# ------------------------------------------------- device data plane
+class _OracleOps:
+    """shard.SceneOps' interface with the CPU oracle behind it and CPU
+    tensors standing in for device memory (the gloo tests)."""
+
+    def __init__(self, sc, opts):
+        from oracle import oracle
+        self.o, self.sc, self.opts, self.maps = oracle, sc, opts, {}
+
+    def stereo(self, jobs):
+        for r, s, a, b in jobs:
+            self.maps[r] = self.o.estimate_depth(self.sc.views, r, s, a, b, self.opts, nthreads=1, normals=False)[0]
+
+    def depth_into(self, v, t):
+        import torch
+        t.copy_(torch.from_numpy(self.maps[v].ravel()))
+
+    def set_depth(self, v, t):
+        v_ = self.sc.views[v]
+        self.maps[v] = t.numpy().reshape(v_.h, v_.w).copy()
+
+    def candidates(self, order, refs):
+        off, flat = _csr(order)
+        depth = [self.maps.get(i) for i in range(len(self.sc.views))]
+        self.cx, self.cc, pv = self.o.fuse_candidates(self.sc.views, depth, off, flat, refs, self.opts, nthreads=1)
+        return len(self.cx), pv
+
+    def candidates_into(self, x, c):
+        import torch
+        n = len(self.cx)
+        x[:n] = torch.from_numpy(self.cx)
+        c[:n] = torch.from_numpy(self.cc)
+
+    def reduce(self, x, c, n, sparse_xyz):
+        return self.o.fuse_reduce(x.numpy(), c.numpy(), sparse_xyz, self.opts)
+
+    def depth_host(self, v):
+        return self.maps[v]
+
+    def sync(self):
+        pass
+
+
+def _device_plane_rank(rank, world, out):
+    from oracle import oracle
+    sc, opts = _tiny()
+    xyz, rgb, depth = shard.run_mvs_sharded_device(sc.views, sc.sparse, opts, ops=_OracleOps(sc, opts),
+                                                   planner=oracle.plan, device="cpu", return_depth=True)
+    np.savez(os.path.join(out, f"r{rank}.npz"), xyz=xyz, rgb=rgb,
+             **{f"d{i}": d for i, d in enumerate(depth) if d is not None})
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_device_data_plane_equals_single_process(world):
+    """The device data plane's steps (depth maps into one send tensor, one
+    all_gather, maps into every rank's scene; candidates counted, gathered
+    as f64 positions and u8 colours, cut and concatenated in view order,
+    deduped), run with the oracle behind the scene operations and CPU
+    tensors: every rank ends with the single-process maps and cloud."""
+    sc, opts = _tiny()
+    ref_depth, _, ref_xyz, ref_rgb = _reference_run(sc, opts)
+    out = _run_ranks(_device_plane_rank, world)
+    for r in range(world):
+        got = dict(np.load(os.path.join(out, f"r{r}.npz")))
+        assert np.array_equal(got["xyz"], ref_xyz) and np.array_equal(got["rgb"], ref_rgb)
+        for i, d in enumerate(ref_depth):
+            if d is not None:
+                assert np.array_equal(got[f"d{i}"].view(np.uint32), d.view(np.uint32))
+
+
+@pytest.mark.gpu
+def test_device_data_plane_on_one_gpu_equals_run_mvs():
+    """World size 1 on the GPU, an NCCL group, the library behind the scene
+    operations (depth maps and candidates through device tensors): run_mvs's
+    depth maps and cloud."""
+    import torch.distributed as dist
+    from rustcolmap_b200 import mvs
+    sc, opts = _tiny()
+    ctx = mvs.Context(0)
+    _, xa, ca, da = mvs.run_mvs(sc.views, sc.sparse, opts, ctx=ctx, return_depth=True)
+    import datetime
+
+    import torch
+    torch.cuda.set_device(0)
+    port = _free_port()
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=60), device_id=torch.device("cuda", 0))
+    try:
+        xb, cb, db = shard.run_mvs_sharded_device(sc.views, sc.sparse, opts, ctx=ctx, return_depth=True)
+    finally:
+        dist.destroy_process_group()
+    ctx.close()
+    assert np.array_equal(xa, xb) and np.array_equal(ca, cb)
+    for a, b in zip(da, db):
+        if b is not None:
+            assert np.array_equal(a.depth.view(np.uint32), b.view(np.uint32))
