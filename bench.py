@@ -436,6 +436,84 @@ def run_sfm(args):
         dist.destroy_process_group()
 
 
+def run_shard(args, cfg):
+    """--shard: ONE scene split over the N ranks (strong scaling): each rank
+    runs stereo (learned init + 2 sweeps) for its share of the reference
+    views, the depth maps and fusion candidates move device to device
+    through NCCL, and every rank dedups the same candidate list
+    (shard.run_mvs_sharded_device).  A step is the whole scene; value =
+    depth maps of the scene per second, max over ranks."""
+    import dataclasses
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    from rustcolmap_b200 import learned, mvs, shard
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if ws > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    else:  # one rank: the same collectives on a group of one
+        import socket
+        with socket.socket() as so:
+            so.bind(("127.0.0.1", 0))
+            port = so.getsockname()[1]
+        dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                                timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    opts = dataclasses.replace(cfg["opts"], sweeps=2)
+    sc = make_scene(cfg, seed=5, device=local)  # the same scene on every rank
+    n_maps = len(make_jobs(cfg, sc, opts)[0])
+    ctx = mvs.Context(local)
+    net = learned.ProposalNet(ctx, params=learned.load_weights())
+    ops = shard.SceneOps(sc.views, opts, ctx, net=net)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{local}")
+    out = {}
+
+    def step():
+        out["xyz"], out["rgb"], _ = shard.run_mvs_sharded_device(sc.views, sc.sparse, opts, ops=ops,
+                                                                  device=f"cuda:{local}")
+
+    for _ in range(args.warmup):
+        step()
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    dist.barrier()
+    clk = ClockSampler(local)
+    clk.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    e1.record(stream)  # every stream of the step has drained before this
+    e1.synchronize()
+    dist.barrier()
+    clocks = clk.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1), ws, local) / args.steps
+    value = n_maps / (ms / 1e3)
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "depth maps/s", "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong",
+                "vs_baseline": None, "dtype": "f32 (stereo), bf16/f32-acc (proposal net)", "data": "synthetic",
+                "config": {"workload": args.config + ": " + cfg["desc"], "views_per_step": n_maps,
+                           "parallelism": f"one scene sharded over {ws} rank(s): reference views by "
+                                         "longest-processing-time, depth maps and candidates all-gathered "
+                                         "device to device (NCCL)",
+                           "headline_arm": "learned init (proposal_c4 weights) + 2 sweeps"},
+                "fused_points": int(len(out["xyz"])),
+                "gpu_launches": args.steps * (1 + 3 + 6 + 1 + 2 * opts.sweeps + 1 + 5), "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    ops.close()
+    net.close()
+    ctx.close()
+    dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -459,6 +537,8 @@ def main():
     ap.add_argument("--flags", type=int, default=0,
                     help="RCMVS_FLAG_* bits for both arms (2 persistent queue, 4 CUDA graph, 8 autotuned tiles)")
     ap.add_argument("--tile", default="", help="WxH stereo tile (default: the library's 8x8)")
+    ap.add_argument("--shard", action="store_true",
+                    help="one scene split over the --gpus ranks (strong scaling; device-to-device exchanges)")
     args = ap.parse_args()
     assert args.warmup >= 3 or os.environ.get("RCMVS_BENCH_ALLOW_SHORT"), "warm-up must be >= 3 steps"
     if args.config == "sfm":
@@ -470,6 +550,9 @@ def main():
         cfg["desc"] += f" [{args.views} views]"
     if args.impl == "reference":
         run_reference(args, cfg)
+        return
+    if args.shard:
+        run_shard(args, cfg)
         return
 
     import dataclasses

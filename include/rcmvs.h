@@ -63,7 +63,10 @@ typedef struct rcmvs_options {
     uint32_t tile_w;         /* stereo tile width in pixels; 0 = default (8) */
     uint32_t tile_h;         /* stereo tile height in pixels; 0 = default (8) */
     uint32_t flags;          /* RCMVS_FLAG_* bits; 0 = defaults */
-    uint32_t reserved1;
+    uint32_t threads_per_pixel; /* Jacobi passes: 0 or 1 = one thread per pixel
+                                (default); 5 = five lanes per pixel, one per
+                                window column (tiles of at most 128 pixels).
+                                Same results bit for bit. */
 } rcmvs_options;
 
 /* The plane-sweep init evaluates each pixel's hypotheses one at a time, a
@@ -330,6 +333,8 @@ int rcmvs_scene_estimate_depth(rcmvs_ctx* ctx, rcmvs_scene* scene, const rcmvs_j
 typedef struct rcmvs_tune_entry {
     int32_t w, h;            /* resolution class */
     int32_t tile_w, tile_h;  /* chosen shape */
+    int32_t threads_per_pixel; /* of the passes: 1 or 5 */
+    int32_t reserved;
     float ms_best;           /* trial score of the chosen shape (ms) */
     float ms_default;        /* trial score of the 8x8 default (ms) */
 } rcmvs_tune_entry;

@@ -60,7 +60,7 @@ pub struct rcmvs_options {
     pub tile_w: u32,
     pub tile_h: u32,
     pub flags: u32,
-    pub reserved1: u32,
+    pub threads_per_pixel: u32,
 }
 
 /// One registered view at working resolution (`mvs::ViewData`).
@@ -137,6 +137,8 @@ pub struct rcmvs_tune_entry {
     pub h: i32,
     pub tile_w: i32,
     pub tile_h: i32,
+    pub threads_per_pixel: i32,
+    pub reserved: i32,
     pub ms_best: f32,
     pub ms_default: f32,
 }

@@ -34,7 +34,7 @@ class Options(C.Structure):
         ("tile_w", C.c_uint32),
         ("tile_h", C.c_uint32),
         ("flags", C.c_uint32),
-        ("reserved1", C.c_uint32),
+        ("threads_per_pixel", C.c_uint32),
     ]
 
 
@@ -65,7 +65,8 @@ class Job(C.Structure):
 
 class TuneEntry(C.Structure):
     _fields_ = [("w", C.c_int32), ("h", C.c_int32), ("tile_w", C.c_int32), ("tile_h", C.c_int32),
-                ("ms_best", C.c_float), ("ms_default", C.c_float)]
+                ("threads_per_pixel", C.c_int32), ("reserved", C.c_int32), ("ms_best", C.c_float),
+                ("ms_default", C.c_float)]
 
 
 class SiftOptions(C.Structure):

@@ -20,9 +20,11 @@ struct rcmvs_ctx {
     bool count_work = false;
     unsigned long long* d_work = nullptr;
     uint64_t last_evals = 0, last_rows = 0;
-    // autotuned tile shapes per resolution class, one thread count for all
+    // autotuned tile shapes per resolution class, one thread count and one
+    // threads-per-pixel of the passes for all
     std::vector<rcmvs_tune_entry> tuned;
     int tune_nthr = 0;
+    int tune_tpp = 1;
     // per-kernel CUDA-event spans (rcmvs_ctx_timing)
     struct Span {
         std::string name;

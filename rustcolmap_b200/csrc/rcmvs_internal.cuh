@@ -69,11 +69,15 @@ struct TileShape {
 // pulls tile indices from the counter until all `tiles` are taken;
 // otherwise block b computes tile b.
 struct LaunchGeom {
-    int nthr;
+    int nthr;  // threads of a one-thread-per-pixel block (= the largest tile's pixels)
     size_t smem;
     int tiles;
     unsigned int* queue;
+    int tpp = 1;  // threads per pixel of the passes: 1, or 5 (pass_split_kernel)
 };
+// Threads of a split-pass block (5 lanes per pixel, 6 pixels per warp) for
+// tiles of up to px pixels.
+int split_threads(int px);
 
 // ---------------------------------------------------------------- launchers
 // Defined in census.cu and stereo.cu.  All are asynchronous on the given

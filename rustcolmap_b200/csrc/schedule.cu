@@ -43,6 +43,9 @@ int sfail(rcmvs_ctx* ctx, int code, const std::string& msg) {
 float powf_host(float b, float e) { return powf(b, e); }
 
 bool shape_ok(TileShape ts) { return tile_shape_ok(ts); }
+// Split passes (5 lanes per pixel): at most 128 pixels, so a block of
+// split_threads(px) threads at the kernel's 80 registers fits an SM.
+bool split_shape_ok(TileShape ts) { return tile_shape_ok(ts) && ts.tw * ts.th <= 128; }
 TileShape fixed_shape(const rcmvs_options* o) { return default_tile_shape(o); }
 
 const rcmvs_tune_entry* find_class(const rcmvs_ctx* ctx, int w, int h) {
@@ -92,11 +95,12 @@ int assemble(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job* jobs, int n_jobs,
 // Plane-sweep init and one pass over jobs with every job at shape ts, timed
 // separately; *ms = the schedule's estimate, init + 2*max(sweeps,1) passes.
 int trial(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job* jobs, int n_jobs, const rcmvs_options* opts, TileShape ts,
-          cudaEvent_t e0, cudaEvent_t e1, cudaEvent_t e2, float* ms) {
+          int tpp, cudaEvent_t e0, cudaEvent_t e1, cudaEvent_t e2, float* ms) {
     StereoBatch b;
     std::vector<TileShape> shp(n_jobs, ts);
     int rc = assemble(ctx, sc, jobs, n_jobs, shp, false, b);
     if (rc) return rc;
+    b.geom.tpp = tpp;
     void *pj, *ps;
     SCK(sc->arena.get(kSlotTuneJobs, sizeof(DevJob) * n_jobs, &pj));
     SCK(sc->arena.get(kSlotTuneStart, sizeof(int32_t) * (n_jobs + 1), &ps));
@@ -131,7 +135,7 @@ int tune_missing(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job* jobs, int n_j
         int w, h;
         std::vector<rcmvs_job> jobs;
         int64_t px = 0;
-        float ms[kNumCandidates];
+        float ms[2][kNumCandidates];  // [one thread per pixel, split passes][shape]
     };
     std::vector<Class> cls;
     for (int j = 0; j < n_jobs; ++j) {
@@ -160,48 +164,57 @@ int tune_missing(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job* jobs, int n_j
     int rc = RCMVS_OK;
     for (auto& c : cls) {
         float warm = 0.f;  // first launch of a class pays for cold caches
-        rc = trial(ctx, sc, c.jobs.data(), (int)c.jobs.size(), opts, kCandidates[0], ev[0], ev[1], ev[2], &warm);
-        for (int k = 0; k < kNumCandidates && rc == RCMVS_OK; ++k) {
-            float best = INFINITY;
-            for (int rep = 0; rep < 2 && rc == RCMVS_OK; ++rep) {
-                float ms = 0.f;
-                rc = trial(ctx, sc, c.jobs.data(), (int)c.jobs.size(), opts, kCandidates[k], ev[0], ev[1], ev[2],
-                           &ms);
-                best = std::min(best, ms);
+        rc = trial(ctx, sc, c.jobs.data(), (int)c.jobs.size(), opts, kCandidates[0], 1, ev[0], ev[1], ev[2], &warm);
+        for (int t = 0; t < 2 && rc == RCMVS_OK; ++t)
+            for (int k = 0; k < kNumCandidates && rc == RCMVS_OK; ++k) {
+                c.ms[t][k] = INFINITY;
+                if (t == 1 && !split_shape_ok(kCandidates[k])) continue;
+                for (int rep = 0; rep < 2 && rc == RCMVS_OK; ++rep) {
+                    float ms = 0.f;
+                    rc = trial(ctx, sc, c.jobs.data(), (int)c.jobs.size(), opts, kCandidates[k], t ? 5 : 1, ev[0],
+                               ev[1], ev[2], &ms);
+                    c.ms[t][k] = std::min(c.ms[t][k], ms);
+                }
             }
-            c.ms[k] = best;
-        }
         if (rc) break;
     }
     for (auto& e : ev) cudaEventDestroy(e);
     if (rc) return rc;
-    if (ctx->tune_nthr == 0) {  // the thread count with the least summed best time
+    if (ctx->tune_nthr == 0) {  // the (thread count, threads per pixel) with the least summed best time
         double best_sum = INFINITY;
-        for (int nthr : {64, 256, 128, 32}) {
-            double sum = 0;
-            for (const auto& c : cls) {
-                float m = INFINITY;
-                for (int k = 0; k < kNumCandidates; ++k)
-                    if (kCandidates[k].tw * kCandidates[k].th == nthr) m = std::min(m, c.ms[k]);
-                sum += m;
+        for (int t = 0; t < 2; ++t)
+            for (int nthr : {64, 256, 128, 32}) {
+                double sum = 0;
+                for (const auto& c : cls) {
+                    float m = INFINITY;
+                    for (int k = 0; k < kNumCandidates; ++k)
+                        if (kCandidates[k].tw * kCandidates[k].th == nthr) m = std::min(m, c.ms[t][k]);
+                    sum += m;
+                }
+                if (sum < best_sum) {
+                    best_sum = sum;
+                    ctx->tune_nthr = nthr;
+                    ctx->tune_tpp = t ? 5 : 1;
+                }
             }
-            if (sum < best_sum) {
-                best_sum = sum;
-                ctx->tune_nthr = nthr;
-            }
-        }
     }
+    const int t = ctx->tune_tpp == 5 ? 1 : 0;
     for (const auto& c : cls) {
         int kb = -1;
         for (int k = 0; k < kNumCandidates; ++k)
-            if (kCandidates[k].tw * kCandidates[k].th == ctx->tune_nthr && (kb < 0 || c.ms[k] < c.ms[kb])) kb = k;
+            if (kCandidates[k].tw * kCandidates[k].th == ctx->tune_nthr && (kb < 0 || c.ms[t][k] < c.ms[t][kb])) kb = k;
+        if (!(c.ms[t][kb] < INFINITY)) {  // no split shape of this thread count: one thread per pixel
+            return sfail(ctx, RCMVS_E_STATE, "autotuner: no tile shape of the chosen kind for a class");
+        }
         rcmvs_tune_entry e;
+        std::memset(&e, 0, sizeof(e));
         e.w = c.w;
         e.h = c.h;
         e.tile_w = kCandidates[kb].tw;
         e.tile_h = kCandidates[kb].th;
-        e.ms_best = c.ms[kb];
-        e.ms_default = c.ms[0];
+        e.threads_per_pixel = ctx->tune_tpp;
+        e.ms_best = c.ms[t][kb];
+        e.ms_default = c.ms[0][0];
         ctx->tuned.push_back(e);
     }
     return RCMVS_OK;
@@ -266,6 +279,8 @@ void fill_job(const rcmvs_scene* sc, int ref, const int32_t* srcs, int n_src, do
 int build_batch(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job* jobs, int n_jobs, const rcmvs_options* opts,
                 StereoBatch& b) {
     std::vector<TileShape> shp(n_jobs, fixed_shape(opts));
+    int tpp = opts->threads_per_pixel <= 1 ? 1 : (int)opts->threads_per_pixel;
+    if (tpp != 1 && tpp != 5) return sfail(ctx, RCMVS_E_ARG, "threads_per_pixel must be 0, 1 or 5");
     if (opts->flags & RCMVS_FLAG_AUTOTUNE) {
         int rc = tune_missing(ctx, sc, jobs, n_jobs, opts);
         if (rc) return rc;
@@ -274,10 +289,15 @@ int build_batch(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job* jobs, int n_jo
             const rcmvs_tune_entry* e = find_class(ctx, V.w, V.h);
             if (e) shp[j] = TileShape{e->tile_w, e->tile_h};
         }
+        tpp = ctx->tune_tpp;
     } else if (!shape_ok(shp[0])) {
         return sfail(ctx, RCMVS_E_ARG, "tile shape must have tw*th <= 256 threads, a multiple of 32");
+    } else if (tpp == 5 && !split_shape_ok(shp[0])) {
+        return sfail(ctx, RCMVS_E_ARG, "threads_per_pixel 5 takes tiles of at most 128 pixels");
     }
-    return assemble(ctx, sc, jobs, n_jobs, shp, true, b);
+    int rc = assemble(ctx, sc, jobs, n_jobs, shp, true, b);
+    b.geom.tpp = tpp;
+    return rc;
 }
 
 void drop_graph(rcmvs_scene* sc) {
@@ -356,6 +376,7 @@ int run_batch(rcmvs_ctx* ctx, rcmvs_scene* sc, const StereoBatch& b, const Sched
     append(key, b.start.data(), sizeof(int32_t) * (n_jobs + 1));
     append(key, b.geom.nthr);
     append(key, b.geom.smem);
+    append(key, b.geom.tpp);
     append(key, (int)s.init);
     append(key, s.nh);
     append(key, s.n_passes);
@@ -438,11 +459,17 @@ int rcmvs_tune_table(rcmvs_ctx* ctx, rcmvs_tune_entry* out, int32_t cap, int32_t
 
 int rcmvs_tune_set(rcmvs_ctx* ctx, const rcmvs_tune_entry* entries, int32_t n) {
     if (!ctx || n < 0 || (n > 0 && !entries)) return sfail(ctx, RCMVS_E_ARG, "rcmvs_tune_set: bad argument");
-    for (int i = 0; i < n; ++i)
-        if (entries[i].w <= 0 || entries[i].h <= 0 || !shape_ok(TileShape{entries[i].tile_w, entries[i].tile_h}))
+    const int tpp = n > 0 && entries[0].threads_per_pixel == 5 ? 5 : 1;
+    for (int i = 0; i < n; ++i) {
+        const TileShape ts{entries[i].tile_w, entries[i].tile_h};
+        const int t = entries[i].threads_per_pixel <= 1 ? 1 : entries[i].threads_per_pixel;
+        if (entries[i].w <= 0 || entries[i].h <= 0 || !shape_ok(ts) || t != tpp || (tpp == 5 && !split_shape_ok(ts)))
             return sfail(ctx, RCMVS_E_ARG, "rcmvs_tune_set: bad entry " + std::to_string(i));
+    }
     ctx->tuned.assign(entries, entries + n);
+    for (auto& e : ctx->tuned) e.threads_per_pixel = tpp;
     ctx->tune_nthr = n > 0 ? entries[0].tile_w * entries[0].tile_h : 0;
+    ctx->tune_tpp = tpp;
     return RCMVS_OK;
 }
 

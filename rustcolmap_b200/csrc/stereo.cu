@@ -486,6 +486,205 @@ __global__ void __maxnreg__(72)
     if (COUNT) flush_work(wc, d_work);
 }
 
+// ---------------------------------------------------------------- split passes
+// The same pass with five lanes per pixel (threads per pixel = 5, an
+// autotuner axis): lane j of a pixel's group computes window column dx = j of
+// every row, the group exchanges the five Hamming counts by shuffles, and
+// every lane of the group adds them in dx order -- the reference's f32 chain,
+// each lane holding the same sum, so the abort test and all control flow stay
+// uniform within the group.  A lane keeps its column's source-independent
+// values (z = d / denom and z*ray, stereo.rs:187-195) for the five rows once
+// the first source has computed them, so later sources of the same candidate
+// skip the divide.  Six pixels per warp (lanes 30 and 31 idle); a tile of P
+// pixels runs in ceil(P / 6) warps.  Everything a pixel computes, and in
+// which order, is what pass_kernel computes: the results are bit-identical.
+constexpr int SPLIT = 5;     // lanes per pixel
+constexpr int SPLIT_PX = 6;  // pixels per warp
+
+template <bool COUNT>
+__device__ __forceinline__ float plane_cost_split(const Smem& sm, int stw, int lx, int ly, int j, unsigned gmask,
+                                                  int gbase, int nsrc, const uint64_t* __restrict__ census,
+                                                  float nx, float ny, float nz, float d, float hint, float total,
+                                                  WorkCount& wc) {
+    float sum = 0.f;
+    const float thr = hint + 0.12f;
+    if (COUNT && j == 0) wc.evals++;
+    float zc[5], xc[5], yc[5];
+    unsigned dok = 0;
+    for (int si = 0; si < nsrc; ++si) {
+        const SrcRegs s = load_src(sm.src[si], census);
+        const float fsi = (float)(si + 1);
+#pragma unroll
+        for (int dy = 0; dy < 5; ++dy) {
+            const int cell = (ly + dy) * stw + lx + j;
+            if (si == 0) {
+                const float2 r = sm.ray[cell];
+                const float denom = nx * r.x + ny * r.y + nz;
+                const float z = d / denom;
+                zc[dy] = z;
+                xc[dy] = z * r.x;
+                yc[dy] = z * r.y;
+                dok |= (denom < 0.05f ? 0u : 1u) << dy;
+            }
+            const float z = zc[dy], xr = xc[dy], yr = yc[dy];
+            const float xs = s.rs0 * xr + s.rs1 * yr + s.rs2 * z + s.ts0;
+            const float ys = s.rs3 * xr + s.rs4 * yr + s.rs5 * z + s.ts1;
+            const float zs = s.rs6 * xr + s.rs7 * yr + s.rs8 * z + s.ts2;
+            const float xn = xs / zs;
+            const float yn = ys / zs;
+            const float dist = 1.0f + s.k * (xn * xn + yn * yn);
+            int u, v;
+            const bool in_u = trunc_index(s.f * xn * dist + s.cx, s.swf, u);
+            const bool in_v = trunc_index(s.f * yn * dist + s.cy, s.shf, v);
+            const bool ok = ((dok >> dy) & 1u) && !(zs < 1e-3f) && in_u && in_v;
+            const uint64_t cs = __ldg(s.sc + (ok ? (size_t)v * s.sw + u : (size_t)0));
+            const int hv = __popcll(sm.cen[cell] ^ cs);
+            const int h = ok ? hv : 48;
+            // the row's five counts, added in dx order by every lane of the group
+#pragma unroll
+            for (int k = 0; k < SPLIT; ++k) sum += sm.tab[__shfl_sync(gmask, h, gbase + k)];
+            if (COUNT && j == 0) wc.rows++;
+            if (sum / ((float)(dy + 1) * 5.0f * fsi) > thr) return 1e9f;
+        }
+    }
+    return sum / total;
+}
+
+// 80 registers: a few bytes spill; 96 spill nothing but leave fewer warps
+// resident.
+template <bool COUNT, bool PERSIST>
+__global__ void __maxnreg__(80)
+    pass_split_kernel(const DevJob* __restrict__ jobs, const int32_t* __restrict__ job_start, int n_jobs, int tiles,
+                      unsigned int* queue, uint64_t pass, float sig_inv, float sig_n,
+                      const uint64_t* __restrict__ census, const float2* __restrict__ rays, PlaneBuf prev,
+                      PlaneBuf next, unsigned long long* d_work) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int s_tile;
+    WorkCount wc{0, 0};
+    const int lane = threadIdx.x & 31;
+    const int grp = lane / SPLIT, j = lane - grp * SPLIT;
+    const int gbase = grp * SPLIT;
+    const unsigned gmask = 0x1Fu << gbase;
+    const int p = (int)(threadIdx.x >> 5) * SPLIT_PX + grp;  // the group's pixel in the tile
+    for (int it = 0; PERSIST || it == 0; ++it) {
+        const int tile = PERSIST ? next_tile(queue, tiles, it, &s_tile) : (int)blockIdx.x;
+        if (tile < 0) break;
+        Smem sm;
+        Tile T;
+        load_tile(jobs, job_start, n_jobs, tile, census, rays, smem_raw, sm, T);
+        const DevJob* J = T.job;
+        const int lx = p % T.tw, ly = p / T.tw;
+        const int x = T.x0 + lx, y = T.y0 + ly;
+        const int w = J->w, h = J->h;
+        if (lane < SPLIT * SPLIT_PX && p < T.tw * T.th && x < w && y < h) {
+            const int nsrc = J->nsrc;
+            const float total = 5.0f * 5.0f * (float)nsrc;
+            const float inv_min = J->inv_min, inv_max = J->inv_max;
+            const float zlo = J->zmin * 0.5f, zhi = J->zmax * 2.0f;
+            const size_t base = (size_t)J->off;
+            const size_t i = base + (size_t)y * w + x;
+            const int stw = T.stw;
+            const float2 ri = sm.ray[(ly + HALO) * stw + lx + HALO];
+            uint64_t seed = pixel_rng(x, y, pass + 7);
+            const float4 cur = prev.nz[i];
+            const float cur_cost = prev.cost[i];
+            const bool skip_dup = prev.d != nullptr;
+            const float cur_d = skip_dup ? prev.d[i] : 0.f;
+            float best_c = cur_cost;
+            float bn0 = cur.x, bn1 = cur.y, bn2 = cur.z;
+            float bd = cur.w * (bn0 * ri.x + bn1 * ri.y + bn2);
+            auto neighbour = [&](int q, float4& nb, float& d_plane) -> bool {
+                const int ddx = q == 0 ? -1 : (q == 1 ? 1 : 0);
+                const int ddy = q == 2 ? -1 : (q == 3 ? 1 : 0);
+                const int xx = x + ddx, yy = y + ddy;
+                if (xx < 0 || yy < 0 || xx >= w || yy >= h) return false;
+                nb = prev.nz[base + (size_t)yy * w + xx];
+                const float2 rj = sm.ray[(ly + HALO + ddy) * stw + lx + HALO + ddx];
+                const float a_nb = nb.x * rj.x + nb.y * rj.y + nb.z;
+                if (a_nb < 0.1f) return false;
+                d_plane = nb.w * a_nb;
+                const float a_here = nb.x * ri.x + nb.y * ri.y + nb.z;
+                if (a_here < 0.1f) return false;
+                const float zcand = d_plane / a_here;
+                return zlo <= zcand && zcand <= zhi;
+            };
+            unsigned todo = 0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                float4 nb;
+                float d_plane;
+                if (!neighbour(q, nb, d_plane)) continue;
+                if (skip_dup && __float_as_uint(d_plane) == __float_as_uint(cur_d) &&
+                    __float_as_uint(nb.x) == __float_as_uint(cur.x) && __float_as_uint(nb.y) == __float_as_uint(cur.y) &&
+                    __float_as_uint(nb.z) == __float_as_uint(cur.z))
+                    continue;
+                todo |= 1u << q;
+            }
+#pragma unroll 1
+            while (todo) {
+                const int q = __ffs(todo) - 1;
+                todo &= todo - 1;
+                float4 nb;
+                float d_plane;
+                neighbour(q, nb, d_plane);
+                const float c = plane_cost_split<COUNT>(sm, stw, lx, ly, j, gmask, gbase, nsrc, census, nb.x, nb.y,
+                                                        nb.z, d_plane, best_c + 0.02f, total, wc);
+                if (c < best_c) {
+                    best_c = c;
+                    bn0 = nb.x;
+                    bn1 = nb.y;
+                    bn2 = nb.z;
+                    bd = d_plane;
+                }
+            }
+#pragma unroll 1
+            for (int r = 0; r < 3; ++r) {
+                const float inv = 1.0f / fmaxf(cur.w, 1e-6f);
+                const float inv_new = inv + sig_inv * (inv_max - inv_min) * gauss3(seed);
+                if (inv_new <= 0.0f) continue;
+                const float zcand = 1.0f / inv_new;
+                if (!(zlo <= zcand && zcand <= zhi)) continue;
+                float nnx = cur.x + sig_n * gauss3(seed);
+                float nny = cur.y + sig_n * gauss3(seed);
+                float nnz = cur.z + sig_n * gauss3(seed);
+                const float len = sqrtf(nnx * nnx + nny * nny + nnz * nnz);
+                if (len < 1e-6f) continue;
+                nnx = nnx / len;
+                nny = nny / len;
+                nnz = nnz / len;
+                const float a_here = nnx * ri.x + nny * ri.y + nnz;
+                if (a_here < 0.1f) continue;
+                const float d_plane = zcand * a_here;
+                const float c = plane_cost_split<COUNT>(sm, stw, lx, ly, j, gmask, gbase, nsrc, census, nnx, nny,
+                                                        nnz, d_plane, best_c + 0.02f, total, wc);
+                if (c < best_c) {
+                    best_c = c;
+                    bn0 = nnx;
+                    bn1 = nny;
+                    bn2 = nnz;
+                    bd = d_plane;
+                }
+            }
+            if (j == 0) {
+                float4 o = cur;
+                float oc = cur_cost, od = cur_d;
+                if (best_c < cur_cost) {  // stereo.rs:355-367
+                    const float a_here = bn0 * ri.x + bn1 * ri.y + bn2;
+                    if (a_here > 0.05f) {
+                        o = make_float4(bn0, bn1, bn2, bd / a_here);
+                        oc = fminf(best_c, 1.0f);
+                        od = bd;
+                    }
+                }
+                next.nz[i] = o;
+                next.cost[i] = oc;
+                if (skip_dup) next.d[i] = od;
+            }
+        }
+    }
+    if (COUNT) flush_work(wc, d_work);
+}
+
 // ---------------------------------------------------------------- row-step kernels
 // The same init and pass computations with per-thread candidate streams
 // advanced one 5-term window row per loop iteration: a lane whose candidate
@@ -826,6 +1025,9 @@ __global__ void f2i_kernel(const float* in, int n, int32_t* out) {
 
 size_t stereo_smem_bytes(TileShape ts) { return smem_bytes(ts.tw, ts.th); }
 
+// Threads of a split-pass block for tiles of up to `px` pixels.
+int split_threads(int px) { return 32 * ((px + SPLIT_PX - 1) / SPLIT_PX); }
+
 namespace {
 // Blocks of a persistent launch: as many as stay resident on all SMs at
 // once (the queue hands out the tiles), never more than there are tiles.
@@ -862,6 +1064,14 @@ template <bool COUNT, bool PERSIST>
 void pass_as(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, const LaunchGeom& g, uint64_t pass,
              float sig_inv, float sig_n, const uint64_t* census, const float2* rays, PlaneBuf prev, PlaneBuf next,
              unsigned long long* d_work, cudaStream_t st) {
+    if (g.tpp == SPLIT) {
+        LaunchGeom gs = g;
+        gs.nthr = split_threads(g.nthr);
+        pass_split_kernel<COUNT, PERSIST><<<launch_grid(pass_split_kernel<COUNT, PERSIST>, gs), gs.nthr, gs.smem,
+                                            st>>>(d_jobs, d_job_start, n_jobs, g.tiles, g.queue, pass, sig_inv, sig_n,
+                                                  census, rays, prev, next, d_work);
+        return;
+    }
     pass_kernel<COUNT, 3, PERSIST><<<launch_grid(pass_kernel<COUNT, 3, PERSIST>, g), g.nthr, g.smem, st>>>(
         d_jobs, d_job_start, n_jobs, g.tiles, g.queue, pass, sig_inv, sig_n, census, rays, prev, next, d_work);
 }

@@ -70,15 +70,15 @@ class Context:
         buf = (_abi.TuneEntry * 64)()
         n = C.c_int32()
         self.check(self._L.rcmvs_tune_table(self.ptr, buf, 64, C.byref(n)))
-        return [dict(w=e.w, h=e.h, tile_w=e.tile_w, tile_h=e.tile_h, ms_best=e.ms_best, ms_default=e.ms_default)
-                for e in buf[:n.value]]
+        return [dict(w=e.w, h=e.h, tile_w=e.tile_w, tile_h=e.tile_h, threads_per_pixel=e.threads_per_pixel,
+                     ms_best=e.ms_best, ms_default=e.ms_default) for e in buf[:n.value]]
 
     def set_tune_table(self, entries):
         """Loads a tile-shape table (dicts as returned by tune_table)."""
         buf = (_abi.TuneEntry * max(len(entries), 1))()
         for i, e in enumerate(entries):
-            buf[i] = _abi.TuneEntry(e["w"], e["h"], e["tile_w"], e["tile_h"], e.get("ms_best", 0.0),
-                                    e.get("ms_default", 0.0))
+            buf[i] = _abi.TuneEntry(e["w"], e["h"], e["tile_w"], e["tile_h"], e.get("threads_per_pixel", 1), 0,
+                                    e.get("ms_best", 0.0), e.get("ms_default", 0.0))
         self.check(self._L.rcmvs_tune_set(self.ptr, buf, len(entries)))
 
     def close(self):

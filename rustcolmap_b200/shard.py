@@ -194,14 +194,23 @@ class SceneOps:
     reads, and the caller synchronises the collectives' stream before the
     library reads what they wrote."""
 
-    def __init__(self, views, opts, ctx):
+    def __init__(self, views, opts, ctx, net=None, **learned_kw):
         self.views, self.opts = views, opts
+        self.net, self.learned_kw = net, learned_kw
         self.ds = mvs.DeviceScene(views, ctx)
-        self.ds.prepare()
 
     def stereo(self, jobs):
-        if jobs:
+        """Census of every view (sources may be other ranks' views), then
+        this rank's jobs: plain stereo, or seeded by the proposal network
+        when one was given."""
+        self.ds.prepare()
+        if not jobs:
+            return
+        if self.net is None:
             self.ds.estimate(jobs, self.opts)
+        else:
+            from . import learned
+            learned.estimate_learned(self.ds, jobs, self.opts, self.net, **self.learned_kw)
 
     def depth_into(self, v, t):
         self.ds.depth_to_device(v, t.data_ptr())

@@ -40,6 +40,7 @@ class MvsOptions:
     tile_w: int = 0
     tile_h: int = 0
     flags: int = 0  # RCMVS_FLAG_* bits
+    threads_per_pixel: int = 0  # Jacobi passes: 0/1 one thread per pixel, 5 five lanes per pixel
 
     def to_c(self) -> _abi.Options:
         o = _abi.Options()
@@ -56,6 +57,7 @@ class MvsOptions:
         o.tile_w = self.tile_w
         o.tile_h = self.tile_h
         o.flags = self.flags
+        o.threads_per_pixel = self.threads_per_pixel
         return o
 
 

@@ -110,7 +110,8 @@ def test_autotuner_table_and_results(uneven):
     npx = {e["tile_w"] * e["tile_h"] for e in tab}
     assert len(npx) == 1 and npx.pop() in (32, 64, 128, 256)
     for e in tab:
-        assert 0 < e["ms_best"] <= e["ms_default"] or e["tile_w"] * e["tile_h"] != 64
+        assert e["threads_per_pixel"] in (1, 5)
+        assert 0 < e["ms_best"] <= e["ms_default"] or e["tile_w"] * e["tile_h"] != 64 or e["threads_per_pixel"] != 1
     # explicit call on known classes changes nothing
     assert ds.autotune(jobs, opts) == tab
     with pytest.raises(mvs.RcmvsError):
@@ -166,3 +167,54 @@ def test_scene_buffers_reused_across_scenes(uneven):
     orphan = mvs.DeviceScene(sc.views, ctx)
     ctx.close()
     orphan.close()  # its context is gone: the scene frees its own buffers
+
+
+# ---------------------------------------------- five lanes per pixel (passes)
+@pytest.mark.parametrize("tile", [(8, 8), (16, 4), (8, 4), (16, 8), (32, 4)])
+@pytest.mark.parametrize("flags", [0, FLAG_PERSISTENT, FLAG_PERSISTENT | FLAG_CUDA_GRAPH])
+def test_split_passes_match_oracle(uneven, tile, flags):
+    """threads_per_pixel 5 (one lane per window column, the row's counts
+    exchanged by shuffles, source-independent depths kept across sources):
+    the oracle's bits on the uneven batch (K 1-6, three sizes)."""
+    sc, opts, jobs, ref = uneven
+    ctx = mvs.Context(0)
+    ds = mvs.DeviceScene(sc.views, ctx)
+    o = MvsOptions(**{**opts.__dict__, "flags": flags, "tile_w": tile[0], "tile_h": tile[1], "threads_per_pixel": 5})
+    ds.estimate(jobs, o)
+    _check(ds, jobs, ref, f"split passes, tile {tile}, flags {flags}")
+    ds.close()
+    ctx.close()
+
+
+def test_split_passes_count_the_same_work(uneven):
+    """The work counters (plane_cost calls and 5-term rows) of the split
+    passes equal those of one thread per pixel, with and without the
+    duplicate skip."""
+    import os
+    sc, opts, jobs, ref = uneven
+    os.environ["RCMVS_COUNT"] = "1"
+    try:
+        ctx = mvs.Context(0)
+    finally:
+        del os.environ["RCMVS_COUNT"]
+    ds = mvs.DeviceScene(sc.views, ctx)
+    for flags in (0, 16):
+        got = []
+        for tpp in (1, 5):
+            ds.estimate(jobs, MvsOptions(**{**opts.__dict__, "flags": flags, "threads_per_pixel": tpp}))
+            got.append(ctx.last_work())
+            _check(ds, jobs, ref, f"tpp {tpp}")
+        assert got[0] == got[1] and got[0][0] > 0
+    ds.close()
+    ctx.close()
+
+
+def test_split_passes_reject_bad_settings(uneven):
+    sc, opts, jobs, _ = uneven
+    ctx = mvs.Context(0)
+    ds = mvs.DeviceScene(sc.views, ctx)
+    for kw in (dict(threads_per_pixel=3), dict(threads_per_pixel=5, tile_w=16, tile_h=16)):
+        with pytest.raises(mvs.RcmvsError):
+            ds.estimate(jobs, MvsOptions(**{**opts.__dict__, **kw}))
+    ds.close()
+    ctx.close()
