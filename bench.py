@@ -526,6 +526,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--views", type=int, default=0, help="override the number of views (profiling runs)")
+    ap.add_argument("--arc-deg", type=float, default=0.0,
+                    help="cameras on an arc of this many degrees instead of the full orbit (profiling runs with "
+                         "fewer views at the full scene's camera spacing)")
     ap.add_argument("--no-count", action="store_true", help="skip the work-counting rerun")
     ap.add_argument("--one-candidate", action="store_true",
                     help="use the one-candidate-at-a-time init kernel (comparison)")
@@ -537,6 +540,7 @@ def main():
     ap.add_argument("--flags", type=int, default=0,
                     help="RCMVS_FLAG_* bits for both arms (2 persistent queue, 4 CUDA graph, 8 autotuned tiles)")
     ap.add_argument("--tile", default="", help="WxH stereo tile (default: the library's 8x8)")
+    ap.add_argument("--tpp", type=int, default=0, help="threads per pixel of the Jacobi passes (1 or 5)")
     ap.add_argument("--shard", action="store_true",
                     help="one scene split over the --gpus ranks (strong scaling; device-to-device exchanges)")
     args = ap.parse_args()
@@ -548,6 +552,9 @@ def main():
     if args.views and cfg["scene"] is not None:
         cfg["scene"] = dict(cfg["scene"], n_views=args.views)
         cfg["desc"] += f" [{args.views} views]"
+    if args.arc_deg and cfg["scene"] is not None:
+        cfg["scene"] = dict(cfg["scene"], arc_deg=args.arc_deg)
+        cfg["desc"] += f" [{args.arc_deg:g} degree arc]"
     if args.impl == "reference":
         run_reference(args, cfg)
         return
@@ -568,6 +575,7 @@ def main():
     opts.flags |= args.flags
     if args.tile:
         opts.tile_w, opts.tile_h = map(int, args.tile.lower().split("x"))
+    opts.threads_per_pixel = args.tpp
     lopts = dataclasses.replace(opts, sweeps=2)
     t_setup = time.perf_counter()
     sc = make_scene(cfg, seed=5 + 1000 * rank, device=local)
@@ -758,7 +766,7 @@ def main():
             "setup_s": setup_s,
             "kernels": "one-candidate init" if opts.flags & 1 else "row-step init",
             "schedule": {"tile": f"{opts.tile_w}x{opts.tile_h}" if opts.tile_w else "8x8 (library default)",
-                         "flags": opts.flags,
+                         "threads_per_pixel": max(opts.threads_per_pixel, 1), "flags": opts.flags,
                          "persistent_queue": bool(opts.flags & 2), "cuda_graph": bool(opts.flags & 4),
                          "autotuned_tiles": bool(opts.flags & 8), "tune_table": ctx.tune_table()},
         }
