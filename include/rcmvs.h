@@ -94,12 +94,16 @@ typedef struct rcmvs_options {
  * first.  Overrides tile_w/tile_h.  Same results bit for bit. */
 #define RCMVS_FLAG_AUTOTUNE 8u
 
-/* Evaluate every propagation candidate, as the reference does.  By default
- * a Jacobi pass skips a neighbour's plane that is bit for bit the plane
- * (normal and offset d) the pixel's stored cost was computed with: its cost
- * would be that same cost, or an early abort, and never lower, so it can
- * not be accepted.  Skipping changes no output bit, only the work counters
- * (rcmvs_last_work), which with this flag count the reference's calls. */
+/* Evaluate every candidate the way the reference does.  By default two
+ * exact shortcuts run: a Jacobi pass skips a neighbour's plane that is bit
+ * for bit the plane (normal and offset d) the pixel's stored cost was
+ * computed with (its cost would be that same cost, or an early abort, and
+ * never lower, so it can not be accepted), and every evaluation (init and
+ * passes) stops once its window sum reaches best_cost * 25K (the sum only
+ * grows, so the candidate's cost could not be below the best and it could
+ * not be kept).  Neither changes an output bit, only the work counters
+ * (rcmvs_last_work), which with this flag count the reference's calls and
+ * rows. */
 #define RCMVS_FLAG_NO_SKIP_DUPLICATES 16u
 
 /* Diagnostic: run the init (plane sweep, or the learned init) and the gate

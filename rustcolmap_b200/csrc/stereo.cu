@@ -159,6 +159,23 @@ struct WorkCount {
     unsigned long long evals, rows;
 };
 
+// Early rejection (exact): a candidate is kept only if its cost is strictly
+// below best_c, and the window sum only grows (each term adds a
+// non-negative h/48, and f32 addition of a non-negative value never lowers
+// the sum), so once sum >= best_c * total the final cost sum_final / total
+// is >= best_c and the candidate cannot be kept: the evaluation may stop.
+// The bound is rounded up by one ulp so that the f32 product's rounding can
+// never make the test fire early.  Skipping such a candidate changes no
+// state -- best_c and the kept plane are only updated by a kept candidate,
+// and no RNG draw depends on a cost -- so every output bit is the
+// reference's; only the work counters see fewer rows.  +inf disables it
+// (best_c = +inf before the first hypothesis, and the reference call
+// sequence of RCMVS_FLAG_NO_SKIP_DUPLICATES).
+__device__ __forceinline__ float reject_bound(float best_c, float total) {
+    const float t = best_c * total;
+    return t < INFINITY ? __int_as_float(__float_as_int(t) + 1) : INFINITY;
+}
+
 // ---------------------------------------------------------------- plane_cost
 // One support view in registers.
 struct SrcRegs {
@@ -256,7 +273,8 @@ __device__ __forceinline__ float cost_row(const Smem& sm, int row, const SrcRegs
 template <bool FRONTO, bool COUNT, bool HSUM>
 __device__ __forceinline__ float plane_cost(const Smem& sm, int stw, int lx, int ly, int nsrc,
                                             const uint64_t* __restrict__ census, float nx, float ny, float nz,
-                                            float d, float hint, float total, WorkCount& wc, int32_t* hsum) {
+                                            float d, float hint, float total, WorkCount& wc, int32_t* hsum,
+                                            float rej = INFINITY) {
     float sum = 0.f;
     int32_t hs = 0;
     const float thr = hint + 0.12f;
@@ -268,7 +286,7 @@ __device__ __forceinline__ float plane_cost(const Smem& sm, int stw, int lx, int
             sum = cost_row<FRONTO, HSUM>(sm, (ly + dy) * stw + lx, s, nx, ny, nz, d, sum, hs);
             if (COUNT) wc.rows++;
             const float rows_done = (float)(dy + 1);
-            if (sum / (rows_done * 5.0f * fsi) > thr) {
+            if (sum / (rows_done * 5.0f * fsi) > thr || sum >= rej) {
                 if (HSUM) *hsum = hs;
                 return 1e9f;
             }
@@ -312,13 +330,15 @@ __global__ void init_kernel(const DevJob* __restrict__ jobs, const int32_t* __re
             const int nsrc = J->nsrc;
             const float total = 5.0f * 5.0f * (float)nsrc;
             const float inv_min = J->inv_min, inv_max = J->inv_max;
+            const bool early = out.d != nullptr;  // off for the reference call sequence
             float best_c = INFINITY;
             float best_d = 0.f;
             for (int hi = 0; hi < nh; ++hi) {
                 const float inv = inv_min + (inv_max - inv_min) * (float)hi / (float)(nh - 1);
                 const float d = 1.0f / inv;
                 const float c = plane_cost<true, COUNT, false>(sm, T.stw, lx, ly, nsrc, census, 0.f, 0.f, 1.f, d,
-                                                               best_c + 0.02f, total, wc, nullptr);
+                                                               best_c + 0.02f, total, wc, nullptr,
+                                                               early ? reject_bound(best_c, total) : INFINITY);
                 if (c < best_c) {
                     best_c = c;
                     best_d = d;
@@ -428,7 +448,8 @@ __global__ void __maxnreg__(72)
                 float d_plane;
                 neighbour(q, nb, d_plane);  // passed above; same values
                 const float c = plane_cost<false, COUNT, false>(sm, stw, lx, ly, nsrc, census, nb.x, nb.y, nb.z,
-                                                                      d_plane, best_c + 0.02f, total, wc, nullptr);
+                                                                      d_plane, best_c + 0.02f, total, wc, nullptr,
+                                                                      skip_dup ? reject_bound(best_c, total) : INFINITY);
                 if (c < best_c) {
                     best_c = c;
                     bn0 = nb.x;
@@ -458,7 +479,8 @@ __global__ void __maxnreg__(72)
                 if (a_here < 0.1f) continue;
                 const float d_plane = zcand * a_here;
                 const float c = plane_cost<false, COUNT, false>(sm, stw, lx, ly, nsrc, census, nnx, nny, nnz,
-                                                                      d_plane, best_c + 0.02f, total, wc, nullptr);
+                                                                      d_plane, best_c + 0.02f, total, wc, nullptr,
+                                                                      skip_dup ? reject_bound(best_c, total) : INFINITY);
                 if (c < best_c) {
                     best_c = c;
                     bn0 = nnx;
@@ -505,7 +527,7 @@ template <bool COUNT>
 __device__ __forceinline__ float plane_cost_split(const Smem& sm, int stw, int lx, int ly, int j, unsigned gmask,
                                                   int gbase, int nsrc, const uint64_t* __restrict__ census,
                                                   float nx, float ny, float nz, float d, float hint, float total,
-                                                  WorkCount& wc) {
+                                                  WorkCount& wc, float rej) {
     float sum = 0.f;
     const float thr = hint + 0.12f;
     if (COUNT && j == 0) wc.evals++;
@@ -544,7 +566,7 @@ __device__ __forceinline__ float plane_cost_split(const Smem& sm, int stw, int l
 #pragma unroll
             for (int k = 0; k < SPLIT; ++k) sum += sm.tab[__shfl_sync(gmask, h, gbase + k)];
             if (COUNT && j == 0) wc.rows++;
-            if (sum / ((float)(dy + 1) * 5.0f * fsi) > thr) return 1e9f;
+            if (sum / ((float)(dy + 1) * 5.0f * fsi) > thr || sum >= rej) return 1e9f;
         }
     }
     return sum / total;
@@ -628,7 +650,8 @@ __global__ void __maxnreg__(80)
                 float d_plane;
                 neighbour(q, nb, d_plane);
                 const float c = plane_cost_split<COUNT>(sm, stw, lx, ly, j, gmask, gbase, nsrc, census, nb.x, nb.y,
-                                                        nb.z, d_plane, best_c + 0.02f, total, wc);
+                                                        nb.z, d_plane, best_c + 0.02f, total, wc,
+                                                        skip_dup ? reject_bound(best_c, total) : INFINITY);
                 if (c < best_c) {
                     best_c = c;
                     bn0 = nb.x;
@@ -656,7 +679,8 @@ __global__ void __maxnreg__(80)
                 if (a_here < 0.1f) continue;
                 const float d_plane = zcand * a_here;
                 const float c = plane_cost_split<COUNT>(sm, stw, lx, ly, j, gmask, gbase, nsrc, census, nnx, nny,
-                                                        nnz, d_plane, best_c + 0.02f, total, wc);
+                                                        nnz, d_plane, best_c + 0.02f, total, wc,
+                                                        skip_dup ? reject_bound(best_c, total) : INFINITY);
                 if (c < best_c) {
                     best_c = c;
                     bn0 = nnx;
@@ -724,6 +748,8 @@ __global__ void __launch_bounds__(256, MINB)
         float d = hyp_depth(inv_min, inv_max, 0, nh);
         float sum = 0.f;
         float thr = INFINITY;  // (best_c + 0.02) + 0.12 with best_c = +inf
+        float rej = INFINITY;  // early-rejection bound (reject_bound)
+        const bool early = out.d != nullptr;  // off for the reference call sequence
         int32_t hs = 0;
         bool live = inside;
         if (COUNT && live) wc.evals++;
@@ -733,7 +759,7 @@ __global__ void __launch_bounds__(256, MINB)
                 const SrcRegs s = load_src(sm.src[si], census);
                 sum = cost_row<true, false>(sm, (ly + dy) * T.stw + lx, s, 0.f, 0.f, 1.f, d, sum, hs);
                 if (COUNT) wc.rows++;
-                aborted = sum / ((float)(dy + 1) * 5.0f * (float)(si + 1)) > thr;
+                aborted = sum / ((float)(dy + 1) * 5.0f * (float)(si + 1)) > thr || sum >= rej;
                 fin = aborted || (si == nsrc - 1 && dy == 4);
             }
             if (fin) {
@@ -750,6 +776,7 @@ __global__ void __launch_bounds__(256, MINB)
                     si = 0;
                     dy = 0;
                     thr = (best_c + 0.02f) + 0.12f;
+                    if (early) rej = reject_bound(best_c, total);
                     if (COUNT) wc.evals++;
                 }
             } else if (++dy == 5) {
@@ -870,14 +897,15 @@ __global__ void __launch_bounds__(256, 3)
         float plane_d = 0.f;
         bool live = inside && learned && next_local();
         int si = 0, dy = 0;
-        float sum = 0.f, thr = INFINITY;
+        float sum = 0.f, thr = INFINITY, rej = INFINITY;
+        const bool early = out.d != nullptr;  // early rejection off for the reference call sequence
         int32_t hs = 0;
         while (live) {
             bool fin = true, aborted = false;
             if (nsrc > 0) {
                 const SrcRegs s = load_src(sm.src[si], census);
                 sum = cost_row<false, false>(sm, (ly + dy) * T.stw + lx, s, pnx, pny, pnz, cd, sum, hs);
-                aborted = sum / ((float)(dy + 1) * 5.0f * (float)(si + 1)) > thr;
+                aborted = sum / ((float)(dy + 1) * 5.0f * (float)(si + 1)) > thr || sum >= rej;
                 fin = aborted || (si == nsrc - 1 && dy == 4);
             }
             if (fin) {
@@ -892,6 +920,7 @@ __global__ void __launch_bounds__(256, 3)
                 si = 0;
                 dy = 0;
                 thr = (best_c + 0.02f) + 0.12f;
+                if (early) rej = reject_bound(best_c, total);
             } else if (++dy == 5) {
                 dy = 0;
                 ++si;
@@ -925,13 +954,14 @@ __global__ void __launch_bounds__(256, 3)
             int hi = 0, ssi = 0, sdy = 0;
             float d = hyp_depth(inv_min, inv_max, 0, nh);
             float ssum = 0.f, sthr = (bc + 0.02f) + 0.12f;
+            float srej = early ? reject_bound(bc, total) : INFINITY;
             bool slive = true;
             while (slive) {
                 bool fin = true, aborted = false;
                 if (nsrc > 0) {
                     const SrcRegs s = load_src(sm.src[ssi], census);
                     ssum = cost_row<true, false>(sm, (ply + sdy) * T.stw + plx, s, 0.f, 0.f, 1.f, d, ssum, hs);
-                    aborted = ssum / ((float)(sdy + 1) * 5.0f * (float)(ssi + 1)) > sthr;
+                    aborted = ssum / ((float)(sdy + 1) * 5.0f * (float)(ssi + 1)) > sthr || ssum >= srej;
                     fin = aborted || (ssi == nsrc - 1 && sdy == 4);
                 }
                 if (fin) {
@@ -949,6 +979,7 @@ __global__ void __launch_bounds__(256, 3)
                         ssi = 0;
                         sdy = 0;
                         sthr = (bc + 0.02f) + 0.12f;
+                        if (early) srej = reject_bound(bc, total);
                     }
                 } else if (++sdy == 5) {
                     sdy = 0;

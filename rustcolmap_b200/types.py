@@ -18,7 +18,7 @@ FLAG_ONE_CANDIDATE = 1  # one-candidate-at-a-time init schedule
 FLAG_PERSISTENT = 2     # persistent (view, tile) work-queue launches
 FLAG_CUDA_GRAPH = 4     # replay the init/pass/gate schedule from a CUDA graph
 FLAG_AUTOTUNE = 8       # per-resolution-class tile shapes from the autotuner
-FLAG_NO_SKIP_DUPLICATES = 16  # evaluate repeated propagation candidates too (reference call counts)
+FLAG_NO_SKIP_DUPLICATES = 16  # reference call sequence: no duplicate skip, no early rejection (work counts)
 FLAG_INIT_ONLY = 32     # diagnostic: init and gate only, no passes
 FLAG_SEED_AND_SWEEP = 64  # learned init: seeded pixels also run the plane sweep
 FLAGS_BATCHED = FLAG_PERSISTENT | FLAG_CUDA_GRAPH | FLAG_AUTOTUNE
