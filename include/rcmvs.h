@@ -539,7 +539,7 @@ int rcmvs_net_train_step(rcmvs_ctx* ctx, rcmvs_net* net, const void* x_dev,
                          const float* labels_dev, int32_t n, int32_t h, int32_t w, float lr,
                          int32_t apply, float* loss_out, float* grads_host);
 /* Network input of each job's reference view (quarter resolution
- * (w/4)x(h/4), jobs back to back) into out_dev (BF16). */
+ * (w/4)x(h/4), jobs back to back) into out_dev (BF16, 16-byte aligned). */
 int rcmvs_scene_costvol(rcmvs_ctx* ctx, rcmvs_scene* scene, const rcmvs_job* jobs, int32_t n_jobs,
                         void* out_dev);
 /* Stereo seeded by the network: a pixel whose prediction has confidence >=

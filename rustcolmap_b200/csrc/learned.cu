@@ -61,41 +61,68 @@ __global__ void downsample4_kernel(const DevView* __restrict__ full, const DevVi
 }
 
 // ------------------------------------------------------------ cost volume
-// One thread per quarter-resolution pixel of a job.  Output channel p < 32 is
-// the mean Hamming fraction of fronto-parallel plane p (inverse depths at the
-// centres of 32 equal bins of [1/zmax, 1/zmin]); channel 32 is grey/255;
-// channels 33..47 are zero.
-__global__ void costvol_kernel(const DevJob* __restrict__ jobs, const int32_t* __restrict__ blk_start, int n_jobs,
-                               const int64_t* __restrict__ out_off, const uint64_t* __restrict__ census_q,
-                               const float2* __restrict__ rays_q, const uint8_t* __restrict__ gray_q,
-                               bf16* __restrict__ out) {
-    const int j = find_item(blk_start, n_jobs, blockIdx.x);
+// Output channel p < 32 of a quarter-resolution pixel is the mean Hamming
+// fraction of fronto-parallel plane p (inverse depths at the centres of 32
+// equal bins of [1/zmax, 1/zmin]) over its clamped 3x3 window and the K
+// support views; channel 32 is grey/255; channels 33..47 are zero.
+//
+// On a fronto-parallel plane every window cell sits at depth d, so the
+// count of window cell c -- the Hamming distance between c's census and the
+// source census where c's ray at depth d projects -- depends on the cell,
+// the plane and the source only, not on which pixel's window holds it.  So
+// one block takes a 32x8 tile: per plane, its threads compute each of the
+// 34x10 cells (tile + clamped 1-cell halo) once, summed over the sources,
+// into shared memory, and every pixel adds its nine cells: the same integer
+// sums as evaluating each pixel's window, with 340/256 instead of 9
+// projections per pixel and source.  A pixel keeps its 32 costs as packed
+// BF16 pairs (in shared memory) and writes its 96-byte record with 16-byte
+// stores.
+constexpr int CV_TW = 32, CV_TH = 8;
+constexpr int CV_HW = CV_TW + 2, CV_HH = CV_TH + 2;
+
+__global__ void __launch_bounds__(CV_TW * CV_TH)
+    costvol_kernel(const DevJob* __restrict__ jobs, const int32_t* __restrict__ tile_start, int n_jobs,
+                   const int64_t* __restrict__ out_off, const uint64_t* __restrict__ census_q,
+                   const float2* __restrict__ rays_q, const uint8_t* __restrict__ gray_q, bf16* __restrict__ out) {
+    __shared__ DevSrc s_src[RCMVS_MAX_SOURCES];
+    __shared__ uint64_t s_cen[CV_HH * CV_HW];
+    __shared__ float2 s_ray[CV_HH * CV_HW];
+    __shared__ int s_h[CV_HH * CV_HW];
+    __shared__ uint32_t s_out[CV_TW * CV_TH][COSTVOL_PLANES / 2 + 1];  // packed BF16 pairs (+1: no bank conflicts)
+    const int j = find_item(tile_start, n_jobs, blockIdx.x);
     const DevJob& J = jobs[j];
-    const int64_t i = (int64_t)(blockIdx.x - blk_start[j]) * blockDim.x + threadIdx.x;
-    if (i >= (int64_t)J.w * J.h) return;
-    const int x = (int)(i % J.w), y = (int)(i / J.w);
+    const int t = blockIdx.x - tile_start[j];
+    const int tiles_x = (J.w + CV_TW - 1) / CV_TW;
+    const int x0 = (t % tiles_x) * CV_TW, y0 = (t / tiles_x) * CV_TH;
     const size_t base = (size_t)J.off;
-    uint64_t cref[9];
-    float2 ray[9];
-#pragma unroll
-    for (int q = 0; q < 9; ++q) {
-        const int xx = min(max(x + q % 3 - 1, 0), J.w - 1);
-        const int yy = min(max(y + q / 3 - 1, 0), J.h - 1);
-        cref[q] = census_q[base + (size_t)yy * J.w + xx];
-        ray[q] = rays_q[base + (size_t)yy * J.w + xx];
+    const int nsrc = J.nsrc;
+    {
+        const uint32_t* srcw = reinterpret_cast<const uint32_t*>(J.src);
+        uint32_t* dstw = reinterpret_cast<uint32_t*>(s_src);
+        for (int i = threadIdx.x; i < nsrc * (int)(sizeof(DevSrc) / 4); i += blockDim.x) dstw[i] = srcw[i];
     }
-    bf16* o = out + (size_t)(out_off[j] + i) * COSTVOL_C;
-    const float norm = 1.0f / (9.0f * 48.0f * (float)max(J.nsrc, 1));
+    for (int c = threadIdx.x; c < CV_HH * CV_HW; c += blockDim.x) {
+        const int xx = min(max(x0 - 1 + c % CV_HW, 0), J.w - 1);
+        const int yy = min(max(y0 - 1 + c / CV_HW, 0), J.h - 1);
+        s_cen[c] = census_q[base + (size_t)yy * J.w + xx];
+        s_ray[c] = rays_q[base + (size_t)yy * J.w + xx];
+    }
+    const int lx = threadIdx.x % CV_TW, ly = threadIdx.x / CV_TW;
+    const int x = x0 + lx, y = y0 + ly;
+    const bool inside = x < J.w && y < J.h;
+    const float norm = 1.0f / (9.0f * 48.0f * (float)max(nsrc, 1));
+    uint32_t* packed = s_out[threadIdx.x];
     for (int p = 0; p < COSTVOL_PLANES; ++p) {
         const float inv = J.inv_min + (J.inv_max - J.inv_min) * ((float)p + 0.5f) / (float)COSTVOL_PLANES;
         const float d = 1.0f / inv;
-        int hsum = 0;
-        for (int s = 0; s < J.nsrc; ++s) {
-            const DevSrc& S = J.src[s];
-            const uint64_t* sc = census_q + S.off;
-#pragma unroll
-            for (int q = 0; q < 9; ++q) {
-                const float xr = d * ray[q].x, yr = d * ray[q].y;
+        __syncthreads();  // the staged tile (p = 0) / the previous plane's sums are read
+        for (int c = threadIdx.x; c < CV_HH * CV_HW; c += blockDim.x) {
+            const float2 r = s_ray[c];
+            const uint64_t cref = s_cen[c];
+            const float xr = d * r.x, yr = d * r.y;
+            int hs = 0;
+            for (int s = 0; s < nsrc; ++s) {
+                const DevSrc& S = s_src[s];
                 const float xs = S.rs[0] * xr + S.rs[1] * yr + S.rs[2] * d + S.ts[0];
                 const float ys = S.rs[3] * xr + S.rs[4] * yr + S.rs[5] * d + S.ts[1];
                 const float zs = S.rs[6] * xr + S.rs[7] * yr + S.rs[8] * d + S.ts[2];
@@ -105,15 +132,32 @@ __global__ void costvol_kernel(const DevJob* __restrict__ jobs, const int32_t* _
                     const float dist = 1.0f + S.k * (xn * xn + yn * yn);
                     const int u = __float2int_rz(S.f * xn * dist + S.cx);
                     const int v = __float2int_rz(S.f * yn * dist + S.cy);
-                    if (u >= 0 && v >= 0 && u < S.w && v < S.h) h = __popcll(cref[q] ^ sc[(size_t)v * S.w + u]);
+                    if (u >= 0 && v >= 0 && u < S.w && v < S.h)
+                        h = __popcll(cref ^ __ldg(census_q + S.off + (size_t)v * S.w + u));
                 }
-                hsum += h;
+                hs += h;
             }
+            s_h[c] = hs;
         }
-        o[p] = __float2bfloat16((float)hsum * norm);
+        __syncthreads();
+        int hsum = 0;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) hsum += s_h[(ly + q / 3) * CV_HW + lx + q % 3];
+        const uint32_t b = __bfloat16_as_ushort(__float2bfloat16((float)hsum * norm));
+        if (p & 1)
+            packed[p >> 1] |= b << 16;
+        else
+            packed[p >> 1] = b;
     }
-    o[COSTVOL_PLANES] = __float2bfloat16((float)gray_q[base + i] * (1.0f / 255.0f));
-    for (int c = COSTVOL_PLANES + 1; c < COSTVOL_C; ++c) o[c] = __float2bfloat16(0.0f);
+    if (!inside) return;
+    const int64_t i = (int64_t)y * J.w + x;
+    const uint32_t g = __bfloat16_as_ushort(__float2bfloat16((float)gray_q[base + i] * (1.0f / 255.0f)));
+    uint4* o = reinterpret_cast<uint4*>(out + (size_t)(out_off[j] + i) * COSTVOL_C);  // 96 B, 16-B aligned
+#pragma unroll
+    for (int k = 0; k < COSTVOL_PLANES / 8; ++k)
+        o[k] = make_uint4(packed[4 * k], packed[4 * k + 1], packed[4 * k + 2], packed[4 * k + 3]);
+    o[COSTVOL_PLANES / 8] = make_uint4(g, 0u, 0u, 0u);
+    o[COSTVOL_PLANES / 8 + 1] = make_uint4(0u, 0u, 0u, 0u);
 }
 
 // ------------------------------------------------------------ convolution
@@ -447,12 +491,14 @@ cudaError_t launch_downsample4(const DevView* full, const DevView* quarter, cons
     return cudaGetLastError();
 }
 
+int costvol_tiles(int w, int h) { return ((w + CV_TW - 1) / CV_TW) * ((h + CV_TH - 1) / CV_TH); }
+
 cudaError_t launch_costvol(const DevJob* jobs, const int32_t* blk_start, int n_jobs, int total_blocks,
                            const int64_t* out_off, const uint64_t* census_q, const float2* rays_q,
                            const uint8_t* gray_q, void* out, cudaStream_t st) {
     if (total_blocks <= 0) return cudaSuccess;
-    costvol_kernel<<<total_blocks, 128, 0, st>>>(jobs, blk_start, n_jobs, out_off, census_q, rays_q, gray_q,
-                                                 reinterpret_cast<bf16*>(out));
+    costvol_kernel<<<total_blocks, CV_TW * CV_TH, 0, st>>>(jobs, blk_start, n_jobs, out_off, census_q, rays_q,
+                                                           gray_q, reinterpret_cast<bf16*>(out));
     return cudaGetLastError();
 }
 

@@ -19,6 +19,9 @@ constexpr int NET_COUT_REAL[NET_LAYERS] = {32, 32, 32, 32, 32, 5};
 
 cudaError_t launch_downsample4(const DevView* full, const DevView* quarter, const int32_t* blk_start, int n_views,
                                int total_blocks, const uint8_t* gray, uint8_t* gray_q, cudaStream_t st);
+// Blocks (32x8 quarter-pixel tiles) the cost-volume kernel uses for a
+// w x h quarter view; a batch's jobs take consecutive tile ranges.
+int costvol_tiles(int w, int h);
 cudaError_t launch_costvol(const DevJob* jobs, const int32_t* blk_start, int n_jobs, int total_blocks,
                            const int64_t* out_off, const uint64_t* census_q, const float2* rays_q,
                            const uint8_t* gray_q, void* out, cudaStream_t st);

@@ -361,7 +361,7 @@ int quarter_jobs(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job* jobs, int n_j
         }
         blk[j] = nb;
         off[j] = px;
-        nb += (int)(((int64_t)Q.w * Q.h + 127) / 128);
+        nb += costvol_tiles(Q.w, Q.h);
         px += (int64_t)Q.w * Q.h;
     }
     blk[n_jobs] = nb;
