@@ -119,6 +119,13 @@ typedef struct rcmvs_options {
  * pixel skips the sweep. */
 #define RCMVS_FLAG_SEED_AND_SWEEP 64u
 
+/* The plane sweep of the init walks the hypotheses block by block: for each
+ * hypothesis and support view the window counts of a tile and its halo are
+ * computed once into shared memory (on a fronto-parallel plane a window
+ * cell's count does not depend on which pixel's window holds it) and every
+ * pixel runs the reference's chain over them.  Same results bit for bit. */
+#define RCMVS_FLAG_TABLE_INIT 128u
+
 /* Fills `MvsOptions::default()` (mvs/src/lib.rs:56-70); extensions off. */
 void rcmvs_options_default(rcmvs_options* opts);
 

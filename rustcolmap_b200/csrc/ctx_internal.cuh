@@ -176,7 +176,7 @@ struct StereoBatch {
 
 // The launch schedule of a batch: init -> n_passes Jacobi passes -> gate.
 struct Schedule {
-    enum Init { ROWS = 0, ONE_CANDIDATE = 1, LEARNED = 2 } init = ROWS;
+    enum Init { ROWS = 0, ONE_CANDIDATE = 1, LEARNED = 2, TABLE = 3 } init = ROWS;
     int nh = 64;
     uint64_t n_passes = 12;
     float cost_thr = 0.38f;

@@ -43,6 +43,12 @@ int sfail(rcmvs_ctx* ctx, int code, const std::string& msg) {
 float powf_host(float b, float e) { return powf(b, e); }
 
 bool shape_ok(TileShape ts) { return tile_shape_ok(ts); }
+// launch_init's kernel for the option flags: 1 one candidate at a time, 2 the
+// table sweep, 0 the row-step sweep.
+int init_variant(uint32_t flags) {
+    if (flags & RCMVS_FLAG_ONE_CANDIDATE) return 1;
+    return (flags & RCMVS_FLAG_TABLE_INIT) ? 2 : 0;
+}
 // Split passes (5 lanes per pixel): at most 128 pixels, so a block of
 // split_threads(px) threads at the kernel's 80 registers fits an SM.
 bool split_shape_ok(TileShape ts) { return tile_shape_ok(ts) && ts.tw * ts.th <= 128; }
@@ -110,7 +116,7 @@ int trial(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job* jobs, int n_jobs, co
     const DevJob* dj = (const DevJob*)pj;
     const int32_t* dst = (const int32_t*)ps;
     const int nh = (int)std::max<uint32_t>(opts->num_hyp, 2u);
-    const int variant = (opts->flags & RCMVS_FLAG_ONE_CANDIDATE) ? 1 : 0;
+    const int variant = init_variant(opts->flags);
     const bool skip_dup = !(opts->flags & RCMVS_FLAG_NO_SKIP_DUPLICATES);
     PlaneBuf A{sc->plane_a, sc->pcost_a, skip_dup ? sc->pd_a : nullptr};
     PlaneBuf B{sc->plane_b, sc->pcost_b, skip_dup ? sc->pd_b : nullptr};
@@ -347,7 +353,7 @@ int run_batch(rcmvs_ctx* ctx, rcmvs_scene* sc, const StereoBatch& b, const Sched
                                     s.logit_thr, s.n_local, s.span, s.sweep_seeded, s.d_learned, st);
         else
             e = launch_init(dj, dst, n_jobs, g, s.nh, sc->census, sc->rays, A, s.d_work, st,
-                            s.init == Schedule::ONE_CANDIDATE ? 1 : 0);
+                            s.init == Schedule::ONE_CANDIDATE ? 1 : (s.init == Schedule::TABLE ? 2 : 0));
         hk.end(s.init == Schedule::LEARNED ? "learned_init" : "stereo_init");
         if (e) return e;
         for (uint64_t pass = 0; pass < s.n_passes; ++pass) {

@@ -794,6 +794,110 @@ __global__ void __launch_bounds__(256, MINB)
     if (COUNT) flush_work(wc, d_work);
 }
 
+// ---------------------------------------------------------------- table init
+// The plane sweep with the window counts shared between pixels.  On a
+// fronto-parallel plane (n = (0,0,1), so denom = 1 and z = d for every
+// window cell) the count of a window cell -- where its ray at depth d lands
+// in a source and the Hamming distance to the census there -- depends on the
+// cell, the hypothesis and the source only, not on which pixel's window
+// holds it.  So the block walks the hypotheses together: for hypothesis hi
+// and source si it computes the count of every cell of the tile and its
+// halo once into shared memory (a tile of 64 pixels has 144 cells instead
+// of 64 x 25 window terms), then every pixel runs the reference's serial f32
+// chain for that source -- its five counts per row added in dx order, the
+// abort test and the early rejection after each row -- reading the counts
+// from the table.  A source's table is built only while some pixel of the
+// block still needs it, so hypotheses that every pixel drops early cost
+// little.  Each pixel's chain, hints and best-cost updates are those of
+// stereo.rs:247-269: the results are bit-identical to init_rows_kernel.
+constexpr int TABLE_CELLS = 1312;  // (tw + 4) x (th + 4) for every tile shape of at most 256 pixels
+
+template <bool COUNT, bool PERSIST>
+__global__ void __launch_bounds__(256)
+    init_table_kernel(const DevJob* __restrict__ jobs, const int32_t* __restrict__ job_start, int n_jobs,
+                      int tiles, unsigned int* queue, int nh, const uint64_t* __restrict__ census,
+                      const float2* __restrict__ rays, PlaneBuf out, unsigned long long* d_work) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int s_tile;
+    __shared__ uint8_t s_h[TABLE_CELLS];
+    WorkCount wc{0, 0};
+    for (int it = 0; PERSIST || it == 0; ++it) {
+        const int tile = PERSIST ? next_tile(queue, tiles, it, &s_tile) : (int)blockIdx.x;
+        if (tile < 0) break;
+        Smem sm;
+        Tile T;
+        load_tile(jobs, job_start, n_jobs, tile, census, rays, smem_raw, sm, T);
+        const DevJob* J = T.job;
+        const int lx = threadIdx.x % T.tw, ly = threadIdx.x / T.tw;
+        const int x = T.x0 + lx, y = T.y0 + ly;
+        const bool inside = (int)threadIdx.x < T.tw * T.th && x < J->w && y < J->h;
+        const int nsrc = J->nsrc;
+        const float total = 5.0f * 5.0f * (float)nsrc;
+        const float inv_min = J->inv_min, inv_max = J->inv_max;
+        const bool early = out.d != nullptr;  // off for the reference call sequence
+        const int cells = T.stw * (T.th + 2 * HALO);
+        float best_c = INFINITY, best_d = 0.f;
+        for (int hi = 0; hi < nh; ++hi) {
+            const float d = hyp_depth(inv_min, inv_max, hi, nh);
+            const float thr = (best_c + 0.02f) + 0.12f;  // +inf before the first hypothesis
+            const float rej = early ? reject_bound(best_c, total) : INFINITY;
+            bool alive = inside;
+            float sum = 0.f;
+            if (COUNT && inside) wc.evals++;
+            for (int si = 0; si < nsrc; ++si) {
+                if (!__syncthreads_or(alive)) break;  // also: the previous table is no longer read
+                const SrcRegs s = load_src(sm.src[si], census);
+                for (int c = threadIdx.x; c < cells; c += blockDim.x) {
+                    const float2 r = sm.ray[c];
+                    const float xr = d * r.x;
+                    const float yr = d * r.y;
+                    const float xs = s.rs0 * xr + s.rs1 * yr + s.rs2 * d + s.ts0;
+                    const float ys = s.rs3 * xr + s.rs4 * yr + s.rs5 * d + s.ts1;
+                    const float zs = s.rs6 * xr + s.rs7 * yr + s.rs8 * d + s.ts2;
+                    const float xn = xs / zs;
+                    const float yn = ys / zs;
+                    const float dist = 1.0f + s.k * (xn * xn + yn * yn);
+                    int u, v;
+                    const bool in_u = trunc_index(s.f * xn * dist + s.cx, s.swf, u);
+                    const bool in_v = trunc_index(s.f * yn * dist + s.cy, s.shf, v);
+                    const bool ok = !(zs < 1e-3f) && in_u && in_v;  // denom = 1 >= 0.05
+                    const uint64_t cs = __ldg(s.sc + (ok ? (size_t)v * s.sw + u : (size_t)0));
+                    s_h[c] = ok ? (uint8_t)__popcll(sm.cen[c] ^ cs) : (uint8_t)48;
+                }
+                __syncthreads();
+                if (alive) {
+                    const float fsi = (float)(si + 1);
+#pragma unroll
+                    for (int dy = 0; dy < 5; ++dy) {
+                        const int row = (ly + dy) * T.stw + lx;
+#pragma unroll
+                        for (int dx = 0; dx < 5; ++dx) sum += sm.tab[s_h[row + dx]];
+                        if (COUNT) wc.rows++;
+                        if (sum / ((float)(dy + 1) * 5.0f * fsi) > thr || sum >= rej) {
+                            alive = false;
+                            break;
+                        }
+                    }
+                }
+            }
+            if (inside) {
+                const float c = alive ? sum / total : 1e9f;
+                if (c < best_c) {
+                    best_c = c;
+                    best_d = d;
+                }
+            }
+        }
+        if (inside) {
+            const size_t i = (size_t)J->off + (size_t)y * J->w + x;
+            out.nz[i] = make_float4(0.0f, 0.0f, 1.0f, best_d);
+            out.cost[i] = fminf(best_c, 1.0f);
+            if (out.d) out.d[i] = best_d;  // n = (0,0,1): d = z
+        }
+    }
+    if (COUNT) flush_work(wc, d_work);
+}
+
 // ---------------------------------------------------------------- learned init
 // Patch-match init from learned proposals (no reference counterpart).  A
 // pixel whose quarter-resolution cell predicts a plane with confidence
@@ -1086,6 +1190,10 @@ void init_as(int variant, const DevJob* d_jobs, const int32_t* d_job_start, int 
     if (variant == 1)
         init_kernel<COUNT, PERSIST><<<launch_grid(init_kernel<COUNT, PERSIST>, g), g.nthr, g.smem, st>>>(
             d_jobs, d_job_start, n_jobs, g.tiles, g.queue, nh, census, rays, out, d_work);
+    else if (variant == 2)
+        init_table_kernel<COUNT, PERSIST><<<launch_grid(init_table_kernel<COUNT, PERSIST>, g), g.nthr, g.smem,
+                                            st>>>(d_jobs, d_job_start, n_jobs, g.tiles, g.queue, nh, census, rays,
+                                                  out, d_work);
     else
         init_rows_kernel<COUNT, 4, PERSIST><<<launch_grid(init_rows_kernel<COUNT, 4, PERSIST>, g), g.nthr, g.smem,
                                               st>>>(d_jobs, d_job_start, n_jobs, g.tiles, g.queue, nh, census, rays,

@@ -41,7 +41,8 @@ def _check(ds, jobs, ref, what):
             assert np.array_equal(gb, wb), f"{what}: view {r} {name}: {(gb != wb).sum()} of {gb.size} differ"
 
 
-@pytest.mark.parametrize("flags", [0, FLAG_PERSISTENT, FLAG_CUDA_GRAPH, FLAG_PERSISTENT | FLAG_CUDA_GRAPH])
+@pytest.mark.parametrize("flags", [0, FLAG_PERSISTENT, FLAG_CUDA_GRAPH, FLAG_PERSISTENT | FLAG_CUDA_GRAPH, 128,
+                                   128 | FLAG_PERSISTENT | FLAG_CUDA_GRAPH])
 def test_schedules_match_oracle(uneven, flags):
     sc, opts, jobs, ref = uneven
     ctx = mvs.Context(0)

@@ -338,24 +338,27 @@ def test_fusion_saturated_projection_matches_oracle(ctx):
 
 @pytest.mark.parametrize("ref", [1, 6])
 def test_row_step_and_one_candidate_kernels_agree(ctx, corner_scene, c1_opts, ref):
-    """The default row-step schedule and the one-candidate-at-a-time kernels
-    (RCMVS_FLAG_ONE_CANDIDATE) give the same bits, and with the duplicate
-    skip off (RCMVS_FLAG_NO_SKIP_DUPLICATES) the work counters agree with the
+    """The default row-step schedule, the one-candidate-at-a-time kernels
+    (RCMVS_FLAG_ONE_CANDIDATE) and the table sweep (RCMVS_FLAG_TABLE_INIT)
+    give the same bits, and with the shortcuts off
+    (RCMVS_FLAG_NO_SKIP_DUPLICATES) the work counters agree with the
     oracle's plane_cost call and row counts."""
     import dataclasses
     import os
     v = corner_scene.views
     srcs, zr, _ = mvs.plan(corner_scene.sparse, v, c1_opts)
     a = mvs.estimate_depth(v, ref, srcs[ref], zr[ref, 0], zr[ref, 1], c1_opts, ctx, normals=True)
-    one = dataclasses.replace(c1_opts, flags=1)
-    b = mvs.estimate_depth(v, ref, srcs[ref], zr[ref, 0], zr[ref, 1], one, ctx, normals=True)
-    for x, y in ((a.depth, b.depth), (a.cost, b.cost), (a.normal, b.normal)):
-        assert_bits_equal(x, y)
+    for flags in (1, 128):  # one candidate at a time; the table sweep
+        o = dataclasses.replace(c1_opts, flags=flags)
+        b = mvs.estimate_depth(v, ref, srcs[ref], zr[ref, 0], zr[ref, 1], o, ctx, normals=True)
+        for x, y in ((a.depth, b.depth), (a.cost, b.cost), (a.normal, b.normal)):
+            assert_bits_equal(x, y, f"flags {flags}")
     os.environ["RCMVS_COUNT"] = "1"
     cctx = mvs.Context(0)
     del os.environ["RCMVS_COUNT"]
     _, _, _, work = oracle.estimate_depth(v, ref, srcs[ref], zr[ref, 0], zr[ref, 1], c1_opts)
-    for o in (dataclasses.replace(c1_opts, flags=16), dataclasses.replace(c1_opts, flags=1 | 16)):
+    for o in (dataclasses.replace(c1_opts, flags=16), dataclasses.replace(c1_opts, flags=1 | 16),
+              dataclasses.replace(c1_opts, flags=128 | 16)):
         ds = mvs.DeviceScene(v, cctx)
         ds.estimate([(ref, srcs[ref], zr[ref, 0], zr[ref, 1])], o)
         assert cctx.last_work() == work
@@ -378,7 +381,7 @@ def test_duplicate_skip_keeps_bits_and_saves_rows(ctx, corner_scene, c1_opts, re
     cctx = mvs.Context(0)
     del os.environ["RCMVS_COUNT"]
     counts = {}
-    for flags in (0, 16, 1, 2 | 4):
+    for flags in (0, 16, 1, 2 | 4, 128, 128 | 2):
         ds = mvs.DeviceScene(v, cctx)
         ds.estimate([job], dataclasses.replace(c1_opts, flags=flags))
         dm = ds.depth(ref, normals=True)
@@ -388,5 +391,5 @@ def test_duplicate_skip_keeps_bits_and_saves_rows(ctx, corner_scene, c1_opts, re
         ds.close()
     cctx.close()
     assert counts[16] == (evals_ref, rows_ref)
-    assert counts[0] == counts[1] == counts[2 | 4]
+    assert counts[0] == counts[1] == counts[2 | 4] == counts[128] == counts[128 | 2]
     assert counts[0][1] < 0.9 * rows_ref, (counts[0], rows_ref)
