@@ -20,6 +20,7 @@
 // census with a 2-pixel clamped halo in shared memory; support-view census
 // words are gathered through the read-only path (L1/L2).
 #include <algorithm>
+#include <climits>
 
 #include "rcmvs_internal.cuh"
 #include "learned.cuh"
@@ -921,6 +922,14 @@ __global__ void __launch_bounds__(256)
 // scattered over a tile occupy one warp's lanes together instead of holding
 // every warp that contains one for all 64 hypotheses.  Every pixel's
 // computation is the same; only which thread does it changes.
+// Phase 1's table (init_learned_rows_kernel).  The quarter cells that meet a
+// tile of at most 256 pixels number at most 64 (a 256 x 1 or 1 x 256 tile;
+// tiles start at multiples of their sides), and the window boxes of their
+// pixels hold at most (tw + 4 x cell columns) x (th + 4 x cell rows) cells,
+// 2560 for those two shapes, the largest.
+constexpr int LT_SLOTS = 72;
+constexpr int LT_ENTRIES = 2624;
+
 template <bool PERSIST>
 __global__ void __launch_bounds__(256, 3)
     init_learned_rows_kernel(const DevJob* __restrict__ jobs, const int32_t* __restrict__ job_start, int n_jobs,
@@ -933,6 +942,13 @@ __global__ void __launch_bounds__(256, 3)
     __shared__ int s_n;
     __shared__ unsigned short s_list[256];
     __shared__ float s_seed_cost[256];  // phase 1's best cost per tile pixel (+inf: not seeded)
+    // phase 1's table: per quarter cell of the tile (slot), the box of window
+    // cells its seeded pixels read, the cell's current plane, and the counts
+    __shared__ int s_bx0[LT_SLOTS], s_bx1[LT_SLOTS], s_by0[LT_SLOTS], s_by1[LT_SLOTS];
+    __shared__ int s_off[LT_SLOTS + 1];
+    __shared__ int s_epoch[LT_SLOTS];
+    __shared__ float4 s_pl[LT_SLOTS];
+    __shared__ uint8_t s_cnt[LT_ENTRIES];
     for (int it = 0; PERSIST || it == 0; ++it) {
         const int tile = PERSIST ? next_tile(queue, tiles, it, &s_tile) : (int)blockIdx.x;
         if (tile < 0) break;
@@ -954,8 +970,10 @@ __global__ void __launch_bounds__(256, 3)
         bool learned = false;
         float pnx = 0.f, pny = 0.f, pnz = 1.f, pa = 1.f, pac = 1.f, t0 = 0.f;
         const int wq = J->w >> 2, hq = J->h >> 2;
+        int qx = 0, qy = 0;
         if (inside && wq > 0 && hq > 0) {
-            const int qx = min(x >> 2, wq - 1), qy = min(y >> 2, hq - 1);
+            qx = min(x >> 2, wq - 1);
+            qy = min(y >> 2, hq - 1);
             const float* o = pred + (pred_off[j] + (int64_t)qy * wq + qx) * NET_OUT_C;
             const float len = sqrtf(o[1] * o[1] + o[2] * o[2] + o[3] * o[3]);
             if (o[4] >= logit_thr && len > 1e-6f) {
@@ -973,63 +991,132 @@ __global__ void __launch_bounds__(256, 3)
                 learned = learned && pac >= 0.1f;
             }
         }
-        __syncthreads();  // s_n = 0 is visible
 
-        // phase 1: the local planes of confident lanes, one row per step
-        int k = 0;
-        bool any_local = false;
-        float cz = 0.f, cd = 0.f;
-        auto next_local = [&]() -> bool {
-            while (k < n_local) {
-                const float tk = t0 + span * ((float)k / (float)max(n_local - 1, 1) - 0.5f);
-                ++k;
-                const float inv = inv_min + tk * span_inv;
-                if (!(inv > 0.f)) continue;
-                const float z = 1.f / inv;  // depth on the anchor ray
-                const float dcell = z * pac;
-                const float zi = dcell / pa;  // depth on this pixel's ray
-                if (!(zi >= zlo && zi <= zhi)) continue;
-                cz = zi;
-                cd = dcell;
-                any_local = true;
-                return true;
+        // phase 1: the local planes of the confident pixels.  Every pixel of
+        // a quarter cell that is seeded evaluates the cell's plane (n, d), so
+        // a window cell's count under it -- where the cell's ray meets the
+        // plane, where that point lands in a source, the Hamming distance
+        // there -- is the same for every pixel whose window holds the cell.
+        // Per local plane and source the block computes, for each quarter
+        // cell of the tile (a slot), the counts of the box of window cells
+        // its seeded pixels read, once, into shared memory; then each pixel
+        // runs the reference's chain (five counts per row in dx order, the
+        // abort test, the early rejection) over them.  A source's counts are
+        // computed only for slots that still have a pixel evaluating.
+        const int qx0 = wq > 0 ? min(T.x0 >> 2, wq - 1) : 0, qy0 = hq > 0 ? min(T.y0 >> 2, hq - 1) : 0;
+        const int qx1 = wq > 0 ? min((min(T.x0 + T.tw, J->w) - 1) >> 2, wq - 1) : 0;
+        const int ncx = qx1 - qx0 + 1;
+        const int slot = learned ? (qy - qy0) * ncx + (qx - qx0) : -1;
+        for (int q = threadIdx.x; q < LT_SLOTS; q += blockDim.x) {
+            s_bx0[q] = INT_MAX;
+            s_bx1[q] = INT_MIN;
+            s_by0[q] = INT_MAX;
+            s_by1[q] = INT_MIN;
+            s_epoch[q] = 0;
+        }
+        __syncthreads();  // also: s_n = 0 is visible
+        if (learned) {  // the window cells of this pixel, in shared-tile coordinates
+            atomicMin(&s_bx0[slot], lx);
+            atomicMax(&s_bx1[slot], lx + 2 * HALO);
+            atomicMin(&s_by0[slot], ly);
+            atomicMax(&s_by1[slot], ly + 2 * HALO);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int o = 0;
+            for (int q = 0; q < LT_SLOTS; ++q) {
+                s_off[q] = o;
+                if (s_bx1[q] >= s_bx0[q]) o += (s_bx1[q] - s_bx0[q] + 1) * (s_by1[q] - s_by0[q] + 1);
             }
-            return false;
-        };
+            s_off[LT_SLOTS] = o;
+        }
+        __syncthreads();
+        const int n_entries = s_off[LT_SLOTS];
+        bool any_local = false;
         float best_c = INFINITY;
         float4 plane = make_float4(0.0f, 0.0f, 1.0f, 0.0f);
         float plane_d = 0.f;
-        bool live = inside && learned && next_local();
-        int si = 0, dy = 0;
-        float sum = 0.f, thr = INFINITY, rej = INFINITY;
         const bool early = out.d != nullptr;  // early rejection off for the reference call sequence
         int32_t hs = 0;
-        while (live) {
-            bool fin = true, aborted = false;
-            if (nsrc > 0) {
-                const SrcRegs s = load_src(sm.src[si], census);
-                sum = cost_row<false, false>(sm, (ly + dy) * T.stw + lx, s, pnx, pny, pnz, cd, sum, hs);
-                aborted = sum / ((float)(dy + 1) * 5.0f * (float)(si + 1)) > thr || sum >= rej;
-                fin = aborted || (si == nsrc - 1 && dy == 4);
+        for (int k = 0; k < n_local; ++k) {
+            // this pixel's plane k: the cell's predicted depth on the anchor
+            // ray, the cell's offset d, this pixel's depth
+            bool ev = false;
+            float zi = 0.f, dcell = 0.f;
+            if (learned) {
+                const float tk = t0 + span * ((float)k / (float)max(n_local - 1, 1) - 0.5f);
+                const float inv = inv_min + tk * span_inv;
+                if (inv > 0.f) {
+                    const float z = 1.f / inv;  // depth on the anchor ray
+                    dcell = z * pac;
+                    zi = dcell / pa;  // depth on this pixel's ray
+                    ev = zi >= zlo && zi <= zhi;
+                    s_pl[slot] = make_float4(pnx, pny, pnz, dcell);  // the same values from every pixel of the cell
+                }
             }
-            if (fin) {
-                const float c = aborted ? 1e9f : sum / total;
+            any_local = any_local || ev;
+            const float thr = (best_c + 0.02f) + 0.12f;  // +inf for the first plane
+            const float rej = early ? reject_bound(best_c, total) : INFINITY;
+            bool alive = ev;
+            float sum = 0.f;
+            for (int si = 0; si < nsrc; ++si) {
+                const int epoch = k * 64 + si + 1;
+                if (alive) s_epoch[slot] = epoch;
+                if (!__syncthreads_or(alive)) break;  // also: the previous counts are no longer read
+                const SrcRegs s = load_src(sm.src[si], census);
+                for (int e = threadIdx.x; e < n_entries; e += blockDim.x) {
+                    int q = 0;
+                    while (s_off[q + 1] <= e) ++q;  // the slot of entry e
+                    if (s_epoch[q] != epoch) continue;
+                    const int bw = s_bx1[q] - s_bx0[q] + 1;
+                    const int r = e - s_off[q];
+                    const int c = (s_by0[q] + r / bw) * T.stw + s_bx0[q] + r % bw;
+                    const float4 pl = s_pl[q];
+                    // one window term of cost_row (stereo.rs:185-213)
+                    const float2 rr = sm.ray[c];
+                    const float denom = pl.x * rr.x + pl.y * rr.y + pl.z;
+                    const float z = pl.w / denom;
+                    const float xr = z * rr.x;
+                    const float yr = z * rr.y;
+                    const float xs = s.rs0 * xr + s.rs1 * yr + s.rs2 * z + s.ts0;
+                    const float ys = s.rs3 * xr + s.rs4 * yr + s.rs5 * z + s.ts1;
+                    const float zs = s.rs6 * xr + s.rs7 * yr + s.rs8 * z + s.ts2;
+                    const float xn = xs / zs;
+                    const float yn = ys / zs;
+                    const float dist = 1.0f + s.k * (xn * xn + yn * yn);
+                    int u, v;
+                    const bool in_u = trunc_index(s.f * xn * dist + s.cx, s.swf, u);
+                    const bool in_v = trunc_index(s.f * yn * dist + s.cy, s.shf, v);
+                    const bool ok = !(denom < 0.05f) && !(zs < 1e-3f) && in_u && in_v;
+                    const uint64_t cs = __ldg(s.sc + (ok ? (size_t)v * s.sw + u : (size_t)0));
+                    s_cnt[e] = ok ? (uint8_t)__popcll(sm.cen[c] ^ cs) : (uint8_t)48;
+                }
+                __syncthreads();
+                if (alive) {
+                    const float fsi = (float)(si + 1);
+                    const int bw = s_bx1[slot] - s_bx0[slot] + 1;
+                    const int base = s_off[slot] + (ly - s_by0[slot]) * bw + (lx - s_bx0[slot]);
+#pragma unroll
+                    for (int dy = 0; dy < 5; ++dy) {
+#pragma unroll
+                        for (int dx = 0; dx < 5; ++dx) sum += sm.tab[s_cnt[base + dy * bw + dx]];
+                        if (sum / ((float)(dy + 1) * 5.0f * fsi) > thr || sum >= rej) {
+                            alive = false;
+                            break;
+                        }
+                    }
+                }
+            }
+            if (ev) {
+                const float c = alive ? sum / total : 1e9f;
                 if (c < best_c) {
                     best_c = c;
-                    plane = make_float4(pnx, pny, pnz, cz);
-                    plane_d = cd;
+                    plane = make_float4(pnx, pny, pnz, zi);
+                    plane_d = dcell;
                 }
-                live = next_local();
-                sum = 0.f;
-                si = 0;
-                dy = 0;
-                thr = (best_c + 0.02f) + 0.12f;
-                if (early) rej = reject_bound(best_c, total);
-            } else if (++dy == 5) {
-                dy = 0;
-                ++si;
             }
         }
+        (void)hs;
         const bool seeded = inside && learned && any_local;
         if (seeded) {
             const size_t i = (size_t)J->off + (size_t)y * J->w + x;

@@ -279,9 +279,13 @@ def test_learned_init_with_committed_weights_matches_oracle(ctx, flags):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("w,h,n_local,span,flags", [(98, 71, 3, 0.2, 32), (98, 71, 3, 0.2, 0),
-                                                    (101, 64, 1, 0.0, 64), (64, 43, 5, 1.0, 32 | 64)])
-def test_learned_init_random_proposals_match_oracle(ctx, w, h, n_local, span, flags):
+@pytest.mark.parametrize("w,h,n_local,span,flags,tile", [(98, 71, 3, 0.2, 32, (8, 8)), (98, 71, 3, 0.2, 0, (8, 8)),
+                                                         (101, 64, 1, 0.0, 64, (8, 8)),
+                                                         (64, 43, 5, 1.0, 32 | 64, (8, 8)),
+                                                         (98, 71, 2, 0.3, 32, (16, 16)), (98, 71, 1, 0.0, 0, (32, 4)),
+                                                         (101, 67, 2, 0.1, 32, (4, 8)),
+                                                         (101, 67, 1, 0.0, 32, (2, 16))])
+def test_learned_init_random_proposals_match_oracle(ctx, w, h, n_local, span, flags, tile):
     """Random proposals exercise every branch of the learned init: logits
     around the threshold and NaN, degenerate normals, normals facing away
     (n . ray < 0.1 at the pixel or the anchor), t outside [0, 1] (negative
@@ -289,7 +293,8 @@ def test_learned_init_random_proposals_match_oracle(ctx, w, h, n_local, span, fl
     and view sizes that are not multiples of 4 (clamped quarter cells)."""
     sc = scene.corner_room(seed=9, n_views=4, w=w, h=h, f=1.2 * w, arc_deg=36.0, n_patches=30,
                            per_view_sparse=80, device=0)
-    opts = MvsOptions(max_dim=4096, num_sources=2, sweeps=1, num_hyp=24, flags=flags)
+    opts = MvsOptions(max_dim=4096, num_sources=2, sweeps=1, num_hyp=24, flags=flags, tile_w=tile[0],
+                      tile_h=tile[1])
     srcs, zr, _ = mvs.plan(sc.sparse, sc.views, opts)
     jobs = [(i, srcs[i], zr[i, 0], zr[i, 1]) for i in range(4) if srcs[i]]
     assert jobs
