@@ -9,7 +9,9 @@ gate.  One step = census + rays, patch-match stereo for all 100 views, and
 geometric-consistency fusion with voxel dedup (the PLY vertex records are
 packed on the device).  Two arms run on the same scene: the reference's
 schedule (plane-sweep init + 6 sweeps) and learned init (the committed
-proposal network, rustcolmap_b200/weights/proposal_c4.npy) + 2 sweeps; both
+proposal network, rustcolmap_b200/weights/proposal_c4.npy) + 3 sweeps with a
+0.26 cost gate (the operating point where its ground-truth coverage and
+precision both reach the plain arm's); both
 report the fraction of ground-truth pixels within 1% inverse depth.
 
 value  depth maps/s of the learned arm with inputs resident in HBM
@@ -287,17 +289,29 @@ def _has_gpu():
 METRIC = "1080p depth maps/s at K=10: learned-init vs plain GPU patch-match at equal GT error"
 
 
-def gt_summary(ds, sc, jobs, scene):
+def gt_summary(ds, sc, jobs, scene, stricter_gate=None):
     """Ground truth over every job: fraction of pixels with ground truth that
-    are valid and within 1% inverse depth, and the same over valid pixels."""
+    are valid and within 1% inverse depth ('within_1pct', coverage), and the
+    same over valid pixels ('accuracy', precision).  With stricter_gate the
+    same two figures are added for the maps gated at that cost (a stricter
+    gate only removes pixels, so the run's own maps give them)."""
     within = gt_px = valid = 0
+    w2 = v2 = 0
     for (ref, _, _, _) in jobs:
-        m = scene.gt_metrics(ds.depth(ref).depth, sc.gt_depth[ref])
+        dm = ds.depth(ref)
+        m = scene.gt_metrics(dm.depth, sc.gt_depth[ref])
         within += m["within"]
         gt_px += m["gt_pixels"]
         valid += m["valid"]
-    return {"within_1pct": within / max(gt_px, 1), "accuracy": within / max(valid, 1),
-            "tol": "1% relative inverse depth", "views": len(jobs)}
+        if stricter_gate is not None:
+            m2 = scene.gt_metrics(np.where(dm.cost < stricter_gate, dm.depth, 0).astype(np.float32), sc.gt_depth[ref])
+            w2 += m2["within"]
+            v2 += m2["valid"]
+    out = {"within_1pct": within / max(gt_px, 1), "accuracy": within / max(valid, 1),
+           "tol": "1% relative inverse depth", "views": len(jobs)}
+    if stricter_gate is not None:
+        out[f"at_gate_{stricter_gate:g}"] = {"within_1pct": w2 / max(gt_px, 1), "accuracy": w2 / max(v2, 1)}
+    return out
 
 
 SFM_METRIC = "1600x1200 images/s through SIFT (2048 features) + exhaustive mutual matching of all pairs"
@@ -438,7 +452,7 @@ def run_sfm(args):
 
 def run_shard(args, cfg):
     """--shard: ONE scene split over the N ranks (strong scaling): each rank
-    runs stereo (learned init + 2 sweeps) for its share of the reference
+    runs stereo (the learned arm's schedule) for its share of the reference
     views, the depth maps and fusion candidates move device to device
     through NCCL, and every rank dedups the same candidate list
     (shard.run_mvs_sharded_device).  A step is the whole scene; value =
@@ -464,7 +478,7 @@ def run_shard(args, cfg):
             port = so.getsockname()[1]
         dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
                                 timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
-    opts = dataclasses.replace(cfg["opts"], sweeps=2)
+    opts = learned.learned_options(cfg["opts"])
     sc = make_scene(cfg, seed=5, device=local)  # the same scene on every rank
     n_maps = len(make_jobs(cfg, sc, opts)[0])
     ctx = mvs.Context(local)
@@ -504,7 +518,8 @@ def run_shard(args, cfg):
                            "parallelism": f"one scene sharded over {ws} rank(s): reference views by "
                                          "longest-processing-time, depth maps and candidates all-gathered "
                                          "device to device (NCCL)",
-                           "headline_arm": "learned init (proposal_c4 weights) + 2 sweeps"},
+                           "headline_arm": f"learned init (proposal_c4 weights) + {opts.sweeps} sweeps, "
+                                           f"gate cost < {opts.cost_thr:g}"},
                 "fused_points": int(len(out["xyz"])),
                 "gpu_launches": args.steps * (1 + 3 + 6 + 1 + 2 * opts.sweeps + 1 + 5), "clocks": clocks}
         print(json.dumps(line), flush=True)
@@ -576,7 +591,7 @@ def main():
     if args.tile:
         opts.tile_w, opts.tile_h = map(int, args.tile.lower().split("x"))
     opts.threads_per_pixel = args.tpp
-    lopts = dataclasses.replace(opts, sweeps=2)
+    lopts = learned.learned_options(opts)
     t_setup = time.perf_counter()
     sc = make_scene(cfg, seed=5 + 1000 * rank, device=local)
     jobs, fus = make_jobs(cfg, sc, opts)
@@ -634,7 +649,8 @@ def main():
         kt = {k: ctx.kernel_time(k) for k in names}
         ctx.timing(False)
         ms_max = max_over_ranks(ms, ws, local)
-        return ms_max, kt, npts, ck, gt_summary(ds, sc, jobs, scene)
+        gate = lopts.cost_thr if step is step_plain and lopts.cost_thr < opts.cost_thr else None
+        return ms_max, kt, npts, ck, gt_summary(ds, sc, jobs, scene, stricter_gate=gate)
 
     if args.learned_only:  # tuning runs: no plain arm
         plain_ms, plain_kt, plain_pts, plain_clk, plain_gt = float("nan"), {}, 0, None, {"within_1pct": float("nan")}
@@ -719,7 +735,8 @@ def main():
                        "headline_arm": "plain, 6 sweeps" if args.plain_only else
                        f"learned init (proposal_c4 weights; pixels with confidence >= "
                        f"{args.conf if args.conf is not None else learned.CONF_THR} start from the "
-                       "predicted plane, the others from the 64-plane sweep) + 2 sweeps",
+                       f"predicted plane, the others from the 64-plane sweep) + {lopts.sweeps} sweeps, "
+                       f"gate cost < {lopts.cost_thr:g}",
                        "parallelism": f"views batched on 1 GPU; {ws} rank(s), one independent scene each",
                        "l2": "inputs larger than L2 (census 8 B/px, rays 8 B/px, planes 40 B/px over all views)"},
             "plain": {"value": plain_value, "unit": "depth maps/s", "sweeps": opts.sweeps,

@@ -93,6 +93,21 @@ def costvol(ds, jobs, out_ptr):
 # range around the prediction was both slower and less accurate.)
 LOCAL_HYPS, LOCAL_SPAN, CONF_THR = 1, 0.0, 0.02
 LEARNED_FLAGS = 0  # RCMVS_FLAG_* bits of the learned arm
+# The learned arm's schedule and final gate: learned init + LEARNED_SWEEPS
+# sweeps, a pixel valid when its cost is below LEARNED_COST_THR.  Chosen on
+# the tuning scenes (seeds 5000-5019) as the fastest setting whose coverage
+# (pixels with ground truth that are valid and within 1% inverse depth) and
+# precision (valid pixels within 1%) are both at least the plain method's
+# with 6 sweeps at the reference's gate (0.38); with 2 sweeps no gate
+# reaches both.
+LEARNED_SWEEPS, LEARNED_COST_THR = 3, 0.26
+
+
+def learned_options(opts):
+    """opts with the learned arm's sweeps, gate and flags."""
+    import dataclasses
+    return dataclasses.replace(opts, sweeps=LEARNED_SWEEPS, cost_thr=LEARNED_COST_THR,
+                               flags=opts.flags | LEARNED_FLAGS)
 
 
 def estimate_learned(ds, jobs, opts, net, conf_thr=CONF_THR, n_local=LOCAL_HYPS, span=LOCAL_SPAN):
@@ -234,8 +249,8 @@ def train(net, x, lab, iters=1500, batch=16, lr=1e-3, seed=0, log=print):
     return losses
 
 
-def evaluate(net, seeds, ctx, conf_thr=CONF_THR, sweeps_learned=2, log=print, n_local=LOCAL_HYPS, span=LOCAL_SPAN,
-             flags=None):
+def evaluate(net, seeds, ctx, conf_thr=CONF_THR, sweeps_learned=None, log=print, n_local=LOCAL_HYPS, span=LOCAL_SPAN,
+             flags=None, cost_thr=None):
     """On held-out scenes: the plain method with 6 sweeps, the plain method
     with `sweeps_learned` sweeps (what the network's init replaces it with),
     and learned init + `sweeps_learned` sweeps.  Reports stereo views/s (CUDA
@@ -244,10 +259,12 @@ def evaluate(net, seeds, ctx, conf_thr=CONF_THR, sweeps_learned=2, log=print, n_
     inverse depth ('within') and of valid pixels that are ('accuracy')."""
     import torch
     rows = []
+    sweeps_learned = LEARNED_SWEEPS if sweeps_learned is None else sweeps_learned
     short = MvsOptions(max_dim=C4_OPTS.max_dim, num_sources=C4_OPTS.num_sources, sweeps=sweeps_learned,
                        num_hyp=C4_OPTS.num_hyp)
     lopts = MvsOptions(max_dim=C4_OPTS.max_dim, num_sources=C4_OPTS.num_sources, sweeps=sweeps_learned,
-                       num_hyp=C4_OPTS.num_hyp, flags=LEARNED_FLAGS if flags is None else flags)
+                       num_hyp=C4_OPTS.num_hyp, flags=LEARNED_FLAGS if flags is None else flags,
+                       cost_thr=LEARNED_COST_THR if cost_thr is None else cost_thr)
     for seed in seeds:
         sc = orbit_c4(seed)
         srcs, zr, _ = mvs.plan(sc.sparse, sc.views, C4_OPTS)
