@@ -10,7 +10,7 @@ geometric-consistency fusion with voxel dedup (the PLY vertex records are
 packed on the device).  Two arms run on the same scene: the reference's
 schedule (plane-sweep init + 6 sweeps) and learned init (the committed
 proposal network, rustcolmap_b200/weights/proposal_c4.npy) + 3 sweeps with a
-0.26 cost gate (the operating point where its ground-truth coverage and
+0.25 cost gate (the operating point where its ground-truth coverage and
 precision both reach the plain arm's); both
 report the fraction of ground-truth pixels within 1% inverse depth.
 
@@ -781,7 +781,8 @@ def main():
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in head_kt.items() if v[1]},
             "fused_points": head_pts,
             "setup_s": setup_s,
-            "kernels": "one-candidate init" if opts.flags & 1 else "row-step init",
+            "kernels": ("one-candidate init" if opts.flags & 1 else
+                        "row-step init" if opts.flags & 128 else "table-sweep init"),
             "schedule": {"tile": f"{opts.tile_w}x{opts.tile_h}" if opts.tile_w else "8x8 (library default)",
                          "threads_per_pixel": max(opts.threads_per_pixel, 1), "flags": opts.flags,
                          "persistent_queue": bool(opts.flags & 2), "cuda_graph": bool(opts.flags & 4),

@@ -71,9 +71,8 @@ typedef struct rcmvs_options {
 
 /* The plane-sweep init evaluates each pixel's hypotheses one at a time, a
  * warp waiting at every hypothesis for its slowest lane, instead of the
- * default row-step schedule (each lane advances its own hypothesis stream
- * one 5-term window row per step).  Same results bit for bit; kept for
- * comparison.  The pass kernel always works one candidate at a time, which
+ * default table sweep (RCMVS_FLAG_ROW_STEP_INIT).  Same results bit for
+ * bit; kept for comparison.  The pass kernel always works one candidate at a time, which
  * keeps a warp's source-census gathers on one support view. */
 #define RCMVS_FLAG_ONE_CANDIDATE 1u
 
@@ -119,12 +118,14 @@ typedef struct rcmvs_options {
  * pixel skips the sweep. */
 #define RCMVS_FLAG_SEED_AND_SWEEP 64u
 
-/* The plane sweep of the init walks the hypotheses block by block: for each
- * hypothesis and support view the window counts of a tile and its halo are
- * computed once into shared memory (on a fronto-parallel plane a window
- * cell's count does not depend on which pixel's window holds it) and every
- * pixel runs the reference's chain over them.  Same results bit for bit. */
-#define RCMVS_FLAG_TABLE_INIT 128u
+/* The plane sweep of the init by default walks the hypotheses block by
+ * block: for each hypothesis and support view the window counts of a tile
+ * and its halo are computed once into shared memory (on a fronto-parallel
+ * plane a window cell's count does not depend on which pixel's window holds
+ * it) and every pixel runs the reference's chain over them.  This flag
+ * selects the row-step sweep instead (each lane streams its own hypotheses
+ * one window row at a time).  Same results bit for bit. */
+#define RCMVS_FLAG_ROW_STEP_INIT 128u
 
 /* Fills `MvsOptions::default()` (mvs/src/lib.rs:56-70); extensions off. */
 void rcmvs_options_default(rcmvs_options* opts);

@@ -401,7 +401,7 @@ int rcmvs_scene_estimate_depth(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job*
     constexpr uint32_t kFlags = RCMVS_FLAG_ONE_CANDIDATE | RCMVS_FLAG_PERSISTENT | RCMVS_FLAG_CUDA_GRAPH |
                                 RCMVS_FLAG_AUTOTUNE | RCMVS_FLAG_NO_SKIP_DUPLICATES | RCMVS_FLAG_INIT_ONLY |
                                 RCMVS_FLAG_SEED_AND_SWEEP |  // only affects the learned init
-                                RCMVS_FLAG_TABLE_INIT;
+                                RCMVS_FLAG_ROW_STEP_INIT;
     if (opts->flags & ~kFlags) return fail(ctx, RCMVS_E_ARG, "unknown bits in opts->flags");
     if (n_jobs == 0) return RCMVS_OK;
     CK(cudaSetDevice(ctx->device));
@@ -412,9 +412,9 @@ int rcmvs_scene_estimate_depth(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job*
     unsigned long long* dw = ctx->count_work ? ctx->d_work : nullptr;
     if (dw) CK(cudaMemsetAsync(dw, 0, 2 * sizeof(unsigned long long), st));
     Schedule s;
-    s.init = (opts->flags & RCMVS_FLAG_ONE_CANDIDATE) ? Schedule::ONE_CANDIDATE
-             : (opts->flags & RCMVS_FLAG_TABLE_INIT)   ? Schedule::TABLE
-                                                       : Schedule::ROWS;
+    s.init = (opts->flags & RCMVS_FLAG_ONE_CANDIDATE)  ? Schedule::ONE_CANDIDATE
+             : (opts->flags & RCMVS_FLAG_ROW_STEP_INIT) ? Schedule::ROWS
+                                                        : Schedule::TABLE;
     s.nh = (int)std::max<uint32_t>(opts->num_hyp, 2u);
     s.n_passes = (opts->flags & RCMVS_FLAG_INIT_ONLY) ? 0 : (uint64_t)std::max<uint32_t>(opts->sweeps, 1u) * 2;
     s.cost_thr = opts->cost_thr;

@@ -43,11 +43,11 @@ int sfail(rcmvs_ctx* ctx, int code, const std::string& msg) {
 float powf_host(float b, float e) { return powf(b, e); }
 
 bool shape_ok(TileShape ts) { return tile_shape_ok(ts); }
-// launch_init's kernel for the option flags: 1 one candidate at a time, 2 the
-// table sweep, 0 the row-step sweep.
+// launch_init's kernel for the option flags: 1 one candidate at a time, 0 the
+// row-step sweep, 2 the table sweep (the default: 3x faster on C5).
 int init_variant(uint32_t flags) {
     if (flags & RCMVS_FLAG_ONE_CANDIDATE) return 1;
-    return (flags & RCMVS_FLAG_TABLE_INIT) ? 2 : 0;
+    return (flags & RCMVS_FLAG_ROW_STEP_INIT) ? 0 : 2;
 }
 // Split passes (5 lanes per pixel): at most 128 pixels, so a block of
 // split_threads(px) threads at the kernel's 80 registers fits an SM.

@@ -21,7 +21,7 @@ FLAG_AUTOTUNE = 8       # per-resolution-class tile shapes from the autotuner
 FLAG_NO_SKIP_DUPLICATES = 16  # reference call sequence: no duplicate skip, no early rejection (work counts)
 FLAG_INIT_ONLY = 32     # diagnostic: init and gate only, no passes
 FLAG_SEED_AND_SWEEP = 64  # learned init: seeded pixels also run the plane sweep
-FLAG_TABLE_INIT = 128   # plane sweep over per-tile tables of window counts
+FLAG_ROW_STEP_INIT = 128  # row-step plane sweep instead of the default table sweep
 FLAGS_BATCHED = FLAG_PERSISTENT | FLAG_CUDA_GRAPH | FLAG_AUTOTUNE
 
 

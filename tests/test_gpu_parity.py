@@ -338,9 +338,9 @@ def test_fusion_saturated_projection_matches_oracle(ctx):
 
 @pytest.mark.parametrize("ref", [1, 6])
 def test_row_step_and_one_candidate_kernels_agree(ctx, corner_scene, c1_opts, ref):
-    """The default row-step schedule, the one-candidate-at-a-time kernels
-    (RCMVS_FLAG_ONE_CANDIDATE) and the table sweep (RCMVS_FLAG_TABLE_INIT)
-    give the same bits, and with the shortcuts off
+    """The default table sweep, the one-candidate-at-a-time kernels
+    (RCMVS_FLAG_ONE_CANDIDATE) and the row-step sweep
+    (RCMVS_FLAG_ROW_STEP_INIT) give the same bits, and with the shortcuts off
     (RCMVS_FLAG_NO_SKIP_DUPLICATES) the work counters agree with the
     oracle's plane_cost call and row counts."""
     import dataclasses
@@ -348,7 +348,7 @@ def test_row_step_and_one_candidate_kernels_agree(ctx, corner_scene, c1_opts, re
     v = corner_scene.views
     srcs, zr, _ = mvs.plan(corner_scene.sparse, v, c1_opts)
     a = mvs.estimate_depth(v, ref, srcs[ref], zr[ref, 0], zr[ref, 1], c1_opts, ctx, normals=True)
-    for flags in (1, 128):  # one candidate at a time; the table sweep
+    for flags in (1, 128):  # one candidate at a time; the row-step sweep
         o = dataclasses.replace(c1_opts, flags=flags)
         b = mvs.estimate_depth(v, ref, srcs[ref], zr[ref, 0], zr[ref, 1], o, ctx, normals=True)
         for x, y in ((a.depth, b.depth), (a.cost, b.cost), (a.normal, b.normal)):
