@@ -93,16 +93,16 @@ typedef struct rcmvs_options {
  * first.  Overrides tile_w/tile_h.  Same results bit for bit. */
 #define RCMVS_FLAG_AUTOTUNE 8u
 
-/* Evaluate every candidate the way the reference does.  By default two
+/* Evaluate every candidate the way the reference does.  By default three
  * exact shortcuts run: a Jacobi pass skips a neighbour's plane that is bit
  * for bit the plane (normal and offset d) the pixel's stored cost was
  * computed with (its cost would be that same cost, or an early abort, and
- * never lower, so it can not be accepted), and every evaluation (init and
+ * never lower, so it can not be accepted); every evaluation (init and
  * passes) stops once its window sum reaches best_cost * 25K (the sum only
  * grows, so the candidate's cost could not be below the best and it could
- * not be kept).  Neither changes an output bit, only the work counters
- * (rcmvs_last_work), which with this flag count the reference's calls and
- * rows. */
+ * not be kept); and the repeat skip of RCMVS_FLAG_NO_REPEAT_SKIP.  None
+ * changes an output bit, only the work counters (rcmvs_last_work), which
+ * with this flag count the reference's calls and rows. */
 #define RCMVS_FLAG_NO_SKIP_DUPLICATES 16u
 
 /* Diagnostic: run the init (plane sweep, or the learned init) and the gate
@@ -126,6 +126,18 @@ typedef struct rcmvs_options {
  * selects the row-step sweep instead (each lane streams its own hypotheses
  * one window row at a time).  Same results bit for bit. */
 #define RCMVS_FLAG_ROW_STEP_INIT 128u
+
+/* Turns off the repeat skip alone (it is also off under
+ * RCMVS_FLAG_NO_SKIP_DUPLICATES).  By default a Jacobi pass does not
+ * evaluate the plane of a neighbour that the previous pass left unchanged,
+ * unless that pass refused the pixel's best candidate (n . ray <= 0.05):
+ * the neighbour offered the same plane in the previous pass, where it could
+ * not beat that pass's best, and whether a candidate beats a best value is
+ * monotone in that value (a lower best only makes the early abort and the
+ * rejection bound fire sooner), so it cannot win now.  The first pass after
+ * the init evaluates every candidate.  Same results bit for bit; fewer
+ * window rows. */
+#define RCMVS_FLAG_NO_REPEAT_SKIP 256u
 
 /* Fills `MvsOptions::default()` (mvs/src/lib.rs:56-70); extensions off. */
 void rcmvs_options_default(rcmvs_options* opts);
@@ -605,8 +617,9 @@ int rcmvs_run_mvs_learned(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_vie
  *     a device loads the library's module there, so make the first call on
  *     a device before any stream capture.
  *   - opts->flags may hold RCMVS_FLAG_ONE_CANDIDATE, RCMVS_FLAG_INIT_ONLY,
- *     RCMVS_FLAG_NO_SKIP_DUPLICATES (this entry point never skips) and
- *     RCMVS_FLAG_SEED_AND_SWEEP (no effect here); the scheduling flags
+ *     RCMVS_FLAG_NO_SKIP_DUPLICATES and RCMVS_FLAG_NO_REPEAT_SKIP (this
+ *     entry point never skips) and RCMVS_FLAG_SEED_AND_SWEEP (no effect
+ *     here); the scheduling flags
  *     (PERSISTENT, CUDA_GRAPH, AUTOTUNE) give RCMVS_E_ARG.  The tile is
  *     tile_w x tile_h, default 8x8, as for rcmvs_estimate_depth.
  *   - All calls on a device share the array and leave its contents behind;

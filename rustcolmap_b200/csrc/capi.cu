@@ -202,10 +202,10 @@ void rcmvs_points_free(rcmvs_points* p) {
 namespace {
 
 void** scene_big(rcmvs_scene* sc, int i) {
-    void** m[13] = {(void**)&sc->gray,    (void**)&sc->rgb,     (void**)&sc->census, (void**)&sc->rays,
-                    (void**)&sc->plane_a, (void**)&sc->plane_b, (void**)&sc->pcost_a, (void**)&sc->pcost_b,
-                    (void**)&sc->pd_a,    (void**)&sc->pd_b,    (void**)&sc->depth,   (void**)&sc->cost,
-                    (void**)&sc->normal};
+    void** m[kSceneBig] = {(void**)&sc->gray,    (void**)&sc->rgb,     (void**)&sc->census, (void**)&sc->rays,
+                           (void**)&sc->plane_a, (void**)&sc->plane_b, (void**)&sc->pcost_a, (void**)&sc->pcost_b,
+                           (void**)&sc->pd_a,    (void**)&sc->pd_b,    (void**)&sc->depth,   (void**)&sc->cost,
+                           (void**)&sc->normal,  (void**)&sc->pf_a,    (void**)&sc->pf_b};
     return m[i];
 }
 
@@ -251,7 +251,7 @@ void rcmvs_scene_destroy(rcmvs_scene* sc) {
         // keep the buffers for the context's next scene
         free_spare(sc->ctx);
         rcmvs_ctx::SpareScene& s = sc->ctx->spare;
-        for (int i = 0; i < 13; ++i) s.big[i] = *scene_big(sc, i);
+        for (int i = 0; i < kSceneBig; ++i) s.big[i] = *scene_big(sc, i);
         for (int i = 0; i < 3; ++i) s.small[i] = *scene_small(sc, i);
         s.arena.slots = std::move(sc->arena.slots);
         sc->arena.slots.clear();
@@ -259,7 +259,7 @@ void rcmvs_scene_destroy(rcmvs_scene* sc) {
         s.cap_views = sc->cap_views;
         s.valid = true;
     } else {
-        for (int i = 0; i < 13; ++i)
+        for (int i = 0; i < kSceneBig; ++i)
             if (*scene_big(sc, i)) cudaFree(*scene_big(sc, i));
         for (int i = 0; i < 3; ++i)
             if (*scene_small(sc, i)) cudaFree(*scene_small(sc, i));
@@ -312,7 +312,7 @@ int rcmvs_scene_create(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views,
     rcmvs_ctx::SpareScene& spare = ctx->spare;
     if (spare.valid && spare.cap_px >= np && spare.cap_views >= n_views && (spare.big[1] || !sc->has_rgb)) {
         // the previous scene's buffers and scratch: every one is written before it is read
-        for (int i = 0; i < 13; ++i) *scene_big(sc, i) = spare.big[i];
+        for (int i = 0; i < kSceneBig; ++i) *scene_big(sc, i) = spare.big[i];
         for (int i = 0; i < 3; ++i) *scene_small(sc, i) = spare.small[i];
         sc->arena.slots = std::move(spare.arena.slots);
         spare.arena.slots.clear();
@@ -332,6 +332,8 @@ int rcmvs_scene_create(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views,
     if (!e) e = alloc((void**)&sc->pcost_b, 4 * np);
     if (!e) e = alloc((void**)&sc->pd_a, 4 * np);
     if (!e) e = alloc((void**)&sc->pd_b, 4 * np);
+    if (!e) e = alloc((void**)&sc->pf_a, np);
+    if (!e) e = alloc((void**)&sc->pf_b, np);
     if (!e) e = alloc((void**)&sc->depth, 4 * np);
     if (!e) e = alloc((void**)&sc->cost, 4 * np);
     if (!e) e = alloc((void**)&sc->normal, 12 * np);
@@ -401,7 +403,7 @@ int rcmvs_scene_estimate_depth(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job*
     constexpr uint32_t kFlags = RCMVS_FLAG_ONE_CANDIDATE | RCMVS_FLAG_PERSISTENT | RCMVS_FLAG_CUDA_GRAPH |
                                 RCMVS_FLAG_AUTOTUNE | RCMVS_FLAG_NO_SKIP_DUPLICATES | RCMVS_FLAG_INIT_ONLY |
                                 RCMVS_FLAG_SEED_AND_SWEEP |  // only affects the learned init
-                                RCMVS_FLAG_ROW_STEP_INIT;
+                                RCMVS_FLAG_ROW_STEP_INIT | RCMVS_FLAG_NO_REPEAT_SKIP;
     if (opts->flags & ~kFlags) return fail(ctx, RCMVS_E_ARG, "unknown bits in opts->flags");
     if (n_jobs == 0) return RCMVS_OK;
     CK(cudaSetDevice(ctx->device));
@@ -421,6 +423,7 @@ int rcmvs_scene_estimate_depth(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job*
     s.persistent = (opts->flags & RCMVS_FLAG_PERSISTENT) != 0;
     s.graph = (opts->flags & RCMVS_FLAG_CUDA_GRAPH) != 0;
     s.skip_duplicates = !(opts->flags & RCMVS_FLAG_NO_SKIP_DUPLICATES);
+    s.repeat_skip = !(opts->flags & RCMVS_FLAG_NO_REPEAT_SKIP);
     s.d_work = dw;
     rc = run_batch(ctx, sc, batch, s);
     if (rc) return rc;

@@ -12,6 +12,9 @@ using rcmvs::DeviceArena;
 using rcmvs::SpanHook;
 using rcmvs::TileShape;
 
+// per-pixel device buffers of a scene (rcmvs_scene, SpareScene::big)
+constexpr int kSceneBig = 15;
+
 struct rcmvs_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -36,13 +39,13 @@ struct rcmvs_ctx {
     // by the next scene they are large enough for (rcmvs_scene_create), so
     // repeated rcmvs_run_mvs* calls on a workload allocate nothing.  Freed
     // with the context.  Order of `big`: gray, rgb, census, rays, plane_a,
-    // plane_b, pcost_a, pcost_b, pd_a, pd_b, depth, cost, normal; `small`:
-    // d_views, d_tile_start, d_cams.
+    // plane_b, pcost_a, pcost_b, pd_a, pd_b, depth, cost, normal, pf_a, pf_b;
+    // `small`: d_views, d_tile_start, d_cams.
     struct SpareScene {
         bool valid = false;
         size_t cap_px = 0;
         int cap_views = 0;
-        void* big[13] = {};
+        void* big[kSceneBig] = {};
         void* small[3] = {};
         DeviceArena arena;
     } spare;
@@ -109,6 +112,8 @@ struct rcmvs_scene {
     float* pcost_b = nullptr;
     float* pd_a = nullptr;  // plane offsets d (PlaneBuf::d)
     float* pd_b = nullptr;
+    uint8_t* pf_a = nullptr;  // per-pixel pass flags (PlaneBuf::flag)
+    uint8_t* pf_b = nullptr;
     float* depth = nullptr;
     float* cost = nullptr;
     float* normal = nullptr;
@@ -183,6 +188,7 @@ struct Schedule {
     bool persistent = false;
     bool graph = false;
     bool skip_duplicates = true;  // PlaneBuf::d on: skip repeated propagation candidates
+    bool repeat_skip = true;      // PlaneBuf::flag on (with skip_duplicates): skip candidates that lost before
     unsigned long long* d_work = nullptr;  // work counters (zeroed by the caller)
     // learned init
     const float* pred = nullptr;

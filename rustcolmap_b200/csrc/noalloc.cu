@@ -65,10 +65,11 @@ int scratch_for_current_device(void** out) {
 }
 
 // Flags this entry point accepts: it always runs the one-launch-per-step
-// schedule and never skips duplicate candidates (so NO_SKIP_DUPLICATES holds
-// trivially); SEED_AND_SWEEP concerns the learned init only.
+// schedule and never skips duplicate or repeated candidates (so
+// NO_SKIP_DUPLICATES and NO_REPEAT_SKIP hold trivially); SEED_AND_SWEEP
+// concerns the learned init only.
 constexpr uint32_t kNoallocFlags = RCMVS_FLAG_ONE_CANDIDATE | RCMVS_FLAG_NO_SKIP_DUPLICATES | RCMVS_FLAG_INIT_ONLY |
-                                   RCMVS_FLAG_SEED_AND_SWEEP;
+                                   RCMVS_FLAG_SEED_AND_SWEEP | RCMVS_FLAG_NO_REPEAT_SKIP;
 
 bool finite_pos(double x) { return x > 0.0 && x < 1e300; }
 

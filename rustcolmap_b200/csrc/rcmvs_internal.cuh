@@ -50,11 +50,18 @@ static_assert(sizeof(DevJob) % 8 == 0, "DevJob layout");
 // float4 (nx, ny, nz, z) + float cost.  `d` (nullable) keeps, per pixel, the
 // plane offset d the stored cost was computed with (z = d / (n . ray)); with
 // it the pass kernel skips a propagation candidate that repeats the pixel's
-// own plane bit for bit (see pass_kernel).
+// own plane bit for bit (see pass_kernel).  `flag` (nullable) holds one byte
+// per pixel written by a pass: bit 0 = the pass wrote a new plane, bit 1 =
+// a candidate beat the stored cost but its plane was refused (n . ray <=
+// 0.05), so the stored cost is not the pass's best.  A pass that reads them
+// (prev.flag set, `d` set) skips the propagation candidates that provably
+// lose again (see pass_kernel); prev.flag is null for the first pass after
+// an init.
 struct PlaneBuf {
     float4* nz;   // (nx, ny, nz, z)
     float* cost;
     float* d = nullptr;
+    uint8_t* flag = nullptr;
 };
 
 // Tile shape of one job's stereo launch (pixels per block = tw * th).

@@ -327,8 +327,11 @@ int run_batch(rcmvs_ctx* ctx, rcmvs_scene* sc, const StereoBatch& b, const Sched
     const DevJob* dj = (const DevJob*)pj;
     const int32_t* dst = (const int32_t*)ps;
     unsigned int* queue = (unsigned int*)pq;
-    PlaneBuf A0{sc->plane_a, sc->pcost_a, s.skip_duplicates ? sc->pd_a : nullptr};
-    PlaneBuf B0{sc->plane_b, sc->pcost_b, s.skip_duplicates ? sc->pd_b : nullptr};
+    // pass flags (the repeat skip) only with the duplicate skip: both off is
+    // the reference's own call sequence
+    const bool repeat = s.skip_duplicates && s.repeat_skip;
+    PlaneBuf A0{sc->plane_a, sc->pcost_a, s.skip_duplicates ? sc->pd_a : nullptr, repeat ? sc->pf_a : nullptr};
+    PlaneBuf B0{sc->plane_b, sc->pcost_b, s.skip_duplicates ? sc->pd_b : nullptr, repeat ? sc->pf_b : nullptr};
     std::vector<float> sig(2 * s.n_passes);
     for (uint64_t pass = 0; pass < s.n_passes; ++pass) {
         const float t = (float)pass / (float)s.n_passes;  // stereo.rs:275-277
@@ -359,7 +362,9 @@ int run_batch(rcmvs_ctx* ctx, rcmvs_scene* sc, const StereoBatch& b, const Sched
         for (uint64_t pass = 0; pass < s.n_passes; ++pass) {
             g.queue = queue ? queue + 1 + pass : nullptr;
             hk.begin("stereo_pass");
-            e = launch_pass(dj, dst, n_jobs, g, pass, sig[2 * pass], sig[2 * pass + 1], sc->census, sc->rays, A, B,
+            PlaneBuf P = A;
+            if (pass == 0) P.flag = nullptr;  // the init leaves no pass flags
+            e = launch_pass(dj, dst, n_jobs, g, pass, sig[2 * pass], sig[2 * pass + 1], sc->census, sc->rays, P, B,
                             s.d_work, st);
             hk.end("stereo_pass");
             if (e) return e;
@@ -392,8 +397,8 @@ int run_batch(rcmvs_ctx* ctx, rcmvs_scene* sc, const StereoBatch& b, const Sched
     append(key, s.span);
     append(key, s.sweep_seeded);
     const void* ptrs[] = {pj, ps, pq, s.d_work, s.pred, s.pred_off, s.d_learned, sc->census, sc->rays,
-                          sc->plane_a, sc->plane_b, sc->pcost_a, sc->pcost_b, A0.d, B0.d, sc->depth, sc->cost,
-                          sc->normal};
+                          sc->plane_a, sc->plane_b, sc->pcost_a, sc->pcost_b, A0.d, B0.d, A0.flag, B0.flag,
+                          sc->depth, sc->cost, sc->normal};
     append(key, ptrs, sizeof(ptrs));
     if (!sc->graph || key != sc->graph_key) {
         drop_graph(sc);

@@ -366,6 +366,17 @@ __global__ void init_kernel(const DevJob* __restrict__ jobs, const int32_t* __re
 // `c < best_c` could not hold and the result is unchanged.  In converged
 // regions most propagated planes are such repeats, and they are the costly
 // calls: with c near best_c they rarely abort.
+// Repeat skip (with prev.flag): a neighbour whose plane the previous pass
+// left unchanged offers the pixel the candidate it offered in that pass.
+// Whether a candidate improves on best value b is monotone in b: at a lower b
+// the abort threshold b + 0.14 and the rejection bound are lower, so a
+// candidate that aborted still aborts and one that completed with cost
+// C >= b still has C >= b.  In the previous pass every neighbour candidate
+// was evaluated (or skipped by one of these rules), so none can improve on
+// that pass's final best value; that value is the stored cost unless the
+// pass refused its best plane (flag bit 1), and this pass's best value never
+// exceeds the stored cost.  So with bit 1 clear, a candidate from a
+// neighbour with bit 0 clear cannot win and is not evaluated.
 // Register cap 72 (28 warps per SM with 64-thread blocks) measured fastest
 // at 960x720 K=8: 3% ahead of 80 and 64, 10% ahead of 96.  MINB only names
 // the instantiation.
@@ -404,6 +415,8 @@ __global__ void __maxnreg__(72)
             // exactly cur_cost or abort, never less, and is skipped
             const bool skip_dup = prev.d != nullptr;
             const float cur_d = skip_dup ? prev.d[i] : 0.f;
+            const uint8_t* __restrict__ pflag = prev.flag;
+            const bool repeat = skip_dup && pflag != nullptr && !(pflag[i] & 2);
             float best_c = cur_cost;
             float bn0 = cur.x, bn1 = cur.y, bn2 = cur.z;
             float bd = cur.w * (bn0 * ri.x + bn1 * ri.y + bn2);
@@ -434,6 +447,12 @@ __global__ void __maxnreg__(72)
             for (int q = 0; q < 4; ++q) {
                 float4 nb;
                 float d_plane;
+                if (repeat) {  // an unchanged neighbour's candidate lost in the previous pass
+                    const int xx = x + (q == 0 ? -1 : (q == 1 ? 1 : 0));
+                    const int yy = y + (q == 2 ? -1 : (q == 3 ? 1 : 0));
+                    if (xx >= 0 && yy >= 0 && xx < w && yy < h && !(pflag[base + (size_t)yy * w + xx] & 1))
+                        continue;
+                }
                 if (!neighbour(q, nb, d_plane)) continue;
                 if (skip_dup && __float_as_uint(d_plane) == __float_as_uint(cur_d) &&
                     __float_as_uint(nb.x) == __float_as_uint(cur.x) && __float_as_uint(nb.y) == __float_as_uint(cur.y) &&
@@ -493,17 +512,22 @@ __global__ void __maxnreg__(72)
 
             float4 o = cur;
             float oc = cur_cost, od = cur_d;
+            uint8_t fl = 0;
             if (best_c < cur_cost) {  // stereo.rs:355-367
                 const float a_here = bn0 * ri.x + bn1 * ri.y + bn2;
                 if (a_here > 0.05f) {
                     o = make_float4(bn0, bn1, bn2, bd / a_here);
                     oc = fminf(best_c, 1.0f);
                     od = bd;
+                    fl = 1;
+                } else {
+                    fl = 2;
                 }
             }
             next.nz[i] = o;
             next.cost[i] = oc;
             if (skip_dup) next.d[i] = od;
+            if (next.flag) next.flag[i] = fl;
         }
     }
     if (COUNT) flush_work(wc, d_work);
@@ -613,6 +637,8 @@ __global__ void __maxnreg__(80)
             const float cur_cost = prev.cost[i];
             const bool skip_dup = prev.d != nullptr;
             const float cur_d = skip_dup ? prev.d[i] : 0.f;
+            const uint8_t* __restrict__ pflag = prev.flag;
+            const bool repeat = skip_dup && pflag != nullptr && !(pflag[i] & 2);
             float best_c = cur_cost;
             float bn0 = cur.x, bn1 = cur.y, bn2 = cur.z;
             float bd = cur.w * (bn0 * ri.x + bn1 * ri.y + bn2);
@@ -636,6 +662,12 @@ __global__ void __maxnreg__(80)
             for (int q = 0; q < 4; ++q) {
                 float4 nb;
                 float d_plane;
+                if (repeat) {  // an unchanged neighbour's candidate lost in the previous pass
+                    const int xx = x + (q == 0 ? -1 : (q == 1 ? 1 : 0));
+                    const int yy = y + (q == 2 ? -1 : (q == 3 ? 1 : 0));
+                    if (xx >= 0 && yy >= 0 && xx < w && yy < h && !(pflag[base + (size_t)yy * w + xx] & 1))
+                        continue;
+                }
                 if (!neighbour(q, nb, d_plane)) continue;
                 if (skip_dup && __float_as_uint(d_plane) == __float_as_uint(cur_d) &&
                     __float_as_uint(nb.x) == __float_as_uint(cur.x) && __float_as_uint(nb.y) == __float_as_uint(cur.y) &&
@@ -693,17 +725,22 @@ __global__ void __maxnreg__(80)
             if (j == 0) {
                 float4 o = cur;
                 float oc = cur_cost, od = cur_d;
+                uint8_t fl = 0;
                 if (best_c < cur_cost) {  // stereo.rs:355-367
                     const float a_here = bn0 * ri.x + bn1 * ri.y + bn2;
                     if (a_here > 0.05f) {
                         o = make_float4(bn0, bn1, bn2, bd / a_here);
                         oc = fminf(best_c, 1.0f);
                         od = bd;
+                        fl = 1;
+                    } else {
+                        fl = 2;
                     }
                 }
                 next.nz[i] = o;
                 next.cost[i] = oc;
                 if (skip_dup) next.d[i] = od;
+                if (next.flag) next.flag[i] = fl;
             }
         }
     }

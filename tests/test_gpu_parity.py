@@ -369,8 +369,10 @@ def test_row_step_and_one_candidate_kernels_agree(ctx, corner_scene, c1_opts, re
 @pytest.mark.parametrize("ref", [2, 5])
 def test_duplicate_skip_keeps_bits_and_saves_rows(ctx, corner_scene, c1_opts, ref):
     """Skipping propagated planes that repeat the pixel's own plane bit for
-    bit (the default) gives the oracle's bits with fewer window rows than
-    the reference's call sequence (RCMVS_FLAG_NO_SKIP_DUPLICATES)."""
+    bit and the planes of neighbours the previous pass left unchanged (the
+    default) gives the oracle's bits with fewer window rows than the
+    reference's call sequence (RCMVS_FLAG_NO_SKIP_DUPLICATES); the repeat
+    skip alone (off with RCMVS_FLAG_NO_REPEAT_SKIP) saves rows too."""
     import dataclasses
     import os
     v = corner_scene.views
@@ -381,7 +383,7 @@ def test_duplicate_skip_keeps_bits_and_saves_rows(ctx, corner_scene, c1_opts, re
     cctx = mvs.Context(0)
     del os.environ["RCMVS_COUNT"]
     counts = {}
-    for flags in (0, 16, 1, 2 | 4, 128, 128 | 2):
+    for flags in (0, 16, 1, 2 | 4, 128, 128 | 2, 256, 256 | 2 | 4):
         ds = mvs.DeviceScene(v, cctx)
         ds.estimate([job], dataclasses.replace(c1_opts, flags=flags))
         dm = ds.depth(ref, normals=True)
@@ -393,3 +395,5 @@ def test_duplicate_skip_keeps_bits_and_saves_rows(ctx, corner_scene, c1_opts, re
     assert counts[16] == (evals_ref, rows_ref)
     assert counts[0] == counts[1] == counts[2 | 4] == counts[128] == counts[128 | 2]
     assert counts[0][1] < 0.9 * rows_ref, (counts[0], rows_ref)
+    assert counts[256] == counts[256 | 2 | 4]
+    assert counts[0][1] < counts[256][1] < rows_ref, (counts[0], counts[256], rows_ref)
