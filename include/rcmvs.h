@@ -93,16 +93,19 @@ typedef struct rcmvs_options {
  * first.  Overrides tile_w/tile_h.  Same results bit for bit. */
 #define RCMVS_FLAG_AUTOTUNE 8u
 
-/* Evaluate every candidate the way the reference does.  By default three
+/* Evaluate every candidate the way the reference does.  By default four
  * exact shortcuts run: a Jacobi pass skips a neighbour's plane that is bit
  * for bit the plane (normal and offset d) the pixel's stored cost was
  * computed with (its cost would be that same cost, or an early abort, and
  * never lower, so it can not be accepted); every evaluation (init and
  * passes) stops once its window sum reaches best_cost * 25K (the sum only
  * grows, so the candidate's cost could not be below the best and it could
- * not be kept); and the repeat skip of RCMVS_FLAG_NO_REPEAT_SKIP.  None
- * changes an output bit, only the work counters (rcmvs_last_work), which
- * with this flag count the reference's calls and rows. */
+ * not be kept); every evaluation also stops once the early-abort test
+ * after the first row of the next support view is certain to fire (that
+ * test divides by 5 * (view + 1), less than the current row's divisor, and
+ * the sum only grows); and the repeat skip of RCMVS_FLAG_NO_REPEAT_SKIP.
+ * None changes an output bit, only the work counters (rcmvs_last_work),
+ * which with this flag count the reference's calls and rows. */
 #define RCMVS_FLAG_NO_SKIP_DUPLICATES 16u
 
 /* Diagnostic: run the init (plane sweep, or the learned init) and the gate

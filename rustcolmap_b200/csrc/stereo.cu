@@ -177,6 +177,19 @@ __device__ __forceinline__ float reject_bound(float best_c, float total) {
     return t < INFINITY ? __int_as_float(__float_as_int(t) + 1) : INFINITY;
 }
 
+// Denominator of the abort test after window row dy of support view si
+// (stereo.rs:215-221): rows_done * 5 * (si + 1), exact in f32.  With `ahead`
+// (an exact shortcut, off for the reference's call sequence) it is capped at
+// 5 * (si + 2), the denominator of the test after the first row of the next
+// view.  The window sum never decreases (every term adds h/48 >= 0) and
+// sum / den only grows as den falls, so once sum / (5 * (si + 2)) exceeds the
+// threshold that later test is certain to fire (if none before it does):
+// the evaluation's result, the abort value, is already known.
+__device__ __forceinline__ float abort_den(int dy, int si, int nsrc, bool ahead) {
+    const float den = (float)(dy + 1) * 5.0f * (float)(si + 1);
+    return (ahead && si + 1 < nsrc) ? fminf(den, 5.0f * (float)(si + 2)) : den;
+}
+
 // ---------------------------------------------------------------- plane_cost
 // One support view in registers.
 struct SrcRegs {
@@ -275,19 +288,17 @@ template <bool FRONTO, bool COUNT, bool HSUM>
 __device__ __forceinline__ float plane_cost(const Smem& sm, int stw, int lx, int ly, int nsrc,
                                             const uint64_t* __restrict__ census, float nx, float ny, float nz,
                                             float d, float hint, float total, WorkCount& wc, int32_t* hsum,
-                                            float rej = INFINITY) {
+                                            float rej = INFINITY, bool ahead = false) {
     float sum = 0.f;
     int32_t hs = 0;
     const float thr = hint + 0.12f;
     if (COUNT) wc.evals++;
     for (int si = 0; si < nsrc; ++si) {
         const SrcRegs s = load_src(sm.src[si], census);
-        const float fsi = (float)(si + 1);
         for (int dy = 0; dy < 5; ++dy) {
             sum = cost_row<FRONTO, HSUM>(sm, (ly + dy) * stw + lx, s, nx, ny, nz, d, sum, hs);
             if (COUNT) wc.rows++;
-            const float rows_done = (float)(dy + 1);
-            if (sum / (rows_done * 5.0f * fsi) > thr || sum >= rej) {
+            if (sum / abort_den(dy, si, nsrc, ahead) > thr || sum >= rej) {
                 if (HSUM) *hsum = hs;
                 return 1e9f;
             }
@@ -339,7 +350,7 @@ __global__ void init_kernel(const DevJob* __restrict__ jobs, const int32_t* __re
                 const float d = 1.0f / inv;
                 const float c = plane_cost<true, COUNT, false>(sm, T.stw, lx, ly, nsrc, census, 0.f, 0.f, 1.f, d,
                                                                best_c + 0.02f, total, wc, nullptr,
-                                                               early ? reject_bound(best_c, total) : INFINITY);
+                                                               early ? reject_bound(best_c, total) : INFINITY, early);
                 if (c < best_c) {
                     best_c = c;
                     best_d = d;
@@ -469,7 +480,8 @@ __global__ void __maxnreg__(72)
                 neighbour(q, nb, d_plane);  // passed above; same values
                 const float c = plane_cost<false, COUNT, false>(sm, stw, lx, ly, nsrc, census, nb.x, nb.y, nb.z,
                                                                       d_plane, best_c + 0.02f, total, wc, nullptr,
-                                                                      skip_dup ? reject_bound(best_c, total) : INFINITY);
+                                                                      skip_dup ? reject_bound(best_c, total) : INFINITY,
+                                                                      skip_dup);
                 if (c < best_c) {
                     best_c = c;
                     bn0 = nb.x;
@@ -500,7 +512,8 @@ __global__ void __maxnreg__(72)
                 const float d_plane = zcand * a_here;
                 const float c = plane_cost<false, COUNT, false>(sm, stw, lx, ly, nsrc, census, nnx, nny, nnz,
                                                                       d_plane, best_c + 0.02f, total, wc, nullptr,
-                                                                      skip_dup ? reject_bound(best_c, total) : INFINITY);
+                                                                      skip_dup ? reject_bound(best_c, total) : INFINITY,
+                                                                      skip_dup);
                 if (c < best_c) {
                     best_c = c;
                     bn0 = nnx;
@@ -552,7 +565,7 @@ template <bool COUNT>
 __device__ __forceinline__ float plane_cost_split(const Smem& sm, int stw, int lx, int ly, int j, unsigned gmask,
                                                   int gbase, int nsrc, const uint64_t* __restrict__ census,
                                                   float nx, float ny, float nz, float d, float hint, float total,
-                                                  WorkCount& wc, float rej) {
+                                                  WorkCount& wc, float rej, bool ahead) {
     float sum = 0.f;
     const float thr = hint + 0.12f;
     if (COUNT && j == 0) wc.evals++;
@@ -560,7 +573,6 @@ __device__ __forceinline__ float plane_cost_split(const Smem& sm, int stw, int l
     unsigned dok = 0;
     for (int si = 0; si < nsrc; ++si) {
         const SrcRegs s = load_src(sm.src[si], census);
-        const float fsi = (float)(si + 1);
 #pragma unroll
         for (int dy = 0; dy < 5; ++dy) {
             const int cell = (ly + dy) * stw + lx + j;
@@ -591,7 +603,7 @@ __device__ __forceinline__ float plane_cost_split(const Smem& sm, int stw, int l
 #pragma unroll
             for (int k = 0; k < SPLIT; ++k) sum += sm.tab[__shfl_sync(gmask, h, gbase + k)];
             if (COUNT && j == 0) wc.rows++;
-            if (sum / ((float)(dy + 1) * 5.0f * fsi) > thr || sum >= rej) return 1e9f;
+            if (sum / abort_den(dy, si, nsrc, ahead) > thr || sum >= rej) return 1e9f;
         }
     }
     return sum / total;
@@ -684,7 +696,7 @@ __global__ void __maxnreg__(80)
                 neighbour(q, nb, d_plane);
                 const float c = plane_cost_split<COUNT>(sm, stw, lx, ly, j, gmask, gbase, nsrc, census, nb.x, nb.y,
                                                         nb.z, d_plane, best_c + 0.02f, total, wc,
-                                                        skip_dup ? reject_bound(best_c, total) : INFINITY);
+                                                        skip_dup ? reject_bound(best_c, total) : INFINITY, skip_dup);
                 if (c < best_c) {
                     best_c = c;
                     bn0 = nb.x;
@@ -713,7 +725,7 @@ __global__ void __maxnreg__(80)
                 const float d_plane = zcand * a_here;
                 const float c = plane_cost_split<COUNT>(sm, stw, lx, ly, j, gmask, gbase, nsrc, census, nnx, nny,
                                                         nnz, d_plane, best_c + 0.02f, total, wc,
-                                                        skip_dup ? reject_bound(best_c, total) : INFINITY);
+                                                        skip_dup ? reject_bound(best_c, total) : INFINITY, skip_dup);
                 if (c < best_c) {
                     best_c = c;
                     bn0 = nnx;
@@ -797,7 +809,7 @@ __global__ void __launch_bounds__(256, MINB)
                 const SrcRegs s = load_src(sm.src[si], census);
                 sum = cost_row<true, false>(sm, (ly + dy) * T.stw + lx, s, 0.f, 0.f, 1.f, d, sum, hs);
                 if (COUNT) wc.rows++;
-                aborted = sum / ((float)(dy + 1) * 5.0f * (float)(si + 1)) > thr || sum >= rej;
+                aborted = sum / abort_den(dy, si, nsrc, early) > thr || sum >= rej;
                 fin = aborted || (si == nsrc - 1 && dy == 4);
             }
             if (fin) {
@@ -904,14 +916,13 @@ __global__ void __launch_bounds__(256)
                 }
                 __syncthreads();
                 if (alive) {
-                    const float fsi = (float)(si + 1);
-#pragma unroll
+            #pragma unroll
                     for (int dy = 0; dy < 5; ++dy) {
                         const int row = (ly + dy) * T.stw + lx;
 #pragma unroll
                         for (int dx = 0; dx < 5; ++dx) sum += sm.tab[s_h[row + dx]];
                         if (COUNT) wc.rows++;
-                        if (sum / ((float)(dy + 1) * 5.0f * fsi) > thr || sum >= rej) {
+                        if (sum / abort_den(dy, si, nsrc, early) > thr || sum >= rej) {
                             alive = false;
                             break;
                         }
@@ -1130,14 +1141,13 @@ __global__ void __launch_bounds__(256, 3)
                 }
                 __syncthreads();
                 if (alive) {
-                    const float fsi = (float)(si + 1);
-                    const int bw = s_bx1[slot] - s_bx0[slot] + 1;
+                                const int bw = s_bx1[slot] - s_bx0[slot] + 1;
                     const int base = s_off[slot] + (ly - s_by0[slot]) * bw + (lx - s_bx0[slot]);
 #pragma unroll
                     for (int dy = 0; dy < 5; ++dy) {
 #pragma unroll
                         for (int dx = 0; dx < 5; ++dx) sum += sm.tab[s_cnt[base + dy * bw + dx]];
-                        if (sum / ((float)(dy + 1) * 5.0f * fsi) > thr || sum >= rej) {
+                        if (sum / abort_den(dy, si, nsrc, early) > thr || sum >= rej) {
                             alive = false;
                             break;
                         }
@@ -1189,7 +1199,7 @@ __global__ void __launch_bounds__(256, 3)
                 if (nsrc > 0) {
                     const SrcRegs s = load_src(sm.src[ssi], census);
                     ssum = cost_row<true, false>(sm, (ply + sdy) * T.stw + plx, s, 0.f, 0.f, 1.f, d, ssum, hs);
-                    aborted = ssum / ((float)(sdy + 1) * 5.0f * (float)(ssi + 1)) > sthr || ssum >= srej;
+                    aborted = ssum / abort_den(sdy, ssi, nsrc, early) > sthr || ssum >= srej;
                     fin = aborted || (ssi == nsrc - 1 && sdy == 4);
                 }
                 if (fin) {
