@@ -49,6 +49,7 @@ void DeviceArena::release() {
 using namespace rcmvs;
 
 #include "ctx_internal.cuh"
+#include "learned.cuh"
 
 namespace {
 
@@ -184,6 +185,9 @@ int rcmvs_ctx_synchronize(rcmvs_ctx* ctx) {
     if (!ctx) return RCMVS_E_ARG;
     CK(cudaSetDevice(ctx->device));
     CK(cudaStreamSynchronize(ctx->stream));
+    const int f = rcmvs::tc_fault_take();
+    if (f) return fail(ctx, RCMVS_E_CUDA, f > 0 ? "a tensor-core kernel timed out waiting for its MMAs"
+                                                 : "could not read the tensor-core fault word");
     return RCMVS_OK;
 }
 

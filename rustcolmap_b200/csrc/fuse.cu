@@ -26,6 +26,7 @@ namespace rcmvs {
 namespace {
 
 constexpr int FT = 256;  // threads per block for pixel kernels
+constexpr int RT = 64;   // threads per block of the voxel reduce: few voxels, spread over every SM
 
 __device__ __forceinline__ int find_item(const int32_t* start, int n, int b) {
     int lo = 0, hi = n - 1;
@@ -257,12 +258,42 @@ __global__ void reduce_kernel(const uint32_t* __restrict__ run_off, const uint32
                               const uint32_t* __restrict__ cand, const double* __restrict__ pts,
                               const uint8_t* __restrict__ rgb, double* __restrict__ out_xyz,
                               uint8_t* __restrict__ out_rgb, uint8_t* __restrict__ ply) {
-    const uint32_t r = blockIdx.x * FT + threadIdx.x;
+    const uint32_t r = blockIdx.x * RT + threadIdx.x;
     if (r >= *n_runs_p) return;
     const uint32_t b = run_off[r], n = run_len[r];
     double sx = 0.0, sy = 0.0, sz = 0.0;
     uint16_t cr = 0, cg = 0, cb = 0;
-    for (uint32_t m = 0; m < n; ++m) {
+    // Members four at a time: the four chains of dependent loads (sorted
+    // position -> candidate -> point) are issued together, then added in
+    // member order, so the f64 sums are the sequential ones.
+    constexpr int U = 4;
+    uint32_t m = 0;
+    for (; m + U <= n; m += U) {
+        size_t g[U];
+#pragma unroll
+        for (int k = 0; k < U; ++k) g[k] = cand[sorted_vals[b + m + k]];
+        double px[U], py[U], pz[U];
+        uint8_t qr[U], qg[U], qb[U];
+#pragma unroll
+        for (int k = 0; k < U; ++k) {
+            px[k] = pts[3 * g[k]];
+            py[k] = pts[3 * g[k] + 1];
+            pz[k] = pts[3 * g[k] + 2];
+            qr[k] = rgb[3 * g[k]];
+            qg[k] = rgb[3 * g[k] + 1];
+            qb[k] = rgb[3 * g[k] + 2];
+        }
+#pragma unroll
+        for (int k = 0; k < U; ++k) {
+            sx += px[k];
+            sy += py[k];
+            sz += pz[k];
+            cr = (uint16_t)(cr + qr[k]);
+            cg = (uint16_t)(cg + qg[k]);
+            cb = (uint16_t)(cb + qb[k]);
+        }
+    }
+    for (; m < n; ++m) {
         const size_t g = cand[sorted_vals[b + m]];
         sx += pts[3 * g];
         sy += pts[3 * g + 1];
@@ -494,7 +525,7 @@ int fuse_reduce_device(DeviceArena& A, const uint32_t* d_cand, uint32_t n_cand, 
     FCK(A.get(S_OUTRGB, 3 * (size_t)n_runs, &p_orgb));
     FCK(A.get(S_PLY, 15 * (size_t)n_runs, &p_ply));
     hook.begin("fuse_reduce");
-    reduce_kernel<<<(n_runs + FT - 1) / FT, FT, 0, st>>>((const uint32_t*)p_runoff, (const uint32_t*)p_runlen,
+    reduce_kernel<<<(n_runs + RT - 1) / RT, RT, 0, st>>>((const uint32_t*)p_runoff, (const uint32_t*)p_runlen,
                                                          (const uint32_t*)p_nruns, (const uint32_t*)p_vals2,
                                                          (const uint32_t*)p_cand, pts, rgb, (double*)p_oxyz,
                                                          (uint8_t*)p_orgb, (uint8_t*)p_ply);

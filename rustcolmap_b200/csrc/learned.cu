@@ -5,9 +5,11 @@
 //   costvol_kernel      32-plane fronto-parallel census cost volume at quarter
 //                       resolution: integer Hamming sums over a 3x3 window and
 //                       K support views, normalised to [0, 1]
-//   conv3x3_kernel      3x3 convolution as an implicit GEMM on the tensor
-//                       cores (mma.sync m16n8k16, BF16 in, FP32 accumulate)
-//   conv3x3_wgrad_kernel  weight gradient of the same convolution
+//   conv3x3_kernel      3x3 convolution as an implicit GEMM on the 5th-
+//                       generation tensor cores (tcgen05.mma, BF16 operands
+//                       in shared memory, FP32 accumulator in tensor memory)
+//   conv3x3_wgrad_kernel  weight gradient of the same convolution (mma.sync
+//                       m16n8k16, BF16 in, FP32 accumulate)
 //   loss/Adam kernels   training
 // The patch-match init that consumes the predictions (confident pixels take
 // the predicted plane, the others fall back to the plane sweep) is
@@ -16,6 +18,8 @@
 // Tensors are NHWC, BF16, channels padded to a multiple of 16.
 #include <cuda_bf16.h>
 
+#include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -179,104 +183,230 @@ __device__ __forceinline__ uint32_t pack2(bf16 lo, bf16 hi) {
 
 constexpr int TILE_H = 8, TILE_W = 16;  // output pixels per block: 8 rows x 16 columns (4 warps x 2 rows)
 
+// ---- 5th-generation tensor cores (tcgen05): the forward/data convolution
+// Shared-memory matrix descriptor of a tcgen05.mma operand, no swizzle,
+// K-major: 8-row x 16-byte core matrices, `lbo` bytes between core matrices
+// adjacent in K, `sbo` bytes between core matrices adjacent in M/N (PTX ISA,
+// tcgen05 "Shared memory descriptor"; version 1 at bits 46-47).
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor of tcgen05.mma.kind::f16: FP32 accumulator (bits
+// 4-5 = 1), BF16 A and B (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bits
+// 17-22, M >> 4 at bits 24-28.
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int m, int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+        :
+        : "r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Waits for phase `parity` of the mbarrier at shared address `bar`; gives
+// up after `limit_ns` of wall time (returns false).
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint64_t limit_ns) {
+    const uint64_t t0 = global_ns();
+    while (true) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P1;\n\t}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (global_ns() - t0 > limit_ns) return false;
+    }
+}
+
+template <int N>
+__device__ __forceinline__ void tmem_ld_32x32b(uint32_t taddr, uint32_t* v);
+template <>
+__device__ __forceinline__ void tmem_ld_32x32b<16>(uint32_t taddr, uint32_t* v) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr));
+}
+template <>
+__device__ __forceinline__ void tmem_ld_32x32b<32>(uint32_t taddr, uint32_t* v) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr));
+}
+
+// Set (never cleared by a kernel) when a tensor-core wait gave up; read and
+// cleared by tc_fault_take().
+__device__ int g_tc_fault = 0;
+
+constexpr int TC_TW = 8, TC_TH = 16;          // output tile: 16 rows x 8 columns = the 128 rows of M
+constexpr int TC_SW = TC_TW + 2;              // staged halo tile width
+constexpr int TC_NPIX = (TC_TH + 2) * TC_SW;  // staged pixels
+constexpr int TC_CTAS_PER_SM = 4;
+constexpr uint64_t TC_WAIT_NS = 2000000000ull;  // 2 s: far above a tile's few microseconds
+
 // y = conv3x3(x, w) + b, "same" zero padding; optional ReLU; optional f32
 // output.  w: [9][COUT][CIN] BF16.  mask (optional): x is multiplied by
 // (mask > 0) on load (ReLU derivative of the layer that produced x).
+//
+// Implicit GEMM on the tensor cores: D[128 pixels][COUT] = sum over the 9
+// taps and CIN/16 channel chunks of A[128 pixels][16 channels] x
+// B[16 channels][COUT], one tcgen05.mma (M = 128, N = COUT, K = 16, BF16
+// operands in shared memory, FP32 accumulator in tensor memory) per tap and
+// chunk, issued by one thread.  The output tile is 16 rows x 8 columns, so
+// every 8 consecutive rows of A are 8 consecutive pixels of one staged row:
+// staging the halo tile as [channel group of 8][pixel][8 channels] makes
+// every tap's A a canonical K-major operand in place (core matrix = 8
+// pixels x 16 bytes; the next 8 rows of A are the next staged row, 10 pixels
+// on; the next 8 channels are the next channel group), so no im2col copy is
+// made.  The weights are staged once per CTA as [tap][channel group][COUT][8
+// channels].  Persistent CTAs loop over the tiles; the accumulator (COUT
+// f32 columns of 128 lanes) is read back by the four warps with
+// tcgen05.ld (warp w owns lanes 32w..32w+31).  Every wait is bounded: on a
+// time-out the CTA flags g_tc_fault, waits once more, frees its tensor
+// memory and returns.
 template <int CIN, int COUT, bool RELU, bool OUT_F32, bool MASK>
-__global__ void __launch_bounds__(128) conv3x3_kernel(const bf16* __restrict__ x, const bf16* __restrict__ mask, int H,
-                                                      int W, const bf16* __restrict__ wgt,
+__global__ void __launch_bounds__(128) conv3x3_kernel(const bf16* __restrict__ x, const bf16* __restrict__ mask, int N,
+                                                      int H, int W, const bf16* __restrict__ wgt,
                                                       const float* __restrict__ bias, void* __restrict__ y) {
-    constexpr int SPX = CIN + 8;   // shared pixel stride (bank spread)
-    constexpr int SWR = CIN + 8;   // shared weight row stride
-    extern __shared__ __align__(16) unsigned char smem[];
-    bf16* sx = reinterpret_cast<bf16*>(smem);
-    bf16* sw = sx + (TILE_H + 2) * (TILE_W + 2) * SPX;
-    const int n = blockIdx.z, x0 = blockIdx.x * TILE_W, y0 = blockIdx.y * TILE_H;
-    const size_t img = (size_t)n * H * W;
-    for (int i = threadIdx.x; i < (TILE_H + 2) * (TILE_W + 2) * (CIN / 8); i += 128) {
-        const int c8 = i % (CIN / 8), p = i / (CIN / 8);
-        const int gy = y0 - 1 + p / (TILE_W + 2), gx = x0 - 1 + p % (TILE_W + 2);
-        uint4 v = make_uint4(0, 0, 0, 0);
-        if (gy >= 0 && gy < H && gx >= 0 && gx < W) {
-            const size_t gi = (img + (size_t)gy * W + gx) * CIN + c8 * 8;
-            v = *reinterpret_cast<const uint4*>(x + gi);
-            if (MASK) {
-                const uint4 m = *reinterpret_cast<const uint4*>(mask + gi);
-                const bf16* mv = reinterpret_cast<const bf16*>(&m);
-                bf16* xv = reinterpret_cast<bf16*>(&v);
+    static_assert(CIN % 16 == 0 && (COUT == 16 || COUT == 32), "conv3x3 shape");
+    constexpr int KG = CIN / 8;  // 16-byte channel groups
+    constexpr uint32_t IDESC = umma_idesc_bf16(128, COUT);
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint4* sw = reinterpret_cast<uint4*>(smem);  // [9][KG][COUT]
+    uint4* sx = sw + 9 * KG * COUT;             // [KG][TC_NPIX]
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t s_taddr;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t bar_a = smem_u32(&bar);
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_taddr)),
+                     "r"(32));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar_a), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int i = tid; i < 9 * KG * COUT; i += 128) {
+        const int co = i % COUT, g = (i / COUT) % KG, tap = i / (COUT * KG);
+        sw[i] = *reinterpret_cast<const uint4*>(wgt + (size_t)(tap * COUT + co) * CIN + g * 8);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t taddr = s_taddr;
+    const uint32_t sw_a = smem_u32(sw), sx_a = smem_u32(sx);
+    const int tiles_x = (W + TC_TW - 1) / TC_TW, tiles_y = (H + TC_TH - 1) / TC_TH;
+    const int tiles = tiles_x * tiles_y * N;
+    uint32_t parity = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
+        const int n = t / (tiles_x * tiles_y), r = t % (tiles_x * tiles_y);
+        const int y0 = (r / tiles_x) * TC_TH, x0 = (r % tiles_x) * TC_TW;
+        const size_t img = (size_t)n * H * W;
+        // the halo tile, zero padded, 16 bytes per (pixel, channel group)
+        for (int i = tid; i < TC_NPIX * KG; i += 128) {
+            const int g = i % KG, p = i / KG;
+            const int gy = y0 - 1 + p / TC_SW, gx = x0 - 1 + p % TC_SW;
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if (gy >= 0 && gy < H && gx >= 0 && gx < W) {
+                const size_t gi = (img + (size_t)gy * W + gx) * CIN + g * 8;
+                v = *reinterpret_cast<const uint4*>(x + gi);
+                if (MASK) {
+                    const uint4 m = *reinterpret_cast<const uint4*>(mask + gi);
+                    const bf16* mv = reinterpret_cast<const bf16*>(&m);
+                    bf16* xv = reinterpret_cast<bf16*>(&v);
 #pragma unroll
-                for (int q = 0; q < 8; ++q)
-                    if (!(__bfloat162float(mv[q]) > 0.0f)) xv[q] = __float2bfloat16(0.0f);
+                    for (int q = 0; q < 8; ++q)
+                        if (!(__bfloat162float(mv[q]) > 0.0f)) xv[q] = __float2bfloat16(0.0f);
+                }
+            }
+            sx[g * TC_NPIX + p] = v;
+        }
+        // generic-proxy smem writes -> visible to the tensor core (async proxy)
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (tid == 0) {
+#pragma unroll
+            for (int tap = 0; tap < 9; ++tap) {
+                const int ky = tap / 3, kx = tap % 3;
+#pragma unroll
+                for (int kc = 0; kc < CIN / 16; ++kc) {
+                    const uint64_t a = umma_desc(sx_a + (uint32_t)(((2 * kc) * TC_NPIX + ky * TC_SW + kx) * 16),
+                                                 TC_NPIX * 16, TC_SW * 16);
+                    const uint64_t b = umma_desc(sw_a + (uint32_t)((tap * KG + 2 * kc) * COUT * 16), COUT * 16, 128);
+                    umma_bf16(taddr, a, b, IDESC, (tap | kc) != 0 ? 1u : 0u);
+                }
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar_a)
+                         : "memory");
+        }
+        __syncwarp();
+        const bool got = mbar_wait(bar_a, parity, TC_WAIT_NS);
+        parity ^= 1u;
+        if (!__syncthreads_and(got)) {
+            ok = false;
+            break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        uint32_t v[COUT];
+        tmem_ld_32x32b<COUT>(taddr + ((uint32_t)(32 * warp) << 16), v);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        const int m = 32 * warp + lane, oy = y0 + m / TC_TW, ox = x0 + m % TC_TW;
+        if (oy < H && ox < W) {
+            const size_t o = (img + (size_t)oy * W + ox) * COUT;
+            float f[COUT];
+#pragma unroll
+            for (int c = 0; c < COUT; ++c) {
+                float s = __uint_as_float(v[c]) + (bias ? bias[c] : 0.f);
+                f[c] = RELU ? fmaxf(s, 0.f) : s;
+            }
+            if (OUT_F32) {
+                float4* yo = reinterpret_cast<float4*>(reinterpret_cast<float*>(y) + o);
+#pragma unroll
+                for (int c = 0; c < COUT / 4; ++c) yo[c] = make_float4(f[4 * c], f[4 * c + 1], f[4 * c + 2], f[4 * c + 3]);
+            } else {
+                uint4* yo = reinterpret_cast<uint4*>(reinterpret_cast<bf16*>(y) + o);
+#pragma unroll
+                for (int c = 0; c < COUT / 8; ++c)
+                    yo[c] = make_uint4(pack2(__float2bfloat16(f[8 * c]), __float2bfloat16(f[8 * c + 1])),
+                                       pack2(__float2bfloat16(f[8 * c + 2]), __float2bfloat16(f[8 * c + 3])),
+                                       pack2(__float2bfloat16(f[8 * c + 4]), __float2bfloat16(f[8 * c + 5])),
+                                       pack2(__float2bfloat16(f[8 * c + 6]), __float2bfloat16(f[8 * c + 7])));
             }
         }
-        *reinterpret_cast<uint4*>(sx + p * SPX + c8 * 8) = v;
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     }
-    for (int i = threadIdx.x; i < 9 * COUT * (CIN / 8); i += 128) {
-        const int c8 = i % (CIN / 8), r = i / (CIN / 8);
-        *reinterpret_cast<uint4*>(sw + r * SWR + c8 * 8) = *reinterpret_cast<const uint4*>(wgt + (size_t)r * CIN + c8 * 8);
+    if (!ok) {
+        // the MMAs may still be in flight: wait once more before freeing
+        if (tid == 0) atomicExch(&g_tc_fault, 1);
+        mbar_wait(bar_a, parity ^ 1u, TC_WAIT_NS);
     }
     __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-    float acc[2][COUT / 8][4];
-#pragma unroll
-    for (int m = 0; m < 2; ++m)
-#pragma unroll
-        for (int nt = 0; nt < COUT / 8; ++nt) acc[m][nt][0] = acc[m][nt][1] = acc[m][nt][2] = acc[m][nt][3] = 0.f;
-#pragma unroll 1
-    for (int tap = 0; tap < 9; ++tap) {
-        const int ky = tap / 3, kx = tap % 3;
-#pragma unroll
-        for (int kc = 0; kc < CIN / 16; ++kc) {
-            uint32_t a[2][4];
-#pragma unroll
-            for (int m = 0; m < 2; ++m) {
-                const int row = warp * 2 + m + ky;
-                const bf16* p0 = sx + (row * (TILE_W + 2) + g + kx) * SPX + kc * 16 + 2 * t;
-                const bf16* p1 = p0 + 8 * SPX;
-                a[m][0] = *reinterpret_cast<const uint32_t*>(p0);
-                a[m][1] = *reinterpret_cast<const uint32_t*>(p1);
-                a[m][2] = *reinterpret_cast<const uint32_t*>(p0 + 8);
-                a[m][3] = *reinterpret_cast<const uint32_t*>(p1 + 8);
-            }
-#pragma unroll
-            for (int nt = 0; nt < COUT / 8; ++nt) {
-                const bf16* q = sw + (tap * COUT + nt * 8 + g) * SWR + kc * 16 + 2 * t;
-                const uint32_t b0 = *reinterpret_cast<const uint32_t*>(q);
-                const uint32_t b1 = *reinterpret_cast<const uint32_t*>(q + 8);
-                mma_bf16(acc[0][nt], a[0], b0, b1);
-                mma_bf16(acc[1][nt], a[1], b0, b1);
-            }
-        }
-    }
-#pragma unroll
-    for (int m = 0; m < 2; ++m) {
-        const int oy = y0 + warp * 2 + m;
-        if (oy >= H) continue;
-#pragma unroll
-        for (int half = 0; half < 2; ++half) {
-            const int ox = x0 + g + 8 * half;
-            if (ox >= W) continue;
-            const size_t o = (img + (size_t)oy * W + ox) * COUT;
-#pragma unroll
-            for (int nt = 0; nt < COUT / 8; ++nt) {
-                const int c = nt * 8 + 2 * t;
-                float v0 = acc[m][nt][2 * half] + (bias ? bias[c] : 0.f);
-                float v1 = acc[m][nt][2 * half + 1] + (bias ? bias[c + 1] : 0.f);
-                if (RELU) {
-                    v0 = fmaxf(v0, 0.f);
-                    v1 = fmaxf(v1, 0.f);
-                }
-                if (OUT_F32) {
-                    float* yo = reinterpret_cast<float*>(y) + o + c;
-                    yo[0] = v0;
-                    yo[1] = v1;
-                } else {
-                    *reinterpret_cast<uint32_t*>(reinterpret_cast<bf16*>(y) + o + c) =
-                        pack2(__float2bfloat16(v0), __float2bfloat16(v1));
-                }
-            }
-        }
-    }
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(32));
 }
 
 // dW[tap][co][ci] += sum_p dy[p][co] * x[p + tap][ci] over the block's pixel
@@ -505,14 +635,31 @@ cudaError_t launch_costvol(const DevJob* jobs, const int32_t* blk_start, int n_j
 template <int CIN, int COUT, bool RELU, bool OUT_F32, bool MASK>
 static cudaError_t conv_t(const void* x, const void* mask, int N, int H, int W, const void* w, const float* b, void* y,
                           cudaStream_t st) {
-    const size_t sm = sizeof(bf16) * ((TILE_H + 2) * (TILE_W + 2) * (CIN + 8) + 9 * COUT * (CIN + 8));
+    if (N <= 0 || H <= 0 || W <= 0) return cudaSuccess;
+    // 16-byte operand loads and stores
+    if (((uintptr_t)x | (uintptr_t)w | (uintptr_t)y | (mask ? (uintptr_t)mask : 0)) & 15) return cudaErrorMisalignedAddress;
+    const size_t sm = 16 * ((size_t)9 * (CIN / 8) * COUT + (size_t)(CIN / 8) * TC_NPIX);
     auto k = conv3x3_kernel<CIN, COUT, RELU, OUT_F32, MASK>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e) return e;
-    dim3 grid((W + TILE_W - 1) / TILE_W, (H + TILE_H - 1) / TILE_H, N);
-    k<<<grid, 128, sm, st>>>(reinterpret_cast<const bf16*>(x), reinterpret_cast<const bf16*>(mask), H, W,
+    int dev = 0, sms = 0;
+    if ((e = cudaGetDevice(&dev)) || (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev))) return e;
+    const long long tiles = (long long)((W + TC_TW - 1) / TC_TW) * ((H + TC_TH - 1) / TC_TH) * N;
+    if (tiles > INT_MAX) return cudaErrorInvalidValue;
+    const int grid = (int)std::min<long long>(tiles, (long long)sms * TC_CTAS_PER_SM);
+    k<<<grid, 128, sm, st>>>(reinterpret_cast<const bf16*>(x), reinterpret_cast<const bf16*>(mask), N, H, W,
                              reinterpret_cast<const bf16*>(w), b, y);
     return cudaGetLastError();
+}
+
+int tc_fault_take() {
+    int v = 0;
+    if (cudaMemcpyFromSymbol(&v, g_tc_fault, sizeof(int)) != cudaSuccess) return -1;
+    if (v) {
+        const int z = 0;
+        if (cudaMemcpyToSymbol(g_tc_fault, &z, sizeof(int)) != cudaSuccess) return -1;
+    }
+    return v;
 }
 
 cudaError_t launch_conv3x3(int cin, int cout, bool relu, bool out_f32, const void* x, const void* mask, int N, int H,

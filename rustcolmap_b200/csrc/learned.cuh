@@ -27,6 +27,9 @@ cudaError_t launch_costvol(const DevJob* jobs, const int32_t* blk_start, int n_j
                            const uint8_t* gray_q, void* out, cudaStream_t st);
 cudaError_t launch_conv3x3(int cin, int cout, bool relu, bool out_f32, const void* x, const void* mask, int N, int H,
                            int W, const void* w, const float* b, void* y, cudaStream_t st);
+// Reads and clears the device word the tensor-core kernels set when one of
+// their bounded waits gave up (1), 0 if none did, -1 if it could not be read.
+int tc_fault_take();
 cudaError_t launch_conv3x3_wgrad(int cin, int cout, const void* x, const void* dy, const void* mask, int N, int H,
                                  int W, float* dW, cudaStream_t st);
 cudaError_t launch_bias_grad(int c, const void* dy, const void* mask, int64_t npx, float* db, cudaStream_t st);
