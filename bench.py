@@ -295,7 +295,8 @@ def gt_summary(ds, sc, jobs, scene, stricter_gate=None):
     are valid and within 1% inverse depth ('within_1pct', coverage), and the
     same over valid pixels ('accuracy', precision).  With stricter_gate the
     same two figures are added for the maps gated at that cost (a stricter
-    gate only removes pixels, so the run's own maps give them)."""
+    gate only removes pixels, so the run's own maps give them).  'fused':
+    the fused cloud's distances to the scene's analytic surfaces."""
     within = gt_px = valid = 0
     w2 = v2 = 0
     for (ref, _, _, _) in jobs:
@@ -312,6 +313,12 @@ def gt_summary(ds, sc, jobs, scene, stricter_gate=None):
            "tol": "1% relative inverse depth", "views": len(jobs)}
     if stricter_gate is not None:
         out[f"at_gate_{stricter_gate:g}"] = {"within_1pct": w2 / max(gt_px, 1), "accuracy": w2 / max(v2, 1)}
+    if getattr(sc, "prims", None) and ds.n_points:
+        # fused cloud against the analytic surfaces (scene units; the room is 12 x 12 x 4)
+        d = scene.surface_distance(ds.points()[0], sc.prims)
+        out["fused"] = {"points": int(len(d)), "median_dist": float(np.median(d)),
+                        "mean_dist": float(d.mean()), "within_0.01": float((d <= 0.01).mean()),
+                        "within_0.02": float((d <= 0.02).mean()), "unit": "scene units"}
     return out
 
 

@@ -216,8 +216,17 @@ void rcmvs_ctx_destroy(rcmvs_ctx* ctx);
 const char* rcmvs_last_error(const rcmvs_ctx* ctx);
 /* The context's cudaStream_t, as an opaque pointer (for event timing). */
 void* rcmvs_ctx_stream(rcmvs_ctx* ctx);
-/* Blocks until the context's stream has drained. */
+/* Blocks until the context's stream has drained.  Also returns
+ * RCMVS_E_CUDA (message in rcmvs_last_error) if a tensor-core kernel
+ * queued since the last call gave up one of its bounded waits for its MMAs
+ * (the kernel then freed its tensor memory and returned early). */
 int rcmvs_ctx_synchronize(rcmvs_ctx* ctx);
+/* Diagnostic of that path: one block waits, with a limit of `limit_ns`
+ * (1 us .. 1 s), on an mbarrier nothing arrives on, as the tensor-core
+ * kernels wait for their MMAs, and sets the same fault word when the limit
+ * runs out; the next rcmvs_ctx_synchronize then reports it.  Queued on the
+ * context's stream. */
+int rcmvs_diag_wait_timeout(rcmvs_ctx* ctx, uint64_t limit_ns);
 const char* rcmvs_version(void);
 
 /* ---------------------------------------------------------------- host API */

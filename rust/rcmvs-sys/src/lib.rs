@@ -204,6 +204,7 @@ pub fn rcmvs_options_default(opts: *mut rcmvs_options);
     pub fn rcmvs_last_error(ctx: *const rcmvs_ctx) -> *const c_char;
     pub fn rcmvs_ctx_stream(ctx: *mut rcmvs_ctx) -> *mut c_void;
     pub fn rcmvs_ctx_synchronize(ctx: *mut rcmvs_ctx) -> c_int;
+    pub fn rcmvs_diag_wait_timeout(ctx: *mut rcmvs_ctx, limit_ns: u64) -> c_int;
     pub fn rcmvs_version() -> *const c_char;
     /// census_map (mvs/src/lib.rs:119-142).  Host buffers.
     pub fn rcmvs_census(ctx: *mut rcmvs_ctx, gray: *const u8, w: i32, h: i32, census_out: *mut u64) -> c_int;

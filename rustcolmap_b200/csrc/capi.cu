@@ -181,6 +181,14 @@ const char* rcmvs_last_error(const rcmvs_ctx* ctx) { return ctx ? ctx->err.c_str
 
 void* rcmvs_ctx_stream(rcmvs_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
+int rcmvs_diag_wait_timeout(rcmvs_ctx* ctx, uint64_t limit_ns) {
+    if (!ctx) return RCMVS_E_ARG;
+    if (limit_ns < 1000 || limit_ns > 1000000000ull) return fail(ctx, RCMVS_E_ARG, "limit_ns must be 1 us .. 1 s");
+    CK(cudaSetDevice(ctx->device));
+    CK(rcmvs::launch_wait_probe(limit_ns, ctx->stream));
+    return RCMVS_OK;
+}
+
 int rcmvs_ctx_synchronize(rcmvs_ctx* ctx) {
     if (!ctx) return RCMVS_E_ARG;
     CK(cudaSetDevice(ctx->device));

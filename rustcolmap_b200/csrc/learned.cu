@@ -652,6 +652,25 @@ static cudaError_t conv_t(const void* x, const void* mask, int N, int H, int W, 
     return cudaGetLastError();
 }
 
+namespace {
+__global__ void wait_probe_kernel(uint64_t limit_ns) {
+    __shared__ __align__(8) uint64_t bar;
+    const uint32_t bar_a = smem_u32(&bar);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar_a), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const bool got = mbar_wait(bar_a, 0u, limit_ns);
+    if (!__syncthreads_and(got) && threadIdx.x == 0) atomicExch(&g_tc_fault, 1);
+}
+}  // namespace
+
+cudaError_t launch_wait_probe(uint64_t limit_ns, cudaStream_t st) {
+    wait_probe_kernel<<<1, 32, 0, st>>>(limit_ns);
+    return cudaGetLastError();
+}
+
 int tc_fault_take() {
     int v = 0;
     if (cudaMemcpyFromSymbol(&v, g_tc_fault, sizeof(int)) != cudaSuccess) return -1;

@@ -30,6 +30,9 @@ cudaError_t launch_conv3x3(int cin, int cout, bool relu, bool out_f32, const voi
 // Reads and clears the device word the tensor-core kernels set when one of
 // their bounded waits gave up (1), 0 if none did, -1 if it could not be read.
 int tc_fault_take();
+// One block waits limit_ns on an mbarrier that nothing arrives on and sets
+// the fault word when the wait gives up (rcmvs_diag_wait_timeout).
+cudaError_t launch_wait_probe(uint64_t limit_ns, cudaStream_t st);
 cudaError_t launch_conv3x3_wgrad(int cin, int cout, const void* x, const void* dy, const void* mask, int N, int H,
                                  int W, float* dW, cudaStream_t st);
 cudaError_t launch_bias_grad(int c, const void* dy, const void* mask, int64_t npx, float* db, cudaStream_t st);

@@ -50,6 +50,11 @@ class Context:
     def synchronize(self):
         self.check(self._L.rcmvs_ctx_synchronize(self.ptr))
 
+    def diag_wait_timeout(self, limit_ns):
+        """Queues the bounded-wait diagnostic (rcmvs_diag_wait_timeout): the
+        next synchronize() raises, reporting the timed-out wait."""
+        self.check(self._L.rcmvs_diag_wait_timeout(self.ptr, int(limit_ns)))
+
     def last_work(self):
         e, r = C.c_uint64(), C.c_uint64()
         self.check(self._L.rcmvs_last_work(self.ptr, C.byref(e), C.byref(r)))

@@ -47,6 +47,7 @@ class SyntheticScene:
     sparse: SparseModel
     name: str
     seed: int
+    prims: Optional[list] = None  # the analytic surfaces the views were rendered from
 
 
 def look_at(eye, target, up=(0.0, 0.0, 1.0)):
@@ -229,7 +230,7 @@ def corner_room(seed=0, n_views=8, w=384, h=288, f=440.0, arc_deg=60.0, n_patche
     grays, depths, nrms = render(prims, patches, cams, device=device, normals=normals)
     views = _views(cams, grays, "corner")
     sparse = sample_sparse(views, depths, rng, per_view=per_view_sparse)
-    return SyntheticScene(views, depths, nrms, sparse, "corner_room", seed)
+    return SyntheticScene(views, depths, nrms, sparse, "corner_room", seed, prims)
 
 
 def orbit_room(seed=0, n_views=64, sizes=((960, 720),), f_rel=1.1, n_boxes=20, n_spheres=0, n_patches=200,
@@ -276,7 +277,36 @@ def orbit_room(seed=0, n_views=64, sizes=((960, 720),), f_rel=1.1, n_boxes=20, n
     grays, depths, nrms = render(prims, patches, cams, device=device, normals=normals)
     views = _views(cams, grays, "orbit")
     sparse = sample_sparse(views, depths, rng, per_view=per_view_sparse)
-    return SyntheticScene(views, depths, nrms, sparse, "orbit_room", seed)
+    return SyntheticScene(views, depths, nrms, sparse, "orbit_room", seed, prims)
+
+
+def surface_distance(xyz, prims, chunk=65536):
+    """Distance of each point (n, 3) to the nearest surface of the scene's
+    primitives (rectangles, axis-aligned boxes, spheres), in scene units:
+    the ground-truth error of a fused point cloud."""
+    xyz = np.asarray(xyz, np.float64).reshape(-1, 3)
+    out = np.full(len(xyz), np.inf)
+    for a in range(0, len(xyz), chunk):
+        p = xyz[a:a + chunk]
+        best = np.full(len(p), np.inf)
+        for q in prims:
+            v = np.array(q.p[:11], np.float64)
+            if q.kind == RECT:
+                o, u, w, U, V = v[0:3], v[3:6], v[6:9], v[9], v[10]
+                d = p - o
+                s = np.clip(d @ u, 0.0, U)
+                t = np.clip(d @ w, 0.0, V)
+                dist = np.linalg.norm(d - s[:, None] * u - t[:, None] * w, axis=1)
+            elif q.kind == BOX:
+                lo, hi = v[0:3], v[3:6]
+                outside = np.linalg.norm(p - np.clip(p, lo, hi), axis=1)
+                inside = np.minimum(p - lo, hi - p).min(axis=1)
+                dist = np.where(outside > 0, outside, np.abs(inside))
+            else:
+                dist = np.abs(np.linalg.norm(p - v[0:3], axis=1) - v[3])
+            best = np.minimum(best, dist)
+        out[a:a + chunk] = best
+    return out
 
 
 def gt_metrics(depth, gt, tol=0.01):

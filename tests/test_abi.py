@@ -148,3 +148,21 @@ def test_dense_outputs_match_oracle(tmp_path, n, cap):
 def test_dense_outputs_of_an_empty_cloud(tmp_path):
     mvs.write_dense_outputs(str(tmp_path), np.zeros((0, 3)), np.zeros((0, 3), np.uint8))
     assert (tmp_path / "dense.ply").exists() and not (tmp_path / "dense_web.json").exists()
+
+
+def test_surface_distance_of_the_synthetic_scenes():
+    """The fused-cloud ground truth: points sampled from the rendered depth
+    maps lie on the analytic surfaces, and points moved off a wall, a box
+    face and a sphere by a known amount are that far away."""
+    from rustcolmap_b200 import scene
+    sc = scene.orbit_room(seed=4, n_views=3, sizes=((64, 48),), n_boxes=4, n_spheres=2, per_view_sparse=60)
+    d = scene.surface_distance(sc.sparse.xyz, sc.prims)
+    assert d.max() < 1e-4, d.max()
+    walls = scene.surface_distance(np.array([[0.0, 0.0, 2.0], [5.5, 0.3, 1.0], [0.1, -0.2, -0.25]]), sc.prims[:5])
+    np.testing.assert_allclose(walls, [2.0, 0.5, 0.25], atol=1e-12)
+    box = scene.SyntheticScene([], [], None, None, "t", 0, [scene._box((0, 0, 0), (1, 2, 3), np.random.default_rng(0))])
+    sph = scene._sphere((5.0, 0.0, 0.0), 0.5, np.random.default_rng(0))
+    got = scene.surface_distance(np.array([[0.5, 1.0, 1.0], [2.0, 1.0, 1.5], [0.5, 1.0, 3.25]]), box.prims)
+    np.testing.assert_allclose(got, [0.5, 1.0, 0.25], atol=1e-12)
+    np.testing.assert_allclose(scene.surface_distance(np.array([[5.0, 0.0, 1.0], [5.0, 0.1, 0.0]]), [sph]),
+                               [0.5, 0.4], atol=1e-12)

@@ -103,6 +103,35 @@ def test_net_forward_and_gradients_match_cpu_oracle(ctx):
     net.close()
 
 
+@pytest.mark.gpu
+def test_tensor_core_wait_limit_reports_a_fault(ctx):
+    """The tensor-core kernels wait for their MMAs on an mbarrier with a time
+    limit.  A wait that runs out (here: the diagnostic waits 2 ms on a
+    barrier nothing arrives on) sets the fault word, the next synchronize
+    reports it once, and the context stays usable: the network still runs
+    and matches the oracle afterwards."""
+    import torch
+    from rustcolmap_b200._lib import RcmvsError
+    ctx.synchronize()
+    ctx.diag_wait_timeout(2_000_000)
+    with pytest.raises(RcmvsError, match="timed out"):
+        ctx.synchronize()
+    ctx.synchronize()  # the word was cleared
+    with pytest.raises(RcmvsError):
+        ctx.diag_wait_timeout(10)  # below the 1 us floor
+    rng = np.random.default_rng(2)
+    net = learned.ProposalNet(ctx, seed=5)
+    x, _ = _random_batch(rng, n=1, h=17, w=9)
+    n, h, w = x.shape[:3]
+    xd = torch.from_numpy(x).to(torch.bfloat16).cuda()
+    out = torch.empty((n, h, w, 16), dtype=torch.float32, device="cuda")
+    net.forward(xd.data_ptr(), n, h, w, out.data_ptr())
+    ctx.synchronize()
+    ref = net_oracle.forward(net.params(), x)[0][-1]
+    assert np.abs(out.cpu().numpy() - ref).max() <= 2e-2 * np.abs(ref).max()
+    net.close()
+
+
 def _costvol_numpy(sc, ref, srcs, zmin, zmax):
     """numpy restatement of the cost volume (quarter resolution)."""
     def quarter(v):
