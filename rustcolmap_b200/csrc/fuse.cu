@@ -44,6 +44,9 @@ __device__ __forceinline__ int find_item(const int32_t* start, int n, int b) {
 __device__ __forceinline__ void cam_normalize(const FuseView& v, double u, double w, double& xn, double& yn) {
     xn = (u - v.cx) / v.f;
     yn = (w - v.cy) / v.f;
+    // with k = 0 and a finite radius, d = 1 + 0 * r2 is exactly 1, f * d = f,
+    // and both iterations give back xn, yn: skipped
+    if (v.k == 0.0 && isfinite(xn * xn + yn * yn)) return;
     for (int it = 0; it < 2; ++it) {
         double r2 = xn * xn + yn * yn;
         double d = 1.0 + v.k * r2;

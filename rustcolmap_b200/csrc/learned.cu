@@ -16,6 +16,8 @@
 // init_learned_rows_kernel in stereo.cu.
 //
 // Tensors are NHWC, BF16, channels padded to a multiple of 16.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -262,8 +264,42 @@ __device__ int g_tc_fault = 0;
 constexpr int TC_TW = 8, TC_TH = 16;          // output tile: 16 rows x 8 columns = the 128 rows of M
 constexpr int TC_SW = TC_TW + 2;              // staged halo tile width
 constexpr int TC_NPIX = (TC_TH + 2) * TC_SW;  // staged pixels
-constexpr int TC_CTAS_PER_SM = 4;
+constexpr int TC_GS = 2944;                   // bytes per channel group of a staged tile: 180 x 16, 128-aligned
+constexpr int TC_CTAS_PER_SM = 3;
 constexpr uint64_t TC_WAIT_NS = 2000000000ull;  // 2 s: far above a tile's few microseconds
+
+template <int CIN, int COUT, bool MASK>
+struct ConvSmem {
+    static constexpr int KG = CIN / 8;                      // 16-byte channel groups
+    static constexpr int STAGES = MASK ? 1 : 2;             // TMA double buffer; thread staging single
+    static constexpr int W_BYTES = 9 * KG * COUT * 16;      // weights [tap][group][COUT][8]
+    static constexpr int X_BYTES = KG * TC_GS;              // one staged tile [group][pixel][8]
+    static constexpr int BYTES = 128 + W_BYTES + STAGES * X_BYTES;  // + alignment slack
+    static_assert(W_BYTES % 128 == 0, "128-byte aligned stages");
+};
+
+// One channel group of the staged tile by TMA: the box (8 channels, 10
+// columns, 18 rows, 1 image) at (c0 = 8 * group, x0 - 1, y0 - 1, n) lands
+// as [row][column][8 channels] = [pixel][8 channels], zero filled outside
+// the image.  The innermost coordinate is a multiple of 8 elements (16
+// bytes); the destination is 128-byte aligned.
+__device__ __forceinline__ void tma_load_4d(const void* tmap, uint32_t dst, uint32_t bar, int c0, int c1, int c2,
+                                            int c3) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];"
+        :
+        : "r"(dst), "l"(reinterpret_cast<uint64_t>(tmap)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
 
 // y = conv3x3(x, w) + b, "same" zero padding; optional ReLU; optional f32
 // output.  w: [9][COUT][CIN] BF16.  mask (optional): x is multiplied by
@@ -280,97 +316,145 @@ constexpr uint64_t TC_WAIT_NS = 2000000000ull;  // 2 s: far above a tile's few m
 // pixels x 16 bytes; the next 8 rows of A are the next staged row, 10 pixels
 // on; the next 8 channels are the next channel group), so no im2col copy is
 // made.  The weights are staged once per CTA as [tap][channel group][COUT][8
-// channels].  Persistent CTAs loop over the tiles; the accumulator (COUT
-// f32 columns of 128 lanes) is read back by the four warps with
-// tcgen05.ld (warp w owns lanes 32w..32w+31).  Every wait is bounded: on a
-// time-out the CTA flags g_tc_fault, waits once more, frees its tensor
-// memory and returns.
+// channels].  Persistent CTAs loop over the tiles.  Without a mask the tile
+// arrives by TMA (one box per channel group, zero fill at the borders) into
+// a double buffer: thread 0 starts the next tile's loads before the current
+// tile's MMAs, so they overlap the MMAs and the epilogue.  With a mask (the
+// backward pass) the threads stage the tile, masked, into one buffer.  The
+// accumulator (COUT f32 columns of 128 lanes) is read back by the four warps
+// with tcgen05.ld (warp w owns lanes 32w..32w+31).  Every wait is bounded:
+// on a time-out the CTA flags g_tc_fault, waits once more for what it has in
+// flight, frees its tensor memory and returns.
 template <int CIN, int COUT, bool RELU, bool OUT_F32, bool MASK>
-__global__ void __launch_bounds__(128) conv3x3_kernel(const bf16* __restrict__ x, const bf16* __restrict__ mask, int N,
+__global__ void __launch_bounds__(128) conv3x3_kernel(const __grid_constant__ CUtensorMap tmap,
+                                                      const bf16* __restrict__ x, const bf16* __restrict__ mask, int N,
                                                       int H, int W, const bf16* __restrict__ wgt,
                                                       const float* __restrict__ bias, void* __restrict__ y) {
     static_assert(CIN % 16 == 0 && (COUT == 16 || COUT == 32), "conv3x3 shape");
-    constexpr int KG = CIN / 8;  // 16-byte channel groups
+    using L = ConvSmem<CIN, COUT, MASK>;
+    constexpr int KG = L::KG;
+    constexpr bool TMA = !MASK;
     constexpr uint32_t IDESC = umma_idesc_bf16(128, COUT);
-    extern __shared__ __align__(128) unsigned char smem[];
-    uint4* sw = reinterpret_cast<uint4*>(smem);  // [9][KG][COUT]
-    uint4* sx = sw + 9 * KG * COUT;             // [KG][TC_NPIX]
-    __shared__ __align__(8) uint64_t bar;
+    constexpr uint32_t TILE_TX = (uint32_t)KG * TC_NPIX * 16;  // bytes one tile's boxes deliver
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ __align__(8) uint64_t bars[3];  // [0], [1]: tile loaded (per stage); [2]: MMAs done
     __shared__ uint32_t s_taddr;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const uint32_t bar_a = smem_u32(&bar);
+    // 128-byte aligned base (TMA destinations)
+    const uint32_t raw_a = smem_u32(smem);
+    const uint32_t base_a = (raw_a + 127u) & ~127u;
+    unsigned char* base = smem + (base_a - raw_a);
+    uint4* sw = reinterpret_cast<uint4*>(base);
+    const uint32_t sw_a = base_a, sx_a0 = base_a + L::W_BYTES;
+    const uint32_t full0 = smem_u32(&bars[0]), full1 = smem_u32(&bars[1]);
+    const uint32_t mma_a = smem_u32(&bars[2]);
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_taddr)),
                      "r"(32));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar_a), "r"(1));
+        mbar_init(full0, 1);
+        mbar_init(full1, 1);
+        mbar_init(mma_a, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     for (int i = tid; i < 9 * KG * COUT; i += 128) {
         const int co = i % COUT, g = (i / COUT) % KG, tap = i / (COUT * KG);
         sw[i] = *reinterpret_cast<const uint4*>(wgt + (size_t)(tap * COUT + co) * CIN + g * 8);
     }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t taddr = s_taddr;
-    const uint32_t sw_a = smem_u32(sw), sx_a = smem_u32(sx);
     const int tiles_x = (W + TC_TW - 1) / TC_TW, tiles_y = (H + TC_TH - 1) / TC_TH;
-    const int tiles = tiles_x * tiles_y * N;
-    uint32_t parity = 0;
+    const int per_img = tiles_x * tiles_y, tiles = per_img * N;
+    auto load_tile = [&](int t, int s) {  // thread 0: the TMA boxes of tile t into stage s
+        const int n = t / per_img, r = t % per_img;
+        const int y0 = (r / tiles_x) * TC_TH, x0 = (r % tiles_x) * TC_TW;
+        const uint32_t bar = s ? full1 : full0;
+        mbar_expect_tx(bar, TILE_TX);
+#pragma unroll
+        for (int g = 0; g < KG; ++g)
+            tma_load_4d(&tmap, sx_a0 + (uint32_t)(s * L::X_BYTES + g * TC_GS), bar, 8 * g, x0 - 1, y0 - 1, n);
+    };
+    // loads issued into and waited for per stage (the same in every thread)
+    uint32_t issued0 = 0, issued1 = 0, landed0 = 0, landed1 = 0;
+    uint32_t mma_issued = 0, mma_done = 0;
     bool ok = true;
-    for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
-        const int n = t / (tiles_x * tiles_y), r = t % (tiles_x * tiles_y);
+    if (TMA && (int)blockIdx.x < tiles) {
+        if (tid == 0) load_tile(blockIdx.x, 0);
+        issued0 = 1;
+    }
+    int it = 0;
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x, ++it) {
+        const int s = TMA ? (it & 1) : 0;
+        const int n = t / per_img, r = t % per_img;
         const int y0 = (r / tiles_x) * TC_TH, x0 = (r % tiles_x) * TC_TW;
         const size_t img = (size_t)n * H * W;
-        // the halo tile, zero padded, 16 bytes per (pixel, channel group)
-        for (int i = tid; i < TC_NPIX * KG; i += 128) {
-            const int g = i % KG, p = i / KG;
-            const int gy = y0 - 1 + p / TC_SW, gx = x0 - 1 + p % TC_SW;
-            uint4 v = make_uint4(0, 0, 0, 0);
-            if (gy >= 0 && gy < H && gx >= 0 && gx < W) {
-                const size_t gi = (img + (size_t)gy * W + gx) * CIN + g * 8;
-                v = *reinterpret_cast<const uint4*>(x + gi);
-                if (MASK) {
-                    const uint4 m = *reinterpret_cast<const uint4*>(mask + gi);
-                    const bf16* mv = reinterpret_cast<const bf16*>(&m);
-                    bf16* xv = reinterpret_cast<bf16*>(&v);
-#pragma unroll
-                    for (int q = 0; q < 8; ++q)
-                        if (!(__bfloat162float(mv[q]) > 0.0f)) xv[q] = __float2bfloat16(0.0f);
-                }
+        if (TMA) {
+            // the other stage was read by the previous tile's MMAs, which completed
+            if (t + (int)gridDim.x < tiles) {
+                if (tid == 0) load_tile(t + gridDim.x, s ^ 1);
+                if (s) ++issued0; else ++issued1;
             }
-            sx[g * TC_NPIX + p] = v;
+            const bool got = mbar_wait(s ? full1 : full0, (s ? landed1 : landed0) & 1u, TC_WAIT_NS);
+            if (!__syncthreads_and(got)) {
+                ok = false;
+                break;
+            }
+            if (s) ++landed1; else ++landed0;
+        } else {
+            uint4* sx = reinterpret_cast<uint4*>(base + L::W_BYTES);
+            for (int i = tid; i < TC_NPIX * KG; i += 128) {
+                const int g = i % KG, p = i / KG;
+                const int gy = y0 - 1 + p / TC_SW, gx = x0 - 1 + p % TC_SW;
+                uint4 v = make_uint4(0, 0, 0, 0);
+                if (gy >= 0 && gy < H && gx >= 0 && gx < W) {
+                    const size_t gi = (img + (size_t)gy * W + gx) * CIN + g * 8;
+                    v = *reinterpret_cast<const uint4*>(x + gi);
+                    if (MASK) {
+                        const uint4 m = *reinterpret_cast<const uint4*>(mask + gi);
+                        const bf16* mv = reinterpret_cast<const bf16*>(&m);
+                        bf16* xv = reinterpret_cast<bf16*>(&v);
+#pragma unroll
+                        for (int q = 0; q < 8; ++q)
+                            if (!(__bfloat162float(mv[q]) > 0.0f)) xv[q] = __float2bfloat16(0.0f);
+                    }
+                }
+                sx[g * (TC_GS / 16) + p] = v;
+            }
+            // generic-proxy smem writes -> visible to the tensor core (async proxy)
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         }
-        // generic-proxy smem writes -> visible to the tensor core (async proxy)
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncthreads();
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         if (tid == 0) {
+            const uint32_t sx_a = sx_a0 + (uint32_t)(s * L::X_BYTES);
 #pragma unroll
             for (int tap = 0; tap < 9; ++tap) {
                 const int ky = tap / 3, kx = tap % 3;
 #pragma unroll
                 for (int kc = 0; kc < CIN / 16; ++kc) {
-                    const uint64_t a = umma_desc(sx_a + (uint32_t)(((2 * kc) * TC_NPIX + ky * TC_SW + kx) * 16),
-                                                 TC_NPIX * 16, TC_SW * 16);
+                    const uint64_t a =
+                        umma_desc(sx_a + (uint32_t)((2 * kc) * TC_GS + (ky * TC_SW + kx) * 16), TC_GS, TC_SW * 16);
                     const uint64_t b = umma_desc(sw_a + (uint32_t)((tap * KG + 2 * kc) * COUT * 16), COUT * 16, 128);
                     umma_bf16(taddr, a, b, IDESC, (tap | kc) != 0 ? 1u : 0u);
                 }
             }
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar_a)
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mma_a)
                          : "memory");
         }
+        ++mma_issued;
         __syncwarp();
-        const bool got = mbar_wait(bar_a, parity, TC_WAIT_NS);
-        parity ^= 1u;
+        const bool got = mbar_wait(mma_a, mma_done & 1u, TC_WAIT_NS);
         if (!__syncthreads_and(got)) {
             ok = false;
             break;
         }
+        ++mma_done;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         uint32_t v[COUT];
         tmem_ld_32x32b<COUT>(taddr + ((uint32_t)(32 * warp) << 16), v);
@@ -381,8 +465,8 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const bf16* __restrict__ x
             float f[COUT];
 #pragma unroll
             for (int c = 0; c < COUT; ++c) {
-                float s = __uint_as_float(v[c]) + (bias ? bias[c] : 0.f);
-                f[c] = RELU ? fmaxf(s, 0.f) : s;
+                float sv = __uint_as_float(v[c]) + (bias ? bias[c] : 0.f);
+                f[c] = RELU ? fmaxf(sv, 0.f) : sv;
             }
             if (OUT_F32) {
                 float4* yo = reinterpret_cast<float4*>(reinterpret_cast<float*>(y) + o);
@@ -401,9 +485,12 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const bf16* __restrict__ x
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     }
     if (!ok) {
-        // the MMAs may still be in flight: wait once more before freeing
+        // wait once more for what is still in flight before the smem and the
+        // tensor memory are released
         if (tid == 0) atomicExch(&g_tc_fault, 1);
-        mbar_wait(bar_a, parity ^ 1u, TC_WAIT_NS);
+        if (mma_issued > mma_done) mbar_wait(mma_a, mma_done & 1u, TC_WAIT_NS);
+        for (uint32_t k = landed0; k < issued0; ++k) mbar_wait(full0, k & 1u, TC_WAIT_NS);
+        for (uint32_t k = landed1; k < issued1; ++k) mbar_wait(full1, k & 1u, TC_WAIT_NS);
     }
     __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(32));
@@ -632,22 +719,53 @@ cudaError_t launch_costvol(const DevJob* jobs, const int32_t* blk_start, int n_j
     return cudaGetLastError();
 }
 
+// cuTensorMapEncodeTiled from the driver, looked up once (no libcuda link).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = []() -> PFN_cuTensorMapEncodeTiled_v12000 {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
+    return fn;
+}
+
+// The NHWC BF16 input as a 4-D tensor (C, W, H, N) for TMA, box (8, 10, 18,
+// 1): one channel group of a staged halo tile.
+cudaError_t input_tensor_map(const void* x, int cin, int N, int H, int W, CUtensorMap* out) {
+    auto enc = tensor_map_encoder();
+    if (!enc) return cudaErrorNotSupported;
+    const cuuint64_t dims[4] = {(cuuint64_t)cin, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)N};
+    const cuuint64_t strides[3] = {(cuuint64_t)cin * 2, (cuuint64_t)W * cin * 2, (cuuint64_t)H * W * cin * 2};
+    const cuuint32_t box[4] = {8, (cuuint32_t)TC_SW, (cuuint32_t)(TC_TH + 2), 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const CUresult r = enc(out, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(x), dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
 template <int CIN, int COUT, bool RELU, bool OUT_F32, bool MASK>
 static cudaError_t conv_t(const void* x, const void* mask, int N, int H, int W, const void* w, const float* b, void* y,
                           cudaStream_t st) {
     if (N <= 0 || H <= 0 || W <= 0) return cudaSuccess;
-    // 16-byte operand loads and stores
+    // 16-byte operand loads and stores (and the TMA base address)
     if (((uintptr_t)x | (uintptr_t)w | (uintptr_t)y | (mask ? (uintptr_t)mask : 0)) & 15) return cudaErrorMisalignedAddress;
-    const size_t sm = 16 * ((size_t)9 * (CIN / 8) * COUT + (size_t)(CIN / 8) * TC_NPIX);
+    CUtensorMap tmap;
+    std::memset(&tmap, 0, sizeof(tmap));
+    cudaError_t e;
+    if (!MASK && (e = input_tensor_map(x, CIN, N, H, W, &tmap))) return e;
+    const size_t sm = ConvSmem<CIN, COUT, MASK>::BYTES;
     auto k = conv3x3_kernel<CIN, COUT, RELU, OUT_F32, MASK>;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e) return e;
+    if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm))) return e;
     int dev = 0, sms = 0;
     if ((e = cudaGetDevice(&dev)) || (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev))) return e;
     const long long tiles = (long long)((W + TC_TW - 1) / TC_TW) * ((H + TC_TH - 1) / TC_TH) * N;
     if (tiles > INT_MAX) return cudaErrorInvalidValue;
     const int grid = (int)std::min<long long>(tiles, (long long)sms * TC_CTAS_PER_SM);
-    k<<<grid, 128, sm, st>>>(reinterpret_cast<const bf16*>(x), reinterpret_cast<const bf16*>(mask), N, H, W,
+    k<<<grid, 128, sm, st>>>(tmap, reinterpret_cast<const bf16*>(x), reinterpret_cast<const bf16*>(mask), N, H, W,
                              reinterpret_cast<const bf16*>(w), b, y);
     return cudaGetLastError();
 }

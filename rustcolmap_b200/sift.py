@@ -65,6 +65,34 @@ def extract_sift(img, name="", opts=None, ctx=None):
         ctx._L.rcmvs_sift_frame_free(C.byref(f))
 
 
+def extract_sift_many(images, names=None, opts=None, ctxs=None):
+    """extract_sift of every image, spread over the contexts `ctxs` (one
+    CUDA stream each) with one host thread per context: an extraction waits
+    on its stream a few times per image (keypoint counts, chunked
+    descriptors, results) and the library call releases the GIL, so the
+    images' round trips and kernels overlap.  Image i runs on context
+    i % len(ctxs); each result is the single-context one (same kernels, same
+    order of operations per image).  Returns the frames in image order."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from .mvs import _ctx
+    ctxs = list(ctxs) if ctxs else [_ctx(None)]
+    names = names or [""] * len(images)
+    nw = len(ctxs)
+    if nw == 1 or len(images) < 2:
+        return [extract_sift(im, nm, opts, ctxs[0]) for im, nm in zip(images, names)]
+
+    def share(w):
+        return [(i, extract_sift(images[i], names[i], opts, ctxs[w])) for i in range(w, len(images), nw)]
+
+    frames = [None] * len(images)
+    with ThreadPoolExecutor(nw) as ex:
+        for part in ex.map(share, range(nw)):
+            for i, f in part:
+                frames[i] = f
+    return frames
+
+
 def match_pairs(descs, pairs, ratio=0.8, ctx=None):
     """match_pair for many pairs of frames in one batched call.  descs: list
     of (n_f, 128) f32 descriptor arrays; pairs: list of (i, j).  Returns one
@@ -107,16 +135,24 @@ def job_pairs(n, sequential=False):
     return [(i, j) for i in range(n) for j in range(i + 1, n)]
 
 
-def extract_and_match(images, names=None, opts=None, ratio=0.75, sequential=False, ctx=None):
+def extract_and_match(images, names=None, opts=None, ratio=0.75, sequential=False, ctx=None, workers=4):
     """The feature stage of sfm-lite's run_sfm (sfm-lite/src/lib.rs:137-225,
-    two-view verification excluded): SIFT of every decoded image, then
-    match_pair on every job pair in one batched call.  `ratio` defaults to
-    sfm-lite's Options::default() (lib.rs:61).  Returns (frames, pairs,
-    matches) with matches[p] = (a indices, b indices) of pairs[p]."""
+    two-view verification excluded): SIFT of every decoded image (spread
+    over `workers` contexts on ctx's device, extract_sift_many), then
+    match_pair on every job pair in one batched call on ctx.  `ratio`
+    defaults to sfm-lite's Options::default() (lib.rs:61).  Returns (frames,
+    pairs, matches) with matches[p] = (a indices, b indices) of pairs[p]."""
+    from .mvs import Context, _ctx
     if len(images) < 2:
         raise RcmvsError(-1, "need at least 2 images")
+    ctx = _ctx(ctx)
     names = names or [""] * len(images)
-    frames = [extract_sift(im, nm, opts, ctx) for im, nm in zip(images, names)]
+    extra = [Context(ctx.device) for _ in range(max(1, min(workers, len(images))) - 1)]
+    try:
+        frames = extract_sift_many(images, names, opts, [ctx] + extra)
+    finally:
+        for c in extra:
+            c.close()
     pairs = job_pairs(len(frames), sequential)
     return frames, pairs, match_pairs([f.desc for f in frames], pairs, ratio, ctx)
 

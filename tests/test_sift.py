@@ -13,7 +13,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle
-from rustcolmap_b200 import scene, sift
+from rustcolmap_b200 import mvs, scene, sift
 
 DESC_TOL = 1e-4
 
@@ -266,6 +266,26 @@ def test_extract_and_match_pipeline(ctx):
         oa, ob = oracle.match_pair(frames[i].desc, frames[j].desc, 0.75)
         assert np.array_equal(a, oa) and np.array_equal(b, ob)
     assert sum(len(a) for a, _ in matches) > 0
+
+
+@pytest.mark.gpu
+def test_extract_sift_many_equals_one_context(ctx):
+    """Spreading the images over three contexts (streams + host threads)
+    gives every image's single-context frame bit for bit, in image order."""
+    sc = scene.corner_room(seed=6, n_views=7, w=200, h=150, f=220.0, arc_deg=40.0, n_patches=40, per_view_sparse=10)
+    imgs = [np.ascontiguousarray(v.rgb) for v in sc.views] + [np.ascontiguousarray(sc.views[0].gray)]
+    one = [sift.extract_sift(im, ctx=ctx) for im in imgs]
+    extra = [mvs.Context(0), mvs.Context(0)]
+    try:
+        many = sift.extract_sift_many(imgs, ctxs=[ctx] + extra)
+    finally:
+        for c in extra:
+            c.close()
+    assert len(many) == len(one)
+    for a, b in zip(one, many):
+        assert (a.width, a.height, a.n_raw) == (b.width, b.height, b.n_raw)
+        for x, y in ((a.pts, b.pts), (a.desc, b.desc), (a.colors, b.colors)):
+            assert x.shape == y.shape and np.array_equal(x.view(np.uint8), y.view(np.uint8))
 
 
 def test_oracle_match_pair_matches_numpy_random():
