@@ -339,6 +339,7 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const __grid_constant__ CU
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ __align__(8) uint64_t bars[3];  // [0], [1]: tile loaded (per stage); [2]: MMAs done
     __shared__ uint32_t s_taddr;
+    __shared__ float s_bias[COUT];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     // 128-byte aligned base (TMA destinations)
     const uint32_t raw_a = smem_u32(smem);
@@ -363,6 +364,7 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const __grid_constant__ CU
         const int co = i % COUT, g = (i / COUT) % KG, tap = i / (COUT * KG);
         sw[i] = *reinterpret_cast<const uint4*>(wgt + (size_t)(tap * COUT + co) * CIN + g * 8);
     }
+    if (tid < COUT) s_bias[tid] = bias ? bias[tid] : 0.f;
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -465,7 +467,7 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(const __grid_constant__ CU
             float f[COUT];
 #pragma unroll
             for (int c = 0; c < COUT; ++c) {
-                float sv = __uint_as_float(v[c]) + (bias ? bias[c] : 0.f);
+                float sv = __uint_as_float(v[c]) + s_bias[c];
                 f[c] = RELU ? fmaxf(sv, 0.f) : sv;
             }
             if (OUT_F32) {
