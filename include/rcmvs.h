@@ -53,7 +53,11 @@ typedef struct rcmvs_options {
     uint32_t save_depth_vis; /* PNGs are written by the callers that write files
                                 (see rcmvs_depth_vis); rcmvs_run_mvs writes none */
     float cost_thr;          /* max census Hamming fraction of a valid pixel */
-    uint32_t reserved0;
+    uint32_t passes;         /* extension: Jacobi passes; 0 = 2*max(sweeps,1), the
+                                reference's schedule (rcmvs_pass_count).  The
+                                perturbation scales anneal over the passes run
+                                (t = pass / passes), as over 2*sweeps.  At most
+                                RCMVS_MAX_PASSES. */
     double depth_diff;       /* relative depth agreement in fusion */
     double voxel_rel;        /* voxel cell / robust sparse bbox diagonal */
     /* ---- extensions (no reference counterpart) ---- */
@@ -142,8 +146,15 @@ typedef struct rcmvs_options {
  * window rows. */
 #define RCMVS_FLAG_NO_REPEAT_SKIP 256u
 
+#define RCMVS_MAX_PASSES 4096u
+
+
 /* Fills `MvsOptions::default()` (mvs/src/lib.rs:56-70); extensions off. */
 void rcmvs_options_default(rcmvs_options* opts);
+/* The Jacobi passes an estimate with `opts` runs: 0 with
+ * RCMVS_FLAG_INIT_ONLY, else opts->passes when set, else
+ * 2 * max(sweeps, 1) (mvs/src/stereo.rs:271). */
+uint64_t rcmvs_pass_count(const rcmvs_options* opts);
 
 /* One registered view at working resolution.  Replaces `mvs::ViewData`
  * (mvs/src/lib.rs:86-101) with the grey image as u8 (ViewData.gray is

@@ -505,7 +505,8 @@ bool learned_init(const RefWorkspace& ws, const Seed& sd, int32_t x, int32_t y, 
 int estimate_impl(const rcmvs_view* views, int32_t n_views, int32_t ref_idx, const int32_t* srcs, int32_t n_src,
                   double zmin, double zmax, const rcmvs_options* opts, float* depth_out, float* cost_out,
                   float* normal_out, int32_t nthreads, uint64_t* work_out, Seed* sd) {
-    if (!check_views(views, n_views, ref_idx, srcs, n_src) || !opts || !depth_out || !cost_out)
+    if (!check_views(views, n_views, ref_idx, srcs, n_src) || !opts || !depth_out || !cost_out ||
+        opts->passes > RCMVS_MAX_PASSES)
         return RCMVS_E_ARG;
     std::vector<int> needed{ref_idx};
     for (int i = 0; i < n_src; ++i) needed.push_back(srcs[i]);
@@ -538,8 +539,10 @@ int estimate_impl(const rcmvs_view* views, int32_t n_views, int32_t ref_idx, con
         for (uint64_t c : seeded) sd->seeded += c;
 
     // ---- double-buffered passes (stereo.rs:271-371); none with RCMVS_FLAG_INIT_ONLY
-    const uint64_t n_passes =
-        (opts->flags & RCMVS_FLAG_INIT_ONLY) ? 0 : (uint64_t)std::max<uint32_t>(opts->sweeps, 1u) * 2;
+    // the passes option (an extension; 0 = the reference's 2 * max(sweeps, 1))
+    const uint64_t n_passes = (opts->flags & RCMVS_FLAG_INIT_ONLY) ? 0
+                              : opts->passes                     ? (uint64_t)opts->passes
+                                                                 : (uint64_t)std::max<uint32_t>(opts->sweeps, 1u) * 2;
     std::vector<Plane> next = prev;
     const float zlo = ws.zmin * 0.5f, zhi = ws.zmax * 2.0f;
     for (uint64_t pass = 0; pass < n_passes; ++pass) {

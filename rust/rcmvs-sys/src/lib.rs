@@ -39,6 +39,7 @@ pub const RCMVS_FLAG_INIT_ONLY: u32 = 32;
 pub const RCMVS_FLAG_SEED_AND_SWEEP: u32 = 64;
 pub const RCMVS_FLAG_ROW_STEP_INIT: u32 = 128;
 pub const RCMVS_FLAG_NO_REPEAT_SKIP: u32 = 256;
+pub const RCMVS_MAX_PASSES: u32 = 4096;
 
 pub const RCMVS_NOALLOC_MAX_PIXELS: u32 = 307200;
 pub const RCMVS_NOALLOC_MAX_SOURCES: u32 = 4;
@@ -55,7 +56,7 @@ pub struct rcmvs_options {
     pub min_consistent: u32,
     pub save_depth_vis: u32,
     pub cost_thr: f32,
-    pub reserved0: u32,
+    pub passes: u32,
     pub depth_diff: f64,
     pub voxel_rel: f64,
     pub reproj_px: f64,
@@ -196,6 +197,7 @@ pub struct rcmvs_net {
 extern "C" {
     /// MvsOptions::default() (mvs/src/lib.rs:56-70); extensions off.
 pub fn rcmvs_options_default(opts: *mut rcmvs_options);
+    pub fn rcmvs_pass_count(opts: *const rcmvs_options) -> u64;
     /// Releases a library-allocated cloud.
     pub fn rcmvs_points_free(pts: *mut rcmvs_points);
     /// A context on CUDA device `device` (with its own stream).

@@ -27,7 +27,7 @@ class Options(C.Structure):
         ("min_consistent", C.c_uint32),
         ("save_depth_vis", C.c_uint32),
         ("cost_thr", C.c_float),
-        ("reserved0", C.c_uint32),
+        ("passes", C.c_uint32),
         ("depth_diff", C.c_double),
         ("voxel_rel", C.c_double),
         ("reproj_px", C.c_double),

@@ -40,6 +40,7 @@ def mvs():
         "rcmvs_last_error": ([vp], cp),
         "rcmvs_ctx_stream": ([vp], vp),
         "rcmvs_ctx_synchronize": ([vp], C.c_int),
+        "rcmvs_pass_count": ([vp], C.c_uint64),
         "rcmvs_diag_wait_timeout": ([vp, C.c_uint64], C.c_int),
         "rcmvs_version": ([], cp),
         "rcmvs_census": ([vp, vp, i32, i32, vp], C.c_int),
@@ -126,7 +127,7 @@ def exported_symbols():
 
 
 _SIG_NAMES = [
-    "rcmvs_options_default", "rcmvs_ctx_create", "rcmvs_ctx_destroy", "rcmvs_last_error",
+    "rcmvs_options_default", "rcmvs_pass_count", "rcmvs_ctx_create", "rcmvs_ctx_destroy", "rcmvs_last_error",
     "rcmvs_ctx_stream", "rcmvs_ctx_synchronize", "rcmvs_diag_wait_timeout", "rcmvs_version", "rcmvs_census",
     "rcmvs_estimate_depth", "rcmvs_estimate_depth_batch", "rcmvs_fuse_depth_maps",
     "rcmvs_write_ply_binary", "rcmvs_write_dense_outputs", "rcmvs_plan", "rcmvs_run_mvs", "rcmvs_points_free",

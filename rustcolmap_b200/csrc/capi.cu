@@ -117,6 +117,12 @@ extern "C" {
 
 const char* rcmvs_version(void) { return "rcmvs 0.1 (sm_100a)"; }
 
+uint64_t rcmvs_pass_count(const rcmvs_options* o) {
+    if (!o || (o->flags & RCMVS_FLAG_INIT_ONLY)) return 0;
+    if (o->passes) return o->passes;
+    return (uint64_t)(o->sweeps > 1u ? o->sweeps : 1u) * 2u;
+}
+
 void rcmvs_options_default(rcmvs_options* o) {
     if (!o) return;
     std::memset(o, 0, sizeof(*o));
@@ -417,6 +423,7 @@ int rcmvs_scene_estimate_depth(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job*
                                 RCMVS_FLAG_SEED_AND_SWEEP |  // only affects the learned init
                                 RCMVS_FLAG_ROW_STEP_INIT | RCMVS_FLAG_NO_REPEAT_SKIP;
     if (opts->flags & ~kFlags) return fail(ctx, RCMVS_E_ARG, "unknown bits in opts->flags");
+    if (opts->passes > RCMVS_MAX_PASSES) return fail(ctx, RCMVS_E_ARG, "opts->passes above RCMVS_MAX_PASSES");
     if (n_jobs == 0) return RCMVS_OK;
     CK(cudaSetDevice(ctx->device));
     StereoBatch batch;
@@ -430,7 +437,7 @@ int rcmvs_scene_estimate_depth(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job*
              : (opts->flags & RCMVS_FLAG_ROW_STEP_INIT) ? Schedule::ROWS
                                                         : Schedule::TABLE;
     s.nh = (int)std::max<uint32_t>(opts->num_hyp, 2u);
-    s.n_passes = (opts->flags & RCMVS_FLAG_INIT_ONLY) ? 0 : (uint64_t)std::max<uint32_t>(opts->sweeps, 1u) * 2;
+    s.n_passes = rcmvs_pass_count(opts);
     s.cost_thr = opts->cost_thr;
     s.persistent = (opts->flags & RCMVS_FLAG_PERSISTENT) != 0;
     s.graph = (opts->flags & RCMVS_FLAG_CUDA_GRAPH) != 0;

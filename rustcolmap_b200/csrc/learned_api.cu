@@ -407,6 +407,7 @@ int check_seed_args(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job* jobs, int 
     if (n_local < 1 || n_local > 256 || !(span >= 0.f && span <= 1.f) || std::isnan(conf_thr))
         return lfail(ctx, RCMVS_E_ARG, "learned init: n_local must be 1..256, span in [0, 1], conf_thr a number");
     if (opts->flags & ~kSeedFlags) return lfail(ctx, RCMVS_E_ARG, "learned init: unsupported bits in opts->flags");
+    if (opts->passes > RCMVS_MAX_PASSES) return lfail(ctx, RCMVS_E_ARG, "opts->passes above RCMVS_MAX_PASSES");
     if (sc->ctx != ctx) return lfail(ctx, RCMVS_E_ARG, "scene belongs to another context");
     return check_jobs(ctx, sc, jobs, n_jobs);
 }
@@ -450,8 +451,7 @@ int seeded_stereo(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job* jobs, int n_
     Schedule sched;
     sched.init = Schedule::LEARNED;
     sched.nh = (int)std::max<uint32_t>(opts->num_hyp, 2u);
-    sched.n_passes =
-        (opts->flags & RCMVS_FLAG_INIT_ONLY) ? 0 : (uint64_t)std::max<uint32_t>(opts->sweeps, 1u) * 2;
+    sched.n_passes = rcmvs_pass_count(opts);
     sched.cost_thr = opts->cost_thr;
     sched.persistent = (opts->flags & RCMVS_FLAG_PERSISTENT) != 0;
     sched.graph = (opts->flags & RCMVS_FLAG_CUDA_GRAPH) != 0;

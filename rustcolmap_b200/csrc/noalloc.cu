@@ -90,7 +90,7 @@ extern "C" int rcmvs_estimate_depth_noalloc(const rcmvs_view* views, int32_t n_v
                                             const rcmvs_options* opts, float* depth_dev, float* cost_dev,
                                             void* stream) {
     if (!views || n_views <= 0 || ref_idx < 0 || ref_idx >= n_views || n_src < 0 || (n_src > 0 && !srcs) || !opts ||
-        !depth_dev || !cost_dev || (opts->flags & ~kNoallocFlags))
+        !depth_dev || !cost_dev || (opts->flags & ~kNoallocFlags) || opts->passes > RCMVS_MAX_PASSES)
         return RCMVS_E_ARG;
     if (!(finite_pos(zmin) && finite_pos(zmax))) return RCMVS_E_ARG;
     if (n_src > RCMVS_NOALLOC_MAX_SOURCES) return RCMVS_E_LIMIT;
@@ -210,8 +210,7 @@ extern "C" int rcmvs_estimate_depth_noalloc(const rcmvs_view* views, int32_t n_v
     const int variant = (opts->flags & RCMVS_FLAG_ONE_CANDIDATE) ? 1 : 0;
     const LaunchGeom g{ts.tw * ts.th, stereo_smem_bytes(ts), J.tiles, nullptr};
     NCK(launch_init(d_job, d_job_start, 1, g, nh, census, rays, A, nullptr, st, variant));
-    const uint64_t n_passes =
-        (opts->flags & RCMVS_FLAG_INIT_ONLY) ? 0 : (uint64_t)(opts->sweeps > 1u ? opts->sweeps : 1u) * 2;
+    const uint64_t n_passes = rcmvs_pass_count(opts);
     for (uint64_t pass = 0; pass < n_passes; ++pass) {
         const float t = (float)pass / (float)n_passes;  // stereo.rs:275-277
         const float sig_inv = 0.02f * powf(0.28f, t * 4.0f);

@@ -130,7 +130,8 @@ int trial(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job* jobs, int n_jobs, co
     float t_init = 0.f, t_pass = 0.f;
     SCK(cudaEventElapsedTime(&t_init, e0, e1));
     SCK(cudaEventElapsedTime(&t_pass, e1, e2));
-    *ms = t_init + 2.0f * (float)std::max<uint32_t>(opts->sweeps, 1u) * t_pass;
+    const uint64_t np = rcmvs_pass_count(opts);
+    *ms = t_init + (float)(np ? np : 2) * t_pass;
     return RCMVS_OK;
 }
 

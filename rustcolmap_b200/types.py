@@ -43,6 +43,7 @@ class MvsOptions:
     tile_h: int = 0
     flags: int = 0  # RCMVS_FLAG_* bits
     threads_per_pixel: int = 0  # Jacobi passes: 0/1 one thread per pixel, 5 five lanes per pixel
+    passes: int = 0  # Jacobi passes; 0 = 2 * max(sweeps, 1), the reference's schedule
 
     def to_c(self) -> _abi.Options:
         o = _abi.Options()
@@ -60,6 +61,7 @@ class MvsOptions:
         o.tile_h = self.tile_h
         o.flags = self.flags
         o.threads_per_pixel = self.threads_per_pixel
+        o.passes = self.passes
         return o
 
 

@@ -74,6 +74,16 @@ def test_options_default_mirrors_mvsoptions_default():
     assert o.depth_diff == 0.03 and abs(o.cost_thr - 0.38) < 1e-7 and o.voxel_rel == 0.0015
 
 
+def test_pass_count():
+    """2 * max(sweeps, 1) passes (stereo.rs:271) unless the passes extension
+    is set; none with RCMVS_FLAG_INIT_ONLY."""
+    from rustcolmap_b200.types import FLAG_INIT_ONLY
+    n = lambda **kw: _lib.mvs().rcmvs_pass_count(C.byref(MvsOptions(**kw).to_c()))
+    assert n(sweeps=6) == 12 and n(sweeps=0) == 2 and n(sweeps=1) == 2 and n(sweeps=3) == 6
+    assert n(sweeps=3, passes=5) == 5 and n(sweeps=6, passes=1) == 1
+    assert n(sweeps=3, passes=5, flags=FLAG_INIT_ONLY) == 0 and n(sweeps=6, flags=FLAG_INIT_ONLY) == 0
+
+
 def test_write_ply_matches_oracle(tmp_path):
     rng = np.random.default_rng(0)
     xyz = rng.normal(size=(257, 3))

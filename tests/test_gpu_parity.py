@@ -336,6 +336,22 @@ def test_fusion_saturated_projection_matches_oracle(ctx):
         _assert_same_cloud(g, c[:2])
 
 
+@pytest.mark.parametrize("passes,flags", [(1, 0), (3, 0), (5, 0), (5, 16), (7, 256)])
+def test_pass_count_extension_matches_oracle(ctx, corner_scene, c1_opts, passes, flags):
+    """The passes option (odd counts included, with the perturbation
+    annealing over the passes run) gives the oracle's bits, with and without
+    the shortcuts."""
+    import dataclasses
+    v = corner_scene.views
+    o = dataclasses.replace(c1_opts, passes=passes, flags=flags)
+    srcs, zr, _ = mvs.plan(corner_scene.sparse, v, o)
+    for ref in (2, 5):
+        d, c, n, _ = oracle.estimate_depth(v, ref, srcs[ref], zr[ref, 0], zr[ref, 1], o)
+        g = mvs.estimate_depth(v, ref, srcs[ref], zr[ref, 0], zr[ref, 1], o, ctx, normals=True)
+        for x, y in ((g.depth, d), (g.cost, c), (g.normal, n)):
+            assert_bits_equal(x, y, f"passes {passes} flags {flags} ref {ref}")
+
+
 @pytest.mark.parametrize("ref", [1, 6])
 def test_row_step_and_one_candidate_kernels_agree(ctx, corner_scene, c1_opts, ref):
     """The default table sweep, the one-candidate-at-a-time kernels
