@@ -9,9 +9,9 @@ gate.  One step = census + rays, patch-match stereo for all 100 views, and
 geometric-consistency fusion with voxel dedup (the PLY vertex records are
 packed on the device).  Two arms run on the same scene: the reference's
 schedule (plane-sweep init + 6 sweeps) and learned init (the committed
-proposal network, rustcolmap_b200/weights/proposal_c4.npy) + 3 sweeps with a
-0.25 cost gate (the operating point where its ground-truth coverage and
-precision both reach the plain arm's); both
+proposal network, rustcolmap_b200/weights/proposal_c4.npy) + 5 Jacobi passes
+with a 0.255 cost gate (the operating point where its ground-truth coverage
+and precision both reach the plain arm's); both
 report the fraction of ground-truth pixels within 1% inverse depth.
 
 value  depth maps/s of the learned arm with inputs resident in HBM
@@ -747,7 +747,8 @@ def main():
         cpu = {"value": rate, "unit": "depth maps/s", "cores": nt, "kind": "port", "sample": desc, "seconds": dt}
 
     if rank == 0:
-        per_step = (1 + 1 + 2 * opts.sweeps + 1 + 5) if args.plain_only else (1 + 3 + 6 + 1 + 2 * lopts.sweeps + 1 + 5)
+        n_pass = lambda o: o.passes if o.passes else 2 * max(o.sweeps, 1)
+        per_step = (1 + 1 + n_pass(opts) + 1 + 5) if args.plain_only else (1 + 3 + 6 + 1 + n_pass(lopts) + 1 + 5)
         line = {
             "metric": METRIC, "value": value, "unit": "depth maps/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": head_ms / args.steps, "higher_is_better": True,
@@ -757,7 +758,7 @@ def main():
                        "headline_arm": "plain, 6 sweeps" if args.plain_only else
                        f"learned init (proposal_c4 weights; pixels with confidence >= "
                        f"{args.conf if args.conf is not None else learned.CONF_THR} start from the "
-                       f"predicted plane, the others from the 64-plane sweep) + {lopts.sweeps} sweeps, "
+                       f"predicted plane, the others from the 64-plane sweep) + {n_pass(lopts)} passes, "
                        f"gate cost < {lopts.cost_thr:g}",
                        "parallelism": f"views batched on 1 GPU; {ws} rank(s), one independent scene each",
                        "l2": "inputs larger than L2 (census 8 B/px, rays 8 B/px, planes 40 B/px over all views)"},
@@ -765,7 +766,7 @@ def main():
                       "ms_per_step": plain_ms / args.steps, "gt": plain_gt, "fused_points": plain_pts,
                       "kernel_ms_per_step": {k: v[0] / args.steps for k, v in plain_kt.items() if v[1]}},
             "learned": None if args.plain_only else {
-                "value": value, "sweeps": lopts.sweeps, "gt": head_gt, "fused_points": head_pts,
+                "value": value, "passes": n_pass(lopts), "gt": head_gt, "fused_points": head_pts,
                 "seeded_fraction": seeded[0] / max(npx, 1), "speedup_vs_plain": value / plain_value,
                 "gt_within_delta_vs_plain": head_gt["within_1pct"] - plain_gt["within_1pct"]},
             "roofline": {"bound": "hbm", "kernel": "stereo_pass", "achieved": achieved_gbs, "peak": hbm_peak,
