@@ -430,9 +430,10 @@ def test_seeded_oracle_selects_the_gated_proposals():
 
 @pytest.mark.gpu
 def test_committed_network_gains_over_the_plain_method(ctx):
-    """The committed weights on two held-out config-4 scenes (seeds 6000 and
-    6001, outside the training seeds 1000-1399 and the tuning seeds
-    5000-5019), at the library's operating point (learned.LEARNED_PASSES
+    """The committed weights on eight held-out config-4 scenes (seeds
+    6000-6007, outside the training seeds 1000-1399 and the tuning seeds
+    5000-5019; the operating point's precision margin, about 1%, is below
+    the scatter of a two-scene mean), at the library's operating point (learned.LEARNED_PASSES
     passes, gate learned.LEARNED_COST_THR) against the plain method with 6
     sweeps (the reference schedule) and with the same passes.  The learned
     arm must be at least 1.5x as fast as plain-6 (stereo views/s, CUDA
@@ -441,7 +442,7 @@ def test_committed_network_gains_over_the_plain_method(ctx):
     its precision (the same over valid pixels), and must beat the plain
     method with the same passes by 3 points of coverage."""
     net = learned.ProposalNet(ctx, params=learned.load_weights())
-    agg, rows = learned.evaluate(net, [6000, 6001], ctx, log=print)
+    agg, rows = learned.evaluate(net, list(range(6000, 6008)), ctx, log=print)
     net.close()
     p6, p2, le = agg["plain6"], agg["plain_short"], agg["learned"]
     print(f"plain-6 {p6['views_per_s']:.1f} views/s within {p6['within']:.4f} accuracy {p6['accuracy']:.3f}; "
