@@ -706,7 +706,8 @@ def main():
     e2e = None
     if not args.no_e2e:
         pv = pinned_views(sc.views)
-        mvs.run_mvs(pv, sc.sparse, head_opts, ctx=ctx, net=net, **lkw)  # warm
+        for _ in range(max(args.warmup, 1)):  # warm: the first calls settle the context's buffers
+            mvs.run_mvs(pv, sc.sparse, head_opts, ctx=ctx, net=net, **lkw)
         torch.cuda.synchronize()
         barrier(ws)
         t0 = time.perf_counter()
@@ -719,7 +720,9 @@ def main():
         h2d = int(sum(v.gray.nbytes + v.rgb.nbytes for v in pv))
         e2e = {"value": sum_over_ranks(n_maps * args.steps, ws, local) / dt, "unit": "depth maps/s",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(xyz.nbytes + rgb.nbytes),
-               "ms_per_step": 1e3 * dt / args.steps, "call": "rcmvs_run_mvs" + ("" if net is None else "_learned")}
+               "ms_per_step": 1e3 * dt / args.steps, "call": "rcmvs_run_mvs" + ("" if net is None else "_learned"),
+               # device spans of the call's stereo and fusion (CUDA events inside the call), last step
+               "device_ms": {"stereo": 1e3 * st.stereo_s, "fuse": 1e3 * st.fuse_s}}
 
     # roofline of the dominant kernel (the Jacobi pass) in the headline arm
     npx = sum(sc.views[r].w * sc.views[r].h for r, _, _, _ in jobs)

@@ -194,35 +194,44 @@ def quarter_labels(depth, normal, zmin, zmax, min_valid=8):
     return lab
 
 
-def orbit_c4(seed, device=0):
+def orbit_c4(seed, device=0, normals=False):
     """Config 4's scenes: seeded room + 20 boxes, 16 views at 960x720 on a
     120-degree arc (8 degrees apart: on a full orbit, 22.5 degrees apart, the
     plain method's census costs rarely pass its 0.38 gate and it labels
     almost nothing)."""
     return scene.orbit_room(seed=seed, n_views=16, sizes=((960, 720),), f_rel=1.1, n_boxes=20, n_spheres=0,
-                            device=device, per_view_sparse=300, arc_deg=120.0)
+                            device=device, per_view_sparse=300, arc_deg=120.0, normals=normals)
 
 
 C4_OPTS = MvsOptions(max_dim=960, num_sources=4, sweeps=6, num_hyp=64)
 
 
-def make_dataset(seeds, ctx, torch, dev, log=print):
+def make_dataset(seeds, ctx, torch, dev, log=print, labels="plain"):
     """Cost volumes (device, BF16) and labels (device, f32) of every view of
-    the given scenes; labels from the plain GPU patch-match (6 sweeps)."""
+    the given scenes.  labels "plain": from the plain GPU patch-match (6
+    sweeps); "gt": from the rendered ground-truth depth and normals (the
+    renderer's normals face the camera; a patch-match plane's normal n has
+    n . ray > 0, so they are negated)."""
     xs, labs = [], []
     nvalid = 0.0
     t0 = time.time()
     for k, seed in enumerate(seeds):
-        sc = orbit_c4(seed)
+        sc = orbit_c4(seed, normals=labels == "gt")
         srcs, zr, _ = mvs.plan(sc.sparse, sc.views, C4_OPTS)
         jobs = [(i, srcs[i], zr[i, 0], zr[i, 1]) for i in range(len(sc.views)) if srcs[i]]
         ds = mvs.DeviceScene(sc.views, ctx)
-        ds.estimate(jobs, C4_OPTS)
+        if labels == "plain":
+            ds.estimate(jobs, C4_OPTS)
+        else:
+            ds.prepare()  # census and rays, which the cost volume reads
         hq, wq = sc.views[0].h // 4, sc.views[0].w // 4
         x = torch.empty((len(jobs), hq, wq, COSTVOL_C), dtype=torch.bfloat16, device=dev)
         costvol(ds, jobs, x.data_ptr())
-        lab = np.stack([quarter_labels(*(lambda m: (m.depth, m.normal))(ds.depth(j[0], normals=True)), j[2], j[3])
-                        for j in jobs])
+        if labels == "gt":
+            maps = [(sc.gt_depth[j[0]], -sc.gt_normal[j[0]]) for j in jobs]
+        else:
+            maps = [(lambda m: (m.depth, m.normal))(ds.depth(j[0], normals=True)) for j in jobs]
+        lab = np.stack([quarter_labels(d, n, j[2], j[3]) for (d, n), j in zip(maps, jobs)])
         ds.close()
         xs.append(x)
         labs.append(torch.from_numpy(lab).to(dev))
@@ -333,11 +342,13 @@ def main():
     ap.add_argument("--json", default=None)
     ap.add_argument("--local-hyps", type=int, default=LOCAL_HYPS)
     ap.add_argument("--local-span", type=float, default=LOCAL_SPAN)
+    ap.add_argument("--labels", choices=["plain", "gt"], default="plain",
+                    help="train on the plain method's depth maps or on the rendered ground truth")
     a = ap.parse_args()
     ctx = mvs.default_context()
     dev = torch.device("cuda:0")
     if a.cmd == "train":
-        x, lab = make_dataset(list(range(a.seed0, a.seed0 + a.seeds)), ctx, torch, dev)
+        x, lab = make_dataset(list(range(a.seed0, a.seed0 + a.seeds)), ctx, torch, dev, labels=a.labels)
         net = ProposalNet(ctx, seed=0)
         t0 = time.time()
         losses = train(net, x, lab, iters=a.iters, batch=a.batch, lr=a.lr)
