@@ -9,8 +9,8 @@ gate.  One step = census + rays, patch-match stereo for all 100 views, and
 geometric-consistency fusion with voxel dedup (the PLY vertex records are
 packed on the device).  Two arms run on the same scene: the reference's
 schedule (plane-sweep init + 6 sweeps) and learned init (the committed
-proposal network, rustcolmap_b200/weights/proposal_c4.npy) + 5 Jacobi passes
-with a 0.255 cost gate (the operating point where its ground-truth coverage
+proposal network, rustcolmap_b200/weights/proposal_c4.npy) + 4 Jacobi passes
+with a 0.245 cost gate (the operating point where its ground-truth coverage
 and precision both reach the plain arm's); both
 report the fraction of ground-truth pixels within 1% inverse depth.
 

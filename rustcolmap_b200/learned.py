@@ -100,10 +100,11 @@ LEARNED_FLAGS = 0  # RCMVS_FLAG_* bits of the learned arm
 # fastest schedule whose coverage (pixels with ground truth valid and within
 # 1%) and precision (valid pixels within 1%) both reach the plain method's
 # with 6 sweeps at the reference's gate (0.38: 0.2532 / 0.842), at the gate
-# with the largest smaller relative margin of the two.  4 passes reach
-# neither at any gate; 5 passes qualify at gates 0.25-0.26 and 0.255 gives
-# 0.2572 / 0.852 (+1.6% / +1.2%); 6 passes qualify at 0.24-0.265.
-LEARNED_PASSES, LEARNED_COST_THR = 5, 0.255
+# with the largest smaller relative margin of the two.  With the committed
+# weights (800 training scenes) 3 passes reach both at no gate (0.2548 /
+# 0.841 at 0.255); 4 passes qualify at gates 0.24-0.26, and 0.245 gives
+# 0.2595 / 0.862 (+2.5% / +2.4%).
+LEARNED_PASSES, LEARNED_COST_THR = 4, 0.245
 LEARNED_SWEEPS = 3  # sweeps field of the learned arm's options (passes overrides it)
 
 
