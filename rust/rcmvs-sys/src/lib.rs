@@ -39,6 +39,7 @@ pub const RCMVS_FLAG_INIT_ONLY: u32 = 32;
 pub const RCMVS_FLAG_SEED_AND_SWEEP: u32 = 64;
 pub const RCMVS_FLAG_ROW_STEP_INIT: u32 = 128;
 pub const RCMVS_FLAG_NO_REPEAT_SKIP: u32 = 256;
+pub const RCMVS_FLAG_LOCKSTEP_PASSES: u32 = 512;
 pub const RCMVS_MAX_PASSES: u32 = 4096;
 
 pub const RCMVS_NOALLOC_MAX_PIXELS: u32 = 307200;

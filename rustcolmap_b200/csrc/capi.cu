@@ -421,7 +421,7 @@ int rcmvs_scene_estimate_depth(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job*
     constexpr uint32_t kFlags = RCMVS_FLAG_ONE_CANDIDATE | RCMVS_FLAG_PERSISTENT | RCMVS_FLAG_CUDA_GRAPH |
                                 RCMVS_FLAG_AUTOTUNE | RCMVS_FLAG_NO_SKIP_DUPLICATES | RCMVS_FLAG_INIT_ONLY |
                                 RCMVS_FLAG_SEED_AND_SWEEP |  // only affects the learned init
-                                RCMVS_FLAG_ROW_STEP_INIT | RCMVS_FLAG_NO_REPEAT_SKIP;
+                                RCMVS_FLAG_ROW_STEP_INIT | RCMVS_FLAG_NO_REPEAT_SKIP | RCMVS_FLAG_LOCKSTEP_PASSES;
     if (opts->flags & ~kFlags) return fail(ctx, RCMVS_E_ARG, "unknown bits in opts->flags");
     if (opts->passes > RCMVS_MAX_PASSES) return fail(ctx, RCMVS_E_ARG, "opts->passes above RCMVS_MAX_PASSES");
     if (n_jobs == 0) return RCMVS_OK;

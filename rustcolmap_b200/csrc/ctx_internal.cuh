@@ -152,7 +152,8 @@ namespace rcmvs {
 // Arena slots of a scene shared by the translation units (the others are
 // private to capi.cu 2-10, fuse.cu 16-37 and 70-74, learned_api.cu 40-47, depthvis.cu 50-55,
 // resize.cu 60-68, sift.cu 80-159 and match.cu 160-167).
-constexpr int kSlotJobs = 0, kSlotJobStart = 1, kSlotQueue = 11, kSlotTuneJobs = 12, kSlotTuneStart = 13;
+constexpr int kSlotJobs = 0, kSlotJobStart = 1, kSlotQueue = 11, kSlotTuneJobs = 12, kSlotTuneStart = 13,
+              kSlotStreamStart = 14;
 
 // resize.cu: argument and size checks of a resize, and the resize itself
 // on device buffers (d_gray mw*mh, d_rgb mw*mh*3), queued on the context's
@@ -177,6 +178,11 @@ struct StereoBatch {
     std::vector<int32_t> start;  // n_jobs + 1
     std::vector<int> order;      // launch position -> caller's job index
     LaunchGeom geom{};
+    // streamed passes (pass_stream_kernel, the default): the jobs' tile starts
+    // in that kernel's tiling (n_jobs + 1) and its launch geometry
+    bool stream = false;
+    std::vector<int32_t> sstart;
+    LaunchGeom sgeom{};
 };
 
 // The launch schedule of a batch: init -> n_passes Jacobi passes -> gate.

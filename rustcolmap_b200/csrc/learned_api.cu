@@ -399,7 +399,7 @@ int check_jobs(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job* jobs, int n_job
 
 constexpr uint32_t kSeedFlags = RCMVS_FLAG_PERSISTENT | RCMVS_FLAG_CUDA_GRAPH | RCMVS_FLAG_AUTOTUNE |
                                RCMVS_FLAG_NO_SKIP_DUPLICATES | RCMVS_FLAG_INIT_ONLY | RCMVS_FLAG_SEED_AND_SWEEP |
-                               RCMVS_FLAG_NO_REPEAT_SKIP |
+                               RCMVS_FLAG_NO_REPEAT_SKIP | RCMVS_FLAG_LOCKSTEP_PASSES |
                                RCMVS_FLAG_ROW_STEP_INIT;  // the learned init has its own sweep: no effect here
 
 int check_seed_args(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job* jobs, int n_jobs, const rcmvs_options* opts,

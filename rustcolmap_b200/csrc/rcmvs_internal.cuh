@@ -81,7 +81,12 @@ struct LaunchGeom {
     int tiles;
     unsigned int* queue;
     int tpp = 1;  // threads per pixel of the passes: 1, or 5 (pass_split_kernel)
+    bool stream = false;  // passes: pass_stream_kernel over the stream tiling (stream_geom)
 };
+// Streamed passes (pass_stream_kernel): tiles of a w x h view in the
+// kernel's own tiling, and the geometry of a launch over `tiles` of them.
+int stream_tiles(int w, int h);
+LaunchGeom stream_geom(int tiles);
 // Threads of a split-pass block (5 lanes per pixel, 6 pixels per warp) for
 // tiles of up to px pixels.
 int split_threads(int px);

@@ -95,6 +95,16 @@ int assemble(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job* jobs, int n_jobs,
     if (tiles > INT32_MAX) return sfail(ctx, RCMVS_E_LIMIT, "too many tiles in one batch");
     b.start[n_jobs] = (int32_t)tiles;
     b.geom = LaunchGeom{nthr, smem, (int)tiles, nullptr};
+    // the streamed passes' own tiling of the same jobs, in launch order
+    b.sstart.resize(n_jobs + 1);
+    int64_t stiles = 0;
+    for (int p = 0; p < n_jobs; ++p) {
+        b.sstart[p] = (int32_t)stiles;
+        stiles += stream_tiles(b.jobs[p].w, b.jobs[p].h);
+    }
+    if (stiles > INT32_MAX) return sfail(ctx, RCMVS_E_LIMIT, "too many tiles in one batch");
+    b.sstart[n_jobs] = (int32_t)stiles;
+    b.sgeom = stream_geom((int)stiles);
     return RCMVS_OK;
 }
 
@@ -304,6 +314,7 @@ int build_batch(rcmvs_ctx* ctx, rcmvs_scene* sc, const rcmvs_job* jobs, int n_jo
     }
     int rc = assemble(ctx, sc, jobs, n_jobs, shp, true, b);
     b.geom.tpp = tpp;
+    b.stream = tpp == 1 && !(opts->flags & RCMVS_FLAG_LOCKSTEP_PASSES);
     return rc;
 }
 
@@ -325,8 +336,15 @@ int run_batch(rcmvs_ctx* ctx, rcmvs_scene* sc, const StereoBatch& b, const Sched
     // pageable -> device copies return once the host data has been staged
     SCK(cudaMemcpyAsync(pj, b.jobs.data(), sizeof(DevJob) * n_jobs, cudaMemcpyHostToDevice, st));
     SCK(cudaMemcpyAsync(ps, b.start.data(), sizeof(int32_t) * (n_jobs + 1), cudaMemcpyHostToDevice, st));
+    void* pss = nullptr;
+    if (b.stream) {
+        SCK(sc->arena.get(kSlotStreamStart, sizeof(int32_t) * (n_jobs + 1), &pss));
+        SCK(cudaMemcpyAsync(pss, b.sstart.data(), sizeof(int32_t) * (n_jobs + 1), cudaMemcpyHostToDevice, st));
+    }
     const DevJob* dj = (const DevJob*)pj;
     const int32_t* dst = (const int32_t*)ps;
+    // the passes' tile starts and geometry (the streamed tiling by default)
+    const int32_t* pst = b.stream ? (const int32_t*)pss : dst;
     unsigned int* queue = (unsigned int*)pq;
     // pass flags (the repeat skip) only with the duplicate skip: both off is
     // the reference's own call sequence
@@ -360,12 +378,13 @@ int run_batch(rcmvs_ctx* ctx, rcmvs_scene* sc, const StereoBatch& b, const Sched
                             s.init == Schedule::ONE_CANDIDATE ? 1 : (s.init == Schedule::TABLE ? 2 : 0));
         hk.end(s.init == Schedule::LEARNED ? "learned_init" : "stereo_init");
         if (e) return e;
+        LaunchGeom gp = b.stream ? b.sgeom : b.geom;
         for (uint64_t pass = 0; pass < s.n_passes; ++pass) {
-            g.queue = queue ? queue + 1 + pass : nullptr;
+            gp.queue = queue ? queue + 1 + pass : nullptr;
             hk.begin("stereo_pass");
             PlaneBuf P = A;
             if (pass == 0) P.flag = nullptr;  // the init leaves no pass flags
-            e = launch_pass(dj, dst, n_jobs, g, pass, sig[2 * pass], sig[2 * pass + 1], sc->census, sc->rays, P, B,
+            e = launch_pass(dj, pst, n_jobs, gp, pass, sig[2 * pass], sig[2 * pass + 1], sc->census, sc->rays, P, B,
                             s.d_work, st);
             hk.end("stereo_pass");
             if (e) return e;
@@ -389,6 +408,8 @@ int run_batch(rcmvs_ctx* ctx, rcmvs_scene* sc, const StereoBatch& b, const Sched
     append(key, b.geom.nthr);
     append(key, b.geom.smem);
     append(key, b.geom.tpp);
+    append(key, b.stream);
+    append(key, b.sstart.data(), sizeof(int32_t) * (n_jobs + 1));
     append(key, (int)s.init);
     append(key, s.nh);
     append(key, s.n_passes);
@@ -397,7 +418,7 @@ int run_batch(rcmvs_ctx* ctx, rcmvs_scene* sc, const StereoBatch& b, const Sched
     append(key, s.n_local);
     append(key, s.span);
     append(key, s.sweep_seeded);
-    const void* ptrs[] = {pj, ps, pq, s.d_work, s.pred, s.pred_off, s.d_learned, sc->census, sc->rays,
+    const void* ptrs[] = {pj, ps, pss, pq, s.d_work, s.pred, s.pred_off, s.d_learned, sc->census, sc->rays,
                           sc->plane_a, sc->plane_b, sc->pcost_a, sc->pcost_b, A0.d, B0.d, A0.flag, B0.flag,
                           sc->depth, sc->cost, sc->normal};
     append(key, ptrs, sizeof(ptrs));

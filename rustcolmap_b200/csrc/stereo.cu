@@ -546,6 +546,316 @@ __global__ void __maxnreg__(72)
     if (COUNT) flush_work(wc, d_work);
 }
 
+// ---------------------------------------------------------------- streamed passes
+// The same pass with the tile's pixels streamed through the block's lanes.
+// In pass_kernel a warp holds every candidate slot for as long as its
+// slowest lane needs: most evaluations abort after a window row or two while
+// a good candidate runs all 5*K rows, so most lanes wait.  Here a block of
+// STREAM_THREADS threads owns a STREAM_TW x STREAM_TH tile (four pixels per
+// thread) and works in two phases:
+//   1. preparation, one thread per pixel: the pixel's stored plane and cost,
+//      the neighbour candidates that pass the gates and the skip rules
+//      (stereo.rs:292-321), and its three random perturbations drawn from
+//      the pixel's RNG (stereo.rs:323-353).  The perturbations depend on the
+//      stored plane alone, never on a cost, so drawing them ahead of the
+//      evaluations gives the same planes.  The pass's output for a pixel
+//      that accepts nothing (the carried-over plane, stereo.rs:278) is
+//      written here.
+//   2. evaluation: every lane advances its own candidate by one window row
+//      per loop iteration; a lane whose candidate ends starts the pixel's
+//      next one, and a lane whose pixel ends writes it (if a candidate beat
+//      its cost) and claims the next unclaimed pixel of the tile.
+// Each pixel still meets its candidates, hints, rejection bounds and
+// best-cost updates in the reference's order, so every output bit (and each
+// work counter) is pass_kernel's.  Support-view parameters live field-major
+// in shared memory (field f of view s at f * RCMVS_MAX_SOURCES + s), so lanes
+// on different views read different banks and lanes on the same view read
+// one broadcast word.
+constexpr int STREAM_TW = 16, STREAM_TH = 16;
+constexpr int STREAM_PX = STREAM_TW * STREAM_TH;
+constexpr int STREAM_THREADS = 64;
+constexpr int STREAM_CELLS = (STREAM_TW + 2 * HALO) * (STREAM_TH + 2 * HALO);
+constexpr int SF_N = 19;  // rs[9], ts[3], f, cx, cy, k, (float)w, (float)h, w (int bits)
+
+struct StreamSmem {
+    float4* rnd;        // [STREAM_PX][3] random candidates (n, d)
+    uint64_t* cen;      // halo tile
+    float2* ray;        // halo tile
+    const uint64_t** scp;  // [RCMVS_MAX_SOURCES] census of each support view
+    float* sf;          // [SF_N][RCMVS_MAX_SOURCES]
+    float* tab;         // 64 (49 used): h / 48.0f
+    uint32_t* pix;      // [STREAM_PX]: lx | ly << 8 | candidate bits << 16
+    float* pcost;       // [STREAM_PX] stored cost
+};
+
+__host__ __device__ constexpr size_t stream_smem_bytes() {
+    return sizeof(float4) * STREAM_PX * 3 + (sizeof(uint64_t) + sizeof(float2)) * STREAM_CELLS +
+           sizeof(uint64_t*) * RCMVS_MAX_SOURCES + sizeof(float) * SF_N * RCMVS_MAX_SOURCES + 64 * sizeof(float) +
+           (sizeof(uint32_t) + sizeof(float)) * STREAM_PX;
+}
+
+__device__ __forceinline__ StreamSmem carve_stream(unsigned char* base) {
+    StreamSmem s;
+    s.rnd = reinterpret_cast<float4*>(base);
+    s.cen = reinterpret_cast<uint64_t*>(s.rnd + STREAM_PX * 3);
+    s.ray = reinterpret_cast<float2*>(s.cen + STREAM_CELLS);
+    s.scp = reinterpret_cast<const uint64_t**>(s.ray + STREAM_CELLS);
+    s.sf = reinterpret_cast<float*>(s.scp + RCMVS_MAX_SOURCES);
+    s.tab = s.sf + SF_N * RCMVS_MAX_SOURCES;
+    s.pix = reinterpret_cast<uint32_t*>(s.tab + 64);
+    s.pcost = reinterpret_cast<float*>(s.pix + STREAM_PX);
+    return s;
+}
+
+__device__ __forceinline__ SrcRegs load_src_fm(const StreamSmem& sm, int si) {
+    const float* b = sm.sf + si;
+    constexpr int S = RCMVS_MAX_SOURCES;
+    SrcRegs r;
+    r.rs0 = b[0 * S];
+    r.rs1 = b[1 * S];
+    r.rs2 = b[2 * S];
+    r.rs3 = b[3 * S];
+    r.rs4 = b[4 * S];
+    r.rs5 = b[5 * S];
+    r.rs6 = b[6 * S];
+    r.rs7 = b[7 * S];
+    r.rs8 = b[8 * S];
+    r.ts0 = b[9 * S];
+    r.ts1 = b[10 * S];
+    r.ts2 = b[11 * S];
+    r.f = b[12 * S];
+    r.cx = b[13 * S];
+    r.cy = b[14 * S];
+    r.k = b[15 * S];
+    r.swf = b[16 * S];
+    r.shf = b[17 * S];
+    r.sw = __float_as_int(b[18 * S]);
+    r.sh = 0;  // not read by cost_row
+    r.sc = sm.scp[si];
+    return r;
+}
+
+template <bool COUNT, bool PERSIST>
+__global__ void __launch_bounds__(STREAM_THREADS, 8)
+    pass_stream_kernel(const DevJob* __restrict__ jobs, const int32_t* __restrict__ stile_start, int n_jobs, int tiles,
+                       unsigned int* queue, uint64_t pass, float sig_inv, float sig_n,
+                       const uint64_t* __restrict__ census, const float2* __restrict__ rays, PlaneBuf prev,
+                       PlaneBuf next, unsigned long long* d_work) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int s_tile, s_next;
+    const StreamSmem sm = carve_stream(smem_raw);
+    const Smem rs{nullptr, sm.tab, sm.ray, sm.cen};  // the view cost_row reads
+    constexpr int stw = STREAM_TW + 2 * HALO;
+    const bool skip_dup = prev.d != nullptr;
+    const uint8_t* __restrict__ pflag = prev.flag;
+    const int lane = threadIdx.x & 31;
+    WorkCount wc{0, 0};
+    for (int it = 0; PERSIST || it == 0; ++it) {
+        const int tile = PERSIST ? next_tile(queue, tiles, it, &s_tile) : (int)blockIdx.x;
+        if (tile < 0) break;
+        const int j = find_item(stile_start, n_jobs, tile);
+        const DevJob* J = jobs + j;
+        const int w = J->w, h = J->h, nsrc = J->nsrc;
+        const int t = tile - stile_start[j];
+        const int stx = (w + STREAM_TW - 1) / STREAM_TW;
+        const int x0 = (t % stx) * STREAM_TW, y0 = (t / stx) * STREAM_TH;
+        const int vw = min(STREAM_TW, w - x0), vh = min(STREAM_TH, h - y0);
+        const int np = vw * vh;
+        const size_t base = (size_t)J->off;
+
+        // ---- staging: support views (field-major), h/48 table, halo tile
+        for (int i = threadIdx.x; i < nsrc * SF_N; i += STREAM_THREADS) {
+            const int s = i / SF_N, f = i - s * SF_N;
+            const DevSrc& S = J->src[s];
+            float v;
+            if (f < 16)
+                v = reinterpret_cast<const float*>(&S)[f];  // rs[9], ts[3], f, cx, cy, k
+            else if (f == 16)
+                v = (float)S.w;
+            else if (f == 17)
+                v = (float)S.h;
+            else
+                v = __int_as_float(S.w);
+            sm.sf[f * RCMVS_MAX_SOURCES + s] = v;
+        }
+        for (int s = threadIdx.x; s < nsrc; s += STREAM_THREADS) sm.scp[s] = census + J->src[s].off;
+        for (int i = threadIdx.x; i < 49; i += STREAM_THREADS) sm.tab[i] = (float)i / 48.0f;
+        for (int i = threadIdx.x; i < STREAM_CELLS; i += STREAM_THREADS) {
+            const int sx = i % stw, sy = i / stw;
+            const int gx = min(max(x0 - HALO + sx, 0), w - 1);
+            const int gy = min(max(y0 - HALO + sy, 0), h - 1);
+            const size_t g = base + (size_t)gy * w + gx;
+            sm.ray[i] = __ldg(rays + g);
+            sm.cen[i] = __ldg(census + g);
+        }
+        if (threadIdx.x == 0) s_next = 0;
+        __syncthreads();
+
+        const float total = 5.0f * 5.0f * (float)nsrc;
+        const float inv_min = J->inv_min, inv_max = J->inv_max;
+        const float zlo = J->zmin * 0.5f, zhi = J->zmax * 2.0f;
+
+        // ---- phase 1: prepare every pixel of the tile
+        for (int p = threadIdx.x; p < np; p += STREAM_THREADS) {
+            const int lx = p % vw, ly = p / vw;
+            const int x = x0 + lx, y = y0 + ly;
+            const size_t i = base + (size_t)y * w + x;
+            const float2 ri = sm.ray[(ly + HALO) * stw + lx + HALO];
+            uint64_t seed = pixel_rng(x, y, pass + 7);
+            const float4 cur = prev.nz[i];
+            const float cur_cost = prev.cost[i];
+            const float cur_d = skip_dup ? prev.d[i] : 0.f;
+            const bool repeat = skip_dup && pflag != nullptr && !(pflag[i] & 2);
+            unsigned mask = 0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {  // the gates of pass_kernel's neighbour()
+                const int ddx = q == 0 ? -1 : (q == 1 ? 1 : 0);
+                const int ddy = q == 2 ? -1 : (q == 3 ? 1 : 0);
+                const int xx = x + ddx, yy = y + ddy;
+                if (xx < 0 || yy < 0 || xx >= w || yy >= h) continue;
+                const size_t ni = base + (size_t)yy * w + xx;
+                if (repeat && !(pflag[ni] & 1)) continue;
+                const float4 nb = prev.nz[ni];
+                const float2 rj = sm.ray[(ly + HALO + ddy) * stw + lx + HALO + ddx];
+                const float a_nb = nb.x * rj.x + nb.y * rj.y + nb.z;
+                if (a_nb < 0.1f) continue;
+                const float d_plane = nb.w * a_nb;
+                const float a_here = nb.x * ri.x + nb.y * ri.y + nb.z;
+                if (a_here < 0.1f) continue;
+                const float zcand = d_plane / a_here;
+                if (!(zlo <= zcand && zcand <= zhi)) continue;
+                if (skip_dup && __float_as_uint(d_plane) == __float_as_uint(cur_d) &&
+                    __float_as_uint(nb.x) == __float_as_uint(cur.x) && __float_as_uint(nb.y) == __float_as_uint(cur.y) &&
+                    __float_as_uint(nb.z) == __float_as_uint(cur.z))
+                    continue;
+                mask |= 1u << q;
+            }
+#pragma unroll 1
+            for (int r = 0; r < 3; ++r) {  // stereo.rs:323-353, as pass_kernel
+                const float inv = 1.0f / fmaxf(cur.w, 1e-6f);
+                const float inv_new = inv + sig_inv * (inv_max - inv_min) * gauss3(seed);
+                if (inv_new <= 0.0f) continue;
+                const float zcand = 1.0f / inv_new;
+                if (!(zlo <= zcand && zcand <= zhi)) continue;
+                float nnx = cur.x + sig_n * gauss3(seed);
+                float nny = cur.y + sig_n * gauss3(seed);
+                float nnz = cur.z + sig_n * gauss3(seed);
+                const float len = sqrtf(nnx * nnx + nny * nny + nnz * nnz);
+                if (len < 1e-6f) continue;
+                nnx = nnx / len;
+                nny = nny / len;
+                nnz = nnz / len;
+                const float a_here = nnx * ri.x + nny * ri.y + nnz;
+                if (a_here < 0.1f) continue;
+                sm.rnd[p * 3 + r] = make_float4(nnx, nny, nnz, zcand * a_here);
+                mask |= 16u << r;
+            }
+            next.nz[i] = cur;  // nothing accepted (stereo.rs:278)
+            next.cost[i] = cur_cost;
+            if (skip_dup) next.d[i] = cur_d;
+            if (next.flag) next.flag[i] = 0;
+            sm.pix[p] = (uint32_t)lx | (uint32_t)ly << 8 | mask << 16;
+            sm.pcost[p] = cur_cost;
+        }
+        __syncthreads();
+
+        // ---- phase 2: stream the prepared pixels through the lanes
+        int p = -1, cell0 = 0, si = 0, dy = 0;
+        unsigned cm = 0;  // the pixel's candidates not yet started
+        bool live = false, done = false;
+        float cur_cost = 0.f, best_c = 0.f, bn0 = 0.f, bn1 = 0.f, bn2 = 0.f, bd = 0.f;
+        float nx = 0.f, ny = 0.f, nz = 0.f, d = 0.f, sum = 0.f, thr = 0.f, rej = INFINITY;
+        for (;;) {
+            const bool need = !live && !done && cm == 0;
+            const unsigned m = __ballot_sync(0xffffffffu, need);
+            if (m) {
+                if (need && p >= 0 && best_c < cur_cost) {  // stereo.rs:355-367
+                    const float2 ri = sm.ray[cell0 + HALO * stw + HALO];
+                    const float a_here = bn0 * ri.x + bn1 * ri.y + bn2;
+                    const int lx = cell0 % stw, ly = cell0 / stw;
+                    const size_t i = base + (size_t)(y0 + ly) * w + x0 + lx;
+                    if (a_here > 0.05f) {
+                        next.nz[i] = make_float4(bn0, bn1, bn2, bd / a_here);
+                        next.cost[i] = fminf(best_c, 1.0f);
+                        if (skip_dup) next.d[i] = bd;
+                        if (next.flag) next.flag[i] = 1;
+                    } else if (next.flag) {
+                        next.flag[i] = 2;
+                    }
+                }
+                // lanes claiming together take consecutive pixels
+                const int leader = __ffs(m) - 1;
+                int b0 = 0;
+                if (lane == leader) b0 = atomicAdd(&s_next, __popc(m));
+                b0 = __shfl_sync(0xffffffffu, b0, leader);
+                if (need) {
+                    p = b0 + __popc(m & ((1u << lane) - 1u));
+                    if (p >= np) {
+                        done = true;
+                    } else {
+                        const uint32_t pk = sm.pix[p];
+                        cell0 = (int)((pk >> 8) & 255u) * stw + (int)(pk & 255u);
+                        cm = pk >> 16;
+                        cur_cost = sm.pcost[p];
+                        best_c = cur_cost;
+                    }
+                }
+            }
+            if (!live && cm != 0) {  // the pixel's next candidate, in pass_kernel's order
+                const int q = __ffs(cm) - 1;
+                cm &= cm - 1;
+                if (q < 4) {
+                    const int ddx = q == 0 ? -1 : (q == 1 ? 1 : 0);
+                    const int ddy = q == 2 ? -1 : (q == 3 ? 1 : 0);
+                    const int lx = cell0 % stw, ly = cell0 / stw;
+                    const float4 nb = prev.nz[base + (size_t)(y0 + ly + ddy) * w + x0 + lx + ddx];
+                    const float2 rj = sm.ray[cell0 + (HALO + ddy) * stw + HALO + ddx];
+                    nx = nb.x;
+                    ny = nb.y;
+                    nz = nb.z;
+                    d = nb.w * (nb.x * rj.x + nb.y * rj.y + nb.z);
+                } else {
+                    const float4 c = sm.rnd[p * 3 + (q - 4)];
+                    nx = c.x;
+                    ny = c.y;
+                    nz = c.z;
+                    d = c.w;
+                }
+                sum = 0.f;
+                si = 0;
+                dy = 0;
+                thr = (best_c + 0.02f) + 0.12f;
+                rej = skip_dup ? reject_bound(best_c, total) : INFINITY;
+                live = nsrc > 0;  // with no support view the cost is 0/0, never accepted
+                if (COUNT) wc.evals++;
+            }
+            if (__all_sync(0xffffffffu, done)) break;
+            if (live) {
+                const SrcRegs s = load_src_fm(sm, si);
+                int32_t hs = 0;
+                sum = cost_row<false, false>(rs, cell0 + dy * stw, s, nx, ny, nz, d, sum, hs);
+                if (COUNT) wc.rows++;
+                const bool aborted = sum / abort_den(dy, si, nsrc, skip_dup) > thr || sum >= rej;
+                if (aborted || (si == nsrc - 1 && dy == 4)) {
+                    const float c = aborted ? 1e9f : sum / total;
+                    if (c < best_c) {
+                        best_c = c;
+                        bn0 = nx;
+                        bn1 = ny;
+                        bn2 = nz;
+                        bd = d;
+                    }
+                    live = false;
+                } else if (++dy == 5) {
+                    dy = 0;
+                    ++si;
+                }
+            }
+        }
+    }
+    if (COUNT) flush_work(wc, d_work);
+}
+
 // ---------------------------------------------------------------- split passes
 // The same pass with five lanes per pixel (threads per pixel = 5, an
 // autotuner axis): lane j of a pixel's group computes window column dx = j of
@@ -1297,6 +1607,14 @@ size_t stereo_smem_bytes(TileShape ts) { return smem_bytes(ts.tw, ts.th); }
 // Threads of a split-pass block for tiles of up to `px` pixels.
 int split_threads(int px) { return 32 * ((px + SPLIT_PX - 1) / SPLIT_PX); }
 
+int stream_tiles(int w, int h) { return ((w + STREAM_TW - 1) / STREAM_TW) * ((h + STREAM_TH - 1) / STREAM_TH); }
+
+LaunchGeom stream_geom(int tiles) {
+    LaunchGeom g{STREAM_THREADS, stream_smem_bytes(), tiles, nullptr};
+    g.stream = true;
+    return g;
+}
+
 namespace {
 // Blocks of a persistent launch: as many as stay resident on all SMs at
 // once (the queue hands out the tiles), never more than there are tiles.
@@ -1337,6 +1655,13 @@ template <bool COUNT, bool PERSIST>
 void pass_as(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, const LaunchGeom& g, uint64_t pass,
              float sig_inv, float sig_n, const uint64_t* census, const float2* rays, PlaneBuf prev, PlaneBuf next,
              unsigned long long* d_work, cudaStream_t st) {
+    if (g.stream) {
+        pass_stream_kernel<COUNT, PERSIST><<<launch_grid(pass_stream_kernel<COUNT, PERSIST>, g), STREAM_THREADS,
+                                             stream_smem_bytes(), st>>>(d_jobs, d_job_start, n_jobs, g.tiles, g.queue,
+                                                                        pass, sig_inv, sig_n, census, rays, prev, next,
+                                                                        d_work);
+        return;
+    }
     if (g.tpp == SPLIT) {
         LaunchGeom gs = g;
         gs.nthr = split_threads(g.nthr);

@@ -23,6 +23,7 @@ FLAG_INIT_ONLY = 32     # diagnostic: init and gate only, no passes
 FLAG_SEED_AND_SWEEP = 64  # learned init: seeded pixels also run the plane sweep
 FLAG_ROW_STEP_INIT = 128  # row-step plane sweep instead of the default table sweep
 FLAG_NO_REPEAT_SKIP = 256  # evaluate unchanged neighbours' planes again (the repeat skip off)
+FLAG_LOCKSTEP_PASSES = 512  # passes one thread per pixel in lockstep (not streamed)
 FLAGS_BATCHED = FLAG_PERSISTENT | FLAG_CUDA_GRAPH | FLAG_AUTOTUNE
 
 

@@ -7,7 +7,7 @@ import pytest
 
 from oracle import oracle
 from rustcolmap_b200 import MvsOptions, learned, mvs, scene
-from rustcolmap_b200.types import FLAG_AUTOTUNE, FLAG_CUDA_GRAPH, FLAG_PERSISTENT
+from rustcolmap_b200.types import FLAG_AUTOTUNE, FLAG_CUDA_GRAPH, FLAG_LOCKSTEP_PASSES, FLAG_PERSISTENT
 
 pytestmark = pytest.mark.gpu
 
@@ -42,7 +42,8 @@ def _check(ds, jobs, ref, what):
 
 
 @pytest.mark.parametrize("flags", [0, FLAG_PERSISTENT, FLAG_CUDA_GRAPH, FLAG_PERSISTENT | FLAG_CUDA_GRAPH, 128,
-                                   128 | FLAG_PERSISTENT | FLAG_CUDA_GRAPH])
+                                   128 | FLAG_PERSISTENT | FLAG_CUDA_GRAPH, FLAG_LOCKSTEP_PASSES,
+                                   FLAG_LOCKSTEP_PASSES | FLAG_PERSISTENT | FLAG_CUDA_GRAPH])
 def test_schedules_match_oracle(uneven, flags):
     sc, opts, jobs, ref = uneven
     ctx = mvs.Context(0)
@@ -188,8 +189,9 @@ def test_split_passes_match_oracle(uneven, tile, flags):
 
 
 def test_split_passes_count_the_same_work(uneven):
-    """The work counters (plane_cost calls and 5-term rows) of the split
-    passes equal those of one thread per pixel, with and without the
+    """The work counters (plane_cost calls and 5-term rows) of the streamed
+    passes (the default), the lockstep passes (one thread per pixel) and the
+    split passes (five lanes per pixel) are equal, with and without the
     duplicate skip."""
     import os
     sc, opts, jobs, ref = uneven
@@ -201,11 +203,11 @@ def test_split_passes_count_the_same_work(uneven):
     ds = mvs.DeviceScene(sc.views, ctx)
     for flags in (0, 16):
         got = []
-        for tpp in (1, 5):
-            ds.estimate(jobs, MvsOptions(**{**opts.__dict__, "flags": flags, "threads_per_pixel": tpp}))
+        for tpp, extra in ((1, 0), (1, FLAG_LOCKSTEP_PASSES), (5, 0)):
+            ds.estimate(jobs, MvsOptions(**{**opts.__dict__, "flags": flags | extra, "threads_per_pixel": tpp}))
             got.append(ctx.last_work())
-            _check(ds, jobs, ref, f"tpp {tpp}")
-        assert got[0] == got[1] and got[0][0] > 0
+            _check(ds, jobs, ref, f"tpp {tpp} flags {flags | extra}")
+        assert got[0] == got[1] == got[2] and got[0][0] > 0
     ds.close()
     ctx.close()
 

@@ -8,6 +8,7 @@ import pytest
 from conftest import golden_views
 from oracle import oracle
 from rustcolmap_b200 import MvsOptions, mvs, scene
+from rustcolmap_b200.types import FLAG_LOCKSTEP_PASSES
 
 pytestmark = pytest.mark.gpu
 
@@ -134,6 +135,20 @@ def test_estimate_depth_edge_cases(ctx, w, h, srcs, nh, sweeps, tile):
     assert_bits_equal(dm.normal, n, "normal")
     if not srcs:
         assert (dm.depth == 0).all() and (dm.cost == 1).all()
+
+
+@pytest.mark.parametrize("flags", [0, FLAG_LOCKSTEP_PASSES])
+def test_max_support_views_bit_exact(ctx, flags):
+    """RCMVS_MAX_SOURCES (32) support views: every slot of the streamed
+    passes' per-view parameter table is used (and the lockstep kernel's)."""
+    sc = scene.orbit_room(seed=33, n_views=33, sizes=((40, 30),), n_boxes=4, per_view_sparse=40, arc_deg=60.0)
+    opts = MvsOptions(max_dim=4096, num_hyp=6, sweeps=1, flags=flags)
+    srcs = list(range(1, 33))
+    dm = mvs.estimate_depth(sc.views, 0, srcs, 1.0, 11.0, opts, ctx, normals=True)
+    d, c, n, _ = oracle.estimate_depth(sc.views, 0, srcs, 1.0, 11.0, opts)
+    assert_bits_equal(dm.depth, d, "depth")
+    assert_bits_equal(dm.cost, c, "cost")
+    assert_bits_equal(dm.normal, n, "normal")
 
 
 def test_tile_shape_does_not_change_bits(ctx, corner_scene):
