@@ -68,16 +68,17 @@ typedef struct rcmvs_options {
     uint32_t tile_h;         /* stereo tile height in pixels; 0 = default (8) */
     uint32_t flags;          /* RCMVS_FLAG_* bits; 0 = defaults */
     uint32_t threads_per_pixel; /* Jacobi passes: 0 or 1 = one thread per pixel
-                                (default); 5 = five lanes per pixel, one per
-                                window column (tiles of at most 128 pixels).
-                                Same results bit for bit. */
+                                (default: streamed, see
+                                RCMVS_FLAG_LOCKSTEP_PASSES); 5 = five lanes per
+                                pixel, one per window column (tiles of at most
+                                128 pixels).  Same results bit for bit. */
 } rcmvs_options;
 
 /* The plane-sweep init evaluates each pixel's hypotheses one at a time, a
  * warp waiting at every hypothesis for its slowest lane, instead of the
  * default table sweep (RCMVS_FLAG_ROW_STEP_INIT).  Same results bit for
- * bit; kept for comparison.  The pass kernel always works one candidate at a time, which
- * keeps a warp's source-census gathers on one support view. */
+ * bit; kept for comparison.  The Jacobi passes are chosen by
+ * threads_per_pixel and RCMVS_FLAG_LOCKSTEP_PASSES. */
 #define RCMVS_FLAG_ONE_CANDIDATE 1u
 
 /* Persistent (view, tile) work queue: each init/pass launch runs as many
@@ -149,7 +150,7 @@ typedef struct rcmvs_options {
 /* The Jacobi passes run one thread per pixel in lockstep (tiles of
  * tile_w x tile_h): a warp runs each candidate slot for as long as its
  * slowest lane needs.  By default (threads_per_pixel 0 or 1) a pass
- * streams the pixels of 16x16 tiles through blocks of 64 threads: each
+ * streams the pixels of 16x16 tiles through blocks of 128 threads: each
  * lane evaluates its pixel's candidates one window row at a time, starts
  * the next candidate as soon as one ends and claims the tile's next pixel
  * as soon as its pixel ends.  Same results bit for bit (and the same work

@@ -551,7 +551,7 @@ __global__ void __maxnreg__(72)
 // In pass_kernel a warp holds every candidate slot for as long as its
 // slowest lane needs: most evaluations abort after a window row or two while
 // a good candidate runs all 5*K rows, so most lanes wait.  Here a block of
-// STREAM_THREADS threads owns a STREAM_TW x STREAM_TH tile (four pixels per
+// STREAM_THREADS threads owns a STREAM_TW x STREAM_TH tile (two pixels per
 // thread) and works in two phases:
 //   1. preparation, one thread per pixel: the pixel's stored plane and cost,
 //      the neighbour candidates that pass the gates and the skip rules
@@ -571,9 +571,23 @@ __global__ void __maxnreg__(72)
 // in shared memory (field f of view s at f * RCMVS_MAX_SOURCES + s), so lanes
 // on different views read different banks and lanes on the same view read
 // one broadcast word.
-constexpr int STREAM_TW = 16, STREAM_TH = 16;
+// Tile, block and register budget of the streamed passes (build-time
+// settings).  Measured on the 1920x1080 K=10 workload (learned arm, depth
+// maps/s): 16x16 tiles in blocks of 128 threads at 64 registers (8 blocks,
+// 32 warps per SM) 80.0; the same at 76 registers 74.5 (6 blocks), at 56 or
+// 48 registers 75.0 / 60.9 (spills); blocks of 64 threads 71.9 (shared
+// memory holds an SM to 9 blocks); 256 threads (one pixel per thread)
+// 63.8; 32x16 tiles / 128 threads 74.5, / 256 threads 75.6; 16x8 / 32 65.2.
+#ifndef RCMVS_STREAM_TW
+#define RCMVS_STREAM_TW 16
+#define RCMVS_STREAM_TH 16
+#define RCMVS_STREAM_THREADS 128
+#define RCMVS_STREAM_MINB 8
+#endif
+constexpr int STREAM_TW = RCMVS_STREAM_TW, STREAM_TH = RCMVS_STREAM_TH;
 constexpr int STREAM_PX = STREAM_TW * STREAM_TH;
-constexpr int STREAM_THREADS = 64;
+constexpr int STREAM_THREADS = RCMVS_STREAM_THREADS;
+static_assert(STREAM_THREADS % 32 == 0 && STREAM_TW <= 256 && STREAM_TH <= 256, "stream tile");
 constexpr int STREAM_CELLS = (STREAM_TW + 2 * HALO) * (STREAM_TH + 2 * HALO);
 constexpr int SF_N = 19;  // rs[9], ts[3], f, cx, cy, k, (float)w, (float)h, w (int bits)
 
@@ -636,7 +650,10 @@ __device__ __forceinline__ SrcRegs load_src_fm(const StreamSmem& sm, int si) {
 }
 
 template <bool COUNT, bool PERSIST>
-__global__ void __launch_bounds__(STREAM_THREADS, 8)
+#ifndef RCMVS_STREAM_MINB
+#define RCMVS_STREAM_MINB (512 / RCMVS_STREAM_THREADS)
+#endif
+__global__ void __launch_bounds__(STREAM_THREADS, RCMVS_STREAM_MINB)
     pass_stream_kernel(const DevJob* __restrict__ jobs, const int32_t* __restrict__ stile_start, int n_jobs, int tiles,
                        unsigned int* queue, uint64_t pass, float sig_inv, float sig_n,
                        const uint64_t* __restrict__ census, const float2* __restrict__ rays, PlaneBuf prev,
