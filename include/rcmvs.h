@@ -150,12 +150,14 @@ typedef struct rcmvs_options {
 /* The Jacobi passes run one thread per pixel in lockstep (tiles of
  * tile_w x tile_h): a warp runs each candidate slot for as long as its
  * slowest lane needs.  By default (threads_per_pixel 0 or 1) a pass
- * streams the pixels of 16x16 tiles through blocks of 128 threads: each
+ * streams the pixels of 16x16 tiles through blocks of 64 threads: each
  * lane evaluates its pixel's candidates one window row at a time, starts
  * the next candidate as soon as one ends and claims the tile's next pixel
- * as soon as its pixel ends.  Same results bit for bit (and the same work
- * counters); tile_w/tile_h and the autotuner's shapes then apply to the
- * init only. */
+ * as soon as its pixel ends.  The streamed passes run as persistent
+ * launches and keep each block's random candidates in a device scratch of
+ * the scene (48 bytes per tile pixel per resident block, about 29 MB on a
+ * 148-SM GPU).  Same results bit for bit (and the same work counters);
+ * tile_w/tile_h and the autotuner's shapes then apply to the init only. */
 #define RCMVS_FLAG_LOCKSTEP_PASSES 512u
 
 #define RCMVS_MAX_PASSES 4096u

@@ -153,7 +153,7 @@ namespace rcmvs {
 // private to capi.cu 2-10, fuse.cu 16-37 and 70-74, learned_api.cu 40-47, depthvis.cu 50-55,
 // resize.cu 60-68, sift.cu 80-159 and match.cu 160-167).
 constexpr int kSlotJobs = 0, kSlotJobStart = 1, kSlotQueue = 11, kSlotTuneJobs = 12, kSlotTuneStart = 13,
-              kSlotStreamStart = 14;
+              kSlotStreamStart = 14, kSlotStreamScratch = 15;
 
 // resize.cu: argument and size checks of a resize, and the resize itself
 // on device buffers (d_gray mw*mh, d_rgb mw*mh*3), queued on the context's

@@ -82,11 +82,18 @@ struct LaunchGeom {
     unsigned int* queue;
     int tpp = 1;  // threads per pixel of the passes: 1, or 5 (pass_split_kernel)
     bool stream = false;  // passes: pass_stream_kernel over the stream tiling (stream_geom)
+    float4* scratch = nullptr;  // streamed passes: per-block scratch (stream_scratch_bytes)
+    int scratch_blocks = 0;     // blocks the scratch holds (the launch uses at most this many)
 };
 // Streamed passes (pass_stream_kernel): tiles of a w x h view in the
 // kernel's own tiling, and the geometry of a launch over `tiles` of them.
+// The launch is always persistent (g.queue set) over at most
+// stream_grid(g) blocks, each with its own slice of a device scratch of
+// stream_scratch_bytes(blocks) bytes (its pixels' random candidates).
 int stream_tiles(int w, int h);
 LaunchGeom stream_geom(int tiles);
+int stream_grid(const LaunchGeom& g);
+size_t stream_scratch_bytes(int blocks);
 // Threads of a split-pass block (5 lanes per pixel, 6 pixels per warp) for
 // tiles of up to px pixels.
 int split_threads(int px);

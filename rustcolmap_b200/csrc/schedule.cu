@@ -332,14 +332,20 @@ int run_batch(rcmvs_ctx* ctx, rcmvs_scene* sc, const StereoBatch& b, const Sched
     SCK(sc->arena.get(kSlotJobs, sizeof(DevJob) * n_jobs, &pj));
     SCK(sc->arena.get(kSlotJobStart, sizeof(int32_t) * (n_jobs + 1), &ps));
     const int n_launch = 1 + (int)s.n_passes;
-    if (s.persistent) SCK(sc->arena.get(kSlotQueue, sizeof(unsigned int) * n_launch, &pq));
+    // the streamed passes are always persistent (each block owns a slice of
+    // the scratch), so their launches take queue counters too
+    if (s.persistent || b.stream) SCK(sc->arena.get(kSlotQueue, sizeof(unsigned int) * n_launch, &pq));
     // pageable -> device copies return once the host data has been staged
     SCK(cudaMemcpyAsync(pj, b.jobs.data(), sizeof(DevJob) * n_jobs, cudaMemcpyHostToDevice, st));
     SCK(cudaMemcpyAsync(ps, b.start.data(), sizeof(int32_t) * (n_jobs + 1), cudaMemcpyHostToDevice, st));
-    void* pss = nullptr;
+    void *pss = nullptr, *pscr = nullptr;
+    LaunchGeom sgeom = b.sgeom;
     if (b.stream) {
         SCK(sc->arena.get(kSlotStreamStart, sizeof(int32_t) * (n_jobs + 1), &pss));
         SCK(cudaMemcpyAsync(pss, b.sstart.data(), sizeof(int32_t) * (n_jobs + 1), cudaMemcpyHostToDevice, st));
+        sgeom.scratch_blocks = std::min(stream_grid(sgeom), sgeom.tiles);
+        SCK(sc->arena.get(kSlotStreamScratch, stream_scratch_bytes(sgeom.scratch_blocks), &pscr));
+        sgeom.scratch = (float4*)pscr;
     }
     const DevJob* dj = (const DevJob*)pj;
     const int32_t* dst = (const int32_t*)ps;
@@ -368,7 +374,7 @@ int run_batch(rcmvs_ctx* ctx, rcmvs_scene* sc, const StereoBatch& b, const Sched
             (e = cudaMemsetAsync(s.d_learned, 0, sizeof(unsigned long long), st)))
             return e;
         PlaneBuf A = A0, B = B0;
-        g.queue = queue;
+        g.queue = s.persistent ? queue : nullptr;
         hk.begin(s.init == Schedule::LEARNED ? "learned_init" : "stereo_init");
         if (s.init == Schedule::LEARNED)
             e = launch_init_learned(dj, dst, n_jobs, g, s.nh, sc->census, sc->rays, A, s.pred, s.pred_off,
@@ -378,7 +384,7 @@ int run_batch(rcmvs_ctx* ctx, rcmvs_scene* sc, const StereoBatch& b, const Sched
                             s.init == Schedule::ONE_CANDIDATE ? 1 : (s.init == Schedule::TABLE ? 2 : 0));
         hk.end(s.init == Schedule::LEARNED ? "learned_init" : "stereo_init");
         if (e) return e;
-        LaunchGeom gp = b.stream ? b.sgeom : b.geom;
+        LaunchGeom gp = b.stream ? sgeom : b.geom;
         for (uint64_t pass = 0; pass < s.n_passes; ++pass) {
             gp.queue = queue ? queue + 1 + pass : nullptr;
             hk.begin("stereo_pass");
@@ -410,6 +416,7 @@ int run_batch(rcmvs_ctx* ctx, rcmvs_scene* sc, const StereoBatch& b, const Sched
     append(key, b.geom.tpp);
     append(key, b.stream);
     append(key, b.sstart.data(), sizeof(int32_t) * (n_jobs + 1));
+    append(key, sgeom.scratch_blocks);
     append(key, (int)s.init);
     append(key, s.nh);
     append(key, s.n_passes);
@@ -418,7 +425,7 @@ int run_batch(rcmvs_ctx* ctx, rcmvs_scene* sc, const StereoBatch& b, const Sched
     append(key, s.n_local);
     append(key, s.span);
     append(key, s.sweep_seeded);
-    const void* ptrs[] = {pj, ps, pss, pq, s.d_work, s.pred, s.pred_off, s.d_learned, sc->census, sc->rays,
+    const void* ptrs[] = {pj, ps, pss, pscr, pq, s.d_work, s.pred, s.pred_off, s.d_learned, sc->census, sc->rays,
                           sc->plane_a, sc->plane_b, sc->pcost_a, sc->pcost_b, A0.d, B0.d, A0.flag, B0.flag,
                           sc->depth, sc->cost, sc->normal};
     append(key, ptrs, sizeof(ptrs));

@@ -551,16 +551,19 @@ __global__ void __maxnreg__(72)
 // In pass_kernel a warp holds every candidate slot for as long as its
 // slowest lane needs: most evaluations abort after a window row or two while
 // a good candidate runs all 5*K rows, so most lanes wait.  Here a block of
-// STREAM_THREADS threads owns a STREAM_TW x STREAM_TH tile (two pixels per
+// STREAM_THREADS threads owns a STREAM_TW x STREAM_TH tile (four pixels per
 // thread) and works in two phases:
 //   1. preparation, one thread per pixel: the pixel's stored plane and cost,
 //      the neighbour candidates that pass the gates and the skip rules
 //      (stereo.rs:292-321), and its three random perturbations drawn from
 //      the pixel's RNG (stereo.rs:323-353).  The perturbations depend on the
 //      stored plane alone, never on a cost, so drawing them ahead of the
-//      evaluations gives the same planes.  The pass's output for a pixel
-//      that accepts nothing (the carried-over plane, stereo.rs:278) is
-//      written here.
+//      evaluations gives the same planes.  They go to the block's slice of
+//      a device scratch (48 bytes per tile pixel; the launch is persistent,
+//      so a block's slice serves every tile it takes), which keeps shared
+//      memory to the halo tile and lets 16 blocks share an SM.  The pass's
+//      output for a pixel that accepts nothing (the carried-over plane,
+//      stereo.rs:278) is written here.
 //   2. evaluation: every lane advances its own candidate by one window row
 //      per loop iteration; a lane whose candidate ends starts the pixel's
 //      next one, and a lane whose pixel ends writes it (if a candidate beat
@@ -571,18 +574,20 @@ __global__ void __maxnreg__(72)
 // in shared memory (field f of view s at f * RCMVS_MAX_SOURCES + s), so lanes
 // on different views read different banks and lanes on the same view read
 // one broadcast word.
+//
 // Tile, block and register budget of the streamed passes (build-time
 // settings).  Measured on the 1920x1080 K=10 workload (learned arm, depth
-// maps/s): 16x16 tiles in blocks of 128 threads at 64 registers (8 blocks,
-// 32 warps per SM) 80.0; the same at 76 registers 74.5 (6 blocks), at 56 or
-// 48 registers 75.0 / 60.9 (spills); blocks of 64 threads 71.9 (shared
-// memory holds an SM to 9 blocks); 256 threads (one pixel per thread)
-// 63.8; 32x16 tiles / 128 threads 74.5, / 256 threads 75.6; 16x8 / 32 65.2.
+// maps/s): 16x16 tiles in blocks of 64 threads at 64 registers (4 pixels per
+// thread, 16 blocks = 32 warps per SM) 93.9; 32x16 / 128 threads 91.3;
+// 32x32 / 128 (8 pixels per thread, 7 blocks, spills) 88.6; 16x16 / 128
+// (2 pixels per thread) 80.4; 32x16 / 256 76.2.  With the random candidates
+// in shared memory instead of the global scratch (24 KB per block) the best
+// was 16x16 / 128 at 80.0 and 16x16 / 64 reached 71.9 (9 blocks per SM).
 #ifndef RCMVS_STREAM_TW
 #define RCMVS_STREAM_TW 16
 #define RCMVS_STREAM_TH 16
-#define RCMVS_STREAM_THREADS 128
-#define RCMVS_STREAM_MINB 8
+#define RCMVS_STREAM_THREADS 64
+#define RCMVS_STREAM_MINB 16
 #endif
 constexpr int STREAM_TW = RCMVS_STREAM_TW, STREAM_TH = RCMVS_STREAM_TH;
 constexpr int STREAM_PX = STREAM_TW * STREAM_TH;
@@ -592,7 +597,6 @@ constexpr int STREAM_CELLS = (STREAM_TW + 2 * HALO) * (STREAM_TH + 2 * HALO);
 constexpr int SF_N = 19;  // rs[9], ts[3], f, cx, cy, k, (float)w, (float)h, w (int bits)
 
 struct StreamSmem {
-    float4* rnd;        // [STREAM_PX][3] random candidates (n, d)
     uint64_t* cen;      // halo tile
     float2* ray;        // halo tile
     const uint64_t** scp;  // [RCMVS_MAX_SOURCES] census of each support view
@@ -603,15 +607,14 @@ struct StreamSmem {
 };
 
 __host__ __device__ constexpr size_t stream_smem_bytes() {
-    return sizeof(float4) * STREAM_PX * 3 + (sizeof(uint64_t) + sizeof(float2)) * STREAM_CELLS +
+    return (sizeof(uint64_t) + sizeof(float2)) * STREAM_CELLS +
            sizeof(uint64_t*) * RCMVS_MAX_SOURCES + sizeof(float) * SF_N * RCMVS_MAX_SOURCES + 64 * sizeof(float) +
            (sizeof(uint32_t) + sizeof(float)) * STREAM_PX;
 }
 
 __device__ __forceinline__ StreamSmem carve_stream(unsigned char* base) {
     StreamSmem s;
-    s.rnd = reinterpret_cast<float4*>(base);
-    s.cen = reinterpret_cast<uint64_t*>(s.rnd + STREAM_PX * 3);
+    s.cen = reinterpret_cast<uint64_t*>(base);
     s.ray = reinterpret_cast<float2*>(s.cen + STREAM_CELLS);
     s.scp = reinterpret_cast<const uint64_t**>(s.ray + STREAM_CELLS);
     s.sf = reinterpret_cast<float*>(s.scp + RCMVS_MAX_SOURCES);
@@ -657,10 +660,12 @@ __global__ void __launch_bounds__(STREAM_THREADS, RCMVS_STREAM_MINB)
     pass_stream_kernel(const DevJob* __restrict__ jobs, const int32_t* __restrict__ stile_start, int n_jobs, int tiles,
                        unsigned int* queue, uint64_t pass, float sig_inv, float sig_n,
                        const uint64_t* __restrict__ census, const float2* __restrict__ rays, PlaneBuf prev,
-                       PlaneBuf next, unsigned long long* d_work) {
+                       PlaneBuf next, float4* __restrict__ scratch, unsigned long long* d_work) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int s_tile, s_next;
     const StreamSmem sm = carve_stream(smem_raw);
+    // this block's slice of the random-candidate scratch: [STREAM_PX][3]
+    const size_t rnd0 = (size_t)blockIdx.x * STREAM_PX * 3;
     const Smem rs{nullptr, sm.tab, sm.ray, sm.cen};  // the view cost_row reads
     constexpr int stw = STREAM_TW + 2 * HALO;
     const bool skip_dup = prev.d != nullptr;
@@ -764,7 +769,7 @@ __global__ void __launch_bounds__(STREAM_THREADS, RCMVS_STREAM_MINB)
                 nnz = nnz / len;
                 const float a_here = nnx * ri.x + nny * ri.y + nnz;
                 if (a_here < 0.1f) continue;
-                sm.rnd[p * 3 + r] = make_float4(nnx, nny, nnz, zcand * a_here);
+                scratch[rnd0 + p * 3 + r] = make_float4(nnx, nny, nnz, zcand * a_here);
                 mask |= 16u << r;
             }
             next.nz[i] = cur;  // nothing accepted (stereo.rs:278)
@@ -780,17 +785,18 @@ __global__ void __launch_bounds__(STREAM_THREADS, RCMVS_STREAM_MINB)
         int p = -1, cell0 = 0, si = 0, dy = 0;
         unsigned cm = 0;  // the pixel's candidates not yet started
         bool live = false, done = false;
-        float cur_cost = 0.f, best_c = 0.f, bn0 = 0.f, bn1 = 0.f, bn2 = 0.f, bd = 0.f;
+        const size_t tb = base + (size_t)y0 * w + x0;  // the tile's first pixel
+        float best_c = 0.f, bn0 = 0.f, bn1 = 0.f, bn2 = 0.f, bd = 0.f;
         float nx = 0.f, ny = 0.f, nz = 0.f, d = 0.f, sum = 0.f, thr = 0.f, rej = INFINITY;
         for (;;) {
             const bool need = !live && !done && cm == 0;
             const unsigned m = __ballot_sync(0xffffffffu, need);
             if (m) {
-                if (need && p >= 0 && best_c < cur_cost) {  // stereo.rs:355-367
+                if (need && p >= 0 && best_c < sm.pcost[p]) {  // stereo.rs:355-367
                     const float2 ri = sm.ray[cell0 + HALO * stw + HALO];
                     const float a_here = bn0 * ri.x + bn1 * ri.y + bn2;
                     const int lx = cell0 % stw, ly = cell0 / stw;
-                    const size_t i = base + (size_t)(y0 + ly) * w + x0 + lx;
+                    const size_t i = tb + (size_t)ly * w + lx;
                     if (a_here > 0.05f) {
                         next.nz[i] = make_float4(bn0, bn1, bn2, bd / a_here);
                         next.cost[i] = fminf(best_c, 1.0f);
@@ -813,8 +819,7 @@ __global__ void __launch_bounds__(STREAM_THREADS, RCMVS_STREAM_MINB)
                         const uint32_t pk = sm.pix[p];
                         cell0 = (int)((pk >> 8) & 255u) * stw + (int)(pk & 255u);
                         cm = pk >> 16;
-                        cur_cost = sm.pcost[p];
-                        best_c = cur_cost;
+                        best_c = sm.pcost[p];
                     }
                 }
             }
@@ -825,14 +830,14 @@ __global__ void __launch_bounds__(STREAM_THREADS, RCMVS_STREAM_MINB)
                     const int ddx = q == 0 ? -1 : (q == 1 ? 1 : 0);
                     const int ddy = q == 2 ? -1 : (q == 3 ? 1 : 0);
                     const int lx = cell0 % stw, ly = cell0 / stw;
-                    const float4 nb = prev.nz[base + (size_t)(y0 + ly + ddy) * w + x0 + lx + ddx];
+                    const float4 nb = prev.nz[tb + (ptrdiff_t)(ly + ddy) * w + lx + ddx];
                     const float2 rj = sm.ray[cell0 + (HALO + ddy) * stw + HALO + ddx];
                     nx = nb.x;
                     ny = nb.y;
                     nz = nb.z;
                     d = nb.w * (nb.x * rj.x + nb.y * rj.y + nb.z);
                 } else {
-                    const float4 c = sm.rnd[p * 3 + (q - 4)];
+                    const float4 c = scratch[(size_t)blockIdx.x * STREAM_PX * 3 + p * 3 + (q - 4)];
                     nx = c.x;
                     ny = c.y;
                     nz = c.z;
@@ -1632,6 +1637,9 @@ LaunchGeom stream_geom(int tiles) {
     return g;
 }
 
+
+size_t stream_scratch_bytes(int blocks) { return sizeof(float4) * STREAM_PX * 3 * (size_t)blocks; }
+
 namespace {
 // Blocks of a persistent launch: as many as stay resident on all SMs at
 // once (the queue hands out the tiles), never more than there are tiles.
@@ -1651,6 +1659,12 @@ int launch_grid(K kernel, const LaunchGeom& g) {
 }  // namespace
 
 int stereo_resident_grid(const LaunchGeom& g) { return launch_grid(pass_kernel<false, 3, true>, g); }
+int stream_grid(const LaunchGeom& g) {
+    LaunchGeom q = g;
+    unsigned int dummy = 0;
+    q.queue = &dummy;  // any non-null queue: the resident grid
+    return std::max(launch_grid(pass_stream_kernel<false, true>, q), 1);
+}
 
 namespace {
 template <bool COUNT, bool PERSIST>
@@ -1672,11 +1686,12 @@ template <bool COUNT, bool PERSIST>
 void pass_as(const DevJob* d_jobs, const int32_t* d_job_start, int n_jobs, const LaunchGeom& g, uint64_t pass,
              float sig_inv, float sig_n, const uint64_t* census, const float2* rays, PlaneBuf prev, PlaneBuf next,
              unsigned long long* d_work, cudaStream_t st) {
-    if (g.stream) {
-        pass_stream_kernel<COUNT, PERSIST><<<launch_grid(pass_stream_kernel<COUNT, PERSIST>, g), STREAM_THREADS,
-                                             stream_smem_bytes(), st>>>(d_jobs, d_job_start, n_jobs, g.tiles, g.queue,
-                                                                        pass, sig_inv, sig_n, census, rays, prev, next,
-                                                                        d_work);
+    if (g.stream) {  // always persistent: block b owns slice b of the scratch
+        if (!PERSIST) return;
+        const int grid = std::min(launch_grid(pass_stream_kernel<COUNT, true>, g), g.scratch_blocks);
+        pass_stream_kernel<COUNT, true><<<grid, STREAM_THREADS, stream_smem_bytes(), st>>>(
+            d_jobs, d_job_start, n_jobs, g.tiles, g.queue, pass, sig_inv, sig_n, census, rays, prev, next, g.scratch,
+            d_work);
         return;
     }
     if (g.tpp == SPLIT) {
@@ -1714,6 +1729,7 @@ cudaError_t launch_pass(const DevJob* d_jobs, const int32_t* d_job_start, int n_
                         uint64_t pass, float sig_inv, float sig_n, const uint64_t* census, const float2* rays,
                         PlaneBuf prev, PlaneBuf next, unsigned long long* d_work, cudaStream_t st) {
     if (g.tiles <= 0) return cudaSuccess;
+    if (g.stream && (!g.queue || !g.scratch || g.scratch_blocks <= 0)) return cudaErrorInvalidValue;
     if (d_work) {
         if (g.queue)
             pass_as<true, true>(d_jobs, d_job_start, n_jobs, g, pass, sig_inv, sig_n, census, rays, prev, next, d_work,
