@@ -46,10 +46,10 @@ sys.path.insert(0, ROOT)
 
 FP32_NOMINAL_TOPS = 148 * 128 * 1.965e9 / 1e12  # SMs x FP32 lanes x max clock (ops/s, no FMA pairing)
 # DRAM bytes (read + write) per reference pixel of one pass launch, from an
-# ncu capture of the pass kernel on 12 views at 1920x1080, K = 10 (pass 6:
-# 1.973 GB read + 0.619 GB written over 24.88 Mpx), scaled to the measured
-# workload's pixels for roofline.traffic.
-PASS_DRAM_BYTES_PER_PX = (1972510000 + 618701312) / (12 * 1920 * 1080)
+# ncu capture of the streamed pass kernel on 12 views at 1920x1080, K = 10
+# (learned arm, pass 2: 2.573 GB read + 1.300 GB written over 24.88 Mpx),
+# scaled to the measured workload's pixels for roofline.traffic.
+PASS_DRAM_BYTES_PER_PX = (2572771000 + 1299575000) / (12 * 1920 * 1080)
 
 
 def configs():
@@ -776,7 +776,7 @@ def main():
                          "unit": "GB/s", "frac": achieved_gbs / hbm_peak,
                          "traffic": PASS_DRAM_BYTES_PER_PX * npx,
                          "traffic_source": "ncu dram bytes per pixel of a 12-view 1920x1080 K=10 capture of "
-                                           "the pass kernel x this launch's pixels",
+                                           "the streamed pass kernel (learned arm) x this launch's pixels",
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650",
                          "algorithmic_bytes_per_launch": bytes_per_launch, "avg_launch_ms": pass_avg_s * 1e3,
                          "note": "issue-bound kernel: see compute_roofline"},

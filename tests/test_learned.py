@@ -431,7 +431,7 @@ def test_seeded_oracle_selects_the_gated_proposals():
 @pytest.mark.gpu
 def test_committed_network_gains_over_the_plain_method(ctx):
     """The committed weights on eight held-out config-4 scenes (seeds
-    6000-6007, outside the training seeds 1000-1399 and the tuning seeds
+    6000-6007, outside the training seeds 1000-1799 and the tuning seeds
     5000-5019; the operating point's precision margin, about 1%, is below
     the scatter of a two-scene mean), at the library's operating point (learned.LEARNED_PASSES
     passes, gate learned.LEARNED_COST_THR) against the plain method with 6
