@@ -604,12 +604,13 @@ struct StreamSmem {
     float* tab;         // 64 (49 used): h / 48.0f
     uint32_t* pix;      // [STREAM_PX]: lx | ly << 8 | candidate bits << 16
     float* pcost;       // [STREAM_PX] stored cost
+    uint16_t* order;    // [STREAM_PX]: the claim order (pixels with candidates, most candidates first)
 };
 
 __host__ __device__ constexpr size_t stream_smem_bytes() {
     return (sizeof(uint64_t) + sizeof(float2)) * STREAM_CELLS +
            sizeof(uint64_t*) * RCMVS_MAX_SOURCES + sizeof(float) * SF_N * RCMVS_MAX_SOURCES + 64 * sizeof(float) +
-           (sizeof(uint32_t) + sizeof(float)) * STREAM_PX;
+           (sizeof(uint32_t) + sizeof(float) + sizeof(uint16_t)) * STREAM_PX;
 }
 
 __device__ __forceinline__ StreamSmem carve_stream(unsigned char* base) {
@@ -621,6 +622,7 @@ __device__ __forceinline__ StreamSmem carve_stream(unsigned char* base) {
     s.tab = s.sf + SF_N * RCMVS_MAX_SOURCES;
     s.pix = reinterpret_cast<uint32_t*>(s.tab + 64);
     s.pcost = reinterpret_cast<float*>(s.pix + STREAM_PX);
+    s.order = reinterpret_cast<uint16_t*>(s.pcost + STREAM_PX);
     return s;
 }
 
@@ -662,7 +664,7 @@ __global__ void __launch_bounds__(STREAM_THREADS, RCMVS_STREAM_MINB)
                        const uint64_t* __restrict__ census, const float2* __restrict__ rays, PlaneBuf prev,
                        PlaneBuf next, float4* __restrict__ scratch, unsigned long long* d_work) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ int s_tile, s_next;
+    __shared__ int s_tile, s_next, s_bin[8];
     const StreamSmem sm = carve_stream(smem_raw);
     // this block's slice of the random-candidate scratch: [STREAM_PX][3]
     const size_t rnd0 = (size_t)blockIdx.x * STREAM_PX * 3;
@@ -711,6 +713,7 @@ __global__ void __launch_bounds__(STREAM_THREADS, RCMVS_STREAM_MINB)
             sm.cen[i] = __ldg(census + g);
         }
         if (threadIdx.x == 0) s_next = 0;
+        if (threadIdx.x < 8) s_bin[threadIdx.x] = 0;
         __syncthreads();
 
         const float total = 5.0f * 5.0f * (float)nsrc;
@@ -778,6 +781,28 @@ __global__ void __launch_bounds__(STREAM_THREADS, RCMVS_STREAM_MINB)
             if (next.flag) next.flag[i] = 0;
             sm.pix[p] = (uint32_t)lx | (uint32_t)ly << 8 | mask << 16;
             sm.pcost[p] = cur_cost;
+            atomicAdd(&s_bin[7 - __popc(mask)], 1);  // at most 7 candidates
+        }
+        __syncthreads();
+
+        // ---- claim order: most candidates first (the longest work starts
+        // early, so a tile's tail is short); pixels without candidates keep
+        // the output written above and are not claimed.  Pixels are
+        // independent, so the order changes no output bit.
+        if (threadIdx.x == 0) {
+            int acc = 0;
+            for (int b = 0; b < 8; ++b) {
+                const int n = s_bin[b];
+                s_bin[b] = acc;
+                acc += n;
+            }
+        }
+        __syncthreads();
+        // s_bin[7] now counts the pixels with at least one candidate (read
+        // at claim time: it stays fixed until the next tile's barrier)
+        for (int p = threadIdx.x; p < np; p += STREAM_THREADS) {
+            const int c = __popc(sm.pix[p] >> 16);
+            if (c) sm.order[atomicAdd(&s_bin[7 - c], 1)] = (uint16_t)p;
         }
         __syncthreads();
 
@@ -812,10 +837,11 @@ __global__ void __launch_bounds__(STREAM_THREADS, RCMVS_STREAM_MINB)
                 if (lane == leader) b0 = atomicAdd(&s_next, __popc(m));
                 b0 = __shfl_sync(0xffffffffu, b0, leader);
                 if (need) {
-                    p = b0 + __popc(m & ((1u << lane) - 1u));
-                    if (p >= np) {
+                    const int b = b0 + __popc(m & ((1u << lane) - 1u));
+                    if (b >= s_bin[7]) {
                         done = true;
                     } else {
+                        p = sm.order[b];
                         const uint32_t pk = sm.pix[p];
                         cell0 = (int)((pk >> 8) & 255u) * stw + (int)(pk & 255u);
                         cm = pk >> 16;
