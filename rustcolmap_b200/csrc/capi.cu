@@ -179,6 +179,10 @@ void rcmvs_ctx_destroy(rcmvs_ctx* ctx) {
     for (rcmvs_scene* sc : ctx->live) sc->ctx = nullptr;
     ctx->clear_spans();
     if (ctx->d_work) cudaFree(ctx->d_work);
+    if (ctx->upload) {
+        cudaStreamSynchronize(ctx->upload);
+        cudaStreamDestroy(ctx->upload);
+    }
     cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -288,7 +292,19 @@ void rcmvs_scene_destroy(rcmvs_scene* sc) {
 
 int rcmvs_scene_prepare(rcmvs_ctx* ctx, rcmvs_scene* sc);
 
+// rcmvs_scene_create; with `rgb_stream` set, the RGB uploads go on that
+// stream instead (after the work already on ctx->stream) and `rgb_done` is
+// recorded after them: the caller makes fusion wait for it and waits for it
+// before the scene is destroyed or the host views may be released.
+static int scene_create(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views, rcmvs_scene** out,
+                        cudaStream_t rgb_stream, cudaEvent_t rgb_done);
+
 int rcmvs_scene_create(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views, rcmvs_scene** out) {
+    return scene_create(ctx, views, n_views, out, nullptr, nullptr);
+}
+
+static int scene_create(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views, rcmvs_scene** out,
+                        cudaStream_t rgb_stream, cudaEvent_t rgb_done) {
     if (!ctx || !views || n_views <= 0 || !out) return fail(ctx, RCMVS_E_ARG, "rcmvs_scene_create: bad argument");
     *out = nullptr;
     for (int i = 0; i < n_views; ++i) {
@@ -371,23 +387,38 @@ int rcmvs_scene_create(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views,
     std::vector<double> cams4;
     for (auto& c : sc->cams) cams4.insert(cams4.end(), {c.f, c.cx, c.cy, c.k});
     cudaStream_t st = ctx->stream;
+    cudaStream_t rst = rgb_stream ? rgb_stream : st;
+    if (rgb_stream) {  // adopted buffers may still be read by work queued on st
+        if (!e) e = cudaEventRecord(rgb_done, st);
+        if (!e) e = cudaStreamWaitEvent(rgb_stream, rgb_done, 0);
+    }
     for (int i = 0; i < n_views && !e; ++i) {
         const size_t n = (size_t)views[i].w * views[i].h;
         e = cudaMemcpyAsync(sc->gray + sc->views[i].off, views[i].gray, n, cudaMemcpyHostToDevice, st);
-        if (!e && sc->has_rgb)
-            e = cudaMemcpyAsync(sc->rgb + 3 * sc->views[i].off, views[i].rgb, 3 * n, cudaMemcpyHostToDevice, st);
     }
+    for (int i = 0; i < n_views && !e && sc->has_rgb; ++i) {
+        const size_t n = (size_t)views[i].w * views[i].h;
+        e = cudaMemcpyAsync(sc->rgb + 3 * sc->views[i].off, views[i].rgb, 3 * n, cudaMemcpyHostToDevice, rst);
+    }
+    if (!e && rgb_stream) e = cudaEventRecord(rgb_done, rgb_stream);
     if (!e) e = cudaMemcpyAsync(sc->d_views, sc->views.data(), sizeof(DevView) * n_views, cudaMemcpyHostToDevice, st);
     if (!e) e = cudaMemcpyAsync(sc->d_tile_start, tile_start.data(), sizeof(int32_t) * (n_views + 1),
                                 cudaMemcpyHostToDevice, st);
     if (!e) e = cudaMemcpyAsync(sc->d_cams, cams4.data(), sizeof(double) * cams4.size(), cudaMemcpyHostToDevice, st);
-    if (!e) e = cudaStreamSynchronize(st);  // host vectors above go out of scope
+    // Callers of rcmvs_scene_create may release their views on return, so
+    // the uploads finish first.  run_mvs keeps its views until it returns
+    // and synchronises there, so its uploads overlap the host plan glue.
+    // (The pageable host vectors above are staged before their copies
+    // return.)
+    if (!e && !rgb_stream) e = cudaStreamSynchronize(st);
     if (e) {
+        if (rgb_stream) cudaStreamSynchronize(rgb_stream);  // no upload into a released buffer
         rcmvs_scene_destroy(sc);
         return fail(ctx, RCMVS_E_CUDA, std::string("rcmvs_scene_create: ") + cudaGetErrorString(e));
     }
     int rc = rcmvs_scene_prepare(ctx, sc);
     if (rc) {
+        if (rgb_stream) cudaStreamSynchronize(rgb_stream);
         rcmvs_scene_destroy(sc);
         return rc;
     }
@@ -1285,18 +1316,32 @@ static int run_mvs_impl(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views
     CK(cudaEventCreate(&e2));
     CK(cudaEventCreate(&e3));
     const int n = n_views;
+    rcmvs_scene* sc = nullptr;
+    CK(cudaEventRecord(e0, ctx->stream));
+    // the RGB uploads (three quarters of the input bytes) overlap the
+    // stereo: only fusion reads them
+    if (!ctx->upload) CK(cudaStreamCreateWithFlags(&ctx->upload, cudaStreamNonBlocking));
+    cudaEvent_t rgb_done;
+    CK(cudaEventCreateWithFlags(&rgb_done, cudaEventDisableTiming));
+    int rc = scene_create(ctx, views, n, &sc, ctx->upload, rgb_done);
+    if (rc) {
+        cudaEventDestroy(rgb_done);
+        return rc;
+    }
+    // the plan glue runs on the host while the uploads and the census run
     std::vector<int32_t> so(n + 1), ss((size_t)n * std::max<uint32_t>(opts->num_sources, 1u)), fo(n + 1),
         ff((size_t)n * n);
     std::vector<double> zr(2 * n);
-    int rc = rcmvs_plan(sparse, views, n, opts, so.data(), ss.data(), zr.data(), fo.data(), ff.data());
-    if (rc) return fail(ctx, rc, "plan failed");
     std::vector<rcmvs_job> jobs;
+    rc = rcmvs_plan(sparse, views, n, opts, so.data(), ss.data(), zr.data(), fo.data(), ff.data());
+    if (rc) {
+        cudaEventSynchronize(rgb_done);
+        cudaEventDestroy(rgb_done);
+        rcmvs_scene_destroy(sc);
+        return fail(ctx, rc, "plan failed");
+    }
     for (int i = 0; i < n; ++i)
         if (so[i + 1] > so[i]) jobs.push_back(rcmvs_job{i, so[i + 1] - so[i], ss.data() + so[i], zr[2 * i], zr[2 * i + 1]});
-    rcmvs_scene* sc = nullptr;
-    CK(cudaEventRecord(e0, ctx->stream));
-    rc = rcmvs_scene_create(ctx, views, n, &sc);
-    if (rc) return rc;
     auto body = [&]() -> int {
         CK(cudaEventRecord(e1, ctx->stream));
         int r = net ? rcmvs_scene_estimate_depth_learned(ctx, sc, jobs.data(), (int32_t)jobs.size(), opts, net,
@@ -1304,6 +1349,7 @@ static int run_mvs_impl(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views
                     : rcmvs_scene_estimate_depth(ctx, sc, jobs.data(), (int32_t)jobs.size(), opts);
         if (r) return r;
         CK(cudaEventRecord(e2, ctx->stream));
+        CK(cudaStreamWaitEvent(ctx->stream, rgb_done, 0));
         uint64_t np = 0;
         r = rcmvs_scene_fuse(ctx, sc, fo.data(), ff.data(), sparse->xyz, sparse->n_points, opts, &np);
         if (r) return r;
@@ -1347,6 +1393,8 @@ static int run_mvs_impl(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views
         return RCMVS_OK;
     };
     rc = body();
+    cudaEventSynchronize(rgb_done);  // the uploads read the caller's views and write the scene
+    cudaEventDestroy(rgb_done);
     rcmvs_scene_destroy(sc);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

@@ -18,6 +18,9 @@ constexpr int kSceneBig = 15;
 struct rcmvs_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
+    // rcmvs_run_mvs*: the views' RGB uploads run here, beside the stereo on
+    // `stream` (RGB is read by fusion only); created on first use
+    cudaStream_t upload = nullptr;
     std::string err;
     DeviceArena arena;
     bool count_work = false;
