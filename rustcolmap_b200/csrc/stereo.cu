@@ -1336,8 +1336,12 @@ __global__ void __launch_bounds__(256)
 constexpr int LT_SLOTS = 72;
 constexpr int LT_ENTRIES = 2624;
 
+// 64 registers (4 blocks of 256 threads; with the default 8x8 tiles, 16
+// blocks = 32 warps per SM): on the 1920x1080 K=10 workload 164 -> 152 ms
+// per step against 80 registers, whose 24 resident warps per SM left this
+// latency-bound kernel short of warps; the few extra spills cost less.
 template <bool PERSIST>
-__global__ void __launch_bounds__(256, 3)
+__global__ void __launch_bounds__(256, 4)
     init_learned_rows_kernel(const DevJob* __restrict__ jobs, const int32_t* __restrict__ job_start, int n_jobs,
                              int tiles, unsigned int* queue, int nh, const uint64_t* __restrict__ census,
                              const float2* __restrict__ rays, PlaneBuf out, const float* __restrict__ pred,
