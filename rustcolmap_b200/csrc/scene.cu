@@ -316,7 +316,7 @@ extern "C" int rcscene_render(const rcscene_prim* prims, int32_t n_prims, const 
         return 0;
     }
 #ifndef __CUDACC__
-    g_err = "rcscene_render: this build renders on the host only (device = -1)";
+    g_err = "rcscene_render: the host-only library renders on the host only (device = -1)";
     return -1;
 #else
     int rc = 0;
