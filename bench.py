@@ -207,10 +207,11 @@ def pinned_views(views):
 
 
 def cpu_rows(args):
-    """Rows of the CPU band: --cpu-rows, else eight per host thread (the
-    oracle threads over rows, so every thread gets work; at 1920 wide, K=10,
-    12 passes that is about 10 s of CPU work per sample)."""
-    return args.cpu_rows or 8 * (os.cpu_count() or 1)
+    """Rows of the CPU band: --cpu-rows, else sixteen per host thread (the
+    oracle threads over rows, so every thread gets work and the rows' uneven
+    costs even out; at 1920 wide, K=10, 12 passes that is about 10 s of CPU
+    work per sample)."""
+    return args.cpu_rows or 16 * (os.cpu_count() or 1)
 
 
 def cpu_baseline(sc, opts, jobs, rows, threads=0):
@@ -560,7 +561,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c5", choices=["c5", "c3", "c2", "c1", "sfm"])
     ap.add_argument("--cpu-rows", type=int, default=0,
-                    help="rows of the CPU band (cpu_baseline and --impl reference; default 8 per host thread)")
+                    help="rows of the CPU band (cpu_baseline and --impl reference; default 16 per host thread)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--views", type=int, default=0, help="override the number of views (profiling runs)")
