@@ -750,6 +750,10 @@ def main():
     if not args.no_cpu_baseline and rank == 0 and ws == 1:
         rate, dt, desc, nt = cpu_baseline(sc, opts, jobs, cpu_rows(args))
         cpu = {"value": rate, "unit": "depth maps/s", "cores": nt, "kind": "port", "sample": desc, "seconds": dt}
+        # the same port on one thread, on a smaller band (a few seconds)
+        rate1, dt1, desc1, _ = cpu_baseline(sc, opts, jobs, 4, threads=1)
+        cpu["single_thread"] = {"value": rate1, "unit": "depth maps/s", "cores": 1, "sample": desc1,
+                                "seconds": dt1}
 
     if rank == 0:
         n_pass = lambda o: o.passes if o.passes else 2 * max(o.sweeps, 1)

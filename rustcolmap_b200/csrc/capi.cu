@@ -250,6 +250,12 @@ void free_spare(rcmvs_ctx* ctx) {
     s.valid = false;
     s.cap_px = 0;
     s.cap_views = 0;
+    for (void*& p : s.quarter) {
+        if (p) cudaFree(p);
+        p = nullptr;
+    }
+    s.q_cap_px = 0;
+    s.q_cap_views = 0;
 }
 
 }  // namespace
@@ -264,11 +270,9 @@ void rcmvs_scene_destroy(rcmvs_scene* sc) {
         auto& live = sc->ctx->live;
         live.erase(std::remove(live.begin(), live.end(), sc), live.end());
     }
-    void* quarter[] = {sc->gray_q, sc->census_q, sc->rays_q, sc->d_qviews, sc->d_qtile_start, sc->d_qcams,
-                       sc->d_qblk_start};
+    void* quarter[7] = {sc->gray_q, sc->census_q, sc->rays_q, sc->d_qviews, sc->d_qtile_start, sc->d_qcams,
+                        sc->d_qblk_start};
     drop_graph(sc);
-    for (void* p : quarter)
-        if (p) cudaFree(p);
     if (sc->ctx && sc->cap_px > 0) {
         // keep the buffers for the context's next scene
         free_spare(sc->ctx);
@@ -280,7 +284,12 @@ void rcmvs_scene_destroy(rcmvs_scene* sc) {
         s.cap_px = sc->cap_px;
         s.cap_views = sc->cap_views;
         s.valid = true;
+        for (int i = 0; i < 7; ++i) s.quarter[i] = quarter[i];
+        s.q_cap_px = sc->q_cap_px;
+        s.q_cap_views = sc->q_cap_views;
     } else {
+        for (void* p : quarter)
+            if (p) cudaFree(p);
         for (int i = 0; i < kSceneBig; ++i)
             if (*scene_big(sc, i)) cudaFree(*scene_big(sc, i));
         for (int i = 0; i < 3; ++i)

@@ -51,6 +51,12 @@ struct rcmvs_ctx {
         void* big[kSceneBig] = {};
         void* small[3] = {};
         DeviceArena arena;
+        // the learned path's quarter-resolution buffers, in the order of
+        // rcmvs_scene's gray_q .. d_qblk_start, for scenes of at most
+        // q_cap_px quarter pixels and q_cap_views views
+        void* quarter[7] = {};
+        size_t q_cap_px = 0;
+        int q_cap_views = 0;
     } spare;
     // scenes created on this context and not yet destroyed; a context that
     // is destroyed first detaches them (they then free their own buffers)
@@ -145,6 +151,8 @@ struct rcmvs_scene {
     int32_t* d_qblk_start = nullptr;
     int qcensus_tiles = 0, qblocks = 0;
     int64_t nq_px = 0;
+    size_t q_cap_px = 0;  // capacity of the quarter buffers (pixels, views)
+    int q_cap_views = 0;
     // the last captured stereo schedule (RCMVS_FLAG_CUDA_GRAPH) and its key
     cudaGraphExec_t graph = nullptr;
     std::vector<unsigned char> graph_key;

@@ -296,13 +296,38 @@ int ensure_quarter(rcmvs_ctx* ctx, rcmvs_scene* sc) {
     sc->qcensus_tiles = nt;
     const size_t np = (size_t)std::max<int64_t>(off, 1);
     cudaStream_t st = ctx->stream;
-    LCK(cudaMalloc(&sc->gray_q, np));
-    LCK(cudaMalloc(&sc->census_q, 8 * np));
-    LCK(cudaMalloc(&sc->rays_q, 8 * np));
-    LCK(cudaMalloc(&sc->d_qviews, sizeof(DevView) * q.size()));
-    LCK(cudaMalloc(&sc->d_qtile_start, sizeof(int32_t) * tiles.size()));
-    LCK(cudaMalloc(&sc->d_qblk_start, sizeof(int32_t) * blk.size()));
-    LCK(cudaMalloc(&sc->d_qcams, sizeof(double) * cams.size()));
+    rcmvs_ctx::SpareScene& sp = ctx->spare;
+    const int nq = (int)q.size();
+    // in the order of SpareScene::quarter
+    void** qp[7] = {(void**)&sc->gray_q,      (void**)&sc->census_q, (void**)&sc->rays_q,
+                    (void**)&sc->d_qviews,    (void**)&sc->d_qtile_start, (void**)&sc->d_qcams,
+                    (void**)&sc->d_qblk_start};
+    for (void** p : qp) {  // what a failed earlier attempt left
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+    }
+    if (sp.quarter[0] && sp.q_cap_px >= np && sp.q_cap_views >= nq) {
+        // the last destroyed scene's quarter buffers (every one is written
+        // below or by the quarter census before it is read)
+        for (int i = 0; i < 7; ++i) {
+            *qp[i] = sp.quarter[i];
+            sp.quarter[i] = nullptr;
+        }
+        sc->q_cap_px = sp.q_cap_px;
+        sc->q_cap_views = sp.q_cap_views;
+        sp.q_cap_px = 0;
+        sp.q_cap_views = 0;
+    } else {
+        LCK(cudaMalloc(&sc->gray_q, np));
+        LCK(cudaMalloc(&sc->census_q, 8 * np));
+        LCK(cudaMalloc(&sc->rays_q, 8 * np));
+        LCK(cudaMalloc(&sc->d_qviews, sizeof(DevView) * q.size()));
+        LCK(cudaMalloc(&sc->d_qtile_start, sizeof(int32_t) * tiles.size()));
+        LCK(cudaMalloc(&sc->d_qblk_start, sizeof(int32_t) * blk.size()));
+        LCK(cudaMalloc(&sc->d_qcams, sizeof(double) * cams.size()));
+        sc->q_cap_px = np;
+        sc->q_cap_views = nq;
+    }
     LCK(cudaMemcpyAsync(sc->d_qviews, q.data(), sizeof(DevView) * q.size(), cudaMemcpyHostToDevice, st));
     LCK(cudaMemcpyAsync(sc->d_qtile_start, tiles.data(), sizeof(int32_t) * tiles.size(), cudaMemcpyHostToDevice, st));
     LCK(cudaMemcpyAsync(sc->d_qblk_start, blk.data(), sizeof(int32_t) * blk.size(), cudaMemcpyHostToDevice, st));

@@ -429,6 +429,42 @@ def test_seeded_oracle_selects_the_gated_proposals():
 
 
 @pytest.mark.gpu
+def test_learned_scene_adopts_a_larger_scenes_buffers():
+    """A context keeps a destroyed scene's buffers, the learned path's
+    quarter-resolution copies included, and the next scene that fits adopts
+    them instead of allocating.  A smaller scene run after a larger one on
+    one context gives the same maps, bit for bit, as on a fresh context."""
+    import dataclasses
+    small = _seeded_scene()
+    big = scene.orbit_room(seed=6004, n_views=8, sizes=((640, 480),), f_rel=1.1, n_boxes=20, n_spheres=0,
+                           device=0, per_view_sparse=300, arc_deg=60.0)
+    opts = MvsOptions(max_dim=4096, num_sources=4, sweeps=2, num_hyp=64)
+    lopts = dataclasses.replace(opts, passes=learned.LEARNED_PASSES, cost_thr=learned.LEARNED_COST_THR)
+    maps = []
+    for first in (None, big):
+        c = mvs.Context(0)
+        net = learned.ProposalNet(c, params=learned.load_weights())
+        if first is not None:
+            s, z, _ = mvs.plan(first.sparse, first.views, opts)
+            ds = mvs.DeviceScene(first.views, c)
+            learned.estimate_learned(ds, [(i, s[i], z[i, 0], z[i, 1]) for i in range(3) if s[i]], lopts, net)
+            ds.close()  # its buffers stay with the context
+        s, z, _ = mvs.plan(small.sparse, small.views, opts)
+        jobs = [(i, s[i], z[i, 0], z[i, 1]) for i in (1, 4, 6) if s[i]]
+        ds = mvs.DeviceScene(small.views, c)
+        n = learned.estimate_learned(ds, jobs, lopts, net)
+        maps.append((n, [ds.depth(j[0], normals=True) for j in jobs]))
+        ds.close()
+        net.close()
+        c.close()
+    assert maps[0][0] == maps[1][0] > 0
+    for a, b in zip(maps[0][1], maps[1][1]):
+        assert np.array_equal(a.depth.view(np.uint32), b.depth.view(np.uint32))
+        assert np.array_equal(a.cost.view(np.uint32), b.cost.view(np.uint32))
+        assert np.array_equal(a.normal.view(np.uint32), b.normal.view(np.uint32))
+
+
+@pytest.mark.gpu
 def test_committed_network_gains_over_the_plain_method(ctx):
     """The committed weights on eight held-out config-4 scenes (seeds
     6000-6007, outside the training seeds 1000-1799 and the tuning seeds
