@@ -355,7 +355,10 @@ int rcmvs_plan(const rcmvs_sparse* sparse, const rcmvs_view* views, int32_t n_vi
  * decoding and without writing files: plan, batched stereo for every view
  * with sources, fusion.  depth_outs (nullable, n_views entries) receive the
  * depth maps; views without sources get depth 0 / cost 1.  `out` receives
- * the fused cloud; stats (nullable) the run statistics. */
+ * the fused cloud; stats (nullable) the run statistics.  The call is
+ * synchronous: the views' buffers are read until it returns (their RGB is
+ * uploaded on a second stream of the context, beside the stereo) and all
+ * of the call's GPU work has finished when it returns. */
 int rcmvs_run_mvs(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views,
                   const rcmvs_sparse* sparse, const rcmvs_options* opts,
                   const rcmvs_depth_out* depth_outs, rcmvs_points* out,
