@@ -416,9 +416,10 @@ static int scene_create(rcmvs_ctx* ctx, const rcmvs_view* views, int32_t n_views
     if (!e) e = cudaMemcpyAsync(sc->d_cams, cams4.data(), sizeof(double) * cams4.size(), cudaMemcpyHostToDevice, st);
     // Callers of rcmvs_scene_create may release their views on return, so
     // the uploads finish first.  run_mvs keeps its views until it returns
-    // and synchronises there, so its uploads overlap the host plan glue.
-    // (The pageable host vectors above are staged before their copies
-    // return.)
+    // and synchronises there, so its RGB uploads and the census overlap the
+    // host plan glue.  (A copy from the pageable host vectors above waits
+    // for the stream's earlier work, the grey uploads, and returns once its
+    // source has been staged.)
     if (!e && !rgb_stream) e = cudaStreamSynchronize(st);
     if (e) {
         if (rgb_stream) cudaStreamSynchronize(rgb_stream);  // no upload into a released buffer
