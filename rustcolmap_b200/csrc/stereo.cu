@@ -567,7 +567,8 @@ __global__ void __maxnreg__(72)
 //   2. evaluation: every lane advances its own candidate by one window row
 //      per loop iteration; a lane whose candidate ends starts the pixel's
 //      next one, and a lane whose pixel ends writes it (if a candidate beat
-//      its cost) and claims the next unclaimed pixel of the tile.
+//      its cost) and claims the next unclaimed pixel of the tile (pixels
+//      with the most candidates first; those with none are not claimed).
 // Each pixel still meets its candidates, hints, rejection bounds and
 // best-cost updates in the reference's order, so every output bit (and each
 // work counter) is pass_kernel's.  Support-view parameters live field-major
